@@ -1,0 +1,368 @@
+#!/usr/bin/env python
+"""bench.py — particle-substeps/s of the Particles4All simulation step on B200.
+
+One step = Sim.step(1/60) of the workload (2 substeps: grid sort, k PBF
+iterations, rigid shape matching, XSPH, surface tension, finalize, stats) plus
+the anisotropic-kernel pass the renderer runs per frame. Default workload: the
+medium scene with rigid bodies (medium_bodies_264k: 262,144 fluid particles +
+8 cubes of 216, tension, XSPH, anisotropic pass).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference ...   # the reference's algorithm on the host cores
+
+Multi-GPU: scenes are independent, so N GPUs run N replicas (weak scaling); no
+data-path collective. Device time is measured with CUDA events on the
+simulation's stream, max over ranks. Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "particle-substeps/s"
+L2_FLUSH_BYTES = 256 << 20
+# Algorithmic bytes per particle and launch (fixed formula of the workload
+# definition: neighbour re-reads are not counted).
+ALGO_BYTES = {
+    "key_count": 36,        # R pos, vel; W key
+    "reorder": 84,          # R key, pos, vel; W pos, vel, pred   (+64 with bodies)
+    "lambda": 24,           # R pred; W density, lambda
+    "delta": 36,            # R pred, lambda; W pred
+    "xsph_finalize": 68,    # R pos, pred, density; W vel, pos
+    "xsph_normals": 56,     # tension scenes: the extra normal pass (R pred, vel, rho; W corr, normal)
+    "tension_finalize": 68,
+    "aniso": 64,            # R pos; W smoothPos, G
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="medium_bodies_264k")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def workload(name):
+    from particles4all_b200 import configs
+    params, scene = configs.WORKLOADS[name]()
+    aniso = configs.medium_aniso_params() if name.startswith("medium") else None
+    return params, scene, aniso
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def committed_traffic(kernel, wl):
+    """DRAM bytes per launch from the committed ncu summary of this kernel and workload."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{wl}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1].split()[0]))
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.lines, self.proc = gpu, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "50",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.time(), line.strip()))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self, t0, t1):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for ts, line in self.lines:
+            if not (t0 <= ts <= t1 + 0.05):
+                continue
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 10:
+                continue
+            try:
+                sm.append(float(f[2])); mx.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[6:10]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(params, scene, aniso, seconds):
+    """The oracle (a CPU restatement of the reference's passes) on this workload."""
+    import oracle
+    o = oracle.OracleSim()
+    o.reset_scene(params, scene)
+    n = o.info()["n"]
+    subs = 0
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        subs += o.step(1 / 60)
+        if aniso:
+            o.aniso(aniso)
+        steps += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": n * subs / el, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
+            "sample": f"{steps} full steps ({subs} substeps{' + anisotropic pass' if aniso else ''}) "
+                      f"of the same {n}-particle scene in {el:.1f} s"}
+
+
+def run_reference(args):
+    rank, _, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    params, scene, aniso = workload(args.workload)
+    o = oracle.OracleSim()
+    o.reset_scene(params, scene)
+    n = o.info()["n"]
+    base = max(1, params["substeps"])
+    # a step is the full frame, or one substep of it when K frames would not fit
+    t0 = time.perf_counter()
+    o.step(1 / 60)
+    if aniso:
+        o.aniso(aniso)
+    frame_s = time.perf_counter() - t0
+    frame = frame_s * (args.steps + args.warmup) <= 150.0
+    dt = 1 / 60 if frame else (1 / 60) / base
+
+    def one():
+        s = o.step(dt)
+        if aniso and frame:
+            o.aniso(aniso)
+        return s
+    for _ in range(max(0, args.warmup - 1)):
+        one()
+    subs = 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        subs += one()
+    el = time.perf_counter() - t0
+    value = n * subs / el
+    sample = (f"{'full frames' if frame else 'single substeps'} of the {n}-particle scene, "
+              f"{subs} substeps timed, all host threads")
+    line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el * 1000 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": args.workload, "n_particles": n, "substeps_per_step": subs // max(1, args.steps)},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from particles4all_b200 import Sim, _lib
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def allmax(x):
+        if not pg:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    params, scene, aniso = workload(args.workload)
+    stream = torch.cuda.Stream()
+    sim = Sim(device=local)
+    sim.set_stream(stream.cuda_stream)
+    sim.reset_scene(params, scene)
+    n = sim.info()["n"]
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    def frame():
+        s = sim.step(1 / 60)
+        if aniso:
+            sim.aniso(aniso)
+        return s
+
+    for _ in range(max(3, args.warmup)):
+        frame()
+    sim.synchronize()
+    sim.profile(True)
+    sim.profile_reset()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = _lib.lib().p4a_kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    w0 = time.time()
+    subs = 0
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed steps (not inside the events)
+            starts[k].record(stream)
+            subs += frame()
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    w1 = time.time()
+    launches = _lib.lib().p4a_kernel_launches() - launches0
+    clocks.stop()
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    kern = sim.profile_read()
+    sim.profile(False)
+    dev_ms_max = allmax(dev_ms)
+    value = world * n * subs / (dev_ms_max / 1000.0)
+
+    # roofline of the dominant kernel (live per-kernel events of the timed region)
+    top = max(kern.items(), key=lambda kv: kv[1][0])
+    name, (kms, kl) = top
+    per_p = ALGO_BYTES.get(name, 0) + (64 if name == "reorder" and sim.info()["n_bodies"] else 0)
+    avg_s = kms / kl / 1000.0
+    algo = per_p * n
+    peak, peak_kind = peaks()
+    achieved = algo / avg_s / 1e9
+    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": committed_traffic(name, args.workload),
+                "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
+                "avg_launch_us": avg_s * 1e6,
+                "kernels": {k: {"ms_total": round(v[0], 4), "launches": v[1],
+                                "share": round(v[0] / sum(x[0] for x in kern.values()), 4)}
+                            for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
+
+    # end to end through the public API: host state in, step, host state out
+    e2e = None
+    if not args.no_e2e:
+        L = _lib.lib()
+        h = sim._h
+        nbytes = n * 16
+        hp = torch.empty(max(1, n) * 4, dtype=torch.float32, pin_memory=True)
+        hv = torch.empty(max(1, n) * 4, dtype=torch.float32, pin_memory=True)
+        hs = torch.empty(8, dtype=torch.int32, pin_memory=True)
+        L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nbytes)
+        L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nbytes)
+        e_steps = max(3, min(args.steps, 50))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e_subs = 0
+        for _ in range(e_steps):
+            L.p4a_write(h, 0, -1, hp.data_ptr(), 0, nbytes)
+            L.p4a_write(h, 1, -1, hv.data_ptr(), 0, nbytes)
+            e_subs += frame()
+            L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nbytes)
+            L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nbytes)
+            L.p4a_read(h, 17, -1, hs.data_ptr(), 0, 32)
+        t1 = time.perf_counter()
+        barrier()
+        el = allmax(t1 - t0)
+        e2e = {"value": world * n * e_subs / el, "unit": METRIC, "h2d_bytes_per_step": 2 * nbytes,
+               "d2h_bytes_per_step": 2 * nbytes + 32, "steps": e_steps,
+               "what": "per step: live pos+vel written from pinned host, Sim.step + aniso, "
+                       "pos+vel+stats read back to pinned host"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(params, scene, aniso, args.cpu_seconds)
+
+    if rank == 0:
+        st = sim.get_stats()
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": dev_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "n_particles": n, "n_bodies": sim.info()["n_bodies"],
+                       "substeps_per_step": subs // args.steps, "iterations": params["iterations"],
+                       "surface_tension": params["surfaceTensionK"], "aniso_pass": bool(aniso),
+                       "l2": "flushed between timed steps (256 MiB write outside the timed events)",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary(w0, w1),
+            "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")},
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if pg:
+        barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

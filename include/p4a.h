@@ -1,0 +1,304 @@
+/*
+ * p4a.h — C ABI of the B200-native Particles4All simulation step.
+ *
+ * This is the drop-in boundary for the reference's `class Sim` (src/sim.js:9-814):
+ * scene setup (`reset`), the substep loop (`step`), the interactive calls
+ * (`appendFluid`, `applyRayImpulse`, `holdBody`, `releaseBody`, `resizeBox`) and
+ * the device buffers the renderers read (`buf.*`, `livePos/liveVel/liveBody`).
+ * The anisotropic-kernel pass that src/mesh.js:207-261 dispatches on the
+ * simulation's buffers is exposed as p4a_aniso().
+ *
+ * Conventions
+ *  - Every call returns an int status (P4A_OK == 0). The reference has no
+ *    exceptions (device errors are asynchronous, src/main.js:217); here the
+ *    last error text of a handle is available from p4a_last_error().
+ *  - Plain pointers and sizes only. "device pointer" means CUDA global memory on
+ *    the handle's device; "host pointer" means ordinary (pageable or pinned)
+ *    host memory.
+ *  - A handle owns all its device memory. Pointers returned by p4a_buffer()
+ *    stay valid until the next p4a_reset / p4a_reset_scene / p4a_resize_box /
+ *    p4a_append_fluid beyond capacity / p4a_destroy; `gen` in p4a_info
+ *    increments whenever that happens (src/sim.js:73, 740).
+ *  - Calls on one handle are not re-entrant. All device work of a handle is
+ *    issued on one CUDA stream (p4a_set_stream), in call order.
+ *  - Particle arrays are float4 / uint4 per particle, in cell-sorted order,
+ *    ping-ponged between an A and a B copy selected by `parity`, exactly as
+ *    the reference lays them out (src/sim.js:98-101, 811-813).
+ */
+#ifndef P4A_H
+#define P4A_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define P4A_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  P4A_OK = 0,
+  P4A_ERR_ARG = 1,       /* invalid argument                                   */
+  P4A_ERR_OOM = 2,       /* device or pinned host allocation failed            */
+  P4A_ERR_CUDA = 3,      /* a CUDA runtime call failed                         */
+  P4A_ERR_TIMEOUT = 4,   /* a bounded device-side wait gave up                 */
+  P4A_ERR_CAPACITY = 5,  /* a size is beyond the handle's or entry's capacity  */
+  P4A_ERR_STATE = 6,     /* call not valid in the current state (e.g. no reset)*/
+  P4A_ERR_NODEV = 7      /* no CUDA device / extension unavailable             */
+};
+
+/* ---- body shapes (src/scene.js:137-157) -------------------------------- */
+enum { P4A_SHAPE_SPHERE = 0, P4A_SHAPE_TORUS = 1, P4A_SHAPE_BOX = 2 };
+
+/* One entry of params.bodies: "shape:density:startY" (src/scene.js:167-171). */
+typedef struct p4a_body_spec {
+  int32_t shape;     /* P4A_SHAPE_*                                            */
+  double density;    /* body density / fluid density, default 0.5              */
+  double start_y;    /* centre height as a fraction of box[1], default 0.75   */
+} p4a_body_spec;
+
+/*
+ * Scene and solver parameters: the reference's `params` object
+ * (defaultParams, src/scene.js:11-39, plus the keys main.js sets:
+ * noBoundary src/main.js:380, pour src/sim.js:94). JS numbers are doubles, so
+ * the real-valued fields are double; the library rounds them to float where
+ * the reference's uniform upload does (src/sim.js:371-413).
+ */
+typedef struct p4a_params {
+  double spacing;                /* d, default 0.02                                 */
+  double rest_density;           /* rho0, default 1000                              */
+  double gravity;                /* default 9.81                                    */
+  int32_t substeps;              /* default 4                                       */
+  int32_t iterations;            /* Jacobi iterations k, default 4                  */
+  double cfm_epsilon_rel;        /* default 0.01 (cfmEps = rel * denomRest)         */
+  double s_corr_k;               /* default 0.1                                     */
+  double s_corr_dq;              /* default 0.3                                     */
+  double xsph_c;                 /* default 0.05                                    */
+  double omega;                  /* default 1.0                                     */
+  int32_t sor_average;           /* default 0                                       */
+  double surface_tension_k;      /* default 0 (tension off)                         */
+  int32_t target_particle_count; /* default 60000                                   */
+  double box[3];                 /* default {1.5, 1.5, 1.0}                         */
+  int32_t n_bodies;              /* entries used in `bodies`                        */
+  const p4a_body_spec* bodies;   /* may be NULL when n_bodies == 0                  */
+  double body_size;              /* 0 = 0.12 * min(box)                             */
+  int32_t no_boundary;           /* 1 = skip the boundary samples in the solver     */
+  int32_t pour;                  /* 1 = reserve capacity nFluid for appendFluid     */
+  /* Extension, no counterpart in the reference: when > 0 it replaces
+   * cfm_epsilon_rel * denomRest as the absolute CFM epsilon.                 */
+  double cfm_epsilon_abs;
+} p4a_params;
+
+/*
+ * An explicit initial scene (what buildScene returns, src/scene.js:313-314),
+ * for scenes that are not the reference's own fluid block + bodies. Arrays are
+ * HOST pointers. phase[4*i] is the 1-based body id (0 = fluid); bodies must
+ * have at least one particle each. When mass <= 0 the mass is calibrated from
+ * the fluid particles as src/scene.js:277-288 does; when denom_rest <= 0 it is
+ * computed as src/scene.js:289-311 does.
+ */
+typedef struct p4a_scene_desc {
+  int32_t n;                 /* particles                                          */
+  const float* pos;          /* float4[n]                                          */
+  const float* vel;          /* float4[n], may be NULL (zero)                      */
+  const uint32_t* phase;     /* uint4[n],  may be NULL (all fluid)                 */
+  const float* rest;         /* float4[n], may be NULL (zero)                      */
+  int32_t n_bodies;
+  const double* body_density;  /* [n_bodies]                                       */
+  const double* body_centre;   /* [3*n_bodies] initial centre of mass              */
+  double mass;
+  double denom_rest;
+  int32_t pour_budget;       /* extra capacity reserved for p4a_append_fluid       */
+} p4a_scene_desc;
+
+/* Read-only fields the reference's callers read from a Sim (src/sim.js). */
+typedef struct p4a_info {
+  int32_t n, n_fluid, n_body_parts, n_bodies, n_boundary;
+  int32_t cap, pour_budget;
+  int32_t grid_dim[3];
+  int32_t n_cells;
+  int32_t parity, pred_parity;
+  int32_t gen;
+  int32_t last_substeps;
+  double h, mass, denom_rest;
+  double sim_time, last_advanced, time_bank;
+  double body_scale, cov_scale;
+  int32_t held_body;
+  int32_t aniso_gen;
+} p4a_info;
+
+/* Sim.stats after the fixed-point readback (src/sim.js:619-633). */
+typedef struct p4a_stats {
+  double avg_rho, max_rho, max_speed, ke;
+  uint32_t raw[4];    /* statsOut[0..3] as the device wrote them */
+  int32_t valid;      /* 0 until the first step completed         */
+} p4a_stats;
+
+/* Anisotropic kernel parameters (SurfaceMesh fields, src/mesh.js:81-89, and
+ * the uniform packing at src/mesh.js:221-242). */
+typedef struct p4a_aniso_params {
+  double ratio;           /* anisoRatio  k_r, default 4.0          */
+  double ks;              /* anisoKs,         default 1.0          */
+  double stretch;         /* anisoStretch,    default 2.0          */
+  double lonely;          /* anisoLonely  k_n,default 1.0          */
+  int32_t min_neighbours; /* anisoMinNeighbours N_eps, default 25  */
+  double lambda;          /* anisoLambda,     default 0.9          */
+  double radius_scale;    /* anisoRadiusScale,default 2.0          */
+  double min_extent;      /* F[16]: 1.25*voxel/h, or 0             */
+} p4a_aniso_params;
+
+/* Buffer ids for p4a_buffer / p4a_read / p4a_write (src/sim.js:98-161). */
+enum {
+  P4A_BUF_POS = 0,        /* float4[cap], A/B      */
+  P4A_BUF_VEL = 1,        /* float4[cap], A/B      */
+  P4A_BUF_PRED = 2,       /* float4[cap], A/B      */
+  P4A_BUF_BODY = 3,       /* uint4[cap],  A/B      */
+  P4A_BUF_REST = 4,       /* float4[cap], A/B      */
+  P4A_BUF_DENSITY = 5,    /* float[cap]            */
+  P4A_BUF_LAMBDA = 6,     /* float[cap]            */
+  P4A_BUF_CORR = 7,       /* float4[cap]           */
+  P4A_BUF_NORMAL = 8,     /* float4[cap]           */
+  P4A_BUF_CELL_START = 9, /* uint32[nCells+2]      */
+  P4A_BUF_BPOS = 10,      /* float4[max(1,nb)]     */
+  P4A_BUF_BPSI = 11,      /* float[max(1,nb)]      */
+  P4A_BUF_BCELL_START = 12, /* uint32[nCells+2]    */
+  P4A_BUF_BODY_CENTRE = 13, /* float4[max(1,B)]    */
+  P4A_BUF_BODY_REF = 14,    /* float4[max(1,B)]    */
+  P4A_BUF_BODY_ROT = 15,    /* float4[3*max(1,B)], row-major rows */
+  P4A_BUF_BODY_INFO = 16,   /* float4[max(1,B)], .x = 1/density   */
+  P4A_BUF_STATS_OUT = 17,   /* uint32[8]           */
+  P4A_BUF_SMOOTH_POS = 18,  /* float4[n] (aniso)   */
+  P4A_BUF_ANISO_G = 19,     /* float4[2n] (aniso)  */
+  P4A_BUF_COUNT = 20
+};
+/* `which` selector for A/B buffers. */
+enum { P4A_A = 0, P4A_B = 1, P4A_LIVE = -1 };
+
+/* ---- library ----------------------------------------------------------- */
+int p4a_abi_version(void);
+const char* p4a_status_string(int status);
+/* defaultParams(preset) (src/scene.js:11-39). `preset` is "small", "medium",
+ * "large" or "extreme" (src/scene.js:3-9); NULL or unknown = "small". The
+ * bodies array points at static storage of the library. */
+int p4a_default_params(const char* preset, p4a_params* out);
+/* Number of devices and whether the sm_100a kernels can run on `device`. */
+int p4a_device_check(int device);
+
+/* ---- lifetime (new Sim(device), src/sim.js:10-18) ----------------------- */
+typedef struct p4a_sim p4a_sim;
+int p4a_create(int device, p4a_sim** out);
+int p4a_destroy(p4a_sim* sim);
+const char* p4a_last_error(const p4a_sim* sim);
+/* Use `stream` (a cudaStream_t, NULL = the handle's own stream) for all work. */
+int p4a_set_stream(p4a_sim* sim, void* stream);
+int p4a_synchronize(p4a_sim* sim);
+
+/* ---- Sim.reset(params) (src/sim.js:66-221) ------------------------------ */
+int p4a_reset(p4a_sim* sim, const p4a_params* params);
+/* reset() on an explicit scene instead of buildScene(params); the remaining
+ * steps of src/sim.js:75-221 (grid, boundary, buffers, scales, prime) are the
+ * same. params.spacing, rest_density, box and solver fields are used. */
+int p4a_reset_scene(p4a_sim* sim, const p4a_params* params, const p4a_scene_desc* scene);
+
+/* ---- Sim.step(frameDt) (src/sim.js:415-656) ----------------------------- */
+int p4a_step(p4a_sim* sim, double frame_dt, int32_t* substeps_out);
+
+/* ---- interactive API --------------------------------------------------- */
+/* Sim.appendFluid(pos, vel) (src/sim.js:774-809): pos3/vel3 are HOST float3
+ * arrays of `count` entries; appends min(count, cap - n), stored in *added. */
+int p4a_append_fluid(p4a_sim* sim, const float* pos3, const float* vel3, int32_t count,
+                     int32_t* added);
+/* Sim.applyRayImpulse(origin, dir, impulse, radius, speedLimit) (src/sim.js:658-676). */
+int p4a_apply_ray_impulse(p4a_sim* sim, const double origin[3], const double dir[3],
+                          const double impulse[3], double radius, double speed_limit);
+/* Sim.holdBody(body1Based, target, rate, limit) / releaseBody (src/sim.js:678-685). */
+int p4a_hold_body(p4a_sim* sim, int32_t body_1based, const double target[3], double rate,
+                  double limit);
+int p4a_release_body(p4a_sim* sim);
+/* Sim.resizeBox(newBox) (src/sim.js:687-772). */
+int p4a_resize_box(p4a_sim* sim, const double box[3]);
+
+/* ---- fields and buffers ------------------------------------------------ */
+int p4a_get_info(const p4a_sim* sim, p4a_info* out);
+/* Device pointer and byte size of a buffer. `which` = P4A_A, P4A_B or
+ * P4A_LIVE (the `parity` copy, as livePos/liveVel/liveBody, src/sim.js:811-813);
+ * ignored for single buffers. */
+int p4a_buffer(p4a_sim* sim, int32_t id, int32_t which, void** dptr, size_t* bytes);
+/* Synchronous copies between a buffer and host memory (the reference's
+ * copyBufferToBuffer + mapAsync readback, src/main.js:841-852). */
+int p4a_read(p4a_sim* sim, int32_t id, int32_t which, void* host, size_t offset, size_t bytes);
+int p4a_write(p4a_sim* sim, int32_t id, int32_t which, const void* host, size_t offset,
+              size_t bytes);
+/* Sim.stats (src/sim.js:619-633). wait = 0: latest completed readback, as the
+ * reference's async mapAsync; wait = 1: block until the last step's stats. */
+int p4a_get_stats(p4a_sim* sim, int32_t wait, p4a_stats* out);
+/* Sim.bodyPose (src/sim.js:635-655): centre3[3*i], rot9[9*i] column-major. */
+int p4a_body_pose(p4a_sim* sim, int32_t wait, float* centre3, float* rot9, int32_t max_bodies);
+
+/* ---- anisotropic kernel (src/aniso_wgsl.js:3-158, src/mesh.js:207-261) -- */
+/* Runs on the live pos and the current cellStart; results in
+ * P4A_BUF_SMOOTH_POS (float4[n], .w = 0) and P4A_BUF_ANISO_G (float4[2n]:
+ * (G00,G10,G20,G11), (G21,G22,det G,n)). */
+int p4a_aniso(p4a_sim* sim, const p4a_aniso_params* params);
+int p4a_default_aniso_params(p4a_aniso_params* out);
+
+/* ---- GPU timing (the reference's GpuTimer, src/gputimer.js; phase marks
+ * src/sim.js:460-599) --------------------------------------------------- */
+/* With profiling on, every kernel the handle launches is bracketed by CUDA
+ * events on its stream; p4a_profile_read synchronizes and returns, per kernel
+ * name, the accumulated device milliseconds and launch count since the last
+ * p4a_profile_reset. */
+typedef struct p4a_phase_time {
+  char name[24];
+  double ms;
+  int64_t launches;
+} p4a_phase_time;
+int p4a_profile_enable(p4a_sim* sim, int32_t on);
+int p4a_profile_reset(p4a_sim* sim);
+int p4a_profile_read(p4a_sim* sim, p4a_phase_time* out, int32_t max_entries, int32_t* count);
+/* Extension, no counterpart in the reference: kernels launched by this
+ * library in this process (all handles and operator entries). */
+uint64_t p4a_kernel_launches(void);
+
+/* ---- operator entry: predict + grid pass as one call ------------------- */
+/*
+ * The predict pass and the 'grid' pass of Sim.step (src/wgsl.js:56-70,
+ * 352-475; schedule src/sim.js:473-489) on caller-owned DEVICE buffers:
+ * v = vel + dt*(0,-gravity,0), pred = pos + dt*v, then a counting sort of the
+ * particles by cell key (cellIndex(cellOf(pred)), src/wgsl.js:43-49). The sort
+ * is stable: particles of one cell keep their input order.
+ *   pos, vel            float4[n] in
+ *   body, rest          uint4/float4[n] in, may be NULL (then *_out ignored)
+ *   pos_out ... rest_out  outputs in sorted order (vel_out = (v,0), pred_out = (pred,1))
+ *   cell_start          uint32[n_cells+1] out: exclusive scan of cell counts, [n_cells] = n
+ *   slot_out            uint32[n] out (may be NULL): sorted position of input i
+ *   workspace           device scratch of p4a_grid_sort_workspace_size() bytes
+ */
+typedef struct p4a_grid {
+  float box_min[3];
+  float h;
+  int32_t dim[3];
+} p4a_grid;
+size_t p4a_grid_sort_workspace_size(int32_t n, int32_t n_cells);
+int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity,
+                  const float* pos, const float* vel, const uint32_t* body, const float* rest,
+                  float* pos_out, float* vel_out, float* pred_out, uint32_t* body_out,
+                  float* rest_out, uint32_t* cell_start, uint32_t* slot_out, void* workspace,
+                  size_t workspace_bytes, void* stream);
+
+/* ---- host-side scene builder (src/scene.js:159-315) --------------------- */
+/* buildScene(params) into caller-provided host arrays; call once with NULL
+ * arrays to get the counts. pos/vel/rest float4[n], phase uint4[n]. */
+typedef struct p4a_scene_counts {
+  int32_t n, n_fluid, n_body, n_bodies, n_boundary;
+  double mass, denom_rest, h;
+} p4a_scene_counts;
+int p4a_build_scene(const p4a_params* params, p4a_scene_counts* counts, float* pos, float* vel,
+                    float* rest, uint32_t* phase, double* body_centre, double* body_density);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* P4A_H */

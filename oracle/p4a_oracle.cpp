@@ -1,0 +1,1605 @@
+// p4a_oracle.cpp — CPU restatement of the Particles4All simulation step.
+//
+// TEST INFRASTRUCTURE (the checker and the timed CPU baseline), never the product.
+// PARITY UNPINNED: the reference cannot run here and ships no golden vectors; see
+// p4a_oracle.h for what pins this restatement instead.
+//
+// Structure mirrors the reference one pass at a time, in the reference's schedule:
+//   scene setup        src/scene.js:41-315
+//   Sim.reset / prime  src/sim.js:66-286
+//   uniform packing    src/sim.js:371-413   (Params layout src/wgsl.js:4-40)
+//   Sim.step           src/sim.js:415-656
+//   passes             src/wgsl.js:43-832
+//   anisotropic pass   src/aniso_wgsl.js:3-158 with params src/mesh.js:207-242
+// Build with -ffp-contract=off: the only fused multiply-adds are the explicit fmaf
+// calls of the arithmetic contract (p4a_oracle.h).
+#include "p4a_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+struct f4 { float x, y, z, w; };
+struct u4 { uint32_t x, y, z, w; };
+struct f3 { float x, y, z; };
+
+const double kPI = 3.14159265358979323846;  // Math.PI
+
+inline f3 xyz(const f4& v) { return {v.x, v.y, v.z}; }
+inline f3 sub3(f3 a, f3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline f3 add3(f3 a, f3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline f3 mul3(f3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline float dot3(f3 a, f3 b) { return std::fmaf(a.z, b.z, std::fmaf(a.y, b.y, a.x * b.x)); }
+inline f3 fma3(float s, f3 v, f3 acc) {
+  return {std::fmaf(s, v.x, acc.x), std::fmaf(s, v.y, acc.y), std::fmaf(s, v.z, acc.z)};
+}
+inline f3 cross3(f3 b, f3 c) {
+  return {b.y * c.z - b.z * c.y, b.z * c.x - b.x * c.z, b.x * c.y - b.y * c.x};
+}
+inline float length3(f3 a) { return std::sqrt(dot3(a, a)); }
+
+// f32 -> i32 with the semantics of the GPU's cvt.rzi / cvt.rni (saturating, NaN -> 0).
+inline int32_t f2i_sat(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT32_MAX;
+  if (f <= -2147483648.0f) return INT32_MIN;
+  return (int32_t)f;
+}
+inline uint32_t f2u_sat(float f) {
+  if (!(f > 0.0f)) return 0u;
+  if (f >= 4294967296.0f) return UINT32_MAX;
+  return (uint32_t)f;
+}
+// i32(round(x)) of WGSL: round half to even, then the saturating conversion.
+inline int32_t round_i32(float x) { return f2i_sat(std::nearbyint(x)); }
+
+// Column-major 3x3 (m[c] is column c), as WGSL's mat3x3f.
+struct m3 { f3 c[3]; };
+inline m3 ident3() { return {{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}}; }
+inline float det3(const m3& a) { return dot3(a.c[0], cross3(a.c[1], a.c[2])); }
+inline f3 row3(const m3& a, int r) {
+  const float* c0 = &a.c[0].x; const float* c1 = &a.c[1].x; const float* c2 = &a.c[2].x;
+  return {c0[r], c1[r], c2[r]};
+}
+inline float& el(m3& a, int c, int r) { return (&a.c[c].x)[r]; }
+inline float elc(const m3& a, int c, int r) { return (&a.c[c].x)[r]; }
+inline m3 matmul(const m3& A, const m3& B) {  // (A*B)[c][r] = dot3(row r of A, col c of B)
+  m3 o;
+  for (int c = 0; c < 3; c++)
+    for (int r = 0; r < 3; r++) el(o, c, r) = dot3(row3(A, r), B.c[c]);
+  return o;
+}
+inline m3 transpose3(const m3& a) {
+  m3 o;
+  for (int c = 0; c < 3; c++)
+    for (int r = 0; r < 3; r++) el(o, c, r) = elc(a, r, c);
+  return o;
+}
+inline m3 scale3(const m3& a, float s) {
+  m3 o;
+  for (int c = 0; c < 3; c++) o.c[c] = mul3(a.c[c], s);
+  return o;
+}
+
+// Cube root by a fixed Newton iteration on the mantissa (x > 0, normal): the
+// rigid-body resolve's pow(|det|, 1/3) (src/wgsl.js:730). Only IEEE basic
+// operations, so every conforming float32 unit gives the same bits.
+float cbrt_newton(float x) {
+  if (!(x > 0.0f) || std::isinf(x)) return x;
+  uint32_t bits;
+  std::memcpy(&bits, &x, 4);
+  int e = (int)((bits >> 23) & 0xffu);
+  if (e == 0) return 0.0f;  // subnormal: not reached by the callers (|det| >= 1e-12)
+  e -= 127;
+  int q = (e + 300) / 3 - 100;  // floor(e / 3)
+  int r = e - 3 * q;            // 0, 1, 2
+  uint32_t mb = (bits & 0x7fffffu) | 0x3f800000u;
+  float m;
+  std::memcpy(&m, &mb, 4);
+  float t = m;  // [1, 2)
+  if (r >= 1) t = t * 2.0f;
+  if (r >= 2) t = t * 2.0f;  // t in [1, 8)
+  float y = 0.75f + 0.1666667f * t;
+  for (int it = 0; it < 5; it++) y = (2.0f * y + t / (y * y)) * 0.33333334f;
+  uint32_t sb = (uint32_t)(q + 127) << 23;
+  float s;
+  std::memcpy(&s, &sb, 4);
+  return y * s;
+}
+
+// The 192-byte uniform (src/wgsl.js:4-40) as float32 / int32.
+struct Params {
+  float boxMin[3]; float dt;
+  float boxMax[3]; float h;
+  int32_t gridDim[3]; float h2;
+  float clampMin[3]; float poly6;
+  float clampMax[3]; float spikyGrad;
+  float gravity, mass, rho0, invRho0;
+  float cfmEps, sCorrK, sCorrWq, xsphC;
+  uint32_t n, nCells, nBoundary, nBodyParts;
+  uint32_t nBodies; float bodyScale, covScale, omega;
+  uint32_t sorAverage; float invDt, volume, tension;
+  float cohes, cohesTerm;
+};
+
+int g_threads = 0;
+inline void apply_threads() {
+#ifdef _OPENMP
+  if (g_threads > 0) omp_set_num_threads(g_threads);
+#endif
+}
+
+// ---------------------------------------------------------------- scene.js
+struct Scene {
+  int n = 0, nFluid = 0, nBody = 0;
+  std::vector<float> pos, vel, rest;  // float4
+  std::vector<uint32_t> phase;        // uint4
+  std::vector<double> bodyCentre, bodyDensity;
+  std::vector<int> bodyCount;
+  double mass = 0, denomRest = 0, h = 0, d = 0;
+};
+
+inline double poly6Coef(double h) { return 315 / (64 * kPI * std::pow(h, 9)); }
+
+// fluidBlock (src/scene.js:43-64). The LCG runs in float64 like the JS, whose
+// seed*1103515245 is a rounded double product, then ToInt32 & 0x7fffffff.
+std::vector<double> fluidBlock(const p4a_params& p, double d) {
+  const double bx = p.box[0], by = p.box[1], bz = p.box[2];
+  const double margin = d;
+  const double nx = std::max(1.0, std::floor(bx * 0.35 / d));
+  const double nz = std::max(1.0, std::floor((bz - 2 * margin) / d));
+  const double maxLayers = std::max(1.0, std::floor((by - 2 * margin) / d));
+  const double target = p.target_particle_count;
+  const double layers = std::min(std::ceil(target / (nx * nz)), maxLayers);
+  std::vector<double> out;
+  double seed = 12345;
+  auto rnd = [&]() {
+    double s = seed * 1103515245.0 + 12345.0;
+    int64_t si = (int64_t)s;  // integral, |s| < 2^63
+    seed = (double)(int32_t)((uint32_t)si & 0x7fffffffu);
+    return (seed / 2147483647.0 - 0.5) * 0.002 * d;
+  };
+  for (double iy = 0; iy < layers && out.size() / 3 < target; iy++)
+    for (double ix = 0; ix < nx && out.size() / 3 < target; ix++)
+      for (double iz = 0; iz < nz && out.size() / 3 < target; iz++) {
+        double x = margin + (ix + 0.5) * d + rnd();
+        double y = margin + (iy + 0.5) * d + rnd();
+        double z = margin + (iz + 0.5) * d + rnd();
+        out.push_back(x); out.push_back(y); out.push_back(z);
+      }
+  return out;
+}
+
+// sampleBody (src/scene.js:137-157).
+std::vector<double> sampleBody(int shape, double size, double d) {
+  double ext[3];
+  if (shape == P4A_SHAPE_SPHERE) { ext[0] = ext[1] = ext[2] = size; }
+  else if (shape == P4A_SHAPE_TORUS) { ext[0] = size + 0.4 * size; ext[1] = 0.4 * size; ext[2] = size + 0.4 * size; }
+  else { ext[0] = size * 0.9; ext[1] = size * 0.7; ext[2] = size * 0.9; }
+  int steps[3];
+  for (int k = 0; k < 3; k++) steps[k] = (int)std::max(1.0, std::ceil(ext[k] / d));
+  std::vector<double> local;
+  for (int ix = -steps[0]; ix <= steps[0]; ix++)
+    for (int iy = -steps[1]; iy <= steps[1]; iy++)
+      for (int iz = -steps[2]; iz <= steps[2]; iz++) {
+        double x = ix * d, y = iy * d, z = iz * d;
+        bool inside;
+        if (shape == P4A_SHAPE_SPHERE) inside = x * x + y * y + z * z <= size * size;
+        else if (shape == P4A_SHAPE_TORUS) {
+          double planar = std::sqrt(x * x + z * z) - size;
+          inside = planar * planar + y * y <= (0.4 * size) * (0.4 * size);
+        } else inside = std::fabs(x) <= size * 0.9 && std::fabs(y) <= size * 0.7 && std::fabs(z) <= size * 0.9;
+        if (inside) { local.push_back(x); local.push_back(y); local.push_back(z); }
+      }
+  return local;
+}
+
+// Cell buckets in insertion (index) order, as the JS Map of arrays keeps them.
+struct Buckets {
+  std::vector<uint32_t> start, items;
+  template <class KeyFn>
+  void build(int n, int64_t nkeys, KeyFn key) {
+    start.assign((size_t)nkeys + 1, 0u);
+    std::vector<int64_t> k(n);
+    for (int i = 0; i < n; i++) { k[i] = key(i); start[k[i] + 1]++; }
+    for (int64_t c = 0; c < nkeys; c++) start[c + 1] += start[c];
+    items.assign(n, 0u);
+    std::vector<uint32_t> cur(start.begin(), start.end() - 1);
+    for (int i = 0; i < n; i++) items[cur[k[i]]++] = (uint32_t)i;
+  }
+};
+
+// boundaryParticles (src/scene.js:76-135): shell samples and psi = rho0 / sum W.
+void boundaryParticles(const double box[3], double rho0, double d, double h,
+                       std::vector<double>& pts, std::vector<float>& psi) {
+  int nb[3];
+  double step[3];
+  for (int k = 0; k < 3; k++) {
+    nb[k] = (int)std::max(2.0, std::ceil(box[k] / d) + 1);
+    step[k] = box[k] / (nb[k] - 1);
+  }
+  pts.clear();
+  for (int ix = 0; ix < nb[0]; ix++)
+    for (int iy = 0; iy < nb[1]; iy++)
+      for (int iz = 0; iz < nb[2]; iz++) {
+        bool shell = ix == 0 || ix == nb[0] - 1 || iy == 0 || iy == nb[1] - 1 || iz == 0 || iz == nb[2] - 1;
+        if (shell) { pts.push_back(ix * step[0]); pts.push_back(iy * step[1]); pts.push_back(iz * step[2]); }
+      }
+  const int n = (int)(pts.size() / 3);
+  int dim[3];
+  for (int k = 0; k < 3; k++) dim[k] = (int)std::max(1.0, std::ceil(box[k] / h));
+  auto cellOf = [&](double x, double y, double z, int c[3]) {
+    c[0] = (int)std::min<double>(dim[0] - 1, std::max(0.0, std::floor(x / h)));
+    c[1] = (int)std::min<double>(dim[1] - 1, std::max(0.0, std::floor(y / h)));
+    c[2] = (int)std::min<double>(dim[2] - 1, std::max(0.0, std::floor(z / h)));
+  };
+  auto key = [&](int a, int b, int c) { return ((int64_t)c * dim[1] + b) * dim[0] + a; };
+  Buckets buckets;
+  buckets.build(n, (int64_t)dim[0] * dim[1] * dim[2], [&](int i) {
+    int c[3];
+    cellOf(pts[i * 3], pts[i * 3 + 1], pts[i * 3 + 2], c);
+    return key(c[0], c[1], c[2]);
+  });
+  const double coef = poly6Coef(h), h2 = h * h;
+  psi.assign(std::max(1, n), 0.0f);
+  apply_threads();
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    int c[3];
+    cellOf(pts[i * 3], pts[i * 3 + 1], pts[i * 3 + 2], c);
+    double sum = 0;
+    for (int dc = -1; dc <= 1; dc++) {
+      if (c[2] + dc < 0 || c[2] + dc >= dim[2]) continue;
+      for (int db = -1; db <= 1; db++) {
+        if (c[1] + db < 0 || c[1] + db >= dim[1]) continue;
+        for (int da = -1; da <= 1; da++) {
+          if (c[0] + da < 0 || c[0] + da >= dim[0]) continue;
+          const int64_t kk = key(c[0] + da, c[1] + db, c[2] + dc);
+          for (uint32_t m = buckets.start[kk]; m < buckets.start[kk + 1]; m++) {
+            const int j = (int)buckets.items[m];
+            double dx = pts[i * 3] - pts[j * 3];
+            double dy = pts[i * 3 + 1] - pts[j * 3 + 1];
+            double dz = pts[i * 3 + 2] - pts[j * 3 + 2];
+            double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 >= h2) continue;
+            double t = h2 - r2;
+            sum += t * t * t;
+          }
+        }
+      }
+    }
+    sum *= coef;
+    psi[i] = (float)(sum > 0 ? rho0 / sum : 0);
+  }
+}
+
+// Mass calibration and denomRest (src/scene.js:232-311) over the fluid particles
+// [0, nFluid) of a float4 position array.
+void calibrate(const std::vector<float>& pos, int nFluid, double d, double h, double rho0,
+               bool doMass, bool doDenom, double& mass, double& denomRest, const double box[3]) {
+  const double coef = poly6Coef(h), h2 = h * h;
+  const double spiky = -45 / (kPI * std::pow(h, 6));
+  int dim[3];
+  for (int k = 0; k < 3; k++) dim[k] = (int)std::max(1.0, std::floor(box[k] / h));
+  auto cellOf = [&](int i, int c[3]) {
+    for (int k = 0; k < 3; k++)
+      c[k] = (int)std::min<double>(dim[k] - 1, std::max(0.0, std::floor((double)pos[i * 4 + k] / h)));
+  };
+  auto key = [&](int a, int b, int c) { return ((int64_t)c * dim[1] + b) * dim[0] + a; };
+  Buckets buckets;
+  buckets.build(nFluid, (int64_t)dim[0] * dim[1] * dim[2], [&](int i) {
+    int c[3];
+    cellOf(i, c);
+    return key(c[0], c[1], c[2]);
+  });
+  auto forEach = [&](int i, auto&& f) {
+    int c[3];
+    cellOf(i, c);
+    for (int dc = -1; dc <= 1; dc++) {
+      if (c[2] + dc < 0 || c[2] + dc >= dim[2]) continue;
+      for (int db = -1; db <= 1; db++) {
+        if (c[1] + db < 0 || c[1] + db >= dim[1]) continue;
+        for (int da = -1; da <= 1; da++) {
+          if (c[0] + da < 0 || c[0] + da >= dim[0]) continue;
+          const int64_t kk = key(c[0] + da, c[1] + db, c[2] + dc);
+          for (uint32_t m = buckets.start[kk]; m < buckets.start[kk + 1]; m++) {
+            const int j = (int)buckets.items[m];
+            if (j != i) f(j);
+          }
+        }
+      }
+    }
+  };
+  auto densityAt = [&](int i, double m) {
+    double rho = m * coef * h2 * h2 * h2;
+    forEach(i, [&](int j) {
+      double dx = (double)pos[i * 4] - pos[j * 4], dy = (double)pos[i * 4 + 1] - pos[j * 4 + 1],
+             dz = (double)pos[i * 4 + 2] - pos[j * 4 + 2];
+      double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 >= h2) return;
+      double t = h2 - r2;
+      rho += m * coef * t * t * t;
+    });
+    return rho;
+  };
+  apply_threads();
+  if (doMass) {
+    mass = rho0 * d * d * d;
+    double maxRho = 0;
+    const double m0 = mass;
+#pragma omp parallel for reduction(max : maxRho) schedule(dynamic, 512)
+    for (int i = 0; i < nFluid; i++) maxRho = std::max(maxRho, densityAt(i, m0));
+    if (maxRho > 0.5 * rho0) mass *= rho0 / maxRho;
+  }
+  if (doDenom) {
+    denomRest = 0;
+    const double volume = mass / rho0;
+    for (int i = 0; i < nFluid; i++) {
+      if (densityAt(i, mass) < 0.99 * rho0) continue;
+      double gx = 0, gy = 0, gz = 0, sumGrad2 = 0;
+      forEach(i, [&](int j) {
+        double rx = (double)pos[i * 4] - pos[j * 4], ry = (double)pos[i * 4 + 1] - pos[j * 4 + 1],
+               rz = (double)pos[i * 4 + 2] - pos[j * 4 + 2];
+        double r2 = rx * rx + ry * ry + rz * rz;
+        if (r2 < 1e-12 || r2 >= h2) return;
+        double r = std::sqrt(r2), hr = h - r;
+        double s = volume * spiky * hr * hr / r;
+        gx += s * rx; gy += s * ry; gz += s * rz;
+        sumGrad2 += s * s * r2;
+      });
+      denomRest = std::max(denomRest, gx * gx + gy * gy + gz * gz + sumGrad2);
+      if (i > 2000 && denomRest > 0) break;
+    }
+  }
+}
+
+// buildScene (src/scene.js:159-315).
+void buildScene(const p4a_params& p, Scene& sc) {
+  const double d = p.spacing, h = 2 * d;
+  const double bx = p.box[0], by = p.box[1], bz = p.box[2];
+  std::vector<double> fluid = fluidBlock(p, d);
+  const int nFluid = (int)(fluid.size() / 3);
+  const double sz = p.body_size > 0 ? p.body_size : 0.12 * std::min(bx, std::min(by, bz));
+  const int nspec = p.bodies ? p.n_bodies : 0;
+  const double step = std::min(2.5 * sz, bx * 0.25);
+  const double span = step * (nspec - 1);
+  std::vector<double> bodyPts, bodyRest;
+  std::vector<uint32_t> bodyPhase;
+  sc.bodyCentre.clear(); sc.bodyDensity.clear(); sc.bodyCount.clear();
+  for (int r = 0; r < nspec; r++) {
+    const p4a_body_spec& spec = p.bodies[r];
+    std::vector<double> local = sampleBody(spec.shape, sz, d);
+    const int count = (int)(local.size() / 3);
+    if (!count) continue;
+    double density = spec.density != 0 && spec.density == spec.density ? spec.density : 0.5;
+    double startY = spec.start_y != 0 && spec.start_y == spec.start_y ? spec.start_y : 0.75;
+    double centre[3] = {0.5 * bx - 0.5 * span + step * r, by * startY, bz * 0.5};
+    double cx = 0, cy = 0, cz = 0;
+    for (int i = 0; i < count; i++) { cx += local[i * 3]; cy += local[i * 3 + 1]; cz += local[i * 3 + 2]; }
+    cx /= count; cy /= count; cz /= count;
+    const uint32_t id = (uint32_t)sc.bodyCount.size() + 1;
+    for (int i = 0; i < count; i++) {
+      double lx = local[i * 3], ly = local[i * 3 + 1], lz = local[i * 3 + 2];
+      bodyPts.push_back(centre[0] + lx); bodyPts.push_back(centre[1] + ly); bodyPts.push_back(centre[2] + lz);
+      bodyRest.push_back(lx - cx); bodyRest.push_back(ly - cy); bodyRest.push_back(lz - cz);
+      bodyPhase.push_back(id);
+    }
+    sc.bodyCentre.insert(sc.bodyCentre.end(), centre, centre + 3);
+    sc.bodyDensity.push_back(density);
+    sc.bodyCount.push_back(count);
+  }
+  const int nBody = (int)(bodyPts.size() / 3);
+  const int n = nFluid + nBody;
+  sc.n = n; sc.nFluid = nFluid; sc.nBody = nBody; sc.h = h; sc.d = d;
+  sc.pos.assign((size_t)n * 4, 0.0f); sc.vel.assign((size_t)n * 4, 0.0f);
+  sc.rest.assign((size_t)n * 4, 0.0f); sc.phase.assign((size_t)n * 4, 0u);
+  for (int i = 0; i < nFluid; i++)
+    for (int k = 0; k < 3; k++) sc.pos[i * 4 + k] = (float)fluid[i * 3 + k];
+  for (int i = 0; i < nBody; i++) {
+    size_t o = (size_t)(nFluid + i) * 4;
+    for (int k = 0; k < 3; k++) {
+      sc.pos[o + k] = (float)bodyPts[i * 3 + k];
+      sc.rest[o + k] = (float)bodyRest[i * 3 + k];
+    }
+    sc.phase[o] = bodyPhase[i];
+  }
+  calibrate(sc.pos, nFluid, d, h, p.rest_density, true, true, sc.mass, sc.denomRest, p.box);
+}
+
+// ------------------------------------------------------------------- Sim
+struct SimState;
+}  // namespace
+
+struct orc_sim {
+  p4a_params params{};
+  std::vector<p4a_body_spec> specs;
+  Scene sc;
+  int n = 0, cap = 0, pourBudget = 0, nBoundary = 0, nBodies = 0, nBodyParts = 0;
+  double h = 0;
+  int gridDim[3] = {1, 1, 1};
+  int nCells = 1;
+  std::vector<f4> pos[2], vel[2], pred[2], rest[2];
+  std::vector<u4> body[2];
+  std::vector<float> lambda, density;
+  std::vector<uint32_t> slot;
+  std::vector<f4> corr, normal;
+  std::vector<uint32_t> cellCount, cellStart, cursor;
+  std::vector<f4> bpos;
+  std::vector<float> bpsi;
+  std::vector<uint32_t> bcellStart;
+  std::vector<int32_t> bodyAccum, bodyCov;
+  std::vector<f4> bodyCentre, bodyRef, bodyRot, bodyInfo;
+  std::vector<uint32_t> bodyIdx;
+  uint32_t bodyIdxCount = 0;
+  double bodyScale = 0, covScale = 0;
+  std::vector<uint32_t> statsOut = std::vector<uint32_t>(8, 0u);
+  int parity = 0, predParity = 0, gen = 0;
+  double simTime = 0, timeBank = 0, lastAdvanced = 0;
+  int lastSubsteps = 0;
+  int heldBody = -1;
+  double heldTarget[3] = {0, 0, 0}, heldRate = 10, heldLimit = 4;
+  Params P{};
+  p4a_stats stats{};
+  std::vector<f4> smoothPos, anisoG;
+  int anisoGen = 0;
+  bool ready = false;
+};
+
+namespace {
+
+// uploadParams(dt) (src/sim.js:371-413).
+void uploadParams(orc_sim* s, double dt) {
+  const p4a_params& p = s->params;
+  Params& F = s->P;
+  const double h = s->h, d = p.spacing;
+  F.boxMin[0] = F.boxMin[1] = F.boxMin[2] = 0;
+  F.dt = (float)dt;
+  for (int k = 0; k < 3; k++) F.boxMax[k] = (float)p.box[k];
+  F.h = (float)h;
+  for (int k = 0; k < 3; k++) F.gridDim[k] = s->gridDim[k];
+  F.h2 = (float)(h * h);
+  const double halfD = 0.5 * d;
+  for (int k = 0; k < 3; k++) F.clampMin[k] = (float)halfD;
+  const double poly6 = 315 / (64 * kPI * std::pow(h, 9));
+  F.poly6 = (float)poly6;
+  for (int k = 0; k < 3; k++) F.clampMax[k] = (float)(p.box[k] - halfD);
+  F.spikyGrad = (float)(-45 / (kPI * std::pow(h, 6)));
+  F.gravity = (float)p.gravity;
+  F.mass = (float)s->sc.mass;
+  F.rho0 = (float)p.rest_density;
+  F.invRho0 = (float)(1 / p.rest_density);
+  F.cfmEps = (float)(p.cfm_epsilon_abs > 0 ? p.cfm_epsilon_abs
+                                           : std::max(1e-9, p.cfm_epsilon_rel * s->sc.denomRest));
+  F.sCorrK = (float)(p.s_corr_k / (s->sc.denomRest * std::max(1, p.iterations)));
+  const double rq = p.s_corr_dq * h, tq = h * h - rq * rq;
+  const double wq = poly6 * tq * tq * tq;
+  F.sCorrWq = (float)(wq > 0 ? 1 / wq : 0);
+  F.xsphC = (float)p.xsph_c;
+  F.n = (uint32_t)s->n;
+  F.nCells = (uint32_t)s->nCells;
+  F.nBoundary = p.no_boundary ? 0u : (uint32_t)s->nBoundary;
+  F.nBodyParts = (uint32_t)s->nBodyParts;
+  F.nBodies = (uint32_t)s->nBodies;
+  F.bodyScale = (float)s->bodyScale;
+  F.covScale = (float)s->covScale;
+  F.omega = (float)p.omega;
+  F.sorAverage = p.sor_average ? 1u : 0u;
+  F.invDt = (float)(dt > 0 ? 1 / dt : 0);
+  F.volume = (float)(s->sc.mass / p.rest_density);
+  F.tension = (float)p.surface_tension_k;
+  F.cohes = (float)(32 / (kPI * std::pow(h, 9)));
+  F.cohesTerm = (float)(std::pow(h, 6) / 64);
+}
+
+// cellOf / cellIndex (src/wgsl.js:43-49).
+struct I3 { int x, y, z; };
+inline I3 cellOf(const Params& P, f3 p) {
+  I3 c;
+  c.x = f2i_sat(std::floor((p.x - P.boxMin[0]) / P.h));
+  c.y = f2i_sat(std::floor((p.y - P.boxMin[1]) / P.h));
+  c.z = f2i_sat(std::floor((p.z - P.boxMin[2]) / P.h));
+  c.x = std::min(std::max(c.x, 0), P.gridDim[0] - 1);
+  c.y = std::min(std::max(c.y, 0), P.gridDim[1] - 1);
+  c.z = std::min(std::max(c.z, 0), P.gridDim[2] - 1);
+  return c;
+}
+inline uint32_t cellIndex(const Params& P, I3 c) {
+  return (uint32_t)((c.z * P.gridDim[1] + c.y) * P.gridDim[0] + c.x);
+}
+inline float poly6(const Params& P, float r2) {
+  float t = P.h2 - r2;
+  return r2 < P.h2 ? P.poly6 * t * t * t : 0.0f;
+}
+
+// predict (src/wgsl.js:56-70).
+void k_predict(const Params& P, std::vector<f4>& pos, std::vector<f4>& vel, std::vector<f4>& pred) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    const float gx = P.dt * 0.0f, gy = P.dt * -P.gravity, gz = P.dt * 0.0f;
+    f3 v = {vel[i].x + gx, vel[i].y + gy, vel[i].z + gz};
+    vel[i] = {v.x, v.y, v.z, 0.0f};
+    pred[i] = {pos[i].x + P.dt * v.x, pos[i].y + P.dt * v.y, pos[i].z + P.dt * v.z, 1.0f};
+  }
+}
+
+// count + scanBlock + scanBlocks + scanAdd + scatterSlot (src/wgsl.js:352-438) with
+// a stable slot order; cellCount/cursor cleared first (src/sim.js:475-476).
+void k_sort_slots(const Params& P, const std::vector<f4>& pred, std::vector<uint32_t>& cellCount,
+                  std::vector<uint32_t>& cellStart, std::vector<uint32_t>& cursor,
+                  std::vector<uint32_t>& slot) {
+  const int n = (int)P.n;
+  const uint32_t C = P.nCells;
+  std::fill(cellCount.begin(), cellCount.end(), 0u);
+  std::fill(cursor.begin(), cursor.end(), 0u);
+  std::vector<uint32_t> key(n);
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) key[i] = cellIndex(P, cellOf(P, xyz(pred[i])));
+  for (int i = 0; i < n; i++) cellCount[key[i]]++;
+  uint32_t run = 0;
+  for (uint32_t c = 0; c < C; c++) { cellStart[c] = run; run += cellCount[c]; }
+  cellStart[C] = run;
+  for (int i = 0; i < n; i++) slot[i] = cellStart[key[i]] + cursor[key[i]]++;
+}
+
+template <class T>
+void k_scatter(int n, const std::vector<uint32_t>& slot, const std::vector<T>& src, std::vector<T>& dst) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) dst[slot[i]] = src[i];
+}
+
+// lambda (src/wgsl.js:477-543).
+void k_lambda(const Params& P, const std::vector<f4>& pred, std::vector<float>& lambda,
+              std::vector<float>& density, const std::vector<uint32_t>& cs, const std::vector<f4>& bpos,
+              const std::vector<float>& bpsi, const std::vector<uint32_t>& bcs) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    const f3 pi = xyz(pred[i]);
+    const I3 c = cellOf(P, pi);
+    const int x0 = std::max(c.x - 1, 0), x1 = std::min(c.x + 1, P.gridDim[0] - 1);
+    float rho = P.mass * poly6(P, 0.0f);
+    f3 gradSum = {0, 0, 0};
+    float sumGrad2 = 0.0f;
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= P.gridDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= P.gridDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
+        const uint32_t b = cs[rowBase + x0], e = cs[rowBase + x1 + 1];
+        for (uint32_t j = b; j < e; j++) {
+          if (j == (uint32_t)i) continue;
+          const f3 rij = sub3(pi, xyz(pred[j]));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2) continue;
+          rho = std::fmaf(P.mass, poly6(P, r2), rho);
+          if (r2 > 1.0e-12f) {
+            const float r = std::sqrt(r2);
+            const float hr = P.h - r;
+            const float s = P.volume * P.spikyGrad * hr * hr / r;
+            const f3 g = mul3(rij, s);
+            gradSum = add3(gradSum, g);
+            sumGrad2 = sumGrad2 + dot3(g, g);
+          }
+        }
+        if (P.nBoundary > 0u) {
+          const uint32_t bb = bcs[rowBase + x0], be = bcs[rowBase + x1 + 1];
+          for (uint32_t k = bb; k < be; k++) {
+            const f3 rij = sub3(pi, xyz(bpos[k]));
+            const float r2 = dot3(rij, rij);
+            if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+            rho = std::fmaf(bpsi[k], poly6(P, r2), rho);
+            const float r = std::sqrt(r2);
+            const float hr = P.h - r;
+            const float s = bpsi[k] * P.invRho0 * P.spikyGrad * hr * hr / r;
+            gradSum = fma3(s, rij, gradSum);
+          }
+        }
+      }
+    }
+    density[i] = rho;
+    const float C = rho * P.invRho0 - 1.0f;
+    if (C > 0.0f) {
+      const float den = dot3(gradSum, gradSum) + sumGrad2 + P.cfmEps + 1.0e-12f;
+      lambda[i] = -C / den;
+    } else {
+      lambda[i] = 0.0f;
+    }
+  }
+}
+
+// delta (src/wgsl.js:545-612).
+void k_delta(const Params& P, const std::vector<f4>& pred, std::vector<f4>& predOut,
+             const std::vector<float>& lambda, const std::vector<uint32_t>& cs,
+             const std::vector<f4>& bpos, const std::vector<float>& bpsi,
+             const std::vector<uint32_t>& bcs) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    const f3 pi = xyz(pred[i]);
+    const float li = lambda[i];
+    const I3 c = cellOf(P, pi);
+    const int x0 = std::max(c.x - 1, 0), x1 = std::min(c.x + 1, P.gridDim[0] - 1);
+    f3 d = {0, 0, 0}, dB = {0, 0, 0};
+    float nc = 1.0f;
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= P.gridDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= P.gridDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
+        const uint32_t b = cs[rowBase + x0], e = cs[rowBase + x1 + 1];
+        for (uint32_t j = b; j < e; j++) {
+          if (j == (uint32_t)i) continue;
+          const f3 rij = sub3(pi, xyz(pred[j]));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+          const float r = std::sqrt(r2);
+          const float hr = P.h - r;
+          const float s = P.spikyGrad * hr * hr / r;
+          const float t = P.h2 - r2;
+          const float ratio = P.poly6 * t * t * t * P.sCorrWq;
+          const float r2r = ratio * ratio;
+          const float sc = -P.sCorrK * r2r * r2r;
+          const float coef = (li + lambda[j] + sc) * s;
+          d = fma3(coef, rij, d);
+          nc += 1.0f;
+        }
+        if (P.nBoundary > 0u) {
+          const uint32_t bb = bcs[rowBase + x0], be = bcs[rowBase + x1 + 1];
+          for (uint32_t k = bb; k < be; k++) {
+            const f3 rij = sub3(pi, xyz(bpos[k]));
+            const float r2 = dot3(rij, rij);
+            if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+            const float r = std::sqrt(r2);
+            const float hr = P.h - r;
+            const float coef = (li * bpsi[k]) * (P.spikyGrad * hr * hr / r);
+            dB = fma3(coef, rij, dB);
+          }
+        }
+      }
+    }
+    f3 dd = {std::fmaf(dB.x, P.invRho0, d.x * P.volume), std::fmaf(dB.y, P.invRho0, d.y * P.volume),
+             std::fmaf(dB.z, P.invRho0, d.z * P.volume)};
+    float scale = P.omega;
+    if (P.sorAverage == 1u) scale = P.omega / std::max(nc, 1.0f);
+    f3 o = fma3(scale, dd, pi);
+    o.x = std::min(std::max(o.x, P.clampMin[0]), P.clampMax[0]);
+    o.y = std::min(std::max(o.y, P.clampMin[1]), P.clampMax[1]);
+    o.z = std::min(std::max(o.z, P.clampMin[2]), P.clampMax[2]);
+    predOut[i] = {o.x, o.y, o.z, 1.0f};
+  }
+}
+
+// velFromPos (src/wgsl.js:72-83).
+void k_velFromPos(const Params& P, const std::vector<f4>& pos, std::vector<f4>& vel, const std::vector<f4>& pred) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++)
+    vel[i] = {(pred[i].x - pos[i].x) * P.invDt, (pred[i].y - pos[i].y) * P.invDt,
+              (pred[i].z - pos[i].z) * P.invDt, 0.0f};
+}
+
+// xsph (src/wgsl.js:85-123).
+void k_xsph(const Params& P, const std::vector<f4>& pred, const std::vector<f4>& vel,
+            const std::vector<float>& density, std::vector<f4>& corr, const std::vector<uint32_t>& cs) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    const f3 pi = xyz(pred[i]), vi = xyz(vel[i]);
+    const I3 c = cellOf(P, pi);
+    const int x0 = std::max(c.x - 1, 0), x1 = std::min(c.x + 1, P.gridDim[0] - 1);
+    f3 acc = {0, 0, 0};
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= P.gridDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= P.gridDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
+        const uint32_t b = cs[rowBase + x0], e = cs[rowBase + x1 + 1];
+        for (uint32_t j = b; j < e; j++) {
+          if (j == (uint32_t)i) continue;
+          const f3 rij = sub3(pi, xyz(pred[j]));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2) continue;
+          const float f = P.mass * poly6(P, r2) / std::max(density[j], 0.5f * P.rho0);
+          acc = fma3(f, sub3(xyz(vel[j]), vi), acc);
+        }
+      }
+    }
+    corr[i] = {P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f};
+  }
+}
+
+// normals (src/wgsl.js:250-288).
+void k_normals(const Params& P, const std::vector<f4>& pred, const std::vector<float>& density,
+               std::vector<f4>& normal, const std::vector<uint32_t>& cs) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    const f3 pi = xyz(pred[i]);
+    const I3 c = cellOf(P, pi);
+    const int x0 = std::max(c.x - 1, 0), x1 = std::min(c.x + 1, P.gridDim[0] - 1);
+    f3 acc = {0, 0, 0};
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= P.gridDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= P.gridDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
+        const uint32_t b = cs[rowBase + x0], e = cs[rowBase + x1 + 1];
+        for (uint32_t j = b; j < e; j++) {
+          if (j == (uint32_t)i) continue;
+          const f3 rij = sub3(pi, xyz(pred[j]));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+          const float r = std::sqrt(r2);
+          const float hr = P.h - r;
+          const float coef = (P.mass / std::max(density[j], 0.5f * P.rho0)) * (P.spikyGrad * hr * hr / r);
+          acc = fma3(coef, rij, acc);
+        }
+      }
+    }
+    normal[i] = {P.h * acc.x, P.h * acc.y, P.h * acc.z, 0.0f};
+  }
+}
+
+// tension (src/wgsl.js:290-335).
+void k_tension(const Params& P, const std::vector<f4>& pred, const std::vector<float>& density,
+               const std::vector<f4>& normal, std::vector<f4>& corr, const std::vector<uint32_t>& cs) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; i++) {
+    const f3 pi = xyz(pred[i]), ni = xyz(normal[i]);
+    const float rhoi = density[i];
+    const I3 c = cellOf(P, pi);
+    const int x0 = std::max(c.x - 1, 0), x1 = std::min(c.x + 1, P.gridDim[0] - 1);
+    f3 acc = {0, 0, 0};
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= P.gridDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= P.gridDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
+        const uint32_t b = cs[rowBase + x0], e = cs[rowBase + x1 + 1];
+        for (uint32_t j = b; j < e; j++) {
+          if (j == (uint32_t)i) continue;
+          const f3 rij = sub3(pi, xyz(pred[j]));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+          const float r = std::sqrt(r2);
+          const float hrr = P.h - r;
+          const float k = hrr * hrr * hrr * r * r * r;
+          float cw = P.cohes * (2.0f * k - P.cohesTerm);
+          if (2.0f * r > P.h) cw = P.cohes * k;
+          const float sCoh = -P.tension * P.mass * cw / r;
+          const f3 fCoh = mul3(rij, sCoh);
+          const f3 fCurv = mul3(sub3(ni, xyz(normal[j])), -P.tension);
+          const float w = 2.0f * P.rho0 / (rhoi + density[j]);
+          acc = fma3(w, add3(fCoh, fCurv), acc);
+        }
+      }
+    }
+    corr[i] = {std::fmaf(P.dt, acc.x, corr[i].x), std::fmaf(P.dt, acc.y, corr[i].y),
+               std::fmaf(P.dt, acc.z, corr[i].z), 0.0f};
+  }
+}
+
+// finalize (src/wgsl.js:337-350).
+void k_finalize(const Params& P, std::vector<f4>& pos, std::vector<f4>& vel, const std::vector<f4>& pred,
+                const std::vector<f4>& corr) {
+  const int n = (int)P.n;
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < n; i++) {
+    vel[i] = {vel[i].x + corr[i].x, vel[i].y + corr[i].y, vel[i].z + corr[i].z, 0.0f};
+    pos[i] = pred[i];
+  }
+}
+
+// ---- rigid bodies (src/wgsl.js:159-185, 614-783) ----
+void k_bodyClear(orc_sim* s) {
+  std::fill(s->bodyAccum.begin(), s->bodyAccum.end(), 0);
+  std::fill(s->bodyCov.begin(), s->bodyCov.end(), 0);
+  s->bodyIdxCount = 0;
+}
+void k_bodyCompact(orc_sim* s, const std::vector<u4>& body) {
+  for (int i = 0; i < (int)s->P.n; i++)
+    if (body[i].x != 0u) s->bodyIdx[s->bodyIdxCount++] = (uint32_t)i;
+}
+inline void iadd(int32_t& a, int32_t v) { a = (int32_t)((uint32_t)a + (uint32_t)v); }
+void k_bodyCentre(orc_sim* s, const std::vector<f4>& pred, const std::vector<u4>& body) {
+  const Params& P = s->P;
+  for (uint32_t t = 0; t < P.nBodyParts; t++) {
+    const uint32_t i = s->bodyIdx[t];
+    const uint32_t b = body[i].x;
+    if (b == 0u) continue;
+    const uint32_t base = (b - 1u) * 4u;
+    const f4& c = s->bodyCentre[b - 1u];
+    const f3 d = mul3(sub3(xyz(pred[i]), xyz(c)), P.bodyScale);
+    iadd(s->bodyAccum[base + 0], round_i32(d.x));
+    iadd(s->bodyAccum[base + 1], round_i32(d.y));
+    iadd(s->bodyAccum[base + 2], round_i32(d.z));
+    iadd(s->bodyAccum[base + 3], 1);
+  }
+}
+// bodySeed with the binding swap of src/sim.js:346: writes bodyRef from bodyCentre.
+void k_bodySeed(orc_sim* s) {
+  const Params& P = s->P;
+  for (uint32_t b = 0; b < P.nBodies; b++) {
+    const uint32_t a = b * 4u;
+    const float count = (float)s->bodyAccum[a + 3];
+    if (count <= 0.0f) continue;
+    const f3 r = xyz(s->bodyCentre[b]);
+    const float den = P.bodyScale * count;
+    const f3 d = {(float)s->bodyAccum[a] / den, (float)s->bodyAccum[a + 1] / den, (float)s->bodyAccum[a + 2] / den};
+    s->bodyRef[b] = {r.x + d.x, r.y + d.y, r.z + d.z, 0.0f};
+  }
+}
+void k_bodyRefLoad(orc_sim* s) {
+  for (size_t b = 0; b < s->bodyRef.size(); b++) s->bodyCentre[b] = s->bodyRef[b];
+}
+void k_bodyCov(orc_sim* s, const std::vector<f4>& pred, const std::vector<u4>& body, const std::vector<f4>& rest) {
+  const Params& P = s->P;
+  for (uint32_t t = 0; t < P.nBodyParts; t++) {
+    const uint32_t i = s->bodyIdx[t];
+    const uint32_t b = body[i].x;
+    if (b == 0u) continue;
+    const f3 p = sub3(xyz(pred[i]), xyz(s->bodyRef[b - 1u]));
+    const f3 q = xyz(rest[i]);
+    int32_t* cv = &s->bodyCov[(b - 1u) * 9u];
+    iadd(cv[0], round_i32(p.x * q.x * P.covScale));
+    iadd(cv[1], round_i32(p.y * q.x * P.covScale));
+    iadd(cv[2], round_i32(p.z * q.x * P.covScale));
+    iadd(cv[3], round_i32(p.x * q.y * P.covScale));
+    iadd(cv[4], round_i32(p.y * q.y * P.covScale));
+    iadd(cv[5], round_i32(p.z * q.y * P.covScale));
+    iadd(cv[6], round_i32(p.x * q.z * P.covScale));
+    iadd(cv[7], round_i32(p.y * q.z * P.covScale));
+    iadd(cv[8], round_i32(p.z * q.z * P.covScale));
+  }
+}
+// mat3x3fInverse (src/wgsl.js:749-760), returned transposed: columns r0/d, r1/d, r2/d.
+inline m3 inverseTransposed(const m3& m) {
+  const f3 a = m.c[0], b = m.c[1], c = m.c[2];
+  const f3 r0 = cross3(b, c), r1 = cross3(c, a), r2 = cross3(a, b);
+  const float d = dot3(a, r0);
+  const float invd = std::fabs(d) > 1.0e-20f ? 1.0f / d : 0.0f;
+  return {{mul3(r0, invd), mul3(r1, invd), mul3(r2, invd)}};
+}
+void k_bodyResolve(orc_sim* s) {
+  const Params& P = s->P;
+  for (uint32_t b = 0; b < P.nBodies; b++) {
+    const uint32_t a = b * 4u;
+    const float count = (float)s->bodyAccum[a + 3];
+    if (count <= 0.0f) continue;
+    const f3 prev = xyz(s->bodyCentre[b]);
+    const float den = P.bodyScale * count;
+    f3 delta = {(float)s->bodyAccum[a] / den, (float)s->bodyAccum[a + 1] / den, (float)s->bodyAccum[a + 2] / den};
+    const float invRatio = s->bodyInfo[b].x;
+    if (invRatio > 0.0f) delta = mul3(delta, invRatio);
+    s->bodyCentre[b] = {prev.x + delta.x, prev.y + delta.y, prev.z + delta.z, 0.0f};
+    const int32_t* cv = &s->bodyCov[b * 9u];
+    m3 A = {{{(float)cv[0], (float)cv[1], (float)cv[2]},
+             {(float)cv[3], (float)cv[4], (float)cv[5]},
+             {(float)cv[6], (float)cv[7], (float)cv[8]}}};
+    A = scale3(A, 1.0f / P.covScale);
+    float det = det3(A);
+    if (std::fabs(det) < 1.0e-12f) { A = ident3(); det = 1.0f; }
+    const float sc = cbrt_newton(std::fabs(det));
+    if (sc > 1.0e-6f) A = scale3(A, 1.0f / sc);
+    m3 R = A;
+    for (int it = 0; it < 8; it++) {
+      const m3 inv = inverseTransposed(R);
+      m3 next;
+      for (int c = 0; c < 3; c++) next.c[c] = mul3(add3(R.c[c], inv.c[c]), 0.5f);
+      const f3 d0 = sub3(next.c[0], R.c[0]), d1 = sub3(next.c[1], R.c[1]), d2 = sub3(next.c[2], R.c[2]);
+      R = next;
+      if (dot3(d0, d0) + dot3(d1, d1) + dot3(d2, d2) < 1.0e-12f) break;
+    }
+    for (int r = 0; r < 3; r++) {
+      const f3 row = row3(R, r);
+      s->bodyRot[b * 3u + r] = {row.x, row.y, row.z, 0.0f};
+    }
+  }
+}
+void k_bodyProject(orc_sim* s, std::vector<f4>& pred, const std::vector<u4>& body, const std::vector<f4>& rest) {
+  const Params& P = s->P;
+  for (uint32_t t = 0; t < P.nBodyParts; t++) {
+    const uint32_t i = s->bodyIdx[t];
+    const uint32_t b = body[i].x;
+    if (b == 0u) continue;
+    const uint32_t r = (b - 1u) * 3u;
+    const f3 q = xyz(rest[i]);
+    const f3 p = {dot3(xyz(s->bodyRot[r]), q), dot3(xyz(s->bodyRot[r + 1]), q), dot3(xyz(s->bodyRot[r + 2]), q)};
+    const f3 c = xyz(s->bodyCentre[b - 1u]);
+    pred[i] = {c.x + p.x, c.y + p.y, c.z + p.z, 1.0f};
+  }
+}
+
+// bodyDrag (src/wgsl.js:187-214) over the compacted body list.
+void k_bodyDrag(orc_sim* s, std::vector<f4>& vel, const std::vector<u4>& body, float blend) {
+  const float goal[3] = {(float)s->heldTarget[0], (float)s->heldTarget[1], (float)s->heldTarget[2]};
+  const float rate = (float)s->heldRate, limit = (float)s->heldLimit;
+  const uint32_t held = (uint32_t)s->heldBody;
+  for (uint32_t t = 0; t < (uint32_t)s->nBodyParts; t++) {
+    const uint32_t i = s->bodyIdx[t];
+    if (body[i].x != held) continue;
+    const f4& c = s->bodyCentre[held - 1u];
+    f3 vWant = {(goal[0] - c.x) * rate, (goal[1] - c.y) * rate, (goal[2] - c.z) * rate};
+    const float sp = length3(vWant);
+    if (sp > limit) vWant = mul3(vWant, limit / sp);
+    const f3 v = xyz(vel[i]);
+    const f3 dv = mul3(sub3(vWant, v), blend);
+    vel[i] = {v.x + dv.x, v.y + dv.y, v.z + dv.z, vel[i].w};
+  }
+}
+
+// stats (src/wgsl.js:785-832): 256-wide workgroup trees, then u32 atomics.
+void k_stats(orc_sim* s, const std::vector<float>& density, const std::vector<f4>& vel) {
+  const Params& P = s->P;
+  const int n = (int)P.n;
+  const int groups = std::max(1, (n + 255) / 256);
+  std::vector<uint32_t> partial((size_t)groups * 4);
+#pragma omp parallel for schedule(static)
+  for (int g = 0; g < groups; g++) {
+    float sRho[256], sMaxRho[256], sMaxV[256], sKe[256];
+    for (int t = 0; t < 256; t++) {
+      const int i = g * 256 + t;
+      float rho = 0.0f, mrho = 0.0f, mv = 0.0f, ke = 0.0f;
+      if (i < n) {
+        rho = density[i] * P.invRho0;
+        mrho = rho;
+        const f3 v = xyz(vel[i]);
+        const float v2 = dot3(v, v);
+        mv = std::sqrt(v2);
+        ke = 0.5f * P.mass * v2;
+      }
+      sRho[t] = rho; sMaxRho[t] = mrho; sMaxV[t] = mv; sKe[t] = ke;
+    }
+    for (int off = 128; off > 0; off >>= 1)
+      for (int t = 0; t < off; t++) {
+        sRho[t] = sRho[t] + sRho[t + off];
+        sMaxRho[t] = std::max(sMaxRho[t], sMaxRho[t + off]);
+        sMaxV[t] = std::max(sMaxV[t], sMaxV[t + off]);
+        sKe[t] = sKe[t] + sKe[t + off];
+      }
+    partial[g * 4 + 0] = f2u_sat(sRho[0] * 1024.0f);
+    partial[g * 4 + 1] = f2u_sat(sMaxRho[0] * 1024.0f);
+    partial[g * 4 + 2] = f2u_sat(sMaxV[0] * 1024.0f);
+    partial[g * 4 + 3] = f2u_sat(sKe[0] * 1024.0f);
+  }
+  for (int g = 0; g < groups; g++) {
+    s->statsOut[0] += partial[g * 4 + 0];
+    s->statsOut[1] = std::max(s->statsOut[1], partial[g * 4 + 1]);
+    s->statsOut[2] = std::max(s->statsOut[2], partial[g * 4 + 2]);
+    s->statsOut[3] += partial[g * 4 + 3];
+  }
+}
+
+// ------------------------------------------------------------ Sim host code
+// sortBoundary (src/sim.js:255-286).
+void sortBoundary(orc_sim* s, const std::vector<double>& pts, const std::vector<float>& psi, int nb) {
+  const int* dim = s->gridDim;
+  const double h = s->h;
+  std::vector<uint32_t> counts(s->nCells + 2, 0u), cell(nb);
+  std::vector<float> bp((size_t)std::max(1, nb) * 4, 0.0f);
+  for (int i = 0; i < nb; i++)
+    for (int k = 0; k < 3; k++) bp[i * 4 + k] = (float)pts[i * 3 + k];
+  for (int i = 0; i < nb; i++) {
+    int c[3];
+    for (int k = 0; k < 3; k++)
+      c[k] = (int)std::min<double>(dim[k] - 1, std::max(0.0, std::floor((double)bp[i * 4 + k] / h)));
+    cell[i] = (uint32_t)((c[2] * dim[1] + c[1]) * dim[0] + c[0]);
+    counts[cell[i]]++;
+  }
+  s->bcellStart.assign(s->nCells + 2, 0u);
+  uint32_t run = 0;
+  for (int c = 0; c <= s->nCells; c++) { s->bcellStart[c] = run; run += counts[c]; }
+  s->bcellStart[s->nCells + 1] = run;
+  std::vector<uint32_t> cursor = s->bcellStart;
+  s->bpos.assign(std::max(1, nb), f4{0, 0, 0, 0});
+  s->bpsi.assign(std::max(1, nb), 0.0f);
+  for (int i = 0; i < nb; i++) {
+    const uint32_t o = cursor[cell[i]]++;
+    s->bpos[o] = {bp[i * 4], bp[i * 4 + 1], bp[i * 4 + 2], 0.0f};
+    s->bpsi[o] = psi[i];
+  }
+}
+
+void allocCells(orc_sim* s) {
+  s->cellCount.assign(s->nCells + 1, 0u);
+  s->cellStart.assign(s->nCells + 2, 0u);
+  s->cursor.assign(s->nCells + 1, 0u);
+}
+
+void setBoundary(orc_sim* s) {
+  std::vector<double> pts;
+  std::vector<float> psi;
+  boundaryParticles(s->params.box, s->params.rest_density, s->params.spacing, s->h, pts, psi);
+  s->nBoundary = (int)(pts.size() / 3);
+  sortBoundary(s, pts, psi, s->nBoundary);
+}
+
+// The grid pass with the predict before it (src/sim.js:473-492), at parity `par`.
+void gridPass(orc_sim* s, int par) {
+  const int o = par ^ 1;
+  const Params& P = s->P;
+  k_predict(P, s->pos[par], s->vel[par], s->pred[par]);
+  k_sort_slots(P, s->pred[par], s->cellCount, s->cellStart, s->cursor, s->slot);
+  const int n = (int)P.n;
+  k_scatter(n, s->slot, s->pos[par], s->pos[o]);
+  k_scatter(n, s->slot, s->vel[par], s->vel[o]);
+  k_scatter(n, s->slot, s->pred[par], s->pred[o]);
+  k_scatter(n, s->slot, s->body[par], s->body[o]);
+  k_scatter(n, s->slot, s->rest[par], s->rest[o]);
+}
+
+// primeGrid (src/sim.js:223-253).
+void primeGrid(orc_sim* s) {
+  uploadParams(s, 0);
+  gridPass(s, s->parity);
+  s->parity ^= 1;
+  s->predParity = s->parity;
+  uploadParams(s, 1.0 / 240);
+  // The compacted body list the drag pass reads before the first 'bodies' pass.
+  if (s->nBodyParts > 0) { k_bodyClear(s); k_bodyCompact(s, s->body[s->parity]); }
+}
+
+int resetCommon(orc_sim* s) {
+  Scene& sc = s->sc;
+  const p4a_params& p = s->params;
+  s->simTime = 0;
+  s->gen++;
+  const int n = sc.n;
+  s->h = sc.h;
+  for (int k = 0; k < 3; k++) s->gridDim[k] = (int)std::max(1.0, std::floor(p.box[k] / s->h));
+  s->nCells = s->gridDim[0] * s->gridDim[1] * s->gridDim[2];
+  const int cap = n + s->pourBudget;
+  s->cap = cap;
+  for (int t = 0; t < 2; t++) {
+    s->pos[t].assign(cap, f4{0, 0, 0, 0}); s->vel[t].assign(cap, f4{0, 0, 0, 0});
+    s->pred[t].assign(cap, f4{0, 0, 0, 0}); s->rest[t].assign(cap, f4{0, 0, 0, 0});
+    s->body[t].assign(cap, u4{0, 0, 0, 0});
+  }
+  s->lambda.assign(cap, 0.0f); s->density.assign(cap, 0.0f); s->slot.assign(cap, 0u);
+  s->corr.assign(cap, f4{0, 0, 0, 0}); s->normal.assign(cap, f4{0, 0, 0, 0});
+  allocCells(s);
+  setBoundary(s);
+  const int nBodies = (int)sc.bodyDensity.size();
+  s->nBodies = nBodies;
+  s->nBodyParts = sc.nBody;
+  const int nb1 = std::max(1, nBodies);
+  s->bodyAccum.assign(nb1 * 4, 0); s->bodyCov.assign(nb1 * 9, 0);
+  s->bodyCentre.assign(nb1, f4{0, 0, 0, 0}); s->bodyRef.assign(nb1, f4{0, 0, 0, 0});
+  s->bodyRot.assign(nb1 * 3, f4{0, 0, 0, 0}); s->bodyInfo.assign(nb1, f4{0, 0, 0, 0});
+  s->bodyIdx.assign(std::max(1, sc.nBody), 0u);
+  s->bodyIdxCount = 0;
+  for (int i = 0; i < nBodies; i++) {
+    s->bodyInfo[i].x = (float)(1 / std::max(1e-6, sc.bodyDensity[i]));
+    s->bodyCentre[i] = {(float)sc.bodyCentre[i * 3], (float)sc.bodyCentre[i * 3 + 1], (float)sc.bodyCentre[i * 3 + 2], 0.0f};
+    s->bodyRef[i] = s->bodyCentre[i];
+    for (int r = 0; r < 3; r++) (&s->bodyRot[i * 3 + r].x)[r] = 1.0f;
+  }
+  // Fixed-point scales (src/sim.js:163-171).
+  double maxCount = 1, maxRest = 1e-3;
+  std::vector<int> counts(nBodies, 0);
+  for (int i = 0; i < n; i++)
+    if (sc.phase[i * 4] >= 1 && (int)sc.phase[i * 4] <= nBodies) counts[sc.phase[i * 4] - 1]++;
+  for (int b = 0; b < nBodies; b++) maxCount = std::max(maxCount, (double)counts[b]);
+  for (int i = 0; i < n; i++) {
+    double r = std::hypot((double)sc.rest[i * 4], (double)sc.rest[i * 4 + 1], (double)sc.rest[i * 4 + 2]);
+    if (r > maxRest) maxRest = r;
+  }
+  const double extent = std::max(p.box[0], std::max(p.box[1], p.box[2]));
+  s->bodyScale = 1e9 / (extent * maxCount);
+  s->covScale = 1e9 / (extent * maxRest * maxCount);
+  std::fill(s->statsOut.begin(), s->statsOut.end(), 0u);
+  s->stats = p4a_stats{};
+  s->stats.avg_rho = 1; s->stats.max_rho = 1;
+  for (int i = 0; i < n; i++) {
+    s->pos[0][i] = {sc.pos[i * 4], sc.pos[i * 4 + 1], sc.pos[i * 4 + 2], sc.pos[i * 4 + 3]};
+    s->vel[0][i] = {sc.vel[i * 4], sc.vel[i * 4 + 1], sc.vel[i * 4 + 2], sc.vel[i * 4 + 3]};
+    s->pred[0][i] = s->pos[0][i];
+    s->body[0][i] = {sc.phase[i * 4], sc.phase[i * 4 + 1], sc.phase[i * 4 + 2], sc.phase[i * 4 + 3]};
+    s->rest[0][i] = {sc.rest[i * 4], sc.rest[i * 4 + 1], sc.rest[i * 4 + 2], sc.rest[i * 4 + 3]};
+  }
+  s->n = n;
+  s->parity = 0;
+  s->predParity = 0;
+  s->heldBody = -1;
+  s->heldTarget[0] = s->heldTarget[1] = s->heldTarget[2] = 0;
+  s->heldRate = 10; s->heldLimit = 4;
+  uploadParams(s, 1.0 / 240);
+  primeGrid(s);
+  s->ready = true;
+  return P4A_OK;
+}
+
+void copyParams(orc_sim* s, const p4a_params* p) {
+  s->params = *p;
+  s->specs.assign(p->bodies, p->bodies + (p->bodies ? p->n_bodies : 0));
+  s->params.bodies = s->specs.empty() ? nullptr : s->specs.data();
+  s->params.n_bodies = (int32_t)s->specs.size();
+}
+
+}  // namespace
+
+extern "C" {
+
+orc_sim* orc_create(void) { return new orc_sim(); }
+void orc_destroy(orc_sim* s) { delete s; }
+void orc_set_threads(int threads) { g_threads = threads; }
+int orc_get_threads(void) {
+#ifdef _OPENMP
+  apply_threads();
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+float orc_cbrt_newton(float x) { return cbrt_newton(x); }
+
+int orc_build_scene(const p4a_params* p, p4a_scene_counts* counts, float* pos, float* vel,
+                    float* rest, uint32_t* phase, double* body_centre, double* body_density) {
+  if (!p || !counts) return P4A_ERR_ARG;
+  Scene sc;
+  buildScene(*p, sc);
+  std::vector<double> pts;
+  std::vector<float> psi;
+  boundaryParticles(p->box, p->rest_density, p->spacing, sc.h, pts, psi);
+  counts->n = sc.n; counts->n_fluid = sc.nFluid; counts->n_body = sc.nBody;
+  counts->n_bodies = (int32_t)sc.bodyDensity.size(); counts->n_boundary = (int32_t)(pts.size() / 3);
+  counts->mass = sc.mass; counts->denom_rest = sc.denomRest; counts->h = sc.h;
+  if (pos) std::memcpy(pos, sc.pos.data(), sc.pos.size() * 4);
+  if (vel) std::memcpy(vel, sc.vel.data(), sc.vel.size() * 4);
+  if (rest) std::memcpy(rest, sc.rest.data(), sc.rest.size() * 4);
+  if (phase) std::memcpy(phase, sc.phase.data(), sc.phase.size() * 4);
+  if (body_centre) std::memcpy(body_centre, sc.bodyCentre.data(), sc.bodyCentre.size() * 8);
+  if (body_density) std::memcpy(body_density, sc.bodyDensity.data(), sc.bodyDensity.size() * 8);
+  return P4A_OK;
+}
+
+int orc_boundary(const p4a_params* p, double d, double h, int32_t* count, double* pts, float* psi) {
+  std::vector<double> vp;
+  std::vector<float> vs;
+  boundaryParticles(p->box, p->rest_density, d, h, vp, vs);
+  *count = (int32_t)(vp.size() / 3);
+  if (pts) std::memcpy(pts, vp.data(), vp.size() * 8);
+  if (psi) std::memcpy(psi, vs.data(), (size_t)*count * 4);
+  return P4A_OK;
+}
+
+int orc_reset(orc_sim* s, const p4a_params* p) {
+  if (!s || !p || p->spacing <= 0) return P4A_ERR_ARG;
+  copyParams(s, p);
+  buildScene(s->params, s->sc);
+  s->pourBudget = p->pour ? s->sc.nFluid : 0;
+  return resetCommon(s);
+}
+
+int orc_reset_scene(orc_sim* s, const p4a_params* p, const p4a_scene_desc* d) {
+  if (!s || !p || !d || d->n < 0 || !d->pos || p->spacing <= 0) return P4A_ERR_ARG;
+  copyParams(s, p);
+  Scene& sc = s->sc;
+  sc = Scene();
+  sc.n = d->n; sc.d = p->spacing; sc.h = 2 * p->spacing;
+  sc.pos.assign(d->pos, d->pos + (size_t)d->n * 4);
+  sc.vel = d->vel ? std::vector<float>(d->vel, d->vel + (size_t)d->n * 4) : std::vector<float>((size_t)d->n * 4, 0.0f);
+  sc.rest = d->rest ? std::vector<float>(d->rest, d->rest + (size_t)d->n * 4) : std::vector<float>((size_t)d->n * 4, 0.0f);
+  sc.phase = d->phase ? std::vector<uint32_t>(d->phase, d->phase + (size_t)d->n * 4) : std::vector<uint32_t>((size_t)d->n * 4, 0u);
+  int nFluid = 0;
+  for (int i = 0; i < d->n; i++) if (sc.phase[i * 4] == 0) nFluid++;
+  // The calibration of scene.js runs over the leading fluid block; an explicit
+  // scene lists its fluid first too.
+  sc.nFluid = nFluid;
+  sc.nBody = d->n - nFluid;
+  sc.bodyDensity.assign(d->body_density, d->body_density + d->n_bodies);
+  sc.bodyCentre.assign(d->body_centre, d->body_centre + 3 * d->n_bodies);
+  sc.mass = d->mass;
+  sc.denomRest = d->denom_rest;
+  const bool doMass = !(d->mass > 0), doDenom = !(d->denom_rest > 0);
+  if (doMass || doDenom)
+    calibrate(sc.pos, nFluid, sc.d, sc.h, p->rest_density, doMass, doDenom, sc.mass, sc.denomRest, p->box);
+  s->pourBudget = std::max(0, d->pour_budget);
+  return resetCommon(s);
+}
+
+int orc_step(orc_sim* s, double frameDt, int32_t* substeps_out) {
+  if (!s || !s->ready) return P4A_ERR_STATE;
+  apply_threads();
+  const p4a_params& p = s->params;
+  const int base = std::max(1, p.substeps);
+  const double dtTarget = (1.0 / 60) / base;
+  s->timeBank = s->timeBank + frameDt;
+  double subD = std::floor(s->timeBank / dtTarget + 1e-4);
+  const double workCap = base * 8;
+  if (subD > workCap) { subD = workCap; s->timeBank = 0; }
+  else s->timeBank -= subD * dtTarget;
+  const int sub = (int)subD;
+  s->lastSubsteps = sub;
+  s->lastAdvanced = subD * dtTarget;
+  if (substeps_out) *substeps_out = sub;
+  if (sub < 1) { s->lastAdvanced = 0; return P4A_OK; }
+  const double dt = dtTarget;
+  uploadParams(s, dt);
+  const bool dragging = s->heldBody >= 1 && s->nBodyParts > 0;
+  const float blend = (float)(1 - std::exp(-std::max(dt, 0.0) / 0.02));
+  const Params& P = s->P;
+  for (int st = 0; st < sub; st++) {
+    const int par = s->parity;
+    if (dragging) k_bodyDrag(s, s->vel[par], s->body[par], blend);
+    gridPass(s, par);
+    s->parity ^= 1;
+    s->predParity = s->parity;
+    const int par2 = s->parity;
+    int pp = s->predParity;
+    if (s->nBodyParts > 0) {
+      k_bodyClear(s);
+      k_bodyCompact(s, s->body[par2]);
+      k_bodyCentre(s, s->pred[pp], s->body[par2]);
+      k_bodySeed(s);
+      k_bodyRefLoad(s);
+    }
+    for (int it = 0; it < std::max(1, p.iterations); it++) {
+      k_lambda(P, s->pred[pp], s->lambda, s->density, s->cellStart, s->bpos, s->bpsi, s->bcellStart);
+      k_delta(P, s->pred[pp], s->pred[pp ^ 1], s->lambda, s->cellStart, s->bpos, s->bpsi, s->bcellStart);
+      pp ^= 1;
+      if (s->nBodyParts > 0) {
+        k_bodyClear(s);
+        k_bodyCentre(s, s->pred[pp], s->body[par2]);
+        k_bodySeed(s);
+        k_bodyCov(s, s->pred[pp], s->body[par2], s->rest[par2]);
+        k_bodyResolve(s);
+        k_bodyProject(s, s->pred[pp], s->body[par2], s->rest[par2]);
+      }
+    }
+    s->predParity = pp;
+    if (s->predParity != s->parity) {
+      std::copy(s->pred[s->predParity].begin(), s->pred[s->predParity].begin() + s->n,
+                s->pred[s->predParity ^ 1].begin());
+      s->predParity = s->parity;
+    }
+    k_velFromPos(P, s->pos[par2], s->vel[par2], s->pred[par2]);
+    k_xsph(P, s->pred[par2], s->vel[par2], s->density, s->corr, s->cellStart);
+    if (p.surface_tension_k > 0) {
+      k_normals(P, s->pred[par2], s->density, s->normal, s->cellStart);
+      k_tension(P, s->pred[par2], s->density, s->normal, s->corr, s->cellStart);
+    }
+    k_finalize(P, s->pos[par2], s->vel[par2], s->pred[par2], s->corr);
+    s->simTime += dt;
+  }
+  std::fill(s->statsOut.begin(), s->statsOut.end(), 0u);
+  k_stats(s, s->density, s->vel[s->parity]);
+  const double SCALE = 1024;
+  s->stats.avg_rho = s->statsOut[0] / SCALE / std::max(1, s->n);
+  s->stats.max_rho = s->statsOut[1] / SCALE;
+  s->stats.max_speed = s->statsOut[2] / SCALE;
+  s->stats.ke = s->statsOut[3] / SCALE;
+  for (int k = 0; k < 4; k++) s->stats.raw[k] = s->statsOut[k];
+  s->stats.valid = 1;
+  return P4A_OK;
+}
+
+int orc_append_fluid(orc_sim* s, const float* pos3, const float* vel3, int32_t count, int32_t* added) {
+  if (!s || !s->ready || count < 0) return P4A_ERR_ARG;
+  const int room = std::max(0, s->cap - s->n);
+  const int c = std::min(count, room);
+  if (added) *added = std::max(0, c);
+  if (c <= 0) return P4A_OK;
+  const int n = s->n, par = s->parity, pp = s->predParity;
+  for (int i = 0; i < c; i++) {
+    f4 p4 = {pos3[i * 3], pos3[i * 3 + 1], pos3[i * 3 + 2], 1.0f};
+    f4 v4 = {vel3[i * 3], vel3[i * 3 + 1], vel3[i * 3 + 2], 0.0f};
+    s->pos[par][n + i] = p4;
+    s->vel[par][n + i] = v4;
+    s->pred[pp][n + i] = p4;
+    s->density[n + i] = (float)s->params.rest_density;
+    s->lambda[n + i] = 0.0f;
+    s->corr[n + i] = f4{0, 0, 0, 0};
+    s->normal[n + i] = f4{0, 0, 0, 0};
+    for (int t = 0; t < 2; t++) { s->body[t][n + i] = u4{0, 0, 0, 0}; s->rest[t][n + i] = f4{0, 0, 0, 0}; }
+  }
+  s->n += c;
+  return P4A_OK;
+}
+
+int orc_apply_ray_impulse(orc_sim* s, const double origin[3], const double dir[3], const double impulse[3],
+                          double radius, double speedLimit) {
+  if (!s || !s->ready) return P4A_ERR_STATE;
+  if (!s->n || radius <= 0) return P4A_OK;
+  const double len = std::hypot(impulse[0], impulse[1], impulse[2]);
+  if (len <= 0) return P4A_OK;
+  double dl = std::hypot(dir[0], dir[1], dir[2]);
+  if (!(dl != 0)) dl = 1;
+  const f3 o = {(float)origin[0], (float)origin[1], (float)origin[2]};
+  const f3 dr = {(float)(dir[0] / dl), (float)(dir[1] / dl), (float)(dir[2] / dl)};
+  const f3 im = {(float)impulse[0], (float)impulse[1], (float)impulse[2]};
+  const float R = (float)radius, sl = (float)speedLimit;
+  std::vector<f4>& pos = s->pos[s->parity];
+  std::vector<f4>& vel = s->vel[s->parity];
+  // impulse (src/wgsl.js:216-248).
+  for (int i = 0; i < s->n; i++) {
+    const f3 toP = sub3(xyz(pos[i]), o);
+    const float along = dot3(toP, dr);
+    if (along <= 0.0f) continue;
+    const f3 radial = sub3(toP, mul3(dr, along));
+    const float d2 = dot3(radial, radial);
+    if (d2 >= R * R) continue;
+    const float x = 1.0f - std::sqrt(d2) / R;
+    const f3 v = xyz(vel[i]);
+    const float oldSpeed = length3(v);
+    f3 nv = add3(v, mul3(im, x * x));
+    const float ns = length3(nv);
+    const float allowed = std::max(oldSpeed, sl);
+    if (ns > allowed) nv = mul3(nv, allowed / ns);
+    vel[i] = {nv.x, nv.y, nv.z, 0.0f};
+  }
+  return P4A_OK;
+}
+
+int orc_hold_body(orc_sim* s, int32_t body1, const double target[3], double rate, double limit) {
+  if (!s) return P4A_ERR_ARG;
+  s->heldBody = (body1 >= 1 && body1 <= s->nBodies) ? body1 : -1;
+  for (int k = 0; k < 3; k++) s->heldTarget[k] = target[k];
+  s->heldRate = rate;
+  s->heldLimit = limit;
+  return P4A_OK;
+}
+int orc_release_body(orc_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  s->heldBody = -1;
+  return P4A_OK;
+}
+
+int orc_resize_box(orc_sim* s, const double newBox[3]) {
+  if (!s || !s->ready) return P4A_ERR_STATE;
+  p4a_params& p = s->params;
+  const double oldBox[3] = {p.box[0], p.box[1], p.box[2]};
+  bool moved = false;
+  for (int a = 0; a < 3; a++) if (std::fabs(newBox[a] - oldBox[a]) > 1e-9) moved = true;
+  if (!moved) return P4A_OK;
+  for (int a = 0; a < 3; a++) p.box[a] = newBox[a];
+  for (int k = 0; k < 3; k++) s->gridDim[k] = (int)std::max(1.0, std::floor(newBox[k] / s->h));
+  const int cells = s->gridDim[0] * s->gridDim[1] * s->gridDim[2];
+  const bool changed = cells != s->nCells;
+  s->nCells = cells;
+  if (changed) allocCells(s);
+  setBoundary(s);
+  s->gen++;
+  // resize (src/wgsl.js:125-157) on the live pos.
+  const float halfD = (float)(0.5 * p.spacing);
+  const float oldSize[3] = {(float)oldBox[0], (float)oldBox[1], (float)oldBox[2]};
+  const float newSize[3] = {(float)newBox[0], (float)newBox[1], (float)newBox[2]};
+  const float cMin[3] = {halfD, halfD, halfD};
+  const float cMax[3] = {(float)(newBox[0] - 0.5 * p.spacing), (float)(newBox[1] - 0.5 * p.spacing),
+                         (float)(newBox[2] - 0.5 * p.spacing)};
+  std::vector<f4>& pos = s->pos[s->parity];
+  for (int i = 0; i < s->n; i++) {
+    float* pv = &pos[i].x;
+    for (int a = 0; a < 3; a++) {
+      if (newSize[a] < oldSize[a]) {
+        const float t = std::min(std::max((pv[a] - 0.0f) / oldSize[a], 0.0f), 1.0f);
+        pv[a] = 0.0f + t * newSize[a];
+      }
+      pv[a] = std::min(std::max(pv[a], cMin[a]), cMax[a]);
+    }
+  }
+  return P4A_OK;
+}
+
+// Anisotropic kernel (src/aniso_wgsl.js:3-158) with the uniform of src/mesh.js:221-242.
+int orc_aniso(orc_sim* s, const p4a_aniso_params* ap) {
+  if (!s || !s->ready || !ap) return P4A_ERR_ARG;
+  const int n = s->n;
+  if (n <= 0) return P4A_OK;
+  if (s->smoothPos.size() < (size_t)n) { s->smoothPos.assign(n, f4{0, 0, 0, 0}); s->anisoG.assign(2 * (size_t)n, f4{0, 0, 0, 0}); s->anisoGen++; }
+  const double support = s->h;
+  const double radiusD = ap->radius_scale * support;
+  const int cells = (int)std::ceil(ap->radius_scale);
+  const double sigmaBulk = 0.15 * radiusD * radiusD;
+  const float lambdaA = (float)ap->lambda, invSupport = (float)(1 / support), sup = (float)support;
+  const float radius = (float)radiusD, kr = (float)ap->ratio, kn = (float)ap->lonely;
+  const float ks = (float)(ap->ks / sigmaBulk), stretch = (float)ap->stretch, minExtent = (float)ap->min_extent;
+  const int neps = ap->min_neighbours;
+  const int* G = s->gridDim;
+  const std::vector<f4>& pos = s->pos[s->parity];
+  const std::vector<uint32_t>& cs = s->cellStart;
+  apply_threads();
+#pragma omp parallel for schedule(dynamic, 128)
+  for (int i = 0; i < n; i++) {
+    const f3 xi = xyz(pos[i]);
+    I3 c;
+    c.x = std::min(std::max(f2i_sat(std::floor((xi.x - 0.0f) * invSupport)), 0), G[0] - 1);
+    c.y = std::min(std::max(f2i_sat(std::floor((xi.y - 0.0f) * invSupport)), 0), G[1] - 1);
+    c.z = std::min(std::max(f2i_sat(std::floor((xi.z - 0.0f) * invSupport)), 0), G[2] - 1);
+    const int x0 = std::max(c.x - cells, 0), x1 = std::min(c.x + cells, G[0] - 1);
+    const float r2max = radius * radius;
+    const float invR = 1.0f / radius;
+    const f3 rel = {xi.x - 0.0f, xi.y - 0.0f, xi.z - 0.0f};
+    f3 sd = {0, 0, 0};
+    m3 m2 = {{{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}};
+    float wsum = 0.0f;
+    int nn = 0;
+    for (int dz = -cells; dz <= cells; dz++) {
+      const int z = c.z + dz;
+      if (z < 0 || z >= G[2]) continue;
+      const float dzMin = std::max(std::max((float)z * sup - rel.z, rel.z - (float)(z + 1) * sup), 0.0f);
+      const float dz2 = dzMin * dzMin;
+      if (dz2 >= r2max) continue;
+      for (int dy = -cells; dy <= cells; dy++) {
+        const int y = c.y + dy;
+        if (y < 0 || y >= G[1]) continue;
+        const float dyMin = std::max(std::max((float)y * sup - rel.y, rel.y - (float)(y + 1) * sup), 0.0f);
+        if (dz2 + dyMin * dyMin >= r2max) continue;
+        const uint32_t rowBase = (uint32_t)((z * G[1] + y) * G[0]);
+        const uint32_t jb = cs[rowBase + x0], je = cs[rowBase + x1 + 1];
+        for (uint32_t j = jb; j < je; j++) {
+          const f3 d = sub3(xyz(pos[j]), xi);
+          const float r2 = dot3(d, d);
+          if (r2 >= r2max) continue;
+          const float t = std::sqrt(r2) * invR;
+          const float w = 1.0f - t * t * t;
+          sd = fma3(w, d, sd);
+          m2.c[0] = fma3(d.x * w, d, m2.c[0]);
+          m2.c[1] = fma3(d.y * w, d, m2.c[1]);
+          m2.c[2] = fma3(d.z * w, d, m2.c[2]);
+          wsum = wsum + w;
+          nn = nn + 1;
+        }
+      }
+    }
+    auto storeG = [&](const m3& Gm, float last) {
+      s->anisoG[i * 2 + 0] = {elc(Gm, 0, 0), elc(Gm, 1, 0), elc(Gm, 2, 0), elc(Gm, 1, 1)};
+      s->anisoG[i * 2 + 1] = {elc(Gm, 2, 1), elc(Gm, 2, 2), det3(Gm), last};
+    };
+    if (wsum <= 0.0f) {
+      s->smoothPos[i] = {xi.x, xi.y, xi.z, 0.0f};
+      storeG(scale3(ident3(), kn / sup), 0.0f);
+      continue;
+    }
+    const f3 dbar = {sd.x / wsum, sd.y / wsum, sd.z / wsum};
+    s->smoothPos[i] = {xi.x + dbar.x * lambdaA, xi.y + dbar.y * lambdaA, xi.z + dbar.z * lambdaA, 0.0f};
+    m3 cov;
+    const float db[3] = {dbar.x, dbar.y, dbar.z};
+    for (int k = 0; k < 3; k++) {
+      cov.c[k] = {m2.c[k].x / wsum - dbar.x * db[k], m2.c[k].y / wsum - dbar.y * db[k],
+                  m2.c[k].z / wsum - dbar.z * db[k]};
+    }
+    // jacobi (src/aniso_wgsl.js:30-55)
+    m3 a = cov, v = ident3();
+    for (int sweep = 0; sweep < 6; sweep++)
+      for (int pI = 0; pI < 2; pI++)
+        for (int qI = pI + 1; qI < 3; qI++) {
+          const float apq = elc(a, qI, pI);
+          if (std::fabs(apq) < 1.0e-12f) continue;
+          const float theta = (elc(a, qI, qI) - elc(a, pI, pI)) / (2.0f * apq);
+          const float sgn = theta > 0.0f ? 1.0f : (theta < 0.0f ? -1.0f : 0.0f);
+          float t = sgn / (std::fabs(theta) + std::sqrt(theta * theta + 1.0f));
+          if (theta == 0.0f) t = 1.0f;
+          const float cth = 1.0f / std::sqrt(t * t + 1.0f);
+          const float sn = t * cth;
+          m3 r = ident3();
+          el(r, pI, pI) = cth; el(r, qI, qI) = cth;
+          el(r, qI, pI) = sn; el(r, pI, qI) = -sn;
+          a = matmul(matmul(transpose3(r), a), r);
+          v = matmul(v, r);
+        }
+    const m3& R = v;
+    const f3 sig = {elc(a, 0, 0), elc(a, 1, 1), elc(a, 2, 2)};
+    const float s1 = std::max(sig.x, std::max(sig.y, sig.z));
+    const float sl = s1 / kr;
+    f3 ext = {ks * std::max(sig.x, sl), ks * std::max(sig.y, sl), ks * std::max(sig.z, sl)};
+    const float den = std::max(1.0f, std::max(ext.x, std::max(ext.y, ext.z)) / stretch);
+    ext = {ext.x / den, ext.y / den, ext.z / den};
+    ext = {std::max(ext.x, minExtent), std::max(ext.y, minExtent), std::max(ext.z, minExtent)};
+    const f3 inv = {1.0f / (sup * ext.x), 1.0f / (sup * ext.y), 1.0f / (sup * ext.z)};
+    m3 D = {{{inv.x, 0, 0}, {0, inv.y, 0}, {0, 0, inv.z}}};
+    const m3 Gan = matmul(matmul(R, D), transpose3(R));
+    const m3 Giso = scale3(ident3(), kn / sup);
+    const float lo = (float)neps * 0.4f, hi = (float)neps * 1.6f;
+    float tt = ((float)nn - lo) / (hi - lo);
+    tt = std::min(std::max(tt, 0.0f), 1.0f);
+    const float w = tt * tt * (3.0f - 2.0f * tt);
+    m3 Gm;
+    for (int k = 0; k < 3; k++) {
+      Gm.c[k] = {Giso.c[k].x * (1.0f - w) + Gan.c[k].x * w, Giso.c[k].y * (1.0f - w) + Gan.c[k].y * w,
+                 Giso.c[k].z * (1.0f - w) + Gan.c[k].z * w};
+    }
+    storeG(Gm, (float)nn);
+  }
+  return P4A_OK;
+}
+
+int orc_get_info(const orc_sim* s, p4a_info* o) {
+  if (!s || !o) return P4A_ERR_ARG;
+  *o = p4a_info{};
+  o->n = s->n; o->n_fluid = s->sc.nFluid; o->n_body_parts = s->nBodyParts; o->n_bodies = s->nBodies;
+  o->n_boundary = s->nBoundary; o->cap = s->cap; o->pour_budget = s->pourBudget;
+  for (int k = 0; k < 3; k++) o->grid_dim[k] = s->gridDim[k];
+  o->n_cells = s->nCells; o->parity = s->parity; o->pred_parity = s->predParity; o->gen = s->gen;
+  o->last_substeps = s->lastSubsteps; o->h = s->h; o->mass = s->sc.mass; o->denom_rest = s->sc.denomRest;
+  o->sim_time = s->simTime; o->last_advanced = s->lastAdvanced; o->time_bank = s->timeBank;
+  o->body_scale = s->bodyScale; o->cov_scale = s->covScale; o->held_body = s->heldBody;
+  o->aniso_gen = s->anisoGen;
+  return P4A_OK;
+}
+
+int orc_stats(const orc_sim* s, p4a_stats* out) {
+  if (!s || !out) return P4A_ERR_ARG;
+  *out = s->stats;
+  return P4A_OK;
+}
+
+int orc_buffer(orc_sim* s, int32_t id, int32_t which, void** ptr, size_t* bytes) {
+  if (!s || !ptr) return P4A_ERR_ARG;
+  const int w = which < 0 ? s->parity : (which & 1);
+  auto set = [&](void* p, size_t b) { *ptr = p; if (bytes) *bytes = b; return P4A_OK; };
+  switch (id) {
+    case P4A_BUF_POS: return set(s->pos[w].data(), s->pos[w].size() * 16);
+    case P4A_BUF_VEL: return set(s->vel[w].data(), s->vel[w].size() * 16);
+    case P4A_BUF_PRED: return set(s->pred[w].data(), s->pred[w].size() * 16);
+    case P4A_BUF_BODY: return set(s->body[w].data(), s->body[w].size() * 16);
+    case P4A_BUF_REST: return set(s->rest[w].data(), s->rest[w].size() * 16);
+    case P4A_BUF_DENSITY: return set(s->density.data(), s->density.size() * 4);
+    case P4A_BUF_LAMBDA: return set(s->lambda.data(), s->lambda.size() * 4);
+    case P4A_BUF_CORR: return set(s->corr.data(), s->corr.size() * 16);
+    case P4A_BUF_NORMAL: return set(s->normal.data(), s->normal.size() * 16);
+    case P4A_BUF_CELL_START: return set(s->cellStart.data(), s->cellStart.size() * 4);
+    case P4A_BUF_BPOS: return set(s->bpos.data(), s->bpos.size() * 16);
+    case P4A_BUF_BPSI: return set(s->bpsi.data(), s->bpsi.size() * 4);
+    case P4A_BUF_BCELL_START: return set(s->bcellStart.data(), s->bcellStart.size() * 4);
+    case P4A_BUF_BODY_CENTRE: return set(s->bodyCentre.data(), s->bodyCentre.size() * 16);
+    case P4A_BUF_BODY_REF: return set(s->bodyRef.data(), s->bodyRef.size() * 16);
+    case P4A_BUF_BODY_ROT: return set(s->bodyRot.data(), s->bodyRot.size() * 16);
+    case P4A_BUF_BODY_INFO: return set(s->bodyInfo.data(), s->bodyInfo.size() * 16);
+    case P4A_BUF_STATS_OUT: return set(s->statsOut.data(), s->statsOut.size() * 4);
+    case P4A_BUF_SMOOTH_POS: return set(s->smoothPos.data(), s->smoothPos.size() * 16);
+    case P4A_BUF_ANISO_G: return set(s->anisoG.data(), s->anisoG.size() * 16);
+    default: return P4A_ERR_ARG;
+  }
+}
+
+int orc_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, const float* pos,
+                  const float* vel, const uint32_t* body, const float* rest, float* pos_out,
+                  float* vel_out, float* pred_out, uint32_t* body_out, float* rest_out,
+                  uint32_t* cell_start, uint32_t* slot_out) {
+  if (!grid || n < 0) return P4A_ERR_ARG;
+  Params P{};
+  for (int k = 0; k < 3; k++) { P.boxMin[k] = grid->box_min[k]; P.gridDim[k] = grid->dim[k]; }
+  P.h = grid->h; P.dt = dt; P.gravity = gravity; P.n = (uint32_t)n;
+  P.nCells = (uint32_t)(grid->dim[0] * grid->dim[1] * grid->dim[2]);
+  std::vector<f4> vp(n), vv(n), vpred(n);
+  std::memcpy(vp.data(), pos, (size_t)n * 16);
+  std::memcpy(vv.data(), vel, (size_t)n * 16);
+  apply_threads();
+  k_predict(P, vp, vv, vpred);
+  std::vector<uint32_t> cnt(P.nCells + 1), cs(P.nCells + 2, 0u), cur(P.nCells + 1), slot(n);
+  k_sort_slots(P, vpred, cnt, cs, cur, slot);
+  for (int i = 0; i < n; i++) {
+    const uint32_t s = slot[i];
+    std::memcpy(pos_out + 4 * (size_t)s, &vp[i], 16);
+    std::memcpy(vel_out + 4 * (size_t)s, &vv[i], 16);
+    std::memcpy(pred_out + 4 * (size_t)s, &vpred[i], 16);
+    if (body && body_out) std::memcpy(body_out + 4 * (size_t)s, body + 4 * (size_t)i, 16);
+    if (rest && rest_out) std::memcpy(rest_out + 4 * (size_t)s, rest + 4 * (size_t)i, 16);
+    if (slot_out) slot_out[i] = s;
+  }
+  std::memcpy(cell_start, cs.data(), (P.nCells + 1) * 4);
+  return P4A_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,12 @@
+"""particles4all_b200 — B200-native (sm_100a CUDA) Particles4All simulation step.
+
+The product is libp4a.so (C ABI in include/p4a.h); this package is its Python
+host: `Sim` mirrors the reference's `class Sim` (src/sim.js), `default_params`
+its `defaultParams` (src/scene.js:11-39), and `configs` the seeded benchmark
+scenes.
+"""
+from ._lib import P4AError, device_available, lib  # noqa: F401
+from .params import PRESETS, default_aniso, default_params  # noqa: F401
+from .sim import Sim  # noqa: F401
+
+__all__ = ["Sim", "default_params", "default_aniso", "PRESETS", "P4AError", "device_available", "lib"]

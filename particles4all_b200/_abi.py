@@ -1,0 +1,97 @@
+"""ctypes mirror of the C structs and constants declared in include/p4a.h."""
+import ctypes as C
+
+P4A_OK, P4A_ERR_ARG, P4A_ERR_OOM, P4A_ERR_CUDA = 0, 1, 2, 3
+P4A_ERR_TIMEOUT, P4A_ERR_CAPACITY, P4A_ERR_STATE, P4A_ERR_NODEV = 4, 5, 6, 7
+
+SHAPES = {"sphere": 0, "torus": 1, "box": 2}
+
+BUF = dict(
+    pos=0, vel=1, pred=2, body=3, rest=4, density=5, lambda_=6, corr=7, normal=8,
+    cellStart=9, bpos=10, bpsi=11, bcellStart=12, bodyCentre=13, bodyRef=14,
+    bodyRot=15, bodyInfo=16, statsOut=17, smoothPos=18, aniso=19,
+)
+# element dtype / components of each buffer (numpy dtype string, components)
+BUF_LAYOUT = {
+    0: ("f4", 4), 1: ("f4", 4), 2: ("f4", 4), 3: ("u4", 4), 4: ("f4", 4),
+    5: ("f4", 1), 6: ("f4", 1), 7: ("f4", 4), 8: ("f4", 4), 9: ("u4", 1),
+    10: ("f4", 4), 11: ("f4", 1), 12: ("u4", 1), 13: ("f4", 4), 14: ("f4", 4),
+    15: ("f4", 4), 16: ("f4", 4), 17: ("u4", 1), 18: ("f4", 4), 19: ("f4", 4),
+}
+A, B, LIVE = 0, 1, -1
+
+
+class BodySpec(C.Structure):
+    _fields_ = [("shape", C.c_int32), ("density", C.c_double), ("start_y", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("spacing", C.c_double), ("rest_density", C.c_double), ("gravity", C.c_double),
+        ("substeps", C.c_int32), ("iterations", C.c_int32),
+        ("cfm_epsilon_rel", C.c_double), ("s_corr_k", C.c_double), ("s_corr_dq", C.c_double),
+        ("xsph_c", C.c_double), ("omega", C.c_double), ("sor_average", C.c_int32),
+        ("surface_tension_k", C.c_double), ("target_particle_count", C.c_int32),
+        ("box", C.c_double * 3), ("n_bodies", C.c_int32), ("bodies", C.POINTER(BodySpec)),
+        ("body_size", C.c_double), ("no_boundary", C.c_int32), ("pour", C.c_int32),
+        ("cfm_epsilon_abs", C.c_double),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("pos", C.c_void_p), ("vel", C.c_void_p), ("phase", C.c_void_p),
+        ("rest", C.c_void_p), ("n_bodies", C.c_int32), ("body_density", C.c_void_p),
+        ("body_centre", C.c_void_p), ("mass", C.c_double), ("denom_rest", C.c_double),
+        ("pour_budget", C.c_int32),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("n_fluid", C.c_int32), ("n_body_parts", C.c_int32),
+        ("n_bodies", C.c_int32), ("n_boundary", C.c_int32), ("cap", C.c_int32),
+        ("pour_budget", C.c_int32), ("grid_dim", C.c_int32 * 3), ("n_cells", C.c_int32),
+        ("parity", C.c_int32), ("pred_parity", C.c_int32), ("gen", C.c_int32),
+        ("last_substeps", C.c_int32), ("h", C.c_double), ("mass", C.c_double),
+        ("denom_rest", C.c_double), ("sim_time", C.c_double), ("last_advanced", C.c_double),
+        ("time_bank", C.c_double), ("body_scale", C.c_double), ("cov_scale", C.c_double),
+        ("held_body", C.c_int32), ("aniso_gen", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("avg_rho", C.c_double), ("max_rho", C.c_double), ("max_speed", C.c_double),
+        ("ke", C.c_double), ("raw", C.c_uint32 * 4), ("valid", C.c_int32),
+    ]
+
+
+class AnisoParams(C.Structure):
+    _fields_ = [
+        ("ratio", C.c_double), ("ks", C.c_double), ("stretch", C.c_double),
+        ("lonely", C.c_double), ("min_neighbours", C.c_int32), ("lambda_", C.c_double),
+        ("radius_scale", C.c_double), ("min_extent", C.c_double),
+    ]
+
+
+class Grid(C.Structure):
+    _fields_ = [("box_min", C.c_float * 3), ("h", C.c_float), ("dim", C.c_int32 * 3)]
+
+
+class SceneCounts(C.Structure):
+    _fields_ = [
+        ("n", C.c_int32), ("n_fluid", C.c_int32), ("n_body", C.c_int32),
+        ("n_bodies", C.c_int32), ("n_boundary", C.c_int32), ("mass", C.c_double),
+        ("denom_rest", C.c_double), ("h", C.c_double),
+    ]
+
+
+class PhaseTime(C.Structure):
+    _fields_ = [("name", C.c_char * 24), ("ms", C.c_double), ("launches", C.c_int64)]
+
+
+def info_dict(info):
+    d = {k: getattr(info, k) for k, _ in Info._fields_}
+    d["grid_dim"] = list(info.grid_dim)
+    return d

@@ -1,0 +1,219 @@
+"""Seeded synthetic scenes for the benchmark workloads.
+
+The reference has no benchmark scenes of its own (its presets are browser
+settings); these generators build the scenes the workload definitions name,
+as explicit scenes for Sim.reset_scene:
+
+  dam_break_32k     32,768 fluid particles on a 32^3 lattice, d = 0.5, jitter
+                    U(+-0.01 d), in the corner of a [0,40]x[0,24]x[0,20] box;
+                    h = 2d = 1; rho0 = 1 with the mass normalised on the
+                    unjittered lattice; CFM epsilon 100 (absolute); 4
+                    iterations; 2 substeps per 1/60 s; g = 9.8; no bodies,
+                    no tension.
+  medium_bodies_264k  262,144 fluid particles on a 64^3 lattice in the box
+                    scaled x2, plus 8 rigid 6x6x6 cubes (1,728 particles) at
+                    density 0.5 rho0 with seeded orientations and positions
+                    above the water; surface tension 0.5; XSPH c = 0.01;
+                    anisotropic pass k_r = 4, N_eps = 25, lambda = 0.9.
+  large_hose_2m     2,097,152 fluid particles on a 128^3 lattice in the box
+                    scaled x4, 64 seeded boxes/spheres 4-10 particles across
+                    at densities U[0.3, 1.5] rho0, tension on, 8 iterations,
+                    and a hose of 2,048 particles per step at 3 m/s until the
+                    total reaches 2.5M.
+
+Values the workloads leave open take the dam-break values (rho0 = 1,
+epsilon = 100, g = 9.8, 2 substeps).
+"""
+import math
+
+import numpy as np
+
+KERNEL_POLY6 = 315.0 / (64.0 * math.pi)
+
+
+def lattice_mass(d, h, rho0=1.0):
+    """Particle mass that makes the density of an unjittered cubic lattice of
+    spacing d equal rho0 with the poly6 kernel of radius h (self term included)."""
+    m = int(math.ceil(h / d)) + 1
+    r = np.arange(-m, m + 1) * d
+    x, y, z = np.meshgrid(r, r, r, indexing="ij")
+    r2 = (x * x + y * y + z * z).ravel()
+    h2 = h * h
+    t = h2 - r2[r2 < h2]
+    w = KERNEL_POLY6 / h ** 9 * np.sum(t * t * t)
+    return rho0 / w
+
+
+def _rotation(rng):
+    """A uniformly random rotation matrix (from a normalised Gaussian quaternion)."""
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([
+        [1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+        [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+        [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)],
+    ])
+
+
+def _fluid_lattice(nx, ny, nz, d, jitter, rng, origin):
+    ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    base = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1).astype(np.float64)
+    pos = origin + (base + 0.5) * d
+    pos += rng.uniform(-jitter, jitter, size=pos.shape)
+    return pos
+
+
+def _body_points(shape, across, d):
+    """Local lattice points of a box (across^3) or a sphere of diameter across."""
+    r = (np.arange(across) - (across - 1) / 2.0) * d
+    x, y, z = np.meshgrid(r, r, r, indexing="ij")
+    pts = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    if shape == "sphere":
+        rad = across * d / 2.0
+        pts = pts[np.sum(pts * pts, 1) <= rad * rad + 1e-9]
+    return pts - pts.mean(0)
+
+
+def _assemble(fluid, bodies, params, mass, pour_budget=0):
+    """Scene dict: fluid first, then each body's particles (rest = world offset)."""
+    n_f = fluid.shape[0]
+    n_b = sum(b["offsets"].shape[0] for b in bodies)
+    n = n_f + n_b
+    pos = np.zeros((n, 4), np.float32)
+    rest = np.zeros((n, 4), np.float32)
+    phase = np.zeros((n, 4), np.uint32)
+    pos[:n_f, :3] = fluid
+    o = n_f
+    for k, b in enumerate(bodies):
+        m = b["offsets"].shape[0]
+        pos[o:o + m, :3] = b["centre"] + b["offsets"]
+        rest[o:o + m, :3] = b["offsets"]
+        phase[o:o + m, 0] = k + 1
+        o += m
+    return {
+        "pos": pos, "vel": np.zeros((n, 4), np.float32), "rest": rest, "phase": phase,
+        "n_bodies": len(bodies),
+        "body_density": np.array([b["density"] for b in bodies], np.float64),
+        "body_centre": np.array([b["centre"] for b in bodies], np.float64).reshape(-1, 3),
+        "mass": mass, "denom_rest": 0.0, "pour_budget": pour_budget, "n_fluid": n_f,
+    }
+
+
+def _place_bodies(rng, count, lo, hi, min_dist):
+    centres = []
+    tries = 0
+    while len(centres) < count and tries < 100000:
+        tries += 1
+        c = rng.uniform(lo, hi)
+        if all(np.linalg.norm(c - e) >= min_dist for e in centres):
+            centres.append(c)
+    if len(centres) < count:
+        raise ValueError("could not place the bodies without overlap")
+    return centres
+
+
+def _base_params(box, iterations, tension, xsph, substeps=2):
+    return {
+        "spacing": 0.5, "restDensity": 1.0, "gravity": 9.8, "substeps": substeps,
+        "iterations": iterations, "cfmEpsilonRel": 0.01, "cfmEpsilonAbs": 100.0,
+        "sCorrK": 0.1, "sCorrDq": 0.3, "xsphC": xsph, "omega": 1.0, "sorAverage": False,
+        "surfaceTensionK": tension, "box": list(box), "bodies": [], "bodySize": 0,
+        "noBoundary": False, "pour": False,
+    }
+
+
+def dam_break_32k(seed=0, side=32):
+    """The plain single-scene dam break (side^3 lattice; side = 32 is the workload)."""
+    d, h = 0.5, 1.0
+    rng = np.random.default_rng(seed)
+    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
+    params = _base_params([40.0, 24.0, 20.0], iterations=4, tension=0.0, xsph=0.05)
+    return params, _assemble(fluid, [], params, lattice_mass(d, h))
+
+
+def medium_bodies_264k(seed=1, side=64, n_cubes=8, cube=6):
+    """The medium scene with 8 floating cubes (side = 64 is the workload)."""
+    d, h = 0.5, 1.0
+    rng = np.random.default_rng(seed)
+    box = np.array([80.0, 48.0, 40.0]) * (side / 64.0)
+    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
+    top = d + side * d
+    span = cube * d
+    lo = np.array([span + 1.0, top + span, span + 1.0])
+    hi = np.array([box[0] - span - 1.0, min(box[1] - span - 1.0, top + 3 * span), box[2] - span - 1.0])
+    centres = _place_bodies(rng, n_cubes, lo, hi, min_dist=2.0 * span)
+    local = _body_points("box", cube, d)
+    bodies = [{"centre": c, "offsets": local @ _rotation(rng).T, "density": 0.5} for c in centres]
+    params = _base_params(box, iterations=4, tension=0.5, xsph=0.01)
+    return params, _assemble(fluid, bodies, params, lattice_mass(d, h))
+
+
+def medium_aniso_params():
+    """Anisotropic-kernel settings of the medium workload: k_r = 4, N_eps = 25,
+    lambda = 0.9. Yu & Turk's k_s = 1400 is the constant that makes k_s * sigma
+    about 1 for a full neighbourhood at their particle scale; the reference
+    expresses the same normalisation as anisoKs / sigma_bulk with anisoKs = 1
+    (src/mesh.js:226,238), which is what is used here."""
+    return {"ratio": 4.0, "ks": 1.0, "stretch": 2.0, "lonely": 1.0, "min_neighbours": 25,
+            "lambda": 0.9, "radius_scale": 2.0, "min_extent": 0.0}
+
+
+def large_hose_2m(seed=2, side=128, n_bodies=64, target_total=2_500_000):
+    """The large scene with 64 mixed bodies and a hose (side = 128 is the workload)."""
+    d, h = 0.5, 1.0
+    rng = np.random.default_rng(seed)
+    box = np.array([160.0, 96.0, 80.0]) * (side / 128.0)
+    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
+    top = d + side * d
+    bodies = []
+    lo = np.array([6.0, top + 6.0, 6.0])
+    hi = np.array([box[0] - 6.0, box[1] - 6.0, box[2] - 6.0])
+    centres = _place_bodies(rng, n_bodies, lo, hi, min_dist=6.0)
+    for c in centres:
+        shape = "box" if rng.random() < 0.5 else "sphere"
+        across = int(rng.integers(4, 11))
+        local = _body_points(shape, across, d) @ _rotation(rng).T
+        bodies.append({"centre": c, "offsets": local, "density": float(rng.uniform(0.3, 1.5))})
+    params = _base_params(box, iterations=8, tension=0.5, xsph=0.01)
+    scene = _assemble(fluid, bodies, params, lattice_mass(d, h))
+    scene["pour_budget"] = max(0, target_total - scene["pos"].shape[0])
+    return params, scene
+
+
+class Hose:
+    """A hose emitting `per_step` particles per step at `speed` from the near wall:
+    square k x k lattice layers (k = ceil(sqrt(per_step))) with seeded jitter, the
+    layered emitter of src/main.js:106-160 at a fixed rate."""
+
+    def __init__(self, box, d, per_step=2048, speed=3.0, height=0.6, seed=22222, limit=None):
+        self.box, self.d, self.per_step, self.speed = box, d, per_step, speed
+        self.k = int(math.ceil(math.sqrt(per_step)))
+        self.nozzle = np.array([2.0 * d + d, height * box[1], 0.5 * box[2]])
+        self.rng = np.random.default_rng(seed)
+        self.left = limit
+
+    def emit(self):
+        n = self.per_step if self.left is None else min(self.per_step, self.left)
+        if n <= 0:
+            return None, None
+        k, d = self.k, self.d
+        iy, iz = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
+        yz = np.stack([iy.ravel(), iz.ravel()], 1)[:n].astype(np.float64)
+        pos = np.zeros((n, 3))
+        pos[:, 0] = self.nozzle[0]
+        pos[:, 1] = self.nozzle[1] + (yz[:, 0] - (k - 1) / 2.0) * d
+        pos[:, 2] = self.nozzle[2] + (yz[:, 1] - (k - 1) / 2.0) * d
+        pos += self.rng.uniform(-0.001 * d, 0.001 * d, size=pos.shape)
+        vel = np.zeros((n, 3))
+        vel[:, 0] = self.speed
+        if self.left is not None:
+            self.left -= n
+        return pos.astype(np.float32), vel.astype(np.float32)
+
+
+WORKLOADS = {
+    "dam_break_32k": dam_break_32k,
+    "medium_bodies_264k": medium_bodies_264k,
+    "large_hose_2m": large_hose_2m,
+}

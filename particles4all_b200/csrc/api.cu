@@ -1,0 +1,1074 @@
+// api.cu — the C ABI of include/p4a.h: host orchestration of the simulation step.
+//
+// This replaces the reference's `class Sim` (src/sim.js:9-814). The schedule of a
+// substep follows src/sim.js:458-596 with these B200-side fusions:
+//   predict            recomputed inside the key and reorder passes (never stored)
+//   grid pass          key_count -> scan -> fill -> reorder (kernels_grid.cu)
+//   bodies pass        one CTA per body (kernels_body.cu)
+//   k iterations       lambda, delta (+ velFromPos on the last), body_match
+//   odd-k pred copy    fused into the finalize kernel
+//   finish             xsph+finalize, or xsph+normals then tension+finalize
+//   stats              fused into the last substep's finalize
+// The time bank, substep count, uniform packing and parity bookkeeping are the
+// reference's, in double precision like the JS.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/p4a.h"
+#include "p4a_internal.h"
+#include "scene.h"
+
+using namespace p4a;
+
+namespace {
+const double kPi = 3.14159265358979323846;
+
+// Kernel names for the per-kernel timing of p4a_profile_* (the counterpart of the
+// reference's GpuTimer marks 'predict', 'grid', 'bodies', 'solve', 'finish', 'stats').
+enum Phase {
+  PH_DRAG, PH_KEY_COUNT, PH_SCAN, PH_FILL, PH_REORDER, PH_BODY_SEED, PH_LAMBDA, PH_DELTA,
+  PH_BODY_MATCH, PH_XSPH_FINALIZE, PH_XSPH_NORMALS, PH_TENSION_FINALIZE, PH_ANISO, PH_IMPULSE,
+  PH_RESIZE, PH_STATS_CLEAR, PH_COUNT, PH_END = PH_COUNT
+};
+const char* const kPhaseNames[PH_COUNT] = {
+    "body_drag", "key_count", "scan", "fill", "reorder", "body_seed", "lambda", "delta",
+    "body_match", "xsph_finalize", "xsph_normals", "tension_finalize", "aniso", "impulse",
+    "resize", "stats_clear"};
+
+std::atomic<uint64_t> g_launches{0};
+}  // namespace
+
+struct p4a_sim {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  std::string err;
+  p4a_params params{};
+  std::vector<p4a_body_spec> specs;
+  HostScene sc;
+  int n = 0, cap = 0, pourBudget = 0, nBoundary = 0, nBodies = 0, nBodyParts = 0;
+  double h = 0;
+  int gridDim[3] = {1, 1, 1};
+  int nCells = 1;
+  DevScene d{};
+  std::vector<void*> sceneAllocs;  // freed on reset / destroy
+  std::vector<void*> cellAllocs;   // freed on reset / resize
+  std::vector<void*> boundaryAllocs;
+  std::vector<uint32_t> bodyStartHost;
+  double bodyScale = 0, covScale = 0;
+  int parity = 0, predParity = 0, gen = 0;
+  double simTime = 0, timeBank = 0, lastAdvanced = 0;
+  int lastSubsteps = 0;
+  int heldBody = -1;
+  double heldTarget[3] = {0, 0, 0}, heldRate = 10, heldLimit = 4;
+  SimParams P{};
+  uint32_t scanEpoch = 0;
+  // readback (stats, error word, pose), latest-completed semantics
+  uint32_t* pinned = nullptr;  // [8 stats][1 err][pad] then pose floats
+  size_t pinnedBytes = 0;
+  cudaEvent_t readEvent = nullptr;
+  bool readPending = false;
+  bool poseValid = false;
+  p4a_stats stats{};
+  std::vector<float> pose;  // per body: centre xyz, then 3 rows xyz(w)
+  // aniso outputs
+  float4* smoothPos = nullptr;
+  float4* anisoG = nullptr;
+  size_t anisoCap = 0;
+  int anisoGen = 0;
+  bool ready = false;
+  // per-kernel timing (p4a_profile_*)
+  bool prof = false;
+  std::vector<cudaEvent_t> evPool;
+  std::vector<int> evPhase;
+  int evUsed = 0;
+  double phaseMs[PH_COUNT] = {};
+  long long phaseLaunches[PH_COUNT] = {};
+};
+
+namespace {
+
+int fail(p4a_sim* s, int code, const char* fmt, ...) {
+  if (s) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    s->err = buf;
+  }
+  return code;
+}
+
+#define CUDA_TRY(s, call)                                                              \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      return fail((s), e_ == cudaErrorMemoryAllocation ? P4A_ERR_OOM : P4A_ERR_CUDA,   \
+                  "%s: %s", #call, cudaGetErrorString(e_));                            \
+    }                                                                                  \
+  } while (0)
+
+// Accumulates the recorded kernel intervals into the per-kernel totals.
+int resolve_marks(p4a_sim* s) {
+  if (s->evUsed == 0) return P4A_OK;
+  CUDA_TRY(s, cudaEventSynchronize(s->evPool[s->evUsed - 1]));
+  for (int k = 0; k + 1 < s->evUsed; k++) {
+    const int ph = s->evPhase[k];
+    if (ph >= PH_COUNT) continue;
+    float ms = 0.0f;
+    CUDA_TRY(s, cudaEventElapsedTime(&ms, s->evPool[k], s->evPool[k + 1]));
+    s->phaseMs[ph] += ms;
+    s->phaseLaunches[ph]++;
+  }
+  s->evUsed = 0;
+  return P4A_OK;
+}
+
+// Called before each kernel the handle launches (and with PH_END after the last):
+// counts launches and, with profiling on, records the event that opens the interval.
+void mark(p4a_sim* s, int phase) {
+  if (phase < PH_COUNT && phase != PH_STATS_CLEAR) g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (!s->prof) return;
+  if (s->evUsed == (int)s->evPool.size()) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    s->evPool.push_back(e);
+    s->evPhase.push_back(PH_END);
+  }
+  cudaEventRecord(s->evPool[s->evUsed], s->stream);
+  s->evPhase[s->evUsed] = phase;
+  s->evUsed++;
+  if (phase == PH_END && s->evUsed >= 4096) resolve_marks(s);  // keeps the event pool bounded
+}
+
+template <class T>
+int dalloc(p4a_sim* s, std::vector<void*>& list, T** out, size_t count) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(16, count * sizeof(T));
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess)
+    return fail(s, P4A_ERR_OOM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  e = cudaMemsetAsync(p, 0, bytes, s->stream);
+  if (e != cudaSuccess) {
+    cudaFree(p);
+    return fail(s, P4A_ERR_CUDA, "cudaMemsetAsync: %s", cudaGetErrorString(e));
+  }
+  list.push_back(p);
+  *out = (T*)p;
+  return P4A_OK;
+}
+
+void free_list(std::vector<void*>& list) {
+  for (void* p : list) cudaFree(p);
+  list.clear();
+}
+
+// uploadParams(dt) (src/sim.js:371-413).
+void pack_params(p4a_sim* s, double dt) {
+  const p4a_params& p = s->params;
+  SimParams& F = s->P;
+  const double h = s->h, d = p.spacing;
+  F.boxMin[0] = F.boxMin[1] = F.boxMin[2] = 0.0f;
+  F.dt = (float)dt;
+  for (int k = 0; k < 3; k++) F.boxMax[k] = (float)p.box[k];
+  F.h = (float)h;
+  for (int k = 0; k < 3; k++) F.gridDim[k] = s->gridDim[k];
+  F.h2 = (float)(h * h);
+  const double halfD = 0.5 * d;
+  for (int k = 0; k < 3; k++) F.clampMin[k] = (float)halfD;
+  const double poly6 = 315 / (64 * kPi * std::pow(h, 9));
+  F.poly6 = (float)poly6;
+  for (int k = 0; k < 3; k++) F.clampMax[k] = (float)(p.box[k] - halfD);
+  F.spikyGrad = (float)(-45 / (kPi * std::pow(h, 6)));
+  F.gravity = (float)p.gravity;
+  F.mass = (float)s->sc.mass;
+  F.rho0 = (float)p.rest_density;
+  F.invRho0 = (float)(1 / p.rest_density);
+  F.cfmEps = (float)(p.cfm_epsilon_abs > 0 ? p.cfm_epsilon_abs
+                                           : std::max(1e-9, p.cfm_epsilon_rel * s->sc.denomRest));
+  F.sCorrK = (float)(p.s_corr_k / (s->sc.denomRest * std::max(1, p.iterations)));
+  const double rq = p.s_corr_dq * h, tq = h * h - rq * rq;
+  const double wq = poly6 * tq * tq * tq;
+  F.sCorrWq = (float)(wq > 0 ? 1 / wq : 0);
+  F.xsphC = (float)p.xsph_c;
+  F.n = (uint32_t)s->n;
+  F.nCells = (uint32_t)s->nCells;
+  F.nBoundary = p.no_boundary ? 0u : (uint32_t)s->nBoundary;
+  F.nBodyParts = (uint32_t)s->nBodyParts;
+  F.nBodies = (uint32_t)s->nBodies;
+  F.bodyScale = (float)s->bodyScale;
+  F.covScale = (float)s->covScale;
+  F.omega = (float)p.omega;
+  F.sorAverage = p.sor_average ? 1u : 0u;
+  F.invDt = (float)(dt > 0 ? 1 / dt : 0);
+  F.volume = (float)(s->sc.mass / p.rest_density);
+  F.tension = (float)p.surface_tension_k;
+  F.cohes = (float)(32 / (kPi * std::pow(h, 9)));
+  F.cohesTerm = (float)(std::pow(h, 6) / 64);
+}
+
+uint32_t next_epoch(p4a_sim* s) {
+  s->scanEpoch = (s->scanEpoch + 1) & 0x3fffffffu;
+  if (s->scanEpoch == 0) s->scanEpoch = 1;
+  return s->scanEpoch;
+}
+
+// Cell arrays: histogram, cellStart, scan tile state (src/sim.js:107-110).
+int alloc_cells(p4a_sim* s) {
+  free_list(s->cellAllocs);
+  int rc;
+  if ((rc = dalloc(s, s->cellAllocs, &s->d.cellCount, (size_t)s->nCells + 1))) return rc;
+  if ((rc = dalloc(s, s->cellAllocs, &s->d.cellStart, (size_t)s->nCells + 2))) return rc;
+  if ((rc = dalloc(s, s->cellAllocs, &s->d.scanState, (size_t)scan_tiles(s->nCells)))) return rc;
+  if ((rc = dalloc(s, s->cellAllocs, &s->d.scanTicket, 4))) return rc;
+  return P4A_OK;
+}
+
+// boundaryParticles + sortBoundary, uploaded (src/sim.js:112-127, 721-736).
+int upload_boundary(p4a_sim* s) {
+  HostBoundary hb;
+  build_boundary(s->params.box, s->params.rest_density, s->params.spacing, s->h, s->gridDim, hb);
+  free_list(s->boundaryAllocs);
+  int rc;
+  const int nb = hb.count;
+  if ((rc = dalloc(s, s->boundaryAllocs, &s->d.bpos, (size_t)std::max(1, nb)))) return rc;
+  if ((rc = dalloc(s, s->boundaryAllocs, &s->d.bpsi, (size_t)std::max(1, nb)))) return rc;
+  if ((rc = dalloc(s, s->boundaryAllocs, &s->d.bcellStart, (size_t)s->nCells + 2))) return rc;
+  CUDA_TRY(s, cudaMemcpyAsync(s->d.bpos, hb.pos.data(), hb.pos.size() * 4, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemcpyAsync(s->d.bpsi, hb.psi.data(), hb.psi.size() * 4, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemcpyAsync(s->d.bcellStart, hb.cellStart.data(), hb.cellStart.size() * 4,
+                              cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));  // host vectors go out of scope
+  s->nBoundary = nb;
+  return P4A_OK;
+}
+
+// The grid pass at parity `par` into parity par^1 (src/sim.js:473-492).
+void grid_pass(p4a_sim* s, int par) {
+  const int q = par ^ 1;
+  DevScene& d = s->d;
+  cudaStream_t st = s->stream;
+  mark(s, PH_KEY_COUNT);
+  launch_key_count(s->P, d.pos[par], d.vel[par], d.key, d.rank, d.cellCount,
+                   s->nBodies ? d.bodyFill : nullptr, (uint32_t)s->nBodies, st);
+  mark(s, PH_SCAN);
+  launch_scan(d.cellCount, d.cellStart, s->nCells, d.scanState, d.scanTicket, next_epoch(s),
+              d.errorWord, st);
+  mark(s, PH_FILL);
+  launch_fill((uint32_t)s->n, d.key, d.rank, d.cellStart, d.unordered, st);
+  mark(s, PH_REORDER);
+  launch_reorder(s->P, d.key, d.cellStart, d.unordered, d.pos[par], d.vel[par], d.body[par],
+                 d.rest[par], d.pos[q], d.vel[q], d.pred[q], d.body[q], d.rest[q], nullptr,
+                 s->nBodies ? d.bodyStart : nullptr, d.bodyFill, s->nBodies ? d.bodyList : nullptr, st);
+}
+
+int reset_common(p4a_sim* s) {
+  HostScene& sc = s->sc;
+  const p4a_params& p = s->params;
+  s->ready = false;
+  s->simTime = 0;
+  s->gen++;
+  const int n = sc.n;
+  s->h = sc.h;
+  for (int k = 0; k < 3; k++) s->gridDim[k] = (int)std::max(1.0, std::floor(p.box[k] / s->h));
+  s->nCells = s->gridDim[0] * s->gridDim[1] * s->gridDim[2];
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  free_list(s->sceneAllocs);
+  s->d = DevScene{};
+  const size_t cap = (size_t)n + s->pourBudget;
+  s->cap = (int)cap;
+  int rc;
+  auto& L = s->sceneAllocs;
+  for (int t = 0; t < 2; t++) {
+    if ((rc = dalloc(s, L, &s->d.pos[t], cap)) || (rc = dalloc(s, L, &s->d.vel[t], cap)) ||
+        (rc = dalloc(s, L, &s->d.pred[t], cap)) || (rc = dalloc(s, L, &s->d.body[t], cap)) ||
+        (rc = dalloc(s, L, &s->d.rest[t], cap)))
+      return rc;
+  }
+  if ((rc = dalloc(s, L, &s->d.lambda, cap)) || (rc = dalloc(s, L, &s->d.density, cap)) ||
+      (rc = dalloc(s, L, &s->d.corr, cap)) || (rc = dalloc(s, L, &s->d.normal, cap)) ||
+      (rc = dalloc(s, L, &s->d.key, cap)) || (rc = dalloc(s, L, &s->d.rank, cap)) ||
+      (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
+      (rc = dalloc(s, L, &s->d.errorWord, 4)))
+    return rc;
+  if ((rc = alloc_cells(s))) return rc;
+  if ((rc = upload_boundary(s))) return rc;
+  // bodies (src/sim.js:129-161)
+  const int nBodies = (int)sc.bodyDensity.size();
+  s->nBodies = nBodies;
+  s->nBodyParts = sc.nBody;
+  const int nb1 = std::max(1, nBodies);
+  if ((rc = dalloc(s, L, &s->d.bodyAccum, (size_t)nb1 * 4)) || (rc = dalloc(s, L, &s->d.bodyCov, (size_t)nb1 * 9)) ||
+      (rc = dalloc(s, L, &s->d.bodyCentre, nb1)) || (rc = dalloc(s, L, &s->d.bodyRef, nb1)) ||
+      (rc = dalloc(s, L, &s->d.bodyRot, (size_t)nb1 * 3)) || (rc = dalloc(s, L, &s->d.bodyInfo, nb1)) ||
+      (rc = dalloc(s, L, &s->d.bodyStart, (size_t)nb1 + 1)) || (rc = dalloc(s, L, &s->d.bodyFill, nb1)) ||
+      (rc = dalloc(s, L, &s->d.bodyList, (size_t)std::max(1, sc.nBody))))
+    return rc;
+  std::vector<int> counts(nBodies, 0);
+  for (int i = 0; i < n; i++) {
+    const uint32_t b = sc.phase[(size_t)i * 4];
+    if (b >= 1 && (int)b <= nBodies) counts[b - 1]++;
+  }
+  s->bodyStartHost.assign(nb1 + 1, 0u);
+  for (int b = 0; b < nBodies; b++) s->bodyStartHost[b + 1] = s->bodyStartHost[b] + counts[b];
+  if (nBodies) {
+    std::vector<float> info((size_t)nBodies * 4, 0.0f), centre((size_t)nBodies * 4, 0.0f),
+        rot((size_t)nBodies * 12, 0.0f);
+    for (int i = 0; i < nBodies; i++) {
+      info[i * 4] = (float)(1 / std::max(1e-6, sc.bodyDensity[i]));
+      for (int k = 0; k < 3; k++) centre[i * 4 + k] = (float)sc.bodyCentre[i * 3 + k];
+      for (int r = 0; r < 3; r++) rot[i * 12 + r * 4 + r] = 1.0f;
+    }
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.bodyInfo, info.data(), info.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.bodyCentre, centre.data(), centre.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.bodyRef, centre.data(), centre.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.bodyRot, rot.data(), rot.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.bodyStart, s->bodyStartHost.data(), s->bodyStartHost.size() * 4,
+                                cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  }
+  // fixed-point scales (src/sim.js:163-171)
+  double maxCount = 1, maxRest = 1e-3;
+  for (int b = 0; b < nBodies; b++) maxCount = std::max(maxCount, (double)counts[b]);
+  for (int i = 0; i < n; i++) {
+    const double r = std::hypot((double)sc.rest[(size_t)i * 4], (double)sc.rest[(size_t)i * 4 + 1],
+                                (double)sc.rest[(size_t)i * 4 + 2]);
+    if (r > maxRest) maxRest = r;
+  }
+  const double extent = std::max(p.box[0], std::max(p.box[1], p.box[2]));
+  s->bodyScale = 1e9 / (extent * maxCount);
+  s->covScale = 1e9 / (extent * maxRest * maxCount);
+  // pinned readback: 8 stats words, error word, pose (16 floats per body)
+  const size_t want = 64 + (size_t)nb1 * 16 * sizeof(float);
+  if (s->pinnedBytes < want) {
+    if (s->readEvent) cudaEventSynchronize(s->readEvent);
+    if (s->pinned) cudaFreeHost(s->pinned);
+    s->pinned = nullptr;
+    CUDA_TRY(s, cudaHostAlloc((void**)&s->pinned, want, cudaHostAllocDefault));
+    s->pinnedBytes = want;
+  }
+  s->readPending = false;
+  s->poseValid = false;
+  s->stats = p4a_stats{};
+  s->stats.avg_rho = 1;
+  s->stats.max_rho = 1;
+  s->pose.assign((size_t)nBodies * 12, 0.0f);
+  for (int b = 0; b < nBodies; b++) {
+    for (int k = 0; k < 3; k++) s->pose[b * 12 + k] = (float)sc.bodyCentre[b * 3 + k];
+    for (int r = 0; r < 3; r++) s->pose[b * 12 + 3 + r * 3 + r] = 1.0f;
+  }
+  // initial particle state into parity A (src/sim.js:191-195)
+  const size_t nb = (size_t)n * 16;
+  if (n > 0) {
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.pos[0], sc.pos.data(), nb, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.vel[0], sc.vel.data(), nb, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.pred[0], sc.pos.data(), nb, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.body[0], sc.phase.data(), nb, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->d.rest[0], sc.rest.data(), nb, cudaMemcpyHostToDevice, s->stream));
+  }
+  s->n = n;
+  s->parity = 0;
+  s->predParity = 0;
+  s->heldBody = -1;
+  s->heldTarget[0] = s->heldTarget[1] = s->heldTarget[2] = 0;
+  s->heldRate = 10;
+  s->heldLimit = 4;
+  // primeGrid (src/sim.js:223-253)
+  pack_params(s, 0);
+  grid_pass(s, s->parity);
+  mark(s, PH_END);
+  s->parity ^= 1;
+  s->predParity = s->parity;
+  pack_params(s, 1.0 / 240);
+  CUDA_TRY(s, cudaGetLastError());
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  s->ready = true;
+  return P4A_OK;
+}
+
+void copy_params(p4a_sim* s, const p4a_params* p) {
+  s->params = *p;
+  s->specs.assign(p->bodies, p->bodies + (p->bodies ? p->n_bodies : 0));
+  s->params.bodies = s->specs.empty() ? nullptr : s->specs.data();
+  s->params.n_bodies = (int32_t)s->specs.size();
+}
+
+int check_error_word(p4a_sim* s) {
+  const uint32_t w = s->pinned ? s->pinned[8] : 0u;
+  if (w & ERR_SCAN_TIMEOUT)
+    return fail(s, P4A_ERR_TIMEOUT, "cell scan: a bounded wait on a predecessor tile gave up");
+  return P4A_OK;
+}
+
+// Completes an outstanding readback if it finished (or waits for it).
+int poll_readback(p4a_sim* s, bool wait) {
+  if (!s->readPending) return P4A_OK;
+  if (wait) {
+    CUDA_TRY(s, cudaEventSynchronize(s->readEvent));
+  } else {
+    const cudaError_t q = cudaEventQuery(s->readEvent);
+    if (q == cudaErrorNotReady) return P4A_OK;
+    if (q != cudaSuccess) return fail(s, P4A_ERR_CUDA, "readback: %s", cudaGetErrorString(q));
+  }
+  s->readPending = false;
+  const uint32_t* v = s->pinned;
+  const double SCALE = 1024;
+  s->stats.avg_rho = v[0] / SCALE / std::max(1, s->n);
+  s->stats.max_rho = v[1] / SCALE;
+  s->stats.max_speed = v[2] / SCALE;
+  s->stats.ke = v[3] / SCALE;
+  for (int k = 0; k < 4; k++) s->stats.raw[k] = v[k];
+  s->stats.valid = 1;
+  if (s->nBodies) {
+    const float* f = (const float*)(s->pinned + 16);
+    for (int b = 0; b < s->nBodies; b++) {
+      for (int k = 0; k < 3; k++) s->pose[b * 12 + k] = f[b * 4 + k];
+      const float* rows = f + (size_t)s->nBodies * 4 + (size_t)b * 12;
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) s->pose[b * 12 + 3 + r * 3 + c] = rows[r * 4 + c];
+    }
+    s->poseValid = true;
+  }
+  return check_error_word(s);
+}
+
+int buffer_ptr(p4a_sim* s, int32_t id, int32_t which, void** p, size_t* bytes) {
+  const int w = which < 0 ? s->parity : (which & 1);
+  const size_t cap = (size_t)s->cap;
+  const size_t nb1 = (size_t)std::max(1, s->nBodies);
+  const size_t nbd = (size_t)std::max(1, s->nBoundary);
+  const size_t cells = (size_t)s->nCells + 2;
+  switch (id) {
+    case P4A_BUF_POS: *p = s->d.pos[w]; *bytes = cap * 16; break;
+    case P4A_BUF_VEL: *p = s->d.vel[w]; *bytes = cap * 16; break;
+    case P4A_BUF_PRED: *p = s->d.pred[w]; *bytes = cap * 16; break;
+    case P4A_BUF_BODY: *p = s->d.body[w]; *bytes = cap * 16; break;
+    case P4A_BUF_REST: *p = s->d.rest[w]; *bytes = cap * 16; break;
+    case P4A_BUF_DENSITY: *p = s->d.density; *bytes = cap * 4; break;
+    case P4A_BUF_LAMBDA: *p = s->d.lambda; *bytes = cap * 4; break;
+    case P4A_BUF_CORR: *p = s->d.corr; *bytes = cap * 16; break;
+    case P4A_BUF_NORMAL: *p = s->d.normal; *bytes = cap * 16; break;
+    case P4A_BUF_CELL_START: *p = s->d.cellStart; *bytes = cells * 4; break;
+    case P4A_BUF_BPOS: *p = s->d.bpos; *bytes = nbd * 16; break;
+    case P4A_BUF_BPSI: *p = s->d.bpsi; *bytes = nbd * 4; break;
+    case P4A_BUF_BCELL_START: *p = s->d.bcellStart; *bytes = cells * 4; break;
+    case P4A_BUF_BODY_CENTRE: *p = s->d.bodyCentre; *bytes = nb1 * 16; break;
+    case P4A_BUF_BODY_REF: *p = s->d.bodyRef; *bytes = nb1 * 16; break;
+    case P4A_BUF_BODY_ROT: *p = s->d.bodyRot; *bytes = nb1 * 48; break;
+    case P4A_BUF_BODY_INFO: *p = s->d.bodyInfo; *bytes = nb1 * 16; break;
+    case P4A_BUF_STATS_OUT: *p = s->d.statsOut; *bytes = 32; break;
+    case P4A_BUF_SMOOTH_POS: *p = s->smoothPos; *bytes = s->smoothPos ? (size_t)s->n * 16 : 0; break;
+    case P4A_BUF_ANISO_G: *p = s->anisoG; *bytes = s->anisoG ? (size_t)s->n * 32 : 0; break;
+    default: return fail(s, P4A_ERR_ARG, "unknown buffer id %d", id);
+  }
+  return P4A_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int p4a_abi_version(void) { return P4A_ABI_VERSION; }
+
+const char* p4a_status_string(int status) {
+  switch (status) {
+    case P4A_OK: return "ok";
+    case P4A_ERR_ARG: return "invalid argument";
+    case P4A_ERR_OOM: return "out of memory";
+    case P4A_ERR_CUDA: return "CUDA error";
+    case P4A_ERR_TIMEOUT: return "device wait timed out";
+    case P4A_ERR_CAPACITY: return "capacity exceeded";
+    case P4A_ERR_STATE: return "invalid state";
+    case P4A_ERR_NODEV: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+int p4a_default_params(const char* preset, p4a_params* out) {
+  static const p4a_body_spec kDefaultBodies[3] = {
+      {P4A_SHAPE_SPHERE, 0.5, 0.75}, {P4A_SHAPE_TORUS, 0.8, 0.75}, {P4A_SHAPE_BOX, 1.4, 0.75}};
+  if (!out) return P4A_ERR_ARG;
+  p4a_params p{};
+  p.spacing = 0.02;
+  p.rest_density = 1000;
+  p.gravity = 9.81;
+  p.substeps = 4;
+  p.iterations = 4;
+  p.cfm_epsilon_rel = 0.01;
+  p.s_corr_k = 0.1;
+  p.s_corr_dq = 0.3;
+  p.xsph_c = 0.05;
+  p.omega = 1.0;
+  p.sor_average = 0;
+  p.surface_tension_k = 0;
+  p.target_particle_count = 60000;
+  p.box[0] = 1.5; p.box[1] = 1.5; p.box[2] = 1.0;
+  p.n_bodies = 3;
+  p.bodies = kDefaultBodies;
+  p.body_size = 0;
+  p.no_boundary = 0;
+  p.pour = 1;
+  p.cfm_epsilon_abs = 0;
+  if (preset && std::strcmp(preset, "extreme") == 0) {  // src/scene.js:7-8
+    p.target_particle_count = 1000000;
+    p.box[0] = p.box[1] = p.box[2] = 3.0;
+  }
+  *out = p;
+  return P4A_OK;
+}
+
+int p4a_device_check(int device) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return P4A_ERR_NODEV;
+  if (device < 0 || device >= count) return P4A_ERR_ARG;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return P4A_ERR_NODEV;
+  return prop.major == 10 && prop.minor == 0 ? P4A_OK : P4A_ERR_NODEV;
+}
+
+int p4a_create(int device, p4a_sim** out) {
+  if (!out) return P4A_ERR_ARG;
+  *out = nullptr;
+  const int chk = p4a_device_check(device);
+  if (chk != P4A_OK) return chk;
+  p4a_sim* s = new p4a_sim();
+  s->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->readEvent, cudaEventDisableTiming) != cudaSuccess) {
+    delete s;
+    return P4A_ERR_CUDA;
+  }
+  s->ownStream = true;
+  *out = s;
+  return P4A_OK;
+}
+
+int p4a_destroy(p4a_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_list(s->sceneAllocs);
+  free_list(s->cellAllocs);
+  free_list(s->boundaryAllocs);
+  if (s->smoothPos) cudaFree(s->smoothPos);
+  if (s->anisoG) cudaFree(s->anisoG);
+  if (s->pinned) cudaFreeHost(s->pinned);
+  if (s->readEvent) cudaEventDestroy(s->readEvent);
+  for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
+  if (s->ownStream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return P4A_OK;
+}
+
+const char* p4a_last_error(const p4a_sim* s) { return s ? s->err.c_str() : "null handle"; }
+
+int p4a_set_stream(p4a_sim* s, void* stream) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  if (stream) {
+    if (s->ownStream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->ownStream = false;
+  } else if (!s->ownStream) {
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    s->ownStream = true;
+  }
+  return P4A_OK;
+}
+
+int p4a_synchronize(p4a_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return poll_readback(s, true);
+}
+
+int p4a_reset(p4a_sim* s, const p4a_params* params) {
+  if (!s || !params || !(params->spacing > 0) || params->n_bodies < 0 ||
+      (params->n_bodies > 0 && !params->bodies))
+    return fail(s, P4A_ERR_ARG, "p4a_reset: invalid params");
+  cudaSetDevice(s->device);
+  copy_params(s, params);
+  build_scene(s->params, s->sc);
+  s->pourBudget = params->pour ? s->sc.nFluid : 0;
+  return reset_common(s);
+}
+
+int p4a_reset_scene(p4a_sim* s, const p4a_params* params, const p4a_scene_desc* sd) {
+  if (!s || !params || !sd || sd->n < 0 || (sd->n > 0 && !sd->pos) || !(params->spacing > 0) ||
+      sd->n_bodies < 0 || (sd->n_bodies > 0 && (!sd->body_density || !sd->body_centre)))
+    return fail(s, P4A_ERR_ARG, "p4a_reset_scene: invalid scene");
+  cudaSetDevice(s->device);
+  copy_params(s, params);
+  HostScene& sc = s->sc;
+  sc = HostScene();
+  const size_t n = (size_t)sd->n;
+  sc.n = sd->n;
+  sc.d = params->spacing;
+  sc.h = 2 * params->spacing;
+  sc.pos.assign(sd->pos, sd->pos + n * 4);
+  sc.vel = sd->vel ? std::vector<float>(sd->vel, sd->vel + n * 4) : std::vector<float>(n * 4, 0.0f);
+  sc.rest = sd->rest ? std::vector<float>(sd->rest, sd->rest + n * 4) : std::vector<float>(n * 4, 0.0f);
+  sc.phase = sd->phase ? std::vector<uint32_t>(sd->phase, sd->phase + n * 4) : std::vector<uint32_t>(n * 4, 0u);
+  int nFluid = 0;
+  for (size_t i = 0; i < n; i++) {
+    const uint32_t b = sc.phase[i * 4];
+    if (b == 0) nFluid++;
+    else if ((int)b > sd->n_bodies) return fail(s, P4A_ERR_ARG, "particle %zu: body id %u > n_bodies", i, b);
+  }
+  sc.nFluid = nFluid;
+  sc.nBody = sd->n - nFluid;
+  sc.bodyDensity.assign(sd->body_density, sd->body_density + sd->n_bodies);
+  sc.bodyCentre.assign(sd->body_centre, sd->body_centre + 3 * (size_t)sd->n_bodies);
+  sc.mass = sd->mass;
+  sc.denomRest = sd->denom_rest;
+  const bool doMass = !(sd->mass > 0), doDenom = !(sd->denom_rest > 0);
+  if (doMass || doDenom) calibrate_scene(s->params, sc, doMass, doDenom);
+  s->pourBudget = std::max(0, sd->pour_budget);
+  return reset_common(s);
+}
+
+int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
+  if (!s) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "p4a_step before p4a_reset");
+  cudaSetDevice(s->device);
+  const p4a_params& p = s->params;
+  // time bank (src/sim.js:418-429)
+  const int base = std::max(1, p.substeps);
+  const double dtTarget = (1.0 / 60) / base;
+  s->timeBank = s->timeBank + frameDt;
+  double subD = std::floor(s->timeBank / dtTarget + 1e-4);
+  const double workCap = base * 8;
+  if (subD > workCap) {
+    subD = workCap;
+    s->timeBank = 0;
+  } else {
+    s->timeBank -= subD * dtTarget;
+  }
+  const int sub = (int)subD;
+  s->lastSubsteps = sub;
+  s->lastAdvanced = subD * dtTarget;
+  if (substeps_out) *substeps_out = sub;
+  if (sub < 1) {
+    s->lastAdvanced = 0;
+    return P4A_OK;
+  }
+  const double dt = dtTarget;
+  pack_params(s, dt);
+  const SimParams& P = s->P;
+  DevScene& d = s->d;
+  cudaStream_t st = s->stream;
+  const bool bodies = s->nBodyParts > 0 && s->nBodies > 0;
+  const bool dragging = s->heldBody >= 1 && s->nBodyParts > 0;
+  const float blend = (float)(1 - std::exp(-std::max(dt, 0.0) / 0.02));
+  const float goal[3] = {(float)s->heldTarget[0], (float)s->heldTarget[1], (float)s->heldTarget[2]};
+  const int iters = std::max(1, p.iterations);
+  const bool tension = p.surface_tension_k > 0;
+  for (int step = 0; step < sub; step++) {
+    const int par = s->parity, q = par ^ 1;
+    if (dragging) {
+      const uint32_t hb = (uint32_t)s->heldBody;
+      mark(s, PH_DRAG);
+      launch_body_drag(d, d.vel[par], d.body[par], hb, s->bodyStartHost[hb] - s->bodyStartHost[hb - 1],
+                       s->bodyStartHost[hb - 1], goal, (float)s->heldRate, blend, (float)s->heldLimit, st);
+    }
+    grid_pass(s, par);
+    s->parity = q;
+    s->predParity = q;
+    int cur = q;
+    if (bodies) {
+      mark(s, PH_BODY_SEED);
+      launch_body_seed(P, d, d.pred[cur], st);
+    }
+    for (int it = 0; it < iters; it++) {
+      const bool last = it == iters - 1;
+      mark(s, PH_LAMBDA);
+      launch_lambda(P, d, d.pred[cur], st);
+      mark(s, PH_DELTA);
+      launch_delta(P, d, d.pred[cur], d.pred[cur ^ 1], d.pos[q], last ? d.vel[par] : nullptr, st);
+      cur ^= 1;
+      if (bodies) {
+        mark(s, PH_BODY_MATCH);
+        launch_body_match(P, d, d.pred[cur], d.rest[q], d.pos[q], last ? d.vel[par] : nullptr, st);
+      }
+    }
+    float4* predCopy = cur != q ? d.pred[q] : nullptr;
+    const bool statsNow = step == sub - 1;
+    if (statsNow) {
+      mark(s, PH_STATS_CLEAR);
+      CUDA_TRY(s, cudaMemsetAsync(d.statsOut, 0, 32, st));
+    }
+    if (tension) {
+      mark(s, PH_XSPH_NORMALS);
+      launch_xsph_normals(P, d, d.pred[cur], d.vel[par], st);
+      mark(s, PH_TENSION_FINALIZE);
+      launch_tension_finalize(P, d, d.pred[cur], d.vel[par], d.pos[q], d.vel[q], predCopy, statsNow, st);
+    } else {
+      mark(s, PH_XSPH_FINALIZE);
+      launch_xsph_finalize(P, d, d.pred[cur], d.vel[par], d.pos[q], d.vel[q], predCopy, statsNow, st);
+    }
+    s->simTime += dt;
+  }
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  // stats and pose readback (src/sim.js:598-655), at most one in flight
+  if (!s->readPending) {
+    CUDA_TRY(s, cudaMemcpyAsync(s->pinned, d.statsOut, 32, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(s, cudaMemcpyAsync(s->pinned + 8, d.errorWord, 4, cudaMemcpyDeviceToHost, st));
+    if (s->nBodies) {
+      float* f = (float*)(s->pinned + 16);
+      CUDA_TRY(s, cudaMemcpyAsync(f, d.bodyCentre, (size_t)s->nBodies * 16, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(s, cudaMemcpyAsync(f + (size_t)s->nBodies * 4, d.bodyRot, (size_t)s->nBodies * 48,
+                                  cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(s, cudaEventRecord(s->readEvent, st));
+    s->readPending = true;
+  }
+  return P4A_OK;
+}
+
+int p4a_append_fluid(p4a_sim* s, const float* pos3, const float* vel3, int32_t count, int32_t* added) {
+  if (!s || count < 0 || (count > 0 && (!pos3 || !vel3))) return fail(s, P4A_ERR_ARG, "appendFluid: bad arguments");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "appendFluid before reset");
+  cudaSetDevice(s->device);
+  const int room = std::max(0, s->cap - s->n);
+  const int c = std::min(count, room);
+  if (added) *added = std::max(0, c);
+  if (c <= 0) return P4A_OK;
+  std::vector<float> p4((size_t)c * 4), v4((size_t)c * 4, 0.0f), rho((size_t)c, (float)s->params.rest_density);
+  for (int i = 0; i < c; i++) {
+    for (int k = 0; k < 3; k++) {
+      p4[i * 4 + k] = pos3[i * 3 + k];
+      v4[i * 4 + k] = vel3[i * 3 + k];
+    }
+    p4[i * 4 + 3] = 1.0f;
+  }
+  const size_t o4 = (size_t)s->n, bytes4 = (size_t)c * 16, bytes1 = (size_t)c * 4;
+  cudaStream_t st = s->stream;
+  DevScene& d = s->d;
+  CUDA_TRY(s, cudaMemcpyAsync(d.pos[s->parity] + o4, p4.data(), bytes4, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(s, cudaMemcpyAsync(d.vel[s->parity] + o4, v4.data(), bytes4, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(s, cudaMemcpyAsync(d.pred[s->predParity] + o4, p4.data(), bytes4, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(s, cudaMemcpyAsync(d.density + o4, rho.data(), bytes1, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(s, cudaMemsetAsync(d.lambda + o4, 0, bytes1, st));
+  CUDA_TRY(s, cudaMemsetAsync(d.corr + o4, 0, bytes4, st));
+  CUDA_TRY(s, cudaMemsetAsync(d.normal + o4, 0, bytes4, st));
+  for (int t = 0; t < 2; t++) {
+    CUDA_TRY(s, cudaMemsetAsync(d.body[t] + o4, 0, bytes4, st));
+    CUDA_TRY(s, cudaMemsetAsync(d.rest[t] + o4, 0, bytes4, st));
+  }
+  CUDA_TRY(s, cudaStreamSynchronize(st));  // host staging vectors go out of scope
+  s->n += c;
+  return P4A_OK;
+}
+
+int p4a_apply_ray_impulse(p4a_sim* s, const double origin[3], const double dir[3], const double impulse[3],
+                          double radius, double speedLimit) {
+  if (!s || !origin || !dir || !impulse) return fail(s, P4A_ERR_ARG, "applyRayImpulse: null argument");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "applyRayImpulse before reset");
+  if (!s->n || radius <= 0) return P4A_OK;
+  const double len = std::hypot(impulse[0], impulse[1], impulse[2]);
+  if (len <= 0) return P4A_OK;
+  double dl = std::hypot(dir[0], dir[1], dir[2]);
+  if (!(dl != 0)) dl = 1;
+  cudaSetDevice(s->device);
+  const float o[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
+  const float dr[3] = {(float)(dir[0] / dl), (float)(dir[1] / dl), (float)(dir[2] / dl)};
+  const float im[3] = {(float)impulse[0], (float)impulse[1], (float)impulse[2]};
+  mark(s, PH_IMPULSE);
+  launch_impulse((uint32_t)s->n, s->d.pos[s->parity], s->d.vel[s->parity], o, dr, im, (float)radius,
+                 (float)speedLimit, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  return P4A_OK;
+}
+
+int p4a_hold_body(p4a_sim* s, int32_t body1, const double target[3], double rate, double limit) {
+  if (!s || !target) return fail(s, P4A_ERR_ARG, "holdBody: null argument");
+  s->heldBody = (body1 >= 1 && body1 <= s->nBodies) ? body1 : -1;
+  for (int k = 0; k < 3; k++) s->heldTarget[k] = target[k];
+  s->heldRate = rate;
+  s->heldLimit = limit;
+  return P4A_OK;
+}
+
+int p4a_release_body(p4a_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  s->heldBody = -1;
+  return P4A_OK;
+}
+
+int p4a_resize_box(p4a_sim* s, const double newBox[3]) {
+  if (!s || !newBox) return fail(s, P4A_ERR_ARG, "resizeBox: null argument");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "resizeBox before reset");
+  cudaSetDevice(s->device);
+  p4a_params& p = s->params;
+  const double oldBox[3] = {p.box[0], p.box[1], p.box[2]};
+  bool moved = false;
+  for (int a = 0; a < 3; a++)
+    if (std::fabs(newBox[a] - oldBox[a]) > 1e-9) moved = true;
+  if (!moved) return P4A_OK;
+  for (int a = 0; a < 3; a++) p.box[a] = newBox[a];
+  for (int k = 0; k < 3; k++) s->gridDim[k] = (int)std::max(1.0, std::floor(newBox[k] / s->h));
+  const int cells = s->gridDim[0] * s->gridDim[1] * s->gridDim[2];
+  const bool changed = cells != s->nCells;
+  s->nCells = cells;
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  int rc;
+  if (changed && (rc = alloc_cells(s))) return rc;
+  if ((rc = upload_boundary(s))) return rc;
+  s->gen++;
+  const float halfD = (float)(0.5 * p.spacing);
+  const float oldS[3] = {(float)oldBox[0], (float)oldBox[1], (float)oldBox[2]};
+  const float newS[3] = {(float)newBox[0], (float)newBox[1], (float)newBox[2]};
+  const float cMin[3] = {halfD, halfD, halfD};
+  const float cMax[3] = {(float)(newBox[0] - 0.5 * p.spacing), (float)(newBox[1] - 0.5 * p.spacing),
+                         (float)(newBox[2] - 0.5 * p.spacing)};
+  mark(s, PH_RESIZE);
+  launch_resize((uint32_t)s->n, s->d.pos[s->parity], oldS, newS, cMin, cMax, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  return P4A_OK;
+}
+
+int p4a_get_info(const p4a_sim* s, p4a_info* o) {
+  if (!s || !o) return P4A_ERR_ARG;
+  *o = p4a_info{};
+  o->n = s->n; o->n_fluid = s->sc.nFluid; o->n_body_parts = s->nBodyParts; o->n_bodies = s->nBodies;
+  o->n_boundary = s->nBoundary; o->cap = s->cap; o->pour_budget = s->pourBudget;
+  for (int k = 0; k < 3; k++) o->grid_dim[k] = s->gridDim[k];
+  o->n_cells = s->nCells; o->parity = s->parity; o->pred_parity = s->predParity; o->gen = s->gen;
+  o->last_substeps = s->lastSubsteps; o->h = s->h; o->mass = s->sc.mass; o->denom_rest = s->sc.denomRest;
+  o->sim_time = s->simTime; o->last_advanced = s->lastAdvanced; o->time_bank = s->timeBank;
+  o->body_scale = s->bodyScale; o->cov_scale = s->covScale; o->held_body = s->heldBody;
+  o->aniso_gen = s->anisoGen;
+  return P4A_OK;
+}
+
+int p4a_buffer(p4a_sim* s, int32_t id, int32_t which, void** dptr, size_t* bytes) {
+  if (!s || !dptr) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "buffer query before reset");
+  size_t b = 0;
+  const int rc = buffer_ptr(s, id, which, dptr, &b);
+  if (bytes) *bytes = b;
+  return rc;
+}
+
+int p4a_read(p4a_sim* s, int32_t id, int32_t which, void* host, size_t offset, size_t bytes) {
+  if (!s || (!host && bytes)) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "read before reset");
+  void* p = nullptr;
+  size_t total = 0;
+  int rc = buffer_ptr(s, id, which, &p, &total);
+  if (rc) return rc;
+  if (offset > total || bytes > total - offset)
+    return fail(s, P4A_ERR_ARG, "read of %zu bytes at %zu beyond buffer size %zu", bytes, offset, total);
+  if (!bytes) return P4A_OK;
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaMemcpyAsync(host, (const char*)p + offset, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return P4A_OK;
+}
+
+int p4a_write(p4a_sim* s, int32_t id, int32_t which, const void* host, size_t offset, size_t bytes) {
+  if (!s || (!host && bytes)) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "write before reset");
+  void* p = nullptr;
+  size_t total = 0;
+  int rc = buffer_ptr(s, id, which, &p, &total);
+  if (rc) return rc;
+  if (offset > total || bytes > total - offset)
+    return fail(s, P4A_ERR_ARG, "write of %zu bytes at %zu beyond buffer size %zu", bytes, offset, total);
+  if (!bytes) return P4A_OK;
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return P4A_OK;
+}
+
+int p4a_get_stats(p4a_sim* s, int32_t wait, p4a_stats* out) {
+  if (!s || !out) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  const int rc = poll_readback(s, wait != 0);
+  *out = s->stats;
+  return rc;
+}
+
+int p4a_body_pose(p4a_sim* s, int32_t wait, float* centre3, float* rot9, int32_t maxBodies) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  const int rc = poll_readback(s, wait != 0);
+  const int nb = std::min(maxBodies, s->nBodies);
+  for (int b = 0; b < nb; b++) {
+    if (centre3)
+      for (int k = 0; k < 3; k++) centre3[b * 3 + k] = s->pose[b * 12 + k];
+    if (rot9)  // column-major, as Sim.bodyPose (src/sim.js:648-650)
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) rot9[b * 9 + c * 3 + r] = s->pose[b * 12 + 3 + r * 3 + c];
+  }
+  return rc;
+}
+
+int p4a_default_aniso_params(p4a_aniso_params* a) {
+  if (!a) return P4A_ERR_ARG;
+  a->ratio = 4.0;
+  a->ks = 1.0;
+  a->stretch = 2.0;
+  a->lonely = 1.0;
+  a->min_neighbours = 25;
+  a->lambda = 0.9;
+  a->radius_scale = 2.0;
+  a->min_extent = 0.0;
+  return P4A_OK;
+}
+
+int p4a_aniso(p4a_sim* s, const p4a_aniso_params* ap) {
+  if (!s || !ap) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "aniso before reset");
+  const int n = s->n;
+  if (n <= 0) return P4A_OK;
+  cudaSetDevice(s->device);
+  if ((size_t)n > s->anisoCap) {  // src/mesh.js:210-220
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->smoothPos) cudaFree(s->smoothPos);
+    if (s->anisoG) cudaFree(s->anisoG);
+    s->smoothPos = nullptr;
+    s->anisoG = nullptr;
+    s->anisoCap = 0;
+    CUDA_TRY(s, cudaMalloc((void**)&s->smoothPos, (size_t)n * 16));
+    CUDA_TRY(s, cudaMalloc((void**)&s->anisoG, (size_t)n * 32));
+    s->anisoCap = (size_t)n;
+    s->anisoGen++;
+  }
+  const double support = s->h;
+  const double radius = ap->radius_scale * support;
+  const double sigmaBulk = 0.15 * radius * radius;
+  AnisoParams A{};
+  A.count = (uint32_t)n;
+  A.lambda = (float)ap->lambda;
+  A.invSupport = (float)(1 / support);
+  A.support = (float)support;
+  A.boxMin[0] = A.boxMin[1] = A.boxMin[2] = 0.0f;
+  A.radius = (float)radius;
+  for (int k = 0; k < 3; k++) A.gridDim[k] = s->gridDim[k];
+  A.cells = (int32_t)std::ceil(ap->radius_scale);
+  A.kr = (float)ap->ratio;
+  A.kn = (float)ap->lonely;
+  A.ks = (float)(ap->ks / sigmaBulk);
+  A.stretch = (float)ap->stretch;
+  A.minExtent = (float)ap->min_extent;
+  A.neps = ap->min_neighbours;
+  mark(s, PH_ANISO);
+  launch_aniso(A, s->d.pos[s->parity], s->d.cellStart, s->smoothPos, s->anisoG, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  return P4A_OK;
+}
+
+int p4a_profile_enable(p4a_sim* s, int32_t on) {
+  if (!s) return P4A_ERR_ARG;
+  if (!on && s->prof) {
+    mark(s, PH_END);
+    const int rc = resolve_marks(s);
+    s->prof = false;
+    return rc;
+  }
+  s->prof = on != 0;
+  return P4A_OK;
+}
+
+int p4a_profile_reset(p4a_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  const int rc = resolve_marks(s);
+  for (int k = 0; k < PH_COUNT; k++) {
+    s->phaseMs[k] = 0;
+    s->phaseLaunches[k] = 0;
+  }
+  return rc;
+}
+
+int p4a_profile_read(p4a_sim* s, p4a_phase_time* out, int32_t maxEntries, int32_t* count) {
+  if (!s || (!out && maxEntries > 0)) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  const int rc = resolve_marks(s);
+  int c = 0;
+  for (int k = 0; k < PH_COUNT; k++) {
+    if (!s->phaseLaunches[k]) continue;
+    if (c < maxEntries) {
+      std::snprintf(out[c].name, sizeof(out[c].name), "%s", kPhaseNames[k]);
+      out[c].ms = s->phaseMs[k];
+      out[c].launches = s->phaseLaunches[k];
+    }
+    c++;
+  }
+  if (count) *count = c;
+  return rc;
+}
+
+uint64_t p4a_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
+
+// ---- operator entry: predict + grid pass on caller buffers ---------------
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+size_t p4a_grid_sort_workspace_size(int32_t n, int32_t nCells) {
+  if (n < 0 || nCells <= 0) return 0;
+  const size_t un = (size_t)std::max(1, n);
+  return 3 * align256(un * 4) + align256(((size_t)nCells + 1) * 4) +
+         align256((size_t)scan_tiles(nCells) * 8) + align256(4) + align256(4);
+}
+
+int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, const float* pos,
+                  const float* vel, const uint32_t* body, const float* rest, float* pos_out,
+                  float* vel_out, float* pred_out, uint32_t* body_out, float* rest_out,
+                  uint32_t* cell_start, uint32_t* slot_out, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+  if (!grid || n < 0 || grid->dim[0] < 1 || grid->dim[1] < 1 || grid->dim[2] < 1 || !(grid->h > 0))
+    return P4A_ERR_ARG;
+  const long long cellsLL = (long long)grid->dim[0] * grid->dim[1] * grid->dim[2];
+  if (cellsLL > 0x7fffffffLL) return P4A_ERR_CAPACITY;
+  const int nCells = (int)cellsLL;
+  if (n > 0 && (!pos || !vel || !pos_out || !vel_out || !pred_out)) return P4A_ERR_ARG;
+  if ((body && !body_out) || (rest && !rest_out) || !cell_start) return P4A_ERR_ARG;
+  if (!workspace || workspace_bytes < p4a_grid_sort_workspace_size(n, nCells)) return P4A_ERR_CAPACITY;
+  cudaStream_t st = (cudaStream_t)stream;
+  char* w = (char*)workspace;
+  const size_t un = (size_t)std::max(1, n);
+  uint32_t* key = (uint32_t*)w; w += align256(un * 4);
+  uint32_t* rank = (uint32_t*)w; w += align256(un * 4);
+  uint32_t* unordered = (uint32_t*)w; w += align256(un * 4);
+  uint32_t* cellCount = (uint32_t*)w; w += align256(((size_t)nCells + 1) * 4);
+  unsigned long long* state = (unsigned long long*)w; w += align256((size_t)scan_tiles(nCells) * 8);
+  uint32_t* ticket = (uint32_t*)w; w += align256(4);
+  uint32_t* errw = (uint32_t*)w;
+  const size_t zeroBytes = (size_t)((char*)errw + 4 - (char*)cellCount);
+  if (cudaMemsetAsync(cellCount, 0, zeroBytes, st) != cudaSuccess) return P4A_ERR_CUDA;
+  SimParams P{};
+  for (int k = 0; k < 3; k++) { P.boxMin[k] = grid->box_min[k]; P.gridDim[k] = grid->dim[k]; }
+  P.h = grid->h;
+  P.dt = dt;
+  P.gravity = gravity;
+  P.n = (uint32_t)n;
+  P.nCells = (uint32_t)nCells;
+  g_launches.fetch_add(4, std::memory_order_relaxed);
+  launch_key_count(P, (const float4*)pos, (const float4*)vel, key, rank, cellCount, nullptr, 0, st);
+  launch_scan(cellCount, cell_start, nCells, state, ticket, 1u, errw, st);
+  launch_fill((uint32_t)n, key, rank, cell_start, unordered, st);
+  launch_reorder(P, key, cell_start, unordered, (const float4*)pos, (const float4*)vel,
+                 (const uint4*)body, (const float4*)rest, (float4*)pos_out, (float4*)vel_out,
+                 (float4*)pred_out, (uint4*)body_out, (float4*)rest_out, slot_out, nullptr, nullptr,
+                 nullptr, st);
+  return cudaGetLastError() == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+}
+
+}  // extern "C"

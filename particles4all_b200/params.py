@@ -1,0 +1,155 @@
+"""The reference's params object: PRESETS / defaultParams (src/scene.js:3-39), the
+preset .ini keys that reach the simulation (src/settingsini.js:3-33, applied by
+src/main.js:361-381), and its conversion to the C struct of include/p4a.h.
+
+Params are plain dicts with the reference's JS key names (spacing, restDensity,
+gravity, substeps, iterations, cfmEpsilonRel, sCorrK, sCorrDq, xsphC, omega,
+sorAverage, surfaceTensionK, targetParticleCount, box, bodies, bodySize,
+noBoundary, pour) so that code written against the reference reads the same.
+"""
+import ctypes as C
+import math
+
+from . import _abi
+
+# src/scene.js:3-9. The ini presets are parsed from the same keys the reference's
+# presets/*.ini files carry (see PRESET_INI below).
+PRESETS = {
+    "small": {"ini": "presets/small.ini"},
+    "medium": {"ini": "presets/medium.ini"},
+    "large": {"ini": "presets/large.ini"},
+    "extreme": {"particles": 1000000, "box": [3.0, 3.0, 3.0], "substeps": 4, "iterations": 4,
+                "bodies": ["sphere:0.5", "torus:0.8", "box:1.4"]},
+}
+
+
+def default_params(preset="small"):
+    """defaultParams(preset) (src/scene.js:11-39)."""
+    p = PRESETS.get(preset, {})
+    out = {
+        "preset": preset, "spacing": 0.02, "restDensity": 1000, "gravity": 9.81,
+        "substeps": 4, "iterations": 4, "cfmEpsilonRel": 0.01, "sCorrK": 0.1,
+        "sCorrDq": 0.3, "xsphC": 0.05, "omega": 1.0, "sorAverage": False,
+        "surfaceTensionK": 0, "targetParticleCount": 60000, "box": [1.5, 1.5, 1.0],
+        "bodies": ["sphere:0.5", "torus:0.8", "box:1.4"], "bodySize": 0,
+    }
+    if "substeps" in p:
+        out["substeps"] = p["substeps"]
+    if "iterations" in p:
+        out["iterations"] = p["iterations"]
+    if "particles" in p:
+        out["targetParticleCount"] = p["particles"]
+    if "box" in p:
+        out["box"] = list(p["box"])
+    if "bodies" in p:
+        out["bodies"] = list(p["bodies"])
+    out.update(p.get("params", {}))
+    return out
+
+
+# ini key -> params key for the keys that reach Sim (src/settingsini.js:3-33 maps
+# ini keys to URL keys; src/main.js:361-381 maps URL keys to params).
+_INI_TO_PARAM = {
+    "substeps": ("substeps", int), "iterations": ("iterations", int),
+    "cfm": ("cfmEpsilonRel", float), "scorrk": ("sCorrK", float),
+    "scorrdq": ("sCorrDq", float), "xsph": ("xsphC", float),
+    "tension": ("surfaceTensionK", float), "gravity": ("gravity", float),
+    "omega": ("omega", float), "particles": ("targetParticleCount", int),
+    "spacing": ("spacing", float), "bodysize": ("bodySize", float),
+}
+
+
+def parse_ini(text):
+    """parseIni (src/settingsini.js:45-55): key=value lines, # and ; comments."""
+    kv = {}
+    for raw in str(text).splitlines():
+        line = raw.strip()
+        if not line or line.startswith("#") or line.startswith(";"):
+            continue
+        eq = line.find("=")
+        if eq <= 0:
+            continue
+        kv[line[:eq].strip().lower()] = line[eq + 1:].strip()
+    return kv
+
+
+def apply_ini(params, text):
+    """Apply the simulation keys of a preset .ini to a params dict (the path
+    iniToQuery -> URL query -> qNum of src/settingsini.js:59-93, src/main.js:361-390)."""
+    kv = parse_ini(text)
+    for k, (name, conv) in _INI_TO_PARAM.items():
+        if k in kv:
+            params[name] = conv(float(kv[k])) if conv is int else conv(kv[k])
+    if "soraverage" in kv:
+        params["sorAverage"] = kv["soraverage"] not in ("0", "false", "")
+    if "box" in kv:
+        vals = [float(x) for x in kv["box"].replace(",", " ").split()]
+        if len(vals) >= 3 and all(math.isfinite(v) for v in vals):
+            params["box"] = vals[:3]
+    if "body" in kv:
+        params["bodies"] = [b for b in kv["body"].split(",") if b]
+    return params
+
+
+def _spec(s):
+    bits = s.split(":")
+    shape = bits[0]
+
+    def num(i, dflt):
+        try:
+            v = float(bits[i]) if len(bits) > i else dflt
+        except ValueError:
+            v = float("nan")
+        return v if (v == v and v != 0) else dflt   # Number(x) || dflt
+    return _abi.SHAPES.get(shape, 2), num(1, 0.5), num(2, 0.75)
+
+
+class CParams:
+    """Owns a p4a_params struct (and its bodies array) built from a params dict."""
+
+    def __init__(self, p):
+        bodies = [_spec(b) for b in p.get("bodies", [])]
+        self._bodies = (_abi.BodySpec * max(1, len(bodies)))()
+        for i, (shape, dens, sy) in enumerate(bodies):
+            self._bodies[i].shape, self._bodies[i].density, self._bodies[i].start_y = shape, dens, sy
+        s = _abi.Params()
+        s.spacing = p.get("spacing", 0.02)
+        s.rest_density = p.get("restDensity", 1000)
+        s.gravity = p.get("gravity", 9.81)
+        s.substeps = int(p.get("substeps", 4))
+        s.iterations = int(p.get("iterations", 4))
+        s.cfm_epsilon_rel = p.get("cfmEpsilonRel", 0.01)
+        s.s_corr_k = p.get("sCorrK", 0.1)
+        s.s_corr_dq = p.get("sCorrDq", 0.3)
+        s.xsph_c = p.get("xsphC", 0.05)
+        s.omega = p.get("omega", 1.0)
+        s.sor_average = 1 if p.get("sorAverage") else 0
+        s.surface_tension_k = p.get("surfaceTensionK", 0)
+        s.target_particle_count = int(p.get("targetParticleCount", 60000))
+        box = p.get("box", [1.5, 1.5, 1.0])
+        for k in range(3):
+            s.box[k] = box[k]
+        s.n_bodies = len(bodies)
+        s.bodies = C.cast(self._bodies, C.POINTER(_abi.BodySpec))
+        s.body_size = p.get("bodySize", 0)
+        s.no_boundary = 1 if p.get("noBoundary") else 0
+        s.pour = 0 if p.get("pour") is False else 1
+        s.cfm_epsilon_abs = p.get("cfmEpsilonAbs", 0.0)
+        self.struct = s
+
+    def ref(self):
+        return C.byref(self.struct)
+
+
+def default_aniso():
+    """SurfaceMesh defaults (src/mesh.js:81-89); min_extent 0 (anisoLimitToField off)."""
+    return {"ratio": 4.0, "ks": 1.0, "stretch": 2.0, "lonely": 1.0, "min_neighbours": 25,
+            "lambda": 0.9, "radius_scale": 2.0, "min_extent": 0.0}
+
+
+def aniso_struct(a):
+    s = _abi.AnisoParams()
+    s.ratio, s.ks, s.stretch, s.lonely = a["ratio"], a["ks"], a["stretch"], a["lonely"]
+    s.min_neighbours = int(a["min_neighbours"])
+    s.lambda_, s.radius_scale, s.min_extent = a["lambda"], a["radius_scale"], a["min_extent"]
+    return s

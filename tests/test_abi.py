@@ -1,0 +1,103 @@
+"""The C-ABI library loads, exports every entry point include/p4a.h declares, and
+fails loudly (no fallback) where a GPU is needed but absent. CPU only."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from particles4all_b200 import _abi, _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "p4a.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(p4a_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "p4a_step" in syms and "p4a_reset" in syms and "p4a_grid_sort" in syms
+    assert len(syms) >= 25
+
+
+def test_library_exports_every_declared_symbol(built):
+    L = _lib.lib()
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+
+
+def test_ctypes_signatures_cover_header(built):
+    assert set(declared_symbols()) == set(_lib.SIGNATURES)
+
+
+def test_abi_version_and_status_strings(built):
+    L = _lib.lib()
+    assert L.p4a_abi_version() == 1
+    assert L.p4a_status_string(0) == b"ok"
+    assert L.p4a_status_string(4) == b"device wait timed out"
+
+
+def test_struct_layouts_match_c_compiler(tmp_path):
+    """Every ctypes mirror has the size and field offsets gcc gives the C struct."""
+    structs = {"p4a_body_spec": _abi.BodySpec, "p4a_params": _abi.Params,
+               "p4a_scene_desc": _abi.SceneDesc, "p4a_info": _abi.Info, "p4a_stats": _abi.Stats,
+               "p4a_aniso_params": _abi.AnisoParams, "p4a_grid": _abi.Grid,
+               "p4a_scene_counts": _abi.SceneCounts}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "p4a.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            cf = "lambda" if fname == "lambda_" else fname
+            lines.append(f'printf("{cname} {fname} %zu\\n", offsetof({cname}, {cf}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    for line in filter(None, out):
+        cname, field, val = line.split()
+        cls = structs[cname]
+        got = C.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert got == int(val), (cname, field, got, val)
+
+
+def test_default_params_match_reference(built):
+    p = _abi.Params()
+    assert _lib.lib().p4a_default_params(b"small", C.byref(p)) == 0
+    # src/scene.js:14-31
+    assert (p.spacing, p.rest_density, p.gravity, p.substeps, p.iterations) == (0.02, 1000, 9.81, 4, 4)
+    assert (p.cfm_epsilon_rel, p.s_corr_k, p.s_corr_dq, p.xsph_c, p.omega) == (0.01, 0.1, 0.3, 0.05, 1.0)
+    assert (p.target_particle_count, list(p.box), p.n_bodies) == (60000, [1.5, 1.5, 1.0], 3)
+    assert [(p.bodies[i].shape, p.bodies[i].density) for i in range(3)] == [(0, 0.5), (1, 0.8), (2, 1.4)]
+
+
+def test_no_device_fails_loudly(built):
+    if _lib.device_available():
+        pytest.skip("a GPU is present")
+    L = _lib.lib()
+    h = C.c_void_p()
+    rc = L.p4a_create(0, C.byref(h))
+    assert rc == _abi.P4A_ERR_NODEV and not h.value
+    from particles4all_b200 import Sim, P4AError
+    with pytest.raises(P4AError):
+        Sim()
+
+
+def test_grid_sort_rejects_bad_arguments(built):
+    L = _lib.lib()
+    g = _abi.Grid()
+    g.h = 1.0
+    for k in range(3):
+        g.dim[k] = 4
+    assert L.p4a_grid_sort_workspace_size(100, 64) > 0
+    assert L.p4a_grid_sort_workspace_size(-1, 64) == 0
+    # missing workspace -> capacity error before any device work
+    rc = L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 9), C.c_void_p(16), None, None, 0, None)
+    assert rc == _abi.P4A_ERR_CAPACITY
+    g.dim[0] = 0
+    assert L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 11), None, 0, None) == _abi.P4A_ERR_ARG
