@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(kBlock) k_xsph_finalize(
         const int y = c.y + dy;
         if (y < 0 || y >= P.gridDim[1]) continue;
         const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-        const uint32_t b = __ldg(&cs[rowBase + x0]), e = __ldg(&cs[rowBase + x1 + 1]);
+        const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
         for (uint32_t j = b; j < e; j++) {
           const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
           const float r2 = dot3(rij, rij);
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kBlock) k_xsph_normals(
       const int y = c.y + dy;
       if (y < 0 || y >= P.gridDim[1]) continue;
       const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-      const uint32_t b = __ldg(&cs[rowBase + x0]), e = __ldg(&cs[rowBase + x1 + 1]);
+      const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
       for (uint32_t j = b; j < e; j++) {
         const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
         const float r2 = dot3(rij, rij);
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kBlock) k_tension_finalize(
         const int y = c.y + dy;
         if (y < 0 || y >= P.gridDim[1]) continue;
         const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-        const uint32_t b = __ldg(&cs[rowBase + x0]), e = __ldg(&cs[rowBase + x1 + 1]);
+        const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
         for (uint32_t j = b; j < e; j++) {
           const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
           const float r2 = dot3(rij, rij);

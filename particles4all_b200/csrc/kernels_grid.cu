@@ -66,6 +66,10 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
   if (tid == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const int tile = (int)s_tile;
+  if (tile >= nTiles) {  // only after an earlier launch failed mid-way: never index past the state
+    if (threadIdx.x == 0) atomicOr(err, ERR_SCAN_TIMEOUT);
+    return;
+  }
   const long long base = (long long)tile * kScanTile + (long long)tid * kScanItems;
   uint32_t v[kScanItems];
   uint32_t sum = 0;
@@ -148,7 +152,8 @@ __global__ void __launch_bounds__(kBlock) k_fill(uint32_t n, const uint32_t* __r
                                                  uint32_t* __restrict__ unordered) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= n) return;
-  unordered[__ldg(&cellStart[key[i]]) + rank[i]] = i;
+  const uint32_t at = __ldg(&cellStart[key[i]]) + rank[i];
+  if (at < n) unordered[at] = i;  // always true after a completed scan
 }
 
 __global__ void __launch_bounds__(kBlock) k_reorder(
@@ -162,10 +167,11 @@ __global__ void __launch_bounds__(kBlock) k_reorder(
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= P.n) return;
   const uint32_t k = key[i];
-  const uint32_t b = __ldg(&cellStart[k]), e = __ldg(&cellStart[k + 1]);
+  // min() keeps every access in bounds even if a scan gave up (error word set)
+  const uint32_t e = min(__ldg(&cellStart[k + 1]), P.n), b = min(__ldg(&cellStart[k]), e);
   uint32_t r = 0;
   for (uint32_t m = b; m < e; m++) r += __ldg(&unordered[m]) < i ? 1u : 0u;
-  const uint32_t s = b + r;
+  const uint32_t s = min(b + r, P.n - 1u);
   const float4 p4 = __ldg(&pos[i]);
   F3 v, pr;
   predict_one(P, p4, __ldg(&vel[i]), v, pr);

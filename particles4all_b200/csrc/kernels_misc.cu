@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(128) k_aniso(const __grid_constant__ AnisoPara
       const float dyMin = fmaxf(fmaxf((float)y * A.support - rel.y, rel.y - (float)(y + 1) * A.support), 0.0f);
       if (dz2 + dyMin * dyMin >= r2max) continue;
       const uint32_t rowBase = (uint32_t)((z * A.gridDim[1] + y) * A.gridDim[0]);
-      const uint32_t jb = __ldg(&cs[rowBase + x0]), je = __ldg(&cs[rowBase + x1 + 1]);
+      const uint32_t jb = __ldg(&cs[rowBase + x0]), je = min(__ldg(&cs[rowBase + x1 + 1]), A.count);
       for (uint32_t j = jb; j < je; j++) {
         const F3 d = sub3(xyz(__ldg(&pos[j])), xi);
         const float r2 = dot3(d, d);
