@@ -76,6 +76,7 @@ struct p4a_sim {
   size_t pinnedBytes = 0;
   cudaEvent_t readEvent = nullptr;
   bool readPending = false;
+  bool readStale = false;  // a step finished after the last readback was issued
   bool poseValid = false;
   p4a_stats stats{};
   std::vector<float> pose;  // per body: centre xyz, then 3 rows xyz(w)
@@ -357,6 +358,7 @@ int reset_common(p4a_sim* s) {
     s->pinnedBytes = want;
   }
   s->readPending = false;
+  s->readStale = false;
   s->poseValid = false;
   s->stats = p4a_stats{};
   s->stats.avg_rho = 1;
@@ -406,6 +408,25 @@ int check_error_word(p4a_sim* s) {
   const uint32_t w = s->pinned ? s->pinned[8] : 0u;
   if (w & ERR_SCAN_TIMEOUT)
     return fail(s, P4A_ERR_TIMEOUT, "cell scan: a bounded wait on a predecessor tile gave up");
+  return P4A_OK;
+}
+
+// Queues the copy of statsOut, the error word and the body pose into pinned memory
+// behind the work already on the stream (src/sim.js:604-614).
+int issue_readback(p4a_sim* s) {
+  cudaStream_t st = s->stream;
+  DevScene& d = s->d;
+  CUDA_TRY(s, cudaMemcpyAsync(s->pinned, d.statsOut, 32, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(s, cudaMemcpyAsync(s->pinned + 8, d.errorWord, 4, cudaMemcpyDeviceToHost, st));
+  if (s->nBodies) {
+    float* f = (float*)(s->pinned + 16);
+    CUDA_TRY(s, cudaMemcpyAsync(f, d.bodyCentre, (size_t)s->nBodies * 16, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(s, cudaMemcpyAsync(f + (size_t)s->nBodies * 4, d.bodyRot, (size_t)s->nBodies * 48,
+                                cudaMemcpyDeviceToHost, st));
+  }
+  CUDA_TRY(s, cudaEventRecord(s->readEvent, st));
+  s->readPending = true;
+  s->readStale = false;
   return P4A_OK;
 }
 
@@ -664,6 +685,10 @@ int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
     return P4A_OK;
   }
   const double dt = dtTarget;
+  {
+    const int rc = poll_readback(s, false);  // a finished readback frees the slot
+    if (rc) return rc;
+  }
   pack_params(s, dt);
   const SimParams& P = s->P;
   DevScene& d = s->d;
@@ -722,18 +747,8 @@ int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
   mark(s, PH_END);
   CUDA_TRY(s, cudaGetLastError());
   // stats and pose readback (src/sim.js:598-655), at most one in flight
-  if (!s->readPending) {
-    CUDA_TRY(s, cudaMemcpyAsync(s->pinned, d.statsOut, 32, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(s, cudaMemcpyAsync(s->pinned + 8, d.errorWord, 4, cudaMemcpyDeviceToHost, st));
-    if (s->nBodies) {
-      float* f = (float*)(s->pinned + 16);
-      CUDA_TRY(s, cudaMemcpyAsync(f, d.bodyCentre, (size_t)s->nBodies * 16, cudaMemcpyDeviceToHost, st));
-      CUDA_TRY(s, cudaMemcpyAsync(f + (size_t)s->nBodies * 4, d.bodyRot, (size_t)s->nBodies * 48,
-                                  cudaMemcpyDeviceToHost, st));
-    }
-    CUDA_TRY(s, cudaEventRecord(s->readEvent, st));
-    s->readPending = true;
-  }
+  if (!s->readPending) return issue_readback(s);
+  s->readStale = true;
   return P4A_OK;
 }
 
@@ -896,10 +911,19 @@ int p4a_write(p4a_sim* s, int32_t id, int32_t which, const void* host, size_t of
   return P4A_OK;
 }
 
+// wait = 1: the values of the last step, read back now if its own readback was
+// skipped because an earlier one was still in flight.
+static int refresh_readback(p4a_sim* s, bool wait) {
+  int rc = poll_readback(s, wait);
+  if (rc || !wait || !s->readStale || !s->ready) return rc;
+  if ((rc = issue_readback(s))) return rc;
+  return poll_readback(s, true);
+}
+
 int p4a_get_stats(p4a_sim* s, int32_t wait, p4a_stats* out) {
   if (!s || !out) return P4A_ERR_ARG;
   cudaSetDevice(s->device);
-  const int rc = poll_readback(s, wait != 0);
+  const int rc = refresh_readback(s, wait != 0);
   *out = s->stats;
   return rc;
 }
@@ -907,7 +931,7 @@ int p4a_get_stats(p4a_sim* s, int32_t wait, p4a_stats* out) {
 int p4a_body_pose(p4a_sim* s, int32_t wait, float* centre3, float* rot9, int32_t maxBodies) {
   if (!s) return P4A_ERR_ARG;
   cudaSetDevice(s->device);
-  const int rc = poll_readback(s, wait != 0);
+  const int rc = refresh_readback(s, wait != 0);
   const int nb = std::min(maxBodies, s->nBodies);
   for (int b = 0; b < nb; b++) {
     if (centre3)
