@@ -118,7 +118,7 @@ def _base_params(box, iterations, tension, xsph, substeps=2):
         "spacing": 0.5, "restDensity": 1.0, "gravity": 9.8, "substeps": substeps,
         "iterations": iterations, "cfmEpsilonRel": 0.01, "cfmEpsilonAbs": 100.0,
         "sCorrK": 0.1, "sCorrDq": 0.3, "xsphC": xsph, "omega": 1.0, "sorAverage": False,
-        "surfaceTensionK": tension, "box": list(box), "bodies": [], "bodySize": 0,
+        "surfaceTensionK": tension, "box": [float(b) for b in box], "bodies": [], "bodySize": 0,
         "noBoundary": False, "pour": False,
     }
 
@@ -136,10 +136,12 @@ def medium_bodies_264k(seed=1, side=64, n_cubes=8, cube=6):
     """The medium scene with 8 floating cubes (side = 64 is the workload)."""
     d, h = 0.5, 1.0
     rng = np.random.default_rng(seed)
-    box = np.array([80.0, 48.0, 40.0]) * (side / 64.0)
-    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
     top = d + side * d
     span = cube * d
+    box = np.array([80.0, 48.0, 40.0]) * (side / 64.0)
+    # room above the water for the cubes at reduced sizes (no change at side = 64)
+    box = np.maximum(box, [4 * span + 4.0, top + 4 * span + 2.0, 4 * span + 4.0])
+    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
     lo = np.array([span + 1.0, top + span, span + 1.0])
     hi = np.array([box[0] - span - 1.0, min(box[1] - span - 1.0, top + 3 * span), box[2] - span - 1.0])
     centres = _place_bodies(rng, n_cubes, lo, hi, min_dist=2.0 * span)
@@ -163,9 +165,10 @@ def large_hose_2m(seed=2, side=128, n_bodies=64, target_total=2_500_000):
     """The large scene with 64 mixed bodies and a hose (side = 128 is the workload)."""
     d, h = 0.5, 1.0
     rng = np.random.default_rng(seed)
-    box = np.array([160.0, 96.0, 80.0]) * (side / 128.0)
-    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
     top = d + side * d
+    box = np.array([160.0, 96.0, 80.0]) * (side / 128.0)
+    box = np.maximum(box, [40.0, top + 20.0, 40.0])  # room for the bodies at reduced sizes
+    fluid = _fluid_lattice(side, side, side, d, 0.01 * d, rng, np.array([d, d, d]))
     bodies = []
     lo = np.array([6.0, top + 6.0, 6.0])
     hi = np.array([box[0] - 6.0, box[1] - 6.0, box[2] - 6.0])
