@@ -288,6 +288,31 @@ int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity,
                   float* rest_out, uint32_t* cell_start, uint32_t* slot_out, void* workspace,
                   size_t workspace_bytes, void* stream);
 
+/* ---- operator entry without allocation ---------------------------------- */
+/*
+ * No counterpart in the reference. The same operation as p4a_grid_sort for
+ * callers that cannot allocate device memory: a host that owns every device
+ * allocation through its own arena (a renderer or plugin host with a fixed
+ * budget), or a real-time frame loop in which a cudaMalloc, which may synchronise
+ * the device, would stall the frame. The caller still passes every input and
+ * output buffer; the scratch comes from one fixed device array inside the
+ * library (about 8.4 MB, held by every GPU that loads the library until exit).
+ *   - n <= P4A_NOALLOC_MAX_PARTICLES and dim[0]*dim[1]*dim[2] <=
+ *     P4A_NOALLOC_MAX_CELLS, else P4A_ERR_CAPACITY with no device work.
+ *   - Allocates nothing. The first call on a device looks up the array's
+ *     address (once per device); make that first call before any stream capture.
+ *   - The array is shared by all calls: the parts that must start at zero are
+ *     cleared on `stream` at the start of each call, and calls whose work
+ *     overlaps on the GPU race on it.
+ */
+#define P4A_NOALLOC_MAX_PARTICLES 524288
+#define P4A_NOALLOC_MAX_CELLS 524288
+int p4a_grid_sort_noalloc(const p4a_grid* grid, int32_t n, float dt, float gravity,
+                          const float* pos, const float* vel, const uint32_t* body,
+                          const float* rest, float* pos_out, float* vel_out, float* pred_out,
+                          uint32_t* body_out, float* rest_out, uint32_t* cell_start,
+                          uint32_t* slot_out, void* stream);
+
 /* ---- host-side scene builder (src/scene.js:159-315) --------------------- */
 /* buildScene(params) into caller-provided host arrays; call once with NULL
  * arrays to get the counts. pos/vel/rest float4[n], phase uint4[n]. */

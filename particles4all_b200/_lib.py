@@ -42,6 +42,7 @@ SIGNATURES = {
     "p4a_profile_reset": ([_vp], C.c_int),
     "p4a_profile_read": ([_vp, _vp, _i32, C.POINTER(_i32)], C.c_int),
     "p4a_kernel_launches": ([], C.c_uint64),
+    "p4a_grid_sort_noalloc": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp], C.c_int),
 }
 
 _lib = None

@@ -1,0 +1,117 @@
+// grid_sort_noalloc.cu — p4a_grid_sort_noalloc: the predict + grid-sort operator
+// for callers that cannot allocate device memory.
+//
+// Who needs it: hosts that own every device allocation themselves (a renderer or
+// plugin host with a fixed memory budget and its own arena) and real-time frame
+// loops where a cudaMalloc, which may synchronise the device, would stall the
+// frame. Such callers can pass their input and output buffers but cannot hand the
+// operator a workspace, so the operator's scratch (cell keys, arrival ranks, the
+// bucket lists, the cell histogram and the scan's tile states) lives in one
+// file-scope device array instead. That array is part of the library image: every
+// GPU that loads libp4a holds it until the process exits.
+//
+// The entry point calls no cudaMalloc, cudaFree or other allocating routine. On the
+// first call on a device it looks up the array's device address with
+// cudaGetSymbolAddress (once per device, under a lock); make that first call before
+// any stream capture. The array is shared by every call: the parts that must start
+// at zero are cleared on the caller's stream at the start of each call, and calls
+// whose work overlaps on the GPU (different streams, or different host threads
+// without ordering) race on it.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "../../include/p4a.h"
+#include "p4a_internal.h"
+
+namespace p4a {
+namespace {
+constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t kMaxN = P4A_NOALLOC_MAX_PARTICLES;
+constexpr size_t kMaxCells = P4A_NOALLOC_MAX_CELLS;
+constexpr size_t kMaxTiles = (kMaxCells + kScanTile - 1) / kScanTile;
+// layout: key, rank, unordered | cellCount | scan tile states | ticket | error word
+constexpr size_t kOffRank = align256(kMaxN * 4);
+constexpr size_t kOffUnordered = kOffRank + align256(kMaxN * 4);
+constexpr size_t kOffCount = kOffUnordered + align256(kMaxN * 4);
+constexpr size_t kOffState = kOffCount + align256((kMaxCells + 1) * 4);
+constexpr size_t kOffTicket = kOffState + align256(kMaxTiles * 8);
+constexpr size_t kOffErr = kOffTicket + 256;
+constexpr size_t kScratchBytes = kOffErr + 256;
+}  // namespace
+}  // namespace p4a
+
+// The operator's scratch, one per device that loads the library.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[p4a::kScratchBytes];
+
+namespace p4a {
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_setup_mu;
+void* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once).
+int scratch_address(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return P4A_ERR_CUDA;
+  if (dev < 0 || dev >= kMaxDevices) return P4A_ERR_NODEV;
+  std::lock_guard<std::mutex> lock(g_setup_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return P4A_ERR_CUDA;
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return P4A_OK;
+}
+
+}  // namespace
+}  // namespace p4a
+
+extern "C" int p4a_grid_sort_noalloc(const p4a_grid* grid, int32_t n, float dt, float gravity,
+                                     const float* pos, const float* vel, const uint32_t* body,
+                                     const float* rest, float* pos_out, float* vel_out,
+                                     float* pred_out, uint32_t* body_out, float* rest_out,
+                                     uint32_t* cell_start, uint32_t* slot_out, void* stream) {
+  using namespace p4a;
+  if (!grid || n < 0 || grid->dim[0] < 1 || grid->dim[1] < 1 || grid->dim[2] < 1 || !(grid->h > 0))
+    return P4A_ERR_ARG;
+  const long long cells = (long long)grid->dim[0] * grid->dim[1] * grid->dim[2];
+  if ((size_t)n > kMaxN || cells > (long long)kMaxCells) return P4A_ERR_CAPACITY;
+  if (n > 0 && (!pos || !vel || !pos_out || !vel_out || !pred_out)) return P4A_ERR_ARG;
+  if ((body && !body_out) || (rest && !rest_out) || !cell_start) return P4A_ERR_ARG;
+  void* base = nullptr;
+  const int rc = scratch_address(&base);
+  if (rc != P4A_OK) return rc;
+  char* w = (char*)base;
+  uint32_t* key = (uint32_t*)w;
+  uint32_t* rank = (uint32_t*)(w + kOffRank);
+  uint32_t* unordered = (uint32_t*)(w + kOffUnordered);
+  uint32_t* cellCount = (uint32_t*)(w + kOffCount);
+  unsigned long long* state = (unsigned long long*)(w + kOffState);
+  uint32_t* ticket = (uint32_t*)(w + kOffTicket);
+  uint32_t* errw = (uint32_t*)(w + kOffErr);
+  cudaStream_t st = (cudaStream_t)stream;
+  // histogram, tile states, ticket and error word start at zero on every call
+  if (cudaMemsetAsync(cellCount, 0, kScratchBytes - kOffCount, st) != cudaSuccess) return P4A_ERR_CUDA;
+  const int nCells = (int)cells;
+  SimParams P{};
+  for (int k = 0; k < 3; k++) {
+    P.boxMin[k] = grid->box_min[k];
+    P.gridDim[k] = grid->dim[k];
+  }
+  P.h = grid->h;
+  P.dt = dt;
+  P.gravity = gravity;
+  P.n = (uint32_t)n;
+  P.nCells = (uint32_t)nCells;
+  launch_key_count(P, (const float4*)pos, (const float4*)vel, key, rank, cellCount, nullptr, 0, st);
+  launch_scan(cellCount, cell_start, nCells, state, ticket, 1u, errw, st);
+  launch_fill((uint32_t)n, key, rank, cell_start, unordered, st);
+  launch_reorder(P, key, cell_start, unordered, (const float4*)pos, (const float4*)vel,
+                 (const uint4*)body, (const float4*)rest, (float4*)pos_out, (float4*)vel_out,
+                 (float4*)pred_out, (uint4*)body_out, (float4*)rest_out, slot_out, nullptr, nullptr,
+                 nullptr, st);
+  return cudaGetLastError() == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+}
