@@ -299,8 +299,10 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.corr, cap)) || (rc = dalloc(s, L, &s->d.normal, cap)) ||
       (rc = dalloc(s, L, &s->d.key, cap)) || (rc = dalloc(s, L, &s->d.rank, cap)) ||
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
-      (rc = dalloc(s, L, &s->d.errorWord, 4)))
+      (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbMask, cap * 9)) ||
+      (rc = dalloc(s, L, &s->d.nbLong, cap)))
     return rc;
+  s->d.cap = (uint32_t)cap;
   if ((rc = alloc_cells(s))) return rc;
   if ((rc = upload_boundary(s))) return rc;
   // bodies (src/sim.js:129-161)

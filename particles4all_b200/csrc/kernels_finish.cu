@@ -10,9 +10,11 @@
 //              totals are the same bits
 // The velFromPos velocities live in a scratch buffer (the non-live vel copy), so
 // the final velocity can be written to the live copy while neighbours still read
-// the scratch one.
+// the scratch one. xsph+normals builds the neighbour masks (neighbours.cuh) and
+// stores them for the tension pass, which walks the same positions.
 #include <cuda_runtime.h>
 
+#include "neighbours.cuh"
 #include "p4a_internal.h"
 #include "p4a_math.cuh"
 
@@ -63,7 +65,7 @@ __device__ __forceinline__ void block_stats(const SimParams& P, bool act, float 
 }
 
 // xsph (+ finalize) for scenes without surface tension.
-__global__ void __launch_bounds__(kBlock) k_xsph_finalize(
+__global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(
     const __grid_constant__ SimParams P, const float4* __restrict__ pred,
     const float4* __restrict__ velIn, const float* __restrict__ density,
     const uint32_t* __restrict__ cs, float4* __restrict__ posOut, float4* __restrict__ velOut,
@@ -75,25 +77,22 @@ __global__ void __launch_bounds__(kBlock) k_xsph_finalize(
   if (act) {
     const float4 p4 = __ldg(&pred[i]);
     const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
-    const I3 c = cell_of(P, pi);
-    const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, P.gridDim[0] - 1);
+    const RowWalk w(P, pi);
+    uint32_t longRows = 0u;
     F3 acc = {0.f, 0.f, 0.f};
-    for (int dz = -1; dz <= 1; dz++) {
-      const int z = c.z + dz;
-      if (z < 0 || z >= P.gridDim[2]) continue;
-      for (int dy = -1; dy <= 1; dy++) {
-        const int y = c.y + dy;
-        if (y < 0 || y >= P.gridDim[1]) continue;
-        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-        const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
-        for (uint32_t j = b; j < e; j++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || j == i) continue;
-          const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
-          acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
-        }
-      }
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      const int rb = w.row_base(P, r);
+      if (rb < 0) continue;
+      bool lg;
+      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
+      visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
+        if (j == i) return;
+        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+        const float r2 = dot3(rij, rij);
+        const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
+        acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+      });
     }
     const F3 corr = mul3(acc, P.xsphC);
     vf = add3(vi, corr);
@@ -106,50 +105,52 @@ __global__ void __launch_bounds__(kBlock) k_xsph_finalize(
 }
 
 // xsph + normals (tension scenes): corr = xsphC * acc, normal = h * nacc.
-__global__ void __launch_bounds__(kBlock) k_xsph_normals(
+__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(
     const __grid_constant__ SimParams P, const float4* __restrict__ pred,
     const float4* __restrict__ velIn, const float* __restrict__ density,
-    const uint32_t* __restrict__ cs, float4* __restrict__ corrOut, float4* __restrict__ normalOut) {
+    const uint32_t* __restrict__ cs, float4* __restrict__ corrOut, float4* __restrict__ normalOut,
+    uint64_t* __restrict__ masks, uint32_t* __restrict__ longs, uint32_t cap) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= P.n) return;
   const F3 pi = xyz(__ldg(&pred[i])), vi = xyz(__ldg(&velIn[i]));
-  const I3 c = cell_of(P, pi);
-  const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, P.gridDim[0] - 1);
+  const RowWalk w(P, pi);
+  uint32_t longRows = 0u;
   F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
-  for (int dz = -1; dz <= 1; dz++) {
-    const int z = c.z + dz;
-    if (z < 0 || z >= P.gridDim[2]) continue;
-    for (int dy = -1; dy <= 1; dy++) {
-      const int y = c.y + dy;
-      if (y < 0 || y >= P.gridDim[1]) continue;
-      const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-      const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
-      for (uint32_t j = b; j < e; j++) {
-        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-        const float r2 = dot3(rij, rij);
-        if (r2 >= P.h2 || j == i) continue;
-        const float dj = fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
-        const float f = P.mass * poly6(P, r2) / dj;
-        acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
-        if (r2 < 1.0e-12f) continue;
-        const float r = sqrtf(r2);
-        const float hr = P.h - r;
-        const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / r);
-        nacc = fma3(coef, rij, nacc);
-      }
-    }
+#pragma unroll
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    bool lg;
+    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
+    masks[(size_t)r * cap + i] = mr;
+    if (lg) longRows |= 1u << r;
+    visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
+      if (j == i) return;
+      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const float r2 = dot3(rij, rij);
+      const float dj = fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
+      const float f = P.mass * poly6(P, r2) / dj;
+      acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+      if (r2 < 1.0e-12f) return;
+      const float rr = sqrtf(r2);
+      const float hr = P.h - rr;
+      const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / rr);
+      nacc = fma3(coef, rij, nacc);
+    });
   }
+  longs[i] = longRows;
   corrOut[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
   normalOut[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
 }
 
 // tension + finalize.
-__global__ void __launch_bounds__(kBlock) k_tension_finalize(
+__global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(
     const __grid_constant__ SimParams P, const float4* __restrict__ pred,
     const float4* __restrict__ velIn, const float* __restrict__ density,
     const float4* __restrict__ normal, float4* __restrict__ corr, const uint32_t* __restrict__ cs,
     float4* __restrict__ posOut, float4* __restrict__ velOut, float4* __restrict__ predCopy,
-    uint32_t* __restrict__ statsOut) {
+    uint32_t* __restrict__ statsOut, const uint64_t* __restrict__ masks,
+    const uint32_t* __restrict__ longs, uint32_t cap) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   const bool act = i < P.n;
   F3 vf = {0.f, 0.f, 0.f};
@@ -158,33 +159,29 @@ __global__ void __launch_bounds__(kBlock) k_tension_finalize(
     const float4 p4 = __ldg(&pred[i]);
     const F3 pi = xyz(p4), ni = xyz(__ldg(&normal[i]));
     rhoi = __ldg(&density[i]);
-    const I3 c = cell_of(P, pi);
-    const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, P.gridDim[0] - 1);
+    const RowWalk w(P, pi);
+    const uint32_t longRows = __ldg(&longs[i]);
     F3 acc = {0.f, 0.f, 0.f};
-    for (int dz = -1; dz <= 1; dz++) {
-      const int z = c.z + dz;
-      if (z < 0 || z >= P.gridDim[2]) continue;
-      for (int dy = -1; dy <= 1; dy++) {
-        const int y = c.y + dy;
-        if (y < 0 || y >= P.gridDim[1]) continue;
-        const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-        const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
-        for (uint32_t j = b; j < e; j++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) continue;
-          const float r = sqrtf(r2);
-          const float hrr = P.h - r;
-          const float k = hrr * hrr * hrr * r * r * r;
-          float cw = P.cohes * (2.0f * k - P.cohesTerm);
-          if (2.0f * r > P.h) cw = P.cohes * k;
-          const float sCoh = -P.tension * P.mass * cw / r;
-          const F3 fCoh = mul3(rij, sCoh);
-          const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&normal[j]))), -P.tension);
-          const float w = 2.0f * P.rho0 / (rhoi + __ldg(&density[j]));
-          acc = fma3(w, add3(fCoh, fCurv), acc);
-        }
-      }
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      const int rb = w.row_base(P, r);
+      if (rb < 0) continue;
+      const uint64_t mr = __ldg(&masks[(size_t)r * cap + i]);
+      visit_row(P, w, rb, pi, mr, (longRows >> r) & 1u, pred, cs, [&](uint32_t j) {
+        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+        const float r2 = dot3(rij, rij);
+        if (r2 < 1.0e-12f || j == i) return;
+        const float rr = sqrtf(r2);
+        const float hrr = P.h - rr;
+        const float k = hrr * hrr * hrr * rr * rr * rr;
+        float cw = P.cohes * (2.0f * k - P.cohesTerm);
+        if (2.0f * rr > P.h) cw = P.cohes * k;
+        const float sCoh = -P.tension * P.mass * cw / rr;
+        const F3 fCoh = mul3(rij, sCoh);
+        const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&normal[j]))), -P.tension);
+        const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&density[j]));
+        acc = fma3(wgt, add3(fCoh, fCurv), acc);
+      });
     }
     const float4 c0 = corr[i];
     const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
@@ -208,7 +205,7 @@ void launch_xsph_finalize(const SimParams& P, const DevScene& d, const float4* p
 void launch_xsph_normals(const SimParams& P, const DevScene& d, const float4* pred,
                          const float4* velIn, cudaStream_t st) {
   k_xsph_normals<<<groups(P.n), kBlock, 0, st>>>(P, pred, velIn, d.density, d.cellStart, d.corr,
-                                                 d.normal);
+                                                 d.normal, d.nbMask, d.nbLong, d.cap);
 }
 
 void launch_tension_finalize(const SimParams& P, const DevScene& d, const float4* pred,
@@ -216,7 +213,8 @@ void launch_tension_finalize(const SimParams& P, const DevScene& d, const float4
                              float4* predCopy, bool stats, cudaStream_t st) {
   k_tension_finalize<<<groups(P.n), kBlock, 0, st>>>(P, pred, velIn, d.density, d.normal, d.corr,
                                                      d.cellStart, posOut, velOut, predCopy,
-                                                     stats ? d.statsOut : nullptr);
+                                                     stats ? d.statsOut : nullptr, d.nbMask,
+                                                     d.nbLong, d.cap);
 }
 
 }  // namespace p4a

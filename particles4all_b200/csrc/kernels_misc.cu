@@ -57,7 +57,7 @@ __device__ __forceinline__ void store_g(float4* __restrict__ g, uint32_t i, cons
   g[i * 2 + 1] = make_float4(elc(G, 2, 1), elc(G, 2, 2), det3(G), last);
 }
 
-__global__ void __launch_bounds__(128) k_aniso(const __grid_constant__ AnisoParams A,
+__global__ void __launch_bounds__(128, 10) k_aniso(const __grid_constant__ AnisoParams A,
                                                const float4* __restrict__ pos,
                                                const uint32_t* __restrict__ cs,
                                                float4* __restrict__ smoothPos,

@@ -1,72 +1,76 @@
 // kernels_solve.cu — the PBF Jacobi iteration: lambda (src/wgsl.js:477-543) and
-// delta (src/wgsl.js:545-612). Gather-only: each thread owns one particle and walks
-// the 3x3 row ranges [cellStart[row+x0], cellStart[row+x1+1]) of the cell block
-// around cellOf(current pred) with the cellStart of the substep's sort (the
-// reference's stale-cell semantics), fluid then boundary samples per row, j
-// ascending: the reference's accumulation order. No float atomics, so results are
-// identical from run to run.
+// delta (src/wgsl.js:545-612). Gather-only: each thread owns one particle and visits
+// the neighbours of the 3x3 row ranges around cellOf(current pred), using the
+// cellStart of the substep's sort (the reference's stale-cell semantics), fluid then
+// boundary samples per row, j ascending: the reference's accumulation order, so the
+// sums are bit-identical to it under the float contract. No float atomics.
 //
+// lambda builds the per-row neighbour masks (neighbours.cuh) and stores them; delta
+// runs on the same positions, so it reuses them and skips the candidate tests.
 // The last delta of a substep also writes velFromPos (src/wgsl.js:72-83) for every
 // particle into the scratch velocity buffer; body particles are overwritten by the
 // rigid projection that follows.
 #include <cuda_runtime.h>
 
+#include "neighbours.cuh"
 #include "p4a_internal.h"
 #include "p4a_math.cuh"
 
 namespace p4a {
 
-__global__ void __launch_bounds__(kBlock) k_lambda(
+__global__ void __launch_bounds__(kBlock, 4) k_lambda(
     const __grid_constant__ SimParams P, const float4* __restrict__ pred,
     float* __restrict__ lambda, float* __restrict__ density, const uint32_t* __restrict__ cs,
     const float4* __restrict__ bpos, const float* __restrict__ bpsi,
-    const uint32_t* __restrict__ bcs) {
+    const uint32_t* __restrict__ bcs, uint64_t* __restrict__ masks, uint32_t* __restrict__ longs,
+    uint32_t cap) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= P.n) return;
   const F3 pi = xyz(__ldg(&pred[i]));
-  const I3 c = cell_of(P, pi);
-  const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, P.gridDim[0] - 1);
+  const RowWalk w(P, pi);
+  uint32_t longRows = 0u;
+
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;
-  for (int dz = -1; dz <= 1; dz++) {
-    const int z = c.z + dz;
-    if (z < 0 || z >= P.gridDim[2]) continue;
-    for (int dy = -1; dy <= 1; dy++) {
-      const int y = c.y + dy;
-      if (y < 0 || y >= P.gridDim[1]) continue;
-      const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-      const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
-      for (uint32_t j = b; j < e; j++) {
-        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-        const float r2 = dot3(rij, rij);
-        if (r2 >= P.h2 || j == i) continue;
-        rho = fmaf(P.mass, poly6(P, r2), rho);
-        if (r2 > 1.0e-12f) {
-          const float r = sqrtf(r2);
-          const float hr = P.h - r;
-          const float s = P.volume * P.spikyGrad * hr * hr / r;
-          const F3 g = mul3(rij, s);
-          gradSum = add3(gradSum, g);
-          sumGrad2 = sumGrad2 + dot3(g, g);
-        }
+#pragma unroll
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    bool lg;
+    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
+    masks[(size_t)r * cap + i] = mr;
+    if (lg) longRows |= 1u << r;
+    visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
+      if (j == i) return;
+      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const float r2 = dot3(rij, rij);
+      rho = fmaf(P.mass, poly6(P, r2), rho);
+      if (r2 > 1.0e-12f) {
+        const float rr = sqrtf(r2);
+        const float hr = P.h - rr;
+        const float s = P.volume * P.spikyGrad * hr * hr / rr;
+        const F3 g = mul3(rij, s);
+        gradSum = add3(gradSum, g);
+        sumGrad2 = sumGrad2 + dot3(g, g);
       }
-      if (P.nBoundary > 0u) {
-        const uint32_t bb = __ldg(&bcs[rowBase + x0]), be = __ldg(&bcs[rowBase + x1 + 1]);
-        for (uint32_t k = bb; k < be; k++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&bpos[k])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-          const float psi = __ldg(&bpsi[k]);
-          rho = fmaf(psi, poly6(P, r2), rho);
-          const float r = sqrtf(r2);
-          const float hr = P.h - r;
-          const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / r;
-          gradSum = fma3(s, rij, gradSum);
-        }
+    });
+    if (P.nBoundary > 0u) {
+      const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+      for (uint32_t k = bb; k < be; k++) {
+        const F3 rij = sub3(pi, xyz(__ldg(&bpos[k])));
+        const float r2 = dot3(rij, rij);
+        if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+        const float psi = __ldg(&bpsi[k]);
+        rho = fmaf(psi, poly6(P, r2), rho);
+        const float rr = sqrtf(r2);
+        const float hr = P.h - rr;
+        const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
+        gradSum = fma3(s, rij, gradSum);
       }
     }
   }
+  longs[i] = longRows;
   density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
   if (C > 0.0f) {
@@ -77,54 +81,51 @@ __global__ void __launch_bounds__(kBlock) k_lambda(
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_delta(
+__global__ void __launch_bounds__(kBlock, 5) k_delta(
     const __grid_constant__ SimParams P, const float4* __restrict__ pred,
     float4* __restrict__ predOut, const float* __restrict__ lambda,
     const uint32_t* __restrict__ cs, const float4* __restrict__ bpos,
     const float* __restrict__ bpsi, const uint32_t* __restrict__ bcs,
+    const uint64_t* __restrict__ masks, const uint32_t* __restrict__ longs, uint32_t cap,
     const float4* __restrict__ posLive, float4* __restrict__ velScratch) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= P.n) return;
   const F3 pi = xyz(__ldg(&pred[i]));
   const float li = __ldg(&lambda[i]);
-  const I3 c = cell_of(P, pi);
-  const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, P.gridDim[0] - 1);
+  const RowWalk w(P, pi);
+  const uint32_t longRows = __ldg(&longs[i]);
   F3 d = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
   float nc = 1.0f;
-  for (int dz = -1; dz <= 1; dz++) {
-    const int z = c.z + dz;
-    if (z < 0 || z >= P.gridDim[2]) continue;
-    for (int dy = -1; dy <= 1; dy++) {
-      const int y = c.y + dy;
-      if (y < 0 || y >= P.gridDim[1]) continue;
-      const uint32_t rowBase = (uint32_t)((z * P.gridDim[1] + y) * P.gridDim[0]);
-      const uint32_t b = __ldg(&cs[rowBase + x0]), e = min(__ldg(&cs[rowBase + x1 + 1]), P.n);
-      for (uint32_t j = b; j < e; j++) {
-        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+#pragma unroll
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    const uint64_t mr = __ldg(&masks[(size_t)r * cap + i]);
+    visit_row(P, w, rb, pi, mr, (longRows >> r) & 1u, pred, cs, [&](uint32_t j) {
+      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const float r2 = dot3(rij, rij);
+      if (r2 < 1.0e-12f || j == i) return;
+      const float rr = sqrtf(r2);
+      const float hr = P.h - rr;
+      const float s = P.spikyGrad * hr * hr / rr;
+      const float t = P.h2 - r2;
+      const float ratio = P.poly6 * t * t * t * P.sCorrWq;
+      const float r2r = ratio * ratio;
+      const float sc = -P.sCorrK * r2r * r2r;
+      const float coef = (li + __ldg(&lambda[j]) + sc) * s;
+      d = fma3(coef, rij, d);
+      nc += 1.0f;
+    });
+    if (P.nBoundary > 0u) {
+      const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+      for (uint32_t k = bb; k < be; k++) {
+        const F3 rij = sub3(pi, xyz(__ldg(&bpos[k])));
         const float r2 = dot3(rij, rij);
-        if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) continue;
-        const float r = sqrtf(r2);
-        const float hr = P.h - r;
-        const float s = P.spikyGrad * hr * hr / r;
-        const float t = P.h2 - r2;
-        const float ratio = P.poly6 * t * t * t * P.sCorrWq;
-        const float r2r = ratio * ratio;
-        const float sc = -P.sCorrK * r2r * r2r;
-        const float coef = (li + __ldg(&lambda[j]) + sc) * s;
-        d = fma3(coef, rij, d);
-        nc += 1.0f;
-      }
-      if (P.nBoundary > 0u) {
-        const uint32_t bb = __ldg(&bcs[rowBase + x0]), be = __ldg(&bcs[rowBase + x1 + 1]);
-        for (uint32_t k = bb; k < be; k++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&bpos[k])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-          const float r = sqrtf(r2);
-          const float hr = P.h - r;
-          const float coef = (li * __ldg(&bpsi[k])) * (P.spikyGrad * hr * hr / r);
-          dB = fma3(coef, rij, dB);
-        }
+        if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+        const float rr = sqrtf(r2);
+        const float hr = P.h - rr;
+        const float coef = (li * __ldg(&bpsi[k])) * (P.spikyGrad * hr * hr / rr);
+        dB = fma3(coef, rij, dB);
       }
     }
   }
@@ -146,13 +147,14 @@ __global__ void __launch_bounds__(kBlock) k_delta(
 
 void launch_lambda(const SimParams& P, const DevScene& d, const float4* pred, cudaStream_t st) {
   k_lambda<<<groups(P.n), kBlock, 0, st>>>(P, pred, d.lambda, d.density, d.cellStart, d.bpos,
-                                           d.bpsi, d.bcellStart);
+                                           d.bpsi, d.bcellStart, d.nbMask, d.nbLong, d.cap);
 }
 
 void launch_delta(const SimParams& P, const DevScene& d, const float4* pred, float4* predOut,
                   const float4* posLive, float4* velScratch, cudaStream_t st) {
   k_delta<<<groups(P.n), kBlock, 0, st>>>(P, pred, predOut, d.lambda, d.cellStart, d.bpos,
-                                          d.bpsi, d.bcellStart, posLive, velScratch);
+                                          d.bpsi, d.bcellStart, d.nbMask, d.nbLong, d.cap,
+                                          posLive, velScratch);
 }
 
 }  // namespace p4a

@@ -76,6 +76,9 @@ struct DevScene {
   uint32_t* errorWord;  // [1]
   float4* smoothPos;
   float4* anisoG;
+  uint64_t* nbMask;     // [9][cap] per-row neighbour masks shared by a pair of passes
+  uint32_t* nbLong;     // [cap] rows with more than 64 candidates
+  uint32_t cap;         // particle capacity (stride of nbMask)
 };
 
 constexpr int kBlock = 256;          // particles per block (the reference's workgroup)
