@@ -262,6 +262,56 @@ int p4a_profile_read(p4a_sim* sim, p4a_phase_time* out, int32_t max_entries, int
  * library in this process (all handles and operator entries). */
 uint64_t p4a_kernel_launches(void);
 
+/* ---- batched multi-scene stepping -------------------------------------- */
+/*
+ * Extension, no counterpart in the reference (which steps one scene per Sim).
+ * Many independent scenes live in shared device arenas and are stepped together:
+ * every pass of a substep is ONE launch over all listed scenes, whose blocks pull
+ * (scene, tile) work items; the cell-key sort is one counting sort over the
+ * scenes' disjoint key ranges. Each scene keeps its own parameters, time bank,
+ * parity, iteration count and tension setting, and its results are bit-identical
+ * to stepping it alone with p4a_step.
+ */
+typedef struct p4a_batch p4a_batch;
+typedef struct p4a_batch_config {
+  int64_t max_particles;   /* particle arena: sum of scene capacities        */
+  int64_t max_cells;       /* cell arena: sum of scene cells (+ tile padding)*/
+  int64_t max_boundary;    /* boundary-sample arena                          */
+  int32_t max_scenes;
+  int32_t max_bodies;      /* body arena: sum over scenes of (bodies + 1)    */
+  int64_t max_body_parts;  /* body-particle list arena                       */
+} p4a_batch_config;
+typedef struct p4a_batch_usage {
+  int64_t free_particles, free_cells, free_boundary, free_body_parts;
+  int32_t free_scenes, free_bodies;
+  int32_t live_scenes;
+  int64_t device_bytes;    /* bytes the batch holds on the device            */
+} p4a_batch_usage;
+int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out);
+int p4a_batch_destroy(p4a_batch* b);
+const char* p4a_batch_last_error(const p4a_batch* b);
+int p4a_batch_set_stream(p4a_batch* b, void* stream);
+/* Admit a scene (reset() of the reference on an explicit scene / on params).
+ * P4A_ERR_CAPACITY when an arena has no room: nothing is allocated then. */
+int p4a_batch_add_scene(p4a_batch* b, const p4a_params* params, const p4a_scene_desc* scene,
+                        int32_t* scene_id);
+int p4a_batch_add_preset(p4a_batch* b, const p4a_params* params, int32_t* scene_id);
+int p4a_batch_remove_scene(p4a_batch* b, int32_t scene_id);
+/* Advance each listed scene by frame_dt (its own time bank and substeps). */
+int p4a_batch_step(p4a_batch* b, const int32_t* scene_ids, int32_t count, double frame_dt);
+int p4a_batch_synchronize(p4a_batch* b);
+int p4a_batch_usage_get(const p4a_batch* b, p4a_batch_usage* out);
+/* Per-scene views, as p4a_get_info / p4a_read / p4a_get_stats (which = P4A_LIVE,
+ * P4A_A or P4A_B; the stats wait for the scene's last step). */
+int p4a_batch_scene_info(p4a_batch* b, int32_t scene_id, p4a_info* out);
+int p4a_batch_read(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which, void* host,
+                   size_t offset, size_t bytes);
+int p4a_batch_write(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which, const void* host,
+                    size_t offset, size_t bytes);
+int p4a_batch_stats(p4a_batch* b, int32_t scene_id, p4a_stats* out);
+/* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
+int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
+
 /* ---- operator entry: predict + grid pass as one call ------------------- */
 /*
  * The predict pass and the 'grid' pass of Sim.step (src/wgsl.js:56-70,

@@ -7,6 +7,7 @@ scenes.
 """
 from ._lib import P4AError, device_available, lib  # noqa: F401
 from .params import PRESETS, default_aniso, default_params  # noqa: F401
+from .batch import Batch  # noqa: F401
 from .sim import Sim  # noqa: F401
 
-__all__ = ["Sim", "default_params", "default_aniso", "PRESETS", "P4AError", "device_available", "lib"]
+__all__ = ["Sim", "Batch", "default_params", "default_aniso", "PRESETS", "P4AError", "device_available", "lib"]

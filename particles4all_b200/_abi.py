@@ -91,6 +91,17 @@ class PhaseTime(C.Structure):
     _fields_ = [("name", C.c_char * 24), ("ms", C.c_double), ("launches", C.c_int64)]
 
 
+class BatchConfig(C.Structure):
+    _fields_ = [("max_particles", C.c_int64), ("max_cells", C.c_int64), ("max_boundary", C.c_int64),
+                ("max_scenes", C.c_int32), ("max_bodies", C.c_int32), ("max_body_parts", C.c_int64)]
+
+
+class BatchUsage(C.Structure):
+    _fields_ = [("free_particles", C.c_int64), ("free_cells", C.c_int64), ("free_boundary", C.c_int64),
+                ("free_body_parts", C.c_int64), ("free_scenes", C.c_int32), ("free_bodies", C.c_int32),
+                ("live_scenes", C.c_int32), ("device_bytes", C.c_int64)]
+
+
 def info_dict(info):
     d = {k: getattr(info, k) for k, _ in Info._fields_}
     d["grid_dim"] = list(info.grid_dim)

@@ -43,6 +43,21 @@ SIGNATURES = {
     "p4a_profile_read": ([_vp, _vp, _i32, C.POINTER(_i32)], C.c_int),
     "p4a_kernel_launches": ([], C.c_uint64),
     "p4a_grid_sort_noalloc": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp], C.c_int),
+    "p4a_batch_create": ([C.c_int, _vp, C.POINTER(_vp)], C.c_int),
+    "p4a_batch_destroy": ([_vp], C.c_int),
+    "p4a_batch_last_error": ([_vp], C.c_char_p),
+    "p4a_batch_set_stream": ([_vp, _vp], C.c_int),
+    "p4a_batch_add_scene": ([_vp, _vp, _vp, C.POINTER(_i32)], C.c_int),
+    "p4a_batch_add_preset": ([_vp, _vp, C.POINTER(_i32)], C.c_int),
+    "p4a_batch_remove_scene": ([_vp, _i32], C.c_int),
+    "p4a_batch_step": ([_vp, _vp, _i32, _dbl], C.c_int),
+    "p4a_batch_synchronize": ([_vp], C.c_int),
+    "p4a_batch_usage_get": ([_vp, _vp], C.c_int),
+    "p4a_batch_scene_info": ([_vp, _i32, _vp], C.c_int),
+    "p4a_batch_read": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_batch_write": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_batch_stats": ([_vp, _i32, _vp], C.c_int),
+    "p4a_batch_use_graphs": ([_vp, _i32], C.c_int),
 }
 
 _lib = None

@@ -215,6 +215,14 @@ void pack_params(p4a_sim* s, double dt) {
   F.tension = (float)p.surface_tension_k;
   F.cohes = (float)(32 / (kPi * std::pow(h, 9)));
   F.cohesTerm = (float)(std::pow(h, 6) / 64);
+  F.pOff = 0;
+  F.pEnd = (uint32_t)s->n;
+  F.cOff = 0;
+  F.bOff = 0;
+  F.parity = (uint32_t)s->parity;
+  F.iters = (uint32_t)std::max(1, p.iterations);
+  F.subs = 1;
+  F.slot = 0;
 }
 
 uint32_t next_epoch(p4a_sim* s) {
@@ -255,21 +263,18 @@ int upload_boundary(p4a_sim* s) {
 
 // The grid pass at parity `par` into parity par^1 (src/sim.js:473-492).
 void grid_pass(p4a_sim* s, int par) {
-  const int q = par ^ 1;
   DevScene& d = s->d;
   cudaStream_t st = s->stream;
+  s->P.parity = (uint32_t)par;
   mark(s, PH_KEY_COUNT);
-  launch_key_count(s->P, d.pos[par], d.vel[par], d.key, d.rank, d.cellCount,
-                   s->nBodies ? d.bodyFill : nullptr, (uint32_t)s->nBodies, st);
+  launch_key_count(s->P, d, st);
   mark(s, PH_SCAN);
   launch_scan(d.cellCount, d.cellStart, s->nCells, d.scanState, d.scanTicket, next_epoch(s),
               d.errorWord, st);
   mark(s, PH_FILL);
-  launch_fill((uint32_t)s->n, d.key, d.rank, d.cellStart, d.unordered, st);
+  launch_fill(s->P, d, st);
   mark(s, PH_REORDER);
-  launch_reorder(s->P, d.key, d.cellStart, d.unordered, d.pos[par], d.vel[par], d.body[par],
-                 d.rest[par], d.pos[q], d.vel[q], d.pred[q], d.body[q], d.rest[q], nullptr,
-                 s->nBodies ? d.bodyStart : nullptr, d.bodyFill, s->nBodies ? d.bodyList : nullptr, st);
+  launch_reorder(s->P, d, st);
 }
 
 int reset_common(p4a_sim* s) {
@@ -709,40 +714,36 @@ int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
       launch_body_drag(d, d.vel[par], d.body[par], hb, s->bodyStartHost[hb] - s->bodyStartHost[hb - 1],
                        s->bodyStartHost[hb - 1], goal, (float)s->heldRate, blend, (float)s->heldLimit, st);
     }
-    grid_pass(s, par);
+    s->P.subs = (uint32_t)sub;
+    grid_pass(s, par);  // sets P.parity = par: the passes below read parity par ^ 1
     s->parity = q;
     s->predParity = q;
-    int cur = q;
     if (bodies) {
       mark(s, PH_BODY_SEED);
-      launch_body_seed(P, d, d.pred[cur], st);
+      launch_body_seed(P, d, st);
     }
     for (int it = 0; it < iters; it++) {
-      const bool last = it == iters - 1;
       mark(s, PH_LAMBDA);
-      launch_lambda(P, d, d.pred[cur], st);
+      launch_lambda(P, d, it, st);
       mark(s, PH_DELTA);
-      launch_delta(P, d, d.pred[cur], d.pred[cur ^ 1], d.pos[q], last ? d.vel[par] : nullptr, st);
-      cur ^= 1;
+      launch_delta(P, d, it, st);
       if (bodies) {
         mark(s, PH_BODY_MATCH);
-        launch_body_match(P, d, d.pred[cur], d.rest[q], d.pos[q], last ? d.vel[par] : nullptr, st);
+        launch_body_match(P, d, it, st);
       }
     }
-    float4* predCopy = cur != q ? d.pred[q] : nullptr;
-    const bool statsNow = step == sub - 1;
-    if (statsNow) {
+    if (step == sub - 1) {
       mark(s, PH_STATS_CLEAR);
       CUDA_TRY(s, cudaMemsetAsync(d.statsOut, 0, 32, st));
     }
     if (tension) {
       mark(s, PH_XSPH_NORMALS);
-      launch_xsph_normals(P, d, d.pred[cur], d.vel[par], st);
+      launch_xsph_normals(P, d, st);
       mark(s, PH_TENSION_FINALIZE);
-      launch_tension_finalize(P, d, d.pred[cur], d.vel[par], d.pos[q], d.vel[q], predCopy, statsNow, st);
+      launch_tension_finalize(P, d, step, st);
     } else {
       mark(s, PH_XSPH_FINALIZE);
-      launch_xsph_finalize(P, d, d.pred[cur], d.vel[par], d.pos[q], d.vel[q], predCopy, statsNow, st);
+      launch_xsph_finalize(P, d, step, st);
     }
     s->simTime += dt;
   }
@@ -1079,22 +1080,11 @@ int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, cons
   uint32_t* errw = (uint32_t*)w;
   const size_t zeroBytes = (size_t)((char*)errw + 4 - (char*)cellCount);
   if (cudaMemsetAsync(cellCount, 0, zeroBytes, st) != cudaSuccess) return P4A_ERR_CUDA;
-  SimParams P{};
-  for (int k = 0; k < 3; k++) { P.boxMin[k] = grid->box_min[k]; P.gridDim[k] = grid->dim[k]; }
-  P.h = grid->h;
-  P.dt = dt;
-  P.gravity = gravity;
-  P.n = (uint32_t)n;
-  P.nCells = (uint32_t)nCells;
   g_launches.fetch_add(4, std::memory_order_relaxed);
-  launch_key_count(P, (const float4*)pos, (const float4*)vel, key, rank, cellCount, nullptr, 0, st);
-  launch_scan(cellCount, cell_start, nCells, state, ticket, 1u, errw, st);
-  launch_fill((uint32_t)n, key, rank, cell_start, unordered, st);
-  launch_reorder(P, key, cell_start, unordered, (const float4*)pos, (const float4*)vel,
-                 (const uint4*)body, (const float4*)rest, (float4*)pos_out, (float4*)vel_out,
-                 (float4*)pred_out, (uint4*)body_out, (float4*)rest_out, slot_out, nullptr, nullptr,
-                 nullptr, st);
-  return cudaGetLastError() == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+  const cudaError_t e = run_grid_sort(*grid, n, dt, gravity, pos, vel, body, rest, pos_out, vel_out,
+                                      pred_out, body_out, rest_out, cell_start, slot_out, key, rank,
+                                      unordered, cellCount, state, ticket, errw, st);
+  return e == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
 }
 
 }  // extern "C"

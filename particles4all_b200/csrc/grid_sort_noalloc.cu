@@ -95,23 +95,8 @@ extern "C" int p4a_grid_sort_noalloc(const p4a_grid* grid, int32_t n, float dt, 
   cudaStream_t st = (cudaStream_t)stream;
   // histogram, tile states, ticket and error word start at zero on every call
   if (cudaMemsetAsync(cellCount, 0, kScratchBytes - kOffCount, st) != cudaSuccess) return P4A_ERR_CUDA;
-  const int nCells = (int)cells;
-  SimParams P{};
-  for (int k = 0; k < 3; k++) {
-    P.boxMin[k] = grid->box_min[k];
-    P.gridDim[k] = grid->dim[k];
-  }
-  P.h = grid->h;
-  P.dt = dt;
-  P.gravity = gravity;
-  P.n = (uint32_t)n;
-  P.nCells = (uint32_t)nCells;
-  launch_key_count(P, (const float4*)pos, (const float4*)vel, key, rank, cellCount, nullptr, 0, st);
-  launch_scan(cellCount, cell_start, nCells, state, ticket, 1u, errw, st);
-  launch_fill((uint32_t)n, key, rank, cell_start, unordered, st);
-  launch_reorder(P, key, cell_start, unordered, (const float4*)pos, (const float4*)vel,
-                 (const uint4*)body, (const float4*)rest, (float4*)pos_out, (float4*)vel_out,
-                 (float4*)pred_out, (uint4*)body_out, (float4*)rest_out, slot_out, nullptr, nullptr,
-                 nullptr, st);
-  return cudaGetLastError() == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+  const cudaError_t e = run_grid_sort(*grid, n, dt, gravity, pos, vel, body, rest, pos_out, vel_out,
+                                      pred_out, body_out, rest_out, cell_start, slot_out, key, rank,
+                                      unordered, cellCount, state, ticket, errw, st);
+  return e == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
 }

@@ -12,10 +12,14 @@
 // thread with the reference's float order.
 // The per-body particle lists are rebuilt by the reorder of every sort
 // (bodyList[bodyStart[b] + k]), replacing the reference's global atomic compaction.
+// A work item is a body: plain launches use block b = body b of the one scene,
+// batched launches read (scene slot, body) pairs; body arrays are indexed at
+// P.bOff + b.
 #include <cuda_runtime.h>
 
 #include "p4a_internal.h"
 #include "p4a_math.cuh"
+#include "pass_common.cuh"
 
 namespace p4a {
 
@@ -61,31 +65,27 @@ __device__ __forceinline__ void centre_sums(const SimParams& P, const float4* __
   block_sum_u32<3>(a, s_scratch, s_acc);
 }
 
-__global__ void __launch_bounds__(kBodyBlock) k_body_seed(
-    const __grid_constant__ SimParams P, const float4* __restrict__ pred,
-    const uint32_t* __restrict__ bodyStart, const uint32_t* __restrict__ bodyList,
-    int32_t* __restrict__ bodyAccum, int32_t* __restrict__ bodyCov,
-    float4* __restrict__ bodyCentre, float4* __restrict__ bodyRef) {
+__device__ __forceinline__ void body_seed_body(const SimParams& P, const DevScene& d, uint32_t b) {
   __shared__ uint32_t s_scratch[(kBodyBlock / 32) * 9];
   __shared__ uint32_t s_acc[9];
-  const uint32_t b = blockIdx.x;
-  const uint32_t start = bodyStart[b], count = bodyStart[b + 1] - start;
-  const F3 centre = xyz(bodyCentre[b]);
-  centre_sums(P, pred, bodyList + start, count, centre, s_scratch, s_acc);
+  const uint32_t gb = P.bOff + b;
+  const float4* __restrict__ pred = d.pred[(int)P.parity ^ 1];
+  const uint32_t start = d.bodyStart[gb], count = d.bodyStart[gb + 1] - start;
+  const F3 centre = xyz(d.bodyCentre[gb]);
+  centre_sums(P, pred, d.bodyList + start, count, centre, s_scratch, s_acc);
   if (threadIdx.x == 0) {
     const int32_t ax = (int32_t)s_acc[0], ay = (int32_t)s_acc[1], az = (int32_t)s_acc[2];
-    bodyAccum[b * 4 + 0] = ax; bodyAccum[b * 4 + 1] = ay; bodyAccum[b * 4 + 2] = az;
-    bodyAccum[b * 4 + 3] = (int32_t)count;
+    d.bodyAccum[gb * 4 + 0] = ax; d.bodyAccum[gb * 4 + 1] = ay; d.bodyAccum[gb * 4 + 2] = az;
+    d.bodyAccum[gb * 4 + 3] = (int32_t)count;
 #pragma unroll
-    for (int k = 0; k < 9; k++) bodyCov[b * 9 + k] = 0;
+    for (int k = 0; k < 9; k++) d.bodyCov[gb * 9 + k] = 0;
     const float cnt = (float)(int32_t)count;
     if (cnt > 0.0f) {
       const float den = P.bodyScale * cnt;
-      const float4 r = make_float4(centre.x + (float)ax / den, centre.y + (float)ay / den,
-                                   centre.z + (float)az / den, 0.0f);
-      bodyRef[b] = r;
+      d.bodyRef[gb] = make_float4(centre.x + (float)ax / den, centre.y + (float)ay / den,
+                                  centre.z + (float)az / den, 0.0f);
     }
-    bodyCentre[b] = bodyRef[b];
+    d.bodyCentre[gb] = d.bodyRef[gb];
   }
 }
 
@@ -93,38 +93,34 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_seed(
 __device__ __forceinline__ M3 inverse_transposed(const M3& m) {
   const F3 a = m.c[0], b = m.c[1], c = m.c[2];
   const F3 r0 = cross3(b, c), r1 = cross3(c, a), r2 = cross3(a, b);
-  const float d = dot3(a, r0);
-  const float invd = fabsf(d) > 1.0e-20f ? 1.0f / d : 0.0f;
+  const float det = dot3(a, r0);
+  const float invd = fabsf(det) > 1.0e-20f ? 1.0f / det : 0.0f;
   return {{mul3(r0, invd), mul3(r1, invd), mul3(r2, invd)}};
 }
 
-__global__ void __launch_bounds__(kBodyBlock) k_body_match(
-    const __grid_constant__ SimParams P, float4* __restrict__ pred,
-    const float4* __restrict__ rest, const uint32_t* __restrict__ bodyStart,
-    const uint32_t* __restrict__ bodyList, int32_t* __restrict__ bodyAccum,
-    int32_t* __restrict__ bodyCov, float4* __restrict__ bodyCentre,
-    float4* __restrict__ bodyRef, float4* __restrict__ bodyRot,
-    const float4* __restrict__ bodyInfo, const float4* __restrict__ posLive,
-    float4* __restrict__ velScratch) {
+__device__ __forceinline__ void body_match_body(const SimParams& P, const DevScene& d, uint32_t b, int it) {
   __shared__ uint32_t s_scratch[(kBodyBlock / 32) * 9];
   __shared__ uint32_t s_acc[9];
   __shared__ float s_ref[3];
   __shared__ float s_pose[12];  // centre xyz, rows of R
-  const uint32_t b = blockIdx.x;
-  const uint32_t start = bodyStart[b], count = bodyStart[b + 1] - start;
-  const uint32_t* list = bodyList + start;
-  const F3 centre = xyz(bodyCentre[b]);
+  const int L = (int)P.parity ^ 1;
+  float4* __restrict__ pred = d.pred[L ^ ((it + 1) & 1)];
+  const float4* __restrict__ rest = d.rest[L];
+  const uint32_t gb = P.bOff + b;
+  const uint32_t start = d.bodyStart[gb], count = d.bodyStart[gb + 1] - start;
+  const uint32_t* list = d.bodyList + start;
+  const F3 centre = xyz(d.bodyCentre[gb]);
   // bodyClear + bodyCentre
   centre_sums(P, pred, list, count, centre, s_scratch, s_acc);
   const int32_t ax = (int32_t)s_acc[0], ay = (int32_t)s_acc[1], az = (int32_t)s_acc[2];
   const float cnt = (float)(int32_t)count;
   // bodySeed: bodyRef = bodyCentre + mean offset
   if (threadIdx.x == 0) {
-    F3 r = xyz(bodyRef[b]);
+    F3 r = xyz(d.bodyRef[gb]);
     if (cnt > 0.0f) {
       const float den = P.bodyScale * cnt;
       r = {centre.x + (float)ax / den, centre.y + (float)ay / den, centre.z + (float)az / den};
-      bodyRef[b] = make_float4(r.x, r.y, r.z, 0.0f);
+      d.bodyRef[gb] = make_float4(r.x, r.y, r.z, 0.0f);
     }
     s_ref[0] = r.x; s_ref[1] = r.y; s_ref[2] = r.z;
   }
@@ -149,21 +145,21 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
   block_sum_u32<9>(cv, s_scratch, s_acc);
   // bodyResolve on one thread
   if (threadIdx.x == 0) {
-    bodyAccum[b * 4 + 0] = ax; bodyAccum[b * 4 + 1] = ay; bodyAccum[b * 4 + 2] = az;
-    bodyAccum[b * 4 + 3] = (int32_t)count;
+    d.bodyAccum[gb * 4 + 0] = ax; d.bodyAccum[gb * 4 + 1] = ay; d.bodyAccum[gb * 4 + 2] = az;
+    d.bodyAccum[gb * 4 + 3] = (int32_t)count;
     int32_t c9[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) { c9[k] = (int32_t)s_acc[k]; bodyCov[b * 9 + k] = c9[k]; }
+    for (int k = 0; k < 9; k++) { c9[k] = (int32_t)s_acc[k]; d.bodyCov[gb * 9 + k] = c9[k]; }
     F3 cen = centre;
     float rows[9];
     bool wrote = false;
     if (cnt > 0.0f) {
       const float den = P.bodyScale * cnt;
       F3 delta = {(float)ax / den, (float)ay / den, (float)az / den};
-      const float invRatio = bodyInfo[b].x;
+      const float invRatio = d.bodyInfo[gb].x;
       if (invRatio > 0.0f) delta = mul3(delta, invRatio);
       cen = {centre.x + delta.x, centre.y + delta.y, centre.z + delta.z};
-      bodyCentre[b] = make_float4(cen.x, cen.y, cen.z, 0.0f);
+      d.bodyCentre[gb] = make_float4(cen.x, cen.y, cen.z, 0.0f);
       M3 A = {{{(float)c9[0], (float)c9[1], (float)c9[2]},
                {(float)c9[3], (float)c9[4], (float)c9[5]},
                {(float)c9[6], (float)c9[7], (float)c9[8]}}};
@@ -173,7 +169,7 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
       const float s = cbrt_newton(fabsf(det));
       if (s > 1.0e-6f) A = scale3(A, 1.0f / s);
       M3 R = A;
-      for (int it = 0; it < 8; it++) {
+      for (int k = 0; k < 8; k++) {
         const M3 inv = inverse_transposed(R);
         M3 next;
 #pragma unroll
@@ -186,7 +182,7 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
 #pragma unroll
       for (int r = 0; r < 3; r++) {
         const F3 row = row3(R, r);
-        bodyRot[b * 3 + r] = make_float4(row.x, row.y, row.z, 0.0f);
+        d.bodyRot[gb * 3 + r] = make_float4(row.x, row.y, row.z, 0.0f);
         rows[r * 3 + 0] = row.x; rows[r * 3 + 1] = row.y; rows[r * 3 + 2] = row.z;
       }
       wrote = true;
@@ -194,7 +190,7 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
     if (!wrote) {
 #pragma unroll
       for (int r = 0; r < 3; r++) {
-        const float4 row = bodyRot[b * 3 + r];
+        const float4 row = d.bodyRot[gb * 3 + r];
         rows[r * 3 + 0] = row.x; rows[r * 3 + 1] = row.y; rows[r * 3 + 2] = row.z;
       }
     }
@@ -204,6 +200,7 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
   }
   __syncthreads();
   // bodyProject (+ velFromPos of the body particles on the last iteration)
+  const bool last = it == (int)P.iters - 1;
   const F3 cen = {s_pose[0], s_pose[1], s_pose[2]};
   const F3 r0 = {s_pose[3], s_pose[4], s_pose[5]}, r1 = {s_pose[6], s_pose[7], s_pose[8]},
            r2 = {s_pose[9], s_pose[10], s_pose[11]};
@@ -213,12 +210,33 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_match(
     const F3 p = {dot3(r0, q), dot3(r1, q), dot3(r2, q)};
     const F3 o = add3(cen, p);
     pred[i] = make_float4(o.x, o.y, o.z, 1.0f);
-    if (velScratch) {
-      const float4 p0 = __ldg(&posLive[i]);
-      velScratch[i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,
-                                  (o.z - p0.z) * P.invDt, 0.0f);
+    if (last) {
+      const float4 p0 = __ldg(&d.pos[L][i]);
+      d.vel[L ^ 1][i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,
+                                    (o.z - p0.z) * P.invDt, 0.0f);
     }
   }
+}
+
+__global__ void __launch_bounds__(kBodyBlock) k_body_seed(const __grid_constant__ SimParams P,
+                                                          const __grid_constant__ DevScene d) {
+  body_seed_body(P, d, blockIdx.x);
+}
+__global__ void __launch_bounds__(kBodyBlock) k_body_seed_b(const __grid_constant__ BatchWork w,
+                                                            const __grid_constant__ DevScene d) {
+  uint32_t b;
+  const SimParams& P = batch_scene(w, b);
+  body_seed_body(P, d, b);
+}
+__global__ void __launch_bounds__(kBodyBlock) k_body_match(const __grid_constant__ SimParams P,
+                                                           const __grid_constant__ DevScene d, int it) {
+  body_match_body(P, d, blockIdx.x, it);
+}
+__global__ void __launch_bounds__(kBodyBlock) k_body_match_b(const __grid_constant__ BatchWork w,
+                                                             const __grid_constant__ DevScene d, int it) {
+  uint32_t b;
+  const SimParams& P = batch_scene(w, b);
+  body_match_body(P, d, b, it);
 }
 
 // bodyDrag (src/wgsl.js:187-214) over the held body's particle list.
@@ -243,18 +261,19 @@ __global__ void __launch_bounds__(kBlock) k_body_drag(float4* __restrict__ vel,
   vel[i] = make_float4(v.x + dv.x, v.y + dv.y, v.z + dv.z, v4.w);
 }
 
-void launch_body_seed(const SimParams& P, const DevScene& d, const float4* pred, cudaStream_t st) {
+void launch_body_seed(const SimParams& P, const DevScene& d, cudaStream_t st) {
   if (P.nBodies == 0) return;
-  k_body_seed<<<P.nBodies, kBodyBlock, 0, st>>>(P, pred, d.bodyStart, d.bodyList, d.bodyAccum,
-                                                d.bodyCov, d.bodyCentre, d.bodyRef);
+  k_body_seed<<<P.nBodies, kBodyBlock, 0, st>>>(P, d);
 }
-
-void launch_body_match(const SimParams& P, const DevScene& d, float4* pred, const float4* rest,
-                       const float4* posLive, float4* velScratch, cudaStream_t st) {
+void launch_body_match(const SimParams& P, const DevScene& d, int it, cudaStream_t st) {
   if (P.nBodies == 0) return;
-  k_body_match<<<P.nBodies, kBodyBlock, 0, st>>>(P, pred, rest, d.bodyStart, d.bodyList,
-                                                 d.bodyAccum, d.bodyCov, d.bodyCentre, d.bodyRef,
-                                                 d.bodyRot, d.bodyInfo, posLive, velScratch);
+  k_body_match<<<P.nBodies, kBodyBlock, 0, st>>>(P, d, it);
+}
+void launch_body_seed_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
+  if (nItems > 0) k_body_seed_b<<<nItems, kBodyBlock, 0, st>>>(w, d);
+}
+void launch_body_match_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st) {
+  if (nItems > 0) k_body_match_b<<<nItems, kBodyBlock, 0, st>>>(w, d, it);
 }
 
 void launch_body_drag(const DevScene& d, float4* vel, const uint4* body, uint32_t held,

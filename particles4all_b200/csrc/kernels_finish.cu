@@ -8,15 +8,17 @@
 //   stats      src/wgsl.js:785-832, fused into the last substep's finalize with
 //              the reference's 256-particle workgroup trees, so the fixed-point
 //              totals are the same bits
-// The velFromPos velocities live in a scratch buffer (the non-live vel copy), so
-// the final velocity can be written to the live copy while neighbours still read
-// the scratch one. xsph+normals builds the neighbour masks (neighbours.cuh) and
+// With L = P.parity ^ 1 the live copy after the sort, the final positions are in
+// pred[L ^ (iters & 1)]; the velFromPos velocities are in the non-live copy
+// vel[L ^ 1], so the final velocity can be written to vel[L] while neighbours still
+// read the other one. xsph+normals builds the neighbour masks (neighbours.cuh) and
 // stores them for the tension pass, which walks the same positions.
 #include <cuda_runtime.h>
 
 #include "neighbours.cuh"
 #include "p4a_internal.h"
 #include "p4a_math.cuh"
+#include "pass_common.cuh"
 
 namespace p4a {
 
@@ -47,38 +49,40 @@ __device__ __forceinline__ void block_stats(const SimParams& P, bool act, float 
     __syncthreads();
   }
   if (t < 32) {
-    float a = sR[t], b = sM[t], c = sV[t], d = sK[t];
+    float a = sR[t], b = sM[t], c = sV[t], e = sK[t];
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       a = a + __shfl_down_sync(0xffffffffu, a, off);
       b = fmaxf(b, __shfl_down_sync(0xffffffffu, b, off));
       c = fmaxf(c, __shfl_down_sync(0xffffffffu, c, off));
-      d = d + __shfl_down_sync(0xffffffffu, d, off);
+      e = e + __shfl_down_sync(0xffffffffu, e, off);
     }
     if (t == 0) {
       atomicAdd(&out[0], __float2uint_rz(a * 1024.0f));
       atomicMax(&out[1], __float2uint_rz(b * 1024.0f));
       atomicMax(&out[2], __float2uint_rz(c * 1024.0f));
-      atomicAdd(&out[3], __float2uint_rz(d * 1024.0f));
+      atomicAdd(&out[3], __float2uint_rz(e * 1024.0f));
     }
   }
 }
 
-// xsph (+ finalize) for scenes without surface tension.
-__global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(
-    const __grid_constant__ SimParams P, const float4* __restrict__ pred,
-    const float4* __restrict__ velIn, const float* __restrict__ density,
-    const uint32_t* __restrict__ cs, float4* __restrict__ posOut, float4* __restrict__ velOut,
-    float4* __restrict__ predCopy, uint32_t* __restrict__ statsOut) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  const bool act = i < P.n;
+// xsph (+ finalize) for scenes without surface tension. All threads reach the
+// stats tree, so there is no early return.
+__device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const DevScene& d, uint32_t tile,
+                                                   int substep) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  const bool act = li < P.n;
+  const uint32_t i = P.pOff + li;
+  const int L = (int)P.parity ^ 1;
+  const float4* __restrict__ pred = d.pred[L ^ ((int)P.iters & 1)];
+  const float4* __restrict__ velIn = d.vel[L ^ 1];
+  const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
   F3 vf = {0.f, 0.f, 0.f};
   float rhoi = 0.0f;
   if (act) {
     const float4 p4 = __ldg(&pred[i]);
     const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
     const RowWalk w(P, pi);
-    uint32_t longRows = 0u;
     F3 acc = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int r = 0; r < kRows; r++) {
@@ -90,28 +94,30 @@ __global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(
         if (j == i) return;
         const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
         const float r2 = dot3(rij, rij);
-        const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
+        const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
         acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
       });
     }
     const F3 corr = mul3(acc, P.xsphC);
     vf = add3(vi, corr);
-    velOut[i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
-    posOut[i] = p4;
-    if (predCopy) predCopy[i] = p4;
-    rhoi = __ldg(&density[i]);
+    d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+    d.pos[L][i] = p4;
+    if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
+    rhoi = __ldg(&d.density[i]);
   }
-  if (statsOut) block_stats(P, act, rhoi, vf, statsOut);
+  if (substep == (int)P.subs - 1) block_stats(P, act, rhoi, vf, d.statsOut + 8 * P.slot);
 }
 
 // xsph + normals (tension scenes): corr = xsphC * acc, normal = h * nacc.
-__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(
-    const __grid_constant__ SimParams P, const float4* __restrict__ pred,
-    const float4* __restrict__ velIn, const float* __restrict__ density,
-    const uint32_t* __restrict__ cs, float4* __restrict__ corrOut, float4* __restrict__ normalOut,
-    uint64_t* __restrict__ masks, uint32_t* __restrict__ longs, uint32_t cap) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= P.n) return;
+__device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevScene& d, uint32_t tile) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  if (li >= P.n) return;
+  const uint32_t i = P.pOff + li;
+  const int L = (int)P.parity ^ 1;
+  const float4* __restrict__ pred = d.pred[L ^ ((int)P.iters & 1)];
+  const float4* __restrict__ velIn = d.vel[L ^ 1];
+  const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
+  const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i])), vi = xyz(__ldg(&velIn[i]));
   const RowWalk w(P, pi);
   uint32_t longRows = 0u;
@@ -122,13 +128,13 @@ __global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(
     if (rb < 0) continue;
     bool lg;
     const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
-    masks[(size_t)r * cap + i] = mr;
+    d.nbMask[(size_t)r * cap + i] = mr;
     if (lg) longRows |= 1u << r;
     visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
       if (j == i) return;
       const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
       const float r2 = dot3(rij, rij);
-      const float dj = fmaxf(__ldg(&density[j]), 0.5f * P.rho0);
+      const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
       const float f = P.mass * poly6(P, r2) / dj;
       acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
       if (r2 < 1.0e-12f) return;
@@ -138,35 +144,35 @@ __global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(
       nacc = fma3(coef, rij, nacc);
     });
   }
-  longs[i] = longRows;
-  corrOut[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
-  normalOut[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
+  d.nbLong[i] = longRows;
+  d.corr[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
+  d.normal[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
 }
 
 // tension + finalize.
-__global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(
-    const __grid_constant__ SimParams P, const float4* __restrict__ pred,
-    const float4* __restrict__ velIn, const float* __restrict__ density,
-    const float4* __restrict__ normal, float4* __restrict__ corr, const uint32_t* __restrict__ cs,
-    float4* __restrict__ posOut, float4* __restrict__ velOut, float4* __restrict__ predCopy,
-    uint32_t* __restrict__ statsOut, const uint64_t* __restrict__ masks,
-    const uint32_t* __restrict__ longs, uint32_t cap) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  const bool act = i < P.n;
+__device__ __forceinline__ void tension_finalize_body(const SimParams& P, const DevScene& d,
+                                                      uint32_t tile, int substep) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  const bool act = li < P.n;
+  const uint32_t i = P.pOff + li;
+  const int L = (int)P.parity ^ 1;
+  const float4* __restrict__ pred = d.pred[L ^ ((int)P.iters & 1)];
+  const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
+  const uint32_t cap = d.cap;
   F3 vf = {0.f, 0.f, 0.f};
   float rhoi = 0.0f;
   if (act) {
     const float4 p4 = __ldg(&pred[i]);
-    const F3 pi = xyz(p4), ni = xyz(__ldg(&normal[i]));
-    rhoi = __ldg(&density[i]);
+    const F3 pi = xyz(p4), ni = xyz(__ldg(&d.normal[i]));
+    rhoi = __ldg(&d.density[i]);
     const RowWalk w(P, pi);
-    const uint32_t longRows = __ldg(&longs[i]);
+    const uint32_t longRows = __ldg(&d.nbLong[i]);
     F3 acc = {0.f, 0.f, 0.f};
 #pragma unroll
     for (int r = 0; r < kRows; r++) {
       const int rb = w.row_base(P, r);
       if (rb < 0) continue;
-      const uint64_t mr = __ldg(&masks[(size_t)r * cap + i]);
+      const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
       visit_row(P, w, rb, pi, mr, (longRows >> r) & 1u, pred, cs, [&](uint32_t j) {
         const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
         const float r2 = dot3(rij, rij);
@@ -178,43 +184,76 @@ __global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(
         if (2.0f * rr > P.h) cw = P.cohes * k;
         const float sCoh = -P.tension * P.mass * cw / rr;
         const F3 fCoh = mul3(rij, sCoh);
-        const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&normal[j]))), -P.tension);
-        const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&density[j]));
+        const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
+        const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&d.density[j]));
         acc = fma3(wgt, add3(fCoh, fCurv), acc);
       });
     }
-    const float4 c0 = corr[i];
+    const float4 c0 = d.corr[i];
     const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
-    corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);
-    const F3 vi = xyz(__ldg(&velIn[i]));
+    d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);
+    const F3 vi = xyz(__ldg(&d.vel[L ^ 1][i]));
     vf = add3(vi, cf);
-    velOut[i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
-    posOut[i] = p4;
-    if (predCopy) predCopy[i] = p4;
+    d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+    d.pos[L][i] = p4;
+    if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
   }
-  if (statsOut) block_stats(P, act, rhoi, vf, statsOut);
+  if (substep == (int)P.subs - 1) block_stats(P, act, rhoi, vf, d.statsOut + 8 * P.slot);
 }
 
-void launch_xsph_finalize(const SimParams& P, const DevScene& d, const float4* pred,
-                          const float4* velIn, float4* posOut, float4* velOut, float4* predCopy,
-                          bool stats, cudaStream_t st) {
-  k_xsph_finalize<<<groups(P.n), kBlock, 0, st>>>(P, pred, velIn, d.density, d.cellStart, posOut,
-                                                  velOut, predCopy, stats ? d.statsOut : nullptr);
+__global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(const __grid_constant__ SimParams P,
+                                                             const __grid_constant__ DevScene d,
+                                                             int substep) {
+  xsph_finalize_body(P, d, blockIdx.x, substep);
+}
+__global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize_b(const __grid_constant__ BatchWork w,
+                                                               const __grid_constant__ DevScene d,
+                                                               int substep) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  xsph_finalize_body(P, d, t, substep);
+}
+__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(const __grid_constant__ SimParams P,
+                                                            const __grid_constant__ DevScene d) {
+  xsph_normals_body(P, d, blockIdx.x);
+}
+__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals_b(const __grid_constant__ BatchWork w,
+                                                              const __grid_constant__ DevScene d) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  xsph_normals_body(P, d, t);
+}
+__global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(const __grid_constant__ SimParams P,
+                                                                const __grid_constant__ DevScene d,
+                                                                int substep) {
+  tension_finalize_body(P, d, blockIdx.x, substep);
+}
+__global__ void __launch_bounds__(kBlock, 5) k_tension_finalize_b(const __grid_constant__ BatchWork w,
+                                                                  const __grid_constant__ DevScene d,
+                                                                  int substep) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  tension_finalize_body(P, d, t, substep);
 }
 
-void launch_xsph_normals(const SimParams& P, const DevScene& d, const float4* pred,
-                         const float4* velIn, cudaStream_t st) {
-  k_xsph_normals<<<groups(P.n), kBlock, 0, st>>>(P, pred, velIn, d.density, d.cellStart, d.corr,
-                                                 d.normal, d.nbMask, d.nbLong, d.cap);
+void launch_xsph_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st) {
+  k_xsph_finalize<<<groups(P.n), kBlock, 0, st>>>(P, d, substep);
 }
-
-void launch_tension_finalize(const SimParams& P, const DevScene& d, const float4* pred,
-                             const float4* velIn, float4* posOut, float4* velOut,
-                             float4* predCopy, bool stats, cudaStream_t st) {
-  k_tension_finalize<<<groups(P.n), kBlock, 0, st>>>(P, pred, velIn, d.density, d.normal, d.corr,
-                                                     d.cellStart, posOut, velOut, predCopy,
-                                                     stats ? d.statsOut : nullptr, d.nbMask,
-                                                     d.nbLong, d.cap);
+void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st) {
+  k_xsph_normals<<<groups(P.n), kBlock, 0, st>>>(P, d);
+}
+void launch_tension_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st) {
+  k_tension_finalize<<<groups(P.n), kBlock, 0, st>>>(P, d, substep);
+}
+void launch_xsph_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep, cudaStream_t st) {
+  if (nItems > 0) k_xsph_finalize_b<<<nItems, kBlock, 0, st>>>(w, d, substep);
+}
+void launch_xsph_normals_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
+  if (nItems > 0) k_xsph_normals_b<<<nItems, kBlock, 0, st>>>(w, d);
+}
+void launch_tension_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep,
+                               cudaStream_t st) {
+  if (nItems > 0) k_tension_finalize_b<<<nItems, kBlock, 0, st>>>(w, d, substep);
 }
 
 }  // namespace p4a

@@ -4,37 +4,35 @@
 //   key_count  predict + cellOf + warp-aggregated atomic histogram; each particle
 //              keeps the arrival rank its warp leader got for it
 //   scan       single-pass decoupled-lookback exclusive scan of the histogram into
-//              cellStart (and zeroes the histogram for the next substep)
+//              cellStart (and zeroes the histogram for the next substep); the
+//              batched form restarts the scan at every scene, seeded with the
+//              scene's first particle index
 //   fill       unordered[cellStart[key] + rank] = i   (a per-cell bucket list)
 //   reorder    stable rank = #{ j in the particle's bucket : j < i }, then the
 //              permutation of pos/vel/pred/body/rest into cell order
 // The reference's scatterSlot takes slots in atomic order (src/wgsl.js:436), so its
 // in-cell order is whatever the hardware produced; here it is the stable order
 // (ties by pre-sort index), which is one of the orders the reference can produce
-// and is the same on every run.
+// and is the same on every run. The pass reads parity P.parity and writes the
+// other parity.
 #include <cuda_runtime.h>
 
 #include "p4a_internal.h"
 #include "p4a_math.cuh"
+#include "pass_common.cuh"
 
 namespace p4a {
 
-__global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ SimParams P,
-                                                      const float4* __restrict__ pos,
-                                                      const float4* __restrict__ vel,
-                                                      uint32_t* __restrict__ key,
-                                                      uint32_t* __restrict__ rank,
-                                                      uint32_t* __restrict__ cellCount,
-                                                      uint32_t* __restrict__ bodyFill,
-                                                      uint32_t nBodies) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (bodyFill && i < nBodies) bodyFill[i] = 0u;
-  const bool act = i < P.n;
+__device__ __forceinline__ void key_count_body(const SimParams& P, const DevScene& d, uint32_t tile) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  if (d.bodyFill && li < P.nBodies) d.bodyFill[P.bOff + li] = 0u;
+  const bool act = li < P.n;
+  const uint32_t i = P.pOff + li;
   uint32_t k = 0xffffffffu;
   if (act) {
     F3 v, pr;
-    predict_one(P, __ldg(&pos[i]), __ldg(&vel[i]), v, pr);
-    k = cell_index(P, cell_of(P, pr));
+    predict_one(P, __ldg(&d.pos[P.parity][i]), __ldg(&d.vel[P.parity][i]), v, pr);
+    k = P.cOff + cell_index(P, cell_of(P, pr));
   }
   const unsigned peers = __match_any_sync(0xffffffffu, k);
   if (act) {
@@ -42,11 +40,82 @@ __global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ Si
     const int leader = __ffs(peers) - 1;
     const uint32_t lt = peers & ((1u << lane) - 1u);
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(&cellCount[k], (uint32_t)__popc(peers));
+    if (lane == leader) base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
-    key[i] = k;
-    rank[i] = base + (uint32_t)__popc(lt);
+    d.key[i] = k;
+    d.rank[i] = base + (uint32_t)__popc(lt);
   }
+}
+
+__device__ __forceinline__ void fill_body(const SimParams& P, const DevScene& d, uint32_t tile) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  if (li >= P.n) return;
+  const uint32_t i = P.pOff + li;
+  const uint32_t at = __ldg(&d.cellStart[d.key[i]]) + d.rank[i];
+  if (at < P.pEnd) d.unordered[at] = i;  // always true after a completed scan
+}
+
+__device__ __forceinline__ void reorder_body(const SimParams& P, const DevScene& d, uint32_t tile) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  if (li >= P.n) return;
+  const uint32_t i = P.pOff + li;
+  const int src = P.parity, dst = P.parity ^ 1;
+  const uint32_t k = d.key[i];
+  // min() keeps every access in bounds even if a scan gave up (error word set)
+  const uint32_t e = min(__ldg(&d.cellStart[k + 1]), P.pEnd);
+  const uint32_t b = min(__ldg(&d.cellStart[k]), e);
+  uint32_t r = 0;
+  for (uint32_t m = b; m < e; m++) r += __ldg(&d.unordered[m]) < i ? 1u : 0u;
+  const uint32_t s = min(b + r, P.pEnd - 1u);
+  const float4 p4 = __ldg(&d.pos[src][i]);
+  F3 v, pr;
+  predict_one(P, p4, __ldg(&d.vel[src][i]), v, pr);
+  d.pos[dst][s] = p4;
+  d.vel[dst][s] = make_float4(v.x, v.y, v.z, 0.0f);
+  d.pred[dst][s] = make_float4(pr.x, pr.y, pr.z, 1.0f);
+  if (d.body[src]) {
+    const uint4 bd = __ldg(&d.body[src][i]);
+    d.body[dst][s] = bd;
+    if (d.bodyList && bd.x != 0u && bd.x <= P.nBodies) {
+      const uint32_t gb = P.bOff + bd.x - 1u;
+      const uint32_t slot = atomicAdd(&d.bodyFill[gb], 1u);
+      const uint32_t at = d.bodyStart[gb] + slot;
+      if (at < d.bodyStart[gb + 1]) d.bodyList[at] = s;
+    }
+  }
+  if (d.rest[src]) d.rest[dst][s] = __ldg(&d.rest[src][i]);
+  if (d.slotOut) d.slotOut[li] = s - P.pOff;
+}
+
+__global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ SimParams P,
+                                                      const __grid_constant__ DevScene d) {
+  key_count_body(P, d, blockIdx.x);
+}
+__global__ void __launch_bounds__(kBlock) k_key_count_b(const __grid_constant__ BatchWork w,
+                                                        const __grid_constant__ DevScene d) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  key_count_body(P, d, t);
+}
+__global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimParams P,
+                                                 const __grid_constant__ DevScene d) {
+  fill_body(P, d, blockIdx.x);
+}
+__global__ void __launch_bounds__(kBlock) k_fill_b(const __grid_constant__ BatchWork w,
+                                                   const __grid_constant__ DevScene d) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  fill_body(P, d, t);
+}
+__global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimParams P,
+                                                    const __grid_constant__ DevScene d) {
+  reorder_body(P, d, blockIdx.x);
+}
+__global__ void __launch_bounds__(kBlock) k_reorder_b(const __grid_constant__ BatchWork w,
+                                                      const __grid_constant__ DevScene d) {
+  uint32_t t;
+  const SimParams& P = batch_scene(w, t);
+  reorder_body(P, d, t);
 }
 
 // Tile status word: epoch (30 bits) | flag (2 bits) | value (32 bits).
@@ -55,36 +124,32 @@ __device__ __forceinline__ unsigned long long pack_state(uint32_t epoch, unsigne
   return ((unsigned long long)epoch << 34) | (flag << 32) | (unsigned long long)v;
 }
 
-__global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCount,
-                                                 uint32_t* __restrict__ cellStart, int nCells,
-                                                 unsigned long long* __restrict__ state,
-                                                 uint32_t* __restrict__ ticket, uint32_t epoch,
-                                                 int nTiles, uint32_t* __restrict__ err) {
-  __shared__ uint32_t s_tile, s_prefix;
+// One scan tile: loads up to kScanTile counts at cells [base, base + kScanTile)
+// clipped to `limit`, zeroes them, and writes the exclusive prefix seeded with
+// the tile's predecessors (lookback down to tile `firstTile`, which is seeded with
+// `seed`). Returns nothing; the last tile of a segment writes the segment total.
+__device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
+                                          uint32_t* __restrict__ cellStart, long long cellBase,
+                                          long long limit, int tile, int firstTile, uint32_t seed,
+                                          bool lastOfSegment, unsigned long long* __restrict__ state,
+                                          uint32_t epoch, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_prefix;
   __shared__ uint32_t s_warp[kBlock / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
-  __syncthreads();
-  const int tile = (int)s_tile;
-  if (tile >= nTiles) {  // only after an earlier launch failed mid-way: never index past the state
-    if (threadIdx.x == 0) atomicOr(err, ERR_SCAN_TIMEOUT);
-    return;
-  }
-  const long long base = (long long)tile * kScanTile + (long long)tid * kScanItems;
+  const long long base = cellBase + (long long)tid * kScanItems;
   uint32_t v[kScanItems];
   uint32_t sum = 0;
 #pragma unroll
   for (int j = 0; j < kScanItems; j++) {
     const long long idx = base + j;
-    v[j] = idx < nCells ? cellCount[idx] : 0u;
+    v[j] = idx < limit ? cellCount[idx] : 0u;
     sum += v[j];
   }
 #pragma unroll
   for (int j = 0; j < kScanItems; j++) {
     const long long idx = base + j;
-    if (idx < nCells) cellCount[idx] = 0u;
+    if (idx < limit) cellCount[idx] = 0u;
   }
-  // block exclusive scan of the per-thread sums
   uint32_t incl = sum;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -94,24 +159,25 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
   if (lane == 31) s_warp[warp] = incl;
   __syncthreads();
   if (warp == 0) {
-    uint32_t w = lane < kBlock / 32 ? s_warp[lane] : 0u;
-    uint32_t wi = w;
+    const uint32_t wv = lane < kBlock / 32 ? s_warp[lane] : 0u;
+    uint32_t wi = wv;
 #pragma unroll
     for (int o = 1; o < kBlock / 32; o <<= 1) {
       const uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
       if (lane >= o) wi += t;
     }
-    if (lane < kBlock / 32) s_warp[lane] = wi - w;  // exclusive warp offsets
+    if (lane < kBlock / 32) s_warp[lane] = wi - wv;  // exclusive warp offsets
     const uint32_t aggregate = __shfl_sync(0xffffffffu, wi, kBlock / 32 - 1);
     if (lane == 0) {
-      uint32_t exclusive = 0;
-      if (tile == 0) {
-        atomicExch(&state[0], pack_state(epoch, kFlagPrefix, aggregate));
+      uint32_t exclusive = seed;
+      if (tile == firstTile) {
+        atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, seed + aggregate));
       } else {
         atomicExch(&state[tile], pack_state(epoch, kFlagAgg, aggregate));
+        exclusive = 0;
         int j = tile - 1;
         uint32_t spins = 0;
-        while (j >= 0) {
+        while (j >= firstTile) {
           const unsigned long long w64 = *((volatile unsigned long long*)&state[j]);
           const uint32_t we = (uint32_t)(w64 >> 34);
           const unsigned long long wf = (w64 >> 32) & 3ull;
@@ -130,10 +196,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
         atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, exclusive + aggregate));
       }
       s_prefix = exclusive;
-      if (tile == nTiles - 1) {
-        cellStart[nCells] = exclusive + aggregate;
-        *ticket = 0u;  // every tile has taken its ticket; reset for the next launch
-      }
+      if (lastOfSegment) cellStart[limit] = exclusive + aggregate;
     }
   }
   __syncthreads();
@@ -141,83 +204,121 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
 #pragma unroll
   for (int j = 0; j < kScanItems; j++) {
     const long long idx = base + j;
-    if (idx < nCells) cellStart[idx] = run;
+    if (idx < limit) cellStart[idx] = run;
     run += v[j];
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_fill(uint32_t n, const uint32_t* __restrict__ key,
-                                                 const uint32_t* __restrict__ rank,
-                                                 const uint32_t* __restrict__ cellStart,
-                                                 uint32_t* __restrict__ unordered) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
-  const uint32_t at = __ldg(&cellStart[key[i]]) + rank[i];
-  if (at < n) unordered[at] = i;  // always true after a completed scan
-}
-
-__global__ void __launch_bounds__(kBlock) k_reorder(
-    const __grid_constant__ SimParams P, const uint32_t* __restrict__ key,
-    const uint32_t* __restrict__ cellStart, const uint32_t* __restrict__ unordered,
-    const float4* __restrict__ pos, const float4* __restrict__ vel, const uint4* __restrict__ body,
-    const float4* __restrict__ rest, float4* __restrict__ posOut, float4* __restrict__ velOut,
-    float4* __restrict__ predOut, uint4* __restrict__ bodyOut, float4* __restrict__ restOut,
-    uint32_t* __restrict__ slotOut, const uint32_t* __restrict__ bodyStart,
-    uint32_t* __restrict__ bodyFill, uint32_t* __restrict__ bodyList) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= P.n) return;
-  const uint32_t k = key[i];
-  // min() keeps every access in bounds even if a scan gave up (error word set)
-  const uint32_t e = min(__ldg(&cellStart[k + 1]), P.n), b = min(__ldg(&cellStart[k]), e);
-  uint32_t r = 0;
-  for (uint32_t m = b; m < e; m++) r += __ldg(&unordered[m]) < i ? 1u : 0u;
-  const uint32_t s = min(b + r, P.n - 1u);
-  const float4 p4 = __ldg(&pos[i]);
-  F3 v, pr;
-  predict_one(P, p4, __ldg(&vel[i]), v, pr);
-  posOut[s] = p4;
-  velOut[s] = make_float4(v.x, v.y, v.z, 0.0f);
-  predOut[s] = make_float4(pr.x, pr.y, pr.z, 1.0f);
-  if (body) {
-    const uint4 bd = __ldg(&body[i]);
-    bodyOut[s] = bd;
-    if (bodyList && bd.x != 0u && bd.x <= P.nBodies) {
-      const uint32_t slot = atomicAdd(&bodyFill[bd.x - 1u], 1u);
-      const uint32_t at = bodyStart[bd.x - 1u] + slot;
-      if (at < bodyStart[bd.x]) bodyList[at] = s;
-    }
+__global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCount,
+                                                 uint32_t* __restrict__ cellStart, int nCells,
+                                                 unsigned long long* __restrict__ state,
+                                                 uint32_t* __restrict__ ticket, uint32_t epoch,
+                                                 int nTiles, uint32_t* __restrict__ err) {
+  __shared__ uint32_t s_tile;
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const int tile = (int)s_tile;
+  if (tile >= nTiles) {  // only after an earlier launch failed mid-way: never index past the state
+    if (threadIdx.x == 0) atomicOr(err, ERR_SCAN_TIMEOUT);
+    return;
   }
-  if (rest) restOut[s] = __ldg(&rest[i]);
-  if (slotOut) slotOut[i] = s;
+  scan_tile(cellCount, cellStart, (long long)tile * kScanTile, nCells, tile, 0, 0u,
+            tile == nTiles - 1, state, epoch, err);
+  if (threadIdx.x == 0 && tile == nTiles - 1) *ticket = 0u;  // all tickets taken: reset
 }
 
-void launch_key_count(const SimParams& P, const float4* pos, const float4* vel, uint32_t* key,
-                      uint32_t* rank, uint32_t* cellCount, uint32_t* bodyFill, uint32_t nBodies,
-                      cudaStream_t st) {
-  const long long work = (long long)P.n > (long long)nBodies ? P.n : nBodies;
-  k_key_count<<<groups(work), kBlock, 0, st>>>(P, pos, vel, key, rank, cellCount, bodyFill, nBodies);
+// Batched: items[g] = (scene slot, local tile) in scene order; every scene's
+// segment of tiles is scanned on its own, seeded with its first particle index.
+__global__ void __launch_bounds__(kBlock) k_scan_b(const __grid_constant__ BatchWork w,
+                                                   const __grid_constant__ DevScene d, uint32_t epoch,
+                                                   int nTiles) {
+  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_cOff, s_nCells, s_pOff;
+  if (threadIdx.x == 0) s_tile = atomicAdd(d.scanTicket, 1u);
+  __syncthreads();
+  const int g = (int)s_tile;
+  if (g >= nTiles) {
+    if (threadIdx.x == 0) atomicOr(d.errorWord, ERR_SCAN_TIMEOUT);
+    return;
+  }
+  const uint2 it = w.items[g];
+  if (threadIdx.x == 0) {
+    s_cOff = w.params[it.x].cOff;
+    s_nCells = w.params[it.x].nCells;
+    s_pOff = w.params[it.x].pOff;
+  }
+  __syncthreads();
+  const int lt = (int)it.y;
+  const long long limit = (long long)s_cOff + s_nCells;
+  const bool last = (long long)(lt + 1) * kScanTile >= (long long)s_nCells;
+  scan_tile(d.cellCount, d.cellStart, (long long)s_cOff + (long long)lt * kScanTile, limit, g,
+            g - lt, s_pOff, last, d.scanState, epoch, d.errorWord);
+  if (threadIdx.x == 0 && g == nTiles - 1) *d.scanTicket = 0u;
 }
 
+void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st) {
+  const long long work = (long long)P.n > (long long)P.nBodies ? P.n : P.nBodies;
+  k_key_count<<<groups(work), kBlock, 0, st>>>(P, d);
+}
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells, unsigned long long* state,
                  uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st) {
   const int tiles = scan_tiles(nCells);
   k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err);
 }
-
-void launch_fill(uint32_t n, const uint32_t* key, const uint32_t* rank, const uint32_t* cellStart,
-                 uint32_t* unordered, cudaStream_t st) {
-  k_fill<<<groups(n), kBlock, 0, st>>>(n, key, rank, cellStart, unordered);
+void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st) {
+  k_fill<<<groups(P.n), kBlock, 0, st>>>(P, d);
+}
+void launch_reorder(const SimParams& P, const DevScene& d, cudaStream_t st) {
+  k_reorder<<<groups(P.n), kBlock, 0, st>>>(P, d);
+}
+cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity, const float* pos,
+                          const float* vel, const uint32_t* body, const float* rest, float* posOut,
+                          float* velOut, float* predOut, uint32_t* bodyOut, float* restOut,
+                          uint32_t* cellStart, uint32_t* slotOut, uint32_t* key, uint32_t* rank,
+                          uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
+                          uint32_t* ticket, uint32_t* err, cudaStream_t st) {
+  SimParams P{};
+  for (int k = 0; k < 3; k++) {
+    P.boxMin[k] = g.box_min[k];
+    P.gridDim[k] = g.dim[k];
+  }
+  P.h = g.h;
+  P.dt = dt;
+  P.gravity = gravity;
+  P.n = (uint32_t)n;
+  P.pEnd = (uint32_t)n;
+  const int nCells = g.dim[0] * g.dim[1] * g.dim[2];
+  P.nCells = (uint32_t)nCells;
+  DevScene d{};
+  d.pos[0] = (float4*)pos; d.pos[1] = (float4*)posOut;
+  d.vel[0] = (float4*)vel; d.vel[1] = (float4*)velOut;
+  d.pred[1] = (float4*)predOut;
+  d.body[0] = (uint4*)body; d.body[1] = (uint4*)bodyOut;
+  d.rest[0] = (float4*)rest; d.rest[1] = (float4*)restOut;
+  d.cellCount = cellCount;
+  d.cellStart = cellStart;
+  d.key = key;
+  d.rank = rank;
+  d.unordered = unordered;
+  d.slotOut = slotOut;
+  launch_key_count(P, d, st);
+  launch_scan(cellCount, cellStart, nCells, state, ticket, 1u, err, st);
+  launch_fill(P, d, st);
+  launch_reorder(P, d, st);
+  return cudaGetLastError();
 }
 
-void launch_reorder(const SimParams& P, const uint32_t* key, const uint32_t* cellStart,
-                    const uint32_t* unordered, const float4* pos, const float4* vel,
-                    const uint4* body, const float4* rest, float4* posOut, float4* velOut,
-                    float4* predOut, uint4* bodyOut, float4* restOut, uint32_t* slotOut,
-                    const uint32_t* bodyStart, uint32_t* bodyFill, uint32_t* bodyList,
-                    cudaStream_t st) {
-  k_reorder<<<groups(P.n), kBlock, 0, st>>>(P, key, cellStart, unordered, pos, vel, body, rest,
-                                            posOut, velOut, predOut, bodyOut, restOut, slotOut,
-                                            bodyStart, bodyFill, bodyList);
+void launch_key_count_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
+  if (nItems > 0) k_key_count_b<<<nItems, kBlock, 0, st>>>(w, d);
+}
+void launch_scan_b(const BatchWork& w, int nTiles, const DevScene& d, uint32_t epoch, cudaStream_t st) {
+  if (nTiles > 0) k_scan_b<<<nTiles, kBlock, 0, st>>>(w, d, epoch, nTiles);
+}
+void launch_fill_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
+  if (nItems > 0) k_fill_b<<<nItems, kBlock, 0, st>>>(w, d);
+}
+void launch_reorder_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
+  if (nItems > 0) k_reorder_b<<<nItems, kBlock, 0, st>>>(w, d);
 }
 
 }  // namespace p4a

@@ -47,7 +47,7 @@ __device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& 
                                              const uint32_t* __restrict__ cs, bool& isLong) {
   uint64_t m = 0ull;
   const uint32_t b = __ldg(&cs[rb + w.x0]);
-  const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.n);
+  const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
   const uint32_t len = e > b ? e - b : 0u;
   isLong = len > kMaskBits;
   const uint32_t lim = min(len, kMaskBits);
@@ -84,7 +84,7 @@ __device__ __forceinline__ void visit_row(const SimParams& P, const RowWalk& w, 
       f(b + (uint32_t)k);
     }
   } else {
-    const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.n);
+    const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
     for (uint32_t j = b; j < e; j++) {
       const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
       if (dot3(d, d) < P.h2) f(j);

@@ -1,11 +1,21 @@
-// p4a_internal.h — device parameter block, float contract helpers and kernel
-// launchers shared by the CUDA translation units of libp4a.
+// p4a_internal.h — device parameter block, buffer sets and kernel launchers shared
+// by the CUDA translation units of libp4a.
 //
 // Arithmetic contract (identical to the CPU oracle, so that results match bit
 // for bit): compiled with --fmad=false; the only fused multiply-adds are the
 // explicit fmaf() calls in dot3() and in accumulations "acc += s*v"; division and
 // square root are IEEE round-to-nearest; floats convert to ints with the
 // saturating cvt forms (__float2int_rz / _rn, __float2uint_rz).
+//
+// Every pass runs in one of two forms with the same device code:
+//   plain    one scene; the SimParams block is a kernel parameter and block b
+//            handles the b-th tile of 256 particles (the reference's workgroup);
+//   batched  many scenes in one launch; block b reads a (scene slot, item) pair
+//            from a work list and loads that scene's SimParams into shared memory.
+// Scenes of a batch live side by side in shared arenas: particle range
+// [pOff, pOff + cap), cell range [cOff, cOff + nCells + 2), body range
+// [bOff, bOff + nBodies + 1). Cell keys carry cOff, so one counting sort orders all
+// scenes at once, and cellStart entries are arena particle indices.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -15,7 +25,8 @@
 namespace p4a {
 
 // The reference's 192-byte uniform (src/wgsl.js:4-40), float32/int32 fields in
-// the reference's order. Passed to kernels by value (constant bank).
+// the reference's order, followed by the scene's place in the arenas and the
+// per-substep schedule values the passes need.
 struct SimParams {
   float boxMin[3]; float dt;
   float boxMax[3]; float h;
@@ -28,6 +39,15 @@ struct SimParams {
   uint32_t nBodies; float bodyScale, covScale, omega;
   uint32_t sorAverage; float invDt, volume, tension;
   float cohes, cohesTerm;
+  // arena placement and schedule (not in the reference's uniform)
+  uint32_t pOff;    // first particle of the scene in the particle arrays
+  uint32_t pEnd;    // pOff + n
+  uint32_t cOff;    // first cell of the scene in the cell arrays
+  uint32_t bOff;    // first body of the scene in the body arrays
+  uint32_t parity;  // live parity before this substep's sort
+  uint32_t iters;   // Jacobi iterations (>= 1)
+  uint32_t subs;    // substeps of the current frame (stats after the last)
+  uint32_t slot;    // stats slot (statsOut + 8 * slot)
 };
 
 // Anisotropic-kernel uniform (src/aniso_wgsl.js:4-21, packed by src/mesh.js:227-241).
@@ -42,7 +62,7 @@ struct AnisoParams {
 // Device error word bits (set by kernels, read by the host at sync points).
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };
 
-// Buffers of one scene on the device.
+// Device buffers of a scene, or of the arenas of a batch (same layout).
 struct DevScene {
   float4* pos[2];
   float4* vel[2];
@@ -53,32 +73,39 @@ struct DevScene {
   float* density;
   float4* corr;
   float4* normal;
-  uint32_t* cellCount;  // [nCells+1], all zero between substeps
-  uint32_t* cellStart;  // [nCells+2]
-  uint32_t* key;        // [cap]
-  uint32_t* rank;       // [cap]
-  uint32_t* unordered;  // [cap]
-  unsigned long long* scanState;  // [scan tiles], epoch-tagged
-  uint32_t* scanTicket;           // [1]
+  uint32_t* cellCount;  // all zero between substeps
+  uint32_t* cellStart;
+  uint32_t* key;
+  uint32_t* rank;
+  uint32_t* unordered;
+  unsigned long long* scanState;  // epoch-tagged tile states
+  uint32_t* scanTicket;
   float4* bpos;
   float* bpsi;
   uint32_t* bcellStart;
-  int32_t* bodyAccum;   // [4*B]
-  int32_t* bodyCov;     // [9*B]
+  int32_t* bodyAccum;   // 4 per body
+  int32_t* bodyCov;     // 9 per body
   float4* bodyCentre;
   float4* bodyRef;
-  float4* bodyRot;      // [3*B] rows
+  float4* bodyRot;      // 3 rows per body
   float4* bodyInfo;
-  uint32_t* bodyStart;  // [B+1] prefix of body particle counts
-  uint32_t* bodyFill;   // [B] append cursors, zeroed by the key pass
-  uint32_t* bodyList;   // [nBodyParts] sorted positions of each body's particles
-  uint32_t* statsOut;   // [8]
-  uint32_t* errorWord;  // [1]
+  uint32_t* bodyStart;  // per scene: nBodies + 1 prefix entries of its body list
+  uint32_t* bodyFill;   // append cursors, zeroed by the key pass
+  uint32_t* bodyList;   // arena positions of each body's particles
+  uint32_t* statsOut;   // 8 per stats slot
+  uint32_t* errorWord;
   float4* smoothPos;
   float4* anisoG;
   uint64_t* nbMask;     // [9][cap] per-row neighbour masks shared by a pair of passes
   uint32_t* nbLong;     // [cap] rows with more than 64 candidates
   uint32_t cap;         // particle capacity (stride of nbMask)
+  uint32_t* slotOut;    // optional: sorted position of each input particle
+};
+
+// A batched launch: block b works on item items[b] = (scene slot, tile/body).
+struct BatchWork {
+  const SimParams* params;
+  const uint2* items;
 };
 
 constexpr int kBlock = 256;          // particles per block (the reference's workgroup)
@@ -91,43 +118,50 @@ inline int groups(long long n, int per = kBlock) {
 }
 inline int scan_tiles(int nCells) { return groups(nCells, kScanTile); }
 
-// ---- launchers (stream = the scene's stream) ------------------------------
-// grid pass: predict + counting sort (kernels_grid.cu)
-void launch_key_count(const SimParams& P, const float4* pos, const float4* vel, uint32_t* key,
-                      uint32_t* rank, uint32_t* cellCount, uint32_t* bodyFill, uint32_t nBodies,
-                      cudaStream_t st);
+// ---- plain launchers (one scene; P.parity = live parity before the sort) ----
+void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells,
                  unsigned long long* state, uint32_t* ticket, uint32_t epoch, uint32_t* err,
                  cudaStream_t st);
-void launch_fill(uint32_t n, const uint32_t* key, const uint32_t* rank, const uint32_t* cellStart,
-                 uint32_t* unordered, cudaStream_t st);
-void launch_reorder(const SimParams& P, const uint32_t* key, const uint32_t* cellStart,
-                    const uint32_t* unordered, const float4* pos, const float4* vel,
-                    const uint4* body, const float4* rest, float4* posOut, float4* velOut,
-                    float4* predOut, uint4* bodyOut, float4* restOut, uint32_t* slotOut,
-                    const uint32_t* bodyStart, uint32_t* bodyFill, uint32_t* bodyList,
-                    cudaStream_t st);
-// solver (kernels_solve.cu)
-void launch_lambda(const SimParams& P, const DevScene& d, const float4* pred, cudaStream_t st);
-void launch_delta(const SimParams& P, const DevScene& d, const float4* pred, float4* predOut,
-                  const float4* posLive, float4* velScratch, cudaStream_t st);
-// finish (kernels_finish.cu)
-void launch_xsph_finalize(const SimParams& P, const DevScene& d, const float4* pred,
-                          const float4* velIn, float4* posOut, float4* velOut, float4* predCopy,
-                          bool stats, cudaStream_t st);
-void launch_xsph_normals(const SimParams& P, const DevScene& d, const float4* pred,
-                         const float4* velIn, cudaStream_t st);
-void launch_tension_finalize(const SimParams& P, const DevScene& d, const float4* pred,
-                             const float4* velIn, float4* posOut, float4* velOut,
-                             float4* predCopy, bool stats, cudaStream_t st);
-// bodies (kernels_body.cu)
-void launch_body_seed(const SimParams& P, const DevScene& d, const float4* pred, cudaStream_t st);
-void launch_body_match(const SimParams& P, const DevScene& d, float4* pred, const float4* rest,
-                       const float4* posLive, float4* velScratch, cudaStream_t st);
+void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st);
+void launch_reorder(const SimParams& P, const DevScene& d, cudaStream_t st);
+void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
+void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
+void launch_body_seed(const SimParams& P, const DevScene& d, cudaStream_t st);
+void launch_body_match(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
+void launch_xsph_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st);
+void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st);
+void launch_tension_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st);
+
+// ---- batched launchers (items: tiles of 256 particles, scan tiles, or bodies) ----
+void launch_key_count_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
+void launch_scan_b(const BatchWork& w, int nTiles, const DevScene& d, uint32_t epoch, cudaStream_t st);
+void launch_fill_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
+void launch_reorder_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
+void launch_lambda_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
+void launch_delta_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
+void launch_body_seed_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
+void launch_body_match_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
+void launch_xsph_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep, cudaStream_t st);
+void launch_xsph_normals_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
+void launch_tension_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep,
+                               cudaStream_t st);
+
+// The grid pass as an operator on caller buffers (p4a_grid_sort and
+// p4a_grid_sort_noalloc): input parity 0 = (pos, vel, body, rest), output parity 1
+// = (*_out); key/rank/unordered hold n entries; cellCount, state, ticket and err
+// must be zero on entry. Returns the launch status.
+cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity, const float* pos,
+                          const float* vel, const uint32_t* body, const float* rest, float* posOut,
+                          float* velOut, float* predOut, uint32_t* bodyOut, float* restOut,
+                          uint32_t* cellStart, uint32_t* slotOut, uint32_t* key, uint32_t* rank,
+                          uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
+                          uint32_t* ticket, uint32_t* err, cudaStream_t st);
+
+// ---- plain-only passes ----
 void launch_body_drag(const DevScene& d, float4* vel, const uint4* body, uint32_t held,
                       uint32_t heldCount, uint32_t heldStart, const float goal[3], float rate,
                       float blend, float limit, cudaStream_t st);
-// interactive passes and the anisotropic kernel (kernels_misc.cu)
 void launch_impulse(uint32_t n, const float4* pos, float4* vel, const float origin[3],
                     const float dir[3], const float impulse[3], float radius, float speedLimit,
                     cudaStream_t st);

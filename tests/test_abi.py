@@ -46,7 +46,8 @@ def test_struct_layouts_match_c_compiler(tmp_path):
     structs = {"p4a_body_spec": _abi.BodySpec, "p4a_params": _abi.Params,
                "p4a_scene_desc": _abi.SceneDesc, "p4a_info": _abi.Info, "p4a_stats": _abi.Stats,
                "p4a_aniso_params": _abi.AnisoParams, "p4a_grid": _abi.Grid,
-               "p4a_scene_counts": _abi.SceneCounts}
+               "p4a_scene_counts": _abi.SceneCounts, "p4a_batch_config": _abi.BatchConfig,
+               "p4a_batch_usage": _abi.BatchUsage, "p4a_phase_time": _abi.PhaseTime}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "p4a.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')

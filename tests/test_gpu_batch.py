@@ -1,0 +1,118 @@
+"""Batched multi-scene stepping: every scene stepped inside a batch (one launch
+per pass for all scenes, segmented sort, (scene, tile) work items, CUDA-graph
+replay) must give the bits it gives when stepped alone through the plain Sim,
+whatever else shares the batch. Also: admission by arena capacity, removal and
+reuse of arena ranges."""
+import numpy as np
+import pytest
+
+from particles4all_b200 import Batch, P4AError, Sim, _lib, configs
+from particles4all_b200.params import default_params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def need_gpu(built):
+    if not _lib.device_available():
+        pytest.fail("libp4a cannot use GPU 0")
+
+
+def mixed_scenes():
+    out = []
+    p = default_params("small")
+    p.update({"targetParticleCount": 2500, "box": [0.5, 0.4, 0.3], "bodies": ["sphere:0.5", "box:1.4"],
+              "bodySize": 0.05, "surfaceTensionK": 0.4, "substeps": 2})
+    out.append((p, None))
+    p = default_params("small")
+    p.update({"targetParticleCount": 1800, "box": [0.4, 0.3, 0.3], "bodies": [], "iterations": 3,
+              "sorAverage": True, "omega": 1.2})
+    out.append((p, None))
+    out.append(configs.dam_break_32k(side=10))
+    out.append(configs.medium_bodies_264k(side=12, n_cubes=2))
+    p = default_params("small")
+    p.update({"targetParticleCount": 900, "box": [0.3, 0.3, 0.2], "bodies": ["torus:0.8"],
+              "bodySize": 0.06, "substeps": 1, "noBoundary": True})
+    out.append((p, None))
+    return out
+
+
+def run_alone(params, scene, frames):
+    s = Sim()
+    if scene is None:
+        s.reset(params)
+    else:
+        s.reset_scene(params, scene)
+    for fd in frames:
+        s.step(fd)
+    return s
+
+
+NAMES = ("pos", "vel", "pred", "body", "rest", "density", "lambda_")
+
+
+def assert_same(sim, batch, sid):
+    n = sim.info()["n"]
+    bi = batch.info(sid)
+    assert bi["n"] == n and bi["parity"] == sim.info()["parity"]
+    for name in NAMES:
+        a, b = sim.read(name)[:n], batch.read(sid, name)[:n]
+        assert np.array_equal(a, b), name
+    c = sim.info()["n_cells"]
+    assert np.array_equal(sim.read("cellStart")[: c + 1], batch.read(sid, "cellStart")[: c + 1])
+    if sim.info()["n_bodies"]:
+        for name in ("bodyCentre", "bodyRot"):
+            assert np.array_equal(sim.read(name)[: sim.info()["n_bodies"] * (3 if name == "bodyRot" else 1)],
+                                  batch.read(sid, name)[: sim.info()["n_bodies"] * (3 if name == "bodyRot" else 1)])
+    assert sim.get_stats()["raw"] == batch.stats(sid)["raw"]
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+def test_batch_equals_alone_bit_exact(graphs):
+    scenes = mixed_scenes()
+    frames = [1 / 60] * 6 + [1 / 45, 1 / 90, 1 / 60]
+    b = Batch(max_particles=200_000, max_cells=400_000, max_scenes=16, graphs=graphs)
+    ids = []
+    for p, sc in scenes:
+        ids.append(b.add_preset(p) if sc is None else b.add_scene(p, sc))
+    for fd in frames:
+        b.step(ids, fd)
+    b.synchronize()
+    for (p, sc), sid in zip(scenes, ids):
+        assert_same(run_alone(p, sc, frames), b, sid)
+
+
+def test_subset_steps_and_arena_reuse():
+    scenes = mixed_scenes()
+    b = Batch(max_particles=60_000, max_cells=200_000, max_scenes=8)
+    ids = [b.add_preset(p) if sc is None else b.add_scene(p, sc) for p, sc in scenes[:3]]
+    # step only some scenes in some frames: the others must not move
+    b.step(ids, 1 / 60)
+    b.step(ids[:1], 1 / 60)
+    b.step(ids[1:], 1 / 60)
+    b.synchronize()
+    p0, s0 = scenes[0]
+    assert_same(run_alone(p0, s0, [1 / 60, 1 / 60]), b, ids[0])
+    p1, s1 = scenes[1]
+    assert_same(run_alone(p1, s1, [1 / 60, 1 / 60]), b, ids[1])
+    # remove one, admit another into the freed ranges
+    free0 = b.usage()["free_particles"]
+    b.remove_scene(ids[1])
+    assert b.usage()["free_particles"] > free0
+    p4, s4 = scenes[4]
+    sid = b.add_preset(p4)
+    b.step([sid, ids[0]], 1 / 60)
+    b.synchronize()
+    assert_same(run_alone(p4, s4, [1 / 60]), b, sid)
+    assert_same(run_alone(p0, s0, [1 / 60] * 3), b, ids[0])
+
+
+def test_admission_rejects_when_full():
+    p, sc = configs.dam_break_32k(side=12)  # 1,728 particles
+    b = Batch(max_particles=4000, max_cells=100_000, max_scenes=4)
+    b.add_scene(p, sc)
+    b.add_scene(p, sc)
+    with pytest.raises(P4AError) as e:
+        b.add_scene(p, sc)
+    assert e.value.status == 5
+    assert b.usage()["live_scenes"] == 2
