@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
+    ap.add_argument("--mix-frames", type=int, default=10)
     return ap.parse_args()
 
 
@@ -141,6 +143,82 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+def batched_mix_bench(frames, warmup):
+    """The 96-scene mix stepped (a) as one batch (one launch per pass for all
+    scenes, CUDA-graph frames) and (b) as the plain per-scene loop (96 Sim handles
+    on the same stream, one after the other). Device time per frame from CUDA
+    events; particle-substeps/s for both."""
+    import math
+
+    import torch
+    from particles4all_b200 import Batch, Sim, configs
+    mix = configs.batched_mix()
+    total = sum(sc["pos"].shape[0] for _, sc in mix)
+    cap = sum((sc["pos"].shape[0] + 511) // 256 * 256 for _, sc in mix)
+    cells = sum((int(math.prod(int(b) for b in p["box"])) // 2048 + 2) * 2048 for p, _ in mix)
+    nbound = 0
+    for p, _ in mix:
+        nb = [max(2, math.ceil(b / p["spacing"]) + 1) for b in p["box"]]
+        nbound += nb[0] * nb[1] * nb[2] - (nb[0] - 2) * (nb[1] - 2) * (nb[2] - 2)
+    bodies = sum(sc["n_bodies"] + 1 for _, sc in mix)
+    body_parts = sum(int((sc["phase"][:, 0] > 0).sum()) + 1 for _, sc in mix)
+    stream = torch.cuda.Stream()
+    b = Batch(max_particles=cap + 4096, max_cells=cells, max_scenes=len(mix) + 1, max_bodies=bodies + 8,
+              max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
+    b.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    ids = [b.add_scene(p, sc) for p, sc in mix]
+    admit_s = time.perf_counter() - t0
+    sims = []
+    for p, sc in mix:
+        sim = Sim()
+        sim.set_stream(stream.cuda_stream)
+        sim.reset_scene(p, sc)
+        sims.append(sim)
+
+    def timed(fn, k):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
+        subs = 0
+        for e0, e1 in ev:
+            e0.record(stream)
+            subs += fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return sum(e0.elapsed_time(e1) for e0, e1 in ev), subs
+
+    def batched():
+        b.step(ids, 1 / 60)
+        return 2
+
+    def plain():
+        for sim in sims:
+            sim.step(1 / 60)
+        return 2
+    timed(batched, warmup)
+    timed(plain, warmup)
+    launches0 = _launches()
+    tb, sb = timed(batched, frames)
+    lb = _launches() - launches0
+    launches0 = _launches()
+    tp, sp = timed(plain, frames)
+    lp = _launches() - launches0
+    for sim in sims:
+        sim.close()
+    b.close()
+    vb = total * sb / (tb / 1000.0)
+    vp = total * sp / (tp / 1000.0)
+    return {"scenes": len(mix), "particles": total, "frames": frames, "substeps_per_frame": 2,
+            "batched_value": vb, "plain_value": vp, "speedup": vb / vp, "unit": METRIC,
+            "batched_ms_per_frame": tb / frames, "plain_ms_per_frame": tp / frames,
+            "batched_launches_per_frame": lb / frames, "plain_launches_per_frame": lp / frames,
+            "admit_s_total": admit_s}
+
+
+def _launches():
+    from particles4all_b200 import _lib
+    return _lib.lib().p4a_kernel_launches()
 
 
 def cpu_baseline(params, scene, aniso, seconds):
@@ -329,6 +407,10 @@ def run_ours(args):
                "what": "per step: live pos+vel written from pinned host, Sim.step + aniso, "
                        "pos+vel+stats read back to pinned host"}
 
+    mix = None
+    if world == 1 and not args.no_mix:
+        mix = batched_mix_bench(args.mix_frames, 3)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(params, scene, aniso, args.cpu_seconds)
@@ -346,6 +428,7 @@ def run_ours(args):
                        "l2": "flushed between timed steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "batched_mix": mix,
             "clocks": clocks.summary(w0, w1),
             "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")},
         }

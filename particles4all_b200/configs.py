@@ -215,6 +215,42 @@ class Hose:
         return pos.astype(np.float32), vel.astype(np.float32)
 
 
+def batched_mix(seed=12, count=96, n_lo=4000, n_hi=256000, cube=6):
+    """The batched mix: `count` scenes with particle counts log-uniform in
+    [n_lo, n_hi] (about 6 M in total for 96), boxes of 16-64 cells per axis, 0-6
+    rigid 6x6x6 cubes (density 0.5) with seeded orientations above the water,
+    surface tension 0.5 on half of the scenes, 4 iterations. Returns a list of
+    (params, scene). Seed 12 gives 6,003,226 particles for the 96 scenes."""
+    d, h = 0.5, 1.0
+    rng = np.random.default_rng(seed)
+    mass = lattice_mass(d, h)
+    span = cube * d
+    out = []
+    for _ in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        side = int(math.ceil(n ** (1.0 / 3.0)))
+        lo_cells = max(16, int(math.ceil(side * d)) + 6)
+        box = np.array([float(rng.integers(lo_cells, 65)) for _ in range(3)])
+        n_cubes = int(rng.integers(0, 7))
+        tension = 0.5 if rng.random() < 0.5 else 0.0
+        # the block fills layer by layer (y outermost), as the reference's fluidBlock
+        iy, ix, iz = np.meshgrid(np.arange(side), np.arange(side), np.arange(side), indexing="ij")
+        lat = np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1)[:n].astype(np.float64)
+        fluid = d + (lat + 0.5) * d + rng.uniform(-0.01 * d, 0.01 * d, size=lat.shape)
+        top = d + (lat[:, 1].max() + 1) * d
+        bodies = []
+        if n_cubes:
+            box = np.maximum(box, [4 * span + 4.0, top + 4 * span + 2.0, 4 * span + 4.0])
+            lo = np.array([span + 1.0, top + span, span + 1.0])
+            hi = np.array([box[0] - span - 1.0, min(box[1] - span - 1.0, top + 3 * span), box[2] - span - 1.0])
+            local = _body_points("box", cube, d)
+            for c in _place_bodies(rng, n_cubes, lo, hi, min_dist=2.0 * span):
+                bodies.append({"centre": c, "offsets": local @ _rotation(rng).T, "density": 0.5})
+        params = _base_params(box, iterations=4, tension=tension, xsph=0.01)
+        out.append((params, _assemble(fluid, bodies, params, mass)))
+    return out
+
+
 WORKLOADS = {
     "dam_break_32k": dam_break_32k,
     "medium_bodies_264k": medium_bodies_264k,

@@ -1045,6 +1045,14 @@ int p4a_profile_read(p4a_sim* s, p4a_phase_time* out, int32_t maxEntries, int32_
 
 uint64_t p4a_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
+}  // extern "C"
+
+namespace p4a {
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace p4a
+
+extern "C" {
+
 // ---- operator entry: predict + grid pass on caller buffers ---------------
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 

@@ -135,6 +135,7 @@ struct p4a_batch {
   bool useGraphs = true;
   std::vector<int64_t> graphKey;
   cudaGraphExec_t graph = nullptr;
+  uint64_t graphKernels = 0;  // kernels in the captured frame
 };
 
 namespace {
@@ -260,6 +261,17 @@ void append_to(Seg& seg, std::vector<uint2>& v, uint32_t slot, int64_t count) {
   seg.count += (int)count;
 }
 
+// Kernels one frame of the schedule launches.
+uint64_t frame_kernels(const Schedule& sch) {
+  uint64_t k = 0;
+  for (const auto& u : sch.subs) {
+    k += (u.key.count > 0) + (u.scan.count > 0) + 2 * (u.part.count > 0) + (u.seed.count > 0) +
+         (u.finishPlain.count > 0) + 2 * (u.finishTension.count > 0);
+    for (size_t it = 0; it < u.iter.size(); it++) k += 2 * (u.iter[it].count > 0) + (u.bodyIter[it].count > 0);
+  }
+  return k;
+}
+
 // Launches one frame of the schedule on the batch's stream.
 int run_frame(p4a_batch* b, const Schedule& sch, int nSlots) {
   cudaStream_t st = b->stream;
@@ -349,6 +361,7 @@ int execute(p4a_batch* b, const Schedule& sch, const std::vector<SimParams>& par
   BTRY(b, cudaMemcpyAsync(b->dParams, b->staging[k], pBytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaMemcpyAsync(b->dItems, b->staging[k] + pBytes, iBytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaEventRecord(b->stagingDone[k], b->stream));
+  count_launches(frame_kernels(sch) + (zeroSeg.count > 0 ? 1 : 0));
   auto body = [&]() -> int {
     if (zeroSeg.count > 0)
       k_zero_stats<<<(zeroSeg.count * 8 + 255) / 256, 256, 0, b->stream>>>(b->d.statsOut, b->dItems + zeroSeg.off,

@@ -158,6 +158,9 @@ cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity,
                           uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
                           uint32_t* ticket, uint32_t* err, cudaStream_t st);
 
+// Adds to the process-wide count of kernels launched by the library.
+void count_launches(uint64_t n);
+
 // ---- plain-only passes ----
 void launch_body_drag(const DevScene& d, float4* vel, const uint4* body, uint32_t held,
                       uint32_t heldCount, uint32_t heldStart, const float goal[3], float rate,
