@@ -55,6 +55,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
     ap.add_argument("--mix-frames", type=int, default=10)
+    ap.add_argument("--serve-seconds", type=float, default=15.0,
+                    help="length of each served-workload run (batched, then plain); 0 skips it")
+    ap.add_argument("--serve-budget-gb", type=float, default=160.0)
     return ap.parse_args()
 
 
@@ -216,6 +219,35 @@ def batched_mix_bench(frames, warmup):
             "admit_s_total": admit_s}
 
 
+def served_bench(seconds, budget_gb):
+    """The served workload (Poisson creates at 200/s, 2k-512k particles, 60 Hz
+    closed-loop step requests, exp(10 s) lifetimes, positions read back every 4th
+    step) for `seconds` against the batched server, then the same trace against
+    the plain per-scene server. Arenas sized for min(budget, free device memory)."""
+    import torch
+    from particles4all_b200 import loadgen
+    from particles4all_b200.server import Server
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(budget_gb * 1e9, free - 16e9))
+    out = {"workload": "poisson 200/s, n ~ logU[2k, 512k], 60 Hz closed-loop steps, exp(10 s) lifetimes, "
+                       "pos readback every 4th step", "seconds": seconds, "arena_budget_bytes": budget}
+    for mode in ("batched", "plain"):
+        srv = Server(budget_bytes=budget, max_scenes=4096, plain=(mode == "plain"), builder_threads=6,
+                     upload_bytes=2 << 30, readback_bytes=4 << 30)
+        t0 = time.perf_counter()
+        r = loadgen.run(srv, seconds, seed=4)
+        st = srv.stats()
+        srv.close()
+        r.update({"server_p50_ms": st["step_p50_ms"], "server_p99_ms": st["step_p99_ms"],
+                  "max_queued_creates": st["max_queued_creates"], "frames": st["frames"],
+                  "mean_frame_scenes": st["mean_frame_scenes"], "gpu_seconds": st["gpu_seconds"],
+                  "admit_p50_ms": st["admit_p50_ms"], "admit_p99_ms": st["admit_p99_ms"],
+                  "kernel_launches": st["kernel_launches"], "wall_s": time.perf_counter() - t0})
+        out[mode] = r
+    out["speedup"] = out["batched"]["particle_substeps_per_s"] / max(1e-9, out["plain"]["particle_substeps_per_s"])
+    return out
+
+
 def _launches():
     from particles4all_b200 import _lib
     return _lib.lib().p4a_kernel_launches()
@@ -294,26 +326,11 @@ def run_ours(args):
     import torch
     from particles4all_b200 import Sim, _lib
 
+    from particles4all_b200.replicas import Replicas
     rank, local, world = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-        pg = dist
-
-    def barrier():
-        if pg:
-            pg.barrier()
-
-    def allmax(x):
-        if not pg:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas("nccl")  # replicas only: no collective on the data path
+    barrier, allmax = rep.barrier, rep.max
 
     params, scene, aniso = workload(args.workload)
     stream = torch.cuda.Stream()
@@ -411,6 +428,13 @@ def run_ours(args):
     if world == 1 and not args.no_mix:
         mix = batched_mix_bench(args.mix_frames, 3)
 
+    served = None
+    if world == 1 and args.serve_seconds > 0:
+        try:
+            served = served_bench(args.serve_seconds, args.serve_budget_gb)
+        except Exception as e:  # the headline line is still printed
+            served = {"error": f"{type(e).__name__}: {e}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(params, scene, aniso, args.cpu_seconds)
@@ -429,14 +453,13 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "batched_mix": mix,
+            "served": served,
             "clocks": clocks.summary(w0, w1),
             "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")},
         }
         print(json.dumps(line), flush=True)
     sim.close()
-    if pg:
-        barrier()
-        pg.destroy_process_group()
+    rep.close()
     return 0
 
 

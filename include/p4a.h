@@ -312,6 +312,95 @@ int p4a_batch_stats(p4a_batch* b, int32_t scene_id, p4a_stats* out);
 /* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
 int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
 
+/* ---- serving loop (no counterpart in the reference) --------------------- */
+/*
+ * A request loop over one batch (continuous batching). Clients on any thread
+ * submit create, step and destroy requests; an engine thread builds created
+ * scenes on host worker threads, admits them as scene slots and arena space
+ * free up (admission by free device memory), and packs every live scene that
+ * has a pending step into the next batched frame while the previous frame is
+ * still running on the GPU. Scene state stays resident on the device between
+ * requests. Each request ends in exactly one p4a_completion, read with
+ * p4a_server_poll. A step may ask for the scene's live positions and/or
+ * velocities (float4[n], cell-sorted, as p4a_read of P4A_BUF_POS/VEL); the
+ * output buffers must stay valid until the step's completion has been polled.
+ * Per scene, steps run in submission order, one per frame.
+ * plain = 1 serves the same requests with one plain Sim per scene, stepped one
+ * after another (the comparison for the batched form).
+ */
+typedef struct p4a_server p4a_server;
+typedef struct p4a_server_config {
+  p4a_batch_config arenas;     /* batch arena sizes (ignored by plain = 1)          */
+  int32_t builder_threads;     /* host threads building scenes, default 4           */
+  int32_t max_frames_in_flight;/* frames on the GPU ahead of completion, default 2  */
+  double admit_timeout;        /* seconds a create may wait for room; 0 = forever   */
+  int32_t max_pending_creates; /* creates waiting beyond this are rejected; 0 = no cap */
+  int32_t use_graphs;          /* replay captured frames, default 1                 */
+  int32_t plain;               /* 1 = plain per-scene stepping                      */
+  int64_t upload_bytes;        /* pinned staging for scene uploads, default 1 GiB   */
+  int64_t readback_bytes;      /* pinned staging for step readbacks, default 1 GiB  */
+} p4a_server_config;
+enum { P4A_REQ_CREATE = 1, P4A_REQ_STEP = 2, P4A_REQ_DESTROY = 3 };
+typedef struct p4a_completion {
+  int64_t request;     /* id returned by the submit call                           */
+  int32_t kind;        /* P4A_REQ_*                                                */
+  int32_t scene;       /* scene handle                                             */
+  int32_t status;      /* P4A_OK; P4A_ERR_CAPACITY = create rejected (no room in  */
+                       /* time) or readback staging too small; P4A_ERR_STATE =    */
+                       /* scene gone or server stopping; P4A_ERR_CUDA            */
+  int32_t substeps;    /* STEP: substeps run                                       */
+  int64_t particles;   /* the scene's particle count                               */
+  double submitted;    /* server clock (s) at submission                           */
+  double started;      /* when its work was issued to the GPU                      */
+  double finished;     /* when the engine saw it complete                          */
+} p4a_completion;
+typedef struct p4a_server_stats {
+  int64_t creates, admitted, rejected, destroyed, steps, frames;
+  int32_t live_scenes, queued_creates, max_queued_creates, building;
+  double particle_substeps;    /* of completed steps                               */
+  double step_p50_ms, step_p99_ms, step_mean_ms, step_max_ms;  /* submit -> finish  */
+  double admit_p50_ms, admit_p99_ms;  /* create submit -> admitted                 */
+  double mean_frame_scenes;    /* scenes per stepping frame                        */
+  double gpu_seconds;          /* device time of all frames (CUDA events)          */
+  double first_submit, last_finish;   /* server clock                              */
+  int64_t kernel_launches;     /* frames' kernels (graph replays count each node)  */
+} p4a_server_stats;
+int p4a_server_default_config(p4a_server_config* cfg);
+int p4a_server_create(int device, const p4a_server_config* cfg, p4a_server** out);
+/* Stops the engine: work on the GPU finishes, queued requests complete with
+ * P4A_ERR_STATE, and every completion not yet polled is dropped. */
+int p4a_server_destroy(p4a_server* s);
+const char* p4a_server_last_error(const p4a_server* s);
+double p4a_server_clock(const p4a_server* s);
+/* Create a scene from params (scene = NULL: the reference's buildScene) or from
+ * an explicit scene (copied before the call returns). *scene is the handle
+ * steps and destroys refer to; the create's completion says if it was admitted. */
+int p4a_server_create_scene(p4a_server* s, const p4a_params* params, const p4a_scene_desc* scene,
+                            int32_t* scene_id, int64_t* request);
+int p4a_server_step(p4a_server* s, int32_t scene_id, double frame_dt, float* pos_out,
+                    float* vel_out, size_t out_bytes, int64_t* request);
+int p4a_server_destroy_scene(p4a_server* s, int32_t scene_id, int64_t* request);
+/* Up to max completions; waits up to wait_seconds for the first one. */
+int p4a_server_poll(p4a_server* s, p4a_completion* out, int32_t max, int32_t* count,
+                    double wait_seconds);
+int p4a_server_get_stats(p4a_server* s, p4a_server_stats* out);
+
+/* ---- launch-shape tuning (no counterpart in the reference) -------------- */
+/*
+ * The neighbour kernels run in one of several launch shapes (threads per
+ * block x minimum resident blocks per SM); the arithmetic per particle is the
+ * same in every shape, so the choice changes speed only. A table per kernel
+ * maps a launch's particle count (the scene's for plain steps, the frame's
+ * total for batched ones) to a shape: the first bucket whose max_particles is
+ * >= the count, else variant 0. The table is process-wide.
+ */
+enum { P4A_KERNEL_LAMBDA = 0, P4A_KERNEL_DELTA = 1, P4A_KERNEL_NORMALS = 2, P4A_KERNEL_ANISO = 3 };
+int p4a_kernel_shapes(int32_t kernel, int32_t* threads, int32_t* min_blocks, int32_t max,
+                      int32_t* count);
+int p4a_tune_set(int32_t kernel, int64_t max_particles, int32_t variant);
+int p4a_tune_clear(int32_t kernel);   /* -1 = every kernel */
+int p4a_tune_get(int32_t kernel, int64_t particles, int32_t* variant);
+
 /* ---- operator entry: predict + grid pass as one call ------------------- */
 /*
  * The predict pass and the 'grid' pass of Sim.step (src/wgsl.js:56-70,

@@ -102,6 +102,33 @@ class BatchUsage(C.Structure):
                 ("live_scenes", C.c_int32), ("device_bytes", C.c_int64)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("arenas", BatchConfig), ("builder_threads", C.c_int32), ("max_frames_in_flight", C.c_int32),
+                ("admit_timeout", C.c_double), ("max_pending_creates", C.c_int32), ("use_graphs", C.c_int32),
+                ("plain", C.c_int32), ("upload_bytes", C.c_int64), ("readback_bytes", C.c_int64)]
+
+
+REQ_CREATE, REQ_STEP, REQ_DESTROY = 1, 2, 3
+REQ_NAMES = {1: "create", 2: "step", 3: "destroy"}
+
+
+class Completion(C.Structure):
+    _fields_ = [("request", C.c_int64), ("kind", C.c_int32), ("scene", C.c_int32), ("status", C.c_int32),
+                ("substeps", C.c_int32), ("particles", C.c_int64), ("submitted", C.c_double),
+                ("started", C.c_double), ("finished", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("creates", C.c_int64), ("admitted", C.c_int64), ("rejected", C.c_int64),
+                ("destroyed", C.c_int64), ("steps", C.c_int64), ("frames", C.c_int64),
+                ("live_scenes", C.c_int32), ("queued_creates", C.c_int32), ("max_queued_creates", C.c_int32),
+                ("building", C.c_int32), ("particle_substeps", C.c_double), ("step_p50_ms", C.c_double),
+                ("step_p99_ms", C.c_double), ("step_mean_ms", C.c_double), ("step_max_ms", C.c_double),
+                ("admit_p50_ms", C.c_double), ("admit_p99_ms", C.c_double), ("mean_frame_scenes", C.c_double),
+                ("gpu_seconds", C.c_double), ("first_submit", C.c_double), ("last_finish", C.c_double),
+                ("kernel_launches", C.c_int64)]
+
+
 def info_dict(info):
     d = {k: getattr(info, k) for k, _ in Info._fields_}
     d["grid_dim"] = list(info.grid_dim)

@@ -58,6 +58,20 @@ SIGNATURES = {
     "p4a_batch_write": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
     "p4a_batch_stats": ([_vp, _i32, _vp], C.c_int),
     "p4a_batch_use_graphs": ([_vp, _i32], C.c_int),
+    "p4a_server_default_config": ([_vp], C.c_int),
+    "p4a_server_create": ([C.c_int, _vp, C.POINTER(_vp)], C.c_int),
+    "p4a_server_destroy": ([_vp], C.c_int),
+    "p4a_server_last_error": ([_vp], C.c_char_p),
+    "p4a_server_clock": ([_vp], _dbl),
+    "p4a_server_create_scene": ([_vp, _vp, _vp, C.POINTER(_i32), C.POINTER(C.c_int64)], C.c_int),
+    "p4a_server_step": ([_vp, _i32, _dbl, _vp, _vp, _sz, C.POINTER(C.c_int64)], C.c_int),
+    "p4a_server_destroy_scene": ([_vp, _i32, C.POINTER(C.c_int64)], C.c_int),
+    "p4a_server_poll": ([_vp, _vp, _i32, C.POINTER(_i32), _dbl], C.c_int),
+    "p4a_server_get_stats": ([_vp, _vp], C.c_int),
+    "p4a_kernel_shapes": ([_i32, _vp, _vp, _i32, C.POINTER(_i32)], C.c_int),
+    "p4a_tune_set": ([_i32, C.c_int64, _i32], C.c_int),
+    "p4a_tune_clear": ([_i32], C.c_int),
+    "p4a_tune_get": ([_i32, C.c_int64, C.POINTER(_i32)], C.c_int),
 }
 
 _lib = None
@@ -81,6 +95,8 @@ def lib():
             f.argtypes = args
             f.restype = res
         _lib = L
+        from . import autotune
+        autotune.load(L=L)  # measured launch shapes, when tuning.json is present
     return _lib
 
 

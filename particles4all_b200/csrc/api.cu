@@ -19,6 +19,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1049,6 +1051,24 @@ uint64_t p4a_kernel_launches(void) { return g_launches.load(std::memory_order_re
 
 namespace p4a {
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int resident_grid(const void* kernel, int block) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  const auto key = std::make_pair(dev, kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int perSM = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kernel, block, 0) != cudaSuccess || perSM < 1)
+    perSM = 1;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+  const int g = perSM * sms;
+  cache[key] = g;
+  return g;
+}
 }  // namespace p4a
 
 extern "C" {

@@ -22,123 +22,13 @@
 #include <vector>
 
 #include "../../include/p4a.h"
+#include "batch_internal.h"
 #include "p4a_internal.h"
 #include "scene.h"
 
 using namespace p4a;
 
-namespace {
-
-const double kPi = 3.14159265358979323846;
-constexpr int kMaxSubsteps = 64;  // per frame (the time bank caps at 8 x substeps)
-
-// First-fit allocator of aligned ranges in [0, capacity).
-class RangeAlloc {
- public:
-  void init(int64_t cap) {
-    free_.clear();
-    cap_ = cap;
-    if (cap > 0) free_[0] = cap;
-  }
-  int64_t alloc(int64_t size, int64_t align) {
-    if (size <= 0) size = 1;
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      const int64_t start = (it->first + align - 1) / align * align;
-      const int64_t end = it->first + it->second;
-      if (start + size > end) continue;
-      const int64_t f0 = it->first;
-      free_.erase(it);
-      if (start > f0) free_[f0] = start - f0;
-      if (end > start + size) free_[start + size] = end - (start + size);
-      return start;
-    }
-    return -1;
-  }
-  void release(int64_t off, int64_t size) {
-    if (size <= 0) size = 1;
-    auto it = free_.emplace(off, size).first;
-    auto next = std::next(it);
-    if (next != free_.end() && it->first + it->second == next->first) {
-      it->second += next->second;
-      free_.erase(next);
-    }
-    if (it != free_.begin()) {
-      auto prev = std::prev(it);
-      if (prev->first + prev->second == it->first) {
-        prev->second += it->second;
-        free_.erase(it);
-      }
-    }
-  }
-  int64_t free_total() const {
-    int64_t t = 0;
-    for (auto& kv : free_) t += kv.second;
-    return t;
-  }
-
- private:
-  std::map<int64_t, int64_t> free_;
-  int64_t cap_ = 0;
-};
-
-struct Range {
-  int64_t off = -1, size = 0;
-};
-
-struct BScene {
-  bool live = false;
-  p4a_params params{};
-  std::vector<p4a_body_spec> specs;
-  double mass = 0, denomRest = 0, h = 0;
-  int n = 0, nFluid = 0, cap = 0, nBodies = 0, nBodyParts = 0, nBoundary = 0;
-  int gridDim[3] = {1, 1, 1};
-  int nCells = 1;
-  double bodyScale = 0, covScale = 0;
-  Range part, cells, bodies, list, bound;
-  int parity = 0;
-  double timeBank = 0, simTime = 0, lastAdvanced = 0;
-  int lastSubsteps = 0;
-  int gen = 0;
-  bool statsValid = false;
-  SimParams P{};
-};
-
-// One launch of a frame schedule: a segment of the work-item buffer.
-struct Seg {
-  int64_t off = 0;
-  int count = 0;
-};
-
-}  // namespace
-
-struct p4a_batch {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool ownStream = false;
-  std::string err;
-  p4a_batch_config cfg{};
-  DevScene d{};
-  std::vector<void*> allocs;
-  size_t deviceBytes = 0;
-  RangeAlloc partA, cellA, boundA, bodyA, listA;
-  std::vector<BScene> scenes;
-  int64_t scanTilesCap = 0;
-  // per-frame schedule upload (double-buffered pinned staging)
-  SimParams* dParams = nullptr;  // [kMaxSubsteps][max_scenes]
-  uint2* dItems = nullptr;
-  int64_t itemsCap = 0;
-  unsigned char* staging[2] = {nullptr, nullptr};
-  size_t stagingCap = 0;
-  cudaEvent_t stagingDone[2] = {nullptr, nullptr};
-  int stagingIdx = 0;
-  // CUDA graphs of frame schedules
-  bool useGraphs = true;
-  std::vector<int64_t> graphKey;
-  cudaGraphExec_t graph = nullptr;
-  uint64_t graphKernels = 0;  // kernels in the captured frame
-};
-
-namespace {
+namespace p4a {
 
 int bfail(p4a_batch* b, int code, const char* fmt, ...) {
   if (b) {
@@ -152,13 +42,11 @@ int bfail(p4a_batch* b, int code, const char* fmt, ...) {
   return code;
 }
 
-#define BTRY(b, call)                                                                    \
-  do {                                                                                   \
-    cudaError_t e_ = (call);                                                             \
-    if (e_ != cudaSuccess)                                                               \
-      return bfail((b), e_ == cudaErrorMemoryAllocation ? P4A_ERR_OOM : P4A_ERR_CUDA,    \
-                   "%s: %s", #call, cudaGetErrorString(e_));                             \
-  } while (0)
+}  // namespace p4a
+
+namespace {
+
+const double kPi = 3.14159265358979323846;
 
 template <class T>
 int balloc(p4a_batch* b, T** out, int64_t count) {
@@ -228,105 +116,106 @@ void pack(BScene& s, double dt, int slot) {
   F.slot = (uint32_t)slot;
 }
 
-void release_scene(p4a_batch* b, BScene& s) {
-  if (s.part.off >= 0) b->partA.release(s.part.off, s.part.size);
-  if (s.cells.off >= 0) b->cellA.release(s.cells.off, s.cells.size);
-  if (s.bodies.off >= 0) b->bodyA.release(s.bodies.off, s.bodies.size);
-  if (s.list.off >= 0) b->listA.release(s.list.off, s.list.size);
-  if (s.bound.off >= 0) b->boundA.release(s.bound.off, s.bound.size);
-  s = BScene();
-}
-
-// A frame schedule: per substep the work-item segments of every launch.
-struct Schedule {
-  std::vector<uint2> items;
-  struct Sub {
-    Seg key, scan, part, seed, finishPlain, finishTension;
-    std::vector<Seg> iter, bodyIter;
-  };
-  std::vector<Sub> subs;
-  int maxIters = 0;
+// Kinds of the launches of a frame, in the order a substep issues them.
+enum LaunchKind : int {
+  LK_ZERO, LK_KEY, LK_SCAN, LK_FILL, LK_REORDER, LK_SEED, LK_LAMBDA, LK_DELTA, LK_MATCH,
+  LK_FINISH, LK_NORMALS, LK_TENSION
 };
 
-Seg push_tiles(std::vector<uint2>& v, uint32_t slot, int64_t tiles) {
-  Seg s{(int64_t)v.size(), (int)tiles};
-  for (int64_t t = 0; t < tiles; t++) v.push_back(make_uint2(slot, (uint32_t)t));
-  return s;
+struct LaunchRec {
+  int kind, sub, it;
+  WorkSeg seg;
+};
+
+// One frame: the work items of every launch (item .x = the scene's row in the
+// frame's params table), the launches in issue order, and the params rows
+// [sub][row] of the frame's scenes. `shape` (substeps, then the iteration count of
+// each substep) fixes the launch sequence: frames of one shape replay one graph.
+struct Frame {
+  std::vector<uint2> items;
+  std::vector<LaunchRec> launches;
+  std::vector<SimParams> params;
+  int nSubs = 0, nRows = 0;
+  int variant[TK_COUNT] = {0, 0, 0, 0};  // launch shapes of the tuned kernels
+  std::vector<int> shape;
+};
+
+WorkSeg push_items(Frame& F, uint32_t row, int64_t count, WorkSeg seg) {
+  if (seg.count == 0) seg.off = (uint32_t)F.items.size();
+  for (int64_t t = 0; t < count; t++) F.items.push_back(make_uint2(row, (uint32_t)t));
+  seg.count += (uint32_t)count;
+  return seg;
 }
 
-void append_to(Seg& seg, std::vector<uint2>& v, uint32_t slot, int64_t count) {
-  // Segments are built scene by scene; keep each launch's items contiguous.
-  if (seg.count == 0) seg.off = (int64_t)v.size();
-  for (int64_t t = 0; t < count; t++) v.push_back(make_uint2(slot, (uint32_t)t));
-  seg.count += (int)count;
-}
+void add_launch(Frame& F, int kind, int sub, int it, WorkSeg seg) { F.launches.push_back({kind, sub, it, seg}); }
 
-// Kernels one frame of the schedule launches.
-uint64_t frame_kernels(const Schedule& sch) {
-  uint64_t k = 0;
-  for (const auto& u : sch.subs) {
-    k += (u.key.count > 0) + (u.scan.count > 0) + 2 * (u.part.count > 0) + (u.seed.count > 0) +
-         (u.finishPlain.count > 0) + 2 * (u.finishTension.count > 0);
-    for (size_t it = 0; it < u.iter.size(); it++) k += 2 * (u.iter[it].count > 0) + (u.bodyIter[it].count > 0);
-  }
-  return k;
-}
-
-// Launches one frame of the schedule on the batch's stream.
-int run_frame(p4a_batch* b, const Schedule& sch, int nSlots) {
+// Launches one frame on the batch's stream. Graph form: every launch of the shape
+// is issued with the resident grid and fixed-size clears (counts are read on the
+// device); direct form: empty launches are skipped and grids fit the counts.
+int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched) {
   cudaStream_t st = b->stream;
   DevScene& d = b->d;
-  for (size_t s = 0; s < sch.subs.size(); s++) {
-    const Schedule::Sub& u = sch.subs[s];
+  const int stride = b->cfg.max_scenes;
+  uint64_t n = 0;
+  BTRY(b, cudaMemsetAsync(b->dCursors, 0, F.launches.size() * sizeof(uint32_t), st));
+  for (size_t L = 0; L < F.launches.size(); L++) {
+    const LaunchRec& r = F.launches[L];
+    if (!graphForm && r.seg.count == 0) continue;
     BatchWork w;
-    w.params = b->dParams + s * (size_t)nSlots;
-    auto at = [&](const Seg& g) {
-      BatchWork x = w;
-      x.items = b->dItems + g.off;
-      return x;
-    };
-    launch_key_count_b(at(u.key), u.key.count, d, st);
-    BTRY(b, cudaMemsetAsync(d.scanState, 0, (size_t)u.scan.count * 8, st));
-    {
-      // the scan addresses its tile states from 0: pass the segment's items
-      BatchWork x = at(u.scan);
-      launch_scan_b(x, u.scan.count, d, 1u, st);
+    w.params = b->dParams + (size_t)r.sub * stride;
+    w.items = b->dItems;
+    w.seg = b->dSegs + L;
+    w.cursor = b->dCursors + L;
+    const int maxItems = graphForm ? 0x7fffffff : (int)r.seg.count;
+    switch (r.kind) {
+      case LK_ZERO: launch_zero_stats_b(w, d.statsOut, st); break;
+      case LK_KEY: launch_key_count_b(w, maxItems, d, st); break;
+      case LK_SCAN:
+        BTRY(b, cudaMemsetAsync(d.scanState, 0, (graphForm ? (size_t)b->scanTilesCap : r.seg.count) * 8, st));
+        launch_scan_b(w, maxItems, d, 1u, st);
+        break;
+      case LK_FILL: launch_fill_b(w, maxItems, d, st); break;
+      case LK_REORDER: launch_reorder_b(w, maxItems, d, st); break;
+      case LK_SEED: launch_body_seed_b(w, maxItems, d, st); break;
+      case LK_LAMBDA: launch_lambda_b(w, maxItems, d, r.it, st, F.variant[TK_LAMBDA]); break;
+      case LK_DELTA: launch_delta_b(w, maxItems, d, r.it, st, F.variant[TK_DELTA]); break;
+      case LK_MATCH: launch_body_match_b(w, maxItems, d, r.it, st); break;
+      case LK_FINISH: launch_xsph_finalize_b(w, maxItems, d, r.sub, st); break;
+      case LK_NORMALS: launch_xsph_normals_b(w, maxItems, d, st, F.variant[TK_NORMALS]); break;
+      case LK_TENSION: launch_tension_finalize_b(w, maxItems, d, r.sub, st); break;
     }
-    launch_fill_b(at(u.part), u.part.count, d, st);
-    launch_reorder_b(at(u.part), u.part.count, d, st);
-    launch_body_seed_b(at(u.seed), u.seed.count, d, st);
-    for (int it = 0; it < (int)u.iter.size(); it++) {
-      launch_lambda_b(at(u.iter[it]), u.iter[it].count, d, it, st);
-      launch_delta_b(at(u.iter[it]), u.iter[it].count, d, it, st);
-      launch_body_match_b(at(u.bodyIter[it]), u.bodyIter[it].count, d, it, st);
-    }
-    launch_xsph_finalize_b(at(u.finishPlain), u.finishPlain.count, d, (int)s, st);
-    launch_xsph_normals_b(at(u.finishTension), u.finishTension.count, d, st);
-    launch_tension_finalize_b(at(u.finishTension), u.finishTension.count, d, (int)s, st);
+    n++;
   }
   BTRY(b, cudaGetLastError());
+  if (launched) *launched = n;
   return P4A_OK;
 }
 
-__global__ void k_zero_stats(uint32_t* __restrict__ stats, const uint2* __restrict__ items, int count) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < count * 8) stats[items[t / 8].x * 8 + (t % 8)] = 0u;
+void drop_graphs(p4a_batch* b) {
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
 }
 
-int ensure_items(p4a_batch* b, int64_t nItems) {
-  if (nItems <= b->itemsCap) return P4A_OK;
+int ensure_device_lists(p4a_batch* b, int64_t nItems, int64_t nLaunches) {
+  if (nItems <= b->itemsCap && nLaunches <= b->launchCap) return P4A_OK;
   BTRY(b, cudaStreamSynchronize(b->stream));
-  if (b->dItems) {
-    cudaFree(b->dItems);
+  drop_graphs(b);  // graphs hold the old addresses
+  if (nItems > b->itemsCap) {
+    if (b->dItems) cudaFree(b->dItems);
     b->dItems = nullptr;
+    const int64_t cap = std::max<int64_t>(nItems * 2, 4096);
+    BTRY(b, cudaMalloc((void**)&b->dItems, (size_t)cap * sizeof(uint2)));
+    b->itemsCap = cap;
   }
-  const int64_t cap = std::max<int64_t>(nItems * 2, 4096);
-  BTRY(b, cudaMalloc((void**)&b->dItems, (size_t)cap * sizeof(uint2)));
-  b->itemsCap = cap;
-  if (b->graph) {
-    cudaGraphExecDestroy(b->graph);
-    b->graph = nullptr;
-    b->graphKey.clear();
+  if (nLaunches > b->launchCap) {
+    if (b->dSegs) cudaFree(b->dSegs);
+    if (b->dCursors) cudaFree(b->dCursors);
+    b->dSegs = nullptr;
+    b->dCursors = nullptr;
+    const int64_t cap = std::max<int64_t>(nLaunches * 2, 256);
+    BTRY(b, cudaMalloc((void**)&b->dSegs, (size_t)cap * sizeof(WorkSeg)));
+    BTRY(b, cudaMalloc((void**)&b->dCursors, (size_t)cap * sizeof(uint32_t)));
+    b->launchCap = cap;
   }
   return P4A_OK;
 }
@@ -344,51 +233,56 @@ int ensure_staging(p4a_batch* b, size_t bytes) {
   return P4A_OK;
 }
 
-// Uploads params tables + items and runs the frame (graph replay when the
-// schedule's shape is unchanged). zeroItems lists the scenes whose stats restart.
-int execute(p4a_batch* b, const Schedule& sch, const std::vector<SimParams>& params, int nSlots,
-            const Seg& zeroSeg, const std::vector<int64_t>& key) {
-  const size_t pBytes = params.size() * sizeof(SimParams);
-  const size_t iBytes = sch.items.size() * sizeof(uint2);
+// Uploads the frame's params rows, items and segments, then runs it: a replay of
+// the graph of its shape when graphs are on (captured on first use).
+int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
+  const size_t rowBytes = (size_t)F.nRows * sizeof(SimParams);
+  const size_t pBytes = rowBytes * F.nSubs;
+  const size_t iBytes = F.items.size() * sizeof(uint2);
+  const size_t sBytes = F.launches.size() * sizeof(WorkSeg);
   int rc;
-  if ((rc = ensure_items(b, (int64_t)sch.items.size()))) return rc;
-  if ((rc = ensure_staging(b, pBytes + iBytes))) return rc;
+  if ((rc = ensure_device_lists(b, (int64_t)F.items.size(), (int64_t)F.launches.size()))) return rc;
+  if ((rc = ensure_staging(b, pBytes + iBytes + sBytes))) return rc;
   const int k = b->stagingIdx;
   b->stagingIdx ^= 1;
-  BTRY(b, cudaEventSynchronize(b->stagingDone[k]));  // the copy two frames ago has finished
-  std::memcpy(b->staging[k], params.data(), pBytes);
-  std::memcpy(b->staging[k] + pBytes, sch.items.data(), iBytes);
-  BTRY(b, cudaMemcpyAsync(b->dParams, b->staging[k], pBytes, cudaMemcpyHostToDevice, b->stream));
-  BTRY(b, cudaMemcpyAsync(b->dItems, b->staging[k] + pBytes, iBytes, cudaMemcpyHostToDevice, b->stream));
+  BTRY(b, cudaEventSynchronize(b->stagingDone[k]));  // the upload two frames ago has finished
+  unsigned char* h = b->staging[k];
+  std::memcpy(h, F.params.data(), pBytes);
+  std::memcpy(h + pBytes, F.items.data(), iBytes);
+  WorkSeg* segs = reinterpret_cast<WorkSeg*>(h + pBytes + iBytes);
+  for (size_t L = 0; L < F.launches.size(); L++) segs[L] = F.launches[L].seg;
+  for (int s = 0; s < F.nSubs; s++)
+    BTRY(b, cudaMemcpyAsync(b->dParams + (size_t)s * b->cfg.max_scenes, h + rowBytes * s, rowBytes,
+                            cudaMemcpyHostToDevice, b->stream));
+  if (iBytes) BTRY(b, cudaMemcpyAsync(b->dItems, h + pBytes, iBytes, cudaMemcpyHostToDevice, b->stream));
+  BTRY(b, cudaMemcpyAsync(b->dSegs, segs, sBytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaEventRecord(b->stagingDone[k], b->stream));
-  count_launches(frame_kernels(sch) + (zeroSeg.count > 0 ? 1 : 0));
-  auto body = [&]() -> int {
-    if (zeroSeg.count > 0)
-      k_zero_stats<<<(zeroSeg.count * 8 + 255) / 256, 256, 0, b->stream>>>(b->d.statsOut, b->dItems + zeroSeg.off,
-                                                                           zeroSeg.count);
-    return run_frame(b, sch, nSlots);
-  };
-  if (!b->useGraphs) return body();
-  if (!b->graph || b->graphKey != key) {
-    if (b->graph) {
-      cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
-    }
+  if (!(allowGraph && b->useGraphs)) {
+    uint64_t n = 0;
+    rc = run_frame(b, F, false, &n);
+    count_launches(n);
+    return rc;
+  }
+  auto it = b->graphs.find(F.shape);
+  if (it == b->graphs.end()) {
+    if (b->graphs.size() >= 16) drop_graphs(b);
     cudaGraph_t g = nullptr;
     BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const int brc = body();
+    const int brc = run_frame(b, F, true, nullptr);
     const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
     if (brc) {
       if (g) cudaGraphDestroy(g);
       return brc;
     }
     if (ec != cudaSuccess) return bfail(b, P4A_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
-    const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphExec_t ge = nullptr;
+    const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
     if (ei != cudaSuccess) return bfail(b, P4A_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
-    b->graphKey = key;
+    it = b->graphs.emplace(F.shape, ge).first;
   }
-  BTRY(b, cudaGraphLaunch(b->graph, b->stream));
+  BTRY(b, cudaGraphLaunch(it->second, b->stream));
+  count_launches(F.launches.size());
   return P4A_OK;
 }
 
@@ -399,19 +293,28 @@ int scene_ok(p4a_batch* b, int32_t id) {
   return P4A_OK;
 }
 
-// Admits a host scene: arena ranges, uploads, prime (src/sim.js:66-253).
-int admit(p4a_batch* b, const p4a_params& params, HostScene& sc, int pourBudget, int32_t* outId) {
-  int slot = -1;
-  for (int k = 0; k < (int)b->scenes.size(); k++)
-    if (!b->scenes[k].live) {
-      slot = k;
-      break;
-    }
-  if (slot < 0) return bfail(b, P4A_ERR_CAPACITY, "all %d scene slots are in use", b->cfg.max_scenes);
-  BScene s;
+}  // namespace
+
+namespace p4a {
+
+void release_scene(p4a_batch* b, BScene& s) {
+  if (s.part.off >= 0) b->partA.release(s.part.off, s.part.size);
+  if (s.cells.off >= 0) b->cellA.release(s.cells.off, s.cells.size);
+  if (s.bodies.off >= 0) b->bodyA.release(s.bodies.off, s.bodies.size);
+  if (s.list.off >= 0) b->listA.release(s.list.off, s.list.size);
+  if (s.bound.off >= 0) b->boundA.release(s.bound.off, s.bound.size);
+  s = BScene();
+}
+
+static size_t a16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+int prepare_scene(const p4a_params& params, HostScene& sc, int pourBudget, PreparedScene& ps,
+                  std::string& err) {
+  BScene& s = ps.s;
+  s = BScene();
   s.params = params;
   s.specs.assign(params.bodies, params.bodies + (params.bodies ? params.n_bodies : 0));
-  s.params.bodies = s.specs.empty() ? nullptr : s.specs.data();
+  s.params.bodies = nullptr;  // re-pointed at s.specs when the scene is placed
   s.params.n_bodies = (int32_t)s.specs.size();
   s.h = sc.h;
   s.mass = sc.mass;
@@ -420,12 +323,93 @@ int admit(p4a_batch* b, const p4a_params& params, HostScene& sc, int pourBudget,
   s.nFluid = sc.nFluid;
   s.cap = sc.n + std::max(0, pourBudget);
   for (int k = 0; k < 3; k++) s.gridDim[k] = (int)std::max(1.0, std::floor(params.box[k] / s.h));
+  const double cells = (double)s.gridDim[0] * s.gridDim[1] * s.gridDim[2];
+  if (cells > 0x7fff0000) {
+    err = "scene grid has too many cells";
+    return P4A_ERR_CAPACITY;
+  }
   s.nCells = s.gridDim[0] * s.gridDim[1] * s.gridDim[2];
   s.nBodies = (int)sc.bodyDensity.size();
   s.nBodyParts = sc.nBody;
-  HostBoundary hb;
-  build_boundary(params.box, params.rest_density, params.spacing, s.h, s.gridDim, hb);
-  s.nBoundary = hb.count;
+  build_boundary(params.box, params.rest_density, params.spacing, s.h, s.gridDim, ps.hb);
+  s.nBoundary = ps.hb.count;
+  // counts and fixed-point scales (src/sim.js:163-171)
+  ps.bodyCounts.assign(s.nBodies, 0);
+  for (int i = 0; i < s.n; i++) {
+    const uint32_t id = sc.phase[(size_t)i * 4];
+    if (id >= 1 && (int)id <= s.nBodies) ps.bodyCounts[id - 1]++;
+  }
+  double maxCount = 1, maxRest = 1e-3;
+  for (int k = 0; k < s.nBodies; k++) maxCount = std::max(maxCount, (double)ps.bodyCounts[k]);
+  for (int i = 0; i < s.n; i++) {
+    const double r = std::hypot((double)sc.rest[(size_t)i * 4], (double)sc.rest[(size_t)i * 4 + 1],
+                                (double)sc.rest[(size_t)i * 4 + 2]);
+    if (r > maxRest) maxRest = r;
+  }
+  const double extent = std::max(params.box[0], std::max(params.box[1], params.box[2]));
+  s.bodyScale = 1e9 / (extent * maxCount);
+  s.covScale = 1e9 / (extent * maxRest * maxCount);
+  // blob layout
+  ps.nb1 = s.nBodies + 1;
+  const size_t n16 = (size_t)s.n * 16;
+  size_t o = 0;
+  ps.oPos = o; o = a16(o + n16);
+  ps.oVel = o; o = a16(o + n16);
+  ps.oPhase = o; o = a16(o + n16);
+  ps.oRest = o; o = a16(o + n16);
+  ps.oBpos = o; o = a16(o + ps.hb.pos.size() * 4);
+  ps.oBpsi = o; o = a16(o + ps.hb.psi.size() * 4);
+  ps.oBcs = o; o = a16(o + ps.hb.cellStart.size() * 4);
+  ps.oInfo = o; o = a16(o + (size_t)ps.nb1 * 16);
+  ps.oCentre = o; o = a16(o + (size_t)ps.nb1 * 16);
+  ps.oRot = o; o = a16(o + (size_t)ps.nb1 * 48);
+  ps.oBstart = o; o = a16(o + (size_t)ps.nb1 * 4);
+  ps.bytes = o;
+  ps.sc = std::move(sc);  // the particle arrays, until write_blob
+  return P4A_OK;
+}
+
+void write_blob(const PreparedScene& ps, unsigned char* blob) {
+  const BScene& s = ps.s;
+  const HostScene& sc = ps.sc;
+  const size_t n16 = (size_t)s.n * 16;
+  if (n16) {
+    std::memcpy(blob + ps.oPos, sc.pos.data(), n16);
+    std::memcpy(blob + ps.oVel, sc.vel.data(), n16);
+    std::memcpy(blob + ps.oPhase, sc.phase.data(), n16);
+    std::memcpy(blob + ps.oRest, sc.rest.data(), n16);
+  }
+  std::memcpy(blob + ps.oBpos, ps.hb.pos.data(), ps.hb.pos.size() * 4);
+  std::memcpy(blob + ps.oBpsi, ps.hb.psi.data(), ps.hb.psi.size() * 4);
+  std::memcpy(blob + ps.oBcs, ps.hb.cellStart.data(), ps.hb.cellStart.size() * 4);
+  // bodies (src/sim.js:129-161); bodyStart relative to the scene's list range
+  float* info = reinterpret_cast<float*>(blob + ps.oInfo);
+  float* centre = reinterpret_cast<float*>(blob + ps.oCentre);
+  float* rot = reinterpret_cast<float*>(blob + ps.oRot);
+  uint32_t* bstart = reinterpret_cast<uint32_t*>(blob + ps.oBstart);
+  std::memset(info, 0, (size_t)ps.nb1 * 16);
+  std::memset(centre, 0, (size_t)ps.nb1 * 16);
+  std::memset(rot, 0, (size_t)ps.nb1 * 48);
+  uint32_t run = 0;
+  for (int k = 0; k < s.nBodies; k++) {
+    info[k * 4] = (float)(1 / std::max(1e-6, sc.bodyDensity[k]));
+    for (int c = 0; c < 3; c++) centre[k * 4 + c] = (float)sc.bodyCentre[k * 3 + c];
+    for (int r = 0; r < 3; r++) rot[k * 12 + r * 4 + r] = 1.0f;
+    bstart[k] = run;
+    run += (uint32_t)ps.bodyCounts[k];
+  }
+  bstart[s.nBodies] = run;
+}
+
+int place_scene(p4a_batch* b, PreparedScene& ps, unsigned char* blob, cudaStream_t st, int32_t* outSlot) {
+  int slot = -1;
+  for (int k = 0; k < (int)b->scenes.size(); k++)
+    if (!b->scenes[k].live) {
+      slot = k;
+      break;
+    }
+  if (slot < 0) return bfail(b, P4A_ERR_CAPACITY, "all %d scene slots are in use", b->cfg.max_scenes);
+  BScene s = ps.s;
   // arena ranges (nothing is kept if any arena is full)
   const int64_t cellsPadded = (int64_t)((s.nCells + 2 + kScanTile - 1) / kScanTile) * kScanTile;
   s.part = {b->partA.alloc(std::max(1, s.cap), kBlock), std::max(1, s.cap)};
@@ -436,105 +420,228 @@ int admit(p4a_batch* b, const p4a_params& params, HostScene& sc, int pourBudget,
   if (s.part.off < 0 || s.cells.off < 0 || s.bodies.off < 0 || s.list.off < 0 || s.bound.off < 0) {
     const bool p = s.part.off < 0, c = s.cells.off < 0;
     release_scene(b, s);
-    return bfail(b, P4A_ERR_CAPACITY, "no room for a %d-particle scene (%s full)", sc.n,
+    return bfail(b, P4A_ERR_CAPACITY, "no room for a %d-particle scene (%s full)", s.n,
                  p ? "particle arena" : c ? "cell arena" : "body/boundary arena");
   }
-  // counts and fixed-point scales (src/sim.js:163-171)
-  std::vector<int> counts(s.nBodies, 0);
-  for (int i = 0; i < s.n; i++) {
-    const uint32_t id = sc.phase[(size_t)i * 4];
-    if (id >= 1 && (int)id <= s.nBodies) counts[id - 1]++;
-  }
-  double maxCount = 1, maxRest = 1e-3;
-  for (int k = 0; k < s.nBodies; k++) maxCount = std::max(maxCount, (double)counts[k]);
-  for (int i = 0; i < s.n; i++) {
-    const double r = std::hypot((double)sc.rest[(size_t)i * 4], (double)sc.rest[(size_t)i * 4 + 1],
-                                (double)sc.rest[(size_t)i * 4 + 2]);
-    if (r > maxRest) maxRest = r;
-  }
-  const double extent = std::max(params.box[0], std::max(params.box[1], params.box[2]));
-  s.bodyScale = 1e9 / (extent * maxCount);
-  s.covScale = 1e9 / (extent * maxRest * maxCount);
+  // arena offsets into the blob's index-valued pieces
+  uint32_t* bcs = reinterpret_cast<uint32_t*>(blob + ps.oBcs);
+  for (size_t k = 0; k < ps.hb.cellStart.size(); k++) bcs[k] += (uint32_t)s.bound.off;
+  uint32_t* bstart = reinterpret_cast<uint32_t*>(blob + ps.oBstart);
+  for (int k = 0; k < ps.nb1; k++) bstart[k] += (uint32_t)s.list.off;
   DevScene& d = b->d;
-  cudaStream_t st = b->stream;
   // particles into parity 0 of the range; everything else of the range cleared
-  const size_t po = (size_t)s.part.off, nb = (size_t)s.n * 16;
+  const size_t po = (size_t)s.part.off, nb = (size_t)s.n * 16, pr = (size_t)s.part.size * 16;
   for (int t = 0; t < 2; t++) {
-    BTRY(b, cudaMemsetAsync(d.pos[t] + po, 0, (size_t)s.part.size * 16, st));
-    BTRY(b, cudaMemsetAsync(d.vel[t] + po, 0, (size_t)s.part.size * 16, st));
-    BTRY(b, cudaMemsetAsync(d.pred[t] + po, 0, (size_t)s.part.size * 16, st));
-    BTRY(b, cudaMemsetAsync(d.body[t] + po, 0, (size_t)s.part.size * 16, st));
-    BTRY(b, cudaMemsetAsync(d.rest[t] + po, 0, (size_t)s.part.size * 16, st));
+    BTRY(b, cudaMemsetAsync(d.pos[t] + po, 0, pr, st));
+    BTRY(b, cudaMemsetAsync(d.vel[t] + po, 0, pr, st));
+    BTRY(b, cudaMemsetAsync(d.pred[t] + po, 0, pr, st));
+    BTRY(b, cudaMemsetAsync(d.body[t] + po, 0, pr, st));
+    BTRY(b, cudaMemsetAsync(d.rest[t] + po, 0, pr, st));
   }
-  if (s.n > 0) {
-    BTRY(b, cudaMemcpyAsync(d.pos[0] + po, sc.pos.data(), nb, cudaMemcpyHostToDevice, st));
-    BTRY(b, cudaMemcpyAsync(d.vel[0] + po, sc.vel.data(), nb, cudaMemcpyHostToDevice, st));
-    BTRY(b, cudaMemcpyAsync(d.pred[0] + po, sc.pos.data(), nb, cudaMemcpyHostToDevice, st));
-    BTRY(b, cudaMemcpyAsync(d.body[0] + po, sc.phase.data(), nb, cudaMemcpyHostToDevice, st));
-    BTRY(b, cudaMemcpyAsync(d.rest[0] + po, sc.rest.data(), nb, cudaMemcpyHostToDevice, st));
+  if (nb) {
+    BTRY(b, cudaMemcpyAsync(d.pos[0] + po, blob + ps.oPos, nb, cudaMemcpyHostToDevice, st));
+    BTRY(b, cudaMemcpyAsync(d.vel[0] + po, blob + ps.oVel, nb, cudaMemcpyHostToDevice, st));
+    BTRY(b, cudaMemcpyAsync(d.pred[0] + po, blob + ps.oPos, nb, cudaMemcpyHostToDevice, st));
+    BTRY(b, cudaMemcpyAsync(d.body[0] + po, blob + ps.oPhase, nb, cudaMemcpyHostToDevice, st));
+    BTRY(b, cudaMemcpyAsync(d.rest[0] + po, blob + ps.oRest, nb, cudaMemcpyHostToDevice, st));
   }
   // boundary samples and their cellStart in arena indices
-  std::vector<uint32_t> bcs(hb.cellStart);
-  for (auto& v : bcs) v += (uint32_t)s.bound.off;
-  BTRY(b, cudaMemcpyAsync(d.bpos + s.bound.off, hb.pos.data(), hb.pos.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bpsi + s.bound.off, hb.psi.data(), hb.psi.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bcellStart + s.cells.off, bcs.data(), bcs.size() * 4, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bpos + s.bound.off, blob + ps.oBpos, ps.hb.pos.size() * 4, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bpsi + s.bound.off, blob + ps.oBpsi, ps.hb.psi.size() * 4, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bcellStart + s.cells.off, blob + ps.oBcs, ps.hb.cellStart.size() * 4,
+                          cudaMemcpyHostToDevice, st));
   BTRY(b, cudaMemsetAsync(d.cellStart + s.cells.off, 0, (size_t)(s.nCells + 2) * 4, st));
-  // bodies (src/sim.js:129-161)
-  const int nb1 = s.nBodies + 1;
-  std::vector<float> info((size_t)nb1 * 4, 0.0f), centre((size_t)nb1 * 4, 0.0f), rot((size_t)nb1 * 12, 0.0f);
-  std::vector<uint32_t> bstart((size_t)nb1, 0u);
-  uint32_t run = (uint32_t)s.list.off;
-  for (int k = 0; k < s.nBodies; k++) {
-    info[k * 4] = (float)(1 / std::max(1e-6, sc.bodyDensity[k]));
-    for (int c = 0; c < 3; c++) centre[k * 4 + c] = (float)sc.bodyCentre[k * 3 + c];
-    for (int r = 0; r < 3; r++) rot[k * 12 + r * 4 + r] = 1.0f;
-    bstart[k] = run;
-    run += (uint32_t)counts[k];
-  }
-  bstart[s.nBodies] = run;
-  const size_t bo = (size_t)s.bodies.off;
-  BTRY(b, cudaMemcpyAsync(d.bodyInfo + bo, info.data(), info.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bodyCentre + bo, centre.data(), centre.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bodyRef + bo, centre.data(), centre.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bodyRot + bo, rot.data(), rot.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemcpyAsync(d.bodyStart + bo, bstart.data(), bstart.size() * 4, cudaMemcpyHostToDevice, st));
-  BTRY(b, cudaMemsetAsync(d.bodyAccum + bo * 4, 0, (size_t)nb1 * 16, st));
-  BTRY(b, cudaMemsetAsync(d.bodyCov + bo * 9, 0, (size_t)nb1 * 36, st));
-  BTRY(b, cudaMemsetAsync(d.bodyFill + bo, 0, (size_t)nb1 * 4, st));
+  const size_t bo = (size_t)s.bodies.off, nb1 = (size_t)ps.nb1;
+  BTRY(b, cudaMemcpyAsync(d.bodyInfo + bo, blob + ps.oInfo, nb1 * 16, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bodyCentre + bo, blob + ps.oCentre, nb1 * 16, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bodyRef + bo, blob + ps.oCentre, nb1 * 16, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bodyRot + bo * 3, blob + ps.oRot, nb1 * 48, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemcpyAsync(d.bodyStart + bo, blob + ps.oBstart, nb1 * 4, cudaMemcpyHostToDevice, st));
+  BTRY(b, cudaMemsetAsync(d.bodyAccum + bo * 4, 0, nb1 * 16, st));
+  BTRY(b, cudaMemsetAsync(d.bodyCov + bo * 9, 0, nb1 * 36, st));
+  BTRY(b, cudaMemsetAsync(d.bodyFill + bo, 0, nb1 * 4, st));
   BTRY(b, cudaMemsetAsync(d.statsOut + (size_t)slot * 8, 0, 32, st));
-  // primeGrid (src/sim.js:223-253): a grid pass with dt = 0 from parity 0
   s.parity = 0;
   s.live = true;
-  pack(s, 0.0, slot);
+  s.primed = false;
   b->scenes[slot] = std::move(s);
   BScene& S = b->scenes[slot];
-  S.specs.assign(params.bodies, params.bodies + (params.bodies ? params.n_bodies : 0));
   S.params.bodies = S.specs.empty() ? nullptr : S.specs.data();
-  Schedule sch;
-  sch.subs.resize(1);
-  const int64_t keyTiles = groups(std::max(S.n, S.nBodies));
-  sch.subs[0].key = push_tiles(sch.items, (uint32_t)slot, keyTiles);
-  sch.subs[0].scan = push_tiles(sch.items, (uint32_t)slot, scan_tiles(S.nCells));
-  sch.subs[0].part = push_tiles(sch.items, (uint32_t)slot, groups(S.n));
-  std::vector<SimParams> params1((size_t)slot + 1);
-  params1[slot] = S.P;
-  const bool graphs = b->useGraphs;
-  b->useGraphs = false;
-  const int rc = execute(b, sch, params1, slot + 1, Seg{}, {});
-  b->useGraphs = graphs;
+  *outSlot = slot;
+  return P4A_OK;
+}
+
+int prime_scenes(p4a_batch* b, const std::vector<int>& slots) {
+  if (slots.empty()) return P4A_OK;
+  Frame F;
+  F.nSubs = 1;
+  F.nRows = (int)slots.size();
+  F.params.resize(slots.size());
+  WorkSeg key{0, 0}, scan{0, 0}, part{0, 0};
+  for (size_t k = 0; k < slots.size(); k++) {
+    BScene& S = b->scenes[slots[k]];
+    S.parity = 0;
+    pack(S, 0.0, slots[k]);
+    F.params[k] = S.P;
+  }
+  for (size_t k = 0; k < slots.size(); k++) {
+    const BScene& S = b->scenes[slots[k]];
+    key = push_items(F, (uint32_t)k, groups(std::max(S.n, S.nBodies)), key);
+  }
+  for (size_t k = 0; k < slots.size(); k++) scan = push_items(F, (uint32_t)k, scan_tiles(b->scenes[slots[k]].nCells), scan);
+  for (size_t k = 0; k < slots.size(); k++) part = push_items(F, (uint32_t)k, groups(b->scenes[slots[k]].n), part);
+  add_launch(F, LK_KEY, 0, 0, key);
+  add_launch(F, LK_SCAN, 0, 0, scan);
+  add_launch(F, LK_FILL, 0, 0, part);
+  add_launch(F, LK_REORDER, 0, 0, part);
+  const int rc = execute(b, F, false);
+  if (rc) return rc;
+  for (int slot : slots) {
+    BScene& S = b->scenes[slot];
+    S.parity = 1;
+    S.primed = true;
+    S.gen++;
+  }
+  return P4A_OK;
+}
+
+int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t count) {
+  std::vector<int> subs(count, 0);
+  int maxSub = 0;
+  for (int k = 0; k < count; k++) {
+    BScene& s = b->scenes[ids[k]];
+    // time bank (src/sim.js:418-429)
+    const int base = std::max(1, s.params.substeps);
+    const double dtTarget = (1.0 / 60) / base;
+    s.timeBank = s.timeBank + frameDt[k];
+    double subD = std::floor(s.timeBank / dtTarget + 1e-4);
+    const double workCap = base * 8;
+    if (subD > workCap) {
+      subD = workCap;
+      s.timeBank = 0;
+    } else {
+      s.timeBank -= subD * dtTarget;
+    }
+    subs[k] = std::min((int)subD, kMaxSubsteps);
+    s.lastSubsteps = subs[k];
+    s.lastAdvanced = subs[k] < 1 ? 0 : subD * dtTarget;
+    maxSub = std::max(maxSub, subs[k]);
+  }
+  if (maxSub == 0) return P4A_OK;
+  Frame F;
+  F.nSubs = maxSub;
+  F.nRows = count;
+  F.params.resize((size_t)maxSub * count);
+  int64_t total = 0;
+  for (int k = 0; k < count; k++) total += b->scenes[ids[k]].n;
+  for (int k = 0; k < TK_COUNT; k++) {
+    F.variant[k] = tuned_variant(k, total);
+    F.shape.push_back(F.variant[k]);
+  }
+  F.shape.push_back(maxSub);
+  WorkSeg zero{0, 0};
+  for (int k = 0; k < count; k++)
+    if (subs[k] > 0) zero = push_items(F, (uint32_t)k, 1, zero);
+  add_launch(F, LK_ZERO, 0, 0, zero);
+  std::map<std::vector<int64_t>, WorkSeg> segCache;
+  for (int s = 0; s < maxSub; s++) {
+    int maxIt = 0;
+    for (int k = 0; k < count; k++)
+      if (subs[k] > s) maxIt = std::max(maxIt, std::max(1, b->scenes[ids[k]].params.iterations));
+    F.shape.push_back(maxIt);
+    // launches with the same (scene, item count) list share one segment of items
+    auto seg = [&](auto&& countOf) {
+      std::vector<int64_t> sig;
+      for (int k = 0; k < count; k++) {
+        if (subs[k] <= s) continue;
+        const int64_t c = countOf(b->scenes[ids[k]]);
+        if (c > 0) sig.insert(sig.end(), {(int64_t)k, c});
+      }
+      auto hit = segCache.find(sig);
+      if (hit != segCache.end()) return hit->second;
+      WorkSeg g{0, 0};
+      for (size_t q = 0; q < sig.size(); q += 2) g = push_items(F, (uint32_t)sig[q], sig[q + 1], g);
+      segCache.emplace(std::move(sig), g);
+      return g;
+    };
+    const WorkSeg key = seg([](const BScene& S) { return (int64_t)groups(std::max(S.n, S.nBodies)); });
+    const WorkSeg scan = seg([](const BScene& S) { return (int64_t)scan_tiles(S.nCells); });
+    const WorkSeg part = seg([](const BScene& S) { return (int64_t)groups(S.n); });
+    const WorkSeg seed = seg([](const BScene& S) { return (int64_t)(S.nBodyParts > 0 ? S.nBodies : 0); });
+    add_launch(F, LK_KEY, s, 0, key);
+    add_launch(F, LK_SCAN, s, 0, scan);
+    add_launch(F, LK_FILL, s, 0, part);
+    add_launch(F, LK_REORDER, s, 0, part);
+    add_launch(F, LK_SEED, s, 0, seed);
+    for (int it = 0; it < maxIt; it++) {
+      const WorkSeg iter = seg([&](const BScene& S) {
+        return (int64_t)(std::max(1, S.params.iterations) > it ? groups(S.n) : 0);
+      });
+      const WorkSeg match = seg([&](const BScene& S) {
+        return (int64_t)(std::max(1, S.params.iterations) > it && S.nBodyParts > 0 ? S.nBodies : 0);
+      });
+      add_launch(F, LK_LAMBDA, s, it, iter);
+      add_launch(F, LK_DELTA, s, it, iter);
+      add_launch(F, LK_MATCH, s, it, match);
+    }
+    const WorkSeg plain = seg([](const BScene& S) {
+      return (int64_t)(S.params.surface_tension_k > 0 ? 0 : groups(S.n));
+    });
+    const WorkSeg tension = seg([](const BScene& S) {
+      return (int64_t)(S.params.surface_tension_k > 0 ? groups(S.n) : 0);
+    });
+    add_launch(F, LK_FINISH, s, 0, plain);
+    add_launch(F, LK_NORMALS, s, 0, tension);
+    add_launch(F, LK_TENSION, s, 0, tension);
+    for (int k = 0; k < count; k++) {
+      if (subs[k] <= s) continue;
+      BScene& S = b->scenes[ids[k]];
+      const double dt = (1.0 / 60) / std::max(1, S.params.substeps);
+      pack(S, dt, ids[k]);
+      S.P.parity = (uint32_t)(S.parity ^ (s & 1));
+      S.P.subs = (uint32_t)subs[k];
+      F.params[(size_t)s * count + k] = S.P;
+    }
+  }
+  const int rc = execute(b, F, true);
+  if (rc) return rc;
+  for (int k = 0; k < count; k++) {
+    BScene& S = b->scenes[ids[k]];
+    if (subs[k] < 1) continue;
+    S.parity ^= (subs[k] & 1);
+    S.simTime += subs[k] * ((1.0 / 60) / std::max(1, S.params.substeps));
+    S.statsValid = true;
+  }
+  return P4A_OK;
+}
+
+}  // namespace p4a
+
+namespace {
+
+// Admits a host scene on the batch's stream and waits for it (src/sim.js:66-253).
+int admit(p4a_batch* b, const p4a_params& params, HostScene& sc, int pourBudget, int32_t* outId) {
+  PreparedScene ps;
+  std::string err;
+  int rc = prepare_scene(params, sc, pourBudget, ps, err);
+  if (rc) return bfail(b, rc, "%s", err.c_str());
+  std::vector<unsigned char> blob(ps.bytes);
+  write_blob(ps, blob.data());
+  int32_t slot = -1;
+  if ((rc = place_scene(b, ps, blob.data(), b->stream, &slot))) return rc;
+  rc = prime_scenes(b, {slot});
   if (rc) {
-    release_scene(b, S);
+    cudaStreamSynchronize(b->stream);
+    release_scene(b, b->scenes[slot]);
     return rc;
   }
-  BTRY(b, cudaStreamSynchronize(st));  // host vectors above go out of scope
-  S.parity = 1;
-  S.gen++;
+  BTRY(b, cudaStreamSynchronize(b->stream));  // the blob goes out of scope
   *outId = slot;
   return P4A_OK;
 }
 
 }  // namespace
+
 
 extern "C" {
 
@@ -603,9 +710,12 @@ int p4a_batch_destroy(p4a_batch* b) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  if (b->graph) cudaGraphExecDestroy(b->graph);
+  drop_graphs(b);
   for (void* p : b->allocs) cudaFree(p);
   if (b->dItems) cudaFree(b->dItems);
+  if (b->dSegs) cudaFree(b->dSegs);
+  if (b->dCursors) cudaFree(b->dCursors);
+  if (b->upStream) cudaStreamDestroy(b->upStream);
   for (int k = 0; k < 2; k++) {
     if (b->staging[k]) cudaFreeHost(b->staging[k]);
     if (b->stagingDone[k]) cudaEventDestroy(b->stagingDone[k]);
@@ -621,11 +731,7 @@ int p4a_batch_set_stream(p4a_batch* b, void* stream) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   BTRY(b, cudaStreamSynchronize(b->stream));
-  if (b->graph) {
-    cudaGraphExecDestroy(b->graph);
-    b->graph = nullptr;
-    b->graphKey.clear();
-  }
+  drop_graphs(b);
   if (stream) {
     if (b->ownStream) cudaStreamDestroy(b->stream);
     b->stream = (cudaStream_t)stream;
@@ -694,101 +800,14 @@ int p4a_batch_remove_scene(p4a_batch* b, int32_t id) {
 int p4a_batch_step(p4a_batch* b, const int32_t* ids, int32_t count, double frameDt) {
   if (!b || count < 0 || (count > 0 && !ids)) return bfail(b, P4A_ERR_ARG, "p4a_batch_step: bad list");
   cudaSetDevice(b->device);
-  int nSlots = 0;
-  std::vector<int> subs(count, 0);
-  int maxSub = 0;
+  std::vector<char> seen(b->scenes.size(), 0);
   for (int k = 0; k < count; k++) {
-    int rc = scene_ok(b, ids[k]);
+    const int rc = scene_ok(b, ids[k]);
     if (rc) return rc;
-    BScene& s = b->scenes[ids[k]];
-    // time bank (src/sim.js:418-429)
-    const int base = std::max(1, s.params.substeps);
-    const double dtTarget = (1.0 / 60) / base;
-    s.timeBank = s.timeBank + frameDt;
-    double subD = std::floor(s.timeBank / dtTarget + 1e-4);
-    const double workCap = base * 8;
-    if (subD > workCap) {
-      subD = workCap;
-      s.timeBank = 0;
-    } else {
-      s.timeBank -= subD * dtTarget;
-    }
-    subs[k] = std::min((int)subD, kMaxSubsteps);
-    s.lastSubsteps = subs[k];
-    s.lastAdvanced = subs[k] < 1 ? 0 : subD * dtTarget;
-    maxSub = std::max(maxSub, subs[k]);
-    nSlots = std::max(nSlots, ids[k] + 1);
+    if (seen[ids[k]]++) return bfail(b, P4A_ERR_ARG, "p4a_batch_step: scene %d listed twice", ids[k]);
   }
-  if (maxSub == 0) return P4A_OK;
-  // schedule and per-substep params
-  Schedule sch;
-  sch.subs.resize(maxSub);
-  std::vector<SimParams> params((size_t)maxSub * nSlots);
-  std::vector<int64_t> key;
-  key.push_back(nSlots);
-  Seg zero;
-  zero.off = 0;
-  for (int k = 0; k < count; k++)
-    if (subs[k] > 0) append_to(zero, sch.items, (uint32_t)ids[k], 1);
-  // items of zero are (slot, 0): the zero kernel reads .x only
-  for (int s = 0; s < maxSub; s++) {
-    Schedule::Sub& u = sch.subs[s];
-    int maxIt = 0;
-    for (int k = 0; k < count; k++)
-      if (subs[k] > s) maxIt = std::max(maxIt, std::max(1, b->scenes[ids[k]].params.iterations));
-    u.iter.resize(maxIt);
-    u.bodyIter.resize(maxIt);
-    auto each = [&](auto&& fn) {
-      for (int k = 0; k < count; k++)
-        if (subs[k] > s) fn(b->scenes[ids[k]], (uint32_t)ids[k]);
-    };
-    each([&](BScene& S, uint32_t slot) { append_to(u.key, sch.items, slot, groups(std::max(S.n, S.nBodies))); });
-    each([&](BScene& S, uint32_t slot) { append_to(u.scan, sch.items, slot, scan_tiles(S.nCells)); });
-    each([&](BScene& S, uint32_t slot) { append_to(u.part, sch.items, slot, groups(S.n)); });
-    each([&](BScene& S, uint32_t slot) {
-      if (S.nBodyParts > 0 && S.nBodies > 0) append_to(u.seed, sch.items, slot, S.nBodies);
-    });
-    for (int it = 0; it < maxIt; it++) {
-      each([&](BScene& S, uint32_t slot) {
-        if (std::max(1, S.params.iterations) > it) append_to(u.iter[it], sch.items, slot, groups(S.n));
-      });
-      each([&](BScene& S, uint32_t slot) {
-        if (std::max(1, S.params.iterations) > it && S.nBodyParts > 0 && S.nBodies > 0)
-          append_to(u.bodyIter[it], sch.items, slot, S.nBodies);
-      });
-    }
-    each([&](BScene& S, uint32_t slot) {
-      if (!(S.params.surface_tension_k > 0)) append_to(u.finishPlain, sch.items, slot, groups(S.n));
-    });
-    each([&](BScene& S, uint32_t slot) {
-      if (S.params.surface_tension_k > 0) append_to(u.finishTension, sch.items, slot, groups(S.n));
-    });
-    for (int k = 0; k < count; k++) {
-      if (subs[k] <= s) continue;
-      BScene& S = b->scenes[ids[k]];
-      const double dt = (1.0 / 60) / std::max(1, S.params.substeps);
-      pack(S, dt, ids[k]);
-      S.P.parity = (uint32_t)(S.parity ^ (s & 1));
-      S.P.subs = (uint32_t)subs[k];
-      params[(size_t)s * nSlots + ids[k]] = S.P;
-    }
-    key.insert(key.end(), {u.key.count, u.scan.count, u.part.count, u.seed.count, (int64_t)u.iter.size(),
-                           u.finishPlain.count, u.finishTension.count});
-    for (int it = 0; it < maxIt; it++) key.insert(key.end(), {u.iter[it].count, u.bodyIter[it].count});
-  }
-  // the graph bakes the item segment offsets; the items themselves are uploaded per frame
-  for (auto& u : sch.subs) key.insert(key.end(), {u.key.off, u.scan.off, u.part.off});
-  key.push_back(zero.count);
-  int rc = execute(b, sch, params, nSlots, zero, key);
-  if (rc) return rc;
-  for (int k = 0; k < count; k++) {
-    BScene& S = b->scenes[ids[k]];
-    if (subs[k] < 1) continue;
-    S.parity ^= (subs[k] & 1);
-    S.simTime += subs[k] * ((1.0 / 60) / std::max(1, S.params.substeps));
-    S.statsValid = true;
-  }
-  return P4A_OK;
+  const std::vector<double> dts((size_t)count, frameDt);
+  return step_frame(b, ids, dts.data(), count);
 }
 
 int p4a_batch_synchronize(p4a_batch* b) {
@@ -833,8 +852,10 @@ int p4a_batch_scene_info(p4a_batch* b, int32_t id, p4a_info* o) {
   return P4A_OK;
 }
 
+}  // extern "C"
+
 // Device pointer, element size and element count of a scene's view of a buffer.
-static int scene_buffer(p4a_batch* b, const BScene& s, int32_t id, int32_t which, void** p, size_t* bytes) {
+int p4a::scene_buffer(p4a_batch* b, const BScene& s, int32_t id, int32_t which, void** p, size_t* bytes) {
   const int w = which < 0 ? s.parity : (which & 1);
   DevScene& d = b->d;
   const size_t po = (size_t)s.part.off, n = (size_t)s.cap, bo = (size_t)s.bodies.off;
@@ -858,6 +879,8 @@ static int scene_buffer(p4a_batch* b, const BScene& s, int32_t id, int32_t which
   }
   return P4A_OK;
 }
+
+extern "C" {
 
 int p4a_batch_read(p4a_batch* b, int32_t id, int32_t bid, int32_t which, void* host, size_t offset, size_t bytes) {
   int rc = scene_ok(b, id);

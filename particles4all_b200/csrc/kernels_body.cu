@@ -224,19 +224,16 @@ __global__ void __launch_bounds__(kBodyBlock) k_body_seed(const __grid_constant_
 }
 __global__ void __launch_bounds__(kBodyBlock) k_body_seed_b(const __grid_constant__ BatchWork w,
                                                             const __grid_constant__ DevScene d) {
-  uint32_t b;
-  const SimParams& P = batch_scene(w, b);
-  body_seed_body(P, d, b);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { body_seed_body(P, d, t); });
 }
 __global__ void __launch_bounds__(kBodyBlock) k_body_match(const __grid_constant__ SimParams P,
                                                            const __grid_constant__ DevScene d, int it) {
   body_match_body(P, d, blockIdx.x, it);
 }
 __global__ void __launch_bounds__(kBodyBlock) k_body_match_b(const __grid_constant__ BatchWork w,
-                                                             const __grid_constant__ DevScene d, int it) {
-  uint32_t b;
-  const SimParams& P = batch_scene(w, b);
-  body_match_body(P, d, b, it);
+                                                             const __grid_constant__ DevScene d,
+                                                             int it) {
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { body_match_body(P, d, t, it); });
 }
 
 // bodyDrag (src/wgsl.js:187-214) over the held body's particle list.
@@ -269,11 +266,11 @@ void launch_body_match(const SimParams& P, const DevScene& d, int it, cudaStream
   if (P.nBodies == 0) return;
   k_body_match<<<P.nBodies, kBodyBlock, 0, st>>>(P, d, it);
 }
-void launch_body_seed_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
-  if (nItems > 0) k_body_seed_b<<<nItems, kBodyBlock, 0, st>>>(w, d);
+void launch_body_seed_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st) {
+  k_body_seed_b<<<persistent_grid((const void*)k_body_seed_b, kBodyBlock, maxItems), kBodyBlock, 0, st>>>(w, d);
 }
-void launch_body_match_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st) {
-  if (nItems > 0) k_body_match_b<<<nItems, kBodyBlock, 0, st>>>(w, d, it);
+void launch_body_match_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st) {
+  k_body_match_b<<<persistent_grid((const void*)k_body_match_b, kBodyBlock, maxItems), kBodyBlock, 0, st>>>(w, d, it);
 }
 
 void launch_body_drag(const DevScene& d, float4* vel, const uint4* body, uint32_t held,

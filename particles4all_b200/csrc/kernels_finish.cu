@@ -109,8 +109,7 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
 }
 
 // xsph + normals (tension scenes): corr = xsphC * acc, normal = h * nacc.
-__device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevScene& d, uint32_t tile) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
@@ -209,20 +208,29 @@ __global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(const __grid_consta
 __global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize_b(const __grid_constant__ BatchWork w,
                                                                const __grid_constant__ DevScene d,
                                                                int substep) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  xsph_finalize_body(P, d, t, substep);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { xsph_finalize_body(P, d, t, substep); });
 }
-__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals(const __grid_constant__ SimParams P,
-                                                            const __grid_constant__ DevScene d) {
-  xsph_normals_body(P, d, blockIdx.x);
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_xsph_normals(const __grid_constant__ SimParams P,
+                                                         const __grid_constant__ DevScene d, int) {
+  xsph_normals_body(P, d, blockIdx.x * TB + threadIdx.x);
 }
-__global__ void __launch_bounds__(kBlock, 4) k_xsph_normals_b(const __grid_constant__ BatchWork w,
-                                                              const __grid_constant__ DevScene d) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  xsph_normals_body(P, d, t);
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_xsph_normals_b(const __grid_constant__ BatchWork w,
+                                                           const __grid_constant__ DevScene d, int) {
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
+#pragma unroll 1
+    for (int s = 0; s < kBlock; s += TB) xsph_normals_body(P, d, t * kBlock + s + threadIdx.x);
+  });
 }
+using PlainFn = void (*)(SimParams, DevScene, int);
+using BatchFn = void (*)(BatchWork, DevScene, int);
+static const PlainFn kNormalsP[kVariants] = {k_xsph_normals<256, 4>, k_xsph_normals<256, 5>,
+                                             k_xsph_normals<256, 3>, k_xsph_normals<128, 8>,
+                                             k_xsph_normals<128, 10>, k_xsph_normals<128, 6>};
+static const BatchFn kNormalsB[kVariants] = {k_xsph_normals_b<256, 4>, k_xsph_normals_b<256, 5>,
+                                             k_xsph_normals_b<256, 3>, k_xsph_normals_b<128, 8>,
+                                             k_xsph_normals_b<128, 10>, k_xsph_normals_b<128, 6>};
 __global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(const __grid_constant__ SimParams P,
                                                                 const __grid_constant__ DevScene d,
                                                                 int substep) {
@@ -231,29 +239,31 @@ __global__ void __launch_bounds__(kBlock, 5) k_tension_finalize(const __grid_con
 __global__ void __launch_bounds__(kBlock, 5) k_tension_finalize_b(const __grid_constant__ BatchWork w,
                                                                   const __grid_constant__ DevScene d,
                                                                   int substep) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  tension_finalize_body(P, d, t, substep);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { tension_finalize_body(P, d, t, substep); });
 }
 
 void launch_xsph_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st) {
   k_xsph_finalize<<<groups(P.n), kBlock, 0, st>>>(P, d, substep);
 }
-void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st) {
-  k_xsph_normals<<<groups(P.n), kBlock, 0, st>>>(P, d);
+void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st, int variant) {
+  const int v = variant >= 0 && variant < kVariants ? variant : tuned_variant(TK_NORMALS, P.n);
+  const int tb = kShapes[TK_NORMALS][v].threads;
+  kNormalsP[v]<<<groups(P.n, tb), tb, 0, st>>>(P, d, 0);
 }
 void launch_tension_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st) {
   k_tension_finalize<<<groups(P.n), kBlock, 0, st>>>(P, d, substep);
 }
-void launch_xsph_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep, cudaStream_t st) {
-  if (nItems > 0) k_xsph_finalize_b<<<nItems, kBlock, 0, st>>>(w, d, substep);
+void launch_xsph_finalize_b(const BatchWork& w, int maxItems, const DevScene& d, int substep, cudaStream_t st) {
+  k_xsph_finalize_b<<<persistent_grid((const void*)k_xsph_finalize_b, kBlock, maxItems), kBlock, 0, st>>>(w, d, substep);
 }
-void launch_xsph_normals_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
-  if (nItems > 0) k_xsph_normals_b<<<nItems, kBlock, 0, st>>>(w, d);
+void launch_xsph_normals_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st, int variant) {
+  const int v = variant >= 0 && variant < kVariants ? variant : tuned_variant(TK_NORMALS, (int64_t)maxItems * kBlock);
+  const int tb = kShapes[TK_NORMALS][v].threads;
+  kNormalsB[v]<<<persistent_grid((const void*)kNormalsB[v], tb, maxItems), tb, 0, st>>>(w, d, 0);
 }
-void launch_tension_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep,
+void launch_tension_finalize_b(const BatchWork& w, int maxItems, const DevScene& d, int substep,
                                cudaStream_t st) {
-  if (nItems > 0) k_tension_finalize_b<<<nItems, kBlock, 0, st>>>(w, d, substep);
+  k_tension_finalize_b<<<persistent_grid((const void*)k_tension_finalize_b, kBlock, maxItems), kBlock, 0, st>>>(w, d, substep);
 }
 
 }  // namespace p4a

@@ -93,9 +93,7 @@ __global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ Si
 }
 __global__ void __launch_bounds__(kBlock) k_key_count_b(const __grid_constant__ BatchWork w,
                                                         const __grid_constant__ DevScene d) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  key_count_body(P, d, t);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { key_count_body(P, d, t); });
 }
 __global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimParams P,
                                                  const __grid_constant__ DevScene d) {
@@ -103,9 +101,7 @@ __global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimPara
 }
 __global__ void __launch_bounds__(kBlock) k_fill_b(const __grid_constant__ BatchWork w,
                                                    const __grid_constant__ DevScene d) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  fill_body(P, d, t);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { fill_body(P, d, t); });
 }
 __global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimParams P,
                                                     const __grid_constant__ DevScene d) {
@@ -113,9 +109,7 @@ __global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimP
 }
 __global__ void __launch_bounds__(kBlock) k_reorder_b(const __grid_constant__ BatchWork w,
                                                       const __grid_constant__ DevScene d) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  reorder_body(P, d, t);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { reorder_body(P, d, t); });
 }
 
 // Tile status word: epoch (30 bits) | flag (2 bits) | value (32 bits).
@@ -229,31 +223,15 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
 
 // Batched: items[g] = (scene slot, local tile) in scene order; every scene's
 // segment of tiles is scanned on its own, seeded with its first particle index.
+// Tile states are indexed by g, the item's position in the launch's segment.
 __global__ void __launch_bounds__(kBlock) k_scan_b(const __grid_constant__ BatchWork w,
-                                                   const __grid_constant__ DevScene d, uint32_t epoch,
-                                                   int nTiles) {
-  __shared__ uint32_t s_tile;
-  __shared__ uint32_t s_cOff, s_nCells, s_pOff;
-  if (threadIdx.x == 0) s_tile = atomicAdd(d.scanTicket, 1u);
-  __syncthreads();
-  const int g = (int)s_tile;
-  if (g >= nTiles) {
-    if (threadIdx.x == 0) atomicOr(d.errorWord, ERR_SCAN_TIMEOUT);
-    return;
-  }
-  const uint2 it = w.items[g];
-  if (threadIdx.x == 0) {
-    s_cOff = w.params[it.x].cOff;
-    s_nCells = w.params[it.x].nCells;
-    s_pOff = w.params[it.x].pOff;
-  }
-  __syncthreads();
-  const int lt = (int)it.y;
-  const long long limit = (long long)s_cOff + s_nCells;
-  const bool last = (long long)(lt + 1) * kScanTile >= (long long)s_nCells;
-  scan_tile(d.cellCount, d.cellStart, (long long)s_cOff + (long long)lt * kScanTile, limit, g,
-            g - lt, s_pOff, last, d.scanState, epoch, d.errorWord);
-  if (threadIdx.x == 0 && g == nTiles - 1) *d.scanTicket = 0u;
+                                                   const __grid_constant__ DevScene d, uint32_t epoch) {
+  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
+    const long long limit = (long long)P.cOff + P.nCells;
+    const bool last = (long long)(lt + 1) * kScanTile >= (long long)P.nCells;
+    scan_tile(d.cellCount, d.cellStart, (long long)P.cOff + (long long)lt * kScanTile, limit, (int)g,
+              (int)(g - lt), P.pOff, last, d.scanState, epoch, d.errorWord);
+  });
 }
 
 void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st) {
@@ -308,17 +286,27 @@ cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity,
   return cudaGetLastError();
 }
 
-void launch_key_count_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
-  if (nItems > 0) k_key_count_b<<<nItems, kBlock, 0, st>>>(w, d);
+void launch_key_count_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st) {
+  k_key_count_b<<<persistent_grid((const void*)k_key_count_b, kBlock, maxItems), kBlock, 0, st>>>(w, d);
 }
-void launch_scan_b(const BatchWork& w, int nTiles, const DevScene& d, uint32_t epoch, cudaStream_t st) {
-  if (nTiles > 0) k_scan_b<<<nTiles, kBlock, 0, st>>>(w, d, epoch, nTiles);
+void launch_scan_b(const BatchWork& w, int maxItems, const DevScene& d, uint32_t epoch, cudaStream_t st) {
+  k_scan_b<<<persistent_grid((const void*)k_scan_b, kBlock, maxItems), kBlock, 0, st>>>(w, d, epoch);
 }
-void launch_fill_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
-  if (nItems > 0) k_fill_b<<<nItems, kBlock, 0, st>>>(w, d);
+void launch_fill_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st) {
+  k_fill_b<<<persistent_grid((const void*)k_fill_b, kBlock, maxItems), kBlock, 0, st>>>(w, d);
 }
-void launch_reorder_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st) {
-  if (nItems > 0) k_reorder_b<<<nItems, kBlock, 0, st>>>(w, d);
+void launch_reorder_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st) {
+  k_reorder_b<<<persistent_grid((const void*)k_reorder_b, kBlock, maxItems), kBlock, 0, st>>>(w, d);
+}
+
+__global__ void __launch_bounds__(kBlock) k_zero_stats_b(const __grid_constant__ BatchWork w,
+                                                         uint32_t* __restrict__ stats) {
+  const WorkSeg seg = *w.seg;
+  for (uint32_t t = blockIdx.x * kBlock + threadIdx.x; t < seg.count * 8u; t += gridDim.x * kBlock)
+    stats[w.params[w.items[seg.off + t / 8u].x].slot * 8u + (t % 8u)] = 0u;
+}
+void launch_zero_stats_b(const BatchWork& w, uint32_t* stats, cudaStream_t st) {
+  k_zero_stats_b<<<8, kBlock, 0, st>>>(w, stats);
 }
 
 }  // namespace p4a

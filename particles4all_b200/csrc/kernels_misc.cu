@@ -57,12 +57,9 @@ __device__ __forceinline__ void store_g(float4* __restrict__ g, uint32_t i, cons
   g[i * 2 + 1] = make_float4(elc(G, 2, 1), elc(G, 2, 2), det3(G), last);
 }
 
-__global__ void __launch_bounds__(128, 10) k_aniso(const __grid_constant__ AnisoParams A,
-                                               const float4* __restrict__ pos,
-                                               const uint32_t* __restrict__ cs,
-                                               float4* __restrict__ smoothPos,
-                                               float4* __restrict__ g) {
-  const uint32_t i = blockIdx.x * 128 + threadIdx.x;
+__device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* __restrict__ pos,
+                                           const uint32_t* __restrict__ cs, float4* __restrict__ smoothPos,
+                                           float4* __restrict__ g, uint32_t i) {
   if (i >= A.count) return;
   const F3 xi = xyz(__ldg(&pos[i]));
   I3 c;
@@ -181,9 +178,22 @@ void launch_resize(uint32_t n, float4* pos, const float oldSize[3], const float 
                                          F3{clampMax[0], clampMax[1], clampMax[2]});
 }
 
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_aniso(const __grid_constant__ AnisoParams A,
+                                                  const float4* __restrict__ pos,
+                                                  const uint32_t* __restrict__ cs,
+                                                  float4* __restrict__ smoothPos, float4* __restrict__ g) {
+  aniso_body(A, pos, cs, smoothPos, g, blockIdx.x * TB + threadIdx.x);
+}
+using AnisoFn = void (*)(AnisoParams, const float4*, const uint32_t*, float4*, float4*);
+static const AnisoFn kAniso[kVariants] = {k_aniso<128, 10>, k_aniso<128, 8>, k_aniso<128, 12>,
+                                          k_aniso<256, 5>,  k_aniso<256, 4>, k_aniso<64, 20>};
+
 void launch_aniso(const AnisoParams& A, const float4* pos, const uint32_t* cellStart,
-                  float4* smoothPos, float4* g, cudaStream_t st) {
-  k_aniso<<<groups(A.count, 128), 128, 0, st>>>(A, pos, cellStart, smoothPos, g);
+                  float4* smoothPos, float4* g, cudaStream_t st, int variant) {
+  const int v = variant >= 0 && variant < kVariants ? variant : tuned_variant(TK_ANISO, A.count);
+  const int tb = kShapes[TK_ANISO][v].threads;
+  kAniso[v]<<<groups(A.count, tb), tb, 0, st>>>(A, pos, cellStart, smoothPos, g);
 }
 
 }  // namespace p4a

@@ -21,8 +21,7 @@
 
 namespace p4a {
 
-__device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t tile, int it) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
@@ -84,8 +83,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   }
 }
 
-__device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d, uint32_t tile, int it) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
@@ -150,38 +148,67 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   }
 }
 
-__global__ void __launch_bounds__(kBlock, 4) k_lambda(const __grid_constant__ SimParams P,
-                                                      const __grid_constant__ DevScene d, int it) {
-  lambda_body(P, d, blockIdx.x, it);
+// Plain: block b handles particles [b * TB, (b + 1) * TB). Batched: an item is a
+// tile of kBlock particles, walked TB at a time.
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_lambda(const __grid_constant__ SimParams P,
+                                                   const __grid_constant__ DevScene d, int it) {
+  lambda_body(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
-__global__ void __launch_bounds__(kBlock, 4) k_lambda_b(const __grid_constant__ BatchWork w,
-                                                        const __grid_constant__ DevScene d, int it) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  lambda_body(P, d, t, it);
-}
-__global__ void __launch_bounds__(kBlock, 5) k_delta(const __grid_constant__ SimParams P,
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_lambda_b(const __grid_constant__ BatchWork w,
                                                      const __grid_constant__ DevScene d, int it) {
-  delta_body(P, d, blockIdx.x, it);
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
+#pragma unroll 1
+    for (int s = 0; s < kBlock; s += TB) lambda_body(P, d, t * kBlock + s + threadIdx.x, it);
+  });
 }
-__global__ void __launch_bounds__(kBlock, 5) k_delta_b(const __grid_constant__ BatchWork w,
-                                                       const __grid_constant__ DevScene d, int it) {
-  uint32_t t;
-  const SimParams& P = batch_scene(w, t);
-  delta_body(P, d, t, it);
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_delta(const __grid_constant__ SimParams P,
+                                                  const __grid_constant__ DevScene d, int it) {
+  delta_body(P, d, blockIdx.x * TB + threadIdx.x, it);
+}
+template <int TB, int MB>
+__global__ void __launch_bounds__(TB, MB) k_delta_b(const __grid_constant__ BatchWork w,
+                                                    const __grid_constant__ DevScene d, int it) {
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
+#pragma unroll 1
+    for (int s = 0; s < kBlock; s += TB) delta_body(P, d, t * kBlock + s + threadIdx.x, it);
+  });
 }
 
-void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st) {
-  k_lambda<<<groups(P.n), kBlock, 0, st>>>(P, d, it);
+using PlainFn = void (*)(SimParams, DevScene, int);
+using BatchFn = void (*)(BatchWork, DevScene, int);
+#define P4A_SHAPES(K, suffix)                                                                        \
+  {K##suffix<256, 4>, K##suffix<256, 5>, K##suffix<256, 3>, K##suffix<128, 8>, K##suffix<128, 10>, \
+   K##suffix<128, 6>}
+#define P4A_SHAPES_D(K, suffix)                                                                      \
+  {K##suffix<256, 5>, K##suffix<256, 4>, K##suffix<256, 6>, K##suffix<128, 10>, K##suffix<128, 8>, \
+   K##suffix<128, 12>}
+static const PlainFn kLambdaP[kVariants] = P4A_SHAPES(k_lambda, );
+static const BatchFn kLambdaB[kVariants] = P4A_SHAPES(k_lambda, _b);
+static const PlainFn kDeltaP[kVariants] = P4A_SHAPES_D(k_delta, );
+static const BatchFn kDeltaB[kVariants] = P4A_SHAPES_D(k_delta, _b);
+
+static int pick(int kernel, int variant, int64_t n) {
+  return variant >= 0 && variant < kVariants ? variant : tuned_variant(kernel, n);
 }
-void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st) {
-  k_delta<<<groups(P.n), kBlock, 0, st>>>(P, d, it);
+
+void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant) {
+  const int v = pick(TK_LAMBDA, variant, P.n), tb = kShapes[TK_LAMBDA][v].threads;
+  kLambdaP[v]<<<groups(P.n, tb), tb, 0, st>>>(P, d, it);
 }
-void launch_lambda_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st) {
-  if (nItems > 0) k_lambda_b<<<nItems, kBlock, 0, st>>>(w, d, it);
+void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant) {
+  const int v = pick(TK_DELTA, variant, P.n), tb = kShapes[TK_DELTA][v].threads;
+  kDeltaP[v]<<<groups(P.n, tb), tb, 0, st>>>(P, d, it);
 }
-void launch_delta_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st) {
-  if (nItems > 0) k_delta_b<<<nItems, kBlock, 0, st>>>(w, d, it);
+void launch_lambda_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st, int variant) {
+  const int v = pick(TK_LAMBDA, variant, (int64_t)maxItems * kBlock), tb = kShapes[TK_LAMBDA][v].threads;
+  kLambdaB[v]<<<persistent_grid((const void*)kLambdaB[v], tb, maxItems), tb, 0, st>>>(w, d, it);
+}
+void launch_delta_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st, int variant) {
+  const int v = pick(TK_DELTA, variant, (int64_t)maxItems * kBlock), tb = kShapes[TK_DELTA][v].threads;
+  kDeltaB[v]<<<persistent_grid((const void*)kDeltaB[v], tb, maxItems), tb, 0, st>>>(w, d, it);
 }
 
 }  // namespace p4a

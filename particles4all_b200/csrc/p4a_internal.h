@@ -102,10 +102,18 @@ struct DevScene {
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };
 
-// A batched launch: block b works on item items[b] = (scene slot, tile/body).
+// A batched launch is persistent: its blocks pull work items (scene slot, tile or
+// body) from the launch's segment of the frame's item list through a pull cursor,
+// until the segment is exhausted. Counts and offsets live in device memory, so a
+// captured frame replays for any set of scenes with the same launch sequence.
+struct WorkSeg {
+  uint32_t off, count;  // items [off, off + count) of the frame's list
+};
 struct BatchWork {
-  const SimParams* params;
-  const uint2* items;
+  const SimParams* params;  // this substep's table, indexed by scene slot
+  const uint2* items;       // the frame's item list
+  const WorkSeg* seg;       // this launch's segment
+  uint32_t* cursor;         // this launch's pull cursor, zero when the frame starts
 };
 
 constexpr int kBlock = 256;          // particles per block (the reference's workgroup)
@@ -125,27 +133,51 @@ void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells,
                  cudaStream_t st);
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_reorder(const SimParams& P, const DevScene& d, cudaStream_t st);
-void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
-void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
+// Kernels with tuned launch shapes (threads per block x minimum blocks per SM; the
+// per-particle arithmetic is the same in every shape). `variant` < 0 looks the
+// shape up in the tuning table by the launch's particle count.
+enum TunedKernel { TK_LAMBDA = 0, TK_DELTA = 1, TK_NORMALS = 2, TK_ANISO = 3, TK_COUNT = 4 };
+constexpr int kVariants = 6;
+struct LaunchShape {
+  int threads, minBlocks;
+};
+extern const LaunchShape kShapes[TK_COUNT][kVariants];
+int tuned_variant(int kernel, int64_t particles);
+
+void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant = -1);
+void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant = -1);
 void launch_body_seed(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_body_match(const SimParams& P, const DevScene& d, int it, cudaStream_t st);
 void launch_xsph_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st);
-void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st);
+void launch_xsph_normals(const SimParams& P, const DevScene& d, cudaStream_t st, int variant = -1);
 void launch_tension_finalize(const SimParams& P, const DevScene& d, int substep, cudaStream_t st);
 
 // ---- batched launchers (items: tiles of 256 particles, scan tiles, or bodies) ----
-void launch_key_count_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
-void launch_scan_b(const BatchWork& w, int nTiles, const DevScene& d, uint32_t epoch, cudaStream_t st);
-void launch_fill_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
-void launch_reorder_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
-void launch_lambda_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
-void launch_delta_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
-void launch_body_seed_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
-void launch_body_match_b(const BatchWork& w, int nItems, const DevScene& d, int it, cudaStream_t st);
-void launch_xsph_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep, cudaStream_t st);
-void launch_xsph_normals_b(const BatchWork& w, int nItems, const DevScene& d, cudaStream_t st);
-void launch_tension_finalize_b(const BatchWork& w, int nItems, const DevScene& d, int substep,
+// `maxItems` bounds the launch's item count: the grid is min(maxItems, the blocks
+// resident on the device at once); pass a large value for a launch whose count is
+// only known on the device (a replayed graph).
+void launch_key_count_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_scan_b(const BatchWork& w, int maxItems, const DevScene& d, uint32_t epoch, cudaStream_t st);
+void launch_fill_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_reorder_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_lambda_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st, int variant);
+void launch_delta_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st, int variant);
+void launch_body_seed_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_body_match_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st);
+void launch_xsph_finalize_b(const BatchWork& w, int maxItems, const DevScene& d, int substep, cudaStream_t st);
+void launch_xsph_normals_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st, int variant);
+void launch_tension_finalize_b(const BatchWork& w, int maxItems, const DevScene& d, int substep,
                                cudaStream_t st);
+// Zeroes the stats slots (P.slot) of the scenes listed in w's segment.
+void launch_zero_stats_b(const BatchWork& w, uint32_t* stats, cudaStream_t st);
+
+// Blocks of `kernel` (launched with `block` threads) resident on the current
+// device at once, cached per device and kernel; the grid of a persistent launch.
+int resident_grid(const void* kernel, int block);
+inline int persistent_grid(const void* kernel, int block, int maxItems) {
+  const int r = resident_grid(kernel, block);
+  return maxItems < r ? (maxItems < 1 ? 1 : maxItems) : r;
+}
 
 // The grid pass as an operator on caller buffers (p4a_grid_sort and
 // p4a_grid_sort_noalloc): input parity 0 = (pos, vel, body, rest), output parity 1
@@ -171,6 +203,6 @@ void launch_impulse(uint32_t n, const float4* pos, float4* vel, const float orig
 void launch_resize(uint32_t n, float4* pos, const float oldSize[3], const float newSize[3],
                    const float clampMin[3], const float clampMax[3], cudaStream_t st);
 void launch_aniso(const AnisoParams& A, const float4* pos, const uint32_t* cellStart,
-                  float4* smoothPos, float4* g, cudaStream_t st);
+                  float4* smoothPos, float4* g, cudaStream_t st, int variant = -1);
 
 }  // namespace p4a

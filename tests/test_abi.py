@@ -47,7 +47,9 @@ def test_struct_layouts_match_c_compiler(tmp_path):
                "p4a_scene_desc": _abi.SceneDesc, "p4a_info": _abi.Info, "p4a_stats": _abi.Stats,
                "p4a_aniso_params": _abi.AnisoParams, "p4a_grid": _abi.Grid,
                "p4a_scene_counts": _abi.SceneCounts, "p4a_batch_config": _abi.BatchConfig,
-               "p4a_batch_usage": _abi.BatchUsage, "p4a_phase_time": _abi.PhaseTime}
+               "p4a_batch_usage": _abi.BatchUsage, "p4a_phase_time": _abi.PhaseTime,
+               "p4a_server_config": _abi.ServerConfig, "p4a_completion": _abi.Completion,
+               "p4a_server_stats": _abi.ServerStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "p4a.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
@@ -87,6 +89,13 @@ def test_no_device_fails_loudly(built):
     from particles4all_b200 import Sim, P4AError
     with pytest.raises(P4AError):
         Sim()
+    cfg = _abi.ServerConfig()
+    assert L.p4a_server_default_config(C.byref(cfg)) == 0
+    assert cfg.max_frames_in_flight == 2 and cfg.use_graphs == 1 and cfg.arenas.max_scenes == 1024
+    assert L.p4a_server_create(0, C.byref(cfg), C.byref(h)) == _abi.P4A_ERR_NODEV and not h.value
+    from particles4all_b200.server import Server
+    with pytest.raises(P4AError):
+        Server(budget_bytes=1 << 30)
 
 
 def test_grid_sort_rejects_bad_arguments(built):
@@ -102,3 +111,33 @@ def test_grid_sort_rejects_bad_arguments(built):
     assert rc == _abi.P4A_ERR_CAPACITY
     g.dim[0] = 0
     assert L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 11), None, 0, None) == _abi.P4A_ERR_ARG
+
+
+def test_tuning_table_host_side(built, tmp_path):
+    """The launch-shape table is host state: set / get / clear and the JSON round
+    trip of the autotuner work without a GPU."""
+    from particles4all_b200 import autotune
+    L = _lib.lib()
+    cnt = C.c_int32()
+    t = (C.c_int32 * 8)()
+    m = (C.c_int32 * 8)()
+    assert L.p4a_kernel_shapes(0, t, m, 8, C.byref(cnt)) == 0 and cnt.value == 6
+    assert (t[0], m[0]) == (256, 4) and all(t[k] in (64, 128, 256) for k in range(6))
+    assert L.p4a_kernel_shapes(9, t, m, 8, C.byref(cnt)) == _abi.P4A_ERR_ARG
+    v = C.c_int32()
+    try:
+        L.p4a_tune_clear(-1)
+        assert L.p4a_tune_set(1, 1000, 3) == 0 and L.p4a_tune_set(1, 100, 2) == 0
+        for n, want in ((50, 2), (100, 2), (101, 3), (1000, 3), (1001, 0)):
+            assert L.p4a_tune_get(1, n, C.byref(v)) == 0 and v.value == want, n
+        assert L.p4a_tune_set(1, 100, 7) == _abi.P4A_ERR_ARG
+        path = tmp_path / "t.json"
+        path.write_text('{"kernels": {"aniso": [[10, 5], [1000000, 1]]}}')
+        autotune.load(str(path), L)
+        assert L.p4a_tune_get(3, 5, C.byref(v)) == 0 and v.value == 5
+        assert L.p4a_tune_get(3, 500, C.byref(v)) == 0 and v.value == 1
+        L.p4a_tune_clear(3)
+        assert L.p4a_tune_get(3, 5, C.byref(v)) == 0 and v.value == 0
+    finally:
+        L.p4a_tune_clear(-1)
+        autotune.load(L=L)
