@@ -73,6 +73,23 @@ def workload(name):
     return params, scene, aniso
 
 
+def hose_for(params, scene):
+    """The workload's hose (2,048 particles per step at 3 m/s until the pour budget
+    is used), or None."""
+    from particles4all_b200 import configs
+    budget = int(scene.get("pour_budget", 0) or 0)
+    if budget <= 0:
+        return None
+    return configs.Hose(params["box"], params["spacing"], per_step=2048, speed=3.0, limit=budget)
+
+
+def pour(sim, hose):
+    if hose is None:
+        return 0
+    pos, vel = hose.emit()
+    return 0 if pos is None else sim.appendFluid(pos, vel)
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -232,8 +249,8 @@ def served_bench(seconds, budget_gb):
     out = {"workload": "poisson 200/s, n ~ logU[2k, 512k], 60 Hz closed-loop steps, exp(10 s) lifetimes, "
                        "pos readback every 4th step", "seconds": seconds, "arena_budget_bytes": budget}
     for mode in ("batched", "plain"):
-        srv = Server(budget_bytes=budget, max_scenes=4096, plain=(mode == "plain"), builder_threads=6,
-                     upload_bytes=2 << 30, readback_bytes=4 << 30)
+        srv = Server(budget_bytes=budget, max_scenes=4096, plain=(mode == "plain"), builder_threads=10,
+                     upload_bytes=4 << 30, readback_bytes=4 << 30)
         t0 = time.perf_counter()
         r = loadgen.run(srv, seconds, seed=4)
         st = srv.stats()
@@ -258,21 +275,26 @@ def cpu_baseline(params, scene, aniso, seconds):
     import oracle
     o = oracle.OracleSim()
     o.reset_scene(params, scene)
-    n = o.info()["n"]
+    hose = hose_for(params, scene)
+    ps = 0.0
     subs = 0
     steps = 0
     t0 = time.perf_counter()
     while True:
-        subs += o.step(1 / 60)
+        pour(o, hose)
+        s = o.step(1 / 60)
         if aniso:
             o.aniso(aniso)
+        subs += s
+        ps += o.info()["n"] * s
         steps += 1
         if time.perf_counter() - t0 >= seconds:
             break
     el = time.perf_counter() - t0
-    return {"value": n * subs / el, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
-            "sample": f"{steps} full steps ({subs} substeps{' + anisotropic pass' if aniso else ''}) "
-                      f"of the same {n}-particle scene in {el:.1f} s"}
+    n = o.info()["n"]
+    return {"value": ps / el, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
+            "sample": f"{steps} full steps ({subs} substeps{' + anisotropic pass' if aniso else ''}"
+                      f"{' + hose' if hose else ''}) of the same scene ({n} particles at the end) in {el:.1f} s"}
 
 
 def run_reference(args):
@@ -283,6 +305,7 @@ def run_reference(args):
     params, scene, aniso = workload(args.workload)
     o = oracle.OracleSim()
     o.reset_scene(params, scene)
+    hose = hose_for(params, scene)
     n = o.info()["n"]
     base = max(1, params["substeps"])
     # a step is the full frame, or one substep of it when K frames would not fit
@@ -295,18 +318,24 @@ def run_reference(args):
     dt = 1 / 60 if frame else (1 / 60) / base
 
     def one():
+        if frame:
+            pour(o, hose)
         s = o.step(dt)
         if aniso and frame:
             o.aniso(aniso)
-        return s
+        return s, o.info()["n"] * s
     for _ in range(max(0, args.warmup - 1)):
         one()
     subs = 0
+    ps = 0.0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        subs += one()
+        s, p = one()
+        subs += s
+        ps += p
     el = time.perf_counter() - t0
-    value = n * subs / el
+    value = ps / el
+    n = o.info()["n"]
     sample = (f"{'full frames' if frame else 'single substeps'} of the {n}-particle scene, "
               f"{subs} substeps timed, all host threads")
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
@@ -338,12 +367,16 @@ def run_ours(args):
     sim.set_stream(stream.cuda_stream)
     sim.reset_scene(params, scene)
     n = sim.info()["n"]
+    hose = hose_for(params, scene)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    done = [0.0]  # particle-substeps
 
     def frame():
+        pour(sim, hose)
         s = sim.step(1 / 60)
         if aniso:
             sim.aniso(aniso)
+        done[0] += sim.info()["n"] * s
         return s
 
     for _ in range(max(3, args.warmup)):
@@ -359,6 +392,7 @@ def run_ours(args):
     barrier()
     torch.cuda.synchronize()
     w0 = time.time()
+    done[0] = 0.0
     subs = 0
     with torch.cuda.stream(stream):
         for k in range(args.steps):
@@ -375,14 +409,16 @@ def run_ours(args):
     kern = sim.profile_read()
     sim.profile(False)
     dev_ms_max = allmax(dev_ms)
-    value = world * n * subs / (dev_ms_max / 1000.0)
+    done_timed = done[0]
+    value = world * done_timed / (dev_ms_max / 1000.0)
 
     # roofline of the dominant kernel (live per-kernel events of the timed region)
     top = max(kern.items(), key=lambda kv: kv[1][0])
     name, (kms, kl) = top
     per_p = ALGO_BYTES.get(name, 0) + (64 if name == "reorder" and sim.info()["n_bodies"] else 0)
     avg_s = kms / kl / 1000.0
-    algo = per_p * n
+    n_avg = done_timed / max(1, subs)  # mean particles per substep (grows with a hose)
+    algo = per_p * n_avg
     peak, peak_kind = peaks()
     achieved = algo / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -398,31 +434,37 @@ def run_ours(args):
     if not args.no_e2e:
         L = _lib.lib()
         h = sim._h
-        nbytes = n * 16
-        hp = torch.empty(max(1, n) * 4, dtype=torch.float32, pin_memory=True)
-        hv = torch.empty(max(1, n) * 4, dtype=torch.float32, pin_memory=True)
+        cap = max(1, sim.info()["cap"])
+        hp = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
+        hv = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
         hs = torch.empty(8, dtype=torch.int32, pin_memory=True)
-        L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nbytes)
-        L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nbytes)
+        nb0 = sim.info()["n"] * 16
+        L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nb0)
+        L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nb0)
         e_steps = max(3, min(args.steps, 50))
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        e_subs = 0
+        done[0] = 0.0
+        h2d = d2h = 0
         for _ in range(e_steps):
-            L.p4a_write(h, 0, -1, hp.data_ptr(), 0, nbytes)
-            L.p4a_write(h, 1, -1, hv.data_ptr(), 0, nbytes)
-            e_subs += frame()
-            L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nbytes)
-            L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nbytes)
+            nb = sim.info()["n"] * 16
+            L.p4a_write(h, 0, -1, hp.data_ptr(), 0, nb)
+            L.p4a_write(h, 1, -1, hv.data_ptr(), 0, nb)
+            frame()
+            nb2 = sim.info()["n"] * 16
+            L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nb2)
+            L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nb2)
             L.p4a_read(h, 17, -1, hs.data_ptr(), 0, 32)
+            h2d += 2 * nb
+            d2h += 2 * nb2 + 32
         t1 = time.perf_counter()
         barrier()
         el = allmax(t1 - t0)
-        e2e = {"value": world * n * e_subs / el, "unit": METRIC, "h2d_bytes_per_step": 2 * nbytes,
-               "d2h_bytes_per_step": 2 * nbytes + 32, "steps": e_steps,
-               "what": "per step: live pos+vel written from pinned host, Sim.step + aniso, "
-                       "pos+vel+stats read back to pinned host"}
+        e2e = {"value": world * done[0] / el, "unit": METRIC, "h2d_bytes_per_step": h2d // e_steps,
+               "d2h_bytes_per_step": d2h // e_steps, "steps": e_steps,
+               "what": "per step: live pos+vel written from pinned host, Sim.step (+ hose, + aniso as the "
+                       "workload has them), pos+vel+stats read back to pinned host"}
 
     mix = None
     if world == 1 and not args.no_mix:
@@ -446,7 +488,9 @@ def run_ours(args):
             "warmup": max(3, args.warmup), "ms_per_step": dev_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": args.workload, "n_particles": n, "n_bodies": sim.info()["n_bodies"],
+            "config": {"workload": args.workload, "n_particles": n, "n_particles_end": sim.info()["n"],
+                       "hose": "2,048 particles per step at 3 m/s" if hose else None,
+                       "n_bodies": sim.info()["n_bodies"],
                        "substeps_per_step": subs // args.steps, "iterations": params["iterations"],
                        "surface_tension": params["surfaceTensionK"], "aniso_pass": bool(aniso),
                        "l2": "flushed between timed steps (256 MiB write outside the timed events)",

@@ -171,7 +171,10 @@ enum {
   P4A_BUF_STATS_OUT = 17,   /* uint32[8]           */
   P4A_BUF_SMOOTH_POS = 18,  /* float4[n] (aniso)   */
   P4A_BUF_ANISO_G = 19,     /* float4[2n] (aniso)  */
-  P4A_BUF_COUNT = 20
+  P4A_BUF_MESH_FIELD = 20,  /* float[vertDim xyz] (mesh): density field   */
+  P4A_BUF_MESH_NFIELD = 21, /* float[vertDim xyz] (mesh): normal field    */
+  P4A_BUF_MESH_VERTS = 22,  /* uint2[3 * stored triangles] (mesh)         */
+  P4A_BUF_COUNT = 23
 };
 /* `which` selector for A/B buffers. */
 enum { P4A_A = 0, P4A_B = 1, P4A_LIVE = -1 };
@@ -261,6 +264,41 @@ int p4a_profile_read(p4a_sim* sim, p4a_phase_time* out, int32_t max_entries, int
 /* Extension, no counterpart in the reference: kernels launched by this
  * library in this process (all handles and operator entries). */
 uint64_t p4a_kernel_launches(void);
+
+/* ---- surface mesh (src/mesh.js:99-340, src/mesh_wgsl.js:23-238) --------- */
+/*
+ * SurfaceMesh.generate on the simulation's live buffers: a density field on the
+ * vertices of a voxel grid over the box (configure([0,0,0], box, resolution)),
+ * `field_passes` blur passes of it, a normal field of `normal_passes` further
+ * passes, and marching tetrahedra (six per voxel) writing triangles as packed
+ * vertices: uint2 {x | y << 16, z | octahedral normal << 16}, positions in
+ * 1/65535 of the grid, 3 per triangle. Triangles are stored in voxel order (the
+ * reference's order is its atomic counter's); at most max_triangles are stored and
+ * *triangles (may be NULL; then the call does not wait) receives the total, as
+ * the reference's counter does.
+ * blur_axes = 0 blurs every pass along x: the reference writes each pass's axis into
+ * one uniform with queue.writeBuffer while encoding, and the last write of a frame
+ * (generate's final setParams, axis x) is what all of its passes read. 1 cycles
+ * x, y, z per pass as the pass structure intends.
+ */
+typedef struct p4a_mesh_params {
+  int32_t resolution;     /* voxels along the longest box side (meshRes), default 128   */
+  double iso;             /* meshIso, default 0.4                                       */
+  int32_t field_passes;   /* fieldSmooth, default 0                                     */
+  int32_t normal_passes;  /* normalSmoothPasses, default 2                              */
+  int64_t max_triangles;  /* maxTriangles, default 3,000,000                            */
+  int32_t blur_axes;      /* 0 = as the reference executes (x), 1 = x, y, z             */
+} p4a_mesh_params;
+typedef struct p4a_mesh_info {
+  int32_t vert_dim[3];
+  double origin[3];
+  double voxel;
+  int64_t triangles;      /* total of the last p4a_mesh that was waited for             */
+  int32_t mesh_gen;       /* increments when the mesh buffers are reallocated           */
+} p4a_mesh_info;
+int p4a_default_mesh_params(p4a_mesh_params* out);
+int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
+int p4a_mesh_get_info(p4a_sim* s, p4a_mesh_info* out);
 
 /* ---- batched multi-scene stepping -------------------------------------- */
 /*

@@ -16,7 +16,7 @@ import numpy as np
 
 from particles4all_b200 import _abi
 from particles4all_b200._scene_desc import scene_desc
-from particles4all_b200.params import CParams, aniso_struct
+from particles4all_b200.params import CParams, aniso_struct, mesh_struct
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "liboracle_p4a.so")
@@ -45,7 +45,7 @@ def lib():
             "orc_append_fluid": [vp, vp, vp, i32, C.POINTER(i32)],
             "orc_apply_ray_impulse": [vp, vp, vp, vp, dbl, dbl],
             "orc_hold_body": [vp, i32, vp, dbl, dbl], "orc_release_body": [vp],
-            "orc_resize_box": [vp, vp], "orc_aniso": [vp, vp], "orc_get_info": [vp, vp],
+            "orc_resize_box": [vp, vp], "orc_aniso": [vp, vp], "orc_mesh": [vp, vp, vp], "orc_get_info": [vp, vp],
             "orc_stats": [vp, vp], "orc_buffer": [vp, i32, i32, C.POINTER(vp), C.POINTER(C.c_size_t)],
             "orc_build_scene": [vp, vp, vp, vp, vp, vp, vp, vp],
             "orc_boundary": [vp, dbl, dbl, C.POINTER(i32), vp, vp],
@@ -183,6 +183,12 @@ class OracleSim:
     def aniso(self, aparams):
         s = aniso_struct(aparams)
         _check(self._L.orc_aniso(self._h, C.byref(s)), "aniso")
+
+    def mesh(self, mparams):
+        m = mesh_struct(mparams)
+        t = C.c_int64()
+        _check(self._L.orc_mesh(self._h, C.byref(m), C.byref(t)), "mesh")
+        return t.value
 
     def info(self):
         i = _abi.Info()

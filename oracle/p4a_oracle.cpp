@@ -450,6 +450,9 @@ struct orc_sim {
   p4a_stats stats{};
   std::vector<f4> smoothPos, anisoG;
   int anisoGen = 0;
+  std::vector<float> meshField, meshNField;
+  std::vector<uint32_t> meshVerts;  // 2 words per vertex
+  int64_t meshTris = 0;
   bool ready = false;
 };
 
@@ -1538,6 +1541,222 @@ int orc_get_info(const orc_sim* s, p4a_info* o) {
   return P4A_OK;
 }
 
+// ---- surface mesh: SurfaceMesh.configure + generate (src/mesh.js:99-352) ----------
+namespace {
+
+struct MeshU {  // the uniform of src/mesh_wgsl.js:3-21 as src/mesh.js:137-153 packs it
+  int dim[3];
+  float voxel, origin[3], iso, invSupport, support2, poly6, mass, rho0;
+  int simDim[3];
+  uint32_t maxTris, skipBodies;
+};
+
+inline float mesh_at(const std::vector<float>& f, const MeshU& M, int x, int y, int z) {
+  x = std::min(std::max(x, 0), M.dim[0] - 1);
+  y = std::min(std::max(y, 0), M.dim[1] - 1);
+  z = std::min(std::max(z, 0), M.dim[2] - 1);
+  return f[(size_t)((z * M.dim[1] + y) * M.dim[0] + x)];
+}
+
+// meshSmooth (src/mesh_wgsl.js:71-92) along `axis`, in place over every grid line.
+void mesh_blur(std::vector<float>& f, const MeshU& M, int axis) {
+  const int len = M.dim[axis];
+  const size_t stride = axis == 0 ? 1 : axis == 1 ? (size_t)M.dim[0] : (size_t)M.dim[0] * M.dim[1];
+  const int o1 = axis == 0 ? 1 : 0, o2 = axis == 2 ? 1 : 2;
+  std::vector<float> a(len), b(len);
+  for (int u = 0; u < M.dim[o2]; u++)
+    for (int w = 0; w < M.dim[o1]; w++) {
+      const size_t base = (size_t)u * (o2 == 1 ? M.dim[0] : (size_t)M.dim[0] * M.dim[1]) +
+                          (size_t)w * (o1 == 0 ? 1 : M.dim[0]);
+      for (int k = 0; k < len; k++) a[k] = f[base + k * stride];
+      for (int k = 0; k < len; k++)
+        b[k] = (0.25f * a[std::max(k - 1, 0)] + 0.5f * a[k]) + 0.25f * a[std::min(k + 1, len - 1)];
+      for (int k = 0; k < len; k++) f[base + k * stride] = b[k];
+    }
+}
+
+struct MCorner {
+  float d;
+  f3 p, g;
+};
+
+uint32_t mesh_pack(const MeshU& M, f3 pg, f3 nIn, uint32_t* hi) {
+  const float px = std::min(std::max(pg.x / (float)(M.dim[0] - 1), 0.0f), 1.0f);
+  const float py = std::min(std::max(pg.y / (float)(M.dim[1] - 1), 0.0f), 1.0f);
+  const float pz = std::min(std::max(pg.z / (float)(M.dim[2] - 1), 0.0f), 1.0f);
+  const uint32_t qx = f2u_sat(px * 65535.0f + 0.5f), qy = f2u_sat(py * 65535.0f + 0.5f),
+                 qz = f2u_sat(pz * 65535.0f + 0.5f);
+  const float l1 = std::max((std::fabs(nIn.x) + std::fabs(nIn.y)) + std::fabs(nIn.z), 1.0e-12f);
+  const f3 nv = {nIn.x / l1, nIn.y / l1, nIn.z / l1};
+  float ex = nv.x, ey = nv.y;
+  if (nv.z < 0.0f) {
+    ex = (1.0f - std::fabs(nv.y)) * (nv.x >= 0.0f ? 1.0f : -1.0f);
+    ey = (1.0f - std::fabs(nv.x)) * (nv.y >= 0.0f ? 1.0f : -1.0f);
+  }
+  const uint32_t ox = f2u_sat(std::min(std::max(ex * 0.5f + 0.5f, 0.0f), 1.0f) * 255.0f + 0.5f);
+  const uint32_t oy = f2u_sat(std::min(std::max(ey * 0.5f + 0.5f, 0.0f), 1.0f) * 255.0f + 0.5f);
+  *hi = qz | ((ox | (oy << 8)) << 16);
+  return qx | (qy << 16);
+}
+
+void mesh_edge(const MeshU& M, const MCorner& a, const MCorner& b, uint32_t out[2]) {
+  const float t = (M.iso - a.d) / (b.d - a.d);
+  const float s = 1.0f - t;
+  const f3 p = {a.p.x * s + b.p.x * t, a.p.y * s + b.p.y * t, a.p.z * s + b.p.z * t};
+  const f3 g = {a.g.x * s + b.g.x * t, a.g.y * s + b.g.y * t, a.g.z * s + b.g.z * t};
+  out[0] = mesh_pack(M, p, {-g.x, -g.y, -g.z}, &out[1]);
+}
+
+struct MeshSink {
+  std::vector<uint32_t>* verts;
+  uint64_t count = 0, limit = 0;
+  void tri(const uint32_t a[2], const uint32_t b[2], const uint32_t c[2]) {
+    if (count < limit) {
+      uint32_t* o = verts->data() + count * 6;
+      o[0] = a[0]; o[1] = a[1]; o[2] = b[0]; o[3] = b[1]; o[4] = c[0]; o[5] = c[1];
+    }
+    count++;
+  }
+};
+
+// emitTet / emitLone / emitQuad (src/mesh_wgsl.js:154-196)
+void mesh_tet(const MeshU& M, MeshSink& S, const MCorner& a, const MCorner& b, const MCorner& c,
+              const MCorner& d) {
+  const bool ia = a.d > M.iso, ib = b.d > M.iso, ic = c.d > M.iso, id = d.d > M.iso;
+  const int nin = (int)ia + (int)ib + (int)ic + (int)id;
+  if (nin == 0 || nin == 4) return;
+  auto lone = [&](const MCorner& l, const MCorner& p1, const MCorner& p2, const MCorner& p3) {
+    uint32_t e1[2], e2[2], e3[2];
+    mesh_edge(M, l, p1, e1);
+    mesh_edge(M, l, p2, e2);
+    mesh_edge(M, l, p3, e3);
+    S.tri(e1, e2, e3);
+  };
+  auto quad = [&](const MCorner& qa, const MCorner& qb, const MCorner& qc, const MCorner& qd) {
+    uint32_t q0[2], q1[2], q2[2], q3[2];
+    mesh_edge(M, qa, qc, q0);
+    mesh_edge(M, qa, qd, q1);
+    mesh_edge(M, qb, qd, q2);
+    mesh_edge(M, qb, qc, q3);
+    S.tri(q0, q1, q2);
+    S.tri(q0, q2, q3);
+  };
+  if (nin == 1 || nin == 3) {
+    const bool look = nin == 1;
+    if (ia == look) lone(a, b, c, d);
+    else if (ib == look) lone(b, a, c, d);
+    else if (ic == look) lone(c, a, b, d);
+    else lone(d, a, b, c);
+  } else {
+    if (ia && ib) quad(a, b, c, d);
+    else if (ia && ic) quad(a, c, b, d);
+    else if (ia && id) quad(a, d, b, c);
+    else if (ib && ic) quad(b, c, a, d);
+    else if (ib && id) quad(b, d, a, c);
+    else quad(c, d, a, b);
+  }
+}
+
+}  // namespace
+
+int orc_mesh(orc_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
+  if (!s || !s->ready || !mp || mp->resolution < 1 || mp->max_triangles < 0) return P4A_ERR_ARG;
+  const double* box = s->params.box;
+  const double longest = std::max(box[0], std::max(box[1], box[2]));
+  const double voxel = longest / mp->resolution;
+  MeshU M{};
+  for (int k = 0; k < 3; k++) {
+    M.dim[k] = (int)std::ceil(box[k] / voxel) + 2 + 1;
+    M.origin[k] = (float)(0.0 - voxel);
+    M.simDim[k] = s->gridDim[k];
+  }
+  M.voxel = (float)voxel;
+  M.iso = (float)mp->iso;
+  M.invSupport = (float)(1 / s->h);
+  M.support2 = (float)(s->h * s->h);
+  M.poly6 = (float)(315 / (64 * kPI * std::pow(s->h, 9)));
+  M.mass = s->P.mass;
+  M.rho0 = (float)s->params.rest_density;
+  M.maxTris = (uint32_t)mp->max_triangles;
+  M.skipBodies = s->nBodyParts > 0 ? 1u : 0u;
+  const size_t nVerts = (size_t)M.dim[0] * M.dim[1] * M.dim[2];
+  const int par = s->parity;
+  const std::vector<f4>& pos = s->pos[par];
+  const std::vector<u4>& body = s->body[par];
+  // meshDensity (src/mesh_wgsl.js:23-69)
+  std::vector<float>& F = s->meshField;
+  F.assign(nVerts, 0.0f);
+  const float rhoMin = 0.5f * M.rho0;
+#pragma omp parallel for schedule(dynamic, 1024)
+  for (long long idx = 0; idx < (long long)nVerts; idx++) {
+    const int vx = (int)(idx % M.dim[0]), vy = (int)((idx / M.dim[0]) % M.dim[1]),
+              vz = (int)(idx / ((long long)M.dim[0] * M.dim[1]));
+    const f3 p = {M.origin[0] + M.voxel * (float)vx, M.origin[1] + M.voxel * (float)vy,
+                  M.origin[2] + M.voxel * (float)vz};
+    const int cx = std::min(std::max(f2i_sat(std::floor((p.x - 0.0f) * M.invSupport)), 0), M.simDim[0] - 1);
+    const int cy = std::min(std::max(f2i_sat(std::floor((p.y - 0.0f) * M.invSupport)), 0), M.simDim[1] - 1);
+    const int cz = std::min(std::max(f2i_sat(std::floor((p.z - 0.0f) * M.invSupport)), 0), M.simDim[2] - 1);
+    const int x0 = std::max(cx - 1, 0), x1 = std::min(cx + 1, M.simDim[0] - 1);
+    float acc = 0.0f;
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = cz + dz;
+      if (z < 0 || z >= M.simDim[2]) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int y = cy + dy;
+        if (y < 0 || y >= M.simDim[1]) continue;
+        const uint32_t rowBase = (uint32_t)((z * M.simDim[1] + y) * M.simDim[0]);
+        const uint32_t b = s->cellStart[rowBase + x0];
+        const uint32_t e = std::min(s->cellStart[rowBase + x1 + 1], (uint32_t)s->n);
+        for (uint32_t j = b; j < e; j++) {
+          if (M.skipBodies != 0u && body[j].x != 0u) continue;
+          const float vol = M.mass / std::max(s->density[j], rhoMin);
+          const f3 r = sub3(p, xyz(pos[j]));
+          const float r2 = dot3(r, r);
+          if (r2 >= M.support2) continue;
+          const float t = M.support2 - r2;
+          acc = std::fmaf(((vol * M.poly6) * t) * t, t, acc);
+        }
+      }
+    }
+    F[(size_t)idx] = acc;
+  }
+  // blur passes, then the normal field
+  for (int k = 0; k < 3 * mp->field_passes; k++) mesh_blur(F, M, mp->blur_axes ? k % 3 : 0);
+  s->meshNField = F;
+  for (int k = 0; k < 3 * mp->normal_passes; k++) mesh_blur(s->meshNField, M, mp->blur_axes ? k % 3 : 0);
+  const std::vector<float>& NF = mp->normal_passes > 0 ? s->meshNField : F;
+  // meshMarch (src/mesh_wgsl.js:198-238), triangles in voxel order
+  const size_t tris = (size_t)mp->max_triangles;
+  s->meshVerts.assign(std::max<size_t>(1, tris) * 6, 0u);
+  MeshSink sink{&s->meshVerts, 0, tris};
+  static const int tets[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+  for (int vz = 0; vz < M.dim[2] - 1; vz++)
+    for (int vy = 0; vy < M.dim[1] - 1; vy++)
+      for (int vx = 0; vx < M.dim[0] - 1; vx++) {
+        MCorner cn[8];
+        int mask = 0;
+        for (int k = 0; k < 8; k++) {
+          const int x = vx + (k & 1), y = vy + ((k >> 1) & 1), z = vz + ((k >> 2) & 1);
+          cn[k].d = mesh_at(F, M, x, y, z);
+          mask |= (cn[k].d > M.iso ? 1 : 0) << k;
+        }
+        if (mask == 0 || mask == 255) continue;
+        for (int k = 0; k < 8; k++) {
+          const int x = vx + (k & 1), y = vy + ((k >> 1) & 1), z = vz + ((k >> 2) & 1);
+          cn[k].p = {(float)x, (float)y, (float)z};
+          cn[k].g = {mesh_at(NF, M, x + 1, y, z) - mesh_at(NF, M, x - 1, y, z),
+                     mesh_at(NF, M, x, y + 1, z) - mesh_at(NF, M, x, y - 1, z),
+                     mesh_at(NF, M, x, y, z + 1) - mesh_at(NF, M, x, y, z - 1)};
+        }
+        for (int t = 0; t < 6; t++) mesh_tet(M, sink, cn[tets[t][0]], cn[tets[t][1]], cn[tets[t][2]], cn[tets[t][3]]);
+      }
+  s->meshTris = (int64_t)sink.count;
+  s->meshVerts.resize((size_t)std::min<uint64_t>(sink.count, tris) * 6);
+  if (!(mp->normal_passes > 0)) s->meshNField = F;
+  if (triangles) *triangles = s->meshTris;
+  return P4A_OK;
+}
+
 int orc_stats(const orc_sim* s, p4a_stats* out) {
   if (!s || !out) return P4A_ERR_ARG;
   *out = s->stats;
@@ -1569,6 +1788,9 @@ int orc_buffer(orc_sim* s, int32_t id, int32_t which, void** ptr, size_t* bytes)
     case P4A_BUF_STATS_OUT: return set(s->statsOut.data(), s->statsOut.size() * 4);
     case P4A_BUF_SMOOTH_POS: return set(s->smoothPos.data(), s->smoothPos.size() * 16);
     case P4A_BUF_ANISO_G: return set(s->anisoG.data(), s->anisoG.size() * 16);
+    case P4A_BUF_MESH_FIELD: return set(s->meshField.data(), s->meshField.size() * 4);
+    case P4A_BUF_MESH_NFIELD: return set(s->meshNField.data(), s->meshNField.size() * 4);
+    case P4A_BUF_MESH_VERTS: return set(s->meshVerts.data(), s->meshVerts.size() * 4);
     default: return P4A_ERR_ARG;
   }
 }

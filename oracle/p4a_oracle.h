@@ -61,6 +61,8 @@ int orc_hold_body(orc_sim* s, int32_t body_1based, const double target[3], doubl
 int orc_release_body(orc_sim* s);
 int orc_resize_box(orc_sim* s, const double box[3]);
 int orc_aniso(orc_sim* s, const p4a_aniso_params* ap);
+/* SurfaceMesh.configure + generate (src/mesh.js:99-352): triangles in voxel order. */
+int orc_mesh(orc_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
 int orc_get_info(const orc_sim* s, p4a_info* out);
 int orc_stats(const orc_sim* s, p4a_stats* out);
 /* Host pointer + bytes of a buffer (same ids / which as p4a_buffer). */

@@ -9,7 +9,8 @@ SHAPES = {"sphere": 0, "torus": 1, "box": 2}
 BUF = dict(
     pos=0, vel=1, pred=2, body=3, rest=4, density=5, lambda_=6, corr=7, normal=8,
     cellStart=9, bpos=10, bpsi=11, bcellStart=12, bodyCentre=13, bodyRef=14,
-    bodyRot=15, bodyInfo=16, statsOut=17, smoothPos=18, aniso=19,
+    bodyRot=15, bodyInfo=16, statsOut=17, smoothPos=18, aniso=19, meshField=20, meshNField=21,
+    meshVerts=22,
 )
 # element dtype / components of each buffer (numpy dtype string, components)
 BUF_LAYOUT = {
@@ -17,6 +18,7 @@ BUF_LAYOUT = {
     5: ("f4", 1), 6: ("f4", 1), 7: ("f4", 4), 8: ("f4", 4), 9: ("u4", 1),
     10: ("f4", 4), 11: ("f4", 1), 12: ("u4", 1), 13: ("f4", 4), 14: ("f4", 4),
     15: ("f4", 4), 16: ("f4", 4), 17: ("u4", 1), 18: ("f4", 4), 19: ("f4", 4),
+    20: ("f4", 1), 21: ("f4", 1), 22: ("u4", 2),
 }
 A, B, LIVE = 0, 1, -1
 
@@ -73,6 +75,16 @@ class AnisoParams(C.Structure):
         ("lonely", C.c_double), ("min_neighbours", C.c_int32), ("lambda_", C.c_double),
         ("radius_scale", C.c_double), ("min_extent", C.c_double),
     ]
+
+
+class MeshParams(C.Structure):
+    _fields_ = [("resolution", C.c_int32), ("iso", C.c_double), ("field_passes", C.c_int32),
+                ("normal_passes", C.c_int32), ("max_triangles", C.c_int64), ("blur_axes", C.c_int32)]
+
+
+class MeshInfo(C.Structure):
+    _fields_ = [("vert_dim", C.c_int32 * 3), ("origin", C.c_double * 3), ("voxel", C.c_double),
+                ("triangles", C.c_int64), ("mesh_gen", C.c_int32)]
 
 
 class Grid(C.Structure):

@@ -72,6 +72,9 @@ SIGNATURES = {
     "p4a_tune_set": ([_i32, C.c_int64, _i32], C.c_int),
     "p4a_tune_clear": ([_i32], C.c_int),
     "p4a_tune_get": ([_i32, C.c_int64, C.POINTER(_i32)], C.c_int),
+    "p4a_default_mesh_params": ([_vp], C.c_int),
+    "p4a_mesh": ([_vp, _vp, C.POINTER(C.c_int64)], C.c_int),
+    "p4a_mesh_get_info": ([_vp, _vp], C.c_int),
 }
 
 _lib = None

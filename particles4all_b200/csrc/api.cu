@@ -38,12 +38,12 @@ const double kPi = 3.14159265358979323846;
 enum Phase {
   PH_DRAG, PH_KEY_COUNT, PH_SCAN, PH_FILL, PH_REORDER, PH_BODY_SEED, PH_LAMBDA, PH_DELTA,
   PH_BODY_MATCH, PH_XSPH_FINALIZE, PH_XSPH_NORMALS, PH_TENSION_FINALIZE, PH_ANISO, PH_IMPULSE,
-  PH_RESIZE, PH_STATS_CLEAR, PH_COUNT, PH_END = PH_COUNT
+  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_COUNT, PH_END = PH_COUNT
 };
 const char* const kPhaseNames[PH_COUNT] = {
     "body_drag", "key_count", "scan", "fill", "reorder", "body_seed", "lambda", "delta",
     "body_match", "xsph_finalize", "xsph_normals", "tension_finalize", "aniso", "impulse",
-    "resize", "stats_clear"};
+    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march"};
 
 std::atomic<uint64_t> g_launches{0};
 }  // namespace
@@ -87,6 +87,20 @@ struct p4a_sim {
   float4* anisoG = nullptr;
   size_t anisoCap = 0;
   int anisoGen = 0;
+  // surface mesh (p4a_mesh)
+  float* meshField[3] = {nullptr, nullptr, nullptr};  // field, normal field, blur scratch
+  uint32_t* meshCounts = nullptr;                     // per voxel, zero between calls
+  uint32_t* meshOffsets = nullptr;                    // [nvox + 1]
+  unsigned long long* meshScan = nullptr;
+  uint32_t* meshTicket = nullptr;
+  uint2* meshVerts = nullptr;
+  size_t meshVertCap = 0, meshVoxCap = 0, meshTriCap = 0;
+  int fieldSlot = 0, nfieldSlot = 1;  // which of meshField[] hold the fields
+  int meshGen = 0;
+  int32_t meshDim[3] = {0, 0, 0};
+  double meshOrigin = 0, meshVoxel = 0;
+  int64_t meshTris = 0;
+  uint32_t meshEpoch = 0;
   bool ready = false;
   // per-kernel timing (p4a_profile_*)
   bool prof = false;
@@ -498,6 +512,17 @@ int buffer_ptr(p4a_sim* s, int32_t id, int32_t which, void** p, size_t* bytes) {
     case P4A_BUF_STATS_OUT: *p = s->d.statsOut; *bytes = 32; break;
     case P4A_BUF_SMOOTH_POS: *p = s->smoothPos; *bytes = s->smoothPos ? (size_t)s->n * 16 : 0; break;
     case P4A_BUF_ANISO_G: *p = s->anisoG; *bytes = s->anisoG ? (size_t)s->n * 32 : 0; break;
+    case P4A_BUF_MESH_FIELD:
+    case P4A_BUF_MESH_NFIELD: {
+      const size_t nv = (size_t)s->meshDim[0] * s->meshDim[1] * s->meshDim[2];
+      *p = s->meshField[id == P4A_BUF_MESH_FIELD ? s->fieldSlot : s->nfieldSlot];
+      *bytes = *p ? nv * 4 : 0;
+      break;
+    }
+    case P4A_BUF_MESH_VERTS:
+      *p = s->meshVerts;
+      *bytes = s->meshVerts ? (size_t)std::min<int64_t>(s->meshTris, (int64_t)s->meshTriCap) * 24 : 0;
+      break;
     default: return fail(s, P4A_ERR_ARG, "unknown buffer id %d", id);
   }
   return P4A_OK;
@@ -591,6 +616,13 @@ int p4a_destroy(p4a_sim* s) {
   free_list(s->boundaryAllocs);
   if (s->smoothPos) cudaFree(s->smoothPos);
   if (s->anisoG) cudaFree(s->anisoG);
+  for (float* f : s->meshField)
+    if (f) cudaFree(f);
+  if (s->meshCounts) cudaFree(s->meshCounts);
+  if (s->meshOffsets) cudaFree(s->meshOffsets);
+  if (s->meshScan) cudaFree(s->meshScan);
+  if (s->meshTicket) cudaFree(s->meshTicket);
+  if (s->meshVerts) cudaFree(s->meshVerts);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
@@ -1001,6 +1033,157 @@ int p4a_aniso(p4a_sim* s, const p4a_aniso_params* ap) {
   launch_aniso(A, s->d.pos[s->parity], s->d.cellStart, s->smoothPos, s->anisoG, s->stream);
   mark(s, PH_END);
   CUDA_TRY(s, cudaGetLastError());
+  return P4A_OK;
+}
+
+int p4a_default_mesh_params(p4a_mesh_params* m) {
+  if (!m) return P4A_ERR_ARG;
+  *m = p4a_mesh_params{};
+  m->resolution = 128;  // src/main.js:320
+  m->iso = 0.4;         // src/main.js:321
+  m->field_passes = 0;  // src/main.js:323
+  m->normal_passes = 2; // src/main.js:324
+  m->max_triangles = 3000000;  // src/mesh.js:17
+  m->blur_axes = 0;
+  return P4A_OK;
+}
+
+// SurfaceMesh.configure + generate (src/mesh.js:99-146, 326-352) on the live buffers.
+int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
+  if (!s || !mp || mp->resolution < 1 || mp->max_triangles < 0 || mp->field_passes < 0 ||
+      mp->normal_passes < 0 || mp->max_triangles > 0x7fffffffLL)
+    return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "mesh before reset");
+  cudaSetDevice(s->device);
+  const double* box = s->params.box;
+  const double longest = std::max(box[0], std::max(box[1], box[2]));
+  const double voxel = longest / mp->resolution;
+  int32_t dim[3];
+  for (int k = 0; k < 3; k++) dim[k] = (int32_t)std::ceil(box[k] / voxel) + 2 + 1;
+  const double nv = (double)dim[0] * dim[1] * dim[2];
+  if (nv > 0x7fffffff || std::max(dim[0], std::max(dim[1], dim[2])) > 8192)
+    return fail(s, P4A_ERR_CAPACITY, "mesh grid too large");
+  const size_t nVerts = (size_t)nv;
+  const size_t nvox = (size_t)(dim[0] - 1) * (dim[1] - 1) * (dim[2] - 1);
+  const size_t tris = (size_t)mp->max_triangles;
+  if (nVerts > s->meshVertCap || nvox > s->meshVoxCap || tris != s->meshTriCap) {  // src/mesh.js:105-125
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (nVerts > s->meshVertCap) {
+      for (float*& f : s->meshField) {
+        if (f) cudaFree(f);
+        f = nullptr;
+      }
+      s->meshVertCap = 0;
+      for (float*& f : s->meshField) CUDA_TRY(s, cudaMalloc((void**)&f, nVerts * 4));
+      s->meshVertCap = nVerts;
+    }
+    if (nvox > s->meshVoxCap) {
+      if (s->meshCounts) cudaFree(s->meshCounts);
+      if (s->meshOffsets) cudaFree(s->meshOffsets);
+      if (s->meshScan) cudaFree(s->meshScan);
+      s->meshCounts = s->meshOffsets = nullptr;
+      s->meshScan = nullptr;
+      s->meshVoxCap = 0;
+      CUDA_TRY(s, cudaMalloc((void**)&s->meshCounts, nvox * 4));
+      CUDA_TRY(s, cudaMemset(s->meshCounts, 0, nvox * 4));
+      CUDA_TRY(s, cudaMalloc((void**)&s->meshOffsets, (nvox + 1) * 4));
+      CUDA_TRY(s, cudaMalloc((void**)&s->meshScan, (size_t)scan_tiles((int)nvox) * 8));
+      CUDA_TRY(s, cudaMemset(s->meshScan, 0, (size_t)scan_tiles((int)nvox) * 8));
+      if (!s->meshTicket) {
+        CUDA_TRY(s, cudaMalloc((void**)&s->meshTicket, 16));
+        CUDA_TRY(s, cudaMemset(s->meshTicket, 0, 16));
+      }
+      s->meshVoxCap = nvox;
+    }
+    if (tris != s->meshTriCap) {
+      if (s->meshVerts) cudaFree(s->meshVerts);
+      s->meshVerts = nullptr;
+      s->meshTriCap = 0;
+      CUDA_TRY(s, cudaMalloc((void**)&s->meshVerts, std::max<size_t>(1, tris) * 24));
+      s->meshTriCap = tris;
+    }
+    s->meshGen++;
+  }
+  // uniform (src/mesh.js:137-153)
+  const double h = s->h;
+  MeshParams M{};
+  for (int k = 0; k < 3; k++) {
+    M.vertDim[k] = dim[k];
+    M.gridOrigin[k] = (float)(0.0 - voxel);
+    M.boxMin[k] = 0.0f;
+    M.simGridDim[k] = s->gridDim[k];
+  }
+  M.voxel = (float)voxel;
+  M.iso = (float)mp->iso;
+  M.invSupport = (float)(1 / h);
+  M.support2 = (float)(h * h);
+  M.poly6 = (float)(315 / (64 * kPi * std::pow(h, 9)));
+  M.mass = (float)s->sc.mass;
+  M.rho0 = (float)s->params.rest_density;
+  M.maxTris = (uint32_t)tris;
+  M.skipBodies = s->nBodyParts > 0 ? 1u : 0u;
+  cudaStream_t st = s->stream;
+  const int par = s->parity;
+  float* buf[3] = {s->meshField[0], s->meshField[1], s->meshField[2]};
+  mark(s, PH_MESH_FIELD);
+  launch_mesh_field(M, s->d.pos[par], s->d.density, s->d.cellStart, s->d.body[par], (uint32_t)s->n, buf[0], st);
+  // blur passes: consecutive passes along one axis run in one launch
+  auto blur = [&](int from, int to, int steps) -> int {
+    int cur = from;
+    for (int k = 0; k < steps;) {
+      const int axis = mp->blur_axes ? k % 3 : 0;
+      int run = 1;
+      while (k + run < steps && (mp->blur_axes ? (k + run) % 3 : 0) == axis) run++;
+      const int dst = (k + run == steps) ? to : (cur == 2 ? to : 2);
+      const cudaError_t e = launch_mesh_blur(M, buf[cur], buf[dst], axis, run, st);
+      if (e != cudaSuccess) return fail(s, P4A_ERR_CUDA, "mesh blur: %s", cudaGetErrorString(e));
+      cur = dst;
+      k += run;
+    }
+    return P4A_OK;
+  };
+  mark(s, PH_MESH_BLUR);
+  int rc;
+  if ((rc = blur(0, 0, 3 * mp->field_passes))) return rc;
+  s->fieldSlot = 0;
+  if (mp->normal_passes > 0) {
+    if ((rc = blur(0, 1, 3 * mp->normal_passes))) return rc;
+    s->nfieldSlot = 1;
+  } else {
+    s->nfieldSlot = 0;
+  }
+  mark(s, PH_MESH_MARCH);
+  launch_mesh_count(M, buf[0], s->meshCounts, (uint32_t)nvox, st);
+  launch_scan(s->meshCounts, s->meshOffsets, (int)nvox, s->meshScan, s->meshTicket, ++s->meshEpoch & 0x3fffffffu,
+              s->d.errorWord, st);
+  launch_mesh_emit(M, buf[0], buf[s->nfieldSlot], s->meshOffsets, (uint32_t)nvox, s->meshVerts, st);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  for (int k = 0; k < 3; k++) s->meshDim[k] = dim[k];
+  s->meshOrigin = -voxel;
+  s->meshVoxel = voxel;
+  if (triangles) {
+    uint32_t t = 0;
+    CUDA_TRY(s, cudaMemcpyAsync(&t, s->meshOffsets + nvox, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(s, cudaStreamSynchronize(st));
+    s->meshTris = t;
+    *triangles = t;
+  } else {
+    s->meshTris = (int64_t)tris;  // unknown until waited for: the stored capacity bounds it
+  }
+  return P4A_OK;
+}
+
+int p4a_mesh_get_info(p4a_sim* s, p4a_mesh_info* o) {
+  if (!s || !o) return P4A_ERR_ARG;
+  *o = p4a_mesh_info{};
+  for (int k = 0; k < 3; k++) {
+    o->vert_dim[k] = s->meshDim[k];
+    o->origin[k] = s->meshOrigin;
+  }
+  o->voxel = s->meshVoxel;
+  o->triangles = s->meshTris;
+  o->mesh_gen = s->meshGen;
   return P4A_OK;
 }
 

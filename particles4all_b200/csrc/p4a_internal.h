@@ -59,6 +59,16 @@ struct AnisoParams {
   float minExtent; int32_t neps;
 };
 
+// Mesh uniform (src/mesh_wgsl.js:3-21, packed by src/mesh.js:137-153).
+struct MeshParams {
+  int32_t vertDim[3]; float voxel;
+  float gridOrigin[3]; float iso;
+  float boxMin[3]; float invSupport;
+  int32_t simGridDim[3]; float support2;
+  float poly6, mass, rho0;
+  uint32_t maxTris, skipBodies;
+};
+
 // Device error word bits (set by kernels, read by the host at sync points).
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };
 
@@ -204,5 +214,15 @@ void launch_resize(uint32_t n, float4* pos, const float oldSize[3], const float 
                    const float clampMin[3], const float clampMax[3], cudaStream_t st);
 void launch_aniso(const AnisoParams& A, const float4* pos, const uint32_t* cellStart,
                   float4* smoothPos, float4* g, cudaStream_t st, int variant = -1);
+
+
+// ---- surface mesh (kernels_mesh.cu) ----
+void launch_mesh_field(const MeshParams& M, const float4* pos, const float* rho, const uint32_t* cs,
+                       const uint4* body, uint32_t n, float* field, cudaStream_t st);
+cudaError_t launch_mesh_blur(const MeshParams& M, const float* src, float* dst, int axis, int passes,
+                             cudaStream_t st);
+void launch_mesh_count(const MeshParams& M, const float* field, uint32_t* counts, uint32_t nvox, cudaStream_t st);
+void launch_mesh_emit(const MeshParams& M, const float* field, const float* nfield, const uint32_t* offsets,
+                      uint32_t nvox, uint2* verts, cudaStream_t st);
 
 }  // namespace p4a

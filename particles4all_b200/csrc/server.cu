@@ -47,6 +47,7 @@ using namespace p4a;
 namespace {
 
 using Clock = std::chrono::steady_clock;
+constexpr double kAdmitSecondsPerTurn = 0.004;
 
 // First-fit ranges of one pinned host slab, shared by threads.
 class PinnedPool {
@@ -487,6 +488,8 @@ bool admit(p4a_server* S) {
   std::vector<std::pair<unsigned char*, size_t>> blobs;
   const double t = S->now();
   for (auto it = S->admitQ.begin(); it != S->admitQ.end();) {
+    // bounded admission work per engine turn, so frames keep flowing
+    if (S->now() - t > kAdmitSecondsPerTurn) break;
     const int32_t h = *it;
     SScene& sc = S->scenes[h];
     if (sc.destroyWanted) {

@@ -153,3 +153,19 @@ def aniso_struct(a):
     s.min_neighbours = int(a["min_neighbours"])
     s.lambda_, s.radius_scale, s.min_extent = a["lambda"], a["radius_scale"], a["min_extent"]
     return s
+
+
+def default_mesh():
+    """SurfaceMesh / UI defaults (src/main.js:320-327, src/mesh.js:17): resolution 128,
+    iso 0.4, no field passes, 2 normal passes, 3 M triangles; blur along x as the
+    reference executes it (blur_axes 0)."""
+    return {"resolution": 128, "iso": 0.4, "field_passes": 0, "normal_passes": 2,
+            "max_triangles": 3_000_000, "blur_axes": 0}
+
+
+def mesh_struct(m):
+    s = _abi.MeshParams()
+    s.resolution, s.iso = int(m["resolution"]), float(m["iso"])
+    s.field_passes, s.normal_passes = int(m["field_passes"]), int(m["normal_passes"])
+    s.max_triangles, s.blur_axes = int(m["max_triangles"]), int(m["blur_axes"])
+    return s

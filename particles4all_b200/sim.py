@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _abi
 from ._lib import check, lib
-from .params import CParams, aniso_struct, default_aniso
+from .params import CParams, aniso_struct, default_aniso, default_mesh, mesh_struct
 
 
 class Sim:
@@ -108,6 +108,21 @@ class Sim:
         """The anisotropic-kernel pass (src/aniso_wgsl.js, src/mesh.js:207-261)."""
         s = aniso_struct(aparams or default_aniso())
         check(self._L.p4a_aniso(self._h, C.byref(s)), self._h, "aniso")
+
+    def mesh(self, mparams=None, wait=True):
+        """SurfaceMesh.generate (src/mesh.js:99-352) on the live buffers; returns the
+        triangle count (None when wait=False). Results: read('meshField'),
+        read('meshNField'), read('meshVerts') (uint2 per vertex, 3 per triangle)."""
+        m = mesh_struct(mparams or default_mesh())
+        t = C.c_int64()
+        check(self._L.p4a_mesh(self._h, C.byref(m), C.byref(t) if wait else None), self._h, "mesh")
+        return t.value if wait else None
+
+    def mesh_info(self):
+        i = _abi.MeshInfo()
+        check(self._L.p4a_mesh_get_info(self._h, C.byref(i)), self._h, "mesh_info")
+        return {"vert_dim": list(i.vert_dim), "origin": list(i.origin), "voxel": i.voxel,
+                "triangles": i.triangles, "mesh_gen": i.mesh_gen}
 
     # ---- fields --------------------------------------------------------------
     def info(self):
