@@ -321,6 +321,7 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.key, cap)) || (rc = dalloc(s, L, &s->d.rank, cap)) ||
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbMask, cap * 9)) ||
+      (rc = dalloc(s, L, &s->d.nbBMask, cap * 9)) ||
       (rc = dalloc(s, L, &s->d.nbLong, cap)))
     return rc;
   s->d.cap = (uint32_t)cap;

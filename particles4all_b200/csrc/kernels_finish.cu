@@ -83,21 +83,28 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
     const float4 p4 = __ldg(&pred[i]);
     const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
     const RowWalk w(P, pi);
-    F3 acc = {0.f, 0.f, 0.f};
+    const RowStage<kBlock, false> st;
+    uint32_t todo = 0u, longRows = 0u;
 #pragma unroll
     for (int r = 0; r < kRows; r++) {
       const int rb = w.row_base(P, r);
       if (rb < 0) continue;
       bool lg;
-      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
-      visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
-        if (j == i) return;
-        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-        const float r2 = dot3(rij, rij);
-        const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
-        acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
-      });
+      uint32_t b;
+      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
+      st.set(r, lg ? 0ull : mr, b);
+      longRows |= (uint32_t)lg << r;
+      todo |= (uint32_t)(mr != 0ull || lg) << r;
     }
+    F3 acc = {0.f, 0.f, 0.f};
+    auto fluid = [&](uint32_t j) {
+      if (j == i) return;
+      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const float r2 = dot3(rij, rij);
+      const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
+      acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+    };
+    walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
     const F3 corr = mul3(acc, P.xsphC);
     vf = add3(vi, corr);
     d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
@@ -109,6 +116,7 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
 }
 
 // xsph + normals (tension scenes): corr = xsphC * acc, normal = h * nacc.
+template <int TB>
 __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
@@ -119,31 +127,36 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i])), vi = xyz(__ldg(&velIn[i]));
   const RowWalk w(P, pi);
-  uint32_t longRows = 0u;
-  F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
+  const RowStage<TB, false> st;
+  uint32_t todo = 0u, longRows = 0u;
 #pragma unroll
   for (int r = 0; r < kRows; r++) {
     const int rb = w.row_base(P, r);
     if (rb < 0) continue;
     bool lg;
-    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
+    uint32_t b;
+    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
     d.nbMask[(size_t)r * cap + i] = mr;
-    if (lg) longRows |= 1u << r;
-    visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
-      if (j == i) return;
-      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-      const float r2 = dot3(rij, rij);
-      const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
-      const float f = P.mass * poly6(P, r2) / dj;
-      acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
-      if (r2 < 1.0e-12f) return;
-      const float rr = sqrtf(r2);
-      const float hr = P.h - rr;
-      const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / rr);
-      nacc = fma3(coef, rij, nacc);
-    });
+    st.set(r, lg ? 0ull : mr, b);
+    longRows |= (uint32_t)lg << r;
+    todo |= (uint32_t)(mr != 0ull || lg) << r;
   }
   d.nbLong[i] = longRows;
+  F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
+  auto fluid = [&](uint32_t j) {
+    if (j == i) return;
+    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    const float r2 = dot3(rij, rij);
+    const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
+    const float f = P.mass * poly6(P, r2) / dj;
+    acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+    if (r2 < 1.0e-12f) return;
+    const float rr = sqrtf(r2);
+    const float hr = P.h - rr;
+    const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / rr);
+    nacc = fma3(coef, rij, nacc);
+  };
+  walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
   d.corr[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
   d.normal[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
 }
@@ -166,28 +179,34 @@ __device__ __forceinline__ void tension_finalize_body(const SimParams& P, const 
     rhoi = __ldg(&d.density[i]);
     const RowWalk w(P, pi);
     const uint32_t longRows = __ldg(&d.nbLong[i]);
-    F3 acc = {0.f, 0.f, 0.f};
+    const RowStage<kBlock, false> st;
+    uint32_t todo = 0u;
 #pragma unroll
     for (int r = 0; r < kRows; r++) {
       const int rb = w.row_base(P, r);
       if (rb < 0) continue;
       const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
-      visit_row(P, w, rb, pi, mr, (longRows >> r) & 1u, pred, cs, [&](uint32_t j) {
-        const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-        const float r2 = dot3(rij, rij);
-        if (r2 < 1.0e-12f || j == i) return;
-        const float rr = sqrtf(r2);
-        const float hrr = P.h - rr;
-        const float k = hrr * hrr * hrr * rr * rr * rr;
-        float cw = P.cohes * (2.0f * k - P.cohesTerm);
-        if (2.0f * rr > P.h) cw = P.cohes * k;
-        const float sCoh = -P.tension * P.mass * cw / rr;
-        const F3 fCoh = mul3(rij, sCoh);
-        const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
-        const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&d.density[j]));
-        acc = fma3(wgt, add3(fCoh, fCurv), acc);
-      });
+      const bool lg = (longRows >> r) & 1u;
+      st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]));
+      todo |= (uint32_t)(mr != 0ull || lg) << r;
     }
+    F3 acc = {0.f, 0.f, 0.f};
+    auto fluid = [&](uint32_t j) {
+      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const float r2 = dot3(rij, rij);
+      if (r2 < 1.0e-12f || j == i) return;
+      const float rr = sqrtf(r2);
+      const float hrr = P.h - rr;
+      const float k = hrr * hrr * hrr * rr * rr * rr;
+      float cw = P.cohes * (2.0f * k - P.cohesTerm);
+      if (2.0f * rr > P.h) cw = P.cohes * k;
+      const float sCoh = -P.tension * P.mass * cw / rr;
+      const F3 fCoh = mul3(rij, sCoh);
+      const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
+      const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&d.density[j]));
+      acc = fma3(wgt, add3(fCoh, fCurv), acc);
+    };
+    walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
     const float4 c0 = d.corr[i];
     const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
     d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);
@@ -213,15 +232,12 @@ __global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize_b(const __grid_cons
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_xsph_normals(const __grid_constant__ SimParams P,
                                                          const __grid_constant__ DevScene d, int) {
-  xsph_normals_body(P, d, blockIdx.x * TB + threadIdx.x);
+  xsph_normals_body<TB>(P, d, blockIdx.x * TB + threadIdx.x);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_xsph_normals_b(const __grid_constant__ BatchWork w,
                                                            const __grid_constant__ DevScene d, int) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
-#pragma unroll 1
-    for (int s = 0; s < kBlock; s += TB) xsph_normals_body(P, d, t * kBlock + s + threadIdx.x);
-  });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { xsph_normals_body<TB>(P, d, li); });
 }
 using PlainFn = void (*)(SimParams, DevScene, int);
 using BatchFn = void (*)(BatchWork, DevScene, int);

@@ -23,8 +23,7 @@
 
 namespace p4a {
 
-__device__ __forceinline__ void key_count_body(const SimParams& P, const DevScene& d, uint32_t tile) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void key_count_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (d.bodyFill && li < P.nBodies) d.bodyFill[P.bOff + li] = 0u;
   const bool act = li < P.n;
   const uint32_t i = P.pOff + li;
@@ -47,16 +46,14 @@ __device__ __forceinline__ void key_count_body(const SimParams& P, const DevScen
   }
 }
 
-__device__ __forceinline__ void fill_body(const SimParams& P, const DevScene& d, uint32_t tile) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void fill_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const uint32_t at = __ldg(&d.cellStart[d.key[i]]) + d.rank[i];
   if (at < P.pEnd) d.unordered[at] = i;  // always true after a completed scan
 }
 
-__device__ __forceinline__ void reorder_body(const SimParams& P, const DevScene& d, uint32_t tile) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
+__device__ __forceinline__ void reorder_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int src = P.parity, dst = P.parity ^ 1;
@@ -89,27 +86,27 @@ __device__ __forceinline__ void reorder_body(const SimParams& P, const DevScene&
 
 __global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ SimParams P,
                                                       const __grid_constant__ DevScene d) {
-  key_count_body(P, d, blockIdx.x);
+  key_count_body(P, d, blockIdx.x * kBlock + threadIdx.x);
 }
 __global__ void __launch_bounds__(kBlock) k_key_count_b(const __grid_constant__ BatchWork w,
                                                         const __grid_constant__ DevScene d) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { key_count_body(P, d, t); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { key_count_body(P, d, li); });
 }
 __global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimParams P,
                                                  const __grid_constant__ DevScene d) {
-  fill_body(P, d, blockIdx.x);
+  fill_body(P, d, blockIdx.x * kBlock + threadIdx.x);
 }
 __global__ void __launch_bounds__(kBlock) k_fill_b(const __grid_constant__ BatchWork w,
                                                    const __grid_constant__ DevScene d) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { fill_body(P, d, t); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { fill_body(P, d, li); });
 }
 __global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimParams P,
                                                     const __grid_constant__ DevScene d) {
-  reorder_body(P, d, blockIdx.x);
+  reorder_body(P, d, blockIdx.x * kBlock + threadIdx.x);
 }
 __global__ void __launch_bounds__(kBlock) k_reorder_b(const __grid_constant__ BatchWork w,
                                                       const __grid_constant__ DevScene d) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { reorder_body(P, d, t); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { reorder_body(P, d, li); });
 }
 
 // Tile status word: epoch (30 bits) | flag (2 bits) | value (32 bits).

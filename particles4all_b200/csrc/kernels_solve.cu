@@ -21,6 +21,7 @@
 
 namespace p4a {
 
+template <int TB>
 __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
@@ -31,48 +32,72 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i]));
   const RowWalk w(P, pi);
-  uint32_t longRows = 0u;
-  float rho = P.mass * poly6(P, 0.0f);
-  F3 gradSum = {0.f, 0.f, 0.f};
-  float sumGrad2 = 0.0f;
+  const RowStage<TB, true> st;
+  // phase 1: fluid and boundary masks of every row (stored for delta)
+  uint32_t todo = 0u, longRows = 0u;
 #pragma unroll
   for (int r = 0; r < kRows; r++) {
     const int rb = w.row_base(P, r);
     if (rb < 0) continue;
     bool lg;
-    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg);
-    d.nbMask[(size_t)r * cap + i] = mr;
-    if (lg) longRows |= 1u << r;
-    visit_row(P, w, rb, pi, mr, lg, pred, cs, [&](uint32_t j) {
-      if (j == i) return;
-      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-      const float r2 = dot3(rij, rij);
-      rho = fmaf(P.mass, poly6(P, r2), rho);
-      if (r2 > 1.0e-12f) {
-        const float rr = sqrtf(r2);
-        const float hr = P.h - rr;
-        const float s = P.volume * P.spikyGrad * hr * hr / rr;
-        const F3 g = mul3(rij, s);
-        gradSum = add3(gradSum, g);
-        sumGrad2 = sumGrad2 + dot3(g, g);
-      }
-    });
+    uint32_t b;
+    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
+    uint32_t bm = 0u;
+    bool lgb = false;
     if (P.nBoundary > 0u) {
       const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-      for (uint32_t k = bb; k < be; k++) {
-        const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
-        const float r2 = dot3(rij, rij);
-        if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-        const float psi = __ldg(&d.bpsi[k]);
-        rho = fmaf(psi, poly6(P, r2), rho);
-        const float rr = sqrtf(r2);
-        const float hr = P.h - rr;
-        const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
-        gradSum = fma3(s, rij, gradSum);
-      }
+      if (be > bb) bm = boundary_mask(P, bb, be, pi, d.bpos, lgb);
     }
+    d.nbMask[(size_t)r * cap + i] = mr;
+    d.nbBMask[(size_t)r * cap + i] = bm;
+    st.set(r, lg ? 0ull : mr, b, lgb ? 0u : bm);
+    longRows |= ((uint32_t)lg << r) | ((uint32_t)lgb << (16 + r));
+    todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
   }
   d.nbLong[i] = longRows;
+  // phase 2
+  float rho = P.mass * poly6(P, 0.0f);
+  F3 gradSum = {0.f, 0.f, 0.f};
+  float sumGrad2 = 0.0f;
+  auto fluid = [&](uint32_t j) {
+    if (j == i) return;
+    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    const float r2 = dot3(rij, rij);
+    rho = fmaf(P.mass, poly6(P, r2), rho);
+    if (r2 > 1.0e-12f) {
+      const float rr = sqrtf(r2);
+      const float hr = P.h - rr;
+      const float s = P.volume * P.spikyGrad * hr * hr / rr;
+      const F3 g = mul3(rij, s);
+      gradSum = add3(gradSum, g);
+      sumGrad2 = sumGrad2 + dot3(g, g);
+    }
+  };
+  // one boundary sample k (1e-12 <= r^2 < h^2)
+  auto sample = [&](uint32_t k) {
+    const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+    const float r2 = dot3(rij, rij);
+    const float psi = __ldg(&d.bpsi[k]);
+    rho = fmaf(psi, poly6(P, r2), rho);
+    const float rr = sqrtf(r2);
+    const float hr = P.h - rr;
+    const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
+    gradSum = fma3(s, rij, gradSum);
+  };
+  walk_rows(
+      st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
+      [&](int r, uint32_t k) { sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
+      [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
+      [&](int r) {
+        const int rb = w.row_base(P, r);
+        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+        for (uint32_t k = bb; k < be; k++) {
+          const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+          sample(k);
+        }
+      });
   d.density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
   if (C > 0.0f) {
@@ -83,6 +108,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   }
 }
 
+template <int TB>
 __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
@@ -97,41 +123,57 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   const float li_ = __ldg(&lambda[i]);
   const RowWalk w(P, pi);
   const uint32_t longRows = __ldg(&d.nbLong[i]);
-  F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
-  float nc = 1.0f;
+  const RowStage<TB, true> st;
+  uint32_t todo = 0u;
 #pragma unroll
   for (int r = 0; r < kRows; r++) {
     const int rb = w.row_base(P, r);
     if (rb < 0) continue;
     const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
-    visit_row(P, w, rb, pi, mr, (longRows >> r) & 1u, pred, cs, [&](uint32_t j) {
-      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
-      const float r2 = dot3(rij, rij);
-      if (r2 < 1.0e-12f || j == i) return;
-      const float rr = sqrtf(r2);
-      const float hr = P.h - rr;
-      const float s = P.spikyGrad * hr * hr / rr;
-      const float t = P.h2 - r2;
-      const float ratio = P.poly6 * t * t * t * P.sCorrWq;
-      const float r2r = ratio * ratio;
-      const float sc = -P.sCorrK * r2r * r2r;
-      const float coef = (li_ + __ldg(&lambda[j]) + sc) * s;
-      dsum = fma3(coef, rij, dsum);
-      nc += 1.0f;
-    });
-    if (P.nBoundary > 0u) {
-      const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-      for (uint32_t k = bb; k < be; k++) {
-        const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
-        const float r2 = dot3(rij, rij);
-        if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-        const float rr = sqrtf(r2);
-        const float hr = P.h - rr;
-        const float coef = (li_ * __ldg(&d.bpsi[k])) * (P.spikyGrad * hr * hr / rr);
-        dB = fma3(coef, rij, dB);
-      }
-    }
+    const uint32_t bm = __ldg(&d.nbBMask[(size_t)r * cap + i]);
+    const bool lg = (longRows >> r) & 1u, lgb = (longRows >> (16 + r)) & 1u;
+    st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]), lgb ? 0u : bm);
+    todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
   }
+  F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
+  float nc = 1.0f;
+  auto fluid = [&](uint32_t j) {
+    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    const float r2 = dot3(rij, rij);
+    if (r2 < 1.0e-12f || j == i) return;
+    const float rr = sqrtf(r2);
+    const float hr = P.h - rr;
+    const float s = P.spikyGrad * hr * hr / rr;
+    const float t = P.h2 - r2;
+    const float ratio = P.poly6 * t * t * t * P.sCorrWq;
+    const float r2r = ratio * ratio;
+    const float sc = -P.sCorrK * r2r * r2r;
+    const float coef = (li_ + __ldg(&lambda[j]) + sc) * s;
+    dsum = fma3(coef, rij, dsum);
+    nc += 1.0f;
+  };
+  auto sample = [&](uint32_t k) {
+    const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+    const float r2 = dot3(rij, rij);
+    const float rr = sqrtf(r2);
+    const float hr = P.h - rr;
+    const float coef = (li_ * __ldg(&d.bpsi[k])) * (P.spikyGrad * hr * hr / rr);
+    dB = fma3(coef, rij, dB);
+  };
+  walk_rows(
+      st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
+      [&](int r, uint32_t k) { sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
+      [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
+      [&](int r) {
+        const int rb = w.row_base(P, r);
+        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+        for (uint32_t k = bb; k < be; k++) {
+          const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+          const float r2 = dot3(rij, rij);
+          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
+          sample(k);
+        }
+      });
   const F3 dd = {fmaf(dB.x, P.invRho0, dsum.x * P.volume), fmaf(dB.y, P.invRho0, dsum.y * P.volume),
                  fmaf(dB.z, P.invRho0, dsum.z * P.volume)};
   float scale = P.omega;
@@ -148,33 +190,27 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   }
 }
 
-// Plain: block b handles particles [b * TB, (b + 1) * TB). Batched: an item is a
-// tile of kBlock particles, walked TB at a time.
+// Plain: block b handles particles [b * TB, (b + 1) * TB). Batched: warps pull
+// 32-particle slices of the segment's tiles.
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda(const __grid_constant__ SimParams P,
                                                    const __grid_constant__ DevScene d, int it) {
-  lambda_body(P, d, blockIdx.x * TB + threadIdx.x, it);
+  lambda_body<TB>(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda_b(const __grid_constant__ BatchWork w,
                                                      const __grid_constant__ DevScene d, int it) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
-#pragma unroll 1
-    for (int s = 0; s < kBlock; s += TB) lambda_body(P, d, t * kBlock + s + threadIdx.x, it);
-  });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { lambda_body<TB>(P, d, li, it); });
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_delta(const __grid_constant__ SimParams P,
                                                   const __grid_constant__ DevScene d, int it) {
-  delta_body(P, d, blockIdx.x * TB + threadIdx.x, it);
+  delta_body<TB>(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_delta_b(const __grid_constant__ BatchWork w,
                                                     const __grid_constant__ DevScene d, int it) {
-  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) {
-#pragma unroll 1
-    for (int s = 0; s < kBlock; s += TB) delta_body(P, d, t * kBlock + s + threadIdx.x, it);
-  });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { delta_body<TB>(P, d, li, it); });
 }
 
 using PlainFn = void (*)(SimParams, DevScene, int);

@@ -15,6 +15,13 @@
 // the first stores them, the second skips phase 1. Rows with more than 64
 // candidates (never seen at rest density, where a row holds ~24) fall back to
 // the reference's direct loop.
+//
+// Phase 2 is one loop over all nine rows (walk_rows), not a loop per row: each
+// thread's row masks and row starts are staged in shared memory and every
+// iteration handles exactly one neighbour of every lane that has one left. Lanes
+// of a warp hold different numbers of neighbours per row, so a loop per row runs
+// each row to its warp maximum (about half the lanes idle in the expensive body);
+// the single loop runs to the warp maximum of the totals instead.
 #pragma once
 #include "p4a_math.cuh"
 
@@ -41,12 +48,13 @@ struct RowWalk {
 };
 
 // Phase 1 for one row (row base rb >= 0): the mask of candidates with r^2 < h^2;
-// sets *isLong when the row has more than 64 candidates.
+// sets *isLong when the row has more than 64 candidates and *b to the row's start.
 __device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& w, int rb, F3 pi,
                                              const float4* __restrict__ pred,
-                                             const uint32_t* __restrict__ cs, bool& isLong) {
+                                             const uint32_t* __restrict__ cs, bool& isLong,
+                                             uint32_t& b) {
   uint64_t m = 0ull;
-  const uint32_t b = __ldg(&cs[rb + w.x0]);
+  b = __ldg(&cs[rb + w.x0]);
   const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
   const uint32_t len = e > b ? e - b : 0u;
   isLong = len > kMaskBits;
@@ -68,28 +76,108 @@ __device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& 
   return m;
 }
 
-// Phase 2 over one row: calls f(j) for the row's fluid neighbours in ascending j
-// (from the mask, or by the direct loop for a long row). The caller handles the
-// row's boundary samples after it.
+// The reference's direct loop over one row's fluid candidates (rows longer than 64).
 template <class F>
-__device__ __forceinline__ void visit_row(const SimParams& P, const RowWalk& w, int rb, F3 pi,
-                                          uint64_t m, bool longRow,
-                                          const float4* __restrict__ pred,
-                                          const uint32_t* __restrict__ cs, F&& f) {
+__device__ __forceinline__ void long_row(const SimParams& P, const RowWalk& w, int rb, F3 pi,
+                                         const float4* __restrict__ pred,
+                                         const uint32_t* __restrict__ cs, F&& f) {
   const uint32_t b = __ldg(&cs[rb + w.x0]);
-  if (!longRow) {
-    while (m) {
-      const int k = __ffsll((long long)m) - 1;
-      m &= m - 1ull;
-      f(b + (uint32_t)k);
-    }
-  } else {
-    const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
-    for (uint32_t j = b; j < e; j++) {
-      const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
-      if (dot3(d, d) < P.h2) f(j);
+  const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
+  for (uint32_t j = b; j < e; j++) {
+    const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
+    if (dot3(d, d) < P.h2) f(j);
+  }
+}
+
+// Phase 1 for one row's boundary samples [bb, be): the mask of samples with
+// 1e-12 <= r^2 < h^2 (the ones the reference's boundary terms use); sets *isLong
+// when the row has more than 32 samples.
+constexpr uint32_t kBMaskBits = 32;
+__device__ __forceinline__ uint32_t boundary_mask(const SimParams& P, uint32_t bb, uint32_t be, F3 pi,
+                                                  const float4* __restrict__ bpos, bool& isLong) {
+  const uint32_t len = be > bb ? be - bb : 0u;
+  isLong = len > kBMaskBits;
+  const uint32_t lim = min(len, kBMaskBits);
+  uint32_t m = 0u;
+  for (uint32_t k = 0; k < lim; k++) {
+    const F3 d = sub3(pi, xyz(__ldg(&bpos[bb + k])));
+    const float r2 = dot3(d, d);
+    if (r2 < P.h2 && r2 >= 1.0e-12f) m |= 1u << k;
+  }
+  return m;
+}
+
+// Per-thread row staging in shared memory for a block of TB threads: fluid mask,
+// row start and (when the pass has boundary terms, B) boundary mask of each of the
+// nine rows, in columns [r * TB + threadIdx.x].
+template <int TB, bool B>
+struct RowStage {
+  uint64_t* mask;
+  uint32_t* base;
+  uint32_t* bmask;
+  __device__ __forceinline__ RowStage() {
+    __shared__ uint64_t sMask[kRows * TB];
+    __shared__ uint32_t sBase[kRows * TB];
+    mask = sMask + threadIdx.x;
+    base = sBase + threadIdx.x;
+    if constexpr (B) {
+      __shared__ uint32_t sBMask[kRows * TB];
+      bmask = sBMask + threadIdx.x;
+    } else {
+      bmask = nullptr;
     }
   }
+  __device__ __forceinline__ void set(int r, uint64_t m, uint32_t b, uint32_t bm = 0u) const {
+    mask[r * TB] = m;
+    base[r * TB] = b;
+    if constexpr (B) bmask[r * TB] = bm;
+  }
+};
+
+// Phase 2 over all rows in order. Each row's events are its fluid neighbours (set
+// bits, j ascending), then its boundary samples (set bits, k ascending): every loop
+// iteration handles one event of every lane that has one left, with fluid(j) or
+// bound(r, k) (k the sample's offset in the row's boundary range). A row longer
+// than its mask runs longFluid(r) in place of its fluid bits, or longBound(r) in
+// place of its boundary bits. `todo` has bit r set for every row with anything to
+// visit; lr / lb are the long-row bits.
+template <int TB, bool B, class FFluid, class FBound, class FLongF, class FLongB>
+__device__ __forceinline__ void walk_rows(const RowStage<TB, B>& st, uint32_t todo, uint32_t lr, uint32_t lb,
+                                          FFluid&& fluid, FBound&& bound, FLongF&& longFluid,
+                                          FLongB&& longBound) {
+  int r = -1;
+  uint64_t m = 0ull;
+  uint32_t mb = 0u, base = 0u;
+  for (;;) {
+    while ((m | (uint64_t)mb) == 0ull) {
+      if (r >= 0) {
+        if ((lb >> r) & 1u) longBound(r);
+        todo &= todo - 1u;  // r is the lowest pending row
+      }
+      if (todo == 0u) return;
+      r = __ffs(todo) - 1;
+      m = st.mask[r * TB];
+      base = st.base[r * TB];
+      if constexpr (B) mb = st.bmask[r * TB];
+      if ((lr >> r) & 1u) longFluid(r);  // a long row's fluid comes before its boundary samples
+    }
+    if (m != 0ull) {
+      const int k = __ffsll((long long)m) - 1;
+      m &= m - 1ull;
+      fluid(base + (uint32_t)k);
+    } else {
+      const int k = __ffs(mb) - 1;
+      mb &= mb - 1u;
+      bound(r, (uint32_t)k);
+    }
+  }
+}
+
+// Fluid-only form (passes without boundary terms).
+template <int TB, class FFluid, class FLongF>
+__device__ __forceinline__ void walk_fluid_rows(const RowStage<TB, false>& st, uint32_t todo, uint32_t lr,
+                                                FFluid&& fluid, FLongF&& longFluid) {
+  walk_rows(st, todo, lr, 0u, fluid, [](int, uint32_t) {}, longFluid, [](int) {});
 }
 
 // The masks shared by a pair of passes are stored [row][particle] (row-major over

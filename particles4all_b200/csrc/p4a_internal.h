@@ -107,7 +107,9 @@ struct DevScene {
   float4* smoothPos;
   float4* anisoG;
   uint64_t* nbMask;     // [9][cap] per-row neighbour masks shared by a pair of passes
-  uint32_t* nbLong;     // [cap] rows with more than 64 candidates
+  uint32_t* nbBMask;    // [9][cap] per-row boundary-sample masks (lambda -> delta)
+  uint32_t* nbLong;     // [cap] bit r: row r has more than 64 fluid candidates;
+                        // bit 16 + r: more than 32 boundary candidates
   uint32_t cap;         // particle capacity (stride of nbMask)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };

@@ -41,4 +41,38 @@ __device__ __forceinline__ void for_each_item(const BatchWork& w, F&& f) {
   }
 }
 
+// Warp-granular form for passes whose particles are independent: each warp pulls
+// slices of 32 particles (item k = slice k % 8 of tile k / 8 of the segment) and
+// calls f(P, li) with li the scene-local particle index of its lane. Warps never
+// wait on one another, so a warp that finishes a slice early starts the next one
+// instead of idling at a block barrier. Each warp keeps its own copy of the
+// current scene's SimParams. f is called by all 32 lanes together.
+constexpr int kSlices = kBlock / 32;
+template <class F>
+__device__ __forceinline__ void for_each_slice(const BatchWork& w, F&& f) {
+  __shared__ __align__(16) SimParams sP[kSlices];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  SimParams& P = sP[warp];
+  const WorkSeg seg = *w.seg;
+  const uint32_t total = seg.count * (uint32_t)kSlices;
+  uint32_t slot = 0xffffffffu, next = 0u;
+  if (lane == 0) next = atomicAdd(w.cursor, 1u);
+  next = __shfl_sync(0xffffffffu, next, 0);
+  while (next < total) {
+    const uint32_t k = next;
+    if (lane == 0) next = atomicAdd(w.cursor, 1u);  // claim the next slice now
+    const uint2 it = w.items[seg.off + k / kSlices];
+    if (it.x != slot) {
+      __syncwarp();
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(w.params + it.x);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&P);
+      for (int q = lane; q < (int)(sizeof(SimParams) / 4); q += 32) dst[q] = src[q];
+      __syncwarp();
+      slot = it.x;
+    }
+    f(static_cast<const SimParams&>(P), it.y * (uint32_t)kBlock + (k % kSlices) * 32u + (uint32_t)lane);
+    next = __shfl_sync(0xffffffffu, next, 0);
+  }
+}
+
 }  // namespace p4a

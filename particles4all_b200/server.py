@@ -27,7 +27,7 @@ from .params import CParams
 # p4a_batch_create): per particle slot the ping-pong particle arrays, solver
 # scratch, sort keys and neighbour masks; per cell the histogram, cellStart and
 # boundary cellStart; per boundary sample its position and psi.
-BYTES_PER_PARTICLE = 288
+BYTES_PER_PARTICLE = 324
 BYTES_PER_CELL = 12
 BYTES_PER_BOUNDARY = 20
 

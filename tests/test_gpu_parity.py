@@ -249,3 +249,50 @@ def test_verify_harness_checks():
     assert np.isfinite(pred).all() and np.isfinite(dens).all() and np.isfinite(lam).all()
     half = 0.5 * p["spacing"]
     assert (pred[:, :3] >= half - 1e-6).all() and (pred[:, :3] <= np.array(p["box"]) - half + 1e-6).all()
+
+
+def _long_run_stats(sim, n_bodies, rest, body, mass, rho0, body_density):
+    """Mean / max density constraint error (rho/rho0 - 1)^+, particle count and the
+    rigid-body volumes (N_b m / rho_body plus the extent of the oriented bounding box
+    of the body's rest offsets under its pose)."""
+    n = sim.info()["n"]
+    rho = (sim.read("density") if hasattr(sim, "read") else sim.buffer("density"))[:n].astype(np.float64)
+    err = np.maximum(rho / rho0 - 1.0, 0.0)
+    out = {"n": n, "mean_err": float(err.mean()), "max_err": float(err.max()), "volumes": []}
+    rot = (sim.read("bodyRot") if hasattr(sim, "read") else sim.buffer("bodyRot"))[: 3 * n_bodies, :3]
+    for b in range(n_bodies):
+        sel = body[:n, 0] == b + 1
+        R = rot[3 * b: 3 * b + 3].astype(np.float64)
+        q = rest[:n, :3][sel].astype(np.float64) @ R.T
+        ext = float(np.prod(q.max(0) - q.min(0)))
+        out["volumes"].append(sel.sum() * mass / (body_density[b] * rho0) + ext)
+    return out
+
+
+@pytest.mark.parametrize("workload", ["dam_break_32k", "bodies_small"])
+def test_thousand_steps_statistics(workload):
+    """1,000 steps on the GPU and in the oracle: mean and max density-constraint
+    error, particle count and rigid-body volumes agree within 2 % (they are in fact
+    bit-identical, since every step is)."""
+    if workload == "dam_break_32k":
+        p, sc = configs.dam_break_32k()
+    else:
+        p, sc = configs.medium_bodies_264k(side=12, n_cubes=2)
+    g, o = pair(p, sc)
+    for _ in range(1000):
+        g.step(1 / 60)
+        o.step(1 / 60)
+    gi = g.info()
+    nb = gi["n_bodies"]
+    dens = list(sc.get("body_density", [])) if nb else []
+    sg = _long_run_stats(g, nb, g.read("rest"), g.read("body"), gi["mass"], p["restDensity"], dens)
+    so = _long_run_stats(o, nb, o.buffer("rest"), o.buffer("body"), gi["mass"], p["restDensity"], dens)
+    assert sg["n"] == so["n"]
+    for k in ("mean_err", "max_err"):
+        assert abs(sg[k] - so[k]) <= 0.02 * max(abs(so[k]), 1e-6), (k, sg[k], so[k])
+    for vg, vo in zip(sg["volumes"], so["volumes"]):
+        assert abs(vg - vo) <= 0.02 * abs(vo)
+    assert sg == so  # bit-identical state gives identical statistics
+    assert g.get_stats()["raw"] == o.stats()["raw"]
+    compare(g, o)
+    g.close()
