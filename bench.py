@@ -33,6 +33,7 @@ L2_FLUSH_BYTES = 256 << 20
 # definition: neighbour re-reads are not counted).
 ALGO_BYTES = {
     "key_count": 36,        # R pos, vel; W key
+    "fill": 12,             # R key, rank; W unordered
     "reorder": 84,          # R key, pos, vel; W pos, vel, pred   (+64 with bodies)
     "lambda": 24,           # R pred; W density, lambda
     "delta": 36,            # R pred, lambda; W pred
@@ -382,8 +383,21 @@ def run_ours(args):
     for _ in range(max(3, args.warmup)):
         frame()
     sim.synchronize()
+    # per-kernel breakdown: a pass with a CUDA event around every launch, before the
+    # timed pass (whose steps run without the extra event records)
+    prof_steps = max(3, min(args.steps, 30))
     sim.profile(True)
     sim.profile_reset()
+    done[0] = 0.0
+    prof_subs = 0
+    with torch.cuda.stream(stream):
+        for _ in range(prof_steps):
+            flush.zero_()
+            prof_subs += frame()
+    sim.synchronize()
+    kern = sim.profile_read()
+    sim.profile(False)
+    prof_n_avg = done[0] / max(1, prof_subs)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     clocks = ClockSampler(local)
@@ -406,28 +420,56 @@ def run_ours(args):
     launches = _lib.lib().p4a_kernel_launches() - launches0
     clocks.stop()
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    kern = sim.profile_read()
-    sim.profile(False)
-    dev_ms_max = allmax(dev_ms)
     done_timed = done[0]
+    dev_ms_max = allmax(dev_ms)
     value = world * done_timed / (dev_ms_max / 1000.0)
 
     # roofline of the dominant kernel (live per-kernel events of the timed region)
     top = max(kern.items(), key=lambda kv: kv[1][0])
     name, (kms, kl) = top
-    per_p = ALGO_BYTES.get(name, 0) + (64 if name == "reorder" and sim.info()["n_bodies"] else 0)
+    total_ms = sum(x[0] for x in kern.values())
+
+    def kernel_bytes(k):
+        return ALGO_BYTES.get(k, 0) + (64 if k == "reorder" and sim.info()["n_bodies"] else 0)
+
+    def kernel_line(k, v):
+        """Per-kernel share and HBM fraction (algorithmic bytes / average launch time)."""
+        out = {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / total_ms, 4),
+               "us_per_launch": round(v[0] / max(1, v[1]) * 1000, 2)}
+        if kernel_bytes(k):
+            gbs = kernel_bytes(k) * prof_n_avg / (v[0] / max(1, v[1]) / 1000.0) / 1e9
+            out.update({"algorithmic_gbs": round(gbs, 1), "hbm_frac": round(gbs / peaks()[0], 4)})
+        return out
+
+    per_p = kernel_bytes(name)
     avg_s = kms / kl / 1000.0
     n_avg = done_timed / max(1, subs)  # mean particles per substep (grows with a hose)
-    algo = per_p * n_avg
+    algo = per_p * prof_n_avg
     peak, peak_kind = peaks()
     achieved = algo / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": committed_traffic(name, args.workload),
                 "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
                 "avg_launch_us": avg_s * 1e6,
-                "kernels": {k: {"ms_total": round(v[0], 4), "launches": v[1],
-                                "share": round(v[0] / sum(x[0] for x in kern.values()), 4)}
-                            for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
+                "kernels": {k: kernel_line(k, v) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
+
+    # whole-step HBM roofline with the fixed per-particle-substep formula of the
+    # workload definition: sort (36 + 4 + 84), k x (lambda 24 + delta 36), finish 68,
+    # bodies +64 per particle and 88 x k per body particle, tension +56, scan 8 per
+    # cell, and 64 per particle per frame for the anisotropic pass
+    k_it = max(1, int(params["iterations"]))
+    info_now = sim.info()
+    bpp = 36 + 4 + 84 + k_it * (24 + 36) + 68 + (64 if info_now["n_bodies"] else 0) + \
+        (56 if params.get("surfaceTensionK", 0) > 0 else 0)
+    step_bytes = done_timed * bpp + subs * (info_now["n_body_parts"] * 88 * k_it + 8 * info_now["n_cells"])
+    if aniso:
+        step_bytes += args.steps * n_avg * 64
+    step_achieved = step_bytes / (dev_ms / 1000.0) / 1e9
+    step_roofline = {"bound": "hbm", "achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                     "frac": step_achieved / peak, "peak_source": peak_kind,
+                     "bytes_per_particle_substep": bpp,
+                     "what": "whole step: fixed algorithmic bytes of the workload definition over the "
+                             "device time of the timed steps"}
 
     # end to end through the public API: host state in, step, host state out
     e2e = None
@@ -495,7 +537,8 @@ def run_ours(args):
                        "surface_tension": params["surfaceTensionK"], "aniso_pass": bool(aniso),
                        "l2": "flushed between timed steps (256 MiB write outside the timed events)",
                        "parallelism": f"replicas x{world}"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches,
             "batched_mix": mix,
             "served": served,
             "clocks": clocks.summary(w0, w1),

@@ -239,6 +239,8 @@ void pack_params(p4a_sim* s, double dt) {
   F.iters = (uint32_t)std::max(1, p.iterations);
   F.subs = 1;
   F.slot = 0;
+  F.skinH2 = (float)((h + kSkin * h) * (h + kSkin * h));
+  F.skinHalf = (float)((kSkin * h - 1e-4 * h) * 0.5);
 }
 
 uint32_t next_epoch(p4a_sim* s) {
@@ -321,7 +323,8 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.key, cap)) || (rc = dalloc(s, L, &s->d.rank, cap)) ||
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbMask, cap * 9)) ||
-      (rc = dalloc(s, L, &s->d.nbBMask, cap * 9)) ||
+      (rc = dalloc(s, L, &s->d.nbBMask, cap * 9)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
+      (rc = dalloc(s, L, &s->d.disp, kDispSlots)) ||
       (rc = dalloc(s, L, &s->d.nbLong, cap)))
     return rc;
   s->d.cap = (uint32_t)cap;

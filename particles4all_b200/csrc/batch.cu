@@ -114,6 +114,8 @@ void pack(BScene& s, double dt, int slot) {
   F.iters = (uint32_t)std::max(1, p.iterations);
   F.subs = 1;
   F.slot = (uint32_t)slot;
+  F.skinH2 = (float)((h + kSkin * h) * (h + kSkin * h));
+  F.skinHalf = (float)((kSkin * h - 1e-4 * h) * 0.5);
 }
 
 // Kinds of the launches of a frame, in the order a substep issues them.
@@ -679,6 +681,7 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
       ((rc = balloc(b, &d.lambda, P)) || (rc = balloc(b, &d.density, P)) || (rc = balloc(b, &d.corr, P)) ||
        (rc = balloc(b, &d.normal, P)) || (rc = balloc(b, &d.key, P)) || (rc = balloc(b, &d.rank, P)) ||
        (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbMask, P * 9)) || (rc = balloc(b, &d.nbBMask, P * 9)) ||
+       (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
        (rc = balloc(b, &d.nbLong, P)) || (rc = balloc(b, &d.cellCount, Cc)) ||
        (rc = balloc(b, &d.cellStart, Cc)) || (rc = balloc(b, &d.bcellStart, Cc)) ||
        (rc = balloc(b, &d.scanState, b->scanTilesCap)) || (rc = balloc(b, &d.scanTicket, 4)) ||

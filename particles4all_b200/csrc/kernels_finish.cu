@@ -91,7 +91,7 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
       if (rb < 0) continue;
       bool lg;
       uint32_t b;
-      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
+      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.h2);
       st.set(r, lg ? 0ull : mr, b);
       longRows |= (uint32_t)lg << r;
       todo |= (uint32_t)(mr != 0ull || lg) << r;
@@ -135,7 +135,7 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
     if (rb < 0) continue;
     bool lg;
     uint32_t b;
-    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
+    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.h2);
     d.nbMask[(size_t)r * cap + i] = mr;
     st.set(r, lg ? 0ull : mr, b);
     longRows |= (uint32_t)lg << r;

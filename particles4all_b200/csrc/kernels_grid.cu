@@ -25,6 +25,7 @@ namespace p4a {
 
 __device__ __forceinline__ void key_count_body(const SimParams& P, const DevScene& d, uint32_t li) {
   if (d.bodyFill && li < P.nBodies) d.bodyFill[P.bOff + li] = 0u;
+  if (d.disp && li < (uint32_t)kDispSlots) d.disp[P.slot * kDispSlots + li] = 0.0f;
   const bool act = li < P.n;
   const uint32_t i = P.pOff + li;
   uint32_t k = 0xffffffffu;

@@ -9,6 +9,14 @@
 // sort): iteration `it` reads pred[L ^ (it & 1)] and delta writes the other copy.
 // lambda builds the per-row neighbour masks (neighbours.cuh) and stores them; delta
 // runs on the same positions, so it reuses them and skips the candidate tests.
+// The masks are built with the radius h + skin and also serve later iterations of
+// the substep: every delta (and the rigid projection) records the largest
+// displacement of its iteration, and an iteration reuses the masks of the last
+// rebuild while the summed displacements since then stay within skin / 2 (so every
+// pair now within h was within h + skin then) and the particle is still in the cell
+// it was in then (so its candidate rows are the same). Phase 2 tests r^2 < h^2 on
+// every masked candidate, so the visited neighbours and their order are exactly the
+// reference's either way.
 // The last delta of a substep also writes velFromPos (src/wgsl.js:72-83) for every
 // particle into the non-live velocity copy; body particles are overwritten by the
 // rigid projection that follows.
@@ -33,28 +41,59 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   const F3 pi = xyz(__ldg(&pred[i]));
   const RowWalk w(P, pi);
   const RowStage<TB, true> st;
-  // phase 1: fluid and boundary masks of every row (stored for delta)
-  uint32_t todo = 0u, longRows = 0u;
-#pragma unroll
-  for (int r = 0; r < kRows; r++) {
-    const int rb = w.row_base(P, r);
-    if (rb < 0) continue;
-    bool lg;
-    uint32_t b;
-    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b);
-    uint32_t bm = 0u;
-    bool lgb = false;
-    if (P.nBoundary > 0u) {
-      const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-      if (be > bb) bm = boundary_mask(P, bb, be, pi, d.bpos, lgb);
+  // reuse the masks of the last rebuild while the displacement bound allows
+  const uint32_t cell = cell_index(P, w.c);
+  bool reuse = false;
+  if (it > 0 && it < kDispSlots) {
+    const float* disp = d.disp + (size_t)P.slot * kDispSlots;
+    int ref = 0;
+    float D = 0.0f;
+    for (int t = 0; t < it; t++) {
+      D += __ldg(&disp[t]);
+      if (D * 1.00001f > P.skinHalf) {  // iteration t + 1 rebuilt
+        ref = t + 1;
+        D = 0.0f;
+      }
     }
-    d.nbMask[(size_t)r * cap + i] = mr;
-    d.nbBMask[(size_t)r * cap + i] = bm;
-    st.set(r, lg ? 0ull : mr, b, lgb ? 0u : bm);
-    longRows |= ((uint32_t)lg << r) | ((uint32_t)lgb << (16 + r));
-    todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
+    reuse = ref < it && __ldg(&d.nbCell[i]) == cell;
   }
-  d.nbLong[i] = longRows;
+  uint32_t todo = 0u, longRows = 0u;
+  if (reuse) {
+    longRows = __ldg(&d.nbLong[i]);
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      const int rb = w.row_base(P, r);
+      if (rb < 0) continue;
+      const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
+      const uint32_t bm = __ldg(&d.nbBMask[(size_t)r * cap + i]);
+      const bool lg = (longRows >> r) & 1u, lgb = (longRows >> (16 + r)) & 1u;
+      st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]), lgb ? 0u : bm);
+      todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
+    }
+  } else {
+    // phase 1: fluid and boundary masks of every row, radius h + skin (stored)
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      const int rb = w.row_base(P, r);
+      if (rb < 0) continue;
+      bool lg;
+      uint32_t b;
+      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.skinH2);
+      uint32_t bm = 0u;
+      bool lgb = false;
+      if (P.nBoundary > 0u) {
+        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+        if (be > bb) bm = boundary_mask(P, bb, be, pi, d.bpos, lgb, P.skinH2);
+      }
+      d.nbMask[(size_t)r * cap + i] = mr;
+      d.nbBMask[(size_t)r * cap + i] = bm;
+      st.set(r, lg ? 0ull : mr, b, lgb ? 0u : bm);
+      longRows |= ((uint32_t)lg << r) | ((uint32_t)lgb << (16 + r));
+      todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
+    }
+    d.nbLong[i] = longRows;
+    d.nbCell[i] = cell;
+  }
   // phase 2
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
@@ -63,6 +102,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     if (j == i) return;
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2) return;  // in the skin of the mask only
     rho = fmaf(P.mass, poly6(P, r2), rho);
     if (r2 > 1.0e-12f) {
       const float rr = sqrtf(r2);
@@ -73,10 +113,11 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
       sumGrad2 = sumGrad2 + dot3(g, g);
     }
   };
-  // one boundary sample k (1e-12 <= r^2 < h^2)
+  // one boundary sample k (1e-12 <= r^2 < h^2 is tested here or by the caller)
   auto sample = [&](uint32_t k) {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2) return;
     const float psi = __ldg(&d.bpsi[k]);
     rho = fmaf(psi, poly6(P, r2), rho);
     const float rr = sqrtf(r2);
@@ -140,7 +181,7 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   auto fluid = [&](uint32_t j) {
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
-    if (r2 < 1.0e-12f || j == i) return;
+    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;  // r^2 >= h^2: in the mask's skin only
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = P.spikyGrad * hr * hr / rr;
@@ -155,6 +196,7 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   auto sample = [&](uint32_t k) {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2) return;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float coef = (li_ * __ldg(&d.bpsi[k])) * (P.spikyGrad * hr * hr / rr);
@@ -183,6 +225,7 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   o.y = fminf(fmaxf(o.y, P.clampMin[1]), P.clampMax[1]);
   o.z = fminf(fmaxf(o.z, P.clampMin[2]), P.clampMax[2]);
   predOut[i] = make_float4(o.x, o.y, o.z, 1.0f);
+  if (it < kDispSlots) record_displacement(d, P, it, sub3(o, pi));
   if (it == (int)P.iters - 1) {  // velFromPos into the non-live velocity copy
     const float4 p0 = __ldg(&d.pos[L][i]);
     d.vel[L ^ 1][i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,

@@ -47,12 +47,13 @@ struct RowWalk {
   }
 };
 
-// Phase 1 for one row (row base rb >= 0): the mask of candidates with r^2 < h^2;
-// sets *isLong when the row has more than 64 candidates and *b to the row's start.
+// Phase 1 for one row (row base rb >= 0): the mask of candidates with r^2 < r2lim
+// (h^2, or (h + skin)^2 for masks that later iterations reuse); sets *isLong when the
+// row has more than 64 candidates and *b to the row's start.
 __device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& w, int rb, F3 pi,
                                              const float4* __restrict__ pred,
                                              const uint32_t* __restrict__ cs, bool& isLong,
-                                             uint32_t& b) {
+                                             uint32_t& b, float r2lim) {
   uint64_t m = 0ull;
   b = __ldg(&cs[rb + w.x0]);
   const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
@@ -65,13 +66,13 @@ __device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& 
     const float4 q2 = __ldg(&pred[b + k + 2]), q3 = __ldg(&pred[b + k + 3]);
     const F3 d0 = sub3(pi, xyz(q0)), d1 = sub3(pi, xyz(q1));
     const F3 d2 = sub3(pi, xyz(q2)), d3 = sub3(pi, xyz(q3));
-    const uint32_t bits = (dot3(d0, d0) < P.h2 ? 1u : 0u) | (dot3(d1, d1) < P.h2 ? 2u : 0u) |
-                          (dot3(d2, d2) < P.h2 ? 4u : 0u) | (dot3(d3, d3) < P.h2 ? 8u : 0u);
+    const uint32_t bits = (dot3(d0, d0) < r2lim ? 1u : 0u) | (dot3(d1, d1) < r2lim ? 2u : 0u) |
+                          (dot3(d2, d2) < r2lim ? 4u : 0u) | (dot3(d3, d3) < r2lim ? 8u : 0u);
     m |= (uint64_t)bits << k;
   }
   for (; k < lim; k++) {
     const F3 d0 = sub3(pi, xyz(__ldg(&pred[b + k])));
-    if (dot3(d0, d0) < P.h2) m |= 1ull << k;
+    if (dot3(d0, d0) < r2lim) m |= 1ull << k;
   }
   return m;
 }
@@ -90,11 +91,12 @@ __device__ __forceinline__ void long_row(const SimParams& P, const RowWalk& w, i
 }
 
 // Phase 1 for one row's boundary samples [bb, be): the mask of samples with
-// 1e-12 <= r^2 < h^2 (the ones the reference's boundary terms use); sets *isLong
-// when the row has more than 32 samples.
+// 1e-12 <= r^2 < r2lim (the ones the reference's boundary terms use, when r2lim is
+// h^2); sets *isLong when the row has more than 32 samples.
 constexpr uint32_t kBMaskBits = 32;
 __device__ __forceinline__ uint32_t boundary_mask(const SimParams& P, uint32_t bb, uint32_t be, F3 pi,
-                                                  const float4* __restrict__ bpos, bool& isLong) {
+                                                  const float4* __restrict__ bpos, bool& isLong,
+                                                  float r2lim) {
   const uint32_t len = be > bb ? be - bb : 0u;
   isLong = len > kBMaskBits;
   const uint32_t lim = min(len, kBMaskBits);
@@ -102,7 +104,7 @@ __device__ __forceinline__ uint32_t boundary_mask(const SimParams& P, uint32_t b
   for (uint32_t k = 0; k < lim; k++) {
     const F3 d = sub3(pi, xyz(__ldg(&bpos[bb + k])));
     const float r2 = dot3(d, d);
-    if (r2 < P.h2 && r2 >= 1.0e-12f) m |= 1u << k;
+    if (r2 < r2lim && r2 >= 1.0e-12f) m |= 1u << k;
   }
   return m;
 }

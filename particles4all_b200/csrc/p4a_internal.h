@@ -47,8 +47,17 @@ struct SimParams {
   uint32_t parity;  // live parity before this substep's sort
   uint32_t iters;   // Jacobi iterations (>= 1)
   uint32_t subs;    // substeps of the current frame (stats after the last)
-  uint32_t slot;    // stats slot (statsOut + 8 * slot)
+  uint32_t slot;    // stats slot (statsOut + 8 * slot) and displacement slot
+  // neighbour masks reused across Jacobi iterations (kernels_solve.cu)
+  float skinH2;     // (h + skin)^2: radius of the reused candidate masks
+  float skinHalf;   // reuse while the displacement bound stays <= this
 };
+
+// Jacobi iterations whose displacement bounds are tracked per substep; later
+// iterations rebuild their masks.
+constexpr int kDispSlots = 16;
+// Skin of the reused masks, in units of h.
+constexpr double kSkin = 0.1;
 
 // Anisotropic-kernel uniform (src/aniso_wgsl.js:4-21, packed by src/mesh.js:227-241).
 struct AnisoParams {
@@ -110,6 +119,8 @@ struct DevScene {
   uint32_t* nbBMask;    // [9][cap] per-row boundary-sample masks (lambda -> delta)
   uint32_t* nbLong;     // [cap] bit r: row r has more than 64 fluid candidates;
                         // bit 16 + r: more than 32 boundary candidates
+  uint32_t* nbCell;     // [cap] cell index the lambda masks were built in
+  float* disp;          // [slots][kDispSlots] max |dp| of each iteration of the substep
   uint32_t cap;         // particle capacity (stride of nbMask)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };

@@ -108,4 +108,15 @@ __device__ __forceinline__ M3 scale3(const M3& a, float s) {
   return {{mul3(a.c[0], s), mul3(a.c[1], s), mul3(a.c[2], s)}};
 }
 
+// The largest |dp| of iteration `it` of the scene (max over the lanes that call
+// together, one atomic per group): the bound that decides whether the next
+// iteration may reuse the neighbour masks.
+__device__ __forceinline__ void record_displacement(const DevScene& d, const SimParams& P, int it, F3 dp) {
+  const float len = sqrtf(dot3(dp, dp));
+  const unsigned am = __activemask();
+  const uint32_t m = __reduce_max_sync(am, __float_as_uint(len));  // non-negative floats order as ints
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1))
+    atomicMax(reinterpret_cast<unsigned int*>(d.disp + (size_t)P.slot * kDispSlots + it), m);
+}
+
 }  // namespace p4a
