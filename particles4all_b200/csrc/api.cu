@@ -324,6 +324,7 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbMask, cap * 9)) ||
       (rc = dalloc(s, L, &s->d.nbBMask, cap * 9)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
+      (rc = dalloc(s, L, &s->d.nbMaskX, cap * 9)) || (rc = dalloc(s, L, &s->d.nbBMaskX, cap * 9)) ||
       (rc = dalloc(s, L, &s->d.disp, kDispSlots)) ||
       (rc = dalloc(s, L, &s->d.nbLong, cap)))
     return rc;

@@ -681,7 +681,7 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
       ((rc = balloc(b, &d.lambda, P)) || (rc = balloc(b, &d.density, P)) || (rc = balloc(b, &d.corr, P)) ||
        (rc = balloc(b, &d.normal, P)) || (rc = balloc(b, &d.key, P)) || (rc = balloc(b, &d.rank, P)) ||
        (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbMask, P * 9)) || (rc = balloc(b, &d.nbBMask, P * 9)) ||
-       (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
+       (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.nbMaskX, P * 9)) || (rc = balloc(b, &d.nbBMaskX, P * 9)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
        (rc = balloc(b, &d.nbLong, P)) || (rc = balloc(b, &d.cellCount, Cc)) ||
        (rc = balloc(b, &d.cellStart, Cc)) || (rc = balloc(b, &d.bcellStart, Cc)) ||
        (rc = balloc(b, &d.scanState, b->scanTilesCap)) || (rc = balloc(b, &d.scanTicket, 4)) ||

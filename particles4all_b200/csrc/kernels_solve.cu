@@ -58,6 +58,8 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     reuse = ref < it && __ldg(&d.nbCell[i]) == cell;
   }
   uint32_t todo = 0u, longRows = 0u;
+#pragma unroll
+  for (int r = 0; r < kRows; r++) st.set(r, 0ull, 0u, 0u);
   if (reuse) {
     longRows = __ldg(&d.nbLong[i]);
 #pragma unroll
@@ -98,11 +100,11 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;
-  auto fluid = [&](uint32_t j) {
-    if (j == i) return;
+  auto fluid = [&](uint32_t j) -> bool {
+    if (j == i) return false;
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return;  // in the skin of the mask only
+    if (r2 >= P.h2) return false;  // in the skin of the mask only
     rho = fmaf(P.mass, poly6(P, r2), rho);
     if (r2 > 1.0e-12f) {
       const float rr = sqrtf(r2);
@@ -112,22 +114,24 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
       gradSum = add3(gradSum, g);
       sumGrad2 = sumGrad2 + dot3(g, g);
     }
+    return true;
   };
   // one boundary sample k (1e-12 <= r^2 < h^2 is tested here or by the caller)
-  auto sample = [&](uint32_t k) {
+  auto sample = [&](uint32_t k) -> bool {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return;
+    if (r2 >= P.h2) return false;
     const float psi = __ldg(&d.bpsi[k]);
     rho = fmaf(psi, poly6(P, r2), rho);
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
     gradSum = fma3(s, rij, gradSum);
+    return true;
   };
   walk_rows(
       st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
-      [&](int r, uint32_t k) { sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
+      [&](int r, uint32_t k) { return sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
       [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
       [&](int r) {
         const int rb = w.row_base(P, r);
@@ -138,7 +142,14 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
           if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
           sample(k);
         }
-      });
+      },
+      [&](int r, uint64_t em, uint32_t ebm) { st.set(r, em, 0u, ebm); });  // the row's stage is free now
+  // exact masks for delta, all rows at once (rows that were not walked hold zero)
+#pragma unroll
+  for (int r = 0; r < kRows; r++) {
+    d.nbMaskX[(size_t)r * cap + i] = st.mask[r * TB];
+    d.nbBMaskX[(size_t)r * cap + i] = st.bmask[r * TB];
+  }
   d.density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
   if (C > 0.0f) {
@@ -170,18 +181,18 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   for (int r = 0; r < kRows; r++) {
     const int rb = w.row_base(P, r);
     if (rb < 0) continue;
-    const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
-    const uint32_t bm = __ldg(&d.nbBMask[(size_t)r * cap + i]);
+    const uint64_t mr = __ldg(&d.nbMaskX[(size_t)r * cap + i]);  // lambda's exact masks
+    const uint32_t bm = __ldg(&d.nbBMaskX[(size_t)r * cap + i]);
     const bool lg = (longRows >> r) & 1u, lgb = (longRows >> (16 + r)) & 1u;
     st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]), lgb ? 0u : bm);
     todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
   }
   F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
   float nc = 1.0f;
-  auto fluid = [&](uint32_t j) {
+  auto fluid = [&](uint32_t j) -> bool {
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;  // r^2 >= h^2: in the mask's skin only
+    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return false;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = P.spikyGrad * hr * hr / rr;
@@ -192,19 +203,21 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     const float coef = (li_ + __ldg(&lambda[j]) + sc) * s;
     dsum = fma3(coef, rij, dsum);
     nc += 1.0f;
+    return true;
   };
-  auto sample = [&](uint32_t k) {
+  auto sample = [&](uint32_t k) -> bool {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return;
+    if (r2 >= P.h2) return false;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float coef = (li_ * __ldg(&d.bpsi[k])) * (P.spikyGrad * hr * hr / rr);
     dB = fma3(coef, rij, dB);
+    return true;
   };
   walk_rows(
       st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
-      [&](int r, uint32_t k) { sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
+      [&](int r, uint32_t k) { return sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
       [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
       [&](int r) {
         const int rb = w.row_base(P, r);
@@ -215,7 +228,8 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
           if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
           sample(k);
         }
-      });
+      },
+      [](int, uint64_t, uint32_t) {});
   const F3 dd = {fmaf(dB.x, P.invRho0, dsum.x * P.volume), fmaf(dB.y, P.invRho0, dsum.y * P.volume),
                  fmaf(dB.z, P.invRho0, dsum.z * P.volume)};
   float scale = P.omega;

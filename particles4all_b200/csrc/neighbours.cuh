@@ -139,21 +139,24 @@ struct RowStage {
 // Phase 2 over all rows in order. Each row's events are its fluid neighbours (set
 // bits, j ascending), then its boundary samples (set bits, k ascending): every loop
 // iteration handles one event of every lane that has one left, with fluid(j) or
-// bound(r, k) (k the sample's offset in the row's boundary range). A row longer
-// than its mask runs longFluid(r) in place of its fluid bits, or longBound(r) in
-// place of its boundary bits. `todo` has bit r set for every row with anything to
-// visit; lr / lb are the long-row bits.
-template <int TB, bool B, class FFluid, class FBound, class FLongF, class FLongB>
+// bound(r, k) (k the sample's offset in the row's boundary range), which return
+// whether the candidate was within h. A row longer than its mask runs longFluid(r)
+// in place of its fluid bits, or longBound(r) in place of its boundary bits. When a
+// row is done, rowDone(r, em, ebm) receives the masks of the candidates that were
+// within h. `todo` has bit r set for every row with anything to visit; lr / lb are
+// the long-row bits.
+template <int TB, bool B, class FFluid, class FBound, class FLongF, class FLongB, class FDone>
 __device__ __forceinline__ void walk_rows(const RowStage<TB, B>& st, uint32_t todo, uint32_t lr, uint32_t lb,
                                           FFluid&& fluid, FBound&& bound, FLongF&& longFluid,
-                                          FLongB&& longBound) {
+                                          FLongB&& longBound, FDone&& rowDone) {
   int r = -1;
-  uint64_t m = 0ull;
-  uint32_t mb = 0u, base = 0u;
+  uint64_t m = 0ull, em = 0ull;
+  uint32_t mb = 0u, ebm = 0u, base = 0u;
   for (;;) {
     while ((m | (uint64_t)mb) == 0ull) {
       if (r >= 0) {
         if ((lb >> r) & 1u) longBound(r);
+        rowDone(r, em, ebm);
         todo &= todo - 1u;  // r is the lowest pending row
       }
       if (todo == 0u) return;
@@ -161,25 +164,29 @@ __device__ __forceinline__ void walk_rows(const RowStage<TB, B>& st, uint32_t to
       m = st.mask[r * TB];
       base = st.base[r * TB];
       if constexpr (B) mb = st.bmask[r * TB];
+      em = 0ull;
+      ebm = 0u;
       if ((lr >> r) & 1u) longFluid(r);  // a long row's fluid comes before its boundary samples
     }
     if (m != 0ull) {
       const int k = __ffsll((long long)m) - 1;
       m &= m - 1ull;
-      fluid(base + (uint32_t)k);
+      if (fluid(base + (uint32_t)k)) em |= 1ull << k;
     } else {
       const int k = __ffs(mb) - 1;
       mb &= mb - 1u;
-      bound(r, (uint32_t)k);
+      if (bound(r, (uint32_t)k)) ebm |= 1u << k;
     }
   }
 }
 
-// Fluid-only form (passes without boundary terms).
+// Fluid-only form (passes without boundary terms); fluid(j) returns void.
 template <int TB, class FFluid, class FLongF>
 __device__ __forceinline__ void walk_fluid_rows(const RowStage<TB, false>& st, uint32_t todo, uint32_t lr,
                                                 FFluid&& fluid, FLongF&& longFluid) {
-  walk_rows(st, todo, lr, 0u, fluid, [](int, uint32_t) {}, longFluid, [](int) {});
+  walk_rows(
+      st, todo, lr, 0u, [&](uint32_t j) { fluid(j); return false; }, [](int, uint32_t) { return false; },
+      longFluid, [](int) {}, [](int, uint64_t, uint32_t) {});
 }
 
 // The masks shared by a pair of passes are stored [row][particle] (row-major over

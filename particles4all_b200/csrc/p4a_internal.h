@@ -57,7 +57,7 @@ struct SimParams {
 // iterations rebuild their masks.
 constexpr int kDispSlots = 16;
 // Skin of the reused masks, in units of h.
-constexpr double kSkin = 0.1;
+constexpr double kSkin = 0.05;
 
 // Anisotropic-kernel uniform (src/aniso_wgsl.js:4-21, packed by src/mesh.js:227-241).
 struct AnisoParams {
@@ -120,6 +120,8 @@ struct DevScene {
   uint32_t* nbLong;     // [cap] bit r: row r has more than 64 fluid candidates;
                         // bit 16 + r: more than 32 boundary candidates
   uint32_t* nbCell;     // [cap] cell index the lambda masks were built in
+  uint64_t* nbMaskX;    // [9][cap] the exact (radius h) masks of lambda's iteration, for delta
+  uint32_t* nbBMaskX;   // [9][cap]
   float* disp;          // [slots][kDispSlots] max |dp| of each iteration of the substep
   uint32_t cap;         // particle capacity (stride of nbMask)
   uint32_t* slotOut;    // optional: sorted position of each input particle
