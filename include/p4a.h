@@ -326,6 +326,9 @@ typedef struct p4a_batch_usage {
   int64_t device_bytes;    /* bytes the batch holds on the device            */
 } p4a_batch_usage;
 int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out);
+/* Device bytes p4a_batch_create would allocate for cfg (its arenas; the per-frame
+ * work lists, a few bytes per work item, come on top). Needs no device. */
+int p4a_batch_footprint(const p4a_batch_config* cfg, int64_t* bytes);
 int p4a_batch_destroy(p4a_batch* b);
 const char* p4a_batch_last_error(const p4a_batch* b);
 int p4a_batch_set_stream(p4a_batch* b, void* stream);

@@ -44,6 +44,7 @@ SIGNATURES = {
     "p4a_kernel_launches": ([], C.c_uint64),
     "p4a_grid_sort_noalloc": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp], C.c_int),
     "p4a_batch_create": ([C.c_int, _vp, C.POINTER(_vp)], C.c_int),
+    "p4a_batch_footprint": ([_vp, C.POINTER(C.c_int64)], C.c_int),
     "p4a_batch_destroy": ([_vp], C.c_int),
     "p4a_batch_last_error": ([_vp], C.c_char_p),
     "p4a_batch_set_stream": ([_vp, _vp], C.c_int),

@@ -52,6 +52,11 @@ template <class T>
 int balloc(p4a_batch* b, T** out, int64_t count) {
   void* p = nullptr;
   const size_t bytes = std::max<size_t>(16, (size_t)count * sizeof(T));
+  if (b->sizeOnly) {  // p4a_batch_footprint: count the bytes, allocate nothing
+    b->deviceBytes += bytes;
+    *out = nullptr;
+    return P4A_OK;
+  }
   cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) return bfail(b, P4A_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
   if ((e = cudaMemset(p, 0, bytes)) != cudaSuccess) {
@@ -642,31 +647,22 @@ int admit(p4a_batch* b, const p4a_params& params, HostScene& sc, int pourBudget,
   return P4A_OK;
 }
 
-}  // namespace
+bool config_ok(const p4a_batch_config* cfg) {
+  return cfg && cfg->max_particles > 0 && cfg->max_cells > 0 && cfg->max_scenes > 0 &&
+         cfg->max_particles <= 0x7fffffffLL && cfg->max_cells <= 0x7fffffffLL;
+}
 
+p4a_batch_config normalised(p4a_batch_config c) {
+  if (c.max_bodies < 1) c.max_bodies = 1;
+  if (c.max_body_parts < 1) c.max_body_parts = 1;
+  if (c.max_boundary < 1) c.max_boundary = 1;
+  return c;
+}
 
-extern "C" {
-
-int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
-  if (!cfg || !out || cfg->max_particles <= 0 || cfg->max_cells <= 0 || cfg->max_scenes <= 0 ||
-      cfg->max_particles > 0x7fffffffLL || cfg->max_cells > 0x7fffffffLL)
-    return P4A_ERR_ARG;
-  *out = nullptr;
-  const int chk = p4a_device_check(device);
-  if (chk != P4A_OK) return chk;
-  if (cudaSetDevice(device) != cudaSuccess) return P4A_ERR_CUDA;
-  p4a_batch* b = new p4a_batch();
-  b->device = device;
-  b->cfg = *cfg;
-  if (b->cfg.max_bodies < 1) b->cfg.max_bodies = 1;
-  if (b->cfg.max_body_parts < 1) b->cfg.max_body_parts = 1;
-  if (b->cfg.max_boundary < 1) b->cfg.max_boundary = 1;
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete b;
-    return P4A_ERR_CUDA;
-  }
-  b->ownStream = true;
-  for (int k = 0; k < 2; k++) cudaEventCreateWithFlags(&b->stagingDone[k], cudaEventDisableTiming);
+// Every arena of a batch, sized from b->cfg (its minimums already applied). With
+// b->sizeOnly set nothing is allocated and b->deviceBytes receives the total.
+int alloc_arenas(p4a_batch* b) {
+  const p4a_batch_config* cfg = &b->cfg;
   const int64_t P = cfg->max_particles, Cc = cfg->max_cells + (int64_t)cfg->max_scenes * (kScanTile + 2);
   b->scanTilesCap = Cc / kScanTile + cfg->max_scenes + 1;
   DevScene& d = b->d;
@@ -694,11 +690,46 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
        (rc = balloc(b, &d.statsOut, (int64_t)cfg->max_scenes * 8)) ||
        (rc = balloc(b, &b->dParams, (int64_t)kMaxSubsteps * cfg->max_scenes))))
     ;
+  return rc;
+}
+
+}  // namespace
+
+
+extern "C" {
+
+int p4a_batch_footprint(const p4a_batch_config* cfg, int64_t* bytes) {
+  if (!bytes || !config_ok(cfg)) return P4A_ERR_ARG;
+  p4a_batch b;
+  b.sizeOnly = true;
+  b.cfg = normalised(*cfg);
+  const int rc = alloc_arenas(&b);
+  *bytes = (int64_t)b.deviceBytes;
+  return rc;
+}
+
+int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
+  if (!config_ok(cfg) || !out) return P4A_ERR_ARG;
+  *out = nullptr;
+  const int chk = p4a_device_check(device);
+  if (chk != P4A_OK) return chk;
+  if (cudaSetDevice(device) != cudaSuccess) return P4A_ERR_CUDA;
+  p4a_batch* b = new p4a_batch();
+  b->device = device;
+  b->cfg = normalised(*cfg);
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete b;
+    return P4A_ERR_CUDA;
+  }
+  b->ownStream = true;
+  for (int k = 0; k < 2; k++) cudaEventCreateWithFlags(&b->stagingDone[k], cudaEventDisableTiming);
+  const int64_t P = cfg->max_particles, Cc = cfg->max_cells + (int64_t)cfg->max_scenes * (kScanTile + 2);
+  int rc = alloc_arenas(b);
   if (rc) {
     p4a_batch_destroy(b);
     return rc;
   }
-  d.cap = (uint32_t)P;
+  b->d.cap = (uint32_t)P;
   b->partA.init(P);
   b->cellA.init(Cc);
   b->boundA.init(b->cfg.max_boundary);

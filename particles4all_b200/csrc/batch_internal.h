@@ -98,6 +98,7 @@ struct p4a_batch {
   p4a::DevScene d{};
   std::vector<void*> allocs;
   size_t deviceBytes = 0;
+  bool sizeOnly = false;  // balloc counts bytes instead of allocating (p4a_batch_footprint)
   p4a::RangeAlloc partA, cellA, boundA, bodyA, listA;
   std::vector<p4a::BScene> scenes;
   int64_t scanTilesCap = 0;

@@ -23,23 +23,38 @@ from ._lib import P4AError, lib
 from ._scene_desc import scene_desc
 from .params import CParams
 
-# Device bytes the batch arenas take per unit of capacity (the allocation list of
-# p4a_batch_create): per particle slot the ping-pong particle arrays, solver
-# scratch, sort keys and neighbour masks; per cell the histogram, cellStart and
-# boundary cellStart; per boundary sample its position and psi.
-BYTES_PER_PARTICLE = 324
-BYTES_PER_CELL = 12
-BYTES_PER_BOUNDARY = 20
+def _arenas(p, max_scenes):
+    """Arena sizes for p particle slots: one cell and half a boundary sample per
+    particle slot (the ratio of dam-break scenes), an eighth of a slot for body
+    particles and 16 bodies per scene."""
+    return dict(max_particles=int(p), max_cells=int(p), max_boundary=max(1, int(p) // 2),
+                max_scenes=int(max_scenes), max_bodies=int(max_scenes) * 16, max_body_parts=max(1, int(p) // 8))
+
+
+def arena_bytes(arenas):
+    """Device bytes of the batch arenas for these sizes, as p4a_batch_create
+    allocates them (p4a_batch_footprint)."""
+    cfg = _abi.BatchConfig()
+    for k, v in arenas.items():
+        setattr(cfg, k, int(v))
+    out = C.c_int64()
+    rc = lib().p4a_batch_footprint(C.byref(cfg), C.byref(out))
+    if rc != 0:
+        raise P4AError(rc, "p4a_batch_footprint")
+    return int(out.value)
 
 
 def arenas_for_budget(budget_bytes, max_scenes=4096):
-    """Arena sizes whose allocation fits in `budget_bytes` of device memory: one cell
-    and half a boundary sample per particle slot (the ratio of dam-break scenes)."""
-    per = BYTES_PER_PARTICLE + BYTES_PER_CELL + BYTES_PER_BOUNDARY / 2 + 1
-    p = int(budget_bytes // per)
-    p = min(p, (1 << 31) - (1 << 24))
-    return dict(max_particles=p, max_cells=p, max_boundary=max(1, p // 2), max_scenes=int(max_scenes),
-                max_bodies=int(max_scenes) * 16, max_body_parts=max(1, p // 8))
+    """The largest arena sizes (in the ratios of _arenas) whose allocation fits in
+    `budget_bytes` of device memory."""
+    p0 = 1 << 20
+    f0, f1 = arena_bytes(_arenas(p0, max_scenes)), arena_bytes(_arenas(2 * p0, max_scenes))
+    slope = (f1 - f0) / p0
+    p = int((budget_bytes - (f0 - slope * p0)) / slope)
+    p = max(1, min(p, (1 << 31) - (1 << 24)))
+    while p > 1 and arena_bytes(_arenas(p, max_scenes)) > budget_bytes:
+        p = int(p * 0.999)
+    return _arenas(p, max_scenes)
 
 
 class Server:

@@ -141,3 +141,22 @@ def test_tuning_table_host_side(built, tmp_path):
     finally:
         L.p4a_tune_clear(-1)
         autotune.load(L=L)
+
+
+def test_batch_footprint_sizes_server_arenas(built):
+    """p4a_batch_footprint counts the arenas p4a_batch_create would allocate (no
+    device needed), and the serving loop's arena sizing stays within its budget."""
+    from particles4all_b200 import server
+    L = _lib.lib()
+    out = C.c_int64()
+    cfg = _abi.BatchConfig()
+    assert L.p4a_batch_footprint(C.byref(cfg), C.byref(out)) == _abi.P4A_ERR_ARG
+    small, big = server._arenas(1 << 16, 64), server._arenas(1 << 17, 64)
+    fs, fb = server.arena_bytes(small), server.arena_bytes(big)
+    # per particle slot at least the ten float4 ping-pong arrays, the solver arrays
+    # and the two pairs of nine-row neighbour masks (u64 + u32 each)
+    assert (fb - fs) / (1 << 16) >= 160 + 44 + 2 * 9 * 12
+    for budget in (1 << 30, 8 << 30, 160_000_000_000):
+        a = server.arenas_for_budget(budget, 4096)
+        assert server.arena_bytes(a) <= budget
+        assert server.arena_bytes(server._arenas(int(a["max_particles"] * 1.01), 4096)) > budget
