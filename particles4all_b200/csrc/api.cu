@@ -322,11 +322,9 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.corr, cap)) || (rc = dalloc(s, L, &s->d.normal, cap)) ||
       (rc = dalloc(s, L, &s->d.key, cap)) || (rc = dalloc(s, L, &s->d.rank, cap)) ||
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
-      (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbMask, cap * 9)) ||
-      (rc = dalloc(s, L, &s->d.nbBMask, cap * 9)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
-      (rc = dalloc(s, L, &s->d.nbMaskX, cap * 9)) || (rc = dalloc(s, L, &s->d.nbBMaskX, cap * 9)) ||
-      (rc = dalloc(s, L, &s->d.disp, kDispSlots)) ||
-      (rc = dalloc(s, L, &s->d.nbLong, cap)))
+      (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbList, cap * kListCap)) ||
+      (rc = dalloc(s, L, &s->d.nbCount, cap)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
+      (rc = dalloc(s, L, &s->d.disp, kDispSlots)))
     return rc;
   s->d.cap = (uint32_t)cap;
   if ((rc = alloc_cells(s))) return rc;

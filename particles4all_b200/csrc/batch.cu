@@ -676,9 +676,9 @@ int alloc_arenas(p4a_batch* b) {
   if (!rc &&
       ((rc = balloc(b, &d.lambda, P)) || (rc = balloc(b, &d.density, P)) || (rc = balloc(b, &d.corr, P)) ||
        (rc = balloc(b, &d.normal, P)) || (rc = balloc(b, &d.key, P)) || (rc = balloc(b, &d.rank, P)) ||
-       (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbMask, P * 9)) || (rc = balloc(b, &d.nbBMask, P * 9)) ||
-       (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.nbMaskX, P * 9)) || (rc = balloc(b, &d.nbBMaskX, P * 9)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
-       (rc = balloc(b, &d.nbLong, P)) || (rc = balloc(b, &d.cellCount, Cc)) ||
+       (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbList, P * kListCap)) || (rc = balloc(b, &d.nbCount, P)) ||
+       (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
+       (rc = balloc(b, &d.cellCount, Cc)) ||
        (rc = balloc(b, &d.cellStart, Cc)) || (rc = balloc(b, &d.bcellStart, Cc)) ||
        (rc = balloc(b, &d.scanState, b->scanTilesCap)) || (rc = balloc(b, &d.scanTicket, 4)) ||
        (rc = balloc(b, &d.errorWord, 4)) || (rc = balloc(b, &d.bpos, b->cfg.max_boundary)) ||

@@ -11,8 +11,9 @@
 // With L = P.parity ^ 1 the live copy after the sort, the final positions are in
 // pred[L ^ (iters & 1)]; the velFromPos velocities are in the non-live copy
 // vel[L ^ 1], so the final velocity can be written to vel[L] while neighbours still
-// read the other one. xsph+normals builds the neighbour masks (neighbours.cuh) and
-// stores them for the tension pass, which walks the same positions.
+// read the other one. Each pass builds its neighbour list with radius h
+// (neighbours.cuh) and walks it; xsph+normals stores the list for the tension pass,
+// which walks the same positions.
 #include <cuda_runtime.h>
 
 #include "neighbours.cuh"
@@ -66,6 +67,20 @@ __device__ __forceinline__ void block_stats(const SimParams& P, bool act, float 
   }
 }
 
+// The neighbour list of the finishing passes (positions after the last Jacobi
+// iteration): lambda's list when the displacement bound still covers it and it
+// holds no boundary samples (which these passes do not visit), else a new list
+// with radius h, stored in nbList.
+__device__ __forceinline__ uint32_t finish_list(const SimParams& P, const DevScene& d, const RowWalk& w,
+                                                uint32_t i, F3 pi, const float4* __restrict__ pred,
+                                                const uint32_t* __restrict__ cs) {
+  if (list_reusable(P, d, (int)P.iters, i, cell_index(P, w.c))) {
+    const uint32_t c = __ldg(&d.nbCount[i]);
+    if (c != kListOverflow && !(c & kHasBound)) return c;
+  }
+  return build_list<false>(P, w, i, pi, pred, cs, nullptr, nullptr, d.nbList, d.cap, P.h2);
+}
+
 // xsph (+ finalize) for scenes without surface tension. All threads reach the
 // stats tree, so there is no early return.
 __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const DevScene& d, uint32_t tile,
@@ -83,28 +98,18 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
     const float4 p4 = __ldg(&pred[i]);
     const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
     const RowWalk w(P, pi);
-    const RowStage<kBlock, false> st;
-    uint32_t todo = 0u, longRows = 0u;
-#pragma unroll
-    for (int r = 0; r < kRows; r++) {
-      const int rb = w.row_base(P, r);
-      if (rb < 0) continue;
-      bool lg;
-      uint32_t b;
-      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.h2);
-      st.set(r, lg ? 0ull : mr, b);
-      longRows |= (uint32_t)lg << r;
-      todo |= (uint32_t)(mr != 0ull || lg) << r;
-    }
+    const uint32_t cap = d.cap;
+    const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
     F3 acc = {0.f, 0.f, 0.f};
     auto fluid = [&](uint32_t j) {
       if (j == i) return;
       const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
       const float r2 = dot3(rij, rij);
+      if (r2 >= P.h2) return;  // in the skin of a reused list only
       const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
       acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
     };
-    walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
+    walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
     const F3 corr = mul3(acc, P.xsphC);
     vf = add3(vi, corr);
     d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
@@ -127,26 +132,14 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i])), vi = xyz(__ldg(&velIn[i]));
   const RowWalk w(P, pi);
-  const RowStage<TB, false> st;
-  uint32_t todo = 0u, longRows = 0u;
-#pragma unroll
-  for (int r = 0; r < kRows; r++) {
-    const int rb = w.row_base(P, r);
-    if (rb < 0) continue;
-    bool lg;
-    uint32_t b;
-    const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.h2);
-    d.nbMask[(size_t)r * cap + i] = mr;
-    st.set(r, lg ? 0ull : mr, b);
-    longRows |= (uint32_t)lg << r;
-    todo |= (uint32_t)(mr != 0ull || lg) << r;
-  }
-  d.nbLong[i] = longRows;
+  const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
+  d.nbCount[i] = count;
   F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
   auto fluid = [&](uint32_t j) {
     if (j == i) return;
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2) return;  // in the skin of a reused list only
     const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
     const float f = P.mass * poly6(P, r2) / dj;
     acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
@@ -156,7 +149,7 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
     const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / rr);
     nacc = fma3(coef, rij, nacc);
   };
-  walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
+  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
   d.corr[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
   d.normal[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
 }
@@ -178,23 +171,12 @@ __device__ __forceinline__ void tension_finalize_body(const SimParams& P, const 
     const F3 pi = xyz(p4), ni = xyz(__ldg(&d.normal[i]));
     rhoi = __ldg(&d.density[i]);
     const RowWalk w(P, pi);
-    const uint32_t longRows = __ldg(&d.nbLong[i]);
-    const RowStage<kBlock, false> st;
-    uint32_t todo = 0u;
-#pragma unroll
-    for (int r = 0; r < kRows; r++) {
-      const int rb = w.row_base(P, r);
-      if (rb < 0) continue;
-      const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
-      const bool lg = (longRows >> r) & 1u;
-      st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]));
-      todo |= (uint32_t)(mr != 0ull || lg) << r;
-    }
+    const uint32_t count = __ldg(&d.nbCount[i]);  // xsph+normals' list for these positions
     F3 acc = {0.f, 0.f, 0.f};
     auto fluid = [&](uint32_t j) {
       const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
       const float r2 = dot3(rij, rij);
-      if (r2 < 1.0e-12f || j == i) return;
+      if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
       const float rr = sqrtf(r2);
       const float hrr = P.h - rr;
       const float k = hrr * hrr * hrr * rr * rr * rr;
@@ -206,7 +188,7 @@ __device__ __forceinline__ void tension_finalize_body(const SimParams& P, const 
       const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&d.density[j]));
       acc = fma3(wgt, add3(fCoh, fCurv), acc);
     };
-    walk_fluid_rows(st, todo, longRows, fluid, [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); });
+    walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
     const float4 c0 = d.corr[i];
     const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
     d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);

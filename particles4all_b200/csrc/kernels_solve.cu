@@ -7,16 +7,15 @@
 //
 // Buffers follow the substep's parity L = P.parity ^ 1 (the live copy after the
 // sort): iteration `it` reads pred[L ^ (it & 1)] and delta writes the other copy.
-// lambda builds the per-row neighbour masks (neighbours.cuh) and stores them; delta
-// runs on the same positions, so it reuses them and skips the candidate tests.
-// The masks are built with the radius h + skin and also serve later iterations of
-// the substep: every delta (and the rigid projection) records the largest
-// displacement of its iteration, and an iteration reuses the masks of the last
-// rebuild while the summed displacements since then stay within skin / 2 (so every
-// pair now within h was within h + skin then) and the particle is still in the cell
-// it was in then (so its candidate rows are the same). Phase 2 tests r^2 < h^2 on
-// every masked candidate, so the visited neighbours and their order are exactly the
-// reference's either way.
+// lambda builds each particle's neighbour list (neighbours.cuh) with the radius
+// h + skin and stores it; delta runs on the same positions and walks the same
+// list. The list also serves later iterations of the substep: every delta (and
+// the rigid projection) records the largest displacement of its iteration, and an
+// iteration reuses the list of the last rebuild while the summed displacements
+// since then stay within skin / 2 (so every pair now within h was within h + skin
+// then) and the particle is still in the cell it was in then (so its candidate
+// rows are the same). Every pass re-tests r^2 < h^2 on each listed candidate, so
+// the visited neighbours and their order are exactly the reference's either way.
 // The last delta of a substep also writes velFromPos (src/wgsl.js:72-83) for every
 // particle into the non-live velocity copy; body particles are overwritten by the
 // rigid projection that follows.
@@ -29,7 +28,6 @@
 
 namespace p4a {
 
-template <int TB>
 __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
@@ -40,71 +38,25 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i]));
   const RowWalk w(P, pi);
-  const RowStage<TB, true> st;
-  // reuse the masks of the last rebuild while the displacement bound allows
+  // reuse the list of the last rebuild while the displacement bound allows
   const uint32_t cell = cell_index(P, w.c);
-  bool reuse = false;
-  if (it > 0 && it < kDispSlots) {
-    const float* disp = d.disp + (size_t)P.slot * kDispSlots;
-    int ref = 0;
-    float D = 0.0f;
-    for (int t = 0; t < it; t++) {
-      D += __ldg(&disp[t]);
-      if (D * 1.00001f > P.skinHalf) {  // iteration t + 1 rebuilt
-        ref = t + 1;
-        D = 0.0f;
-      }
-    }
-    reuse = ref < it && __ldg(&d.nbCell[i]) == cell;
-  }
-  uint32_t todo = 0u, longRows = 0u;
-#pragma unroll
-  for (int r = 0; r < kRows; r++) st.set(r, 0ull, 0u, 0u);
+  const bool reuse = list_reusable(P, d, it, i, cell);
+  uint32_t count;
   if (reuse) {
-    longRows = __ldg(&d.nbLong[i]);
-#pragma unroll
-    for (int r = 0; r < kRows; r++) {
-      const int rb = w.row_base(P, r);
-      if (rb < 0) continue;
-      const uint64_t mr = __ldg(&d.nbMask[(size_t)r * cap + i]);
-      const uint32_t bm = __ldg(&d.nbBMask[(size_t)r * cap + i]);
-      const bool lg = (longRows >> r) & 1u, lgb = (longRows >> (16 + r)) & 1u;
-      st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]), lgb ? 0u : bm);
-      todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
-    }
+    count = __ldg(&d.nbCount[i]);
   } else {
-    // phase 1: fluid and boundary masks of every row, radius h + skin (stored)
-#pragma unroll
-    for (int r = 0; r < kRows; r++) {
-      const int rb = w.row_base(P, r);
-      if (rb < 0) continue;
-      bool lg;
-      uint32_t b;
-      const uint64_t mr = row_mask(P, w, rb, pi, pred, cs, lg, b, P.skinH2);
-      uint32_t bm = 0u;
-      bool lgb = false;
-      if (P.nBoundary > 0u) {
-        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-        if (be > bb) bm = boundary_mask(P, bb, be, pi, d.bpos, lgb, P.skinH2);
-      }
-      d.nbMask[(size_t)r * cap + i] = mr;
-      d.nbBMask[(size_t)r * cap + i] = bm;
-      st.set(r, lg ? 0ull : mr, b, lgb ? 0u : bm);
-      longRows |= ((uint32_t)lg << r) | ((uint32_t)lgb << (16 + r));
-      todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
-    }
-    d.nbLong[i] = longRows;
+    count = build_list<true>(P, w, i, pi, pred, cs, bcs, d.bpos, d.nbList, cap, P.skinH2);
+    d.nbCount[i] = count;
     d.nbCell[i] = cell;
   }
-  // phase 2
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;
-  auto fluid = [&](uint32_t j) -> bool {
-    if (j == i) return false;
+  auto fluid = [&](uint32_t j) {
+    if (j == i) return;
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return false;  // in the skin of the mask only
+    if (r2 >= P.h2) return;  // in the skin of the list only
     rho = fmaf(P.mass, poly6(P, r2), rho);
     if (r2 > 1.0e-12f) {
       const float rr = sqrtf(r2);
@@ -114,41 +66,22 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
       gradSum = add3(gradSum, g);
       sumGrad2 = sumGrad2 + dot3(g, g);
     }
-    return true;
   };
-  // one boundary sample k (1e-12 <= r^2 < h^2 is tested here or by the caller)
-  auto sample = [&](uint32_t k) -> bool {
+  auto bound = [&](uint32_t k) {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return false;
+    if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float psi = __ldg(&d.bpsi[k]);
     rho = fmaf(psi, poly6(P, r2), rho);
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
     gradSum = fma3(s, rij, gradSum);
-    return true;
   };
-  walk_rows(
-      st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
-      [&](int r, uint32_t k) { return sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
-      [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
-      [&](int r) {
-        const int rb = w.row_base(P, r);
-        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-        for (uint32_t k = bb; k < be; k++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-          sample(k);
-        }
-      },
-      [&](int r, uint64_t em, uint32_t ebm) { st.set(r, em, 0u, ebm); });  // the row's stage is free now
-  // exact masks for delta, all rows at once (rows that were not walked hold zero)
-#pragma unroll
-  for (int r = 0; r < kRows; r++) {
-    d.nbMaskX[(size_t)r * cap + i] = st.mask[r * TB];
-    d.nbBMaskX[(size_t)r * cap + i] = st.bmask[r * TB];
+  if (count != kListOverflow) {
+    walk_list(d.nbList, cap, i, count, fluid, bound);
+  } else {
+    walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
   }
   d.density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
@@ -160,7 +93,6 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   }
 }
 
-template <int TB>
 __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
@@ -173,26 +105,13 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i]));
   const float li_ = __ldg(&lambda[i]);
-  const RowWalk w(P, pi);
-  const uint32_t longRows = __ldg(&d.nbLong[i]);
-  const RowStage<TB, true> st;
-  uint32_t todo = 0u;
-#pragma unroll
-  for (int r = 0; r < kRows; r++) {
-    const int rb = w.row_base(P, r);
-    if (rb < 0) continue;
-    const uint64_t mr = __ldg(&d.nbMaskX[(size_t)r * cap + i]);  // lambda's exact masks
-    const uint32_t bm = __ldg(&d.nbBMaskX[(size_t)r * cap + i]);
-    const bool lg = (longRows >> r) & 1u, lgb = (longRows >> (16 + r)) & 1u;
-    st.set(r, lg ? 0ull : mr, __ldg(&cs[rb + w.x0]), lgb ? 0u : bm);
-    todo |= (uint32_t)(mr != 0ull || lg || bm != 0u || lgb) << r;
-  }
+  const uint32_t count = __ldg(&d.nbCount[i]);  // lambda's list for these positions
   F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
   float nc = 1.0f;
-  auto fluid = [&](uint32_t j) -> bool {
+  auto fluid = [&](uint32_t j) {
     const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return false;
+    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = P.spikyGrad * hr * hr / rr;
@@ -203,33 +122,22 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     const float coef = (li_ + __ldg(&lambda[j]) + sc) * s;
     dsum = fma3(coef, rij, dsum);
     nc += 1.0f;
-    return true;
   };
-  auto sample = [&](uint32_t k) -> bool {
+  auto bound = [&](uint32_t k) {
     const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2) return false;
+    if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float coef = (li_ * __ldg(&d.bpsi[k])) * (P.spikyGrad * hr * hr / rr);
     dB = fma3(coef, rij, dB);
-    return true;
   };
-  walk_rows(
-      st, todo, longRows & 0x1ffu, longRows >> 16, fluid,
-      [&](int r, uint32_t k) { return sample(__ldg(&bcs[w.row_base(P, r) + w.x0]) + k); },
-      [&](int r) { long_row(P, w, w.row_base(P, r), pi, pred, cs, fluid); },
-      [&](int r) {
-        const int rb = w.row_base(P, r);
-        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
-        for (uint32_t k = bb; k < be; k++) {
-          const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
-          const float r2 = dot3(rij, rij);
-          if (r2 >= P.h2 || r2 < 1.0e-12f) continue;
-          sample(k);
-        }
-      },
-      [](int, uint64_t, uint32_t) {});
+  if (count != kListOverflow) {
+    walk_list(d.nbList, cap, i, count, fluid, bound);
+  } else {
+    const RowWalk w(P, pi);
+    walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
+  }
   const F3 dd = {fmaf(dB.x, P.invRho0, dsum.x * P.volume), fmaf(dB.y, P.invRho0, dsum.y * P.volume),
                  fmaf(dB.z, P.invRho0, dsum.z * P.volume)};
   float scale = P.omega;
@@ -252,22 +160,22 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda(const __grid_constant__ SimParams P,
                                                    const __grid_constant__ DevScene d, int it) {
-  lambda_body<TB>(P, d, blockIdx.x * TB + threadIdx.x, it);
+  lambda_body(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda_b(const __grid_constant__ BatchWork w,
                                                      const __grid_constant__ DevScene d, int it) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { lambda_body<TB>(P, d, li, it); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { lambda_body(P, d, li, it); });
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_delta(const __grid_constant__ SimParams P,
                                                   const __grid_constant__ DevScene d, int it) {
-  delta_body<TB>(P, d, blockIdx.x * TB + threadIdx.x, it);
+  delta_body(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_delta_b(const __grid_constant__ BatchWork w,
                                                     const __grid_constant__ DevScene d, int it) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { delta_body<TB>(P, d, li, it); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { delta_body(P, d, li, it); });
 }
 
 using PlainFn = void (*)(SimParams, DevScene, int);

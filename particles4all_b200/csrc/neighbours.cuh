@@ -2,33 +2,36 @@
 //
 // The reference walks, for particle i, the 3x3 row ranges
 // [cellStart[row+x0], cellStart[row+x1+1]) of the cell block around
-// cellOf(pred_i) and tests every candidate j against r^2 < h^2 (src/wgsl.js:98-111).
+// cellOf(pred_i) and tests every candidate j against r^2 < h^2 (src/wgsl.js:98-111),
+// the boundary samples of a row after its fluid particles (src/wgsl.js:497-533).
 // Here that walk is split in two phases:
-//   1. a cheap test of every candidate that records, per row, a 64-bit mask of the
-//      candidates within h (bit k <-> j = rowStart + k);
-//   2. the pass's real work over the set bits in ascending order.
-// Phase 2 therefore visits exactly the reference's neighbours in exactly its order
-// (rows z->y, j ascending, the boundary samples of a row after its fluid
-// particles), so sums are bit-identical, while the expensive in-range work no
-// longer runs warp-wide on every candidate iteration. Two passes that walk the
-// same positions (lambda then delta, xsph+normals then tension) share the masks:
-// the first stores them, the second skips phase 1. Rows with more than 64
-// candidates (never seen at rest density, where a row holds ~24) fall back to
-// the reference's direct loop.
-//
-// Phase 2 is one loop over all nine rows (walk_rows), not a loop per row: each
-// thread's row masks and row starts are staged in shared memory and every
-// iteration handles exactly one neighbour of every lane that has one left. Lanes
-// of a warp hold different numbers of neighbours per row, so a loop per row runs
-// each row to its warp maximum (about half the lanes idle in the expensive body);
-// the single loop runs to the warp maximum of the totals instead.
+//   1. build_list tests every candidate once and appends the ones within a radius
+//      (h, or h + skin for lists that later Jacobi iterations reuse) to the
+//      particle's neighbour list, in the reference's visiting order: rows z->y,
+//      fluid j ascending, then the row's boundary samples (tagged kBoundTag);
+//   2. walk_list runs the pass's real work over the list, one entry per loop
+//      iteration, every entry re-tested against r^2 < h^2 with the current
+//      positions by the pass itself.
+// Phase 2 therefore visits exactly the reference's neighbours in exactly its
+// order, so sums are bit-identical, while the expensive in-range work no longer
+// runs warp-wide on every candidate, and the loop has no per-row bookkeeping:
+// lanes of a warp hold different numbers of neighbours per row, so a walk that
+// switches rows inside the loop pays the switch in almost every iteration.
+// The list is stored [entry][particle] (entry k of particle i at k * cap + i), so
+// the lanes of a warp read entry k of 32 consecutive particles with one
+// coalesced load. The particle itself is never listed (it contributes to no
+// pass). A particle with more than kListCap entries is marked kListOverflow and
+// walked with the reference's direct loop instead.
 #pragma once
 #include "p4a_math.cuh"
 
 namespace p4a {
 
 constexpr int kRows = 9;
-constexpr uint32_t kMaskBits = 64;
+constexpr uint32_t kListOverflow = 0xffffffffu;  // count of a particle whose list did not fit
+constexpr uint32_t kBoundTag = 0x80000000u;      // entry = kBoundTag | boundary sample index
+constexpr uint32_t kHasBound = 0x40000000u;      // count flag: the list holds boundary samples
+constexpr uint32_t kCountMask = 0x0000ffffu;
 
 // Row r = 3*(dz+1) + (dy+1), the reference's dz-outer, dy-inner order.
 struct RowWalk {
@@ -47,149 +50,146 @@ struct RowWalk {
   }
 };
 
-// Phase 1 for one row (row base rb >= 0): the mask of candidates with r^2 < r2lim
-// (h^2, or (h + skin)^2 for masks that later iterations reuse); sets *isLong when the
-// row has more than 64 candidates and *b to the row's start.
-__device__ __forceinline__ uint64_t row_mask(const SimParams& P, const RowWalk& w, int rb, F3 pi,
-                                             const float4* __restrict__ pred,
-                                             const uint32_t* __restrict__ cs, bool& isLong,
-                                             uint32_t& b, float r2lim) {
-  uint64_t m = 0ull;
-  b = __ldg(&cs[rb + w.x0]);
-  const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
-  const uint32_t len = e > b ? e - b : 0u;
-  isLong = len > kMaskBits;
-  const uint32_t lim = min(len, kMaskBits);
-  uint32_t k = 0;
-  for (; k + 4 <= lim; k += 4) {
-    const float4 q0 = __ldg(&pred[b + k]), q1 = __ldg(&pred[b + k + 1]);
-    const float4 q2 = __ldg(&pred[b + k + 2]), q3 = __ldg(&pred[b + k + 3]);
-    const F3 d0 = sub3(pi, xyz(q0)), d1 = sub3(pi, xyz(q1));
-    const F3 d2 = sub3(pi, xyz(q2)), d3 = sub3(pi, xyz(q3));
-    const uint32_t bits = (dot3(d0, d0) < r2lim ? 1u : 0u) | (dot3(d1, d1) < r2lim ? 2u : 0u) |
-                          (dot3(d2, d2) < r2lim ? 4u : 0u) | (dot3(d3, d3) < r2lim ? 8u : 0u);
-    m |= (uint64_t)bits << k;
-  }
-  for (; k < lim; k++) {
-    const F3 d0 = sub3(pi, xyz(__ldg(&pred[b + k])));
-    if (dot3(d0, d0) < r2lim) m |= 1ull << k;
-  }
-  return m;
-}
-
-// The reference's direct loop over one row's fluid candidates (rows longer than 64).
-template <class F>
-__device__ __forceinline__ void long_row(const SimParams& P, const RowWalk& w, int rb, F3 pi,
-                                         const float4* __restrict__ pred,
-                                         const uint32_t* __restrict__ cs, F&& f) {
-  const uint32_t b = __ldg(&cs[rb + w.x0]);
-  const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
-  for (uint32_t j = b; j < e; j++) {
-    const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
-    if (dot3(d, d) < P.h2) f(j);
-  }
-}
-
-// Phase 1 for one row's boundary samples [bb, be): the mask of samples with
-// 1e-12 <= r^2 < r2lim (the ones the reference's boundary terms use, when r2lim is
-// h^2); sets *isLong when the row has more than 32 samples.
-constexpr uint32_t kBMaskBits = 32;
-__device__ __forceinline__ uint32_t boundary_mask(const SimParams& P, uint32_t bb, uint32_t be, F3 pi,
-                                                  const float4* __restrict__ bpos, bool& isLong,
-                                                  float r2lim) {
-  const uint32_t len = be > bb ? be - bb : 0u;
-  isLong = len > kBMaskBits;
-  const uint32_t lim = min(len, kBMaskBits);
-  uint32_t m = 0u;
-  for (uint32_t k = 0; k < lim; k++) {
-    const F3 d = sub3(pi, xyz(__ldg(&bpos[bb + k])));
-    const float r2 = dot3(d, d);
-    if (r2 < r2lim && r2 >= 1.0e-12f) m |= 1u << k;
-  }
-  return m;
-}
-
-// Per-thread row staging in shared memory for a block of TB threads: fluid mask,
-// row start and (when the pass has boundary terms, B) boundary mask of each of the
-// nine rows, in columns [r * TB + threadIdx.x].
-template <int TB, bool B>
-struct RowStage {
-  uint64_t* mask;
-  uint32_t* base;
-  uint32_t* bmask;
-  __device__ __forceinline__ RowStage() {
-    __shared__ uint64_t sMask[kRows * TB];
-    __shared__ uint32_t sBase[kRows * TB];
-    mask = sMask + threadIdx.x;
-    base = sBase + threadIdx.x;
+// Phase 1: the list of particle i (scene-local cellStart cs / bcs, arena index i)
+// with every candidate j != i of the nine rows within r^2 < r2lim, and, when B,
+// every boundary sample of each row within r^2 < r2lim after the row's fluid
+// candidates. Returns the entry count (| kHasBound when boundary samples were
+// listed), or kListOverflow.
+template <bool B>
+__device__ __forceinline__ uint32_t build_list(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
+                                               const float4* __restrict__ pred,
+                                               const uint32_t* __restrict__ cs,
+                                               const uint32_t* __restrict__ bcs,
+                                               const float4* __restrict__ bpos, uint32_t* __restrict__ list,
+                                               uint32_t cap, float r2lim) {
+  uint32_t c = 0, flags = 0u;
+  auto push = [&](uint32_t e) {
+    if (c < kListCap) list[(size_t)c * cap + i] = e;
+    c++;
+  };
+#pragma unroll 1
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    const uint32_t b = __ldg(&cs[rb + w.x0]);
+    const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
+    uint32_t j = b;
+    for (; j + 4 <= e; j += 4) {
+      const float4 q0 = __ldg(&pred[j]), q1 = __ldg(&pred[j + 1]);
+      const float4 q2 = __ldg(&pred[j + 2]), q3 = __ldg(&pred[j + 3]);
+      const F3 d0 = sub3(pi, xyz(q0)), d1 = sub3(pi, xyz(q1));
+      const F3 d2 = sub3(pi, xyz(q2)), d3 = sub3(pi, xyz(q3));
+      const bool i0 = dot3(d0, d0) < r2lim, i1 = dot3(d1, d1) < r2lim;
+      const bool i2 = dot3(d2, d2) < r2lim, i3 = dot3(d3, d3) < r2lim;
+      if (i0 && j != i) push(j);
+      if (i1 && j + 1 != i) push(j + 1);
+      if (i2 && j + 2 != i) push(j + 2);
+      if (i3 && j + 3 != i) push(j + 3);
+    }
+    for (; j < e; j++) {
+      const F3 d0 = sub3(pi, xyz(__ldg(&pred[j])));
+      if (dot3(d0, d0) < r2lim && j != i) push(j);
+    }
     if constexpr (B) {
-      __shared__ uint32_t sBMask[kRows * TB];
-      bmask = sBMask + threadIdx.x;
-    } else {
-      bmask = nullptr;
-    }
-  }
-  __device__ __forceinline__ void set(int r, uint64_t m, uint32_t b, uint32_t bm = 0u) const {
-    mask[r * TB] = m;
-    base[r * TB] = b;
-    if constexpr (B) bmask[r * TB] = bm;
-  }
-};
-
-// Phase 2 over all rows in order. Each row's events are its fluid neighbours (set
-// bits, j ascending), then its boundary samples (set bits, k ascending): every loop
-// iteration handles one event of every lane that has one left, with fluid(j) or
-// bound(r, k) (k the sample's offset in the row's boundary range), which return
-// whether the candidate was within h. A row longer than its mask runs longFluid(r)
-// in place of its fluid bits, or longBound(r) in place of its boundary bits. When a
-// row is done, rowDone(r, em, ebm) receives the masks of the candidates that were
-// within h. `todo` has bit r set for every row with anything to visit; lr / lb are
-// the long-row bits.
-template <int TB, bool B, class FFluid, class FBound, class FLongF, class FLongB, class FDone>
-__device__ __forceinline__ void walk_rows(const RowStage<TB, B>& st, uint32_t todo, uint32_t lr, uint32_t lb,
-                                          FFluid&& fluid, FBound&& bound, FLongF&& longFluid,
-                                          FLongB&& longBound, FDone&& rowDone) {
-  int r = -1;
-  uint64_t m = 0ull, em = 0ull;
-  uint32_t mb = 0u, ebm = 0u, base = 0u;
-  for (;;) {
-    while ((m | (uint64_t)mb) == 0ull) {
-      if (r >= 0) {
-        if ((lb >> r) & 1u) longBound(r);
-        rowDone(r, em, ebm);
-        todo &= todo - 1u;  // r is the lowest pending row
+      if (P.nBoundary > 0u) {
+        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+        for (uint32_t k = bb; k < be; k++) {
+          const F3 d0 = sub3(pi, xyz(__ldg(&bpos[k])));
+          if (dot3(d0, d0) < r2lim) {
+            push(kBoundTag | k);
+            flags = kHasBound;
+          }
+        }
       }
-      if (todo == 0u) return;
-      r = __ffs(todo) - 1;
-      m = st.mask[r * TB];
-      base = st.base[r * TB];
-      if constexpr (B) mb = st.bmask[r * TB];
-      em = 0ull;
-      ebm = 0u;
-      if ((lr >> r) & 1u) longFluid(r);  // a long row's fluid comes before its boundary samples
     }
-    if (m != 0ull) {
-      const int k = __ffsll((long long)m) - 1;
-      m &= m - 1ull;
-      if (fluid(base + (uint32_t)k)) em |= 1ull << k;
+  }
+  return c > kListCap ? kListOverflow : c | flags;
+}
+
+// Whether particle i, now in `cell`, may walk the list that lambda built at the
+// last rebuild before iteration `it` of this substep (it = iters: the positions
+// after the last iteration): the summed largest displacements of the iterations
+// since that rebuild stay within skin / 2 and the particle is still in the cell
+// the list was built in. An iteration that rebuilt is one whose own check failed,
+// which every particle sees alike up to the cell test.
+__device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene& d, int it, uint32_t i,
+                                              uint32_t cell) {
+  if (it <= 0 || it >= kDispSlots) return false;
+  const float* disp = d.disp + (size_t)P.slot * kDispSlots;
+  int ref = 0;
+  float D = 0.0f;
+  for (int t = 0; t < it; t++) {
+    D += __ldg(&disp[t]);
+    if (D * 1.00001f > P.skinHalf) {  // iteration t + 1 rebuilt
+      ref = t + 1;
+      D = 0.0f;
+    }
+  }
+  return ref < it && __ldg(&d.nbCell[i]) == cell;
+}
+
+// Phase 2 over a list of `count` entries: fluid(j) for a fluid entry, bound(k) for
+// a boundary sample. The next entry is loaded while the current one is processed.
+template <class FFluid, class FBound>
+__device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
+                                          uint32_t count, FFluid&& fluid, FBound&& bound) {
+  count &= kCountMask;
+  if (count == 0u) return;
+  uint32_t e = __ldg(&list[i]);
+  for (uint32_t k = 1; k <= count; k++) {
+    const uint32_t cur = e;
+    if (k < count) e = __ldg(&list[(size_t)k * cap + i]);
+    if (cur & kBoundTag) {
+      bound(cur & ~kBoundTag);
     } else {
-      const int k = __ffs(mb) - 1;
-      mb &= mb - 1u;
-      if (bound(r, (uint32_t)k)) ebm |= 1u << k;
+      fluid(cur);
     }
   }
 }
 
-// Fluid-only form (passes without boundary terms); fluid(j) returns void.
-template <int TB, class FFluid, class FLongF>
-__device__ __forceinline__ void walk_fluid_rows(const RowStage<TB, false>& st, uint32_t todo, uint32_t lr,
-                                                FFluid&& fluid, FLongF&& longFluid) {
-  walk_rows(
-      st, todo, lr, 0u, [&](uint32_t j) { fluid(j); return false; }, [](int, uint32_t) { return false; },
-      longFluid, [](int) {}, [](int, uint64_t, uint32_t) {});
+// The reference's direct loop (particles whose list overflowed): every candidate
+// j of the nine rows with r^2 < h^2 (j == i included; the passes skip it), then,
+// when B, the row's boundary samples with 1e-12 <= r^2 < h^2.
+template <bool B, class FFluid, class FBound>
+__device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w, F3 pi,
+                                            const float4* __restrict__ pred, const uint32_t* __restrict__ cs,
+                                            const uint32_t* __restrict__ bcs, const float4* __restrict__ bpos,
+                                            FFluid&& fluid, FBound&& bound) {
+#pragma unroll 1
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    const uint32_t b = __ldg(&cs[rb + w.x0]);
+    const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
+    for (uint32_t j = b; j < e; j++) {
+      const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
+      if (dot3(d, d) < P.h2) fluid(j);
+    }
+    if constexpr (B) {
+      if (P.nBoundary > 0u) {
+        const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
+        for (uint32_t k = bb; k < be; k++) {
+          const F3 d = sub3(pi, xyz(__ldg(&bpos[k])));
+          const float r2 = dot3(d, d);
+          if (r2 < P.h2 && r2 >= 1.0e-12f) bound(k);
+        }
+      }
+    }
+  }
 }
 
-// The masks shared by a pair of passes are stored [row][particle] (row-major over
-// the capacity), so each row's loads and stores are coalesced.
+// Fluid-only passes: the list walk, or the direct loop for an overflowed list.
+template <class FFluid>
+__device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
+                                                const float4* __restrict__ pred,
+                                                const uint32_t* __restrict__ cs, const uint32_t* __restrict__ list,
+                                                uint32_t cap, uint32_t count, FFluid&& fluid) {
+  auto none = [](uint32_t) {};
+  if (count != kListOverflow) {
+    walk_list(list, cap, i, count, fluid, none);
+  } else {
+    walk_direct<false>(P, w, pi, pred, cs, nullptr, nullptr, fluid, none);
+  }
+}
 
 }  // namespace p4a

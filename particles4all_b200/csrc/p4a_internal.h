@@ -82,6 +82,8 @@ struct MeshParams {
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };
 
 // Device buffers of a scene, or of the arenas of a batch (same layout).
+constexpr uint32_t kListCap = 96;  // neighbour-list entries per particle (nbList)
+
 struct DevScene {
   float4* pos[2];
   float4* vel[2];
@@ -115,15 +117,11 @@ struct DevScene {
   uint32_t* errorWord;
   float4* smoothPos;
   float4* anisoG;
-  uint64_t* nbMask;     // [9][cap] per-row neighbour masks shared by a pair of passes
-  uint32_t* nbBMask;    // [9][cap] per-row boundary-sample masks (lambda -> delta)
-  uint32_t* nbLong;     // [cap] bit r: row r has more than 64 fluid candidates;
-                        // bit 16 + r: more than 32 boundary candidates
-  uint32_t* nbCell;     // [cap] cell index the lambda masks were built in
-  uint64_t* nbMaskX;    // [9][cap] the exact (radius h) masks of lambda's iteration, for delta
-  uint32_t* nbBMaskX;   // [9][cap]
+  uint32_t* nbList;     // [kListCap][cap] neighbour lists (neighbours.cuh), shared by a pair of passes
+  uint32_t* nbCount;    // [cap] list length, or kListOverflow
+  uint32_t* nbCell;     // [cap] cell index lambda's list was built in
   float* disp;          // [slots][kDispSlots] max |dp| of each iteration of the substep
-  uint32_t cap;         // particle capacity (stride of nbMask)
+  uint32_t cap;         // particle capacity (stride of nbList)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };
 
