@@ -56,6 +56,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
     ap.add_argument("--mix-frames", type=int, default=10)
+    ap.add_argument("--only-mix", choices=["batched", "plain"], default=None,
+                    help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
+                         "frames and exit; for profiling the two forms")
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="length of each served-workload run (batched, then plain); 0 skips it")
     ap.add_argument("--serve-budget-gb", type=float, default=160.0)
@@ -166,17 +169,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def batched_mix_bench(frames, warmup):
-    """The 96-scene mix stepped (a) as one batch (one launch per pass for all
-    scenes, CUDA-graph frames) and (b) as the plain per-scene loop (96 Sim handles
-    on the same stream, one after the other). Device time per frame from CUDA
-    events; particle-substeps/s for both."""
+def mix_arenas(mix):
+    """Batch arena sizes that hold the whole mix."""
     import math
-
-    import torch
-    from particles4all_b200 import Batch, Sim, configs
-    mix = configs.batched_mix()
-    total = sum(sc["pos"].shape[0] for _, sc in mix)
     cap = sum((sc["pos"].shape[0] + 511) // 256 * 256 for _, sc in mix)
     cells = sum((int(math.prod(int(b) for b in p["box"])) // 2048 + 2) * 2048 for p, _ in mix)
     nbound = 0
@@ -185,9 +180,54 @@ def batched_mix_bench(frames, warmup):
         nbound += nb[0] * nb[1] * nb[2] - (nb[0] - 2) * (nb[1] - 2) * (nb[2] - 2)
     bodies = sum(sc["n_bodies"] + 1 for _, sc in mix)
     body_parts = sum(int((sc["phase"][:, 0] > 0).sum()) + 1 for _, sc in mix)
+    return dict(max_particles=cap + 4096, max_cells=cells, max_scenes=len(mix) + 1, max_bodies=bodies + 8,
+                max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
+
+
+def only_mix(form, frames):
+    """The mix stepped in one form only: admission (or reset) then `frames` frames."""
+    import torch
+    from particles4all_b200 import Batch, Sim, configs
+    mix = configs.batched_mix()
     stream = torch.cuda.Stream()
-    b = Batch(max_particles=cap + 4096, max_cells=cells, max_scenes=len(mix) + 1, max_bodies=bodies + 8,
-              max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
+    t0 = time.perf_counter()
+    if form == "batched":
+        b = Batch(**mix_arenas(mix))
+        b.set_stream(stream.cuda_stream)
+        ids = [b.add_scene(p, sc) for p, sc in mix]
+        for _ in range(frames):
+            b.step(ids, 1 / 60)
+        b.synchronize()
+        b.close()
+    else:
+        sims = []
+        for p, sc in mix:
+            sim = Sim()
+            sim.set_stream(stream.cuda_stream)
+            sim.reset_scene(p, sc)
+            sims.append(sim)
+        for _ in range(frames):
+            for sim in sims:
+                sim.step(1 / 60)
+        torch.cuda.synchronize()
+        for sim in sims:
+            sim.close()
+    print(json.dumps({"only_mix": form, "frames": frames, "scenes": len(mix),
+                      "wall_s": time.perf_counter() - t0}), flush=True)
+    return 0
+
+
+def batched_mix_bench(frames, warmup):
+    """The 96-scene mix stepped (a) as one batch (one launch per pass for all
+    scenes, CUDA-graph frames) and (b) as the plain per-scene loop (96 Sim handles
+    on the same stream, one after the other). Device time per frame from CUDA
+    events; particle-substeps/s for both."""
+    import torch
+    from particles4all_b200 import Batch, Sim, configs
+    mix = configs.batched_mix()
+    total = sum(sc["pos"].shape[0] for _, sc in mix)
+    stream = torch.cuda.Stream()
+    b = Batch(**mix_arenas(mix))
     b.set_stream(stream.cuda_stream)
     t0 = time.perf_counter()
     ids = [b.add_scene(p, sc) for p, sc in mix]
@@ -554,6 +594,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.only_mix:
+        return only_mix(args.only_mix, args.mix_frames)
     return run_ours(args)
 
 

@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(TB, MB) k_delta_b(const __grid_constant__ Batc
 using PlainFn = void (*)(SimParams, DevScene, int);
 using BatchFn = void (*)(BatchWork, DevScene, int);
 #define P4A_SHAPES(K, suffix)                                                                        \
-  {K##suffix<256, 4>, K##suffix<256, 5>, K##suffix<256, 3>, K##suffix<128, 8>, K##suffix<128, 10>, \
-   K##suffix<128, 6>}
+  {K##suffix<256, 4>, K##suffix<256, 5>, K##suffix<256, 6>, K##suffix<128, 8>, K##suffix<128, 10>, \
+   K##suffix<128, 12>}
 #define P4A_SHAPES_D(K, suffix)                                                                      \
   {K##suffix<256, 5>, K##suffix<256, 4>, K##suffix<256, 6>, K##suffix<128, 10>, K##suffix<128, 8>, \
    K##suffix<128, 12>}

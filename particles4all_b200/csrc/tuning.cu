@@ -19,7 +19,7 @@
 namespace p4a {
 
 const LaunchShape kShapes[TK_COUNT][kVariants] = {
-    {{256, 4}, {256, 5}, {256, 3}, {128, 8}, {128, 10}, {128, 6}},    // lambda
+    {{256, 4}, {256, 5}, {256, 6}, {128, 8}, {128, 10}, {128, 12}},   // lambda
     {{256, 5}, {256, 4}, {256, 6}, {128, 10}, {128, 8}, {128, 12}},   // delta
     {{256, 4}, {256, 5}, {256, 3}, {128, 8}, {128, 10}, {128, 6}},    // xsph + normals
     {{128, 10}, {128, 8}, {128, 12}, {256, 5}, {256, 4}, {64, 20}},   // aniso
