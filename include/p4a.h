@@ -300,6 +300,71 @@ int p4a_default_mesh_params(p4a_mesh_params* out);
 int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
 int p4a_mesh_get_info(p4a_sim* s, p4a_mesh_info* out);
 
+/* ---- screen-space fluid rendering (src/ssfr.js:7-356) ------------------- */
+/*
+ * FluidSSFR.render on the simulation's live buffers into headless device images:
+ * ellipsoid depth splats of the anisotropic pass's smoothPos / G (p4a_aniso must
+ * have run on the current particles), additive thickness splats, a separable
+ * Gaussian blur of the thickness, the depth filter passes, a body-depth trace,
+ * and the composite (refraction with absorption, Fresnel reflection, GGX sun
+ * highlight, sky / floor / rigid-body background, tone map) into an RGBA8 image
+ * of width x height. Field names follow FluidSSFR's members; matrices are
+ * column-major float[16] as the reference's Float32Array matrices (view, proj,
+ * invViewProj, invView of src/render.js:203-258). `bodies` is the rigid-body
+ * renderer's packed buffer (6 float4 per body: centre + shape code, half extents,
+ * three rotation rows, colour; src/ssfr_composite_wgsl.js:67-84), or NULL with
+ * body_count 0. Environment maps are not supported (hasEnvMap = 0).
+ * Depth ties keep the lower particle index (the first drawn); the thickness is
+ * summed in fixed point, so every buffer is the same bits on every run.
+ */
+typedef struct p4a_ssfr_params {
+  float view[16], proj[16], inv_view_proj[16], inv_view[16];
+  float eye[3];
+  int32_t width, height;          /* target size in pixels                          */
+  double render_scale;            /* renderScale, 1.0 (maps: round(width x scale)) */
+  double splat_radius;            /* splatRadius, 1.0                              */
+  double thickness_radius;        /* thicknessRadius, 0.62 (x spacing)             */
+  double thickness_scale;         /* thicknessScale, 3.0                           */
+  int32_t thickness_filter_size;  /* thicknessFilterSize, 8 (<= 128)               */
+  int32_t thickness_half_res;     /* thicknessHalfRes, 1                           */
+  int32_t filter;                 /* 0 Gaussian, 1 bilateral, 2 narrow range (2)   */
+  int32_t filter_iterations;      /* filterIterations, 2                           */
+  int32_t cleanup_pass;           /* cleanupPass, 1                                */
+  int32_t cleanup_radius;         /* cleanupRadius, 4                              */
+  int32_t filter_max_radius;      /* filterMaxRadius, 32                           */
+  int32_t depth_cull_neighbours;  /* depthCullNeighbours, 0                        */
+  double filter_sigma;            /* filterSigma, 0.7                              */
+  double narrow_delta;            /* narrowDelta, 10.0                             */
+  double narrow_mu;               /* narrowMu, 1.0                                 */
+  double bilateral_range;         /* bilateralRange, 2.0                           */
+  double ior;                     /* 1.333                                         */
+  double absorption;              /* 1.0                                           */
+  double transmit[3];             /* 0.35, 0.62, 0.78                              */
+  double roughness;               /* 0.055                                         */
+  double sun_intensity;           /* 3.0                                           */
+  double sun_elevation;           /* 38 degrees                                    */
+  double sun_azimuth;             /* 40 degrees                                    */
+  double exposure;                /* 1.0                                           */
+  double ground_reflection;       /* 0.0                                           */
+  int32_t floor_plane;            /* 1                                             */
+  int32_t debug;                  /* 0 shaded, 1 normals, 2 depth, 3 thickness,
+                                     4 unfiltered depth, 5 body depth              */
+} p4a_ssfr_params;
+typedef struct p4a_ssfr_info {
+  int32_t width, height;          /* image                                         */
+  int32_t map_w, map_h;           /* depth maps (render scale)                     */
+  int32_t thick_w, thick_h;       /* thickness map                                 */
+  int32_t ssfr_gen;               /* increments when the buffers are reallocated   */
+} p4a_ssfr_info;
+enum { P4A_SSFR_EYEZ = 0, P4A_SSFR_RAWZ = 1, P4A_SSFR_THICK = 2, P4A_SSFR_IMAGE = 3, P4A_SSFR_BODYT = 4 };
+int p4a_default_ssfr_params(p4a_ssfr_params* out);
+int p4a_ssfr(p4a_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t body_count);
+int p4a_ssfr_get_info(p4a_sim* s, p4a_ssfr_info* out);
+/* Device pointer and size of an SSFR buffer (float maps; the image is RGBA8). */
+int p4a_ssfr_buffer(p4a_sim* s, int32_t which, void** dptr, size_t* bytes);
+/* Copies the first `bytes` of an SSFR buffer to host memory (waits for the stream). */
+int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes);
+
 /* ---- batched multi-scene stepping -------------------------------------- */
 /*
  * Extension, no counterpart in the reference (which steps one scene per Sim).

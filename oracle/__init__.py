@@ -50,12 +50,16 @@ def lib():
             "orc_build_scene": [vp, vp, vp, vp, vp, vp, vp, vp],
             "orc_boundary": [vp, dbl, dbl, C.POINTER(i32), vp, vp],
             "orc_grid_sort": [vp, i32, C.c_float, C.c_float] + [vp] * 11,
+            "orc_ssfr": [vp, vp, vp, i32], "orc_ssfr_buffer": [vp, i32, C.POINTER(vp), C.POINTER(C.c_size_t)],
         }.items():
             f = getattr(L, name)
             f.argtypes = args
             f.restype = C.c_int
         L.orc_cbrt_newton.argtypes = [C.c_float]
         L.orc_cbrt_newton.restype = C.c_float
+        for name in ("orc_expf", "orc_logf"):
+            getattr(L, name).argtypes = [C.c_float]
+            getattr(L, name).restype = C.c_float
         _lib = L
     return _lib
 
@@ -189,6 +193,34 @@ class OracleSim:
         t = C.c_int64()
         _check(self._L.orc_mesh(self._h, C.byref(m), C.byref(t)), "mesh")
         return t.value
+
+    def ssfr(self, sparams, bodies=None):
+        """FluidSSFR.render restated on the CPU (same parameters as Sim.ssfr)."""
+        from particles4all_b200.params import ssfr_struct
+        sp = ssfr_struct(sparams)
+        self._ssfr_dims = None
+        if bodies is None or len(bodies) == 0:
+            ptr, count, self._keep_bodies = None, 0, None
+        else:
+            self._keep_bodies = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 24)
+            ptr, count = self._keep_bodies.ctypes.data, self._keep_bodies.shape[0]
+        _check(self._L.orc_ssfr(self._h, C.byref(sp), ptr, count), "ssfr")
+        rs = min(1.0, max(0.25, sp.render_scale))
+        w, h = max(1, int(np.floor(sp.width * rs + 0.5))), max(1, int(np.floor(sp.height * rs + 0.5)))
+        half = sp.thickness_half_res and sp.thickness_filter_size >= 4
+        self._ssfr_dims = {"width": sp.width, "height": sp.height, "map_w": w, "map_h": h,
+                           "thick_w": (w + 1) >> 1 if half else w, "thick_h": (h + 1) >> 1 if half else h}
+
+    def ssfr_read(self, name):
+        p, nb = C.c_void_p(), C.c_size_t()
+        _check(self._L.orc_ssfr_buffer(self._h, _abi.SSFR_BUF[name], C.byref(p), C.byref(nb)), "ssfr_buffer")
+        raw = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), (nb.value,)).copy() if nb.value else \
+            np.zeros(0, np.uint8)
+        dm = self._ssfr_dims
+        if name == "image":
+            return raw.reshape(dm["height"], dm["width"], 4)
+        w, h = (dm["thick_w"], dm["thick_h"]) if name == "thick" else (dm["map_w"], dm["map_h"])
+        return raw.view(np.float32).reshape(h, w)
 
     def info(self):
         i = _abi.Info()

@@ -450,6 +450,9 @@ struct orc_sim {
   p4a_stats stats{};
   std::vector<f4> smoothPos, anisoG;
   int anisoGen = 0;
+  std::vector<float> ssfrEyeZ, ssfrRaw, ssfrThick, ssfrBodyT;
+  std::vector<uint32_t> ssfrImage;
+  int ssfrDims[6] = {0, 0, 0, 0, 0, 0};
   std::vector<float> meshField, meshNField;
   std::vector<uint32_t> meshVerts;  // 2 words per vertex
   int64_t meshTris = 0;
@@ -1823,5 +1826,671 @@ int orc_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, cons
   std::memcpy(cell_start, cs.data(), (P.nCells + 1) * 4);
   return P4A_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Screen-space fluid rendering (src/ssfr.js:173-356, src/ssfr_wgsl.js,
+// src/ssfr_composite_wgsl.js). Rasterisation is restated as the pipeline
+// defines it: instances drawn in order, each quad covering the pixels whose
+// centres lie inside it, the depth test 'less' against 1.0 applied fragment by
+// fragment in draw order, the thickness blended additively (summed in 2^-32 fixed
+// point: the sum does not depend on order). Matrices column-major; M * v as nested
+// fma over columns; dot() as dot3; exp/log by Cody-Waite reduction + Taylor and
+// the atanh series (own restatement, see orc_exp / orc_log).
+namespace {
+
+struct v4o { float x, y, z, w; };
+inline v4o mv4(const float* m, v4o v) {
+  return {std::fmaf(m[12], v.w, std::fmaf(m[8], v.z, std::fmaf(m[4], v.y, m[0] * v.x))),
+          std::fmaf(m[13], v.w, std::fmaf(m[9], v.z, std::fmaf(m[5], v.y, m[1] * v.x))),
+          std::fmaf(m[14], v.w, std::fmaf(m[10], v.z, std::fmaf(m[6], v.y, m[2] * v.x))),
+          std::fmaf(m[15], v.w, std::fmaf(m[11], v.z, std::fmaf(m[7], v.y, m[3] * v.x)))};
+}
+inline f3 mv3(const m3& m, f3 v) { return {dot3(row3(m, 0), v), dot3(row3(m, 1), v), dot3(row3(m, 2), v)}; }
+inline f3 nrm3(f3 a) { const float l = std::sqrt(dot3(a, a)); return {a.x / l, a.y / l, a.z / l}; }
+inline float clampo(float x, float lo, float hi) { return std::fmin(std::fmax(x, lo), hi); }
+inline float sstep(float e0, float e1, float x) {
+  const float t = clampo((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+inline f3 mixo(f3 a, f3 b, float t) {
+  const float u = 1.0f - t;
+  return {a.x * u + b.x * t, a.y * u + b.y * t, a.z * u + b.z * t};
+}
+inline f3 refl(f3 i, f3 n) { const float d = 2.0f * dot3(n, i); return {i.x - d * n.x, i.y - d * n.y, i.z - d * n.z}; }
+inline f3 refr(f3 i, f3 n, float eta) {
+  const float ni = dot3(n, i);
+  const float k = 1.0f - eta * eta * (1.0f - ni * ni);
+  if (k < 0.0f) return {0, 0, 0};
+  const float a = eta * ni + std::sqrt(k);
+  return {eta * i.x - a * n.x, eta * i.y - a * n.y, eta * i.z - a * n.z};
+}
+inline float frac1(float x) { return x - std::floor(x); }
+
+float o_bits(uint32_t b) { float f; std::memcpy(&f, &b, 4); return f; }
+uint32_t o_ubits(float f) { uint32_t b; std::memcpy(&b, &f, 4); return b; }
+float o_scale2(float x, int k) {
+  while (k > 127) { x = x * 1.7014118346046923e38f; k -= 127; }
+  while (k < -126) { x = x * 1.1754943508222875e-38f; k += 126; }
+  return x * o_bits((uint32_t)(k + 127) << 23);
+}
+// e^x: x = k ln2 + r (ln2 = 0.693145751953125 + 1.4286067653e-6), e^r by its Taylor
+// series to r^8 in Horner form, times 2^k.
+float orc_exp(float x) {
+  if (x != x) return x;
+  if (x > 88.72283935546875f) return INFINITY;
+  if (x < -103.97208404541016f) return 0.0f;
+  const float k = std::rint(x * 1.44269502162933349609375f);
+  float r = std::fmaf(-k, 0.693145751953125f, x);
+  r = std::fmaf(-k, 1.428606765330187045e-6f, r);
+  float p = 2.48015873015873e-5f;
+  p = std::fmaf(p, r, 1.984126984126984e-4f);
+  p = std::fmaf(p, r, 1.388888888888889e-3f);
+  p = std::fmaf(p, r, 8.333333333333333e-3f);
+  p = std::fmaf(p, r, 4.166666666666667e-2f);
+  p = std::fmaf(p, r, 1.666666666666667e-1f);
+  p = std::fmaf(p, r, 0.5f);
+  p = std::fmaf(p, r, 1.0f);
+  p = std::fmaf(p, r, 1.0f);
+  return o_scale2(p, (int)k);
+}
+// log x = e ln2 + 2 atanh((m - 1) / (m + 1)), m in [sqrt(1/2), sqrt(2)).
+float orc_log(float x) {
+  if (x != x || x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return x;
+  int e = 0;
+  if (x < 1.1754943508222875e-38f) { x = x * 16777216.0f; e = -24; }
+  const uint32_t b = o_ubits(x);
+  e += (int)((b >> 23) & 0xffu) - 127;
+  float m = o_bits((b & 0x7fffffu) | 0x3f800000u);
+  if (m > 1.41421353816986083984375f) { m = m * 0.5f; e += 1; }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float z = s * s;
+  float p = 0.15384615384615385f;
+  p = std::fmaf(p, z, 0.18181818181818182f);
+  p = std::fmaf(p, z, 0.22222222222222222f);
+  p = std::fmaf(p, z, 0.2857142857142857f);
+  p = std::fmaf(p, z, 0.4f);
+  p = std::fmaf(p, z, 0.6666666666666666f);
+  p = std::fmaf(p, z, 2.0f);
+  const float fe = (float)e;
+  return std::fmaf(fe, 0.693145751953125f, std::fmaf(s, p, fe * 1.428606765330187045e-6f));
+}
+float orc_pow(float x, float y) {
+  if (x > 0.0f) return orc_exp(y * orc_log(x));
+  if (x == 0.0f) return y > 0.0f ? 0.0f : (y == 0.0f ? 1.0f : INFINITY);
+  return NAN;
+}
+
+struct OSplat {
+  const float *view, *proj, *ivp;
+  float pv[16];
+  float vw, vh, kernelScale, quadRadius, thickRadius, maxNeighbours;
+  bool skipBodies;
+};
+m3 o_kernel_g(const std::vector<f4>& g, size_t i) {
+  const f4 a = g[i * 2], b = g[i * 2 + 1];
+  m3 m;
+  m.c[0] = {a.x, a.y, a.z};
+  m.c[1] = {a.y, a.w, b.x};
+  m.c[2] = {a.z, b.x, b.y};
+  return m;
+}
+m3 o_kernel_inverse(const std::vector<f4>& gd, size_t i) {
+  const m3 m = o_kernel_g(gd, i);
+  const float a = elc(m, 0, 0), b = elc(m, 1, 0), c = elc(m, 2, 0);
+  const float d = elc(m, 0, 1), e = elc(m, 1, 1), f = elc(m, 2, 1);
+  const float g = elc(m, 0, 2), h = elc(m, 1, 2), k = elc(m, 2, 2);
+  const float A = e * k - f * h, B = f * g - d * k, C = d * h - e * g;
+  const float det = a * A + b * B + c * C;
+  const float inv = 1.0f / (std::fabs(det) < 1.0e-20f ? 1.0e-20f : det);
+  m3 o;
+  o.c[0] = {A * inv, B * inv, C * inv};
+  o.c[1] = {(c * h - b * k) * inv, (a * k - c * g) * inv, (b * g - a * h) * inv};
+  o.c[2] = {(b * f - c * e) * inv, (c * d - a * f) * inv, (a * e - b * d) * inv};
+  return o;
+}
+// vertex shader (src/ssfr_wgsl.js:48-83) + rasteriser coverage
+bool o_quad(const OSplat& S, const orc_sim* s, size_t ii, int& x0, int& x1, int& y0, int& y1) {
+  const f4 c = s->smoothPos[ii];
+  if (S.skipBodies && s->body[s->parity][ii].x != 0u) return false;
+  if (S.maxNeighbours > 0.0f && s->anisoG[ii * 2 + 1].w > S.maxNeighbours) return false;
+  const v4o ec = mv4(S.view, {c.x, c.y, c.z, 1.0f});
+  const float zeye = std::fmax(-ec.z, 1.0e-4f);
+  const v4o clip = mv4(S.proj, ec);
+  f3 e;
+  if (S.quadRadius > 0.0f) {
+    e = {S.quadRadius, S.quadRadius, S.quadRadius};
+  } else {
+    m3 v3;
+    for (int cc = 0; cc < 3; cc++) v3.c[cc] = {S.view[cc * 4], S.view[cc * 4 + 1], S.view[cc * 4 + 2]};
+    const m3 M = matmul(v3, scale3(o_kernel_inverse(s->anisoG, ii), S.kernelScale));
+    e = {length3(row3(M, 0)), length3(row3(M, 1)), length3(row3(M, 2))};
+  }
+  const float znear = std::fmax(zeye - e.z, 1.0e-4f);
+  const float hx = S.proj[0] * e.x / znear, hy = S.proj[5] * e.y / znear;
+  if (!(clip.w > 0.0f) || clip.z < 0.0f || clip.z > clip.w) return false;
+  const float lx = clip.x - hx * clip.w, rx = clip.x + hx * clip.w;
+  const float ty = clip.y + hy * clip.w, by = clip.y - hy * clip.w;
+  const float fx0 = (lx / clip.w * 0.5f + 0.5f) * S.vw, fx1 = (rx / clip.w * 0.5f + 0.5f) * S.vw;
+  const float fy0 = (0.5f - ty / clip.w * 0.5f) * S.vh, fy1 = (0.5f - by / clip.w * 0.5f) * S.vh;
+  const float a0 = std::fmax(std::ceil(fx0 - 0.5f), 0.0f), a1 = std::fmin(std::ceil(fx1 - 0.5f), S.vw);
+  const float b0 = std::fmax(std::ceil(fy0 - 0.5f), 0.0f), b1 = std::fmin(std::ceil(fy1 - 0.5f), S.vh);
+  if (!(a0 < a1) || !(b0 < b1)) return false;
+  x0 = (int)a0; x1 = (int)a1; y0 = (int)b0; y1 = (int)b1;
+  return true;
+}
+void o_ray(const float* ivp, float nx, float ny, f3& ro, f3& rd) {
+  const v4o nh = mv4(ivp, {nx, ny, -1.0f, 1.0f});
+  const v4o fh = mv4(ivp, {nx, ny, 1.0f, 1.0f});
+  ro = {nh.x / nh.w, nh.y / nh.w, nh.z / nh.w};
+  rd = nrm3(sub3({fh.x / fh.w, fh.y / fh.w, fh.z / fh.w}, ro));
+}
+void o_frag_ray(const OSplat& S, int px, int py, f3& ro, f3& rd) {
+  const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+  o_ray(S.ivp, fx / S.vw * 2.0f - 1.0f, 1.0f - fy / S.vh * 2.0f, ro, rd);
+}
+// depthFS (src/ssfr_wgsl.js:85-108, 122-139)
+bool o_depth_frag(const OSplat& S, const orc_sim* s, size_t ii, int px, int py, float& depth, float& eyeZ) {
+  const f4 c4 = s->smoothPos[ii];
+  const f3 centre = {c4.x, c4.y, c4.z};
+  f3 ro, rd;
+  o_frag_ray(S, px, py, ro, rd);
+  const m3 G = scale3(o_kernel_g(s->anisoG, ii), 1.0f / S.kernelScale);
+  const f3 oc = sub3(ro, centre);
+  const f3 ga = mv3(G, rd), gb = mv3(G, oc);
+  const float A = dot3(ga, ga), B = 2.0f * dot3(ga, gb), C = dot3(gb, gb) - 1.0f;
+  const float disc = B * B - 4.0f * A * C;
+  if (disc <= 0.0f || A <= 0.0f) return false;
+  const float sq = std::sqrt(disc);
+  const float t = (-B - sq) / (2.0f * A);
+  if (!(t > 0.0f)) return false;
+  const f3 p = {ro.x + rd.x * t, ro.y + rd.y * t, ro.z + rd.z * t};
+  const v4o ve = mv4(S.view, {p.x, p.y, p.z, 1.0f});
+  const v4o cl = mv4(S.pv, {p.x, p.y, p.z, 1.0f});
+  depth = clampo(cl.z / cl.w, 0.0f, 1.0f);
+  eyeZ = ve.z;
+  return true;
+}
+float o_fetch(const std::vector<float>& z, int x, int y, int w, int h) {
+  if (x < 0 || y < 0 || x >= w || y >= h) return -1.0e4f;
+  return z[(size_t)y * w + x];
+}
+void o_nr(float& z, float& w, float& wo, float& up, float& lo, float lowerClamp, float thr) {
+  if (z > up) { w = 0.0f; wo = 0.0f; }
+  else if (z < lo) { z = lowerClamp; }
+  else { up = std::fmax(up, z + thr); lo = std::fmin(lo, z - thr); }
+}
+struct OFilt { int dirX, dirY, maxRadius, mode, clean, cleanRadius; float sigmaWorld, proj11, viewH, delta, mu, rangeSigma; };
+void o_filter(const OFilt& F, const std::vector<float>& in, std::vector<float>& out, int W, int H) {
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int py = 0; py < H; py++)
+    for (int px = 0; px < W; px++) {
+      const float zi = in[(size_t)py * W + px];
+      if (zi < -1.0e3f) { out[(size_t)py * W + px] = zi; continue; }
+      const float sigma = std::fmax(F.sigmaWorld * F.viewH * F.proj11 / (2.0f * std::fabs(zi)), 0.5f);
+      int R = (int)std::fmin(3.0f * sigma, (float)F.maxRadius);
+      if (F.clean) R = F.cleanRadius;
+      float sg = sigma;
+      if (F.clean) sg = std::fmax((float)R / 3.0f, 1.0e-3f);
+      const float inv2s2 = 1.0f / (2.0f * sg * sg);
+      float upP = zi + F.delta, loP = zi - F.delta, upM = zi + F.delta, loM = zi - F.delta;
+      const float lc = zi - F.mu;
+      float sum = zi, wsum = 1.0f;
+      if (F.clean) {
+        float up = zi + F.delta, lo = zi - F.delta;
+        for (int dy = 1; dy <= R; dy++)
+          for (int dx = 1; dx <= R; dx++) {
+            const float g = orc_exp(-(float)(dx * dx + dy * dy) * inv2s2);
+            float za = o_fetch(in, px + dx, py + dy, W, H), zb = o_fetch(in, px + dx, py - dy, W, H);
+            float zc = o_fetch(in, px - dx, py + dy, W, H), zd = o_fetch(in, px - dx, py - dy, W, H);
+            float wa = g, wb = g, wc = g, wd = g;
+            o_nr(za, wa, wd, up, lo, lc, F.delta);
+            o_nr(zb, wb, wc, up, lo, lc, F.delta);
+            o_nr(zc, wc, wb, up, lo, lc, F.delta);
+            o_nr(zd, wd, wa, up, lo, lc, F.delta);
+            sum = sum + za * wa + zb * wb + zc * wc + zd * wd;
+            wsum = wsum + wa + wb + wc + wd;
+          }
+        for (int t = 1; t <= R; t++) {
+          const float g = orc_exp(-(float)(t * t) * inv2s2);
+          float zv[4] = {o_fetch(in, px + t, py, W, H), o_fetch(in, px - t, py, W, H),
+                         o_fetch(in, px, py + t, W, H), o_fetch(in, px, py - t, W, H)};
+          float wv[4] = {g, g, g, g};
+          o_nr(zv[0], wv[0], wv[1], up, lo, lc, F.delta);
+          o_nr(zv[1], wv[1], wv[0], up, lo, lc, F.delta);
+          o_nr(zv[2], wv[2], wv[3], up, lo, lc, F.delta);
+          o_nr(zv[3], wv[3], wv[2], up, lo, lc, F.delta);
+          for (int k = 0; k < 4; k++) { sum = sum + zv[k] * wv[k]; wsum = wsum + wv[k]; }
+        }
+      } else {
+        for (int t = 1; t <= R; t++) {
+          float zj = o_fetch(in, px + F.dirX * t, py + F.dirY * t, W, H);
+          float zk = o_fetch(in, px - F.dirX * t, py - F.dirY * t, W, H);
+          const float g = orc_exp(-(float)(t * t) * inv2s2);
+          float wj = g, wk = g;
+          if (F.mode == 2) {
+            o_nr(zj, wj, wk, upP, loP, lc, F.delta);
+            o_nr(zk, wk, wj, upM, loM, lc, F.delta);
+            sum = sum + zj * wj + zk * wk;
+            wsum = wsum + wj + wk;
+          } else {
+            if (!(zj < -1.0e3f)) {
+              float w = g;
+              if (F.mode == 1) { const float dz = zj - zi; w = w * orc_exp(-dz * dz / (2.0f * F.rangeSigma * F.rangeSigma)); }
+              sum = sum + w * zj; wsum = wsum + w;
+            }
+            if (!(zk < -1.0e3f)) {
+              float w = g;
+              if (F.mode == 1) { const float dz = zk - zi; w = w * orc_exp(-dz * dz / (2.0f * F.rangeSigma * F.rangeSigma)); }
+              sum = sum + w * zk; wsum = wsum + w;
+            }
+          }
+        }
+      }
+      out[(size_t)py * W + px] = sum / wsum;
+    }
+}
+
+// composite (src/ssfr_composite_wgsl.js)
+struct OComp {
+  const float *ivp, *iv;
+  f3 boxMin, absorb, sunDir;
+  float proj00, proj11, ior, sunIntensity, roughness, exposure, groundReflection, thicknessScale;
+  int bodyCount, floorPlane, debug;
+  const float* bdata;  // 24 floats per body
+};
+f3 o_bd(const OComp& C, int k) { return {C.bdata[k * 4], C.bdata[k * 4 + 1], C.bdata[k * 4 + 2]}; }
+float o_body_dist(const OComp& C, int i, f3 p) {
+  const int b = i * 6;
+  const f3 centre = o_bd(C, b);
+  const int shape = (int)(C.bdata[b * 4 + 3] + 0.5f);
+  const f3 h = o_bd(C, b + 1);
+  const f3 d0 = sub3(p, centre);
+  const f3 q = {dot3(o_bd(C, b + 2), d0), dot3(o_bd(C, b + 3), d0), dot3(o_bd(C, b + 4), d0)};
+  if (shape == 1) return length3(q) - h.x;
+  if (shape == 2) {
+    const float tx = std::sqrt(std::fmaf(q.z, q.z, q.x * q.x)) - h.x, ty = q.y;
+    return std::sqrt(std::fmaf(ty, ty, tx * tx)) - h.y;
+  }
+  const f3 d = {std::fabs(q.x) - h.x, std::fabs(q.y) - h.y, std::fabs(q.z) - h.z};
+  return length3({std::fmax(d.x, 0.0f), std::fmax(d.y, 0.0f), std::fmax(d.z, 0.0f)}) +
+         std::fmin(std::fmax(d.x, std::fmax(d.y, d.z)), 0.0f);
+}
+struct OTrace { float t; f3 nrm, col; };
+OTrace o_trace(const OComp& C, f3 ro, f3 rd, float tMax) {
+  OTrace o{-1.0f, {0, 1, 0}, {0.8f, 0.8f, 0.8f}};
+  if (C.bodyCount == 0) return o;
+  float t = 1.0e-4f;
+  for (int it = 0; it < 128; it++) {
+    const f3 p = {ro.x + rd.x * t, ro.y + rd.y * t, ro.z + rd.z * t};
+    float dist = 1.0e30f;
+    int id = -1;
+    for (int i = 0; i < C.bodyCount; i++) {
+      const float d = o_body_dist(C, i, p);
+      if (d < dist) { dist = d; id = i; }
+    }
+    if (dist < 5.0e-5f) {
+      const float e = 2.0e-4f;
+      o.nrm = nrm3({o_body_dist(C, id, {p.x + e, p.y, p.z}) - o_body_dist(C, id, {p.x - e, p.y, p.z}),
+                    o_body_dist(C, id, {p.x, p.y + e, p.z}) - o_body_dist(C, id, {p.x, p.y - e, p.z}),
+                    o_body_dist(C, id, {p.x, p.y, p.z + e}) - o_body_dist(C, id, {p.x, p.y, p.z - e})});
+      o.col = o_bd(C, id * 6 + 5);
+      o.t = t;
+      return o;
+    }
+    t += std::fmax(dist, 1.0e-4f);
+    if (t > tMax) break;
+  }
+  return o;
+}
+const f3 kHazeO = {0.62f, 0.74f, 0.90f};
+f3 o_sky(const OComp& C, f3 d) {
+  const float h = clampo(d.y, 0.0f, 1.0f);
+  f3 c = mixo(kHazeO, {0.25f, 0.48f, 0.85f}, sstep(0.0f, 0.16f, h));
+  c = mixo(c, {0.09f, 0.28f, 0.72f}, sstep(0.10f, 0.85f, h));
+  const float s = std::fmax(dot3(d, C.sunDir), 0.0f);
+  const float p1 = orc_pow(s, 3000.0f), p2 = orc_pow(s, 24.0f);
+  c = {c.x + 1.00f * p1 * 14.0f, c.y + 0.96f * p1 * 14.0f, c.z + 0.88f * p1 * 14.0f};
+  c = {c.x + 1.00f * p2 * 0.20f, c.y + 0.92f * p2 * 0.20f, c.z + 0.78f * p2 * 0.20f};
+  return c;
+}
+f3 o_floor(f3 p) {
+  const float gx = std::fabs(frac1(p.x) - 0.5f), gz = std::fabs(frac1(p.z) - 0.5f);
+  const float line = 1.0f - sstep(0.0f, 0.015f, std::fmin(gx, gz));
+  f3 c = mixo({0.30f, 0.305f, 0.315f}, {0.50f, 0.51f, 0.52f}, line * 0.8f);
+  const float fs = std::floor(p.x) + std::floor(p.z);
+  const float chk = fs - 2.0f * std::floor(fs * 0.5f);
+  const float m = 0.88f * (1.0f - chk) + 1.10f * chk;
+  return {c.x * m, c.y * m, c.z * m};
+}
+f3 o_background(const OComp& C, f3 o, f3 d) {
+  if (C.floorPlane != 0 && d.y < -1.0e-4f) {
+    const float t = (C.boxMin.y - o.y) / d.y;
+    if (t > 0.0f) {
+      const f3 p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
+      const float fade = 1.0f - orc_exp(-0.02f * t);
+      return mixo(o_floor(p), kHazeO, fade);
+    }
+  }
+  return o_sky(C, d);
+}
+f3 o_shade_body(const OComp& C, f3 n, f3 base, f3 rd, f3 env) {
+  const float ndl = std::fmax(dot3(n, C.sunDir), 0.0f);
+  const f3 h = nrm3(sub3(C.sunDir, rd));
+  const float spec = orc_pow(std::fmax(dot3(n, h), 0.0f), 60.0f);
+  const float fres = orc_pow(1.0f - std::fmax(dot3({-rd.x, -rd.y, -rd.z}, n), 0.0f), 4.0f);
+  const float k = 0.22f + 0.78f * ndl;
+  return {base.x * k + 0.7f * spec + env.x * fres * 0.25f, base.y * k + 0.7f * spec + env.y * fres * 0.25f,
+          base.z * k + 0.7f * spec + env.z * fres * 0.25f};
+}
+f3 o_env_reflect(const OComp& C, f3 d) {
+  if (d.y >= 0.0f) return o_sky(C, d);
+  return mixo(kHazeO, {0.32f, 0.325f, 0.335f}, clampo(-d.y * 4.0f, 0.0f, 1.0f));
+}
+f3 o_water_reflect(const OComp& C, f3 d, f3 n) {
+  const f3 physical = o_env_reflect(C, d);
+  if (d.y >= 0.0f || C.groundReflection >= 1.0f) return physical;
+  const float top = sstep(0.819152f, 0.939693f, n.y);
+  const float below = sstep(0.0f, 0.10f, -d.y);
+  const float suppress = (1.0f - clampo(C.groundReflection, 0.0f, 1.0f)) * top * below;
+  const float xzl = std::fmax(std::sqrt(std::fmaf(d.z, d.z, d.x * d.x)), 1.0e-4f);
+  return mixo(physical, o_sky(C, {d.x / xzl, 0.0f, d.z / xzl}), suppress);
+}
+f3 o_scene_color(const OComp& C, f3 o, f3 d) {
+  const OTrace b = o_trace(C, o, d, 60.0f);
+  if (b.t < 0.0f) return o_background(C, o, d);
+  const f3 p = {o.x + d.x * b.t, o.y + d.y * b.t, o.z + d.z * b.t};
+  const f3 po = {p.x + b.nrm.x * 1.0e-4f, p.y + b.nrm.y * 1.0e-4f, p.z + b.nrm.z * 1.0e-4f};
+  return o_shade_body(C, b.nrm, b.col, d, o_background(C, po, refl(d, b.nrm)));
+}
+float o_fresnel(float cosI, float n1, float n2) {
+  const float eta = n1 / n2;
+  const float sinT2 = eta * eta * (1.0f - cosI * cosI);
+  if (sinT2 >= 1.0f) return 1.0f;
+  const float cosT = std::sqrt(1.0f - sinT2);
+  const float rs = (n1 * cosI - n2 * cosT) / (n1 * cosI + n2 * cosT);
+  const float rp = (n1 * cosT - n2 * cosI) / (n1 * cosT + n2 * cosI);
+  return clampo(0.5f * (rs * rs + rp * rp), 0.0f, 1.0f);
+}
+float o_ggx(f3 n, f3 v, f3 l, float rough) {
+  const float a = std::fmax(rough * rough, 1.0e-4f);
+  const f3 h = nrm3(add3(l, v));
+  const float ndh = std::fmax(dot3(n, h), 0.0f), ndl = std::fmax(dot3(n, l), 0.0f), ndv = std::fmax(dot3(n, v), 0.0f);
+  const float a2 = a * a;
+  const float d = ndh * ndh * (a2 - 1.0f) + 1.0f;
+  const float ndf = a2 / std::fmax(3.14159265f * d * d, 1.0e-7f);
+  const float k = a * 0.5f;
+  const float gl = ndl / std::fmax(ndl * (1.0f - k) + k, 1.0e-5f);
+  const float gv = ndv / std::fmax(ndv * (1.0f - k) + k, 1.0e-5f);
+  return ndf * gl * gv * ndl / std::fmax(4.0f * ndl * ndv, 1.0e-4f);
+}
+f3 o_tonemap(const OComp& C, f3 c) {
+  f3 col = {c.x * C.exposure, c.y * C.exposure, c.z * C.exposure};
+  const float m = 1.0f + std::fmax(std::fmax(col.x, col.y), col.z) * 0.35f;
+  col = {col.x / m, col.y / m, col.z / m};
+  const float g = (float)(1.0 / 2.2);
+  return {orc_pow(col.x, g), orc_pow(col.y, g), orc_pow(col.z, g)};
+}
+uint32_t o_rgba8(f3 c) {
+  auto u = [](float v) { return (uint32_t)(int)std::floor(clampo(v, 0.0f, 1.0f) * 255.0f + 0.5f); };
+  return u(c.x) | (u(c.y) << 8) | (u(c.z) << 16) | (255u << 24);
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_ssfr(orc_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t bodyCount) {
+  if (!s || !s->ready || !sp || sp->width < 1 || sp->height < 1 || bodyCount < 0 || (bodyCount > 0 && !bodies))
+    return P4A_ERR_ARG;
+  if (s->smoothPos.size() < (size_t)s->n) return P4A_ERR_STATE;
+  const p4a_ssfr_params& q = *sp;
+  apply_threads();
+  const double rs = std::min(1.0, std::max(0.25, q.render_scale));
+  const int W = std::max(1, (int)std::floor(q.width * rs + 0.5)), H = std::max(1, (int)std::floor(q.height * rs + 0.5));
+  const bool half = q.thickness_half_res && q.thickness_filter_size >= 4;
+  const int TW = half ? (W + 1) >> 1 : W, TH = half ? (H + 1) >> 1 : H;
+  const double kPiD = 3.14159265358979323846;
+  const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
+  const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};
+  const double sl = std::sqrt(sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2]);
+  double absorb[3];
+  for (int k = 0; k < 3; k++) absorb[k] = q.absorption * -std::log(std::min(1.0, std::max(1e-3, q.transmit[k])));
+  const double spacing = s->params.spacing, support = s->h;
+  const double r = 0.5 * spacing;
+  const float scale = (float)(q.splat_radius * spacing / support);
+  const float thickRadius = (float)(q.thickness_radius * spacing);
+  OSplat S0{q.view, q.proj, q.inv_view_proj, {}, (float)W, (float)H, scale, 0.0f, thickRadius,
+            (float)q.depth_cull_neighbours, s->nBodyParts > 0};
+  for (int c = 0; c < 4; c++)
+    for (int rr = 0; rr < 4; rr++)
+      S0.pv[c * 4 + rr] = std::fmaf(q.proj[12 + rr], q.view[c * 4 + 3],
+                                    std::fmaf(q.proj[8 + rr], q.view[c * 4 + 2],
+                                              std::fmaf(q.proj[4 + rr], q.view[c * 4 + 1], q.proj[rr] * q.view[c * 4])));
+  OSplat S1 = S0;
+  S1.vw = (float)TW;
+  S1.vh = (float)TH;
+  S1.quadRadius = thickRadius;
+  S1.maxNeighbours = 0.0f;
+  const int n = s->n;
+  // depth: instances in order, test 'less' per fragment against the cleared 1.0
+  std::vector<float> zbuf((size_t)W * H, 1.0f), eyeZ((size_t)W * H, -1.0e4f);
+  for (int ii = 0; ii < n; ii++) {
+    int x0, x1, y0, y1;
+    if (!o_quad(S0, s, (size_t)ii, x0, x1, y0, y1)) continue;
+    for (int py = y0; py < y1; py++)
+      for (int px = x0; px < x1; px++) {
+        float depth, ez;
+        if (!o_depth_frag(S0, s, (size_t)ii, px, py, depth, ez)) continue;
+        const size_t o = (size_t)py * W + px;
+        if (depth < zbuf[o]) { zbuf[o] = depth; eyeZ[o] = ez; }
+      }
+  }
+  s->ssfrRaw = eyeZ;
+  // thickness: additive, in 2^-32 fixed point
+  std::vector<uint64_t> acc((size_t)TW * TH, 0);
+  const float tr2 = thickRadius * thickRadius;
+  for (int ii = 0; ii < n; ii++) {
+    int x0, x1, y0, y1;
+    if (!o_quad(S1, s, (size_t)ii, x0, x1, y0, y1)) continue;
+    const f4 c4 = s->smoothPos[ii];
+    const f3 centre = {c4.x, c4.y, c4.z};
+    for (int py = y0; py < y1; py++)
+      for (int px = x0; px < x1; px++) {
+        f3 ro, rd;
+        o_frag_ray(S1, px, py, ro, rd);
+        const f3 oc = sub3(ro, centre);
+        const float b = dot3(oc, rd), c = dot3(oc, oc) - tr2;
+        const float disc = b * b - c;
+        if (disc <= 0.0f) continue;
+        const float chord = 2.0f * std::sqrt(disc);
+        acc[(size_t)py * TW + px] += (uint64_t)std::llrint(chord * 4294967296.0f);
+      }
+  }
+  std::vector<float> thick((size_t)TW * TH), tmp((size_t)TW * TH);
+  for (size_t i = 0; i < thick.size(); i++) thick[i] = (float)((double)acc[i] * (1.0 / 4294967296.0));
+  // thickness blur (src/ssfr_wgsl.js:155-183, src/ssfr.js:227-233)
+  if (q.thickness_filter_size > 0) {
+    const int size = TW < W ? std::max(1, q.thickness_filter_size >> 1) : q.thickness_filter_size;
+    const float sigma = std::fmax((float)size / 3.0f, 1.0e-3f);
+    const float two = 2.0f * sigma * sigma;
+    for (int p = 0; p < 2; p++) {
+      const int dx = p == 0 ? 1 : 0, dy = p == 0 ? 0 : 1;
+      const std::vector<float>& src = p == 0 ? thick : tmp;
+      std::vector<float>& dst = p == 0 ? tmp : thick;
+      for (int py = 0; py < TH; py++)
+        for (int px = 0; px < TW; px++) {
+          float sum = 0.0f, wsum = 0.0f;
+          for (int i = -size; i <= size; i++) {
+            const int x = std::min(std::max(px + dx * i, 0), TW - 1), y = std::min(std::max(py + dy * i, 0), TH - 1);
+            const float w = orc_exp(-(float)(i * i) / two);
+            sum = sum + src[(size_t)y * TW + x] * w;
+            wsum = wsum + w;
+          }
+          dst[(size_t)py * TW + px] = sum / wsum;
+        }
+    }
+  }
+  s->ssfrThick = thick;
+  // depth filter passes (src/ssfr.js:151-164, 331-338)
+  OFilt fl[3];
+  for (int k = 0; k < 3; k++) {
+    fl[k].dirX = k == 0 ? 1 : 0;
+    fl[k].dirY = k == 1 ? 1 : 0;
+    fl[k].maxRadius = q.filter_max_radius;
+    fl[k].mode = q.filter;
+    fl[k].clean = k == 2 ? 1 : 0;
+    fl[k].cleanRadius = q.cleanup_radius;
+    fl[k].sigmaWorld = (float)(q.filter_sigma * r);
+    fl[k].proj11 = q.proj[5];
+    fl[k].viewH = (float)H;
+    fl[k].delta = (float)(q.narrow_delta * r);
+    fl[k].mu = (float)(q.narrow_mu * r);
+    fl[k].rangeSigma = (float)std::max(q.bilateral_range * r, 1e-4);
+  }
+  std::vector<float> zb[2] = {eyeZ, std::vector<float>((size_t)W * H)};
+  int src = 0;
+  for (int it = 0; it < q.filter_iterations * 2; it++) { o_filter(fl[it % 2], zb[src], zb[1 - src], W, H); src = 1 - src; }
+  if (q.cleanup_pass && q.filter_iterations > 0) { o_filter(fl[2], zb[src], zb[1 - src], W, H); src = 1 - src; }
+  s->ssfrEyeZ = zb[src];
+  // body depth and composite
+  OComp C{};
+  C.ivp = q.inv_view_proj;
+  C.iv = q.inv_view;
+  C.boxMin = {0.0f, 0.0f, 0.0f};
+  C.absorb = {(float)absorb[0], (float)absorb[1], (float)absorb[2]};
+  C.sunDir = {(float)(sun[0] / sl), (float)(sun[1] / sl), (float)(sun[2] / sl)};
+  C.proj00 = q.proj[0];
+  C.proj11 = q.proj[5];
+  C.ior = (float)q.ior;
+  C.sunIntensity = (float)q.sun_intensity;
+  C.roughness = (float)q.roughness;
+  C.exposure = (float)q.exposure;
+  C.groundReflection = (float)q.ground_reflection;
+  C.thicknessScale = (float)q.thickness_scale;
+  C.bodyCount = bodyCount;
+  C.floorPlane = q.floor_plane ? 1 : 0;
+  C.debug = q.debug;
+  C.bdata = bodies;
+  std::vector<float> bodyT((size_t)W * H, 1.0e30f);
+  if (bodyCount > 0) {
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int py = 0; py < H; py++)
+      for (int px = 0; px < W; px++) {
+        f3 ro, rd;
+        o_ray(q.inv_view_proj, ((float)px + 0.5f) / (float)W * 2.0f - 1.0f,
+              1.0f - ((float)py + 0.5f) / (float)H * 2.0f, ro, rd);
+        const OTrace b = o_trace(C, ro, rd, 60.0f);
+        if (b.t >= 0.0f) bodyT[(size_t)py * W + px] = b.t;
+      }
+  }
+  s->ssfrBodyT = bodyT;
+  const std::vector<float>& z = zb[src];
+  const float msx = (float)((double)W / std::max(1, q.width)), msy = (float)((double)H / std::max(1, q.height));
+  s->ssfrImage.assign((size_t)q.width * q.height, 0u);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int y = 0; y < q.height; y++)
+    for (int x = 0; x < q.width; x++) {
+      const float fx = (float)x + 0.5f, fy = (float)y + 0.5f;
+      const float nx = fx / (float)q.width * 2.0f - 1.0f, ny = 1.0f - fy / (float)q.height * 2.0f;
+      const float u = nx * 0.5f + 0.5f, v = 0.5f - ny * 0.5f;
+      const int ipx = (int)(fx * msx), ipy = (int)(fy * msy);
+      const float zi = z[(size_t)ipy * W + ipx];
+      const float tu = u * (float)TW - 0.5f, tv = v * (float)TH - 0.5f;
+      const float fu = std::floor(tu), fv = std::floor(tv);
+      const float au = tu - fu, av = tv - fv;
+      const int i0 = std::min(std::max((int)fu, 0), TW - 1), i1 = std::min(std::max((int)fu + 1, 0), TW - 1);
+      const int j0 = std::min(std::max((int)fv, 0), TH - 1), j1 = std::min(std::max((int)fv + 1, 0), TH - 1);
+      const float top = thick[(size_t)j0 * TW + i0] * (1.0f - au) + thick[(size_t)j0 * TW + i1] * au;
+      const float bot = thick[(size_t)j1 * TW + i0] * (1.0f - au) + thick[(size_t)j1 * TW + i1] * au;
+      float th = (top * (1.0f - av) + bot * av) * C.thicknessScale;
+      f3 ro, rd;
+      o_ray(q.inv_view_proj, nx, ny, ro, rd);
+      uint32_t out;
+      if (C.debug == 3) {
+        out = o_rgba8({th, th * 0.25f, 0.0f});
+      } else if (C.debug == 2 || C.debug == 4) {
+        const float d = C.debug == 4 ? s->ssfrRaw[(size_t)ipy * W + ipx] : zi;
+        float sg = 0.0f;
+        if (!(d < -1.0e3f)) sg = clampo(-d / 4.0f, 0.0f, 1.0f);
+        out = o_rgba8({1.0f - sg, 1.0f - sg, 1.0f - sg});
+      } else {
+        const float tBody = bodyT[(size_t)ipy * W + ipx];
+        if (C.debug == 5) {
+          out = tBody > 1.0e29f ? o_rgba8({0.0f, 0.0f, 0.6f}) : o_rgba8({frac1(tBody), frac1(tBody * 0.1f), 0.0f});
+        } else {
+          const f3 p0 = {-nx * zi / C.proj00, -ny * zi / C.proj11, zi};
+          const v4o pw = mv4(C.iv, {p0.x, p0.y, p0.z, 1.0f});
+          const f3 p = {pw.x, pw.y, pw.z};
+          const bool bodyInFront = tBody < length3(sub3(p, ro));
+          if (zi < -1.0e3f || bodyInFront) {
+            out = o_rgba8(o_tonemap(C, o_scene_color(C, ro, rd)));
+          } else {
+            auto vp = [&](float ax, float ay, float zz) { return f3{-ax * zz / C.proj00, -ay * zz / C.proj11, zz}; };
+            const float pxs = 2.0f / (float)W, pys = 2.0f / (float)H;
+            const float zxp = o_fetch(z, ipx + 1, ipy, W, H), zxm = o_fetch(z, ipx - 1, ipy, W, H);
+            const float zyp = o_fetch(z, ipx, ipy - 1, W, H), zym = o_fetch(z, ipx, ipy + 1, W, H);
+            const f3 dxr = sub3(vp(nx + pxs, ny, zxp), p0), dxl = sub3(p0, vp(nx - pxs, ny, zxm));
+            const f3 dyt = sub3(vp(nx, ny + pys, zyp), p0), dyb = sub3(p0, vp(nx, ny - pys, zym));
+            const f3 dpx = std::fabs(dxr.z) < std::fabs(dxl.z) ? dxr : dxl;
+            const f3 dpy = std::fabs(dyt.z) < std::fabs(dyb.z) ? dyt : dyb;
+            const f3 nView = nrm3(cross3(dpx, dpy));
+            m3 iv3;
+            for (int cc = 0; cc < 3; cc++) iv3.c[cc] = {C.iv[cc * 4], C.iv[cc * 4 + 1], C.iv[cc * 4 + 2]};
+            f3 nn = nrm3(mv3(iv3, nView));
+            if (nn.x != nn.x || nn.y != nn.y || nn.z != nn.z) nn = {-rd.x, -rd.y, -rd.z};
+            if (dot3(nn, rd) > 0.0f) nn = {-nn.x, -nn.y, -nn.z};
+            if (C.debug == 1) {
+              out = o_rgba8({nn.x * 0.5f + 0.5f, nn.y * 0.5f + 0.5f, nn.z * 0.5f + 0.5f});
+            } else {
+              const f3 mrd = {-rd.x, -rd.y, -rd.z};
+              const float kS = o_fresnel(std::fmax(dot3(mrd, nn), 0.0f), 1.0f, C.ior);
+              const f3 rfl = o_water_reflect(C, refl(rd, nn), nn);
+              f3 refrDir = refr(rd, nn, 1.0f / C.ior);
+              if (dot3(refrDir, refrDir) < 1.0e-8f) refrDir = refl(rd, nn);
+              const f3 ro2 = {p.x + refrDir.x * 1.0e-3f, p.y + refrDir.y * 1.0e-3f, p.z + refrDir.z * 1.0e-3f};
+              const OTrace st = o_trace(C, ro2, refrDir, 60.0f);
+              f3 hit;
+              if (st.t >= 0.0f) {
+                hit = o_shade_body(C, st.nrm, st.col, refrDir, o_env_reflect(C, refl(refrDir, st.nrm)));
+                th = std::fmin(th, st.t);
+              } else {
+                hit = o_background(C, ro2, refrDir);
+              }
+              const f3 trans = {hit.x * orc_exp(-C.absorb.x * th), hit.y * orc_exp(-C.absorb.y * th),
+                                hit.z * orc_exp(-C.absorb.z * th)};
+              f3 col = mixo(trans, rfl, kS);
+              const float gs = o_ggx(nn, mrd, C.sunDir, C.roughness);
+              col = {col.x + 1.0f * C.sunIntensity * gs * kS, col.y + 0.97f * C.sunIntensity * gs * kS,
+                     col.z + 0.90f * C.sunIntensity * gs * kS};
+              out = o_rgba8(o_tonemap(C, col));
+            }
+          }
+        }
+      }
+      s->ssfrImage[(size_t)y * q.width + x] = out;
+    }
+  s->ssfrDims[0] = q.width; s->ssfrDims[1] = q.height; s->ssfrDims[2] = W; s->ssfrDims[3] = H;
+  s->ssfrDims[4] = TW; s->ssfrDims[5] = TH;
+  return P4A_OK;
+}
+
+int orc_ssfr_buffer(orc_sim* s, int32_t which, void** ptr, size_t* bytes) {
+  if (!s || !ptr || !bytes) return P4A_ERR_ARG;
+  switch (which) {
+    case P4A_SSFR_EYEZ: *ptr = s->ssfrEyeZ.data(); *bytes = s->ssfrEyeZ.size() * 4; return P4A_OK;
+    case P4A_SSFR_RAWZ: *ptr = s->ssfrRaw.data(); *bytes = s->ssfrRaw.size() * 4; return P4A_OK;
+    case P4A_SSFR_THICK: *ptr = s->ssfrThick.data(); *bytes = s->ssfrThick.size() * 4; return P4A_OK;
+    case P4A_SSFR_IMAGE: *ptr = s->ssfrImage.data(); *bytes = s->ssfrImage.size() * 4; return P4A_OK;
+    case P4A_SSFR_BODYT: *ptr = s->ssfrBodyT.data(); *bytes = s->ssfrBodyT.size() * 4; return P4A_OK;
+    default: return P4A_ERR_ARG;
+  }
+}
+
+float orc_expf(float x) { return orc_exp(x); }
+float orc_logf(float x) { return orc_log(x); }
 
 }  // extern "C"

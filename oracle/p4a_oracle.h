@@ -63,6 +63,12 @@ int orc_resize_box(orc_sim* s, const double box[3]);
 int orc_aniso(orc_sim* s, const p4a_aniso_params* ap);
 /* SurfaceMesh.configure + generate (src/mesh.js:99-352): triangles in voxel order. */
 int orc_mesh(orc_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
+/* FluidSSFR.render (src/ssfr.js:173-356) on the anisotropic pass's output. */
+int orc_ssfr(orc_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t body_count);
+int orc_ssfr_buffer(orc_sim* s, int32_t which, void** ptr, size_t* bytes);
+/* The render passes' exp and log (Cody-Waite + Taylor; atanh series). */
+float orc_expf(float x);
+float orc_logf(float x);
 int orc_get_info(const orc_sim* s, p4a_info* out);
 int orc_stats(const orc_sim* s, p4a_stats* out);
 /* Host pointer + bytes of a buffer (same ids / which as p4a_buffer). */

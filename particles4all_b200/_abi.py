@@ -87,6 +87,30 @@ class MeshInfo(C.Structure):
                 ("triangles", C.c_int64), ("mesh_gen", C.c_int32)]
 
 
+class SsfrParams(C.Structure):
+    _fields_ = [
+        ("view", C.c_float * 16), ("proj", C.c_float * 16), ("inv_view_proj", C.c_float * 16),
+        ("inv_view", C.c_float * 16), ("eye", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32),
+        ("render_scale", C.c_double), ("splat_radius", C.c_double), ("thickness_radius", C.c_double),
+        ("thickness_scale", C.c_double), ("thickness_filter_size", C.c_int32), ("thickness_half_res", C.c_int32),
+        ("filter", C.c_int32), ("filter_iterations", C.c_int32), ("cleanup_pass", C.c_int32),
+        ("cleanup_radius", C.c_int32), ("filter_max_radius", C.c_int32), ("depth_cull_neighbours", C.c_int32),
+        ("filter_sigma", C.c_double), ("narrow_delta", C.c_double), ("narrow_mu", C.c_double),
+        ("bilateral_range", C.c_double), ("ior", C.c_double), ("absorption", C.c_double),
+        ("transmit", C.c_double * 3), ("roughness", C.c_double), ("sun_intensity", C.c_double),
+        ("sun_elevation", C.c_double), ("sun_azimuth", C.c_double), ("exposure", C.c_double),
+        ("ground_reflection", C.c_double), ("floor_plane", C.c_int32), ("debug", C.c_int32),
+    ]
+
+
+class SsfrInfo(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("map_w", C.c_int32), ("map_h", C.c_int32),
+                ("thick_w", C.c_int32), ("thick_h", C.c_int32), ("ssfr_gen", C.c_int32)]
+
+
+SSFR_BUF = {"eyeZ": 0, "rawZ": 1, "thick": 2, "image": 3, "bodyT": 4}
+
+
 class Grid(C.Structure):
     _fields_ = [("box_min", C.c_float * 3), ("h", C.c_float), ("dim", C.c_int32 * 3)]
 

@@ -76,6 +76,11 @@ SIGNATURES = {
     "p4a_default_mesh_params": ([_vp], C.c_int),
     "p4a_mesh": ([_vp, _vp, C.POINTER(C.c_int64)], C.c_int),
     "p4a_mesh_get_info": ([_vp, _vp], C.c_int),
+    "p4a_default_ssfr_params": ([_vp], C.c_int),
+    "p4a_ssfr": ([_vp, _vp, _vp, _i32], C.c_int),
+    "p4a_ssfr_get_info": ([_vp, _vp], C.c_int),
+    "p4a_ssfr_buffer": ([_vp, _i32, C.POINTER(_vp), C.POINTER(_sz)], C.c_int),
+    "p4a_ssfr_read": ([_vp, _i32, _vp, _sz], C.c_int),
 }
 
 _lib = None

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/p4a.h"
+#include "fmath.h"
 #include "p4a_internal.h"
 #include "scene.h"
 
@@ -38,12 +39,12 @@ const double kPi = 3.14159265358979323846;
 enum Phase {
   PH_DRAG, PH_KEY_COUNT, PH_SCAN, PH_FILL, PH_REORDER, PH_BODY_SEED, PH_LAMBDA, PH_DELTA,
   PH_BODY_MATCH, PH_XSPH_FINALIZE, PH_XSPH_NORMALS, PH_TENSION_FINALIZE, PH_ANISO, PH_IMPULSE,
-  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_COUNT, PH_END = PH_COUNT
+  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_SSFR, PH_COUNT, PH_END = PH_COUNT
 };
 const char* const kPhaseNames[PH_COUNT] = {
     "body_drag", "key_count", "scan", "fill", "reorder", "body_seed", "lambda", "delta",
     "body_match", "xsph_finalize", "xsph_normals", "tension_finalize", "aniso", "impulse",
-    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march"};
+    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march", "ssfr"};
 
 std::atomic<uint64_t> g_launches{0};
 }  // namespace
@@ -101,6 +102,12 @@ struct p4a_sim {
   double meshOrigin = 0, meshVoxel = 0;
   int64_t meshTris = 0;
   uint32_t meshEpoch = 0;
+  // screen-space fluid rendering (p4a_ssfr)
+  std::vector<void*> ssfrAllocs;
+  SsfrFrame ssfr{};
+  int ssfrW = 0, ssfrH = 0, ssfrMapW = 0, ssfrMapH = 0, ssfrThW = 0, ssfrThH = 0, ssfrGen = 0;
+  float4* ssfrBodies = nullptr;
+  int ssfrBodyCap = 0;
   bool ready = false;
   // per-kernel timing (p4a_profile_*)
   bool prof = false;
@@ -153,7 +160,8 @@ int resolve_marks(p4a_sim* s) {
 // Called before each kernel the handle launches (and with PH_END after the last):
 // counts launches and, with profiling on, records the event that opens the interval.
 void mark(p4a_sim* s, int phase) {
-  if (phase < PH_COUNT && phase != PH_STATS_CLEAR) g_launches.fetch_add(1, std::memory_order_relaxed);
+  // the SSFR phase counts its own launches (several kernels per phase)
+  if (phase < PH_COUNT && phase != PH_STATS_CLEAR && phase != PH_SSFR) g_launches.fetch_add(1, std::memory_order_relaxed);
   if (!s->prof) return;
   if (s->evUsed == (int)s->evPool.size()) {
     cudaEvent_t e;
@@ -626,6 +634,8 @@ int p4a_destroy(p4a_sim* s) {
   if (s->meshScan) cudaFree(s->meshScan);
   if (s->meshTicket) cudaFree(s->meshTicket);
   if (s->meshVerts) cudaFree(s->meshVerts);
+  free_list(s->ssfrAllocs);
+  if (s->ssfrBodies) cudaFree(s->ssfrBodies);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
@@ -1174,6 +1184,260 @@ int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
   } else {
     s->meshTris = (int64_t)tris;  // unknown until waited for: the stored capacity bounds it
   }
+  return P4A_OK;
+}
+
+int p4a_default_ssfr_params(p4a_ssfr_params* o) {
+  if (!o) return P4A_ERR_ARG;
+  *o = p4a_ssfr_params{};
+  // an identity camera: callers set the four matrices and the eye
+  for (int k = 0; k < 4; k++) o->view[k * 5] = o->proj[k * 5] = o->inv_view_proj[k * 5] = o->inv_view[k * 5] = 1.0f;
+  o->width = 640;
+  o->height = 480;
+  o->render_scale = 1.0;  // FluidSSFR constructor defaults (src/ssfr.js:9-47)
+  o->splat_radius = 1.0;
+  o->thickness_radius = 0.62;
+  o->thickness_scale = 3.0;
+  o->thickness_filter_size = 8;
+  o->thickness_half_res = 1;
+  o->filter = 2;
+  o->filter_iterations = 2;
+  o->cleanup_pass = 1;
+  o->cleanup_radius = 4;
+  o->filter_max_radius = 32;
+  o->depth_cull_neighbours = 0;
+  o->filter_sigma = 0.7;
+  o->narrow_delta = 10.0;
+  o->narrow_mu = 1.0;
+  o->bilateral_range = 2.0;
+  o->ior = 1.333;
+  o->absorption = 1.0;
+  o->transmit[0] = 0.35;
+  o->transmit[1] = 0.62;
+  o->transmit[2] = 0.78;
+  o->roughness = 0.055;
+  o->sun_intensity = 3.0;
+  o->sun_elevation = 38.0;
+  o->sun_azimuth = 40.0;
+  o->exposure = 1.0;
+  o->ground_reflection = 0.0;
+  o->floor_plane = 1;
+  o->debug = 0;
+  return P4A_OK;
+}
+
+int p4a_ssfr(p4a_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t bodyCount) {
+  if (!s || !sp || sp->width < 1 || sp->height < 1 || sp->width > 16384 || sp->height > 16384 ||
+      bodyCount < 0 || (bodyCount > 0 && !bodies) || sp->filter < 0 || sp->filter > 2 ||
+      sp->filter_iterations < 0 || sp->filter_iterations > 16 || sp->cleanup_radius < 0 ||
+      sp->cleanup_radius > 64 || sp->filter_max_radius < 0 || sp->filter_max_radius > 256 ||
+      sp->thickness_filter_size < 0 || sp->thickness_filter_size > 2 * kSsfrMaxBlur)
+    return fail(s, P4A_ERR_ARG, "p4a_ssfr: invalid parameters");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "ssfr before reset");
+  if ((size_t)s->n > s->anisoCap || (s->n > 0 && !s->smoothPos))
+    return fail(s, P4A_ERR_STATE, "ssfr needs the anisotropic pass (p4a_aniso) of the current particles");
+  cudaSetDevice(s->device);
+  const p4a_ssfr_params& q = *sp;
+  // render targets (src/ssfr.js:95-130, 173-178)
+  const double rs = std::min(1.0, std::max(0.25, q.render_scale));
+  const int mapW = std::max(1, (int)std::floor(q.width * rs + 0.5));
+  const int mapH = std::max(1, (int)std::floor(q.height * rs + 0.5));
+  const bool half = q.thickness_half_res && q.thickness_filter_size >= 4;
+  const int tw = half ? (mapW + 1) >> 1 : mapW, th = half ? (mapH + 1) >> 1 : mapH;
+  SsfrFrame& F = s->ssfr;
+  if (mapW != s->ssfrMapW || mapH != s->ssfrMapH || tw != s->ssfrThW || th != s->ssfrThH ||
+      q.width != s->ssfrW || q.height != s->ssfrH) {
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    free_list(s->ssfrAllocs);
+    s->ssfrMapW = s->ssfrMapH = s->ssfrThW = s->ssfrThH = s->ssfrW = s->ssfrH = 0;
+    const size_t mapN = (size_t)mapW * mapH, thN = (size_t)tw * th;
+    int rc;
+    if ((rc = dalloc(s, s->ssfrAllocs, &F.depthKey, mapN)) || (rc = dalloc(s, s->ssfrAllocs, &F.thickAcc, thN)) ||
+        (rc = dalloc(s, s->ssfrAllocs, &F.eyeZ[0], mapN)) || (rc = dalloc(s, s->ssfrAllocs, &F.eyeZ[1], mapN)) ||
+        (rc = dalloc(s, s->ssfrAllocs, &F.raw, mapN)) || (rc = dalloc(s, s->ssfrAllocs, &F.thickMap, thN)) ||
+        (rc = dalloc(s, s->ssfrAllocs, &F.thickTmp, thN)) || (rc = dalloc(s, s->ssfrAllocs, &F.bodyT, mapN)) ||
+        (rc = dalloc(s, s->ssfrAllocs, &F.image, (size_t)q.width * q.height)))
+      return rc;
+    s->ssfrMapW = mapW;
+    s->ssfrMapH = mapH;
+    s->ssfrThW = tw;
+    s->ssfrThH = th;
+    s->ssfrW = q.width;
+    s->ssfrH = q.height;
+    s->ssfrGen++;
+  }
+  if (bodyCount > s->ssfrBodyCap) {
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->ssfrBodies) cudaFree(s->ssfrBodies);
+    s->ssfrBodies = nullptr;
+    s->ssfrBodyCap = 0;
+    CUDA_TRY(s, cudaMalloc((void**)&s->ssfrBodies, (size_t)bodyCount * 6 * 16));
+    s->ssfrBodyCap = bodyCount;
+  }
+  if (bodyCount > 0) {
+    CUDA_TRY(s, cudaMemcpyAsync(s->ssfrBodies, bodies, (size_t)bodyCount * 6 * 16, cudaMemcpyHostToDevice,
+                                s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));  // the caller's array may go away
+  }
+  F.mapW = mapW;
+  F.mapH = mapH;
+  F.thickW = tw;
+  F.thickH = th;
+  F.smoothPos = s->smoothPos;
+  F.g = s->anisoG;
+  F.phase = s->d.body[s->parity];
+  F.bodies = s->ssfrBodies;
+  // host constants (src/ssfr.js:173-226), in double, stored as float
+  const double kPiD = 3.14159265358979323846;
+  const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
+  const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};
+  const double sl = std::sqrt(sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2]);
+  double absorb[3];
+  for (int k = 0; k < 3; k++) absorb[k] = q.absorption * -std::log(std::min(1.0, std::max(1e-3, q.transmit[k])));
+  const double spacing = s->params.spacing, support = s->h;
+  const double scale = q.splat_radius * spacing / support;
+  const double r = 0.5 * spacing;
+  const double thickRadius = q.thickness_radius * spacing;
+  const bool skipBodies = s->nBodyParts > 0;
+  float pv[16];
+  for (int c = 0; c < 4; c++)
+    for (int rr = 0; rr < 4; rr++)
+      pv[c * 4 + rr] = std::fma(q.proj[12 + rr], q.view[c * 4 + 3],
+                                std::fma(q.proj[8 + rr], q.view[c * 4 + 2],
+                                         std::fma(q.proj[4 + rr], q.view[c * 4 + 1], q.proj[rr] * q.view[c * 4])));
+  auto splat = [&](SsfrSplat& S, int vw, int vh, double quadRadius, double maxNb) {
+    memcpy(S.view, q.view, 64);
+    memcpy(S.proj, q.proj, 64);
+    memcpy(S.ivp, q.inv_view_proj, 64);
+    memcpy(S.pv, pv, 64);
+    S.vw = (float)vw;
+    S.vh = (float)vh;
+    S.kernelScale = (float)scale;
+    S.quadRadius = (float)quadRadius;
+    S.thickRadius = (float)thickRadius;
+    S.maxNeighbours = (float)maxNb;
+    S.skipBodies = skipBodies ? 1u : 0u;
+    S.count = (uint32_t)std::max(0, s->n);
+  };
+  splat(F.depth, mapW, mapH, 0.0, (double)q.depth_cull_neighbours);
+  splat(F.thick, tw, th, thickRadius, 0.0);
+  // thickness blur (src/ssfr.js:227-233)
+  const int blurSize = q.thickness_filter_size == 0 ? 0
+                       : (tw < mapW ? std::max(1, q.thickness_filter_size >> 1) : q.thickness_filter_size);
+  if (blurSize > kSsfrMaxBlur) return fail(s, P4A_ERR_ARG, "p4a_ssfr: thickness blur wider than %d", kSsfrMaxBlur);
+  for (int p = 0; p < 2; p++) {
+    SsfrBlur& B = F.blur[p];
+    B = SsfrBlur{};
+    B.dirX = p == 0 ? 1 : 0;
+    B.dirY = p == 0 ? 0 : 1;
+    B.size = blurSize;
+    const float sigma = std::max((float)blurSize / 3.0f, 1.0e-3f);
+    const float twoSigma2 = 2.0f * sigma * sigma;
+    for (int i = -blurSize; i <= blurSize; i++) B.w[i + blurSize] = fm_exp(-(float)(i * i) / twoSigma2);
+  }
+  // depth filter uniforms (src/ssfr.js:151-164, 235-237)
+  auto filt = [&](SsfrFilter& Fl, int dx, int dy, int clean) {
+    Fl = SsfrFilter{};
+    Fl.dirX = dx;
+    Fl.dirY = dy;
+    Fl.maxRadius = q.filter_max_radius;
+    Fl.mode = q.filter;
+    Fl.sigmaWorld = (float)(q.filter_sigma * r);
+    Fl.proj11 = q.proj[5];
+    Fl.viewH = (float)mapH;
+    Fl.delta = (float)(q.narrow_delta * r);
+    Fl.mu = (float)(q.narrow_mu * r);
+    Fl.rangeSigma = (float)std::max(q.bilateral_range * r, 1e-4);
+    Fl.clean = clean;
+    Fl.cleanRadius = q.cleanup_radius;
+  };
+  filt(F.filter[0], 1, 0, 0);
+  filt(F.filter[1], 0, 1, 0);
+  filt(F.filter[2], 0, 0, 1);
+  F.filterPasses = 0;
+  for (int it = 0; it < q.filter_iterations * 2; it++) F.filterSlot[F.filterPasses++] = it % 2;
+  if (q.cleanup_pass && q.filter_iterations > 0) F.filterSlot[F.filterPasses++] = 2;
+  // composite uniform (src/ssfr.js:183-213)
+  SsfrComp& C = F.comp;
+  C = SsfrComp{};
+  memcpy(C.ivp, q.inv_view_proj, 64);
+  memcpy(C.iv, q.inv_view, 64);
+  for (int k = 0; k < 3; k++) {
+    C.eye[k] = q.eye[k];
+    C.boxMin[k] = 0.0f;
+    C.boxMax[k] = (float)s->params.box[k];
+    C.absorb[k] = (float)absorb[k];
+    C.sunDir[k] = (float)(sun[k] / sl);
+  }
+  C.proj00 = q.proj[0];
+  C.proj11 = q.proj[5];
+  C.ior = (float)q.ior;
+  C.sunIntensity = (float)q.sun_intensity;
+  C.roughness = (float)q.roughness;
+  C.exposure = (float)q.exposure;
+  C.groundReflection = (float)q.ground_reflection;
+  C.thicknessScale = (float)q.thickness_scale;
+  C.bodyCount = bodyCount;
+  C.floorPlane = q.floor_plane ? 1 : 0;
+  C.debug = q.debug;
+  C.mapScaleX = (float)((double)mapW / std::max(1, q.width));
+  C.mapScaleY = (float)((double)mapH / std::max(1, q.height));
+  C.width = q.width;
+  C.height = q.height;
+  C.mapW = mapW;
+  C.mapH = mapH;
+  C.thickW = tw;
+  C.thickH = th;
+  mark(s, PH_SSFR);
+  launch_ssfr(F, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  return P4A_OK;
+}
+
+int p4a_ssfr_get_info(p4a_sim* s, p4a_ssfr_info* o) {
+  if (!s || !o) return P4A_ERR_ARG;
+  *o = p4a_ssfr_info{};
+  o->width = s->ssfrW;
+  o->height = s->ssfrH;
+  o->map_w = s->ssfrMapW;
+  o->map_h = s->ssfrMapH;
+  o->thick_w = s->ssfrThW;
+  o->thick_h = s->ssfrThH;
+  o->ssfr_gen = s->ssfrGen;
+  return P4A_OK;
+}
+
+int p4a_ssfr_buffer(p4a_sim* s, int32_t which, void** dptr, size_t* bytes) {
+  if (!s || !dptr || !bytes) return P4A_ERR_ARG;
+  if (s->ssfrW == 0) return fail(s, P4A_ERR_STATE, "p4a_ssfr_buffer before p4a_ssfr");
+  const SsfrFrame& F = s->ssfr;
+  const size_t mapN = (size_t)s->ssfrMapW * s->ssfrMapH, thN = (size_t)s->ssfrThW * s->ssfrThH;
+  switch (which) {
+    case P4A_SSFR_EYEZ: {
+      // the filter's last output: eyeZ[passes % 2]
+      *dptr = F.eyeZ[F.filterPasses % 2];
+      *bytes = mapN * 4;
+      return P4A_OK;
+    }
+    case P4A_SSFR_RAWZ: *dptr = F.raw; *bytes = mapN * 4; return P4A_OK;
+    case P4A_SSFR_THICK: *dptr = F.thickMap; *bytes = thN * 4; return P4A_OK;
+    case P4A_SSFR_IMAGE: *dptr = F.image; *bytes = (size_t)s->ssfrW * s->ssfrH * 4; return P4A_OK;
+    case P4A_SSFR_BODYT: *dptr = F.bodyT; *bytes = mapN * 4; return P4A_OK;
+    default: return fail(s, P4A_ERR_ARG, "p4a_ssfr_buffer: unknown buffer %d", which);
+  }
+}
+
+int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes) {
+  if (!s || (!host && bytes)) return P4A_ERR_ARG;
+  void* p = nullptr;
+  size_t have = 0;
+  const int rc = p4a_ssfr_buffer(s, which, &p, &have);
+  if (rc) return rc;
+  if (bytes > have) return fail(s, P4A_ERR_ARG, "p4a_ssfr_read: %zu bytes asked, buffer holds %zu", bytes, have);
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return P4A_OK;
 }
 

@@ -78,6 +78,55 @@ struct MeshParams {
   uint32_t maxTris, skipBodies;
 };
 
+// Screen-space fluid rendering (kernels_ssfr.cu). Matrices column-major.
+// The splat uniform of src/ssfr_wgsl.js:2-14 (+ proj * view, which the depth
+// fragment applies as one matrix) for one splat pass.
+struct SsfrSplat {
+  float view[16], proj[16], ivp[16], pv[16];
+  float vw, vh, kernelScale, quadRadius, thickRadius, maxNeighbours;
+  uint32_t skipBodies, count;
+};
+constexpr int kSsfrMaxBlur = 64;
+struct SsfrBlur {  // src/ssfr_wgsl.js:156 + the pass's Gaussian weights
+  int dirX, dirY, size, pad;
+  float w[2 * kSsfrMaxBlur + 1];
+};
+struct SsfrFilter {  // src/ssfr_wgsl.js:186-199
+  int dirX, dirY, maxRadius, mode;
+  float sigmaWorld, proj11, viewH, delta, mu, rangeSigma;
+  int clean, cleanRadius;
+};
+struct SsfrComp {  // src/ssfr_composite_wgsl.js:2-26 (no environment map)
+  float ivp[16], iv[16];
+  float eye[3], boxMin[3], boxMax[3], absorb[3], sunDir[3];
+  float proj00, proj11, ior, sunIntensity, roughness, exposure, groundReflection, thicknessScale;
+  int32_t bodyCount, floorPlane, debug;
+  float mapScaleX, mapScaleY;
+  int32_t width, height, mapW, mapH, thickW, thickH;
+};
+struct SsfrFrame {
+  SsfrSplat depth, thick;
+  SsfrBlur blur[2];
+  SsfrFilter filter[3];
+  int filterSlot[64];
+  int filterPasses;
+  SsfrComp comp;
+  int mapW, mapH, thickW, thickH;
+  const float4* smoothPos;
+  const float4* g;
+  const uint4* phase;
+  const float4* bodies;
+  unsigned long long* depthKey;  // [mapW * mapH]
+  unsigned long long* thickAcc;  // [thickW * thickH]
+  float* eyeZ[2];                // [mapW * mapH] ping-pong
+  float* raw;                    // [mapW * mapH] unfiltered eye-space z
+  float* thickMap;               // [thickW * thickH]
+  float* thickTmp;
+  float* bodyT;                  // [mapW * mapH]
+  uchar4* image;                 // [width * height] RGBA8
+};
+void launch_ssfr(const SsfrFrame& f, cudaStream_t st);
+
 // Device error word bits (set by kernels, read by the host at sync points).
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };
 

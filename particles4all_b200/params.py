@@ -10,6 +10,8 @@ noBoundary, pour) so that code written against the reference reads the same.
 import ctypes as C
 import math
 
+import numpy as np
+
 from . import _abi
 
 # src/scene.js:3-9. The ini presets are parsed from the same keys the reference's
@@ -168,4 +170,40 @@ def mesh_struct(m):
     s.resolution, s.iso = int(m["resolution"]), float(m["iso"])
     s.field_passes, s.normal_passes = int(m["field_passes"]), int(m["normal_passes"])
     s.max_triangles, s.blur_axes = int(m["max_triangles"]), int(m["blur_axes"])
+    return s
+
+
+SSFR_MATRICES = ("view", "proj", "inv_view_proj", "inv_view")
+
+
+def default_ssfr():
+    """FluidSSFR's defaults (src/ssfr.js:9-47), an identity camera and a 640 x 480
+    target; set the camera with camera.frame_matrices()."""
+    from ._lib import lib
+    s = _abi.SsfrParams()
+    lib().p4a_default_ssfr_params(C.byref(s))
+    out = {}
+    for name, ctype in _abi.SsfrParams._fields_:
+        v = getattr(s, name)
+        out[name] = list(v) if hasattr(ctype, "_length_") else v
+    return out
+
+
+def ssfr_struct(d):
+    s = _abi.SsfrParams()
+    for name, ctype in _abi.SsfrParams._fields_:
+        if name not in d:
+            continue
+        v = d[name]
+        if hasattr(ctype, "_length_"):
+            arr = getattr(s, name)
+            vals = list(np.asarray(v, dtype=np.float64).ravel())
+            if len(vals) != ctype._length_:
+                raise ValueError(f"ssfr {name}: {len(vals)} values, expected {ctype._length_}")
+            for k, x in enumerate(vals):
+                arr[k] = x
+        elif ctype in (C.c_int32,):
+            setattr(s, name, int(v))
+        else:
+            setattr(s, name, float(v))
     return s

@@ -118,6 +118,39 @@ class Sim:
         check(self._L.p4a_mesh(self._h, C.byref(m), C.byref(t) if wait else None), self._h, "mesh")
         return t.value if wait else None
 
+    def ssfr(self, sparams, bodies=None):
+        """FluidSSFR.render (src/ssfr.js:173-356) into headless device images; needs the
+        anisotropic pass of the current particles. `bodies`: float32 [count, 6, 4]
+        packed rigid bodies for the composite, or None. Read results with
+        ssfr_read('image' | 'eyeZ' | 'rawZ' | 'thick' | 'bodyT')."""
+        from .params import ssfr_struct
+        sp = ssfr_struct(sparams)
+        if bodies is None or len(bodies) == 0:
+            ptr, count, keep = None, 0, None
+        else:
+            keep = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 24)
+            ptr, count = keep.ctypes.data, keep.shape[0]
+        check(self._L.p4a_ssfr(self._h, C.byref(sp), ptr, count), self._h, "ssfr")
+
+    def ssfr_info(self):
+        i = _abi.SsfrInfo()
+        check(self._L.p4a_ssfr_get_info(self._h, C.byref(i)), self._h, "ssfr_info")
+        return {k: getattr(i, k) for k, _ in _abi.SsfrInfo._fields_}
+
+    def ssfr_read(self, name):
+        """A copy of an SSFR buffer: float maps [h, w], the image uint8 [height, width, 4]."""
+        p, nb = C.c_void_p(), C.c_size_t()
+        which = _abi.SSFR_BUF[name]
+        check(self._L.p4a_ssfr_buffer(self._h, which, C.byref(p), C.byref(nb)), self._h, "ssfr_buffer")
+        inf = self.ssfr_info()
+        out = np.empty(nb.value, np.uint8)
+        if nb.value:
+            check(self._L.p4a_ssfr_read(self._h, which, out.ctypes.data, nb.value), self._h, "ssfr_read")
+        if name == "image":
+            return out.reshape(inf["height"], inf["width"], 4)
+        w, h = (inf["thick_w"], inf["thick_h"]) if name == "thick" else (inf["map_w"], inf["map_h"])
+        return out.view(np.float32).reshape(h, w)
+
     def mesh_info(self):
         i = _abi.MeshInfo()
         check(self._L.p4a_mesh_get_info(self._h, C.byref(i)), self._h, "mesh_info")
