@@ -365,6 +365,43 @@ int p4a_ssfr_buffer(p4a_sim* s, int32_t which, void** dptr, size_t* bytes);
 /* Copies the first `bytes` of an SSFR buffer to host memory (waits for the stream). */
 int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes);
 
+/* ---- ray-marched surface (src/ray.js:30-97, src/ray_wgsl.js:1-549) ------- */
+/*
+ * RayMarch.draw on the density field of the last p4a_mesh (call p4a_mesh first;
+ * SurfaceMesh.generateField + smoothField is its field stage): per pixel, the eye
+ * ray walks the voxel grid, finds the iso crossing of the trilinear field in each
+ * cell (cubic fit, bracketed regula falsi), and shades the surface with Fresnel
+ * reflection, absorption along the refracted ray's optical depth through the
+ * field, the GGX sun highlight, sky / floor and rigid bodies (`bodies` as for
+ * p4a_ssfr). The image is RGBA8, width x height. The rasterised-mesh surface input
+ * (useSurface) and environment maps are not supported.
+ */
+typedef struct p4a_ray_params {
+  float proj[16], inv_view_proj[16], inv_view[16];
+  float eye[3];
+  int32_t width, height;
+  double iso;                 /* the field's iso level (meshIso), 0.4             */
+  double ior;                 /* 1.333                                           */
+  double absorption;          /* 1.0                                             */
+  double transmit[3];         /* 0.35, 0.62, 0.78                                */
+  int32_t thickness_steps;    /* thicknessSteps, 48                              */
+  int32_t floor_plane;        /* 1                                               */
+  double ground_reflection;   /* 0.0                                             */
+  double skin_width;          /* skinWidth, 0.05                                 */
+  double roughness;           /* 0.055                                           */
+  double sun_intensity;       /* 3.0                                             */
+  double sun_elevation;       /* 38 degrees                                      */
+  double sun_azimuth;         /* 40 degrees                                      */
+  double exposure;            /* 1.0                                             */
+  int32_t debug;              /* 0 shaded, 1 normals, 2 distance, 3 thickness,
+                                 4 reflection side, 5 slope, 6 reflection        */
+} p4a_ray_params;
+int p4a_default_ray_params(p4a_ray_params* out);
+int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t body_count);
+/* The last p4a_ray image (RGBA8): device pointer, or a host copy (waits). */
+int p4a_ray_buffer(p4a_sim* s, void** dptr, size_t* bytes, int32_t* width, int32_t* height);
+int p4a_ray_read(p4a_sim* s, void* host, size_t bytes);
+
 /* ---- batched multi-scene stepping -------------------------------------- */
 /*
  * Extension, no counterpart in the reference (which steps one scene per Sim).

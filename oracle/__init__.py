@@ -51,6 +51,7 @@ def lib():
             "orc_boundary": [vp, dbl, dbl, C.POINTER(i32), vp, vp],
             "orc_grid_sort": [vp, i32, C.c_float, C.c_float] + [vp] * 11,
             "orc_ssfr": [vp, vp, vp, i32], "orc_ssfr_buffer": [vp, i32, C.POINTER(vp), C.POINTER(C.c_size_t)],
+            "orc_ray": [vp, vp, vp, i32], "orc_ray_image": [vp, C.POINTER(vp), C.POINTER(C.c_size_t)],
         }.items():
             f = getattr(L, name)
             f.argtypes = args
@@ -221,6 +222,22 @@ class OracleSim:
             return raw.reshape(dm["height"], dm["width"], 4)
         w, h = (dm["thick_w"], dm["thick_h"]) if name == "thick" else (dm["map_w"], dm["map_h"])
         return raw.view(np.float32).reshape(h, w)
+
+    def ray(self, rparams, bodies=None):
+        """RayMarch.draw restated on the CPU (same parameters as Sim.ray); returns the
+        RGBA8 image [height, width, 4]."""
+        from particles4all_b200.params import ray_struct
+        rp = ray_struct(rparams)
+        if bodies is None or len(bodies) == 0:
+            ptr, count, keep = None, 0, None
+        else:
+            keep = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 24)
+            ptr, count = keep.ctypes.data, keep.shape[0]
+        _check(self._L.orc_ray(self._h, C.byref(rp), ptr, count), "ray")
+        p, nb = C.c_void_p(), C.c_size_t()
+        _check(self._L.orc_ray_image(self._h, C.byref(p), C.byref(nb)), "ray_image")
+        raw = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), (nb.value,)).copy()
+        return raw.reshape(rp.height, rp.width, 4)
 
     def info(self):
         i = _abi.Info()

@@ -454,6 +454,10 @@ struct orc_sim {
   std::vector<uint32_t> ssfrImage;
   int ssfrDims[6] = {0, 0, 0, 0, 0, 0};
   std::vector<float> meshField, meshNField;
+  int meshDim[3] = {0, 0, 0};
+  double meshOrigin = 0, meshVoxel = 0;
+  std::vector<uint32_t> rayImage;
+  int rayDims[2] = {0, 0};
   std::vector<uint32_t> meshVerts;  // 2 words per vertex
   int64_t meshTris = 0;
   bool ready = false;
@@ -1674,6 +1678,9 @@ int orc_mesh(orc_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
     M.simDim[k] = s->gridDim[k];
   }
   M.voxel = (float)voxel;
+  for (int k = 0; k < 3; k++) s->meshDim[k] = M.dim[k];
+  s->meshOrigin = -voxel;
+  s->meshVoxel = voxel;
   M.iso = (float)mp->iso;
   M.invSupport = (float)(1 / s->h);
   M.support2 = (float)(s->h * s->h);
@@ -2492,5 +2499,306 @@ int orc_ssfr_buffer(orc_sim* s, int32_t which, void** ptr, size_t* bytes) {
 
 float orc_expf(float x) { return orc_exp(x); }
 float orc_logf(float x) { return orc_log(x); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ray-marched surface (src/ray.js:30-97, src/ray_wgsl.js): per pixel, the eye ray
+// through the density field of the last orc_mesh, the cubic iso crossing per
+// cell, shading as the SSFR composite (shared helpers above).
+namespace {
+
+struct ORay {
+  std::vector<float>* field;
+  int dim[3];
+  f3 origin;
+  float voxel, iso, ior, skin, roughness;
+  int thickSteps, debug;
+  float cosDeg[4];
+};
+float o_fget(const ORay& R, int x, int y, int z) {
+  x = std::min(std::max(x, 0), R.dim[0] - 1);
+  y = std::min(std::max(y, 0), R.dim[1] - 1);
+  z = std::min(std::max(z, 0), R.dim[2] - 1);
+  return (*R.field)[((size_t)z * R.dim[1] + y) * R.dim[0] + x];
+}
+struct OCell { float d000, d100, d010, d110, d001, d101, d011, d111; };
+OCell o_cell(const ORay& R, int x, int y, int z) {
+  return {o_fget(R, x, y, z), o_fget(R, x + 1, y, z), o_fget(R, x, y + 1, z), o_fget(R, x + 1, y + 1, z),
+          o_fget(R, x, y, z + 1), o_fget(R, x + 1, y, z + 1), o_fget(R, x, y + 1, z + 1), o_fget(R, x + 1, y + 1, z + 1)};
+}
+inline float lerpo(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+float o_tri_local(const OCell& k, f3 u) {
+  const float x00 = lerpo(k.d000, k.d100, u.x), x10 = lerpo(k.d010, k.d110, u.x);
+  const float x01 = lerpo(k.d001, k.d101, u.x), x11 = lerpo(k.d011, k.d111, u.x);
+  return lerpo(lerpo(x00, x10, u.y), lerpo(x01, x11, u.y), u.z);
+}
+float o_tri_at(const ORay& R, f3 g) {
+  const int cx = (int)std::floor(g.x), cy = (int)std::floor(g.y), cz = (int)std::floor(g.z);
+  return o_tri_local(o_cell(R, cx, cy, cz), {clampo(g.x - (float)cx, 0.0f, 1.0f), clampo(g.y - (float)cy, 0.0f, 1.0f),
+                                              clampo(g.z - (float)cz, 0.0f, 1.0f)});
+}
+struct OCubic { float A, B, C, D; };
+float o_cubic_at(const OCubic& c, float t) { return ((c.A * t + c.B) * t + c.C) * t + c.D; }
+float o_segment(const OCell& k, f3 u0, f3 du, float iso) {
+  const float third = (float)(1.0 / 3.0), two = (float)(2.0 / 3.0);
+  const float f0 = o_tri_local(k, u0);
+  const float f1 = o_tri_local(k, {u0.x + du.x * third, u0.y + du.y * third, u0.z + du.z * third});
+  const float f2 = o_tri_local(k, {u0.x + du.x * two, u0.y + du.y * two, u0.z + du.z * two});
+  const float f3v = o_tri_local(k, {u0.x + du.x, u0.y + du.y, u0.z + du.z});
+  const float g1 = f1 - f0, g2 = f2 - f0, g3 = f3v - f0;
+  OCubic c;
+  c.A = 4.5f * (3.0f * g1 - 3.0f * g2 + g3);
+  c.B = -(27.0f * g1 - 9.0f * g3 + 8.0f * c.A) / 6.0f;
+  c.C = g3 - c.A - c.B;
+  c.D = f0;
+  float e0 = 2.0f, e1 = 2.0f;
+  const float a = 3.0f * c.A, b = 2.0f * c.B, cc = c.C;
+  if (std::fabs(a) > 1.0e-12f) {
+    const float disc = b * b - 4.0f * a * cc;
+    if (disc > 0.0f) {
+      const float sq = std::sqrt(disc);
+      const float r0 = (-b - sq) / (2.0f * a), r1 = (-b + sq) / (2.0f * a);
+      e0 = std::fmin(r0, r1);
+      e1 = std::fmax(r0, r1);
+    }
+  } else if (std::fabs(b) > 1.0e-12f) {
+    e0 = -cc / b;
+  }
+  float bounds[4] = {0.0f, 1.0f, 1.0f, 1.0f};
+  int n = 1;
+  if (e0 > 0.0f && e0 < 1.0f) bounds[n++] = e0;
+  if (e1 > 0.0f && e1 < 1.0f && e1 > e0) bounds[n++] = e1;
+  bounds[n++] = 1.0f;
+  float lo = bounds[0], vlo = o_cubic_at(c, lo) - iso;
+  for (int i = 1; i < n; i++) {
+    float hi = bounds[i], vhi = o_cubic_at(c, hi) - iso;
+    if ((vlo <= 0.0f && vhi >= 0.0f) || (vlo >= 0.0f && vhi <= 0.0f)) {
+      float t = lo;
+      for (int it = 0; it < 12; it++) {  // solveMonotone
+        t = lo + (hi - lo) * (-vlo) / std::fmax(vhi - vlo, 1.0e-9f);
+        t = clampo(t, lo, hi);
+        const float v = o_cubic_at(c, t) - iso;
+        if (v * vlo > 0.0f) { lo = t; vlo = v; } else { hi = t; vhi = v; }
+      }
+      return t;
+    }
+    lo = hi;
+    vlo = vhi;
+  }
+  return -1.0f;
+}
+struct OSlab { bool hit; float t0, t1; };
+OSlab o_box(f3 o, f3 d, f3 lo, f3 hi) {
+  const f3 inv = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+  const f3 a = {(lo.x - o.x) * inv.x, (lo.y - o.y) * inv.y, (lo.z - o.z) * inv.z};
+  const f3 b = {(hi.x - o.x) * inv.x, (hi.y - o.y) * inv.y, (hi.z - o.z) * inv.z};
+  OSlab s;
+  s.t0 = std::fmax(std::fmax(std::fmin(a.x, b.x), std::fmin(a.y, b.y)), std::fmin(a.z, b.z));
+  s.t1 = std::fmin(std::fmin(std::fmax(a.x, b.x), std::fmax(a.y, b.y)), std::fmax(a.z, b.z));
+  s.hit = s.t1 > std::fmax(s.t0, 0.0f);
+  return s;
+}
+float o_march(const ORay& R, const OComp& C, f3 ro, f3 rd, float tStart, float tEnd, f3& pos) {
+  const f3 g0 = {(ro.x - R.origin.x) / R.voxel, (ro.y - R.origin.y) / R.voxel, (ro.z - R.origin.z) / R.voxel};
+  const f3 gd = {rd.x / R.voxel, rd.y / R.voxel, rd.z / R.voxel};
+  const f3 p0 = {g0.x + gd.x * tStart, g0.y + gd.y * tStart, g0.z + gd.z * tStart};
+  int c[3] = {std::min(std::max((int)std::floor(p0.x), 0), R.dim[0] - 2),
+              std::min(std::max((int)std::floor(p0.y), 0), R.dim[1] - 2),
+              std::min(std::max((int)std::floor(p0.z), 0), R.dim[2] - 2)};
+  auto sgn = [](float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); };
+  const float gda[3] = {gd.x, gd.y, gd.z}, g0a[3] = {g0.x, g0.y, g0.z};
+  int stp[3];
+  float tMax[3], tDelta[3];
+  for (int a = 0; a < 3; a++) {
+    stp[a] = (int)sgn(gda[a]);
+    const float invD = 1.0f / std::fmax(std::fabs(gda[a]), 1.0e-12f);
+    const float nextEdge = (float)c[a] + std::fmax((float)stp[a], 0.0f);
+    tMax[a] = (nextEdge - g0a[a]) / gda[a];
+    tDelta[a] = invD;
+    if (gda[a] == 0.0f) { tMax[a] = 1.0e30f; tDelta[a] = 1.0e30f; }
+  }
+  float t = tStart;
+  for (int i = 0; i < 4096; i++) {
+    const float tNext = std::fmin(std::fmin(tMax[0], tMax[1]), tMax[2]);
+    const float segEnd = std::fmin(tNext, tEnd);
+    if (segEnd > t) {
+      const OCell k = o_cell(R, c[0], c[1], c[2]);
+      const f3 u0 = {g0.x + gd.x * t - (float)c[0], g0.y + gd.y * t - (float)c[1], g0.z + gd.z * t - (float)c[2]};
+      const float span = segEnd - t;
+      const f3 du = {gd.x * span, gd.y * span, gd.z * span};
+      const float s = o_segment(k, u0, du, R.iso);
+      if (s >= 0.0f) {
+        const float tHit = t + s * (segEnd - t);
+        const f3 p = {ro.x + rd.x * tHit, ro.y + rd.y * tHit, ro.z + rd.z * tHit};
+        bool inside = false;
+        if (C.bodyCount > 0) {
+          float dist = 1.0e30f;
+          for (int b = 0; b < C.bodyCount; b++) dist = std::fmin(dist, o_body_dist(C, b, p));
+          inside = dist < 0.0f;
+        }
+        if (!inside) { pos = p; return tHit; }
+      }
+    }
+    t = tNext;
+    if (t >= tEnd) break;
+    if (tMax[0] <= tMax[1] && tMax[0] <= tMax[2]) { c[0] += stp[0]; tMax[0] += tDelta[0]; }
+    else if (tMax[1] <= tMax[2]) { c[1] += stp[1]; tMax[1] += tDelta[1]; }
+    else { c[2] += stp[2]; tMax[2] += tDelta[2]; }
+    if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] > R.dim[0] - 2 || c[1] > R.dim[1] - 2 || c[2] > R.dim[2] - 2) break;
+  }
+  return -1.0f;
+}
+float o_optical(const ORay& R, f3 ro, f3 rd, float tMax) {
+  const f3 lo = R.origin;
+  const f3 hi = {lo.x + R.voxel * (float)(R.dim[0] - 1), lo.y + R.voxel * (float)(R.dim[1] - 1),
+                 lo.z + R.voxel * (float)(R.dim[2] - 1)};
+  const OSlab s = o_box(ro, rd, lo, hi);
+  if (!s.hit) return 0.0f;
+  const float a = std::fmax(s.t0, 0.0f), b = std::fmin(std::fmax(s.t1, 0.0f), tMax);
+  if (b <= a) return 0.0f;
+  const float dt = (b - a) / (float)R.thickSteps;
+  float acc = 0.0f;
+  for (int i = 0; i < R.thickSteps; i++) {
+    const float t = a + ((float)i + 0.5f) * dt;
+    acc += sstep(R.iso * 0.55f, R.iso * 1.45f,
+                 o_tri_at(R, {(ro.x + rd.x * t - lo.x) / R.voxel, (ro.y + rd.y * t - lo.y) / R.voxel,
+                              (ro.z + rd.z * t - lo.z) / R.voxel}));
+  }
+  return acc * dt;
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t bodyCount) {
+  if (!s || !s->ready || !rp || rp->width < 1 || rp->height < 1 || bodyCount < 0 || (bodyCount > 0 && !bodies))
+    return P4A_ERR_ARG;
+  if (s->meshDim[0] < 2 || s->meshField.empty()) return P4A_ERR_STATE;
+  const p4a_ray_params& q = *rp;
+  apply_threads();
+  const double kPiD = 3.14159265358979323846;
+  const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
+  const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};
+  const double sl = std::sqrt(sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2]);
+  OComp C{};
+  C.ivp = q.inv_view_proj;
+  C.iv = q.inv_view;
+  C.boxMin = {0.0f, 0.0f, 0.0f};
+  double ab[3];
+  for (int k = 0; k < 3; k++) ab[k] = q.absorption * -std::log(std::min(1.0, std::max(1e-3, q.transmit[k])));
+  C.absorb = {(float)ab[0], (float)ab[1], (float)ab[2]};
+  C.sunDir = {(float)(sun[0] / sl), (float)(sun[1] / sl), (float)(sun[2] / sl)};
+  C.sunIntensity = (float)q.sun_intensity;
+  C.roughness = (float)q.roughness;
+  C.exposure = (float)q.exposure;
+  C.groundReflection = (float)q.ground_reflection;
+  C.bodyCount = bodyCount;
+  C.floorPlane = q.floor_plane ? 1 : 0;
+  C.debug = q.debug;
+  C.bdata = bodies;
+  ORay R{};
+  R.field = &s->meshField;
+  for (int k = 0; k < 3; k++) R.dim[k] = s->meshDim[k];
+  R.origin = {(float)s->meshOrigin, (float)s->meshOrigin, (float)s->meshOrigin};
+  R.voxel = (float)s->meshVoxel;
+  R.iso = (float)q.iso;
+  R.ior = (float)q.ior;
+  R.skin = (float)q.skin_width;
+  R.roughness = (float)q.roughness;
+  R.thickSteps = q.thickness_steps;
+  R.debug = q.debug;
+  const double deg[4] = {5.0, 10.0, 20.0, 40.0};
+  for (int k = 0; k < 4; k++) R.cosDeg[k] = (float)std::cos(deg[k] * kPiD / 180);
+  const f3 eye = {q.eye[0], q.eye[1], q.eye[2]};
+  const f3 volLo = R.origin;
+  const f3 volHi = {volLo.x + R.voxel * (float)(R.dim[0] - 1), volLo.y + R.voxel * (float)(R.dim[1] - 1),
+                    volLo.z + R.voxel * (float)(R.dim[2] - 1)};
+  s->rayImage.assign((size_t)q.width * q.height, 0u);
+  s->rayDims[0] = q.width;
+  s->rayDims[1] = q.height;
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int y = 0; y < q.height; y++)
+    for (int x = 0; x < q.width; x++) {
+      const float nx = ((float)x + 0.5f) / (float)q.width * 2.0f - 1.0f;
+      const float ny = 1.0f - ((float)y + 0.5f) / (float)q.height * 2.0f;
+      const v4o nh = mv4(q.inv_view_proj, {nx, ny, -1.0f, 1.0f}), fh = mv4(q.inv_view_proj, {nx, ny, 1.0f, 1.0f});
+      const f3 nearP = {nh.x / nh.w, nh.y / nh.w, nh.z / nh.w}, farP = {fh.x / fh.w, fh.y / fh.w, fh.z / fh.w};
+      const f3 ro = eye, rd = nrm3(sub3(farP, nearP));
+      float tHit = -1.0f;
+      f3 hit = {0, 0, 0};
+      const OSlab slab = o_box(ro, rd, volLo, volHi);
+      if (slab.hit) tHit = o_march(R, C, ro, rd, std::fmax(slab.t0, 0.0f) + 1.0e-5f, slab.t1, hit);
+      float tMaxBody = 60.0f;
+      if (tHit >= 0.0f) tMaxBody = tHit + R.skin;
+      const OTrace bt = o_trace(C, ro, rd, tMaxBody);
+      f3 col = {0, 0, 0}, n = {0, 1, 0};
+      float thick = 0.0f;
+      if (bt.t >= 0.0f && (tHit < 0.0f || bt.t < tHit + R.skin)) {
+        col = o_shade_body(C, bt.nrm, bt.col, rd, o_env_reflect(C, refl(rd, bt.nrm)));
+      } else if (tHit < 0.0f) {
+        col = o_background(C, ro, rd);
+      } else {
+        const f3 g = {(hit.x - R.origin.x) / R.voxel, (hit.y - R.origin.y) / R.voxel, (hit.z - R.origin.z) / R.voxel};
+        const f3 sn = {o_tri_at(R, {g.x + 1.0f, g.y, g.z}) - o_tri_at(R, {g.x - 1.0f, g.y, g.z}),
+                       o_tri_at(R, {g.x, g.y + 1.0f, g.z}) - o_tri_at(R, {g.x, g.y - 1.0f, g.z}),
+                       o_tri_at(R, {g.x, g.y, g.z + 1.0f}) - o_tri_at(R, {g.x, g.y, g.z - 1.0f})};
+        n = nrm3({-sn.x, -sn.y, -sn.z});
+        if (dot3(n, rd) > 0.0f) n = {-n.x, -n.y, -n.z};
+        const f3 mrd = {-rd.x, -rd.y, -rd.z};
+        const float kS = o_fresnel(std::fmax(dot3(mrd, n), 0.0f), 1.0f, R.ior);
+        const f3 reflDir = refl(rd, n);
+        f3 refrDir = refr(rd, n, 1.0f / R.ior);
+        if (dot3(refrDir, refrDir) < 1.0e-8f) refrDir = reflDir;
+        const f3 rfl = o_water_reflect(C, reflDir, n);
+        const float off = R.voxel * 0.02f;
+        const f3 ro2 = {hit.x + refrDir.x * off, hit.y + refrDir.y * off, hit.z + refrDir.z * off};
+        const OTrace st = o_trace(C, ro2, refrDir, 60.0f);
+        f3 trans = st.t >= 0.0f ? o_shade_body(C, st.nrm, st.col, refrDir, o_env_reflect(C, refl(refrDir, st.nrm)))
+                                : o_background(C, ro2, refrDir);
+        thick = o_optical(R, ro2, refrDir, st.t >= 0.0f ? st.t : 1.0e30f);
+        trans = {trans.x * orc_exp(-C.absorb.x * thick), trans.y * orc_exp(-C.absorb.y * thick),
+                 trans.z * orc_exp(-C.absorb.z * thick)};
+        col = mixo(trans, rfl, kS);
+        const float gs = o_ggx(n, mrd, C.sunDir, R.roughness);
+        col = {col.x + 1.0f * C.sunIntensity * gs * kS, col.y + 0.97f * C.sunIntensity * gs * kS,
+               col.z + 0.90f * C.sunIntensity * gs * kS};
+      }
+      if (R.debug == 1) {
+        col = tHit < 0.0f ? f3{0, 0, 0} : f3{n.x * 0.5f + 0.5f, n.y * 0.5f + 0.5f, n.z * 0.5f + 0.5f};
+      } else if (R.debug == 2) {
+        col = tHit < 0.0f ? f3{0, 0, 0} : f3{frac1(tHit), frac1(tHit * 0.1f), 0.0f};
+      } else if (R.debug == 3) {
+        col = {thick, thick * 0.25f, 0.0f};
+      } else if (R.debug == 4) {
+        f3 c4 = {0.1f, 0.3f, 1.0f};
+        if (refl(rd, n).y < 0.0f) c4 = {1.0f, 0.1f, 0.1f};
+        col = tHit < 0.0f ? f3{0, 0, 0} : c4;
+      } else if (R.debug == 6) {
+        col = tHit < 0.0f ? o_background(C, ro, rd) : o_water_reflect(C, refl(rd, n), n);
+      } else if (R.debug == 5) {
+        if (tHit < 0.0f) {
+          col = {0, 0, 0};
+        } else {
+          const float a = clampo(std::fabs(n.y), 0.0f, 1.0f);
+          if (a > R.cosDeg[0]) col = {0.1f, 0.3f, 1.0f};
+          else if (a > R.cosDeg[1]) col = {0.1f, 0.9f, 0.9f};
+          else if (a > R.cosDeg[2]) col = {0.2f, 0.9f, 0.2f};
+          else if (a > R.cosDeg[3]) col = {0.95f, 0.9f, 0.2f};
+          else col = {1.0f, 0.15f, 0.1f};
+        }
+      }
+      s->rayImage[(size_t)y * q.width + x] = o_rgba8(o_tonemap(C, col));
+    }
+  return P4A_OK;
+}
+
+int orc_ray_image(orc_sim* s, void** ptr, size_t* bytes) {
+  if (!s || !ptr || !bytes) return P4A_ERR_ARG;
+  *ptr = s->rayImage.data();
+  *bytes = s->rayImage.size() * 4;
+  return P4A_OK;
+}
 
 }  // extern "C"

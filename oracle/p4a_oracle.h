@@ -66,6 +66,9 @@ int orc_mesh(orc_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
 /* FluidSSFR.render (src/ssfr.js:173-356) on the anisotropic pass's output. */
 int orc_ssfr(orc_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t body_count);
 int orc_ssfr_buffer(orc_sim* s, int32_t which, void** ptr, size_t* bytes);
+/* RayMarch.draw (src/ray.js:30-97) on the density field of the last orc_mesh. */
+int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t body_count);
+int orc_ray_image(orc_sim* s, void** ptr, size_t* bytes);
 /* The render passes' exp and log (Cody-Waite + Taylor; atanh series). */
 float orc_expf(float x);
 float orc_logf(float x);

@@ -111,6 +111,18 @@ class SsfrInfo(C.Structure):
 SSFR_BUF = {"eyeZ": 0, "rawZ": 1, "thick": 2, "image": 3, "bodyT": 4}
 
 
+class RayParams(C.Structure):
+    _fields_ = [
+        ("proj", C.c_float * 16), ("inv_view_proj", C.c_float * 16), ("inv_view", C.c_float * 16),
+        ("eye", C.c_float * 3), ("width", C.c_int32), ("height", C.c_int32), ("iso", C.c_double),
+        ("ior", C.c_double), ("absorption", C.c_double), ("transmit", C.c_double * 3),
+        ("thickness_steps", C.c_int32), ("floor_plane", C.c_int32), ("ground_reflection", C.c_double),
+        ("skin_width", C.c_double), ("roughness", C.c_double), ("sun_intensity", C.c_double),
+        ("sun_elevation", C.c_double), ("sun_azimuth", C.c_double), ("exposure", C.c_double),
+        ("debug", C.c_int32),
+    ]
+
+
 class Grid(C.Structure):
     _fields_ = [("box_min", C.c_float * 3), ("h", C.c_float), ("dim", C.c_int32 * 3)]
 

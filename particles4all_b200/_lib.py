@@ -81,6 +81,10 @@ SIGNATURES = {
     "p4a_ssfr_get_info": ([_vp, _vp], C.c_int),
     "p4a_ssfr_buffer": ([_vp, _i32, C.POINTER(_vp), C.POINTER(_sz)], C.c_int),
     "p4a_ssfr_read": ([_vp, _i32, _vp, _sz], C.c_int),
+    "p4a_default_ray_params": ([_vp], C.c_int),
+    "p4a_ray": ([_vp, _vp, _vp, _i32], C.c_int),
+    "p4a_ray_buffer": ([_vp, C.POINTER(_vp), C.POINTER(_sz), C.POINTER(_i32), C.POINTER(_i32)], C.c_int),
+    "p4a_ray_read": ([_vp, _vp, _sz], C.c_int),
 }
 
 _lib = None

@@ -39,12 +39,13 @@ const double kPi = 3.14159265358979323846;
 enum Phase {
   PH_DRAG, PH_KEY_COUNT, PH_SCAN, PH_FILL, PH_REORDER, PH_BODY_SEED, PH_LAMBDA, PH_DELTA,
   PH_BODY_MATCH, PH_XSPH_FINALIZE, PH_XSPH_NORMALS, PH_TENSION_FINALIZE, PH_ANISO, PH_IMPULSE,
-  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_SSFR, PH_COUNT, PH_END = PH_COUNT
+  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_SSFR, PH_RAY, PH_COUNT,
+  PH_END = PH_COUNT
 };
 const char* const kPhaseNames[PH_COUNT] = {
     "body_drag", "key_count", "scan", "fill", "reorder", "body_seed", "lambda", "delta",
     "body_match", "xsph_finalize", "xsph_normals", "tension_finalize", "aniso", "impulse",
-    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march", "ssfr"};
+    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march", "ssfr", "ray"};
 
 std::atomic<uint64_t> g_launches{0};
 }  // namespace
@@ -108,6 +109,9 @@ struct p4a_sim {
   int ssfrW = 0, ssfrH = 0, ssfrMapW = 0, ssfrMapH = 0, ssfrThW = 0, ssfrThH = 0, ssfrGen = 0;
   float4* ssfrBodies = nullptr;
   int ssfrBodyCap = 0;
+  uchar4* rayImage = nullptr;  // p4a_ray
+  size_t rayCap = 0;
+  int rayW = 0, rayH = 0;
   bool ready = false;
   // per-kernel timing (p4a_profile_*)
   bool prof = false;
@@ -161,7 +165,7 @@ int resolve_marks(p4a_sim* s) {
 // counts launches and, with profiling on, records the event that opens the interval.
 void mark(p4a_sim* s, int phase) {
   // the SSFR phase counts its own launches (several kernels per phase)
-  if (phase < PH_COUNT && phase != PH_STATS_CLEAR && phase != PH_SSFR) g_launches.fetch_add(1, std::memory_order_relaxed);
+  if (phase < PH_COUNT && phase != PH_STATS_CLEAR && phase != PH_SSFR && phase != PH_RAY) g_launches.fetch_add(1, std::memory_order_relaxed);
   if (!s->prof) return;
   if (s->evUsed == (int)s->evPool.size()) {
     cudaEvent_t e;
@@ -636,6 +640,7 @@ int p4a_destroy(p4a_sim* s) {
   if (s->meshVerts) cudaFree(s->meshVerts);
   free_list(s->ssfrAllocs);
   if (s->ssfrBodies) cudaFree(s->ssfrBodies);
+  if (s->rayImage) cudaFree(s->rayImage);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
@@ -1226,6 +1231,8 @@ int p4a_default_ssfr_params(p4a_ssfr_params* o) {
   return P4A_OK;
 }
 
+static int upload_bodies(p4a_sim* s, const float* bodies, int32_t bodyCount);
+
 int p4a_ssfr(p4a_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t bodyCount) {
   if (!s || !sp || sp->width < 1 || sp->height < 1 || sp->width > 16384 || sp->height > 16384 ||
       bodyCount < 0 || (bodyCount > 0 && !bodies) || sp->filter < 0 || sp->filter > 2 ||
@@ -1266,18 +1273,9 @@ int p4a_ssfr(p4a_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t
     s->ssfrH = q.height;
     s->ssfrGen++;
   }
-  if (bodyCount > s->ssfrBodyCap) {
-    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    if (s->ssfrBodies) cudaFree(s->ssfrBodies);
-    s->ssfrBodies = nullptr;
-    s->ssfrBodyCap = 0;
-    CUDA_TRY(s, cudaMalloc((void**)&s->ssfrBodies, (size_t)bodyCount * 6 * 16));
-    s->ssfrBodyCap = bodyCount;
-  }
-  if (bodyCount > 0) {
-    CUDA_TRY(s, cudaMemcpyAsync(s->ssfrBodies, bodies, (size_t)bodyCount * 6 * 16, cudaMemcpyHostToDevice,
-                                s->stream));
-    CUDA_TRY(s, cudaStreamSynchronize(s->stream));  // the caller's array may go away
+  {
+    const int rc = upload_bodies(s, bodies, bodyCount);
+    if (rc) return rc;
   }
   F.mapW = mapW;
   F.mapH = mapH;
@@ -1435,6 +1433,136 @@ int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes) {
   const int rc = p4a_ssfr_buffer(s, which, &p, &have);
   if (rc) return rc;
   if (bytes > have) return fail(s, P4A_ERR_ARG, "p4a_ssfr_read: %zu bytes asked, buffer holds %zu", bytes, have);
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return P4A_OK;
+}
+
+// Uploads the caller's packed bodies into the sim's body buffer (shared by the
+// render passes); waits, since the host array may go away.
+static int upload_bodies(p4a_sim* s, const float* bodies, int32_t bodyCount) {
+  if (bodyCount > s->ssfrBodyCap) {
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->ssfrBodies) cudaFree(s->ssfrBodies);
+    s->ssfrBodies = nullptr;
+    s->ssfrBodyCap = 0;
+    CUDA_TRY(s, cudaMalloc((void**)&s->ssfrBodies, (size_t)bodyCount * 6 * 16));
+    s->ssfrBodyCap = bodyCount;
+  }
+  if (bodyCount > 0) {
+    CUDA_TRY(s, cudaMemcpyAsync(s->ssfrBodies, bodies, (size_t)bodyCount * 6 * 16, cudaMemcpyHostToDevice,
+                                s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  }
+  return P4A_OK;
+}
+
+int p4a_default_ray_params(p4a_ray_params* o) {
+  if (!o) return P4A_ERR_ARG;
+  *o = p4a_ray_params{};
+  for (int k = 0; k < 4; k++) o->proj[k * 5] = o->inv_view_proj[k * 5] = o->inv_view[k * 5] = 1.0f;
+  o->width = 640;
+  o->height = 480;
+  o->iso = 0.4;  // RayMarch constructor defaults (src/ray.js:16-29), meshIso (src/main.js:320)
+  o->ior = 1.333;
+  o->absorption = 1.0;
+  o->transmit[0] = 0.35;
+  o->transmit[1] = 0.62;
+  o->transmit[2] = 0.78;
+  o->thickness_steps = 48;
+  o->floor_plane = 1;
+  o->ground_reflection = 0.0;
+  o->skin_width = 0.05;
+  o->roughness = 0.055;
+  o->sun_intensity = 3.0;
+  o->sun_elevation = 38.0;
+  o->sun_azimuth = 40.0;
+  o->exposure = 1.0;
+  o->debug = 0;
+  return P4A_OK;
+}
+
+int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t bodyCount) {
+  if (!s || !rp || rp->width < 1 || rp->height < 1 || rp->width > 16384 || rp->height > 16384 || bodyCount < 0 ||
+      (bodyCount > 0 && !bodies) || rp->thickness_steps < 0 || rp->thickness_steps > 4096)
+    return fail(s, P4A_ERR_ARG, "p4a_ray: invalid parameters");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "ray before reset");
+  if (s->meshDim[0] < 2 || !s->meshField[s->fieldSlot])
+    return fail(s, P4A_ERR_STATE, "ray needs the density field of p4a_mesh");
+  cudaSetDevice(s->device);
+  const size_t px = (size_t)rp->width * rp->height;
+  if (px > s->rayCap) {
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->rayImage) cudaFree(s->rayImage);
+    s->rayImage = nullptr;
+    s->rayCap = 0;
+    CUDA_TRY(s, cudaMalloc((void**)&s->rayImage, px * 4));
+    s->rayCap = px;
+  }
+  int rc = upload_bodies(s, bodies, bodyCount);
+  if (rc) return rc;
+  const p4a_ray_params& q = *rp;
+  RayParams R{};
+  memcpy(R.ivp, q.inv_view_proj, 64);
+  memcpy(R.iv, q.inv_view, 64);
+  const double kPiD = 3.14159265358979323846;
+  const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
+  const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};
+  const double sl = std::sqrt(sun[0] * sun[0] + sun[1] * sun[1] + sun[2] * sun[2]);
+  for (int k = 0; k < 3; k++) {
+    R.eye[k] = q.eye[k];
+    R.gridOrigin[k] = (float)s->meshOrigin;
+    R.boxMin[k] = 0.0f;
+    R.boxMax[k] = (float)s->params.box[k];
+    R.absorb[k] = (float)(q.absorption * -std::log(std::min(1.0, std::max(1e-3, q.transmit[k]))));
+    R.sunDir[k] = (float)(sun[k] / sl);
+    R.vertDim[k] = s->meshDim[k];
+  }
+  R.voxel = (float)s->meshVoxel;
+  R.iso = (float)q.iso;
+  R.ior = (float)q.ior;
+  R.skin = (float)q.skin_width;
+  R.sunIntensity = (float)q.sun_intensity;
+  R.roughness = (float)q.roughness;
+  R.exposure = (float)q.exposure;
+  R.groundReflection = (float)q.ground_reflection;
+  R.proj00 = q.proj[0];
+  R.proj11 = q.proj[5];
+  R.thickSteps = q.thickness_steps;
+  R.bodyCount = bodyCount;
+  R.floorPlane = q.floor_plane ? 1 : 0;
+  R.debug = q.debug;
+  R.width = q.width;
+  R.height = q.height;
+  const double deg[4] = {5.0, 10.0, 20.0, 40.0};
+  for (int k = 0; k < 4; k++) R.cosDeg[k] = (float)std::cos(deg[k] * kPiD / 180);
+  mark(s, PH_RAY);
+  launch_ray(R, s->meshField[s->fieldSlot], s->ssfrBodies, s->rayImage, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
+  s->rayW = q.width;
+  s->rayH = q.height;
+  return P4A_OK;
+}
+
+int p4a_ray_buffer(p4a_sim* s, void** dptr, size_t* bytes, int32_t* width, int32_t* height) {
+  if (!s || !dptr || !bytes) return P4A_ERR_ARG;
+  if (s->rayW == 0) return fail(s, P4A_ERR_STATE, "p4a_ray_buffer before p4a_ray");
+  *dptr = s->rayImage;
+  *bytes = (size_t)s->rayW * s->rayH * 4;
+  if (width) *width = s->rayW;
+  if (height) *height = s->rayH;
+  return P4A_OK;
+}
+
+int p4a_ray_read(p4a_sim* s, void* host, size_t bytes) {
+  if (!s || (!host && bytes)) return P4A_ERR_ARG;
+  void* p = nullptr;
+  size_t have = 0;
+  const int rc = p4a_ray_buffer(s, &p, &have, nullptr, nullptr);
+  if (rc) return rc;
+  if (bytes > have) return fail(s, P4A_ERR_ARG, "p4a_ray_read: %zu bytes asked, image holds %zu", bytes, have);
   cudaSetDevice(s->device);
   CUDA_TRY(s, cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, s->stream));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));

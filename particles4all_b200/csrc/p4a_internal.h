@@ -127,6 +127,19 @@ struct SsfrFrame {
 };
 void launch_ssfr(const SsfrFrame& f, cudaStream_t st);
 
+// Ray-march uniform (src/ray_wgsl.js:2-30, packed by src/ray.js:32-78; no
+// environment map, no rasterised-mesh surface), plus the image size and the
+// cosines of debug view 5's angle thresholds.
+struct RayParams {
+  float ivp[16], iv[16];
+  float eye[3], gridOrigin[3], boxMin[3], boxMax[3], absorb[3], sunDir[3];
+  float voxel, iso, ior, skin, sunIntensity, roughness, exposure, groundReflection, proj00, proj11;
+  int32_t vertDim[3], thickSteps, bodyCount, floorPlane, debug;
+  int32_t width, height;
+  float cosDeg[4];
+};
+void launch_ray(const RayParams& R, const float* field, const float4* bodies, uchar4* image, cudaStream_t st);
+
 // Device error word bits (set by kernels, read by the host at sync points).
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };
 

@@ -189,9 +189,29 @@ def default_ssfr():
     return out
 
 
+def default_ray():
+    """RayMarch's defaults (src/ray.js:16-29), iso 0.4, an identity camera and a
+    640 x 480 target."""
+    from ._lib import lib
+    s = _abi.RayParams()
+    lib().p4a_default_ray_params(C.byref(s))
+    out = {}
+    for name, ctype in _abi.RayParams._fields_:
+        v = getattr(s, name)
+        out[name] = list(v) if hasattr(ctype, "_length_") else v
+    return out
+
+
+def ray_struct(d):
+    return _fill(_abi.RayParams(), d)
+
+
 def ssfr_struct(d):
-    s = _abi.SsfrParams()
-    for name, ctype in _abi.SsfrParams._fields_:
+    return _fill(_abi.SsfrParams(), d)
+
+
+def _fill(s, d):
+    for name, ctype in type(s)._fields_:
         if name not in d:
             continue
         v = d[name]
@@ -199,7 +219,7 @@ def ssfr_struct(d):
             arr = getattr(s, name)
             vals = list(np.asarray(v, dtype=np.float64).ravel())
             if len(vals) != ctype._length_:
-                raise ValueError(f"ssfr {name}: {len(vals)} values, expected {ctype._length_}")
+                raise ValueError(f"{name}: {len(vals)} values, expected {ctype._length_}")
             for k, x in enumerate(vals):
                 arr[k] = x
         elif ctype in (C.c_int32,):

@@ -151,6 +151,27 @@ class Sim:
         w, h = (inf["thick_w"], inf["thick_h"]) if name == "thick" else (inf["map_w"], inf["map_h"])
         return out.view(np.float32).reshape(h, w)
 
+    def ray(self, rparams, bodies=None):
+        """RayMarch.draw (src/ray.js:30-97) on the density field of the last mesh();
+        returns nothing, read the image with ray_read()."""
+        from .params import ray_struct
+        rp = ray_struct(rparams)
+        if bodies is None or len(bodies) == 0:
+            ptr, count, keep = None, 0, None
+        else:
+            keep = np.ascontiguousarray(bodies, dtype=np.float32).reshape(-1, 24)
+            ptr, count = keep.ctypes.data, keep.shape[0]
+        check(self._L.p4a_ray(self._h, C.byref(rp), ptr, count), self._h, "ray")
+
+    def ray_read(self):
+        """The last ray() image, uint8 [height, width, 4]."""
+        p, nb, w, h = C.c_void_p(), C.c_size_t(), C.c_int32(), C.c_int32()
+        check(self._L.p4a_ray_buffer(self._h, C.byref(p), C.byref(nb), C.byref(w), C.byref(h)), self._h,
+              "ray_buffer")
+        out = np.empty((h.value, w.value, 4), np.uint8)
+        check(self._L.p4a_ray_read(self._h, out.ctypes.data, nb.value), self._h, "ray_read")
+        return out
+
     def mesh_info(self):
         i = _abi.MeshInfo()
         check(self._L.p4a_mesh_get_info(self._h, C.byref(i)), self._h, "mesh_info")

@@ -1,0 +1,127 @@
+"""CPU checks of the oracle's ray-marched surface (src/ray_wgsl.js): the distance to
+the iso surface (debug view 2) against a float64 march of the same trilinear field
+along each pixel's ray, and pixels that miss the field against the float64 sky /
+floor shading and tone map."""
+import math
+
+import numpy as np
+
+import oracle
+import render_f64
+from particles4all_b200 import configs
+from particles4all_b200.camera import Camera, frame_matrices
+from particles4all_b200.params import default_mesh, default_ray
+
+
+def block_with_field():
+    p, sc = configs.dam_break_32k(side=8)
+    o = oracle.OracleSim()
+    o.reset_scene(p, sc)
+    o.step(1 / 60)
+    m = default_mesh()
+    m["resolution"] = 40
+    o.mesh(m)
+    return o, p
+
+
+def ray_params(w, h, **over):
+    cam = Camera()
+    cam.target = [2.0, 1.5, 2.0]
+    cam.az, cam.el, cam.dist = -0.6, 0.45, 9.0
+    m = frame_matrices(cam, w, h)
+    rp = default_ray()
+    rp.update({k: m[k] for k in ("proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp.update(over)
+    return rp, m
+
+
+def field_hit_f64(o, p, ro, rd, iso):
+    """First iso crossing of the trilinear field along ro + t rd inside the field's
+    volume, by fine sampling and bisection in float64; None on a miss."""
+    info_box = np.array(p["box"], np.float64)
+    voxel = info_box.max() / 40
+    dim = np.array([int(math.ceil(b / voxel)) + 3 for b in info_box])
+    f = o.buffer("meshField").astype(np.float64).reshape(dim[2], dim[1], dim[0])
+    origin = -voxel
+
+    def field(t):
+        g = (ro + rd * t - origin) / voxel
+        c = np.floor(g).astype(int)
+        u = np.clip(g - c, 0, 1)
+
+        def F(x, y, z):
+            return f[min(max(z, 0), dim[2] - 1), min(max(y, 0), dim[1] - 1), min(max(x, 0), dim[0] - 1)]
+        x, y, z = c
+        v = 0.0
+        for dz in (0, 1):
+            for dy in (0, 1):
+                for dx in (0, 1):
+                    w = (u[0] if dx else 1 - u[0]) * (u[1] if dy else 1 - u[1]) * (u[2] if dz else 1 - u[2])
+                    v += w * F(x + dx, y + dy, z + dz)
+        return v - iso
+
+    lo, hi = origin, origin + voxel * (dim - 1)
+    with np.errstate(divide="ignore"):
+        inv = 1.0 / rd
+    a, b = (lo - ro) * inv, (hi - ro) * inv
+    t0, t1 = np.minimum(a, b).max(), np.maximum(a, b).min()
+    if not t1 > max(t0, 0):
+        return None
+    step = voxel * 1e-3
+    t = max(t0, 0) + 1e-5
+    prev = field(t)
+    while t < t1:
+        tn = min(t + step, t1)
+        cur = field(tn)
+        if prev == 0 or (prev < 0) != (cur < 0):
+            lo_t, hi_t = t, tn
+            for _ in range(60):
+                mid = 0.5 * (lo_t + hi_t)
+                if (field(mid) < 0) == (prev < 0):
+                    lo_t = mid
+                else:
+                    hi_t = mid
+            return 0.5 * (lo_t + hi_t)
+        t, prev = tn, cur
+    return None
+
+
+def test_surface_distance_against_float64(built):
+    o, p = block_with_field()
+    w, h = 40, 30
+    rp, m = ray_params(w, h, debug=2)
+    img = o.ray(rp)
+    hits = misses = 0
+    for py in range(0, h, 3):
+        for px in range(0, w, 3):
+            ro, rd = render_f64.pixel_ray(m, w, h, px, py, from_eye=True)
+            t = field_hit_f64(o, p, ro, rd, rp["iso"])
+            if t is None:
+                assert (img[py, px, :3] == 0).all(), (px, py, img[py, px])
+                misses += 1
+                continue
+            frac = t - math.floor(t)
+            if min(frac, 1 - frac) < 0.01 or min(t * 0.1 % 1, 1 - t * 0.1 % 1) < 0.01:
+                continue  # fract() wraps within the tolerance
+            want = render_f64.rgba8([frac, (t * 0.1) % 1.0, 0.0])
+            assert np.abs(img[py, px, :3] - want).max() <= 2, (px, py, img[py, px], want, t)
+            hits += 1
+    assert hits > 10 and misses > 10
+
+
+def test_background_against_float64(built):
+    o, p = block_with_field()
+    w, h = 48, 36
+    rp, m = ray_params(w, h)
+    img = o.ray(rp)
+    dbg = o.ray(dict(rp, debug=2))
+    checked = 0
+    for py in range(0, h, 4):
+        for px in range(0, w, 5):
+            if dbg[py, px, :3].any():
+                continue  # the ray met the surface
+            ro, rd = render_f64.pixel_ray(m, w, h, px, py, from_eye=True)
+            want = render_f64.rgba8(render_f64.background(rp, ro, rd), rp["exposure"])
+            assert np.abs(img[py, px, :3] - want).max() <= 1, (px, py, img[py, px], want)
+            checked += 1
+    assert checked > 20

@@ -9,6 +9,7 @@ import math
 import numpy as np
 
 import oracle
+import render_f64
 from particles4all_b200 import configs
 from particles4all_b200.camera import Camera, frame_matrices
 from particles4all_b200.params import default_aniso, default_ssfr
@@ -114,55 +115,6 @@ def test_particle_pair_depth_and_thickness(built):
     assert np.count_nonzero(want) > 50
 
 
-def background_f64(m, sp, px, py):
-    """float64 transcription of src/ssfr_composite_wgsl.js skyColor / floorColor /
-    background and tonemap for a pixel that sees neither fluid nor bodies."""
-    w, h = sp["width"], sp["height"]
-    nx = (px + 0.5) / w * 2 - 1
-    ny = 1 - (py + 0.5) / h * 2
-    ivp = np.array(m["inv_view_proj"], np.float64).reshape(4, 4).T
-    nh = ivp @ np.array([nx, ny, -1, 1])
-    fh = ivp @ np.array([nx, ny, 1, 1])
-    ro = nh[:3] / nh[3]
-    rd = fh[:3] / fh[3] - ro
-    rd /= np.linalg.norm(rd)
-    el, az = math.radians(sp["sun_elevation"]), math.radians(sp["sun_azimuth"])
-    sun = np.array([math.cos(el) * math.sin(az), math.sin(el), math.cos(el) * math.cos(az)])
-    sun /= np.linalg.norm(sun)
-    haze = np.array([0.62, 0.74, 0.90])
-
-    def smooth(e0, e1, x):
-        t = min(max((x - e0) / (e1 - e0), 0.0), 1.0)
-        return t * t * (3 - 2 * t)
-
-    def sky(d):
-        hh = min(max(d[1], 0.0), 1.0)
-        c = haze * (1 - smooth(0, 0.16, hh)) + np.array([0.25, 0.48, 0.85]) * smooth(0, 0.16, hh)
-        t = smooth(0.10, 0.85, hh)
-        c = c * (1 - t) + np.array([0.09, 0.28, 0.72]) * t
-        s = max(float(d @ sun), 0.0)
-        return c + np.array([1.0, 0.96, 0.88]) * s ** 3000 * 14 + np.array([1.0, 0.92, 0.78]) * s ** 24 * 0.2
-
-    def floor_col(p):
-        g = np.abs(p[[0, 2]] - np.floor(p[[0, 2]]) - 0.5)
-        line = 1 - smooth(0, 0.015, g.min())
-        c = np.array([0.30, 0.305, 0.315]) * (1 - line * 0.8) + np.array([0.50, 0.51, 0.52]) * line * 0.8
-        fs = math.floor(p[0]) + math.floor(p[2])
-        chk = fs - 2 * math.floor(fs * 0.5)
-        return c * (0.88 * (1 - chk) + 1.10 * chk)
-
-    if rd[1] < -1e-4 and (0 - ro[1]) / rd[1] > 0:
-        t = (0 - ro[1]) / rd[1]
-        fade = 1 - math.exp(-0.02 * t)
-        col = floor_col(ro + rd * t) * (1 - fade) + haze * fade
-    else:
-        col = sky(rd)
-    col = col * sp["exposure"]
-    col = col / (1 + col.max() * 0.35)
-    col = col ** (1 / 2.2)
-    return np.floor(np.clip(col, 0, 1) * 255 + 0.5)
-
-
 def test_composite_background_against_float64(built):
     o, p = pair_sim()
     sp, m = camera_for(p, 64, 48, az=0.6, el=0.25, dist=9.0)
@@ -175,7 +127,8 @@ def test_composite_background_against_float64(built):
         for px in range(0, 64, 7):
             if z[py, px] > -1e3:
                 continue
-            want = background_f64(m, sp, px, py)
+            ro, rd = render_f64.pixel_ray(m, sp["width"], sp["height"], px, py)
+            want = render_f64.rgba8(render_f64.background(sp, ro, rd), sp["exposure"])
             assert np.abs(img[py, px, :3].astype(np.float64) - want).max() <= 1.0, (px, py, img[py, px], want)
             checked += 1
     assert checked > 30
