@@ -55,6 +55,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
+    ap.add_argument("--no-render", action="store_true", help="skip the mesh / SSFR / ray-march timings")
     ap.add_argument("--mix-frames", type=int, default=10)
     ap.add_argument("--only-mix", choices=["batched", "plain"], default=None,
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
@@ -306,6 +307,40 @@ def served_bench(seconds, budget_gb):
     return out
 
 
+def render_bench(sim, params, stream, width=1920, height=1080, reps=5):
+    """Device ms per call of the passes that consume the step's buffers, on the
+    scene's current state: the surface mesh (resolution 128), the screen-space
+    fluid rendering and the ray march at width x height (camera framing the box)."""
+    import torch
+    from particles4all_b200 import default_mesh, default_ray, default_ssfr
+    from particles4all_b200.camera import Camera, frame_matrices
+    m = frame_matrices(Camera().frame(params["box"]), width, height)
+    sp = default_ssfr()
+    sp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp = default_ray()
+    rp.update({k: m[k] for k in ("proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    mp = default_mesh()
+
+    def timed(fn):
+        for _ in range(2):
+            fn()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+        for e0, e1 in ev:
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+    out = {"width": width, "height": height, "particles": sim.info()["n"],
+           "mesh_ms": timed(lambda: sim.mesh(mp, wait=False)),
+           "ssfr_ms": timed(lambda: sim.ssfr(sp)),
+           "ray_ms": timed(lambda: sim.ray(rp)),
+           "what": "device ms per call (median of 5): p4a_mesh at resolution 128, p4a_ssfr and p4a_ray at "
+                   f"{width}x{height} on the scene after the timed steps (anisotropic pass already done)"}
+    out["mesh_triangles"] = sim.mesh(mp)
+    return out
+
+
 def _launches():
     from particles4all_b200 import _lib
     return _lib.lib().p4a_kernel_launches()
@@ -548,6 +583,10 @@ def run_ours(args):
                "what": "per step: live pos+vel written from pinned host, Sim.step (+ hose, + aniso as the "
                        "workload has them), pos+vel+stats read back to pinned host"}
 
+    render = None
+    if world == 1 and aniso and not args.no_render:
+        render = render_bench(sim, params, stream)
+
     mix = None
     if world == 1 and not args.no_mix:
         mix = batched_mix_bench(args.mix_frames, 3)
@@ -580,6 +619,7 @@ def run_ours(args):
             "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": launches,
             "batched_mix": mix,
+            "render": render,
             "served": served,
             "clocks": clocks.summary(w0, w1),
             "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")},

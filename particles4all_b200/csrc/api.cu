@@ -269,6 +269,8 @@ int alloc_cells(p4a_sim* s) {
   if ((rc = dalloc(s, s->cellAllocs, &s->d.cellStart, (size_t)s->nCells + 2))) return rc;
   if ((rc = dalloc(s, s->cellAllocs, &s->d.scanState, (size_t)scan_tiles(s->nCells)))) return rc;
   if ((rc = dalloc(s, s->cellAllocs, &s->d.scanTicket, 4))) return rc;
+  s->d.cellStride = (uint32_t)s->nCells + 1;
+  if ((rc = dalloc(s, s->cellAllocs, &s->d.cellDisp, (size_t)kDispSlots * s->d.cellStride))) return rc;
   return P4A_OK;
 }
 
@@ -336,7 +338,7 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbList, cap * kListCap)) ||
       (rc = dalloc(s, L, &s->d.nbCount, cap)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
-      (rc = dalloc(s, L, &s->d.disp, kDispSlots)))
+      (rc = dalloc(s, L, &s->d.disp, kDispSlots)) || (rc = dalloc(s, L, &s->d.nbRef, cap)))
     return rc;
   s->d.cap = (uint32_t)cap;
   if ((rc = alloc_cells(s))) return rc;

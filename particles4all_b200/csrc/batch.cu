@@ -678,6 +678,7 @@ int alloc_arenas(p4a_batch* b) {
        (rc = balloc(b, &d.normal, P)) || (rc = balloc(b, &d.key, P)) || (rc = balloc(b, &d.rank, P)) ||
        (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbList, P * kListCap)) || (rc = balloc(b, &d.nbCount, P)) ||
        (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
+       (rc = balloc(b, &d.cellDisp, (int64_t)kDispSlots * Cc)) || (rc = balloc(b, &d.nbRef, P)) ||
        (rc = balloc(b, &d.cellCount, Cc)) ||
        (rc = balloc(b, &d.cellStart, Cc)) || (rc = balloc(b, &d.bcellStart, Cc)) ||
        (rc = balloc(b, &d.scanState, b->scanTilesCap)) || (rc = balloc(b, &d.scanTicket, 4)) ||
@@ -730,6 +731,7 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
     return rc;
   }
   b->d.cap = (uint32_t)P;
+  b->d.cellStride = (uint32_t)Cc;
   b->partA.init(P);
   b->cellA.init(Cc);
   b->boundA.init(b->cfg.max_boundary);

@@ -211,7 +211,10 @@ __device__ __forceinline__ void body_match_body(const SimParams& P, const DevSce
     const F3 o = add3(cen, p);
     pred[i] = make_float4(o.x, o.y, o.z, 1.0f);
     // the projection moves the particle from this iteration's input position
-    if (it < kDispSlots) record_displacement(d, P, it, sub3(o, xyz(__ldg(&d.pred[L ^ (it & 1)][i]))));
+    if (it < kDispSlots) {
+      record_displacement(d, P, it, sub3(o, xyz(__ldg(&d.pred[L ^ (it & 1)][i]))));
+      record_cell_displacement(d, P, it, o, xyz(__ldg(&d.nbRef[i])));
+    }
     if (last) {
       const float4 p0 = __ldg(&d.pos[L][i]);
       d.vel[L ^ 1][i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,

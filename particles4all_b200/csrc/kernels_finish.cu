@@ -74,10 +74,8 @@ __device__ __forceinline__ void block_stats(const SimParams& P, bool act, float 
 __device__ __forceinline__ uint32_t finish_list(const SimParams& P, const DevScene& d, const RowWalk& w,
                                                 uint32_t i, F3 pi, const float4* __restrict__ pred,
                                                 const uint32_t* __restrict__ cs) {
-  if (list_reusable(P, d, (int)P.iters, i, cell_index(P, w.c))) {
-    const uint32_t c = __ldg(&d.nbCount[i]);
-    if (c != kListOverflow && !(c & kHasBound)) return c;
-  }
+  const uint32_t c = __ldg(&d.nbCount[i]);
+  if (!(c & kHasBound) && list_reusable(P, d, (int)P.iters, i, w, cell_index(P, w.c), c)) return c;
   return build_list<false>(P, w, i, pi, pred, cs, nullptr, nullptr, d.nbList, d.cap, P.h2);
 }
 

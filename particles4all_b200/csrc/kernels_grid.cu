@@ -40,7 +40,14 @@ __device__ __forceinline__ void key_count_body(const SimParams& P, const DevScen
     const int leader = __ffs(peers) - 1;
     const uint32_t lt = peers & ((1u << lane) - 1u);
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
+    if (lane == leader) {
+      base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
+      // this substep's per-cell displacement slots start at zero for every occupied cell
+      if (d.cellDisp) {
+        const uint32_t slots = min(P.iters, (uint32_t)kDispSlots);
+        for (uint32_t t = 0; t < slots; t++) d.cellDisp[(size_t)t * d.cellStride + k] = 0.0f;
+      }
+    }
     base = __shfl_sync(peers, base, leader);
     d.key[i] = k;
     d.rank[i] = base + (uint32_t)__popc(lt);

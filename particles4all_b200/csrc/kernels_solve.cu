@@ -10,12 +10,13 @@
 // lambda builds each particle's neighbour list (neighbours.cuh) with the radius
 // h + skin and stores it; delta runs on the same positions and walks the same
 // list. The list also serves later iterations of the substep: every delta (and
-// the rigid projection) records the largest displacement of its iteration, and an
-// iteration reuses the list of the last rebuild while the summed displacements
-// since then stay within skin / 2 (so every pair now within h was within h + skin
-// then) and the particle is still in the cell it was in then (so its candidate
-// rows are the same). Every pass re-tests r^2 < h^2 on each listed candidate, so
-// the visited neighbours and their order are exactly the reference's either way.
+// the rigid projection) records the largest displacement of its iteration and the
+// largest displacement from the substep's start positions, and a particle reuses
+// its list while those bound every particle's movement since the list was built
+// by skin / 2 (so every pair now within h was within h + skin then) and it is
+// still in the cell it was in then (so its candidate rows are the same); see
+// list_reusable. Every pass re-tests r^2 < h^2 on each listed candidate, so the
+// visited neighbours and their order are exactly the reference's either way.
 // The last delta of a substep also writes velFromPos (src/wgsl.js:72-83) for every
 // particle into the non-live velocity copy; body particles are overwritten by the
 // rigid projection that follows.
@@ -38,14 +39,13 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   const uint32_t cap = d.cap;
   const F3 pi = xyz(__ldg(&pred[i]));
   const RowWalk w(P, pi);
-  // reuse the list of the last rebuild while the displacement bound allows
+  // reuse the stored list while the displacement bounds allow
   const uint32_t cell = cell_index(P, w.c);
-  const bool reuse = list_reusable(P, d, it, i, cell);
-  uint32_t count;
-  if (reuse) {
-    count = __ldg(&d.nbCount[i]);
-  } else {
+  if (it == 0) d.nbRef[i] = make_float4(pi.x, pi.y, pi.z, 0.0f);  // the substep's start positions
+  uint32_t count = it > 0 ? __ldg(&d.nbCount[i]) : kListOverflow;
+  if (!list_reusable(P, d, it, i, w, cell, count)) {
     count = build_list<true>(P, w, i, pi, pred, cs, bcs, d.bpos, d.nbList, cap, P.skinH2);
+    if (count != kListOverflow) count |= (uint32_t)it << kBuildShift;
     d.nbCount[i] = count;
     d.nbCell[i] = cell;
   }
@@ -147,7 +147,10 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   o.y = fminf(fmaxf(o.y, P.clampMin[1]), P.clampMax[1]);
   o.z = fminf(fmaxf(o.z, P.clampMin[2]), P.clampMax[2]);
   predOut[i] = make_float4(o.x, o.y, o.z, 1.0f);
-  if (it < kDispSlots) record_displacement(d, P, it, sub3(o, pi));
+  if (it < kDispSlots) {
+    record_displacement(d, P, it, sub3(o, pi));
+    record_cell_displacement(d, P, it, o, xyz(__ldg(&d.nbRef[i])));
+  }
   if (it == (int)P.iters - 1) {  // velFromPos into the non-live velocity copy
     const float4 p0 = __ldg(&d.pos[L][i]);
     d.vel[L ^ 1][i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,

@@ -32,6 +32,7 @@ constexpr uint32_t kListOverflow = 0xffffffffu;  // count of a particle whose li
 constexpr uint32_t kBoundTag = 0x80000000u;      // entry = kBoundTag | boundary sample index
 constexpr uint32_t kHasBound = 0x40000000u;      // count flag: the list holds boundary samples
 constexpr uint32_t kCountMask = 0x0000ffffu;
+constexpr int kBuildShift = 16;                  // count bits 16-19: the iteration that built the list
 
 // Row r = 3*(dz+1) + (dy+1), the reference's dz-outer, dy-inner order.
 struct RowWalk {
@@ -106,26 +107,47 @@ __device__ __forceinline__ uint32_t build_list(const SimParams& P, const RowWalk
   return c > kListCap ? kListOverflow : c | flags;
 }
 
-// Whether particle i, now in `cell`, may walk the list that lambda built at the
-// last rebuild before iteration `it` of this substep (it = iters: the positions
-// after the last iteration): the summed largest displacements of the iterations
-// since that rebuild stay within skin / 2 and the particle is still in the cell
-// the list was built in. An iteration that rebuilt is one whose own check failed,
-// which every particle sees alike up to the cell test.
+// Whether particle i, now in `cell`, may walk its stored list before iteration `it`
+// of this substep (it = iters: the positions after the last iteration). The list
+// was built at iteration b (its count word's bits 16-19) from the positions then,
+// with radius h + skin, in the cell recorded in nbCell. It still holds every pair
+// now within h when the particle is in the same cell (same candidate rows) and
+// every candidate (the particles sorted into the block's cells) and the particle
+// itself moved at most skin / 2 since iteration b, by either bound:
+//  - S: the sum of the iterations' largest single-iteration displacements since b
+//    over the whole scene (disp[t], recorded by every delta and rigid projection);
+//  - V: per block cell, the largest displacement of the cell's particles from the
+//    substep's start positions now, plus the same at iteration b (cellDisp[t] after
+//    iteration t), since |p(now) - p(b)| <= |p(now) - ref| + |p(b) - ref|.
+// V is local: a fast particle elsewhere in the scene does not force this list to
+// be rebuilt.
 __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene& d, int it, uint32_t i,
-                                              uint32_t cell) {
-  if (it <= 0 || it >= kDispSlots) return false;
+                                              const RowWalk& w, uint32_t cell, uint32_t countWord) {
+  if (it <= 0 || it >= kDispSlots || countWord == kListOverflow) return false;
+  if (__ldg(&d.nbCell[i]) != cell) return false;
+  const int b = (int)((countWord >> kBuildShift) & 0xfu);
+  if (b >= it) return false;
   const float* disp = d.disp + (size_t)P.slot * kDispSlots;
-  int ref = 0;
-  float D = 0.0f;
-  for (int t = 0; t < it; t++) {
-    D += __ldg(&disp[t]);
-    if (D * 1.00001f > P.skinHalf) {  // iteration t + 1 rebuilt
-      ref = t + 1;
-      D = 0.0f;
+  float S = 0.0f;
+  for (int t = b; t < it; t++) S += __ldg(&disp[t]);
+  if (S * 1.00001f <= P.skinHalf) return true;
+  const float* vNow = d.cellDisp + (size_t)(it - 1) * d.cellStride + P.cOff;
+  const float* vB = b > 0 ? d.cellDisp + (size_t)(b - 1) * d.cellStride + P.cOff : nullptr;
+  // the particle's own sort cell (the cell of its start position) may lie outside
+  // the block when it moved more than a cell since the sort
+  const I3 a = cell_of(P, xyz(__ldg(&d.nbRef[i])));
+  const uint32_t ac = cell_index(P, a);
+  float V = __ldg(&vNow[ac]) + (vB ? __ldg(&vB[ac]) : 0.0f);
+#pragma unroll 1
+  for (int r = 0; r < kRows; r++) {
+    const int rb = w.row_base(P, r);
+    if (rb < 0) continue;
+    for (int x = w.x0; x <= w.x1; x++) {
+      const float v = __ldg(&vNow[rb + x]) + (vB ? __ldg(&vB[rb + x]) : 0.0f);
+      V = fmaxf(V, v);
     }
   }
-  return ref < it && __ldg(&d.nbCell[i]) == cell;
+  return V * 1.00001f <= P.skinHalf;
 }
 
 // Phase 2 over a list of `count` entries: fluid(j) for a fluid entry, bound(k) for

@@ -183,6 +183,10 @@ struct DevScene {
   uint32_t* nbCount;    // [cap] list length, or kListOverflow
   uint32_t* nbCell;     // [cap] cell index lambda's list was built in
   float* disp;          // [slots][kDispSlots] max |dp| of each iteration of the substep
+  float* cellDisp;      // [kDispSlots][cellStride] per sort cell: max |p - nbRef| of its particles
+                        // after each iteration
+  uint32_t cellStride;  // cells per cellDisp slot
+  float4* nbRef;        // [cap] positions at the start of the substep's iterations
   uint32_t cap;         // particle capacity (stride of nbList)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };

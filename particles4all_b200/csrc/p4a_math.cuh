@@ -118,5 +118,19 @@ __device__ __forceinline__ void record_displacement(const DevScene& d, const Sim
   if ((threadIdx.x & 31) == (unsigned)(__ffs(am) - 1))
     atomicMax(reinterpret_cast<unsigned int*>(d.disp + (size_t)P.slot * kDispSlots + it), m);
 }
+// The particle's displacement from its substep start position `ref` into the slot of
+// iteration `it` of its sort cell (the cell of `ref`, which is the position the
+// sort binned it by); lanes with the same cell combine into one atomic.
+__device__ __forceinline__ void record_cell_displacement(const DevScene& d, const SimParams& P, int it, F3 p,
+                                                         F3 ref) {
+  const F3 dp = sub3(p, ref);
+  const float len = sqrtf(dot3(dp, dp));
+  const uint32_t c = P.cOff + cell_index(P, cell_of(P, ref));
+  const unsigned am = __activemask();
+  const unsigned peers = __match_any_sync(am, c);
+  const uint32_t m = __reduce_max_sync(peers, __float_as_uint(len));
+  if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1))
+    atomicMax(reinterpret_cast<unsigned int*>(d.cellDisp + (size_t)it * d.cellStride + c), m);
+}
 
 }  // namespace p4a
