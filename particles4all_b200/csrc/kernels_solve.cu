@@ -29,9 +29,11 @@
 
 namespace p4a {
 
+// Called by all 32 lanes of a warp (lanes past the scene's end only take part in the
+// warp's list builds).
 __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
-  if (li >= P.n) return;
-  const uint32_t i = P.pOff + li;
+  const bool act = li < P.n;
+  const uint32_t i = P.pOff + (act ? li : 0u);
   const int L = (int)P.parity ^ 1;
   const float4* __restrict__ pred = d.pred[L ^ (it & 1)];
   const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
@@ -41,14 +43,16 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   const RowWalk w(P, pi);
   // reuse the stored list while the displacement bounds allow
   const uint32_t cell = cell_index(P, w.c);
-  if (it == 0) d.nbRef[i] = make_float4(pi.x, pi.y, pi.z, 0.0f);  // the substep's start positions
-  uint32_t count = it > 0 ? __ldg(&d.nbCount[i]) : kListOverflow;
-  if (!list_reusable(P, d, it, i, w, cell, count)) {
-    count = build_list<true>(P, w, i, pi, pred, cs, bcs, d.bpos, d.nbList, cap, P.skinH2);
+  if (it == 0 && act) d.nbRef[i] = make_float4(pi.x, pi.y, pi.z, 0.0f);  // the substep's start positions
+  uint32_t count = it > 0 && act ? __ldg(&d.nbCount[i]) : kListOverflow;
+  const bool need = act && !list_reusable(P, d, it, i, w, cell, count);
+  count = build_lists_warp<true>(P, need, w, i, pi, pred, cs, bcs, d.bpos, d.nbList, cap, P.skinH2, count);
+  if (need) {
     if (count != kListOverflow) count |= (uint32_t)it << kBuildShift;
     d.nbCount[i] = count;
     d.nbCell[i] = cell;
   }
+  if (!act) return;
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;

@@ -107,6 +107,98 @@ __device__ __forceinline__ uint32_t build_list(const SimParams& P, const RowWalk
   return c > kListCap ? kListOverflow : c | flags;
 }
 
+// build_list for one particle (iL, piL, its row walk wL) by all 32 lanes of a warp:
+// lane k tests candidate base + k of each row, and a ballot orders the appends, so
+// the list (entries, order, count, flags) is the one build_list writes.
+template <bool B>
+__device__ __forceinline__ uint32_t build_list_coop(const SimParams& P, const RowWalk& wL, uint32_t iL, F3 piL,
+                                                    const float4* __restrict__ pred,
+                                                    const uint32_t* __restrict__ cs,
+                                                    const uint32_t* __restrict__ bcs,
+                                                    const float4* __restrict__ bpos, uint32_t* __restrict__ list,
+                                                    uint32_t cap, float r2lim) {
+  const uint32_t lane = threadIdx.x & 31u, below = (1u << lane) - 1u;
+  uint32_t c = 0, flags = 0u;
+#pragma unroll 1
+  for (int r = 0; r < kRows; r++) {
+    const int rb = wL.row_base(P, r);
+    if (rb < 0) continue;
+    const uint32_t b = __ldg(&cs[rb + wL.x0]);
+    const uint32_t e = min(__ldg(&cs[rb + wL.x1 + 1]), P.pEnd);
+    for (uint32_t base = b; base < e; base += 32u) {
+      const uint32_t j = base + lane;
+      bool in = false;
+      if (j < e && j != iL) {
+        const F3 dd = sub3(piL, xyz(__ldg(&pred[j])));
+        in = dot3(dd, dd) < r2lim;
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, in);
+      if (in) {
+        const uint32_t pos = c + (uint32_t)__popc(m & below);
+        if (pos < kListCap) list[(size_t)pos * cap + iL] = j;
+      }
+      c += (uint32_t)__popc(m);
+    }
+    if constexpr (B) {
+      if (P.nBoundary > 0u) {
+        const uint32_t bb = __ldg(&bcs[rb + wL.x0]), be = __ldg(&bcs[rb + wL.x1 + 1]);
+        for (uint32_t base = bb; base < be; base += 32u) {
+          const uint32_t k = base + lane;
+          bool in = false;
+          if (k < be) {
+            const F3 dd = sub3(piL, xyz(__ldg(&bpos[k])));
+            in = dot3(dd, dd) < r2lim;
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, in);
+          if (in) {
+            const uint32_t pos = c + (uint32_t)__popc(m & below);
+            if (pos < kListCap) list[(size_t)pos * cap + iL] = kBoundTag | k;
+          }
+          if (m) flags = kHasBound;
+          c += (uint32_t)__popc(m);
+        }
+      }
+    }
+  }
+  return c > kListCap ? kListOverflow : c | flags;
+}
+
+// The lanes of a warp that `need` a new list get one; all 32 lanes must call.
+// When few lanes need one, the whole warp builds each of their lists in turn
+// (build_list_coop), instead of letting the warp wait while those lanes test
+// their ~216 candidates one by one; when many do, each lane builds its own.
+// Returns the lane's new count word, or `current` for lanes that need none.
+constexpr int kCoopLanes = 12;
+template <bool B>
+__device__ __forceinline__ uint32_t build_lists_warp(const SimParams& P, bool need, const RowWalk& w, uint32_t i,
+                                                     F3 pi, const float4* __restrict__ pred,
+                                                     const uint32_t* __restrict__ cs,
+                                                     const uint32_t* __restrict__ bcs,
+                                                     const float4* __restrict__ bpos, uint32_t* __restrict__ list,
+                                                     uint32_t cap, float r2lim, uint32_t current) {
+  const unsigned needMask = __ballot_sync(0xffffffffu, need);
+  if (needMask == 0u) return current;
+  if (__popc(needMask) > kCoopLanes) return need ? build_list<B>(P, w, i, pi, pred, cs, bcs, bpos, list, cap, r2lim)
+                                                 : current;
+  const int lane = (int)(threadIdx.x & 31u);
+  uint32_t out = current;
+  for (unsigned m = needMask; m != 0u; m &= m - 1u) {
+    const int L = __ffs(m) - 1;
+    RowWalk wL = w;
+    wL.c.x = __shfl_sync(0xffffffffu, w.c.x, L);
+    wL.c.y = __shfl_sync(0xffffffffu, w.c.y, L);
+    wL.c.z = __shfl_sync(0xffffffffu, w.c.z, L);
+    wL.x0 = __shfl_sync(0xffffffffu, w.x0, L);
+    wL.x1 = __shfl_sync(0xffffffffu, w.x1, L);
+    const uint32_t iL = __shfl_sync(0xffffffffu, i, L);
+    const F3 piL = {__shfl_sync(0xffffffffu, pi.x, L), __shfl_sync(0xffffffffu, pi.y, L),
+                    __shfl_sync(0xffffffffu, pi.z, L)};
+    const uint32_t cnt = build_list_coop<B>(P, wL, iL, piL, pred, cs, bcs, bpos, list, cap, r2lim);
+    if (lane == L) out = cnt;
+  }
+  return out;
+}
+
 // Whether particle i, now in `cell`, may walk its stored list before iteration `it`
 // of this substep (it = iters: the positions after the last iteration). The list
 // was built at iteration b (its count word's bits 16-19) from the positions then,
