@@ -105,6 +105,19 @@ def peaks():
         return 6650.0, "fallback"
 
 
+def committed_issue(kernel, wl):
+    """Issue-slot utilisation (smsp__issue_active, pct of peak) of the kernel's
+    committed ncu summary: the roof of an issue- and latency-bound pass."""
+    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{wl}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("issue_active_pct:"):
+                return float(line.split(":", 1)[1].split()[0]) / 100.0
+    except (OSError, ValueError):
+        pass
+    return None
+
+
 def committed_traffic(kernel, wl):
     """DRAM bytes per launch from the committed ncu summary of this kernel and workload."""
     path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{wl}.txt")
@@ -525,6 +538,9 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": committed_traffic(name, args.workload),
                 "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
+                "issue_frac_ncu": committed_issue(name, args.workload),
+                "note": "the neighbour passes are bound by instruction issue and load latency, not HBM: "
+                        "issue_frac_ncu is the kernel's issue-slot utilisation from its committed ncu summary",
                 "avg_launch_us": avg_s * 1e6,
                 "kernels": {k: kernel_line(k, v) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
 
