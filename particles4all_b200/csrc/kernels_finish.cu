@@ -68,14 +68,14 @@ __device__ __forceinline__ void block_stats(const SimParams& P, bool act, float 
 }
 
 // The neighbour list of the finishing passes (positions after the last Jacobi
-// iteration): lambda's list when the displacement bound still covers it and it
-// holds no boundary samples (which these passes do not visit), else a new list
-// with radius h, stored in nbList.
+// iteration): lambda's list when the displacement bound still covers it (its
+// boundary samples are skipped by the walk: these passes have no boundary terms),
+// else a new list with radius h, stored in nbList.
 __device__ __forceinline__ uint32_t finish_list(const SimParams& P, const DevScene& d, const RowWalk& w,
                                                 uint32_t i, F3 pi, const float4* __restrict__ pred,
                                                 const uint32_t* __restrict__ cs) {
   const uint32_t c = __ldg(&d.nbCount[i]);
-  if (!(c & kHasBound) && list_reusable(P, d, (int)P.iters, i, w, cell_index(P, w.c), c)) return c;
+  if (list_reusable(P, d, (int)P.iters, i, w, cell_index(P, w.c), c)) return c;
   return build_list<false>(P, w, i, pi, pred, cs, nullptr, nullptr, d.nbList, d.cap, P.h2);
 }
 
