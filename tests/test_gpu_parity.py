@@ -233,6 +233,29 @@ def test_edge_cases():
     assert g.step(10.0) == 8 * 4 and g.info()["time_bank"] == 0
 
 
+def test_crowded_lists_take_the_direct_walk():
+    """A cluster far denser than rest density (spacing 0.15 h): every particle has
+    more than the list capacity (96) of candidates within h + skin, so lambda,
+    delta and the finishing passes all take the reference's direct loop; a sparse
+    part of the same scene keeps using lists. Both stay bit-identical to the
+    oracle, with tension (normals pass + tension walk) and without."""
+    rng = np.random.default_rng(3)
+    for tension in (0.0, 0.5):
+        p = configs._base_params([12.0, 8.0, 10.0], iterations=4, tension=tension, xsph=0.01)
+        side = np.arange(8) * 0.15
+        x, y, z = np.meshgrid(side, side, side, indexing="ij")
+        dense = np.stack([x.ravel(), y.ravel(), z.ravel()], 1) + [3.0, 1.0, 3.0]
+        sparse = rng.uniform([6.0, 1.0, 2.0], [10.0, 5.0, 8.0], size=(1500, 3))
+        fluid = np.concatenate([dense, sparse]) + rng.uniform(-0.005, 0.005, size=(512 + 1500, 3))
+        sc = configs._assemble(fluid, [], p, configs.lattice_mass(0.5, 1.0))
+        g, o = pair(p, sc)
+        for _ in range(2):
+            assert g.step(1 / 60) == o.step(1 / 60)
+        compare(g, o, names=PARTICLE_BUFS + ("density", "lambda_"))
+        if tension > 0:
+            compare(g, o, names=("normal", "corr"))
+
+
 def test_verify_harness_checks():
     """The reference's own ?verify=1 checks (src/main.js:853-937) on the GPU state."""
     p = small_params(targetParticleCount=5000, bodies=["sphere:0.5"], bodySize=0.05)
