@@ -331,7 +331,7 @@ def render_bench(sim, params, stream, width=1920, height=1080, reps=5):
     sp = default_ssfr()
     sp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
     rp = default_ray()
-    rp.update({k: m[k] for k in ("proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
     mp = default_mesh()
 
     def timed(fn):
@@ -348,8 +348,10 @@ def render_bench(sim, params, stream, width=1920, height=1080, reps=5):
            "mesh_ms": timed(lambda: sim.mesh(mp, wait=False)),
            "ssfr_ms": timed(lambda: sim.ssfr(sp)),
            "ray_ms": timed(lambda: sim.ray(rp)),
+           "ray_field_ms": timed(lambda: sim.ray(dict(rp, use_surface=0))),
            "what": "device ms per call (median of 5): p4a_mesh at resolution 128, p4a_ssfr and p4a_ray at "
-                   f"{width}x{height} on the scene after the timed steps (anisotropic pass already done)"}
+                   f"{width}x{height} on the scene after the timed steps (anisotropic pass already done); "
+                   "ray_ms with the mesh surface pass (the default), ray_field_ms marching the field"}
     out["mesh_triangles"] = sim.mesh(mp)
     return out
 

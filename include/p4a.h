@@ -367,14 +367,14 @@ int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes);
 
 /* ---- ray-marched surface (src/ray.js:30-97, src/ray_wgsl.js:1-549) ------- */
 /*
- * RayMarch.draw on the density field of the last p4a_mesh (call p4a_mesh first;
- * SurfaceMesh.generateField + smoothField is its field stage): per pixel, the eye
- * ray walks the voxel grid, finds the iso crossing of the trilinear field in each
- * cell (cubic fit, bracketed regula falsi), and shades the surface with Fresnel
- * reflection, absorption along the refracted ray's optical depth through the
- * field, the GGX sun highlight, sky / floor and rigid bodies (`bodies` as for
- * p4a_ssfr). The image is RGBA8, width x height. The rasterised-mesh surface input
- * (useSurface) and environment maps are not supported.
+ * RayMarch.draw on the last p4a_mesh (call p4a_mesh first): the surface is the
+ * mesh's triangles drawn into eye-depth and normal maps (SurfaceMesh.drawSurface,
+ * use_surface = 1, the reference's default), or the iso crossing of the trilinear
+ * density field found by walking the voxel grid (cubic fit, bracketed regula falsi;
+ * use_surface = 0). Either way it is shaded with Fresnel reflection, absorption
+ * along the refracted ray's optical depth through the field, the GGX sun
+ * highlight, sky / floor and rigid bodies (`bodies` as for p4a_ssfr). The image is
+ * RGBA8, width x height. Environment maps are not supported.
  */
 typedef struct p4a_ray_params {
   float proj[16], inv_view_proj[16], inv_view[16];
@@ -395,6 +395,10 @@ typedef struct p4a_ray_params {
   double exposure;            /* 1.0                                             */
   int32_t debug;              /* 0 shaded, 1 normals, 2 distance, 3 thickness,
                                  4 reflection side, 5 slope, 6 reflection        */
+  int32_t use_surface;        /* raySurface: 1 (default) the mesh's triangles drawn
+                                 into eye-depth and normal maps give the surface;
+                                 0 the field is marched                          */
+  float view[16];             /* view matrix, for the mesh surface pass          */
 } p4a_ray_params;
 int p4a_default_ray_params(p4a_ray_params* out);
 int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t body_count);

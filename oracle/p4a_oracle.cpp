@@ -2668,6 +2668,107 @@ float o_optical(const ORay& R, f3 ro, f3 rd, float tMax) {
   return acc * dt;
 }
 
+// The mesh surface pass (src/mesh.js:380-396; meshDrawWGSL vs + fsSurf,
+// src/mesh_wgsl.js:268-321): the triangles in order into an eye-depth map (-1e4
+// where empty) and a normal map (w = 1 where covered). A pixel centre inside a
+// triangle or on its edge is covered; the depth test keeps the least screen depth,
+// ties to the lower triangle index; triangles with a vertex outside 0 <= z <= w
+// are dropped. World position and normal are interpolated perspective-correctly.
+struct OSurfTri {
+  v4o clip[3];
+  float sx[3], sy[3], sz[3], area;
+  f3 p[3], n[3];
+};
+bool o_surf_tri(const orc_sim* s, const float* vp, int W, int H, size_t t, OSurfTri& T) {
+  const float voxel = (float)s->meshVoxel, origin = (float)s->meshOrigin;
+  for (int k = 0; k < 3; k++) {
+    const uint32_t vx = s->meshVerts[(3 * t + k) * 2], vy = s->meshVerts[(3 * t + k) * 2 + 1];
+    const float px = (float)(vx & 0xFFFFu) / 65535.0f, py = (float)(vx >> 16) / 65535.0f,
+                pz = (float)(vy & 0xFFFFu) / 65535.0f;
+    T.p[k] = {origin + px * (float)(s->meshDim[0] - 1) * voxel, origin + py * (float)(s->meshDim[1] - 1) * voxel,
+              origin + pz * (float)(s->meshDim[2] - 1) * voxel};
+    const uint32_t oct = vy >> 16;
+    const float ex = (float)(oct & 0xFFu) / 255.0f * 2.0f - 1.0f, ey = (float)(oct >> 8) / 255.0f * 2.0f - 1.0f;
+    f3 m = {ex, ey, 1.0f - std::fabs(ex) - std::fabs(ey)};
+    if (m.z < 0.0f)
+      m = {(1.0f - std::fabs(m.y)) * (m.x >= 0.0f ? 1.0f : -1.0f), (1.0f - std::fabs(m.x)) * (m.y >= 0.0f ? 1.0f : -1.0f),
+           m.z};
+    T.n[k] = nrm3(m);
+    T.clip[k] = mv4(vp, {T.p[k].x, T.p[k].y, T.p[k].z, 1.0f});
+    if (!(T.clip[k].w > 0.0f) || T.clip[k].z < 0.0f || T.clip[k].z > T.clip[k].w) return false;
+    T.sx[k] = (T.clip[k].x / T.clip[k].w * 0.5f + 0.5f) * (float)W;
+    T.sy[k] = (0.5f - T.clip[k].y / T.clip[k].w * 0.5f) * (float)H;
+    T.sz[k] = T.clip[k].z / T.clip[k].w;
+  }
+  T.area = (T.sx[1] - T.sx[0]) * (T.sy[2] - T.sy[0]) - (T.sx[2] - T.sx[0]) * (T.sy[1] - T.sy[0]);
+  return T.area != 0.0f;
+}
+bool o_surf_bary(const OSurfTri& T, float cx, float cy, float b[3]) {
+  float w0 = (T.sx[2] - T.sx[1]) * (cy - T.sy[1]) - (T.sy[2] - T.sy[1]) * (cx - T.sx[1]);
+  float w1 = (T.sx[0] - T.sx[2]) * (cy - T.sy[2]) - (T.sy[0] - T.sy[2]) * (cx - T.sx[2]);
+  float w2 = (T.sx[1] - T.sx[0]) * (cy - T.sy[0]) - (T.sy[1] - T.sy[0]) * (cx - T.sx[0]);
+  float a = T.area;
+  if (a < 0.0f) {
+    w0 = -w0;
+    w1 = -w1;
+    w2 = -w2;
+    a = -a;
+  }
+  if (w0 < 0.0f || w1 < 0.0f || w2 < 0.0f) return false;
+  b[0] = w0 / a;
+  b[1] = w1 / a;
+  b[2] = w2 / a;
+  return true;
+}
+void o_surface(const orc_sim* s, const float* view, const float* vp, int W, int H, std::vector<float>& surfZ,
+               std::vector<f3>& surfN) {
+  const size_t px = (size_t)W * H;
+  std::vector<uint64_t> key(px, ~0ull);
+  const size_t tris = s->meshVerts.size() / 6;
+  for (size_t t = 0; t < tris; t++) {
+    OSurfTri T;
+    if (!o_surf_tri(s, vp, W, H, t, T)) continue;
+    const float lx = std::fmin(T.sx[0], std::fmin(T.sx[1], T.sx[2])), hx = std::fmax(T.sx[0], std::fmax(T.sx[1], T.sx[2]));
+    const float ly = std::fmin(T.sy[0], std::fmin(T.sy[1], T.sy[2])), hy = std::fmax(T.sy[0], std::fmax(T.sy[1], T.sy[2]));
+    const int x0 = (int)std::fmax(std::ceil(lx - 0.5f), 0.0f), x1 = (int)std::fmin(std::floor(hx - 0.5f), (float)W - 1.0f);
+    const int y0 = (int)std::fmax(std::ceil(ly - 0.5f), 0.0f), y1 = (int)std::fmin(std::floor(hy - 0.5f), (float)H - 1.0f);
+    for (int y = y0; y <= y1; y++)
+      for (int x = x0; x <= x1; x++) {
+        float b[3];
+        if (!o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b)) continue;
+        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2];
+        if (!(depth < 1.0f)) continue;
+        uint32_t bits;
+        memcpy(&bits, &depth, 4);
+        const uint64_t k = ((uint64_t)bits << 32) | (uint32_t)t;
+        uint64_t& slot = key[(size_t)y * W + x];
+        if (k < slot) slot = k;
+      }
+  }
+  surfZ.assign(px, -1.0e4f);
+  surfN.assign(px, f3{0.0f, 0.0f, 0.0f});
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      const size_t o = (size_t)y * W + x;
+      if (key[o] == ~0ull) continue;
+      OSurfTri T;
+      float b[3];
+      if (!o_surf_tri(s, vp, W, H, (size_t)(key[o] & 0xffffffffu), T) ||
+          !o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b))
+        continue;
+      const float q0 = b[0] / T.clip[0].w, q1 = b[1] / T.clip[1].w, q2 = b[2] / T.clip[2].w;
+      const float qs = q0 + q1 + q2;
+      const f3 wp = {(q0 * T.p[0].x + q1 * T.p[1].x + q2 * T.p[2].x) / qs,
+                     (q0 * T.p[0].y + q1 * T.p[1].y + q2 * T.p[2].y) / qs,
+                     (q0 * T.p[0].z + q1 * T.p[1].z + q2 * T.p[2].z) / qs};
+      const f3 wn = {(q0 * T.n[0].x + q1 * T.n[1].x + q2 * T.n[2].x) / qs,
+                     (q0 * T.n[0].y + q1 * T.n[1].y + q2 * T.n[2].y) / qs,
+                     (q0 * T.n[0].z + q1 * T.n[1].z + q2 * T.n[2].z) / qs};
+      surfZ[o] = mv4(view, {wp.x, wp.y, wp.z, 1.0f}).z;
+      surfN[o] = nrm3(wn);
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -2718,6 +2819,19 @@ int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
   s->rayImage.assign((size_t)q.width * q.height, 0u);
   s->rayDims[0] = q.width;
   s->rayDims[1] = q.height;
+  const bool useSurface = q.use_surface != 0;
+  std::vector<float> surfZ;
+  std::vector<f3> surfN;
+  if (useSurface) {
+    float vp[16];
+    for (int c = 0; c < 4; c++)
+      for (int rr = 0; rr < 4; rr++)
+        vp[c * 4 + rr] = std::fmaf(q.proj[12 + rr], q.view[c * 4 + 3],
+                                   std::fmaf(q.proj[8 + rr], q.view[c * 4 + 2],
+                                             std::fmaf(q.proj[4 + rr], q.view[c * 4 + 1], q.proj[rr] * q.view[c * 4])));
+    o_surface(s, q.view, vp, q.width, q.height, surfZ, surfN);
+  }
+  const float proj00 = q.proj[0], proj11 = q.proj[5];
 #pragma omp parallel for schedule(dynamic, 2)
   for (int y = 0; y < q.height; y++)
     for (int x = 0; x < q.width; x++) {
@@ -2727,9 +2841,22 @@ int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
       const f3 nearP = {nh.x / nh.w, nh.y / nh.w, nh.z / nh.w}, farP = {fh.x / fh.w, fh.y / fh.w, fh.z / fh.w};
       const f3 ro = eye, rd = nrm3(sub3(farP, nearP));
       float tHit = -1.0f;
-      f3 hit = {0, 0, 0};
-      const OSlab slab = o_box(ro, rd, volLo, volHi);
-      if (slab.hit) tHit = o_march(R, C, ro, rd, std::fmax(slab.t0, 0.0f) + 1.0e-5f, slab.t1, hit);
+      f3 hit = {0, 0, 0}, meshN = {0, 1, 0};
+      if (useSurface) {
+        // meshSurfaceHit (src/ray_wgsl.js:397-412)
+        const size_t o = (size_t)y * q.width + x;
+        const float z = surfZ[o];
+        const f3 nv = surfN[o];
+        if (!(z < -1.0e3f) && !(dot3(nv, nv) < 1.0e-8f)) {
+          const v4o wv = mv4(q.inv_view, {-nx * z / proj00, -ny * z / proj11, z, 1.0f});
+          hit = {wv.x, wv.y, wv.z};
+          meshN = nrm3(nv);
+          tHit = length3(sub3(hit, ro));
+        }
+      } else {
+        const OSlab slab = o_box(ro, rd, volLo, volHi);
+        if (slab.hit) tHit = o_march(R, C, ro, rd, std::fmax(slab.t0, 0.0f) + 1.0e-5f, slab.t1, hit);
+      }
       float tMaxBody = 60.0f;
       if (tHit >= 0.0f) tMaxBody = tHit + R.skin;
       const OTrace bt = o_trace(C, ro, rd, tMaxBody);
@@ -2740,11 +2867,16 @@ int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
       } else if (tHit < 0.0f) {
         col = o_background(C, ro, rd);
       } else {
-        const f3 g = {(hit.x - R.origin.x) / R.voxel, (hit.y - R.origin.y) / R.voxel, (hit.z - R.origin.z) / R.voxel};
-        const f3 sn = {o_tri_at(R, {g.x + 1.0f, g.y, g.z}) - o_tri_at(R, {g.x - 1.0f, g.y, g.z}),
-                       o_tri_at(R, {g.x, g.y + 1.0f, g.z}) - o_tri_at(R, {g.x, g.y - 1.0f, g.z}),
-                       o_tri_at(R, {g.x, g.y, g.z + 1.0f}) - o_tri_at(R, {g.x, g.y, g.z - 1.0f})};
-        n = nrm3({-sn.x, -sn.y, -sn.z});
+        if (useSurface) {
+          n = meshN;
+        } else {
+          const f3 g = {(hit.x - R.origin.x) / R.voxel, (hit.y - R.origin.y) / R.voxel,
+                        (hit.z - R.origin.z) / R.voxel};
+          const f3 sn = {o_tri_at(R, {g.x + 1.0f, g.y, g.z}) - o_tri_at(R, {g.x - 1.0f, g.y, g.z}),
+                         o_tri_at(R, {g.x, g.y + 1.0f, g.z}) - o_tri_at(R, {g.x, g.y - 1.0f, g.z}),
+                         o_tri_at(R, {g.x, g.y, g.z + 1.0f}) - o_tri_at(R, {g.x, g.y, g.z - 1.0f})};
+          n = nrm3({-sn.x, -sn.y, -sn.z});
+        }
         if (dot3(n, rd) > 0.0f) n = {-n.x, -n.y, -n.z};
         const f3 mrd = {-rd.x, -rd.y, -rd.z};
         const float kS = o_fresnel(std::fmax(dot3(mrd, n), 0.0f), 1.0f, R.ior);

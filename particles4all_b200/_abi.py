@@ -119,7 +119,7 @@ class RayParams(C.Structure):
         ("thickness_steps", C.c_int32), ("floor_plane", C.c_int32), ("ground_reflection", C.c_double),
         ("skin_width", C.c_double), ("roughness", C.c_double), ("sun_intensity", C.c_double),
         ("sun_elevation", C.c_double), ("sun_azimuth", C.c_double), ("exposure", C.c_double),
-        ("debug", C.c_int32),
+        ("debug", C.c_int32), ("use_surface", C.c_int32), ("view", C.c_float * 16),
     ]
 
 

@@ -102,6 +102,7 @@ struct p4a_sim {
   int32_t meshDim[3] = {0, 0, 0};
   double meshOrigin = 0, meshVoxel = 0;
   int64_t meshTris = 0;
+  size_t meshNvox = 0;  // voxels of the last p4a_mesh: meshOffsets[meshNvox] is its triangle count
   uint32_t meshEpoch = 0;
   // screen-space fluid rendering (p4a_ssfr)
   std::vector<void*> ssfrAllocs;
@@ -110,6 +111,7 @@ struct p4a_sim {
   float4* ssfrBodies = nullptr;
   int ssfrBodyCap = 0;
   uchar4* rayImage = nullptr;  // p4a_ray
+  char* raySurf = nullptr;     // p4a_ray's mesh surface maps, rayCap pixels
   size_t rayCap = 0;
   int rayW = 0, rayH = 0;
   bool ready = false;
@@ -643,6 +645,7 @@ int p4a_destroy(p4a_sim* s) {
   free_list(s->ssfrAllocs);
   if (s->ssfrBodies) cudaFree(s->ssfrBodies);
   if (s->rayImage) cudaFree(s->rayImage);
+  if (s->raySurf) cudaFree(s->raySurf);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
@@ -1182,6 +1185,7 @@ int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
   for (int k = 0; k < 3; k++) s->meshDim[k] = dim[k];
   s->meshOrigin = -voxel;
   s->meshVoxel = voxel;
+  s->meshNvox = nvox;
   if (triangles) {
     uint32_t t = 0;
     CUDA_TRY(s, cudaMemcpyAsync(&t, s->meshOffsets + nvox, 4, cudaMemcpyDeviceToHost, st));
@@ -1482,6 +1486,8 @@ int p4a_default_ray_params(p4a_ray_params* o) {
   o->sun_azimuth = 40.0;
   o->exposure = 1.0;
   o->debug = 0;
+  o->use_surface = 1;  // raySurface (src/main.js)
+  for (int k = 0; k < 4; k++) o->view[k * 5] = 1.0f;
   return P4A_OK;
 }
 
@@ -1499,7 +1505,10 @@ int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
     if (s->rayImage) cudaFree(s->rayImage);
     s->rayImage = nullptr;
     s->rayCap = 0;
+    if (s->raySurf) cudaFree(s->raySurf);
+    s->raySurf = nullptr;
     CUDA_TRY(s, cudaMalloc((void**)&s->rayImage, px * 4));
+    CUDA_TRY(s, cudaMalloc((void**)&s->raySurf, px * (8 + 4 + 16)));
     s->rayCap = px;
   }
   int rc = upload_bodies(s, bodies, bodyCount);
@@ -1508,6 +1517,13 @@ int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
   RayParams R{};
   memcpy(R.ivp, q.inv_view_proj, 64);
   memcpy(R.iv, q.inv_view, 64);
+  memcpy(R.view, q.view, 64);
+  for (int c = 0; c < 4; c++)
+    for (int rr = 0; rr < 4; rr++)
+      R.vp[c * 4 + rr] = std::fma(q.proj[12 + rr], q.view[c * 4 + 3],
+                                  std::fma(q.proj[8 + rr], q.view[c * 4 + 2],
+                                           std::fma(q.proj[4 + rr], q.view[c * 4 + 1], q.proj[rr] * q.view[c * 4])));
+  R.useSurface = q.use_surface ? 1 : 0;
   const double kPiD = 3.14159265358979323846;
   const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
   const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};
@@ -1540,7 +1556,14 @@ int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
   const double deg[4] = {5.0, 10.0, 20.0, 40.0};
   for (int k = 0; k < 4; k++) R.cosDeg[k] = (float)std::cos(deg[k] * kPiD / 180);
   mark(s, PH_RAY);
-  launch_ray(R, s->meshField[s->fieldSlot], s->ssfrBodies, s->rayImage, s->stream);
+  // surface maps: normals, then 8-byte depth-test keys, then eye z
+  float4* surfN = (float4*)s->raySurf;
+  unsigned long long* key = (unsigned long long*)(s->raySurf + px * 16);
+  float* surfZ = (float*)(s->raySurf + px * 24);
+  if (R.useSurface)
+    launch_surface(R, s->meshVerts, s->meshOffsets + s->meshNvox, (uint32_t)s->meshTriCap, R.gridOrigin, R.vertDim,
+                   R.voxel, key, surfZ, surfN, s->stream);
+  launch_ray(R, s->meshField[s->fieldSlot], s->ssfrBodies, surfZ, surfN, s->rayImage, s->stream);
   mark(s, PH_END);
   CUDA_TRY(s, cudaGetLastError());
   s->rayW = q.width;

@@ -6,12 +6,18 @@
 // turning points and refined by 12 regula-falsi steps; rigid bodies are traced as
 // signed distance fields; the surface is shaded with Fresnel reflection, refraction
 // through an optical depth integrated along the refracted ray, and a GGX sun
-// highlight, then tone-mapped. The rasterised-mesh surface input (useSurface) is
-// not built: the field march is the surface. The field is the one p4a_mesh
-// produced (SurfaceMesh.generateField + smoothField).
+// highlight, then tone-mapped. With useSurface (the reference's default) the
+// surface comes instead from the mesh's triangles drawn into an eye-depth map and a
+// normal map (the surface pass below: a triangle per thread, pixel centres inside
+// the triangle or on its edges, depth test 'less' as an atomicMin of (depth bits,
+// triangle), perspective-correct world position and normal in a resolve pass;
+// triangles with a vertex outside 0 <= z <= w are dropped rather than clipped).
+// The field is the one p4a_mesh produced (SurfaceMesh.generateField + smoothField).
 // Float contract as in kernels_ssfr.cu; acos in debug view 5 is replaced by the
 // equivalent comparison of |n.y| against the cosines of the thresholds.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "fmath.h"
 #include "p4a_internal.h"
@@ -256,8 +262,121 @@ __device__ __forceinline__ float optical_depth(const RayParams& R, const float* 
   return acc * dt;
 }
 
+// ---- mesh surface pass ----
+struct SurfGrid {
+  float origin[3], voxel;
+  int32_t dim[3];
+};
+// meshDrawWGSL vs (src/mesh_wgsl.js:268-286): a packed vertex to world position and
+// unit normal.
+__device__ __forceinline__ void unpack_vertex(const SurfGrid& G, uint2 v, F3& p, F3& n) {
+  const float px = (float)(v.x & 0xFFFFu) / 65535.0f, py = (float)(v.x >> 16) / 65535.0f,
+              pz = (float)(v.y & 0xFFFFu) / 65535.0f;
+  p = {G.origin[0] + px * (float)(G.dim[0] - 1) * G.voxel, G.origin[1] + py * (float)(G.dim[1] - 1) * G.voxel,
+       G.origin[2] + pz * (float)(G.dim[2] - 1) * G.voxel};
+  const uint32_t oct = v.y >> 16;
+  const float ex = (float)(oct & 0xFFu) / 255.0f * 2.0f - 1.0f, ey = (float)(oct >> 8) / 255.0f * 2.0f - 1.0f;
+  F3 m = {ex, ey, 1.0f - fabsf(ex) - fabsf(ey)};
+  if (m.z < 0.0f) {
+    const float tx = (1.0f - fabsf(m.y)) * (m.x >= 0.0f ? 1.0f : -1.0f);
+    const float ty = (1.0f - fabsf(m.x)) * (m.y >= 0.0f ? 1.0f : -1.0f);
+    m = {tx, ty, m.z};
+  }
+  n = normalize3(m);
+}
+struct Tri {
+  V4 clip[3];
+  float sx[3], sy[3], sz[3], area;
+};
+__device__ __forceinline__ bool setup_tri(const RayParams& R, const SurfGrid& G, const uint2* __restrict__ verts,
+                                          uint32_t t, Tri& T, F3 p[3], F3 n[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    unpack_vertex(G, __ldg(&verts[3 * (size_t)t + k]), p[k], n[k]);
+    T.clip[k] = mat_vec4(R.vp, {p[k].x, p[k].y, p[k].z, 1.0f});
+    if (!(T.clip[k].w > 0.0f) || T.clip[k].z < 0.0f || T.clip[k].z > T.clip[k].w) return false;
+    T.sx[k] = (T.clip[k].x / T.clip[k].w * 0.5f + 0.5f) * (float)R.width;
+    T.sy[k] = (0.5f - T.clip[k].y / T.clip[k].w * 0.5f) * (float)R.height;
+    T.sz[k] = T.clip[k].z / T.clip[k].w;
+  }
+  T.area = (T.sx[1] - T.sx[0]) * (T.sy[2] - T.sy[0]) - (T.sx[2] - T.sx[0]) * (T.sy[1] - T.sy[0]);
+  return T.area != 0.0f;
+}
+// Screen-space barycentrics of the pixel centre (cx, cy), normalised so that the
+// inside is b >= 0 for either winding; false outside.
+__device__ __forceinline__ bool bary(const Tri& T, float cx, float cy, float b[3]) {
+  float w0 = (T.sx[2] - T.sx[1]) * (cy - T.sy[1]) - (T.sy[2] - T.sy[1]) * (cx - T.sx[1]);
+  float w1 = (T.sx[0] - T.sx[2]) * (cy - T.sy[2]) - (T.sy[0] - T.sy[2]) * (cx - T.sx[2]);
+  float w2 = (T.sx[1] - T.sx[0]) * (cy - T.sy[0]) - (T.sy[1] - T.sy[0]) * (cx - T.sx[0]);
+  float a = T.area;
+  if (a < 0.0f) {
+    w0 = -w0;
+    w1 = -w1;
+    w2 = -w2;
+    a = -a;
+  }
+  if (w0 < 0.0f || w1 < 0.0f || w2 < 0.0f) return false;
+  b[0] = w0 / a;
+  b[1] = w1 / a;
+  b[2] = w2 / a;
+  return true;
+}
+__global__ void k_surf_raster(const __grid_constant__ RayParams R, const __grid_constant__ SurfGrid G,
+                              const uint2* __restrict__ verts, const uint32_t* __restrict__ total, uint32_t cap,
+                              unsigned long long* __restrict__ key) {
+  const uint32_t count = min(__ldg(total), cap);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    Tri T;
+    F3 p[3], n[3];
+    if (!setup_tri(R, G, verts, t, T, p, n)) continue;
+    const float lo_x = fminf(T.sx[0], fminf(T.sx[1], T.sx[2])), hi_x = fmaxf(T.sx[0], fmaxf(T.sx[1], T.sx[2]));
+    const float lo_y = fminf(T.sy[0], fminf(T.sy[1], T.sy[2])), hi_y = fmaxf(T.sy[0], fmaxf(T.sy[1], T.sy[2]));
+    const int x0 = (int)fmaxf(ceilf(lo_x - 0.5f), 0.0f), x1 = (int)fminf(floorf(hi_x - 0.5f), (float)R.width - 1.0f);
+    const int y0 = (int)fmaxf(ceilf(lo_y - 0.5f), 0.0f), y1 = (int)fminf(floorf(hi_y - 0.5f), (float)R.height - 1.0f);
+    for (int py = y0; py <= y1; py++)
+      for (int px = x0; px <= x1; px++) {
+        float b[3];
+        if (!bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) continue;
+        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2];
+        if (!(depth < 1.0f)) continue;
+        atomicMin(&key[(size_t)py * R.width + px], ((unsigned long long)__float_as_uint(depth) << 32) | t);
+      }
+  }
+}
+__global__ void k_surf_resolve(const __grid_constant__ RayParams R, const __grid_constant__ SurfGrid G,
+                               const uint2* __restrict__ verts, const unsigned long long* __restrict__ key,
+                               float* __restrict__ surfZ, float4* __restrict__ surfN) {
+  const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
+  if (px >= R.width || py >= R.height) return;
+  const size_t o = (size_t)py * R.width + px;
+  const unsigned long long k = key[o];
+  float z = -1.0e4f;
+  float4 nn = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (k != ~0ull) {
+    Tri T;
+    F3 p[3], n[3];
+    float b[3];
+    if (setup_tri(R, G, verts, (uint32_t)(k & 0xffffffffu), T, p, n) &&
+        bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) {
+      // perspective-correct interpolation of the world position and the normal
+      const float q0 = b[0] / T.clip[0].w, q1 = b[1] / T.clip[1].w, q2 = b[2] / T.clip[2].w;
+      const float qs = q0 + q1 + q2;
+      const F3 wp = {(q0 * p[0].x + q1 * p[1].x + q2 * p[2].x) / qs, (q0 * p[0].y + q1 * p[1].y + q2 * p[2].y) / qs,
+                     (q0 * p[0].z + q1 * p[1].z + q2 * p[2].z) / qs};
+      const F3 wn = {(q0 * n[0].x + q1 * n[1].x + q2 * n[2].x) / qs, (q0 * n[0].y + q1 * n[1].y + q2 * n[2].y) / qs,
+                     (q0 * n[0].z + q1 * n[1].z + q2 * n[2].z) / qs};
+      z = mat_vec4(R.view, {wp.x, wp.y, wp.z, 1.0f}).z;  // fsSurf: (V.view * world).z
+      const F3 un = normalize3(wn);
+      nn = make_float4(un.x, un.y, un.z, 1.0f);
+    }
+  }
+  surfZ[o] = z;
+  surfN[o] = nn;
+}
+
 __global__ void k_ray(const __grid_constant__ RayParams R, const float* __restrict__ field,
-                      const float4* __restrict__ bdata, uchar4* __restrict__ image) {
+                      const float4* __restrict__ bdata, const float* __restrict__ surfZ,
+                      const float4* __restrict__ surfN, uchar4* __restrict__ image) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   if (x >= R.width || y >= R.height) return;
   const float nx = ((float)x + 0.5f) / (float)R.width * 2.0f - 1.0f;
@@ -272,7 +391,23 @@ __global__ void k_ray(const __grid_constant__ RayParams R, const float* __restri
                     volLo.z + R.voxel * (float)(R.vertDim[2] - 1)};
   float tHit = -1.0f;
   F3 hit = {0.f, 0.f, 0.f};
-  {
+  F3 meshN = {0.0f, 1.0f, 0.0f};
+  if (R.useSurface != 0) {
+    // meshSurfaceHit (src/ray_wgsl.js:397-412)
+    const size_t o = (size_t)y * R.width + x;
+    const float z = __ldg(&surfZ[o]);
+    if (!(z < -1.0e3f)) {
+      const F3 pv = {-nx * z / R.proj00, -ny * z / R.proj11, z};
+      const V4 wv = mat_vec4(R.iv, {pv.x, pv.y, pv.z, 1.0f});
+      const float4 n4 = __ldg(&surfN[o]);
+      const F3 nv = {n4.x, n4.y, n4.z};
+      if (!(dot3(nv, nv) < 1.0e-8f)) {
+        hit = {wv.x, wv.y, wv.z};
+        meshN = normalize3(nv);
+        tHit = len3(sub3(hit, ro));
+      }
+    }
+  } else {
     const Slab slab = box_hit(ro, rd, volLo, volHi);
     if (slab.hit) {
       const March m = march(R, field, bdata, ro, rd, fmaxf(slab.t0, 0.0f) + 1.0e-5f, slab.t1);
@@ -291,9 +426,14 @@ __global__ void k_ray(const __grid_constant__ RayParams R, const float* __restri
   } else if (tHit < 0.0f) {
     col = background(R, ro, rd);
   } else {
-    const F3 go = f3(R.gridOrigin);
-    const F3 sn = smooth_normal(R, field, {(hit.x - go.x) / R.voxel, (hit.y - go.y) / R.voxel, (hit.z - go.z) / R.voxel});
-    n = normalize3({-sn.x, -sn.y, -sn.z});
+    if (R.useSurface != 0) {
+      n = meshN;
+    } else {
+      const F3 go = f3(R.gridOrigin);
+      const F3 sn =
+          smooth_normal(R, field, {(hit.x - go.x) / R.voxel, (hit.y - go.y) / R.voxel, (hit.z - go.z) / R.voxel});
+      n = normalize3({-sn.x, -sn.y, -sn.z});
+    }
     if (dot3(n, rd) > 0.0f) n = {-n.x, -n.y, -n.z};
     const F3 mrd = {-rd.x, -rd.y, -rd.z};
     const float kS = fresnel_full(fmaxf(dot3(mrd, n), 0.0f), 1.0f, R.ior);
@@ -349,11 +489,33 @@ __global__ void k_ray(const __grid_constant__ RayParams R, const float* __restri
 
 }  // namespace
 
-void launch_ray(const RayParams& R, const float* field, const float4* bodies, uchar4* image, cudaStream_t st) {
+void launch_surface(const RayParams& R, const uint2* verts, const uint32_t* total, uint32_t cap,
+                    const float gridOrigin[3], const int32_t vertDim[3], float voxel,
+                    unsigned long long* key, float* surfZ, float4* surfN, cudaStream_t st) {
+  SurfGrid G;
+  for (int k = 0; k < 3; k++) {
+    G.origin[k] = gridOrigin[k];
+    G.dim[k] = vertDim[k];
+  }
+  G.voxel = voxel;
+  cudaMemsetAsync(key, 0xff, (size_t)R.width * R.height * 8, st);
+  const int tpb = 128;
+  if (cap > 0) {
+    const int grid = (int)std::min<uint32_t>((cap + tpb - 1) / tpb, 148u * 16u);
+    count_launches(1);
+    k_surf_raster<<<grid, tpb, 0, st>>>(R, G, verts, total, cap, key);
+  }
+  const dim3 rgrid((R.width + tpb - 1) / tpb, R.height);
+  count_launches(1);
+  k_surf_resolve<<<rgrid, tpb, 0, st>>>(R, G, verts, key, surfZ, surfN);
+}
+
+void launch_ray(const RayParams& R, const float* field, const float4* bodies, const float* surfZ,
+                const float4* surfN, uchar4* image, cudaStream_t st) {
   const int tpb = 128;
   const dim3 grid((R.width + tpb - 1) / tpb, R.height);
   count_launches(1);
-  k_ray<<<grid, tpb, 0, st>>>(R, field, bodies, image);
+  k_ray<<<grid, tpb, 0, st>>>(R, field, bodies, surfZ, surfN, image);
 }
 
 }  // namespace p4a

@@ -137,8 +137,17 @@ struct RayParams {
   int32_t vertDim[3], thickSteps, bodyCount, floorPlane, debug;
   int32_t width, height;
   float cosDeg[4];
+  int32_t useSurface;
+  float view[16], vp[16];  // view, proj * view (mesh surface pass)
 };
-void launch_ray(const RayParams& R, const float* field, const float4* bodies, uchar4* image, cudaStream_t st);
+// The mesh surface pass (src/mesh.js:380-396, src/mesh_wgsl.js:240-321 vs + fsSurf):
+// the first min(*total, cap) triangles of verts into surfZ (eye-space z, -1e4 where
+// empty) and surfN (normal, w = 1 where covered), key as the depth-test scratch.
+void launch_surface(const RayParams& R, const uint2* verts, const uint32_t* total, uint32_t cap,
+                    const float gridOrigin[3], const int32_t vertDim[3], float voxel,
+                    unsigned long long* key, float* surfZ, float4* surfN, cudaStream_t st);
+void launch_ray(const RayParams& R, const float* field, const float4* bodies, const float* surfZ,
+                const float4* surfN, uchar4* image, cudaStream_t st);
 
 // Device error word bits (set by kernels, read by the host at sync points).
 enum : uint32_t { ERR_SCAN_TIMEOUT = 1u, ERR_BODY_OVERFLOW = 2u };

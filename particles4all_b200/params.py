@@ -190,8 +190,8 @@ def default_ssfr():
 
 
 def default_ray():
-    """RayMarch's defaults (src/ray.js:16-29), iso 0.4, an identity camera and a
-    640 x 480 target."""
+    """RayMarch's defaults (src/ray.js:16-29), iso 0.4, the mesh surface as the
+    surface (raySurface 1), an identity camera and a 640 x 480 target."""
     from ._lib import lib
     s = _abi.RayParams()
     lib().p4a_default_ray_params(C.byref(s))

@@ -152,8 +152,9 @@ class Sim:
         return out.view(np.float32).reshape(h, w)
 
     def ray(self, rparams, bodies=None):
-        """RayMarch.draw (src/ray.js:30-97) on the density field of the last mesh();
-        returns nothing, read the image with ray_read()."""
+        """RayMarch.draw (src/ray.js:30-97) on the last mesh(): its triangles as the
+        surface (use_surface 1, the default) or its density field marched
+        (use_surface 0); returns nothing, read the image with ray_read()."""
         from .params import ray_struct
         rp = ray_struct(rparams)
         if bodies is None or len(bodies) == 0:

@@ -1,6 +1,8 @@
 """The ray-marched surface (src/ray.js:30-97, src/ray_wgsl.js) on the GPU is bit-
-identical to the oracle: the shaded image, with and without rigid bodies, at two
-iso levels and field resolutions, and every debug view."""
+identical to the oracle: the shaded image with the mesh surface pass (the default)
+and with the field march, with and without rigid bodies, at two iso levels and
+field resolutions, and every debug view in both modes. The surface pass's depth
+test does not depend on the order of its atomics."""
 import math
 
 import numpy as np
@@ -39,7 +41,7 @@ def params_for(w, h, **over):
     cam.az, cam.el, cam.dist = -0.5, 0.4, 10.0
     m = frame_matrices(cam, w, h)
     rp = default_ray()
-    rp.update({k: m[k] for k in ("proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
     rp.update(over)
     return rp
 
@@ -62,8 +64,11 @@ def bodies():
 
 CASES = [
     ("default", dict(resolution=48), dict(), False),
-    ("iso", dict(resolution=64, field_passes=1), dict(iso=0.6, thickness_steps=24), False),
+    ("field", dict(resolution=48), dict(use_surface=0), False),
+    ("iso", dict(resolution=64, field_passes=1), dict(iso=0.6, thickness_steps=24, use_surface=0), False),
+    ("iso_surface", dict(resolution=64, field_passes=1), dict(iso=0.6, thickness_steps=24), False),
     ("bodies", dict(resolution=48), dict(floor_plane=0, ground_reflection=0.5), True),
+    ("bodies_field", dict(resolution=48), dict(floor_plane=0, ground_reflection=0.5, use_surface=0), True),
 ]
 
 
@@ -88,13 +93,27 @@ def test_ray_matches_oracle(block, name, mesh, over, with_bodies):
     assert d[..., :3].any() and not d[..., :3].all()  # the surface is in view, with background around it
 
 
+@pytest.mark.parametrize("surface", [1, 0])
 @pytest.mark.parametrize("debug", [1, 2, 3, 4, 5, 6])
-def test_ray_debug_views_match_oracle(block, debug):
+def test_ray_debug_views_match_oracle(block, debug, surface):
     p, g, o = block
     mp = default_mesh()
     mp["resolution"] = 48
     g.mesh(mp)
     o.mesh(mp)
-    rp = params_for(48, 36, debug=debug)
+    rp = params_for(48, 36, debug=debug, use_surface=surface)
     g.ray(rp, bodies())
     assert np.array_equal(g.ray_read(), o.ray(rp, bodies()))
+
+
+def test_ray_surface_repeatable(block):
+    p, g, _ = block
+    mp = default_mesh()
+    mp["resolution"] = 64
+    g.mesh(mp)
+    rp = params_for(160, 120, debug=1)
+    g.ray(rp)
+    first = g.ray_read()
+    for _ in range(3):
+        g.ray(rp)
+        assert np.array_equal(first, g.ray_read())

@@ -1,7 +1,9 @@
 """CPU checks of the oracle's ray-marched surface (src/ray_wgsl.js): the distance to
 the iso surface (debug view 2) against a float64 march of the same trilinear field
-along each pixel's ray, and pixels that miss the field against the float64 sky /
-floor shading and tone map."""
+along each pixel's ray, pixels that miss the field against the float64 sky / floor
+shading and tone map, and the mesh surface pass (src/mesh.js:380-396): distance and
+normal (debug views 2 and 1) against float64 ray / triangle intersections with the
+mesh's decoded vertices and perspective-correct normal interpolation."""
 import math
 
 import numpy as np
@@ -30,7 +32,8 @@ def ray_params(w, h, **over):
     cam.az, cam.el, cam.dist = -0.6, 0.45, 9.0
     m = frame_matrices(cam, w, h)
     rp = default_ray()
-    rp.update({k: m[k] for k in ("proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp["use_surface"] = 0
     rp.update(over)
     return rp, m
 
@@ -125,3 +128,85 @@ def test_background_against_float64(built):
             assert np.abs(img[py, px, :3] - want).max() <= 1, (px, py, img[py, px], want)
             checked += 1
     assert checked > 20
+
+
+def mesh_triangles(o, p):
+    """The mesh's triangles decoded as meshDrawWGSL's vs does (src/mesh_wgsl.js:268-286),
+    in float64: positions (T, 3, 3) and unit vertex normals (T, 3, 3)."""
+    box = np.array(p["box"], np.float64)
+    voxel = float(np.float32(box.max() / 40))
+    dim = np.array([int(math.ceil(b / (box.max() / 40))) + 3 for b in box])
+    v = o.buffer("meshVerts").view(np.uint32).reshape(-1, 3, 2).astype(np.int64)
+    pn = np.stack([v[..., 0] & 0xFFFF, v[..., 0] >> 16, v[..., 1] & 0xFFFF], -1) / 65535.0
+    pos = -voxel + pn * (dim - 1) * voxel
+    oct = v[..., 1] >> 16
+    e = np.stack([oct & 0xFF, oct >> 8], -1) / 255.0 * 2 - 1
+    n = np.concatenate([e, (1 - np.abs(e).sum(-1))[..., None]], -1)
+    neg = n[..., 2] < 0
+    fx = (1 - np.abs(n[..., 1])) * np.where(n[..., 0] >= 0, 1, -1)
+    fy = (1 - np.abs(n[..., 0])) * np.where(n[..., 1] >= 0, 1, -1)
+    n[..., 0] = np.where(neg, fx, n[..., 0])
+    n[..., 1] = np.where(neg, fy, n[..., 1])
+    n /= np.linalg.norm(n, axis=-1, keepdims=True)
+    return pos, n
+
+
+def nearest_triangle(pos, ro, rd):
+    """Moller-Trumbore against every triangle: (t, barycentrics, index) of the
+    nearest hit, or None."""
+    a, b, c = pos[:, 0], pos[:, 1], pos[:, 2]
+    e1, e2 = b - a, c - a
+    pv = np.cross(rd, e2)
+    det = (e1 * pv).sum(1)
+    ok = np.abs(det) > 1e-14
+    inv = np.where(ok, 1 / np.where(ok, det, 1), 0)
+    tv = ro - a
+    u = (tv * pv).sum(1) * inv
+    qv = np.cross(tv, e1)
+    v = (qv @ rd) * inv
+    t = (qv * e2).sum(1) * inv
+    hit = ok & (u >= 0) & (v >= 0) & (u + v <= 1) & (t > 0)
+    if not hit.any():
+        return None
+    i = np.flatnonzero(hit)[np.argmin(t[hit])]
+    return t[i], np.array([1 - u[i] - v[i], u[i], v[i]]), i
+
+
+def test_mesh_surface_against_float64(built):
+    o, p = block_with_field()
+    pos, nrm = mesh_triangles(o, p)
+    assert len(pos) > 500
+    w, h = 48, 36
+    rp, m = ray_params(w, h, debug=2, use_surface=1)
+    dist = o.ray(rp)
+    normals = o.ray(dict(rp, debug=1))
+    # the f64 hit map first, so that pixels at the silhouette (a neighbour differs) are skipped
+    hits = {}
+    for py in range(h):
+        for px in range(w):
+            ro, rd = render_f64.pixel_ray(m, w, h, px, py, from_eye=True)
+            hits[px, py] = (nearest_triangle(pos, ro, rd), rd)
+    checked = misses = 0
+    for py in range(1, h - 1):
+        for px in range(1, w - 1):
+            near = [hits[px + dx, py + dy][0] is None for dx in (-1, 0, 1) for dy in (-1, 0, 1)]
+            if any(near) != all(near):
+                continue
+            hit, rd = hits[px, py]
+            if hit is None:
+                assert (dist[py, px, :3] == 0).all(), (px, py, dist[py, px])
+                misses += 1
+                continue
+            t, bc, i = hit
+            frac = t - math.floor(t)
+            if min(frac, 1 - frac) > 0.01 and min(t * 0.1 % 1, 1 - t * 0.1 % 1) > 0.01:
+                want = render_f64.rgba8([frac, (t * 0.1) % 1.0, 0.0])
+                assert np.abs(dist[py, px, :3] - want).max() <= 2, (px, py, dist[py, px], want, t)
+            n = bc @ nrm[i]
+            n /= np.linalg.norm(n)
+            if n @ rd > 0:
+                n = -n
+            want = render_f64.rgba8(n * 0.5 + 0.5)
+            assert np.abs(normals[py, px, :3] - want).max() <= 2, (px, py, normals[py, px], want)
+            checked += 1
+    assert checked > 100 and misses > 100, (checked, misses)
