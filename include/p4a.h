@@ -234,6 +234,15 @@ int p4a_buffer(p4a_sim* sim, int32_t id, int32_t which, void** dptr, size_t* byt
 int p4a_read(p4a_sim* sim, int32_t id, int32_t which, void* host, size_t offset, size_t bytes);
 int p4a_write(p4a_sim* sim, int32_t id, int32_t which, const void* host, size_t offset,
               size_t bytes);
+/* Asynchronous readback (the reference's copyBufferToBuffer + mapAsync without
+ * the wait, src/main.js:841-852): the copy into `host` (pinned memory, so that it
+ * overlaps) runs on the sim's copy stream, after the work queued so far, while
+ * the caller queues more. Later calls that change that buffer are ordered after
+ * the copy on the device (no host wait); calls that free or reallocate buffers
+ * (reset, resize_box, destroy, set_stream) wait for it. `host` holds the data once
+ * p4a_read_wait (or p4a_synchronize) returns. */
+int p4a_read_async(p4a_sim* sim, int32_t id, int32_t which, void* host, size_t offset, size_t bytes);
+int p4a_read_wait(p4a_sim* sim);
 /* Sim.stats (src/sim.js:619-633). wait = 0: latest completed readback, as the
  * reference's async mapAsync; wait = 1: block until the last step's stats. */
 int p4a_get_stats(p4a_sim* sim, int32_t wait, p4a_stats* out);

@@ -2736,7 +2736,7 @@ void o_surface(const orc_sim* s, const float* view, const float* vp, int W, int 
       for (int x = x0; x <= x1; x++) {
         float b[3];
         if (!o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b)) continue;
-        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2];
+        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;  // -0 -> +0
         if (!(depth < 1.0f)) continue;
         uint32_t bits;
         memcpy(&bits, &depth, 4);

@@ -31,6 +31,8 @@ SIGNATURES = {
     "p4a_buffer": ([_vp, _i32, _i32, C.POINTER(_vp), C.POINTER(_sz)], C.c_int),
     "p4a_read": ([_vp, _i32, _i32, _vp, _sz, _sz], C.c_int),
     "p4a_write": ([_vp, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_read_async": ([_vp, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_read_wait": ([_vp], C.c_int),
     "p4a_get_stats": ([_vp, _i32, _vp], C.c_int),
     "p4a_body_pose": ([_vp, _i32, _vp, _vp, _i32], C.c_int),
     "p4a_aniso": ([_vp, _vp], C.c_int),

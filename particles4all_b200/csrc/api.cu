@@ -54,6 +54,12 @@ struct p4a_sim {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool ownStream = false;
+  // asynchronous readbacks (p4a_read_async): a copy stream ordered after the sim's
+  // stream by copyReady; copyDone marks the last queued copy
+  cudaStream_t copyStream = nullptr;
+  cudaEvent_t copyReady = nullptr, copyDone = nullptr;
+  uint64_t copyInFlight = 0;  // buffer ids read by copies the sim's stream is not yet ordered after
+  bool copyHost = false;      // copies whose host data p4a_read_wait has not waited for
   std::string err;
   p4a_params params{};
   std::vector<p4a_body_spec> specs;
@@ -146,6 +152,29 @@ int fail(p4a_sim* s, int code, const char* fmt, ...) {
                   "%s: %s", #call, cudaGetErrorString(e_));                            \
     }                                                                                  \
   } while (0)
+
+// Orders the sim's stream after the asynchronous readbacks of any buffer in
+// `writes` (a mask of buffer-id bits), so that work queued next cannot change
+// what those copies read. No host wait.
+void after_reads(p4a_sim* s, uint64_t writes) {
+  if (s->copyInFlight & writes) {
+    cudaStreamWaitEvent(s->stream, s->copyDone, 0);
+    s->copyInFlight = 0;  // copyDone covers every copy queued so far
+  }
+}
+constexpr uint64_t kAllBuffers = ~0ull;
+constexpr uint64_t buf_bit(int id) { return 1ull << id; }
+
+// Host wait for every asynchronous readback: before device memory is freed or
+// reallocated, and by p4a_read_wait / p4a_synchronize.
+int drain_reads(p4a_sim* s) {
+  if (s->copyHost) {
+    s->copyHost = false;
+    s->copyInFlight = 0;
+    CUDA_TRY(s, cudaEventSynchronize(s->copyDone));
+  }
+  return P4A_OK;
+}
 
 // Accumulates the recorded kernel intervals into the per-kernel totals.
 int resolve_marks(p4a_sim* s) {
@@ -312,6 +341,8 @@ void grid_pass(p4a_sim* s, int par) {
 }
 
 int reset_common(p4a_sim* s) {
+  const int drc = drain_reads(s);  // the buffers are reallocated
+  if (drc) return drc;
   HostScene& sc = s->sc;
   const p4a_params& p = s->params;
   s->ready = false;
@@ -629,6 +660,7 @@ int p4a_create(int device, p4a_sim** out) {
 int p4a_destroy(p4a_sim* s) {
   if (!s) return P4A_ERR_ARG;
   cudaSetDevice(s->device);
+  drain_reads(s);
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_list(s->sceneAllocs);
   free_list(s->cellAllocs);
@@ -649,6 +681,9 @@ int p4a_destroy(p4a_sim* s) {
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
+  if (s->copyReady) cudaEventDestroy(s->copyReady);
+  if (s->copyDone) cudaEventDestroy(s->copyDone);
+  if (s->copyStream) cudaStreamDestroy(s->copyStream);
   if (s->ownStream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return P4A_OK;
@@ -659,6 +694,8 @@ const char* p4a_last_error(const p4a_sim* s) { return s ? s->err.c_str() : "null
 int p4a_set_stream(p4a_sim* s, void* stream) {
   if (!s) return P4A_ERR_ARG;
   cudaSetDevice(s->device);
+  int rc = drain_reads(s);
+  if (rc) return rc;
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   if (stream) {
     if (s->ownStream) cudaStreamDestroy(s->stream);
@@ -674,6 +711,8 @@ int p4a_set_stream(p4a_sim* s, void* stream) {
 int p4a_synchronize(p4a_sim* s) {
   if (!s) return P4A_ERR_ARG;
   cudaSetDevice(s->device);
+  const int rc = drain_reads(s);
+  if (rc) return rc;
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return poll_readback(s, true);
 }
@@ -727,6 +766,7 @@ int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
   if (!s) return P4A_ERR_ARG;
   if (!s->ready) return fail(s, P4A_ERR_STATE, "p4a_step before p4a_reset");
   cudaSetDevice(s->device);
+  after_reads(s, kAllBuffers);
   const p4a_params& p = s->params;
   // time bank (src/sim.js:418-429)
   const int base = std::max(1, p.substeps);
@@ -816,6 +856,7 @@ int p4a_append_fluid(p4a_sim* s, const float* pos3, const float* vel3, int32_t c
   if (!s || count < 0 || (count > 0 && (!pos3 || !vel3))) return fail(s, P4A_ERR_ARG, "appendFluid: bad arguments");
   if (!s->ready) return fail(s, P4A_ERR_STATE, "appendFluid before reset");
   cudaSetDevice(s->device);
+  after_reads(s, kAllBuffers);
   const int room = std::max(0, s->cap - s->n);
   const int c = std::min(count, room);
   if (added) *added = std::max(0, c);
@@ -857,6 +898,7 @@ int p4a_apply_ray_impulse(p4a_sim* s, const double origin[3], const double dir[3
   double dl = std::hypot(dir[0], dir[1], dir[2]);
   if (!(dl != 0)) dl = 1;
   cudaSetDevice(s->device);
+  after_reads(s, kAllBuffers);
   const float o[3] = {(float)origin[0], (float)origin[1], (float)origin[2]};
   const float dr[3] = {(float)(dir[0] / dl), (float)(dir[1] / dl), (float)(dir[2] / dl)};
   const float im[3] = {(float)impulse[0], (float)impulse[1], (float)impulse[2]};
@@ -887,6 +929,10 @@ int p4a_resize_box(p4a_sim* s, const double newBox[3]) {
   if (!s || !newBox) return fail(s, P4A_ERR_ARG, "resizeBox: null argument");
   if (!s->ready) return fail(s, P4A_ERR_STATE, "resizeBox before reset");
   cudaSetDevice(s->device);
+  {
+    const int drc = drain_reads(s);  // the grid buffers may be reallocated
+    if (drc) return drc;
+  }
   p4a_params& p = s->params;
   const double oldBox[3] = {p.box[0], p.box[1], p.box[2]};
   bool moved = false;
@@ -955,6 +1001,37 @@ int p4a_read(p4a_sim* s, int32_t id, int32_t which, void* host, size_t offset, s
   return P4A_OK;
 }
 
+int p4a_read_async(p4a_sim* s, int32_t id, int32_t which, void* host, size_t offset, size_t bytes) {
+  if (!s || (!host && bytes)) return P4A_ERR_ARG;
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "read before reset");
+  void* p = nullptr;
+  size_t total = 0;
+  int rc = buffer_ptr(s, id, which, &p, &total);
+  if (rc) return rc;
+  if (offset > total || bytes > total - offset)
+    return fail(s, P4A_ERR_ARG, "read of %zu bytes at %zu beyond buffer size %zu", bytes, offset, total);
+  if (!bytes) return P4A_OK;
+  cudaSetDevice(s->device);
+  if (!s->copyStream) {
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking));
+    CUDA_TRY(s, cudaEventCreateWithFlags(&s->copyReady, cudaEventDisableTiming));
+    CUDA_TRY(s, cudaEventCreateWithFlags(&s->copyDone, cudaEventDisableTiming));
+  }
+  CUDA_TRY(s, cudaEventRecord(s->copyReady, s->stream));
+  CUDA_TRY(s, cudaStreamWaitEvent(s->copyStream, s->copyReady, 0));
+  CUDA_TRY(s, cudaMemcpyAsync(host, (const char*)p + offset, bytes, cudaMemcpyDeviceToHost, s->copyStream));
+  CUDA_TRY(s, cudaEventRecord(s->copyDone, s->copyStream));
+  s->copyInFlight |= buf_bit(id);
+  s->copyHost = true;
+  return P4A_OK;
+}
+
+int p4a_read_wait(p4a_sim* s) {
+  if (!s) return P4A_ERR_ARG;
+  cudaSetDevice(s->device);
+  return drain_reads(s);
+}
+
 int p4a_write(p4a_sim* s, int32_t id, int32_t which, const void* host, size_t offset, size_t bytes) {
   if (!s || (!host && bytes)) return P4A_ERR_ARG;
   if (!s->ready) return fail(s, P4A_ERR_STATE, "write before reset");
@@ -966,6 +1043,7 @@ int p4a_write(p4a_sim* s, int32_t id, int32_t which, const void* host, size_t of
     return fail(s, P4A_ERR_ARG, "write of %zu bytes at %zu beyond buffer size %zu", bytes, offset, total);
   if (!bytes) return P4A_OK;
   cudaSetDevice(s->device);
+  after_reads(s, buf_bit(id));
   CUDA_TRY(s, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return P4A_OK;
@@ -1022,7 +1100,10 @@ int p4a_aniso(p4a_sim* s, const p4a_aniso_params* ap) {
   const int n = s->n;
   if (n <= 0) return P4A_OK;
   cudaSetDevice(s->device);
+  after_reads(s, buf_bit(P4A_BUF_SMOOTH_POS) | buf_bit(P4A_BUF_ANISO_G));
   if ((size_t)n > s->anisoCap) {  // src/mesh.js:210-220
+    const int drc = drain_reads(s);
+    if (drc) return drc;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if (s->smoothPos) cudaFree(s->smoothPos);
     if (s->anisoG) cudaFree(s->anisoG);
@@ -1089,7 +1170,10 @@ int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles) {
   const size_t nVerts = (size_t)nv;
   const size_t nvox = (size_t)(dim[0] - 1) * (dim[1] - 1) * (dim[2] - 1);
   const size_t tris = (size_t)mp->max_triangles;
+  after_reads(s, buf_bit(P4A_BUF_MESH_FIELD) | buf_bit(P4A_BUF_MESH_NFIELD) | buf_bit(P4A_BUF_MESH_VERTS));
   if (nVerts > s->meshVertCap || nvox > s->meshVoxCap || tris != s->meshTriCap) {  // src/mesh.js:105-125
+    const int drc = drain_reads(s);
+    if (drc) return drc;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if (nVerts > s->meshVertCap) {
       for (float*& f : s->meshField) {

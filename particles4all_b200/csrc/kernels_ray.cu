@@ -337,7 +337,9 @@ __global__ void k_surf_raster(const __grid_constant__ RayParams R, const __grid_
       for (int px = x0; px <= x1; px++) {
         float b[3];
         if (!bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) continue;
-        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2];
+        // + 0 turns a -0 (a zero weight negated for the winding) into +0, so that the
+        // bits of every depth >= 0 order as the values do
+        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;
         if (!(depth < 1.0f)) continue;
         atomicMin(&key[(size_t)py * R.width + px], ((unsigned long long)__float_as_uint(depth) << 32) | t);
       }

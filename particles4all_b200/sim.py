@@ -266,6 +266,26 @@ class Sim:
             check(self._L.p4a_read(self._h, bid, which, out.ctypes.data, 0, nbytes), self._h, "read")
         return out.reshape(-1, comps) if comps > 1 else out
 
+    def read_async(self, name, host, nbytes=None, which=_abi.LIVE):
+        """Start copying a buffer into `host` (a numpy array, or the address of
+        pinned host memory with `nbytes`) on the sim's copy stream, after the work
+        queued so far; the data is there once read_wait() returns. Keep `host`
+        alive until then."""
+        bid = _abi.BUF[name]
+        if isinstance(host, np.ndarray):
+            if not host.flags.c_contiguous:
+                raise ValueError("read_async needs a contiguous array")
+            ptr, nb = host.ctypes.data, host.nbytes if nbytes is None else int(nbytes)
+            if nb > host.nbytes:
+                raise ValueError(f"read_async of {nb} bytes into an array of {host.nbytes}")
+        else:
+            ptr, nb = int(host), int(nbytes)
+        check(self._L.p4a_read_async(self._h, bid, which, ptr, 0, nb), self._h, "read_async")
+
+    def read_wait(self):
+        """Wait for the copies started by read_async()."""
+        check(self._L.p4a_read_wait(self._h), self._h, "read_wait")
+
     def write(self, name, data, which=_abi.LIVE, offset_elems=0):
         bid = _abi.BUF[name]
         dt, comps = _abi.BUF_LAYOUT[bid]
