@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
     ap.add_argument("--no-render", action="store_true", help="skip the mesh / SSFR / ray-march timings")
     ap.add_argument("--mix-frames", type=int, default=10)
+    ap.add_argument("--only-render", action="store_true",
+                    help="profiling aid: the workload scene, a few steps, then the render-pass timings alone")
     ap.add_argument("--only-mix", choices=["batched", "plain"], default=None,
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
                          "frames and exit; for profiling the two forms")
@@ -228,6 +230,25 @@ def only_mix(form, frames):
             sim.close()
     print(json.dumps({"only_mix": form, "frames": frames, "scenes": len(mix),
                       "wall_s": time.perf_counter() - t0}), flush=True)
+    return 0
+
+
+def only_render(args):
+    """The workload scene stepped a few frames (anisotropic pass included), then the
+    render passes timed as in the full run."""
+    import torch
+    from particles4all_b200 import Sim, default_aniso
+    params, scene, aniso = workload(args.workload)
+    stream = torch.cuda.Stream()
+    sim = Sim()
+    sim.set_stream(stream.cuda_stream)
+    sim.reset_scene(params, scene)
+    for _ in range(max(1, args.warmup)):
+        sim.step(1 / 60)
+    sim.aniso(aniso or default_aniso())
+    out = render_bench(sim, params, stream)
+    sim.close()
+    print(json.dumps({"only_render": out}), flush=True)
     return 0
 
 
@@ -664,6 +685,8 @@ def main():
         return run_reference(args)
     if args.only_mix:
         return only_mix(args.only_mix, args.mix_frames)
+    if args.only_render:
+        return only_render(args)
     return run_ours(args)
 
 
