@@ -250,6 +250,16 @@ class OracleSim:
         return dict(avgRho=s.avg_rho, maxRho=s.max_rho, maxSpeed=s.max_speed, ke=s.ke,
                     raw=list(s.raw), valid=s.valid)
 
+    def write(self, name, data, which=_abi.LIVE):
+        """Overwrite the start of a buffer with `data` (as Sim.write)."""
+        bid = _abi.BUF[name]
+        p, nbytes = C.c_void_p(), C.c_size_t()
+        _check(self._L.orc_buffer(self._h, bid, which, C.byref(p), C.byref(nbytes)), "buffer")
+        a = np.ascontiguousarray(data, _abi.BUF_LAYOUT[bid][0]).reshape(-1)
+        if a.nbytes > nbytes.value:
+            raise ValueError(f"write of {a.nbytes} bytes into a buffer of {nbytes.value}")
+        C.memmove(p, a.ctypes.data, a.nbytes)
+
     def buffer(self, name, which=_abi.LIVE):
         """A numpy copy of a buffer (name as in _abi.BUF)."""
         bid = _abi.BUF[name]

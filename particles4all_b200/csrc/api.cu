@@ -121,6 +121,10 @@ struct p4a_sim {
   size_t rayCap = 0;
   int rayW = 0, rayH = 0;
   bool ready = false;
+  // every particle lies within the last substep's recorded iteration
+  // displacements of the position the sort binned it by: true after a step, until
+  // positions are written, appended, resized or reset
+  bool sortedMoves = false;
   // per-kernel timing (p4a_profile_*)
   bool prof = false;
   std::vector<cudaEvent_t> evPool;
@@ -343,6 +347,7 @@ void grid_pass(p4a_sim* s, int par) {
 int reset_common(p4a_sim* s) {
   const int drc = drain_reads(s);  // the buffers are reallocated
   if (drc) return drc;
+  s->sortedMoves = false;
   HostScene& sc = s->sc;
   const p4a_params& p = s->params;
   s->ready = false;
@@ -844,6 +849,7 @@ int p4a_step(p4a_sim* s, double frameDt, int32_t* substeps_out) {
     }
     s->simTime += dt;
   }
+  if (sub > 0) s->sortedMoves = true;
   mark(s, PH_END);
   CUDA_TRY(s, cudaGetLastError());
   // stats and pose readback (src/sim.js:598-655), at most one in flight
@@ -857,6 +863,7 @@ int p4a_append_fluid(p4a_sim* s, const float* pos3, const float* vel3, int32_t c
   if (!s->ready) return fail(s, P4A_ERR_STATE, "appendFluid before reset");
   cudaSetDevice(s->device);
   after_reads(s, kAllBuffers);
+  s->sortedMoves = false;
   const int room = std::max(0, s->cap - s->n);
   const int c = std::min(count, room);
   if (added) *added = std::max(0, c);
@@ -933,6 +940,7 @@ int p4a_resize_box(p4a_sim* s, const double newBox[3]) {
     const int drc = drain_reads(s);  // the grid buffers may be reallocated
     if (drc) return drc;
   }
+  s->sortedMoves = false;
   p4a_params& p = s->params;
   const double oldBox[3] = {p.box[0], p.box[1], p.box[2]};
   bool moved = false;
@@ -1044,6 +1052,7 @@ int p4a_write(p4a_sim* s, int32_t id, int32_t which, const void* host, size_t of
   if (!bytes) return P4A_OK;
   cudaSetDevice(s->device);
   after_reads(s, buf_bit(id));
+  s->sortedMoves = false;
   CUDA_TRY(s, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return P4A_OK;
@@ -1133,6 +1142,11 @@ int p4a_aniso(p4a_sim* s, const p4a_aniso_params* ap) {
   A.stretch = (float)ap->stretch;
   A.minExtent = (float)ap->min_extent;
   A.neps = ap->min_neighbours;
+  // the row trimming needs every particle within the recorded displacements of
+  // the position the sort binned it by: true right after a step
+  A.disp = s->d.disp;
+  const int iters = std::max(1, s->params.iterations);  // as p4a_step runs them
+  A.dispCount = s->sortedMoves && iters <= kDispSlots ? iters : 0;
   mark(s, PH_ANISO);
   launch_aniso(A, s->d.pos[s->parity], s->d.cellStart, s->smoothPos, s->anisoG, s->stream);
   mark(s, PH_END);

@@ -57,6 +57,14 @@ __device__ __forceinline__ void store_g(float4* __restrict__ g, uint32_t i, cons
   g[i * 2 + 1] = make_float4(elc(G, 2, 1), elc(G, 2, 2), det3(G), last);
 }
 
+// Distance along one axis from coordinate `r` to cell k of n (size `support`),
+// with cell 0 open to -inf and cell n - 1 open to +inf.
+__device__ __forceinline__ float open_gap(int k, int n, float r, float support) {
+  const float below = k > 0 ? (float)k * support - r : 0.0f;
+  const float above = k < n - 1 ? r - (float)(k + 1) * support : 0.0f;
+  return fmaxf(fmaxf(below, above), 0.0f);
+}
+
 __device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* __restrict__ pos,
                                            const uint32_t* __restrict__ cs, float4* __restrict__ smoothPos,
                                            float4* __restrict__ g, uint32_t i) {
@@ -70,6 +78,19 @@ __device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* _
   const float r2max = A.radius * A.radius;
   const float invR = 1.0f / A.radius;
   const F3 rel = {xi.x - A.boxMin[0], xi.y - A.boxMin[1], xi.z - A.boxMin[2]};
+  // Row trimming: a candidate binned into cell X lies within `moved` of X's box
+  // (the first and last cell of an axis taken as reaching to -inf / +inf, since
+  // the sort clamps positions beyond the grid into them), so a cell whose box is
+  // at least radius + moved + slack away holds none with r^2 < radius^2. Per row
+  // only the x cells closer than that are walked: a sub-range of the row's
+  // candidates in the same order, so the sums are the reference loop's.
+  float lim2 = -1.0f;
+  if (A.dispCount > 0) {
+    float moved = 0.0f;
+    for (int t = 0; t < A.dispCount; t++) moved += __ldg(&A.disp[t]);
+    const float lim = A.radius + moved * 1.001f + 1.0e-3f * A.support;
+    lim2 = lim * lim;
+  }
   F3 sd = {0.f, 0.f, 0.f};
   M3 m2 = {{{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}}};
   float wsum = 0.0f;
@@ -86,7 +107,17 @@ __device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* _
       const float dyMin = fmaxf(fmaxf((float)y * A.support - rel.y, rel.y - (float)(y + 1) * A.support), 0.0f);
       if (dz2 + dyMin * dyMin >= r2max) continue;
       const uint32_t rowBase = (uint32_t)((z * A.gridDim[1] + y) * A.gridDim[0]);
-      const uint32_t jb = __ldg(&cs[rowBase + x0]), je = min(__ldg(&cs[rowBase + x1 + 1]), A.count);
+      int xa = x0, xb = x1;
+      if (lim2 > 0.0f) {  // false for a NaN bound: no trimming
+        const float gz = open_gap(z, A.gridDim[2], rel.z, A.support), gy = open_gap(y, A.gridDim[1], rel.y, A.support);
+        const float half2 = lim2 - (gz * gz + gy * gy);
+        if (half2 <= 0.0f) continue;  // no candidate of the row is within the radius
+        const float half = sqrtf(half2);
+        // clamped into [x0, x1], so an infinite bound walks the whole row
+        xa = max(x0, min(x1, __float2int_rd((rel.x - half) * A.invSupport)));
+        xb = min(x1, max(x0, __float2int_rd((rel.x + half) * A.invSupport)));
+      }
+      const uint32_t jb = __ldg(&cs[rowBase + xa]), je = min(__ldg(&cs[rowBase + xb + 1]), A.count);
       for (uint32_t j = jb; j < je; j++) {
         const F3 d = sub3(xyz(__ldg(&pos[j])), xi);
         const float r2 = dot3(d, d);

@@ -66,6 +66,12 @@ struct AnisoParams {
   int32_t gridDim[3]; int32_t cells;
   float kr, kn, ks, stretch;
   float minExtent; int32_t neps;
+  // Row trimming (not in the reference's loop; it only skips candidates whose
+  // r^2 >= radius^2 for certain): dispCount > 0 when every particle is known to
+  // lie within the sum of disp[0 .. dispCount) of the position its cell was
+  // binned by (the last substep's iterations since its sort); 0 turns it off.
+  const float* disp;
+  int32_t dispCount;
 };
 
 // Mesh uniform (src/mesh_wgsl.js:3-21, packed by src/mesh.js:137-153).

@@ -174,6 +174,37 @@ def test_aniso_bit_exact():
     assert np.array_equal(g.read("aniso")[: 2 * n], o.buffer("aniso")[: 2 * n])
 
 
+def test_aniso_after_many_frames_and_moves():
+    """The anisotropic pass after every frame of a splashing scene whose box is not
+    a whole number of cells (particles beyond the grid are binned into the end
+    cells), after a resize and after positions are written: the cells it skips
+    as out of reach never change a bit."""
+    p = small_params(bodies=["sphere:0.5"], bodySize=0.06, targetParticleCount=4000)
+    g, o = pair(p)
+    a = configs.medium_aniso_params()
+    n = g.info()["n"]
+
+    def check():
+        for s in (g, o):
+            s.aniso(a)
+        assert np.array_equal(g.read("smoothPos")[:n], o.buffer("smoothPos")[:n])
+        assert np.array_equal(g.read("aniso")[: 2 * n], o.buffer("aniso")[: 2 * n])
+    for f in range(12):
+        for s in (g, o):
+            s.step(1 / 60)
+            if f == 4:
+                s.applyRayImpulse([0.0, 0.1, 0.15], [1.0, 0.0, 0.0], [6.0, 2.0, 0.0], 0.3, 4.0)
+        check()
+    for s in (g, o):
+        s.resizeBox([0.42, 0.4, 0.3])
+    check()
+    pos = g.read("pos")[:n].copy()
+    pos[: n // 2, 1] += 0.05
+    g.write("pos", pos)
+    o.write("pos", pos)
+    check()
+
+
 def test_interactive_calls_bit_exact():
     p = small_params(bodies=["sphere:0.5", "box:1.4"], bodySize=0.05, targetParticleCount=2000)
     g, o = pair(p)
