@@ -2670,22 +2670,45 @@ float o_optical(const ORay& R, f3 ro, f3 rd, float tMax) {
 
 // The mesh surface pass (src/mesh.js:380-396; meshDrawWGSL vs + fsSurf,
 // src/mesh_wgsl.js:268-321): the triangles in order into an eye-depth map (-1e4
-// where empty) and a normal map (w = 1 where covered). A pixel centre inside a
-// triangle or on its edge is covered; the depth test keeps the least screen depth,
-// ties to the lower triangle index; triangles with a vertex outside 0 <= z <= w
-// are dropped. World position and normal are interpolated perspective-correctly.
-struct OSurfTri {
-  v4o clip[3];
-  float sx[3], sy[3], sz[3], area;
-  f3 p[3], n[3];
+// where empty) and a normal map (w = 1 where covered). Each triangle is clipped to
+// 0 <= z <= w (Sutherland-Hodgman, near plane then far plane, the cut vertices'
+// clip coordinates, positions and normals interpolated linearly) and its visible
+// part drawn as a fan. A pixel centre inside a fan triangle or on its edge is
+// covered; the depth test keeps the least screen depth, ties to the lower
+// (triangle * 4 + fan index). World position and normal are interpolated
+// perspective-correctly.
+struct OSVert {
+  v4o c;
+  f3 p, n;
 };
-bool o_surf_tri(const orc_sim* s, const float* vp, int W, int H, size_t t, OSurfTri& T) {
+constexpr int kOClipMax = 5;
+OSVert o_lerp_vert(const OSVert& A, const OSVert& B, float t) {
+  OSVert o;
+  o.c = {A.c.x + t * (B.c.x - A.c.x), A.c.y + t * (B.c.y - A.c.y), A.c.z + t * (B.c.z - A.c.z),
+         A.c.w + t * (B.c.w - A.c.w)};
+  o.p = {A.p.x + t * (B.p.x - A.p.x), A.p.y + t * (B.p.y - A.p.y), A.p.z + t * (B.p.z - A.p.z)};
+  o.n = {A.n.x + t * (B.n.x - A.n.x), A.n.y + t * (B.n.y - A.n.y), A.n.z + t * (B.n.z - A.n.z)};
+  return o;
+}
+int o_clip_plane(const OSVert* in, int m, OSVert* out, int cap, bool far) {
+  int k = 0;
+  for (int a = 0; a < m; a++) {
+    const OSVert& A = in[a];
+    const OSVert& B = in[a + 1 < m ? a + 1 : 0];
+    const float da = far ? A.c.w - A.c.z : A.c.z, db = far ? B.c.w - B.c.z : B.c.z;
+    if (da >= 0.0f && k < cap) out[k++] = A;
+    if ((da >= 0.0f) != (db >= 0.0f) && k < cap) out[k++] = o_lerp_vert(A, B, da / (da - db));
+  }
+  return k;
+}
+int o_surf_clip(const orc_sim* s, const float* vp, size_t t, OSVert P[kOClipMax]) {
   const float voxel = (float)s->meshVoxel, origin = (float)s->meshOrigin;
+  OSVert a[3], b[kOClipMax - 1];
   for (int k = 0; k < 3; k++) {
     const uint32_t vx = s->meshVerts[(3 * t + k) * 2], vy = s->meshVerts[(3 * t + k) * 2 + 1];
     const float px = (float)(vx & 0xFFFFu) / 65535.0f, py = (float)(vx >> 16) / 65535.0f,
                 pz = (float)(vy & 0xFFFFu) / 65535.0f;
-    T.p[k] = {origin + px * (float)(s->meshDim[0] - 1) * voxel, origin + py * (float)(s->meshDim[1] - 1) * voxel,
+    a[k].p = {origin + px * (float)(s->meshDim[0] - 1) * voxel, origin + py * (float)(s->meshDim[1] - 1) * voxel,
               origin + pz * (float)(s->meshDim[2] - 1) * voxel};
     const uint32_t oct = vy >> 16;
     const float ex = (float)(oct & 0xFFu) / 255.0f * 2.0f - 1.0f, ey = (float)(oct >> 8) / 255.0f * 2.0f - 1.0f;
@@ -2693,12 +2716,27 @@ bool o_surf_tri(const orc_sim* s, const float* vp, int W, int H, size_t t, OSurf
     if (m.z < 0.0f)
       m = {(1.0f - std::fabs(m.y)) * (m.x >= 0.0f ? 1.0f : -1.0f), (1.0f - std::fabs(m.x)) * (m.y >= 0.0f ? 1.0f : -1.0f),
            m.z};
-    T.n[k] = nrm3(m);
-    T.clip[k] = mv4(vp, {T.p[k].x, T.p[k].y, T.p[k].z, 1.0f});
-    if (!(T.clip[k].w > 0.0f) || T.clip[k].z < 0.0f || T.clip[k].z > T.clip[k].w) return false;
-    T.sx[k] = (T.clip[k].x / T.clip[k].w * 0.5f + 0.5f) * (float)W;
-    T.sy[k] = (0.5f - T.clip[k].y / T.clip[k].w * 0.5f) * (float)H;
-    T.sz[k] = T.clip[k].z / T.clip[k].w;
+    a[k].n = nrm3(m);
+    a[k].c = mv4(vp, {a[k].p.x, a[k].p.y, a[k].p.z, 1.0f});
+  }
+  const int m = o_clip_plane(a, 3, b, kOClipMax - 1, false);
+  return o_clip_plane(b, m, P, kOClipMax, true);
+}
+struct OSurfTri {
+  v4o clip[3];
+  float sx[3], sy[3], sz[3], area;
+  f3 p[3], n[3];
+};
+bool o_fan_tri(const OSVert* P, int fan, int W, int H, OSurfTri& T) {
+  for (int k = 0; k < 3; k++) {
+    const OSVert& v = P[k == 0 ? 0 : fan + k];
+    T.clip[k] = v.c;
+    T.p[k] = v.p;
+    T.n[k] = v.n;
+    if (!(v.c.w > 0.0f)) return false;
+    T.sx[k] = (v.c.x / v.c.w * 0.5f + 0.5f) * (float)W;
+    T.sy[k] = (0.5f - v.c.y / v.c.w * 0.5f) * (float)H;
+    T.sz[k] = v.c.z / v.c.w;
   }
   T.area = (T.sx[1] - T.sx[0]) * (T.sy[2] - T.sy[0]) - (T.sx[2] - T.sx[0]) * (T.sy[1] - T.sy[0]);
   return T.area != 0.0f;
@@ -2726,24 +2764,28 @@ void o_surface(const orc_sim* s, const float* view, const float* vp, int W, int 
   std::vector<uint64_t> key(px, ~0ull);
   const size_t tris = s->meshVerts.size() / 6;
   for (size_t t = 0; t < tris; t++) {
-    OSurfTri T;
-    if (!o_surf_tri(s, vp, W, H, t, T)) continue;
-    const float lx = std::fmin(T.sx[0], std::fmin(T.sx[1], T.sx[2])), hx = std::fmax(T.sx[0], std::fmax(T.sx[1], T.sx[2]));
-    const float ly = std::fmin(T.sy[0], std::fmin(T.sy[1], T.sy[2])), hy = std::fmax(T.sy[0], std::fmax(T.sy[1], T.sy[2]));
-    const int x0 = (int)std::fmax(std::ceil(lx - 0.5f), 0.0f), x1 = (int)std::fmin(std::floor(hx - 0.5f), (float)W - 1.0f);
-    const int y0 = (int)std::fmax(std::ceil(ly - 0.5f), 0.0f), y1 = (int)std::fmin(std::floor(hy - 0.5f), (float)H - 1.0f);
-    for (int y = y0; y <= y1; y++)
-      for (int x = x0; x <= x1; x++) {
-        float b[3];
-        if (!o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b)) continue;
-        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;  // -0 -> +0
-        if (!(depth < 1.0f)) continue;
-        uint32_t bits;
-        memcpy(&bits, &depth, 4);
-        const uint64_t k = ((uint64_t)bits << 32) | (uint32_t)t;
-        uint64_t& slot = key[(size_t)y * W + x];
-        if (k < slot) slot = k;
-      }
+    OSVert P[kOClipMax];
+    const int m = o_surf_clip(s, vp, t, P);
+    for (int fan = 0; fan + 2 < m; fan++) {
+      OSurfTri T;
+      if (!o_fan_tri(P, fan, W, H, T)) continue;
+      const float lx = std::fmin(T.sx[0], std::fmin(T.sx[1], T.sx[2])), hx = std::fmax(T.sx[0], std::fmax(T.sx[1], T.sx[2]));
+      const float ly = std::fmin(T.sy[0], std::fmin(T.sy[1], T.sy[2])), hy = std::fmax(T.sy[0], std::fmax(T.sy[1], T.sy[2]));
+      const int x0 = (int)std::fmax(std::ceil(lx - 0.5f), 0.0f), x1 = (int)std::fmin(std::floor(hx - 0.5f), (float)W - 1.0f);
+      const int y0 = (int)std::fmax(std::ceil(ly - 0.5f), 0.0f), y1 = (int)std::fmin(std::floor(hy - 0.5f), (float)H - 1.0f);
+      for (int y = y0; y <= y1; y++)
+        for (int x = x0; x <= x1; x++) {
+          float b[3];
+          if (!o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b)) continue;
+          const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;  // -0 -> +0
+          if (!(depth < 1.0f)) continue;
+          uint32_t bits;
+          memcpy(&bits, &depth, 4);
+          const uint64_t k = ((uint64_t)bits << 32) | (uint32_t)(t * 4 + (size_t)fan);
+          uint64_t& slot = key[(size_t)y * W + x];
+          if (k < slot) slot = k;
+        }
+    }
   }
   surfZ.assign(px, -1.0e4f);
   surfN.assign(px, f3{0.0f, 0.0f, 0.0f});
@@ -2751,10 +2793,13 @@ void o_surface(const orc_sim* s, const float* view, const float* vp, int W, int 
     for (int x = 0; x < W; x++) {
       const size_t o = (size_t)y * W + x;
       if (key[o] == ~0ull) continue;
+      const uint32_t id = (uint32_t)(key[o] & 0xffffffffu);
+      const int fan = (int)(id & 3u);
+      OSVert P[kOClipMax];
+      const int m = o_surf_clip(s, vp, id >> 2, P);
       OSurfTri T;
       float b[3];
-      if (!o_surf_tri(s, vp, W, H, (size_t)(key[o] & 0xffffffffu), T) ||
-          !o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b))
+      if (!(fan + 2 < m) || !o_fan_tri(P, fan, W, H, T) || !o_surf_bary(T, (float)x + 0.5f, (float)y + 0.5f, b))
         continue;
       const float q0 = b[0] / T.clip[0].w, q1 = b[1] / T.clip[1].w, q2 = b[2] / T.clip[2].w;
       const float qs = q0 + q1 + q2;

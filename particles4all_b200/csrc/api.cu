@@ -1596,6 +1596,8 @@ int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
   if (!s->ready) return fail(s, P4A_ERR_STATE, "ray before reset");
   if (s->meshDim[0] < 2 || !s->meshField[s->fieldSlot])
     return fail(s, P4A_ERR_STATE, "ray needs the density field of p4a_mesh");
+  if (rp->use_surface && s->meshTriCap >= (1u << 30))  // the depth test keys hold triangle * 4 + fan index
+    return fail(s, P4A_ERR_CAPACITY, "p4a_ray: the mesh surface pass takes at most 2^30 triangles");
   cudaSetDevice(s->device);
   const size_t px = (size_t)rp->width * rp->height;
   if (px > s->rayCap) {

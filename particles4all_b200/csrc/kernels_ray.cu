@@ -11,7 +11,7 @@
 // normal map (the surface pass below: a triangle per thread, pixel centres inside
 // the triangle or on its edges, depth test 'less' as an atomicMin of (depth bits,
 // triangle), perspective-correct world position and normal in a resolve pass;
-// triangles with a vertex outside 0 <= z <= w are dropped rather than clipped).
+// triangles are clipped to 0 <= z <= w first, their visible part drawn as a fan).
 // The field is the one p4a_mesh produced (SurfaceMesh.generateField + smoothField).
 // Float contract as in kernels_ssfr.cu; acos in debug view 5 is replaced by the
 // equivalent comparison of |n.y| against the cosines of the thresholds.
@@ -284,20 +284,67 @@ __device__ __forceinline__ void unpack_vertex(const SurfGrid& G, uint2 v, F3& p,
   }
   n = normalize3(m);
 }
-struct Tri {
-  V4 clip[3];
-  float sx[3], sy[3], sz[3], area;
+// A vertex of a triangle's visible part: clip coordinates, world position, normal.
+struct SVert {
+  V4 c;
+  F3 p, n;
 };
-__device__ __forceinline__ bool setup_tri(const RayParams& R, const SurfGrid& G, const uint2* __restrict__ verts,
-                                          uint32_t t, Tri& T, F3 p[3], F3 n[3]) {
+constexpr int kClipMax = 5;  // a triangle cut by the two depth planes keeps at most 5 vertices
+__device__ __forceinline__ SVert lerp_vert(const SVert& A, const SVert& B, float t) {
+  SVert o;
+  o.c = {A.c.x + t * (B.c.x - A.c.x), A.c.y + t * (B.c.y - A.c.y), A.c.z + t * (B.c.z - A.c.z),
+         A.c.w + t * (B.c.w - A.c.w)};
+  o.p = {A.p.x + t * (B.p.x - A.p.x), A.p.y + t * (B.p.y - A.p.y), A.p.z + t * (B.p.z - A.p.z)};
+  o.n = {A.n.x + t * (B.n.x - A.n.x), A.n.y + t * (B.n.y - A.n.y), A.n.z + t * (B.n.z - A.n.z)};
+  return o;
+}
+// One Sutherland-Hodgman step: the part of polygon in[0..m) where the plane's
+// distance (z for the near plane, w - z for the far one) is >= 0, at most `cap`
+// vertices. Clip-space attributes are affine in clip space, so the cut vertices
+// interpolate them linearly, as the rasteriser's clipper does.
+template <bool Far>
+__device__ __forceinline__ int clip_plane(const SVert* in, int m, SVert* out, int cap) {
+  int k = 0;
+  for (int a = 0; a < m; a++) {
+    const SVert& A = in[a];
+    const SVert& B = in[a + 1 < m ? a + 1 : 0];
+    const float da = Far ? A.c.w - A.c.z : A.c.z, db = Far ? B.c.w - B.c.z : B.c.z;
+    if (da >= 0.0f && k < cap) out[k++] = A;
+    if ((da >= 0.0f) != (db >= 0.0f) && k < cap) out[k++] = lerp_vert(A, B, da / (da - db));
+  }
+  return k;
+}
+// Triangle t clipped to 0 <= z <= w: its visible part as a convex polygon P[0..m),
+// drawn as the fan (P[0], P[s + 1], P[s + 2]), s < m - 2. Returns m (< 3: nothing).
+__device__ __forceinline__ int clip_triangle(const RayParams& R, const SurfGrid& G, const uint2* __restrict__ verts,
+                                             uint32_t t, SVert P[kClipMax]) {
+  SVert a[3], b[kClipMax - 1];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    unpack_vertex(G, __ldg(&verts[3 * (size_t)t + k]), p[k], n[k]);
-    T.clip[k] = mat_vec4(R.vp, {p[k].x, p[k].y, p[k].z, 1.0f});
-    if (!(T.clip[k].w > 0.0f) || T.clip[k].z < 0.0f || T.clip[k].z > T.clip[k].w) return false;
-    T.sx[k] = (T.clip[k].x / T.clip[k].w * 0.5f + 0.5f) * (float)R.width;
-    T.sy[k] = (0.5f - T.clip[k].y / T.clip[k].w * 0.5f) * (float)R.height;
-    T.sz[k] = T.clip[k].z / T.clip[k].w;
+    unpack_vertex(G, __ldg(&verts[3 * (size_t)t + k]), a[k].p, a[k].n);
+    a[k].c = mat_vec4(R.vp, {a[k].p.x, a[k].p.y, a[k].p.z, 1.0f});
+  }
+  const int m = clip_plane<false>(a, 3, b, kClipMax - 1);
+  return clip_plane<true>(b, m, P, kClipMax);
+}
+struct Tri {
+  V4 clip[3];
+  F3 p[3], n[3];
+  float sx[3], sy[3], sz[3], area;
+};
+// Fan triangle s of polygon P in screen space; false when it has no area or a
+// vertex at or behind the eye.
+__device__ __forceinline__ bool fan_tri(const RayParams& R, const SVert* P, int s, Tri& T) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const SVert& v = P[k == 0 ? 0 : s + k];
+    T.clip[k] = v.c;
+    T.p[k] = v.p;
+    T.n[k] = v.n;
+    if (!(v.c.w > 0.0f)) return false;
+    T.sx[k] = (v.c.x / v.c.w * 0.5f + 0.5f) * (float)R.width;
+    T.sy[k] = (0.5f - v.c.y / v.c.w * 0.5f) * (float)R.height;
+    T.sz[k] = v.c.z / v.c.w;
   }
   T.area = (T.sx[1] - T.sx[0]) * (T.sy[2] - T.sy[0]) - (T.sx[2] - T.sx[0]) * (T.sy[1] - T.sy[0]);
   return T.area != 0.0f;
@@ -326,23 +373,27 @@ __global__ void k_surf_raster(const __grid_constant__ RayParams R, const __grid_
                               unsigned long long* __restrict__ key) {
   const uint32_t count = min(__ldg(total), cap);
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-    Tri T;
-    F3 p[3], n[3];
-    if (!setup_tri(R, G, verts, t, T, p, n)) continue;
-    const float lo_x = fminf(T.sx[0], fminf(T.sx[1], T.sx[2])), hi_x = fmaxf(T.sx[0], fmaxf(T.sx[1], T.sx[2]));
-    const float lo_y = fminf(T.sy[0], fminf(T.sy[1], T.sy[2])), hi_y = fmaxf(T.sy[0], fmaxf(T.sy[1], T.sy[2]));
-    const int x0 = (int)fmaxf(ceilf(lo_x - 0.5f), 0.0f), x1 = (int)fminf(floorf(hi_x - 0.5f), (float)R.width - 1.0f);
-    const int y0 = (int)fmaxf(ceilf(lo_y - 0.5f), 0.0f), y1 = (int)fminf(floorf(hi_y - 0.5f), (float)R.height - 1.0f);
-    for (int py = y0; py <= y1; py++)
-      for (int px = x0; px <= x1; px++) {
-        float b[3];
-        if (!bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) continue;
-        // + 0 turns a -0 (a zero weight negated for the winding) into +0, so that the
-        // bits of every depth >= 0 order as the values do
-        const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;
-        if (!(depth < 1.0f)) continue;
-        atomicMin(&key[(size_t)py * R.width + px], ((unsigned long long)__float_as_uint(depth) << 32) | t);
-      }
+    SVert P[kClipMax];
+    const int m = clip_triangle(R, G, verts, t, P);
+    for (int s = 0; s + 2 < m; s++) {
+      Tri T;
+      if (!fan_tri(R, P, s, T)) continue;
+      const float lo_x = fminf(T.sx[0], fminf(T.sx[1], T.sx[2])), hi_x = fmaxf(T.sx[0], fmaxf(T.sx[1], T.sx[2]));
+      const float lo_y = fminf(T.sy[0], fminf(T.sy[1], T.sy[2])), hi_y = fmaxf(T.sy[0], fmaxf(T.sy[1], T.sy[2]));
+      const int x0 = (int)fmaxf(ceilf(lo_x - 0.5f), 0.0f), x1 = (int)fminf(floorf(hi_x - 0.5f), (float)R.width - 1.0f);
+      const int y0 = (int)fmaxf(ceilf(lo_y - 0.5f), 0.0f), y1 = (int)fminf(floorf(hi_y - 0.5f), (float)R.height - 1.0f);
+      const unsigned long long id = (unsigned long long)(t * 4u + (uint32_t)s);
+      for (int py = y0; py <= y1; py++)
+        for (int px = x0; px <= x1; px++) {
+          float b[3];
+          if (!bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) continue;
+          // + 0 turns a -0 (a zero weight negated for the winding) into +0, so that the
+          // bits of every depth >= 0 order as the values do
+          const float depth = b[0] * T.sz[0] + b[1] * T.sz[1] + b[2] * T.sz[2] + 0.0f;
+          if (!(depth < 1.0f)) continue;
+          atomicMin(&key[(size_t)py * R.width + px], ((unsigned long long)__float_as_uint(depth) << 32) | id);
+        }
+    }
   }
 }
 __global__ void k_surf_resolve(const __grid_constant__ RayParams R, const __grid_constant__ SurfGrid G,
@@ -355,14 +406,17 @@ __global__ void k_surf_resolve(const __grid_constant__ RayParams R, const __grid
   float z = -1.0e4f;
   float4 nn = make_float4(0.f, 0.f, 0.f, 0.f);
   if (k != ~0ull) {
+    const uint32_t id = (uint32_t)(k & 0xffffffffu), s = id & 3u;
+    SVert P[kClipMax];
+    const int m = clip_triangle(R, G, verts, id >> 2, P);
     Tri T;
-    F3 p[3], n[3];
     float b[3];
-    if (setup_tri(R, G, verts, (uint32_t)(k & 0xffffffffu), T, p, n) &&
-        bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) {
+    if ((int)s + 2 < m && fan_tri(R, P, (int)s, T) && bary(T, (float)px + 0.5f, (float)py + 0.5f, b)) {
       // perspective-correct interpolation of the world position and the normal
       const float q0 = b[0] / T.clip[0].w, q1 = b[1] / T.clip[1].w, q2 = b[2] / T.clip[2].w;
       const float qs = q0 + q1 + q2;
+      const F3* p = T.p;
+      const F3* n = T.n;
       const F3 wp = {(q0 * p[0].x + q1 * p[1].x + q2 * p[2].x) / qs, (q0 * p[0].y + q1 * p[1].y + q2 * p[2].y) / qs,
                      (q0 * p[0].z + q1 * p[1].z + q2 * p[2].z) / qs};
       const F3 wn = {(q0 * n[0].x + q1 * n[1].x + q2 * n[2].x) / qs, (q0 * n[0].y + q1 * n[1].y + q2 * n[2].y) / qs,

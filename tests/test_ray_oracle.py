@@ -210,3 +210,76 @@ def test_mesh_surface_against_float64(built):
             assert np.abs(normals[py, px, :3] - want).max() <= 2, (px, py, normals[py, px], want)
             checked += 1
     assert checked > 100 and misses > 100, (checked, misses)
+
+
+def test_mesh_surface_clipped_at_the_near_plane(built):
+    """The eye just above the block's top face, looking down across it: the near
+    plane cuts the triangles of the face in front of the eye, and the pixels there
+    show what lies beyond the plane (the block's far faces, seen from inside), as
+    a rasteriser that clips does. Distance and normal against float64 ray /
+    triangle intersections restricted to 0 <= z <= w in clip space."""
+    o, p = block_with_field()
+    pos, nrm = mesh_triangles(o, p)
+    c = pos.reshape(-1, 3)
+    top = c[(np.abs(c[:, 0] - 2.0) < 1.0) & (np.abs(c[:, 2] - 2.0) < 1.0), 1].max()
+    w, h = 48, 36
+    cam = Camera()
+    cam.target = [2.0, float(top), 2.0]
+    cam.az, cam.el, cam.dist = 0.3, 0.6, 0.05  # eye 0.03 above the face; the cut lies ~0.1 ahead
+    m = frame_matrices(cam, w, h)
+    rp = default_ray()
+    rp.update({k: m[k] for k in ("view", "proj", "inv_view_proj", "inv_view", "eye", "width", "height")})
+    rp.update(debug=2, use_surface=1)
+    dist = o.ray(rp)
+    normals = o.ray(dict(rp, debug=1))
+    pv = (np.array(m["proj"], np.float64).reshape(4, 4).T @ np.array(m["view"], np.float64).reshape(4, 4).T)
+
+    def visible_hit(ro, rd):
+        a, b, cc = pos[:, 0], pos[:, 1], pos[:, 2]
+        e1, e2 = b - a, cc - a
+        pvec = np.cross(rd, e2)
+        det = (e1 * pvec).sum(1)
+        ok = np.abs(det) > 1e-14
+        inv = np.where(ok, 1 / np.where(ok, det, 1), 0)
+        tv = ro - a
+        u = (tv * pvec).sum(1) * inv
+        qv = np.cross(tv, e1)
+        v = (qv @ rd) * inv
+        t = (qv * e2).sum(1) * inv
+        hit = ok & (u >= 0) & (v >= 0) & (u + v <= 1) & (t > 0)
+        pts = ro + t[:, None] * rd
+        clip = np.c_[pts, np.ones(len(pts))] @ pv.T
+        front = hit & (clip[:, 2] < 0)                      # cut away by the near plane
+        vis = hit & (clip[:, 2] >= 0) & (clip[:, 2] <= clip[:, 3])
+        margin = np.abs(clip[:, 2]) < 1e-3 * clip[:, 3]
+        if not vis.any():
+            return None, front.any(), False
+        i = np.flatnonzero(vis)[np.argmin(t[vis])]
+        return (t[i], np.array([1 - u[i] - v[i], u[i], v[i]]), i), front.any(), bool((hit & margin).any())
+
+    hits = {}
+    for py in range(h):
+        for px in range(w):
+            ro, rd = render_f64.pixel_ray(m, w, h, px, py, from_eye=True)
+            hits[px, py] = visible_hit(ro, rd) + (rd,)
+    checked = clipped = 0
+    for py in range(1, h - 1):
+        for px in range(1, w - 1):
+            hit, front, edge, rd = hits[px, py]
+            ts = [hits[px + dx, py + dy][0] for dx in (-1, 0, 1) for dy in (-1, 0, 1)]
+            if edge or any(x is None for x in ts) or max(x[0] for x in ts) - min(x[0] for x in ts) > 0.3:
+                continue  # near the silhouette, the cut line or a depth jump
+            t, bc, i = hit
+            frac = t - math.floor(t)
+            if min(frac, 1 - frac) > 0.01 and min(t * 0.1 % 1, 1 - t * 0.1 % 1) > 0.01:
+                want = render_f64.rgba8([frac, (t * 0.1) % 1.0, 0.0])
+                assert np.abs(dist[py, px, :3] - want).max() <= 2, (px, py, dist[py, px], want, t)
+            n = bc @ nrm[i]
+            n /= np.linalg.norm(n)
+            if n @ rd > 0:
+                n = -n
+            want = render_f64.rgba8(n * 0.5 + 0.5)
+            assert np.abs(normals[py, px, :3] - want).max() <= 2, (px, py, normals[py, px], want)
+            checked += 1
+            clipped += front
+    assert checked > 200 and clipped > 50, (checked, clipped)
