@@ -309,6 +309,24 @@ int p4a_default_mesh_params(p4a_mesh_params* out);
 int p4a_mesh(p4a_sim* s, const p4a_mesh_params* mp, int64_t* triangles);
 int p4a_mesh_get_info(p4a_sim* s, p4a_mesh_info* out);
 
+/* ---- environment map (src/env.js:149-242) ------------------------------- */
+/*
+ * Environment.load / clear: `rgb` is an equirectangular panorama, float RGB,
+ * `height` rows of `width` pixels, top row first (a decoded .hdr or image; the
+ * Python package's hdr.load_hdr decodes Radiance .hdr files). It must be 2:1
+ * (width within 2 * height +- 2). The library resamples it on the host into a cube
+ * map of face size min(2048, max(16, width / 4)), rgba16float, as the reference
+ * does, and keeps it on the device; p4a_ssfr and p4a_ray then take the sky, the
+ * floor's far colour and reflections from it (times env_intensity, turned by
+ * env_yaw). rgb = NULL clears it. The reference's viewer also turns the floor plane
+ * off when a panorama loads, unless it was set explicitly: set floor_plane in the
+ * render parameters to match.
+ */
+int p4a_set_environment(p4a_sim* s, const float* rgb, int32_t width, int32_t height);
+/* The cube map's face size (0 when none) and, when `host` is not NULL, its
+ * 6 * size * size texels of 4 halves each (face, row, column order), `bytes` at most. */
+int p4a_environment_read(p4a_sim* s, int32_t* face_size, void* host, size_t bytes);
+
 /* ---- screen-space fluid rendering (src/ssfr.js:7-356) ------------------- */
 /*
  * FluidSSFR.render on the simulation's live buffers into headless device images:
@@ -322,7 +340,7 @@ int p4a_mesh_get_info(p4a_sim* s, p4a_mesh_info* out);
  * invViewProj, invView of src/render.js:203-258). `bodies` is the rigid-body
  * renderer's packed buffer (6 float4 per body: centre + shape code, half extents,
  * three rotation rows, colour; src/ssfr_composite_wgsl.js:67-84), or NULL with
- * body_count 0. Environment maps are not supported (hasEnvMap = 0).
+ * body_count 0. With an environment map set (p4a_set_environment), hasEnvMap = 1.
  * Depth ties keep the lower particle index (the first drawn); the thickness is
  * summed in fixed point, so every buffer is the same bits on every run.
  */
@@ -358,6 +376,8 @@ typedef struct p4a_ssfr_params {
   int32_t floor_plane;            /* 1                                             */
   int32_t debug;                  /* 0 shaded, 1 normals, 2 depth, 3 thickness,
                                      4 unfiltered depth, 5 body depth              */
+  double env_intensity;           /* environment map intensity, 1.0 (env.intensity) */
+  double env_yaw;                 /* environment map yaw in radians, 0 (env.yaw)   */
 } p4a_ssfr_params;
 typedef struct p4a_ssfr_info {
   int32_t width, height;          /* image                                         */
@@ -383,7 +403,7 @@ int p4a_ssfr_read(p4a_sim* s, int32_t which, void* host, size_t bytes);
  * use_surface = 0). Either way it is shaded with Fresnel reflection, absorption
  * along the refracted ray's optical depth through the field, the GGX sun
  * highlight, sky / floor and rigid bodies (`bodies` as for p4a_ssfr). The image is
- * RGBA8, width x height. Environment maps are not supported.
+ * RGBA8, width x height. With an environment map set, hasEnvMap = 1.
  */
 typedef struct p4a_ray_params {
   float proj[16], inv_view_proj[16], inv_view[16];
@@ -408,6 +428,8 @@ typedef struct p4a_ray_params {
                                  into eye-depth and normal maps give the surface;
                                  0 the field is marched                          */
   float view[16];             /* view matrix, for the mesh surface pass          */
+  double env_intensity;       /* environment map intensity, 1.0                  */
+  double env_yaw;             /* environment map yaw in radians, 0               */
 } p4a_ray_params;
 int p4a_default_ray_params(p4a_ray_params* out);
 int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t body_count);

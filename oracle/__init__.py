@@ -52,6 +52,7 @@ def lib():
             "orc_grid_sort": [vp, i32, C.c_float, C.c_float] + [vp] * 11,
             "orc_ssfr": [vp, vp, vp, i32], "orc_ssfr_buffer": [vp, i32, C.POINTER(vp), C.POINTER(C.c_size_t)],
             "orc_ray": [vp, vp, vp, i32], "orc_ray_image": [vp, C.POINTER(vp), C.POINTER(C.c_size_t)],
+            "orc_set_environment": [vp, vp, i32, i32], "orc_environment": [vp, C.POINTER(vp), C.POINTER(i32)],
         }.items():
             f = getattr(L, name)
             f.argtypes = args
@@ -238,6 +239,24 @@ class OracleSim:
         _check(self._L.orc_ray_image(self._h, C.byref(p), C.byref(nb)), "ray_image")
         raw = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint8)), (nb.value,)).copy()
         return raw.reshape(rp.height, rp.width, 4)
+
+    def set_environment(self, rgb):
+        """Environment.load restated (same arguments as Sim.set_environment)."""
+        if rgb is None:
+            _check(self._L.orc_set_environment(self._h, None, 0, 0), "set_environment")
+            return
+        a = np.ascontiguousarray(rgb, np.float32)
+        _check(self._L.orc_set_environment(self._h, a.ctypes.data, a.shape[1], a.shape[0]), "set_environment")
+
+    def environment(self):
+        """The cube map as uint16 half-float bits [6, size, size, 4], or None."""
+        p, size = C.c_void_p(), C.c_int32()
+        _check(self._L.orc_environment(self._h, C.byref(p), C.byref(size)), "environment")
+        if size.value == 0:
+            return None
+        n = 6 * size.value * size.value * 4
+        raw = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_uint16)), (n,)).copy()
+        return raw.reshape(6, size.value, size.value, 4)
 
     def info(self):
         i = _abi.Info()

@@ -459,6 +459,8 @@ struct orc_sim {
   std::vector<uint32_t> rayImage;
   int rayDims[2] = {0, 0};
   std::vector<uint32_t> meshVerts;  // 2 words per vertex
+  std::vector<uint16_t> envCube;    // 6 faces of envSize^2 texels, 4 halves each
+  int envSize = 0;
   int64_t meshTris = 0;
   bool ready = false;
 };
@@ -2102,13 +2104,94 @@ void o_filter(const OFilt& F, const std::vector<float>& in, std::vector<float>& 
 }
 
 // composite (src/ssfr_composite_wgsl.js)
+// Environment map uniforms (src/ray_wgsl.js:29-31, 46-50): size 0 = none.
+struct OEnv {
+  const uint16_t* texels;
+  int size;
+  float intensity, yawCos, yawSin;
+};
 struct OComp {
   const float *ivp, *iv;
   f3 boxMin, absorb, sunDir;
   float proj00, proj11, ior, sunIntensity, roughness, exposure, groundReflection, thicknessScale;
   int bodyCount, floorPlane, debug;
   const float* bdata;  // 24 floats per body
+  OEnv env;
 };
+// IEEE half to float, exactly.
+float o_half_to_float(uint16_t h) {
+  const uint32_t sgn = (uint32_t)(h & 0x8000u) << 16, e = (h >> 10) & 0x1fu, m = h & 0x3ffu;
+  uint32_t bits;
+  if (e == 0) {
+    if (m == 0) {
+      bits = sgn;
+    } else {  // subnormal: m * 2^-24
+      const float v = (float)m * 5.9604644775390625e-8f;
+      std::memcpy(&bits, &v, 4);
+      bits |= sgn;
+    }
+  } else if (e == 31) {
+    bits = sgn | 0x7f800000u | (m << 13);
+  } else {
+    bits = sgn | ((e + 112u) << 23) | (m << 13);
+  }
+  float v;
+  std::memcpy(&v, &bits, 4);
+  return v;
+}
+// textureSampleLevel(cube, linear clamp-to-edge sampler, d, 0): the face of the
+// largest component (x, then y, then z on ties), (s, t) on it, bilinear within the
+// face with its edges clamped.
+f3 o_cube_sample(const OEnv& E, f3 d) {
+  const float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+  int face;
+  float ma, sc, tc;
+  if (ax >= ay && ax >= az) {
+    face = d.x >= 0.0f ? 0 : 1;
+    ma = ax;
+    sc = d.x >= 0.0f ? -d.z : d.z;
+    tc = -d.y;
+  } else if (ay >= az) {
+    face = d.y >= 0.0f ? 2 : 3;
+    ma = ay;
+    sc = d.x;
+    tc = d.y >= 0.0f ? d.z : -d.z;
+  } else {
+    face = d.z >= 0.0f ? 4 : 5;
+    ma = az;
+    sc = d.z >= 0.0f ? d.x : -d.x;
+    tc = -d.y;
+  }
+  const float n = (float)E.size;
+  const float u = std::fmin(std::fmax(0.5f * (sc / ma + 1.0f) * n - 0.5f, -1.0f), n);
+  const float v = std::fmin(std::fmax(0.5f * (tc / ma + 1.0f) * n - 0.5f, -1.0f), n);
+  const float fu = std::floor(u), fv = std::floor(v);
+  const float tx = u - fu, ty = v - fv;
+  const int x0 = std::max((int)fu, 0), x1 = std::min((int)fu + 1, E.size - 1);
+  const int y0 = std::max((int)fv, 0), y1 = std::min((int)fv + 1, E.size - 1);
+  auto texel = [&](int y, int x) {
+    const uint16_t* t = E.texels + ((((size_t)face * E.size + y) * E.size) + x) * 4;
+    return f3{o_half_to_float(t[0]), o_half_to_float(t[1]), o_half_to_float(t[2])};
+  };
+  const f3 top = mixo(texel(y0, x0), texel(y0, x1), tx), bot = mixo(texel(y1, x0), texel(y1, x1), tx);
+  return mixo(top, bot, ty);
+}
+// envSample (src/ray_wgsl.js:46-50).
+f3 o_env_sample(const OEnv& E, f3 d) {
+  const f3 r = {E.yawCos * d.x + E.yawSin * d.z, d.y, -E.yawSin * d.x + E.yawCos * d.z};
+  const f3 c = o_cube_sample(E, r);
+  return {c.x * E.intensity, c.y * E.intensity, c.z * E.intensity};
+}
+OEnv o_env_uniform(const orc_sim* s, double intensity, double yaw) {
+  OEnv E{};
+  E.texels = s->envCube.data();
+  E.size = s->envCube.empty() ? 0 : s->envSize;
+  E.intensity = (float)intensity;
+  const float y = (float)yaw;
+  E.yawCos = (float)std::cos((double)y);
+  E.yawSin = (float)std::sin((double)y);
+  return E;
+}
 f3 o_bd(const OComp& C, int k) { return {C.bdata[k * 4], C.bdata[k * 4 + 1], C.bdata[k * 4 + 2]}; }
 float o_body_dist(const OComp& C, int i, f3 p) {
   const int b = i * 6;
@@ -2155,6 +2238,7 @@ OTrace o_trace(const OComp& C, f3 ro, f3 rd, float tMax) {
 }
 const f3 kHazeO = {0.62f, 0.74f, 0.90f};
 f3 o_sky(const OComp& C, f3 d) {
+  if (C.env.size > 0) return o_env_sample(C.env, d);
   const float h = clampo(d.y, 0.0f, 1.0f);
   f3 c = mixo(kHazeO, {0.25f, 0.48f, 0.85f}, sstep(0.0f, 0.16f, h));
   c = mixo(c, {0.09f, 0.28f, 0.72f}, sstep(0.10f, 0.85f, h));
@@ -2179,7 +2263,7 @@ f3 o_background(const OComp& C, f3 o, f3 d) {
     if (t > 0.0f) {
       const f3 p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
       const float fade = 1.0f - orc_exp(-0.02f * t);
-      return mixo(o_floor(p), kHazeO, fade);
+      return mixo(o_floor(p), C.env.size > 0 ? o_env_sample(C.env, d) : kHazeO, fade);
     }
   }
   return o_sky(C, d);
@@ -2194,6 +2278,7 @@ f3 o_shade_body(const OComp& C, f3 n, f3 base, f3 rd, f3 env) {
           base.z * k + 0.7f * spec + env.z * fres * 0.25f};
 }
 f3 o_env_reflect(const OComp& C, f3 d) {
+  if (C.env.size > 0) return o_env_sample(C.env, d);
   if (d.y >= 0.0f) return o_sky(C, d);
   return mixo(kHazeO, {0.32f, 0.325f, 0.335f}, clampo(-d.y * 4.0f, 0.0f, 1.0f));
 }
@@ -2377,6 +2462,7 @@ int orc_ssfr(orc_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t
   C.roughness = (float)q.roughness;
   C.exposure = (float)q.exposure;
   C.groundReflection = (float)q.ground_reflection;
+  C.env = o_env_uniform(s, q.env_intensity, q.env_yaw);
   C.thicknessScale = (float)q.thickness_scale;
   C.bodyCount = bodyCount;
   C.floorPlane = q.floor_plane ? 1 : 0;
@@ -2840,6 +2926,7 @@ int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
   C.roughness = (float)q.roughness;
   C.exposure = (float)q.exposure;
   C.groundReflection = (float)q.ground_reflection;
+  C.env = o_env_uniform(s, q.env_intensity, q.env_yaw);
   C.bodyCount = bodyCount;
   C.floorPlane = q.floor_plane ? 1 : 0;
   C.debug = q.debug;
@@ -2975,6 +3062,99 @@ int orc_ray_image(orc_sim* s, void** ptr, size_t* bytes) {
   if (!s || !ptr || !bytes) return P4A_ERR_ARG;
   *ptr = s->rayImage.data();
   *bytes = s->rayImage.size() * 4;
+  return P4A_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Environment.load (src/env.js:180-236), restated: the panorama resampled into the
+// base level of a cube map in double (the JS number type), each sample rounded to
+// float and then to half by toHalf (src/env.js:125-147).
+namespace {
+
+uint16_t o_to_half(float v) {
+  uint32_t x;
+  std::memcpy(&x, &v, 4);
+  const uint32_t sgn = (x >> 16) & 0x8000u;
+  const int e = (int)((x >> 23) & 0xffu) - 112;
+  uint32_t m = x & 0x7fffffu;
+  if (e <= 0) {
+    if (e < -10) return (uint16_t)sgn;
+    m = (m | 0x800000u) >> (1 - e);
+    return (uint16_t)(sgn | ((m + 0x1000u) >> 13));
+  }
+  if (e >= 0x1f) return (uint16_t)(sgn | 0x7c00u);
+  return (uint16_t)(sgn | ((uint32_t)e << 10) | ((m + 0x1000u) >> 13));
+}
+
+// The panorama's bilinear value in direction (dx, dy, dz) (sampleEquirect, src/env.js:94-113).
+void o_equirect(const float* src, int w, int h, double dx, double dy, double dz, float out[3]) {
+  const double kPiD = 3.14159265358979323846;
+  const double len = std::sqrt(dx * dx + dy * dy + dz * dz);
+  dx /= len;
+  dy /= len;
+  dz /= len;
+  const double u = 0.5 + std::atan2(dx, dz) / (2 * kPiD);
+  const double v = std::acos(std::min(1.0, std::max(-1.0, dy))) / kPiD;
+  const double fx = u * w - 0.5, fy = v * h - 0.5;
+  const double x0 = std::floor(fx), y0 = std::floor(fy);
+  const double tx = fx - x0, ty = fy - y0;
+  auto at = [&](long long x, long long y, int c) -> double {
+    x = ((x % w) + w) % w;
+    y = std::min<long long>(h - 1, std::max<long long>(0, y));
+    return src[(y * w + x) * 3 + c];
+  };
+  const long long ix = (long long)x0, iy = (long long)y0;
+  for (int c = 0; c < 3; c++) {
+    const double a = at(ix, iy, c) * (1 - tx) + at(ix + 1, iy, c) * tx;
+    const double b = at(ix, iy + 1, c) * (1 - tx) + at(ix + 1, iy + 1, c) * tx;
+    out[c] = (float)(a * (1 - ty) + b * ty);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_set_environment(orc_sim* s, const float* rgb, int32_t w, int32_t h) {
+  if (!s) return P4A_ERR_ARG;
+  s->envCube.clear();
+  s->envSize = 0;
+  if (!rgb) return P4A_OK;
+  if (w < 2 || h < 1 || w < 2 * h - 2 || w > 2 * h + 2) return P4A_ERR_ARG;
+  const int size = std::min(2048, std::max(16, w / 4));
+  s->envCube.assign((size_t)6 * size * size * 4, 0);
+  const uint16_t one = o_to_half(1.0f);
+  for (int f = 0; f < 6; f++)
+    for (int y = 0; y < size; y++) {
+      const double t = 2 * (y + 0.5) / size - 1;
+      for (int x = 0; x < size; x++) {
+        const double sv = 2 * (x + 0.5) / size - 1;
+        double d[3];  // faceDir (src/env.js:115-124)
+        if (f == 0) { d[0] = 1; d[1] = -t; d[2] = -sv; }
+        else if (f == 1) { d[0] = -1; d[1] = -t; d[2] = sv; }
+        else if (f == 2) { d[0] = sv; d[1] = 1; d[2] = t; }
+        else if (f == 3) { d[0] = sv; d[1] = -1; d[2] = -t; }
+        else if (f == 4) { d[0] = sv; d[1] = -t; d[2] = 1; }
+        else { d[0] = -sv; d[1] = -t; d[2] = -1; }
+        float c[3];
+        o_equirect(rgb, w, h, d[0], d[1], d[2], c);
+        uint16_t* o = &s->envCube[(((size_t)f * size + y) * size + x) * 4];
+        o[0] = o_to_half(c[0]);
+        o[1] = o_to_half(c[1]);
+        o[2] = o_to_half(c[2]);
+        o[3] = one;
+      }
+    }
+  s->envSize = size;
+  return P4A_OK;
+}
+
+int orc_environment(orc_sim* s, const void** ptr, int32_t* size) {
+  if (!s || !ptr || !size) return P4A_ERR_ARG;
+  *ptr = s->envCube.data();
+  *size = s->envSize;
   return P4A_OK;
 }
 

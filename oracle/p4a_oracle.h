@@ -69,6 +69,8 @@ int orc_ssfr_buffer(orc_sim* s, int32_t which, void** ptr, size_t* bytes);
 /* RayMarch.draw (src/ray.js:30-97) on the density field of the last orc_mesh. */
 int orc_ray(orc_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t body_count);
 int orc_ray_image(orc_sim* s, void** ptr, size_t* bytes);
+int orc_set_environment(orc_sim* s, const float* rgb, int32_t width, int32_t height);
+int orc_environment(orc_sim* s, const void** ptr, int32_t* size);
 /* The render passes' exp and log (Cody-Waite + Taylor; atanh series). */
 float orc_expf(float x);
 float orc_logf(float x);

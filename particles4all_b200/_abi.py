@@ -100,6 +100,7 @@ class SsfrParams(C.Structure):
         ("transmit", C.c_double * 3), ("roughness", C.c_double), ("sun_intensity", C.c_double),
         ("sun_elevation", C.c_double), ("sun_azimuth", C.c_double), ("exposure", C.c_double),
         ("ground_reflection", C.c_double), ("floor_plane", C.c_int32), ("debug", C.c_int32),
+        ("env_intensity", C.c_double), ("env_yaw", C.c_double),
     ]
 
 
@@ -120,6 +121,7 @@ class RayParams(C.Structure):
         ("skin_width", C.c_double), ("roughness", C.c_double), ("sun_intensity", C.c_double),
         ("sun_elevation", C.c_double), ("sun_azimuth", C.c_double), ("exposure", C.c_double),
         ("debug", C.c_int32), ("use_surface", C.c_int32), ("view", C.c_float * 16),
+        ("env_intensity", C.c_double), ("env_yaw", C.c_double),
     ]
 
 

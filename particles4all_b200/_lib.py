@@ -87,6 +87,8 @@ SIGNATURES = {
     "p4a_ray": ([_vp, _vp, _vp, _i32], C.c_int),
     "p4a_ray_buffer": ([_vp, C.POINTER(_vp), C.POINTER(_sz), C.POINTER(_i32), C.POINTER(_i32)], C.c_int),
     "p4a_ray_read": ([_vp, _vp, _sz], C.c_int),
+    "p4a_set_environment": ([_vp, _vp, _i32, _i32], C.c_int),
+    "p4a_environment_read": ([_vp, C.POINTER(_i32), _vp, _sz], C.c_int),
 }
 
 _lib = None

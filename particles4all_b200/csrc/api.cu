@@ -116,6 +116,8 @@ struct p4a_sim {
   int ssfrW = 0, ssfrH = 0, ssfrMapW = 0, ssfrMapH = 0, ssfrThW = 0, ssfrThH = 0, ssfrGen = 0;
   float4* ssfrBodies = nullptr;
   int ssfrBodyCap = 0;
+  ushort4* envCube = nullptr;  // p4a_set_environment: 6 faces of envSize^2 rgba16float texels
+  int envSize = 0;
   uchar4* rayImage = nullptr;  // p4a_ray
   char* raySurf = nullptr;     // p4a_ray's mesh surface maps, rayCap pixels
   size_t rayCap = 0;
@@ -683,6 +685,7 @@ int p4a_destroy(p4a_sim* s) {
   if (s->ssfrBodies) cudaFree(s->ssfrBodies);
   if (s->rayImage) cudaFree(s->rayImage);
   if (s->raySurf) cudaFree(s->raySurf);
+  if (s->envCube) cudaFree(s->envCube);
   if (s->pinned) cudaFreeHost(s->pinned);
   if (s->readEvent) cudaEventDestroy(s->readEvent);
   for (cudaEvent_t e : s->evPool) cudaEventDestroy(e);
@@ -1332,6 +1335,56 @@ int p4a_default_ssfr_params(p4a_ssfr_params* o) {
   o->ground_reflection = 0.0;
   o->floor_plane = 1;
   o->debug = 0;
+  o->env_intensity = 1.0;  // Environment constructor (src/env.js:151-153)
+  o->env_yaw = 0.0;
+  return P4A_OK;
+}
+
+// The environment uniforms of a render pass (src/ssfr.js:205-207, src/ray.js:66-68):
+// hasEnvMap, the intensity and the yaw as float32, the yaw's cosine and sine taken
+// once here instead of per pixel.
+static EnvMap env_uniform(const p4a_sim* s, double intensity, double yaw) {
+  EnvMap E{};
+  E.texels = s->envCube;
+  E.size = s->envCube ? s->envSize : 0;
+  E.intensity = (float)intensity;
+  const float y = (float)yaw;
+  E.yawCos = (float)std::cos((double)y);
+  E.yawSin = (float)std::sin((double)y);
+  return E;
+}
+
+int p4a_set_environment(p4a_sim* s, const float* rgb, int32_t width, int32_t height) {
+  if (!s) return P4A_ERR_ARG;
+  if (rgb && (width < 2 || height < 1 || width > 65536 || height > 32768))
+    return fail(s, P4A_ERR_ARG, "p4a_set_environment: bad panorama size %d x %d", width, height);
+  if (rgb && (width < 2 * height - 2 || width > 2 * height + 2))  // src/env.js:183-184
+    return fail(s, P4A_ERR_ARG, "p4a_set_environment: the panorama is %dx%d - an equirectangular panorama is 2:1",
+                width, height);
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));  // renders in flight may still read the old map
+  if (s->envCube) cudaFree(s->envCube);
+  s->envCube = nullptr;
+  s->envSize = 0;
+  if (!rgb) return P4A_OK;  // Environment.clear
+  const int size = env_face_size(width);
+  std::vector<uint16_t> host((size_t)6 * size * size * 4);
+  build_env_cube(rgb, width, height, size, host.data());
+  CUDA_TRY(s, cudaMalloc((void**)&s->envCube, host.size() * 2));
+  CUDA_TRY(s, cudaMemcpy(s->envCube, host.data(), host.size() * 2, cudaMemcpyHostToDevice));
+  s->envSize = size;
+  return P4A_OK;
+}
+
+int p4a_environment_read(p4a_sim* s, int32_t* faceSize, void* host, size_t bytes) {
+  if (!s) return P4A_ERR_ARG;
+  if (faceSize) *faceSize = s->envCube ? s->envSize : 0;
+  if (!host || !s->envCube) return P4A_OK;
+  const size_t have = (size_t)6 * s->envSize * s->envSize * 8;
+  if (bytes > have)
+    return fail(s, P4A_ERR_ARG, "p4a_environment_read: %zu bytes asked, the map holds %zu", bytes, have);
+  cudaSetDevice(s->device);
+  CUDA_TRY(s, cudaMemcpy(host, s->envCube, bytes, cudaMemcpyDeviceToHost));
   return P4A_OK;
 }
 
@@ -1490,6 +1543,7 @@ int p4a_ssfr(p4a_sim* s, const p4a_ssfr_params* sp, const float* bodies, int32_t
   C.mapH = mapH;
   C.thickW = tw;
   C.thickH = th;
+  C.env = env_uniform(s, q.env_intensity, q.env_yaw);
   mark(s, PH_SSFR);
   launch_ssfr(F, s->stream);
   mark(s, PH_END);
@@ -1585,6 +1639,8 @@ int p4a_default_ray_params(p4a_ray_params* o) {
   o->exposure = 1.0;
   o->debug = 0;
   o->use_surface = 1;  // raySurface (src/main.js)
+  o->env_intensity = 1.0;
+  o->env_yaw = 0.0;
   for (int k = 0; k < 4; k++) o->view[k * 5] = 1.0f;
   return P4A_OK;
 }
@@ -1624,6 +1680,7 @@ int p4a_ray(p4a_sim* s, const p4a_ray_params* rp, const float* bodies, int32_t b
                                   std::fma(q.proj[8 + rr], q.view[c * 4 + 2],
                                            std::fma(q.proj[4 + rr], q.view[c * 4 + 1], q.proj[rr] * q.view[c * 4])));
   R.useSurface = q.use_surface ? 1 : 0;
+  R.env = env_uniform(s, q.env_intensity, q.env_yaw);
   const double kPiD = 3.14159265358979323846;
   const double el = q.sun_elevation * kPiD / 180, az = q.sun_azimuth * kPiD / 180;
   const double sun[3] = {std::cos(el) * std::sin(az), std::sin(el), std::cos(el) * std::cos(az)};

@@ -102,13 +102,30 @@ struct SsfrFilter {  // src/ssfr_wgsl.js:186-199
   float sigmaWorld, proj11, viewH, delta, mu, rangeSigma;
   int clean, cleanRadius;
 };
-struct SsfrComp {  // src/ssfr_composite_wgsl.js:2-26 (no environment map)
+// An environment cube map on the device (src/env.js): six faces of size x size
+// rgba16float texels, face-major then row-major; size 0 = no map. The render passes
+// sample it at level 0 in the direction rotated by the yaw (cos, sin), times the
+// intensity.
+struct EnvMap {
+  const ushort4* texels;
+  int32_t size;
+  float intensity, yawCos, yawSin;
+};
+// Environment.load's host part (src/env.js:180-236): the face size for a panorama
+// `width` wide, and the panorama rgb[h][w][3] resampled into 6 * size * size
+// rgba16float texels (alpha 1).
+int env_face_size(int width);
+void build_env_cube(const float* rgb, int w, int h, int size, uint16_t* out);
+uint16_t env_half(float v);
+
+struct SsfrComp {  // src/ssfr_composite_wgsl.js:2-26
   float ivp[16], iv[16];
   float eye[3], boxMin[3], boxMax[3], absorb[3], sunDir[3];
   float proj00, proj11, ior, sunIntensity, roughness, exposure, groundReflection, thicknessScale;
   int32_t bodyCount, floorPlane, debug;
   float mapScaleX, mapScaleY;
   int32_t width, height, mapW, mapH, thickW, thickH;
+  EnvMap env;
 };
 struct SsfrFrame {
   SsfrSplat depth, thick;
@@ -145,6 +162,7 @@ struct RayParams {
   float cosDeg[4];
   int32_t useSurface;
   float view[16], vp[16];  // view, proj * view (mesh surface pass)
+  EnvMap env;
 };
 // The mesh surface pass (src/mesh.js:380-396, src/mesh_wgsl.js:240-321 vs + fsSurf):
 // the first min(*total, cap) triangles of verts into surfZ (eye-space z, -1e4 where

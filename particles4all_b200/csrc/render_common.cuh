@@ -3,8 +3,9 @@
 // rigid-body SDF trace, body shading, reflections, Fresnel, GGX and tone map that
 // src/ssfr_composite_wgsl.js and src/ray_wgsl.js both define (their preludes are
 // the same functions). Shading functions take the pass's uniform U, which has
-// sunDir[3], boxMin[3], floorPlane, groundReflection, bodyCount and exposure.
+// sunDir[3], boxMin[3], floorPlane, groundReflection, bodyCount, exposure and env.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "fmath.h"
@@ -138,8 +139,59 @@ __device__ __forceinline__ BodyTrace trace_bodies(const U& C, const float4* __re
   return o;
 }
 
+// rgba16float texel channel to float (exact).
+__device__ __forceinline__ float half_bits(unsigned short b) { return __half2float(__ushort_as_half(b)); }
+// The cube map at level 0 in direction d: face by the largest component (x, then
+// y, then z on ties), the face's (s, t) in [0, 1], bilinear within the face with
+// its edge texels clamped, as textureSampleLevel with a linear, clamp-to-edge
+// sampler defines it.
+__device__ __forceinline__ F3 cube_sample(const EnvMap& E, F3 d) {
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int face;
+  float ma, sc, tc;
+  if (ax >= ay && ax >= az) {
+    face = d.x >= 0.0f ? 0 : 1;
+    ma = ax;
+    sc = d.x >= 0.0f ? -d.z : d.z;
+    tc = -d.y;
+  } else if (ay >= az) {
+    face = d.y >= 0.0f ? 2 : 3;
+    ma = ay;
+    sc = d.x;
+    tc = d.y >= 0.0f ? d.z : -d.z;
+  } else {
+    face = d.z >= 0.0f ? 4 : 5;
+    ma = az;
+    sc = d.z >= 0.0f ? d.x : -d.x;
+    tc = -d.y;
+  }
+  const float n = (float)E.size;
+  // a NaN or zero direction lands on texel (0, 0) of its face
+  const float u = fminf(fmaxf(0.5f * (sc / ma + 1.0f) * n - 0.5f, -1.0f), n);
+  const float v = fminf(fmaxf(0.5f * (tc / ma + 1.0f) * n - 0.5f, -1.0f), n);
+  const float fu = floorf(u), fv = floorf(v);
+  const float tx = u - fu, ty = v - fv;
+  const int x0 = max((int)fu, 0), x1 = min((int)fu + 1, E.size - 1);
+  const int y0 = max((int)fv, 0), y1 = min((int)fv + 1, E.size - 1);
+  const ushort4* __restrict__ f = E.texels + (size_t)face * E.size * E.size;
+  const ushort4 a = __ldg(&f[y0 * E.size + x0]), b = __ldg(&f[y0 * E.size + x1]);
+  const ushort4 c = __ldg(&f[y1 * E.size + x0]), e = __ldg(&f[y1 * E.size + x1]);
+  const F3 top = lerp3({half_bits(a.x), half_bits(a.y), half_bits(a.z)}, {half_bits(b.x), half_bits(b.y), half_bits(b.z)},
+                       tx);
+  const F3 bot = lerp3({half_bits(c.x), half_bits(c.y), half_bits(c.z)}, {half_bits(e.x), half_bits(e.y), half_bits(e.z)},
+                       tx);
+  return lerp3(top, bot, ty);
+}
+// envSample (src/ray_wgsl.js:46-50, src/ssfr_composite_wgsl.js:38-42).
+__device__ __forceinline__ F3 env_sample(const EnvMap& E, F3 d) {
+  const F3 r = {E.yawCos * d.x + E.yawSin * d.z, d.y, -E.yawSin * d.x + E.yawCos * d.z};
+  const F3 c = cube_sample(E, r);
+  return {c.x * E.intensity, c.y * E.intensity, c.z * E.intensity};
+}
+
 template <class U>
 __device__ __forceinline__ F3 sky_color(const U& C, F3 d) {
+  if (C.env.size > 0) return env_sample(C.env, d);
   const float h = clampf(d.y, 0.0f, 1.0f);
   const F3 haze = {0.62f, 0.74f, 0.90f}, zenith = {0.09f, 0.28f, 0.72f}, mid = {0.25f, 0.48f, 0.85f};
   F3 c = lerp3(haze, mid, smooth(0.0f, 0.16f, h));
@@ -167,7 +219,8 @@ __device__ __forceinline__ F3 background(const U& C, F3 o, F3 d) {
     if (t > 0.0f) {
       const F3 p = {o.x + d.x * t, o.y + d.y * t, o.z + d.z * t};
       const float fade = 1.0f - fm_exp(-0.02f * t);
-      return lerp3(floor_color(p), {0.62f, 0.74f, 0.90f}, fade);
+      const F3 far = C.env.size > 0 ? env_sample(C.env, d) : F3{0.62f, 0.74f, 0.90f};
+      return lerp3(floor_color(p), far, fade);
     }
   }
   return sky_color(C, d);
@@ -184,6 +237,7 @@ __device__ __forceinline__ F3 shade_body(const U& C, F3 n, F3 base, F3 rd, F3 en
 }
 template <class U>
 __device__ __forceinline__ F3 env_reflect(const U& C, F3 d) {
+  if (C.env.size > 0) return env_sample(C.env, d);
   if (d.y >= 0.0f) return sky_color(C, d);
   const float k = clampf(-d.y * 4.0f, 0.0f, 1.0f);
   return lerp3({0.62f, 0.74f, 0.90f}, {0.32f, 0.325f, 0.335f}, k);

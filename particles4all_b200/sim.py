@@ -151,6 +151,29 @@ class Sim:
         w, h = (inf["thick_w"], inf["thick_h"]) if name == "thick" else (inf["map_w"], inf["map_h"])
         return out.view(np.float32).reshape(h, w)
 
+    def set_environment(self, rgb):
+        """Environment.load (src/env.js:180-236): `rgb` a float32 equirectangular
+        panorama [height, width, 3] (2:1), or None to clear (Environment.clear)."""
+        if rgb is None:
+            check(self._L.p4a_set_environment(self._h, None, 0, 0), self._h, "set_environment")
+            return
+        a = np.ascontiguousarray(rgb, np.float32)
+        if a.ndim != 3 or a.shape[2] != 3:
+            raise ValueError("the panorama is [height, width, 3]")
+        check(self._L.p4a_set_environment(self._h, a.ctypes.data, a.shape[1], a.shape[0]), self._h,
+              "set_environment")
+
+    def environment(self):
+        """The cube map as uint16 half-float bits [6, size, size, 4], or None."""
+        size = C.c_int32()
+        check(self._L.p4a_environment_read(self._h, C.byref(size), None, 0), self._h, "environment_read")
+        if size.value == 0:
+            return None
+        out = np.empty((6, size.value, size.value, 4), np.uint16)
+        check(self._L.p4a_environment_read(self._h, C.byref(size), out.ctypes.data, out.nbytes), self._h,
+              "environment_read")
+        return out
+
     def ray(self, rparams, bodies=None):
         """RayMarch.draw (src/ray.js:30-97) on the last mesh(): its triangles as the
         surface (use_surface 1, the default) or its density field marched
