@@ -82,8 +82,8 @@ def apply_ini(params, text):
     for k, (name, conv) in _INI_TO_PARAM.items():
         if k in kv:
             params[name] = conv(float(kv[k])) if conv is int else conv(kv[k])
-    if "soraverage" in kv:
-        params["sorAverage"] = kv["soraverage"] not in ("0", "false", "")
+    # soraverage is on the reference's unsupported list (src/settingsini.js:35-43):
+    # a preset's value is skipped, as there
     if "box" in kv:
         vals = [float(x) for x in kv["box"].replace(",", " ").split()]
         if len(vals) >= 3 and all(math.isfinite(v) for v in vals):
@@ -91,6 +91,82 @@ def apply_ini(params, text):
     if "body" in kv:
         params["bodies"] = [b for b in kv["body"].split(",") if b]
     return params
+
+
+# ini key -> (settings group, field, conversion) for the render settings that
+# src/main.js:320-400 reads from the URL keys src/settingsini.js:3-33 maps the ini
+# keys to; "ray" fields are also copied into the SSFR settings every frame
+# (src/main.js:955-963).
+_INI_TO_RENDER = {
+    "meshres": ("mesh", "resolution", int), "meshiso": ("mesh", "iso", float),
+    "fieldsmooth": ("mesh", "field_passes", int), "normalsmooth": ("mesh", "normal_passes", int),
+    "raysurface": ("ray", "use_surface", int),
+    "anisoratio": ("aniso", "ratio", float), "anisolambda": ("aniso", "lambda", float),
+    "anisonbrs": ("aniso", "min_neighbours", int), "anisolonely": ("aniso", "lonely", float),
+    "anisoradius": ("aniso", "radius_scale", float), "anisostretch": ("aniso", "stretch", float),
+    "anisoks": ("aniso", "ks", float),
+    "ior": ("ray", "ior", float), "absorption": ("ray", "absorption", float),
+    "thicksteps": ("ray", "thickness_steps", int), "groundreflection": ("ray", "ground_reflection", float),
+    "roughness": ("ray", "roughness", float), "sunintensity": ("ray", "sun_intensity", float),
+    "sunelev": ("ray", "sun_elevation", float), "sunazim": ("ray", "sun_azimuth", float),
+    "exposure": ("ray", "exposure", float),
+    "ssfrradius": ("ssfr", "splat_radius", float), "ssfrscale": ("ssfr", "render_scale", float),
+    "ssfrfilter": ("ssfr", "filter", int), "ssfriters": ("ssfr", "filter_iterations", int),
+    "ssfrsigma": ("ssfr", "filter_sigma", float), "ssfrdelta": ("ssfr", "narrow_delta", float),
+    "ssfrmu": ("ssfr", "narrow_mu", float), "ssfrthickr": ("ssfr", "thickness_radius", float),
+    "ssfrthick": ("ssfr", "thickness_scale", float), "ssfrthickblur": ("ssfr", "thickness_filter_size", int),
+    "ssfrrange": ("ssfr", "bilateral_range", float),
+}
+_RAY_TO_SSFR = ("ior", "absorption", "transmit", "roughness", "sun_intensity", "sun_elevation", "sun_azimuth",
+                "exposure", "ground_reflection")
+_VIEWS = {0: "particles", 1: "mesh", 2: "mesh", 3: "ray", 4: "ssfr"}
+
+
+def render_from_ini(text, params):
+    """The render settings of a preset .ini for a scene with `params` (its spacing
+    sets the SSFR depth cull): {"mesh", "aniso", "ssfr", "ray"} parameter dicts for
+    p4a_mesh / p4a_aniso / p4a_ssfr / p4a_ray from the library's defaults with the
+    preset's keys applied as the reference's viewer applies them, "env" (the
+    panorama file name the preset names, its intensity and its yaw in radians) and
+    "view". The ray pass's iso is the mesh's; floorplane sets both passes' floor;
+    ssfrdepthcull is a fraction of the neighbours within the anisotropic radius
+    (src/main.js:965-970)."""
+    kv = parse_ini(text)
+    out = {"mesh": default_mesh(), "aniso": default_aniso(), "ssfr": default_ssfr(), "ray": default_ray()}
+    for k, (group, name, conv) in _INI_TO_RENDER.items():
+        if k in kv:
+            try:
+                out[group][name] = conv(float(kv[k]))
+            except ValueError:
+                pass  # not a number: ignored here (the reference's Number() would give NaN)
+    if "transmit" in kv:
+        t = [float(x) for x in kv["transmit"].replace(",", " ").split()]
+        if len(t) >= 3 and all(math.isfinite(x) for x in t):
+            out["ray"]["transmit"] = t[:3]
+    out["ssfr"]["cleanup_pass"] = 0 if kv.get("ssfrcleanup") == "0" else 1  # on unless "0"
+    out["ray"]["iso"] = out["mesh"]["iso"]
+    for k in _RAY_TO_SSFR:
+        out["ssfr"][k] = out["ray"][k]
+    env = {"file": None, "intensity": 1.0, "yaw": 0.0}
+    if kv.get("cubemap"):
+        name = kv["cubemap"].strip('"').replace("\\", "/").split("/")[-1]
+        env["file"] = name or None
+    if "cubemapintensity" in kv:
+        env["intensity"] = float(kv["cubemapintensity"])
+    if "cubemapyaw" in kv:
+        env["yaw"] = float(kv["cubemapyaw"]) * math.pi / 180
+    for group in ("ssfr", "ray"):
+        out[group]["env_intensity"], out[group]["env_yaw"] = env["intensity"], env["yaw"]
+        if "floorplane" in kv:
+            out[group]["floor_plane"] = 0 if kv["floorplane"] == "0" else 1
+    out["env"] = env
+    frac = float(kv.get("ssfrdepthcull", 0.0))  # depthCullFraction, 0 by default
+    h = 2 * params.get("spacing", 0.02)
+    full = 4.18879 * (out["aniso"]["radius_scale"] * h / max(params.get("spacing", 0.02), 1e-6)) ** 3
+    out["ssfr"]["depth_cull_neighbours"] = math.floor(frac * full) if frac > 0 else 0
+    view = kv.get("display")
+    out["view"] = _VIEWS.get(int(view), None) if view is not None and view.strip().lstrip("-").isdigit() else None
+    return out
 
 
 def _spec(s):

@@ -147,3 +147,49 @@ def test_mass_calibration_brute_force(built):
     want = m0 * 1000 / rho.max() if rho.max() > 500 else m0
     assert math.isclose(sc["mass"], want, rel_tol=1e-12)
     assert sc["denom_rest"] > 0
+
+
+RENDER_INI = """
+display=4
+meshres=96
+meshiso=0.35
+fieldsmooth=2
+raysurface=0
+cubemap="D:\\\\panoramas\\\\sky_2k.hdr"
+cubemapintensity=1.5
+cubemapyaw=90
+floorplane=0
+anisoradius=2.5
+anisonbrs=20
+ior=1.5
+transmit=0.1 0.2 0.3
+sunelev=20
+ssfrradius=0.7
+ssfrfilter=1
+ssfrcleanup=0
+ssfrdepthcull=0.5
+soraverage=1
+"""
+
+
+def test_ini_render_settings():
+    """The render keys of a preset reach the pass parameters as the reference's
+    viewer applies them (src/settingsini.js:3-93, src/main.js:320-400, 955-970)."""
+    from particles4all_b200.params import render_from_ini
+    p = apply_ini(default_params("small"), RENDER_INI)
+    assert p["sorAverage"] is False  # soraverage is on the reference's unsupported list
+    r = render_from_ini(RENDER_INI, p)
+    assert r["view"] == "ssfr"
+    assert (r["mesh"]["resolution"], r["mesh"]["iso"], r["mesh"]["field_passes"]) == (96, 0.35, 2)
+    assert r["ray"]["use_surface"] == 0 and r["ray"]["iso"] == 0.35
+    assert r["env"] == {"file": "sky_2k.hdr", "intensity": 1.5, "yaw": math.pi / 2}
+    for g in ("ssfr", "ray"):
+        assert r[g]["floor_plane"] == 0 and r[g]["env_intensity"] == 1.5 and r[g]["env_yaw"] == math.pi / 2
+        assert r[g]["ior"] == 1.5 and r[g]["transmit"] == [0.1, 0.2, 0.3] and r[g]["sun_elevation"] == 20
+    assert (r["aniso"]["radius_scale"], r["aniso"]["min_neighbours"]) == (2.5, 20)
+    assert (r["ssfr"]["splat_radius"], r["ssfr"]["filter"], r["ssfr"]["cleanup_pass"]) == (0.7, 1, 0)
+    # 0.5 of the lattice neighbours within the anisotropic radius 2.5 h = 5 spacings
+    assert r["ssfr"]["depth_cull_neighbours"] == math.floor(0.5 * 4.18879 * 5.0 ** 3)
+    plain = render_from_ini("", p)
+    assert plain["ssfr"]["cleanup_pass"] == 1 and plain["ssfr"]["depth_cull_neighbours"] == 0
+    assert plain["env"]["file"] is None and plain["view"] is None
