@@ -224,6 +224,28 @@ def test_interactive_calls_bit_exact():
     compare(g, o)
 
 
+def test_viewer_hose_bit_exact():
+    """The reference's frame loop while pouring (src/main.js:986-997): the frame
+    split into substep slices, pourStep after each with the time advanced, on the
+    GPU and the oracle alike."""
+    from particles4all_b200.pour import Pour
+    p = small_params(targetParticleCount=1500, pour=True)
+    g, o = pair(p)
+    hoses = [Pour(budget=g.info()["pour_budget"], height=0.7), Pour(budget=o.info()["pour_budget"], height=0.7)]
+    for _ in range(6):
+        for s, hose in zip((g, o), hoses):
+            want = 1 / 60
+            for _guard in range(64):
+                if want <= 1e-6:
+                    break
+                sl = min(want, 1 / 60 / max(1, p["substeps"]))
+                s.step(sl)
+                hose.step(s, s.info()["last_advanced"], params=p)
+                want -= sl
+    assert hoses[0].left == hoses[1].left < g.info()["pour_budget"]
+    compare(g, o)
+
+
 def test_append_clamps_to_capacity():
     p = small_params(targetParticleCount=500, pour=True)
     g, o = pair(p)
