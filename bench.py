@@ -107,17 +107,40 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def committed_issue(kernel, wl):
-    """Issue-slot utilisation (smsp__issue_active, pct of peak) of the kernel's
-    committed ncu summary: the roof of an issue- and latency-bound pass."""
+def committed_value(kernel, wl, key):
+    """The `key:` figure of the kernel's committed ncu summary for this workload."""
     path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{wl}.txt")
     try:
         for line in open(path):
-            if line.startswith("issue_active_pct:"):
-                return float(line.split(":", 1)[1].split()[0]) / 100.0
+            if line.startswith(key + ":"):
+                return float(line.split(":", 1)[1].split()[0])
     except (OSError, ValueError):
         pass
     return None
+
+
+def committed_issue(kernel, wl):
+    """Issue-slot utilisation (smsp__issue_active, fraction of peak) of the kernel's
+    committed ncu summary: the roof of an issue- and latency-bound pass."""
+    v = committed_value(kernel, wl, "issue_active_pct")
+    return None if v is None else v / 100.0
+
+
+# FP32 work of a neighbour pass that counts only the pairs within h: ~33 neighbours
+# per particle at h = 2 d, ~25 flops each (distance, kernel value and gradient, sums).
+NEIGHBOUR_FLOP_PER_PARTICLE = 33 * 25
+NEIGHBOUR_KERNELS = ("lambda", "delta", "xsph_normals", "tension_finalize", "xsph_finalize")
+
+
+def fp32_peak_tflops():
+    """Nominal FP32 rate: 148 SMs x 128 FP32 lanes x 2 flops (FMA) x the max SM clock."""
+    mhz = 1965.0
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            mhz = float(json.load(f).get("sm_max_mhz", mhz))
+    except (OSError, ValueError):
+        pass
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
 
 
 def committed_traffic(kernel, wl):
@@ -564,10 +587,18 @@ def run_ours(args):
                 "frac": achieved / peak, "traffic": committed_traffic(name, args.workload),
                 "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
                 "issue_frac_ncu": committed_issue(name, args.workload),
+                "l2_hit_pct_ncu": committed_value(name, args.workload, "l2_hit_pct"),
                 "note": "the neighbour passes are bound by instruction issue and load latency, not HBM: "
                         "issue_frac_ncu is the kernel's issue-slot utilisation from its committed ncu summary",
                 "avg_launch_us": avg_s * 1e6,
                 "kernels": {k: kernel_line(k, v) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
+
+    if name in NEIGHBOUR_KERNELS:
+        tf = NEIGHBOUR_FLOP_PER_PARTICLE * prof_n_avg / avg_s / 1e12
+        roofline["fp32"] = {"achieved_tflops": tf, "peak_tflops": fp32_peak_tflops(),
+                            "frac": tf / fp32_peak_tflops(), "flop_per_particle": NEIGHBOUR_FLOP_PER_PARTICLE,
+                            "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x max SM clock",
+                            "what": "FP32 work of the pairs within h only; neither this nor HBM bounds the pass"}
 
     # whole-step HBM roofline with the fixed per-particle-substep formula of the
     # workload definition: sort (36 + 4 + 84), k x (lambda 24 + delta 36), finish 68,
