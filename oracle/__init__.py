@@ -1,8 +1,9 @@
 """CPU oracle of the Particles4All simulation step (ctypes wrapper of liboracle_p4a.so).
 
 TEST INFRASTRUCTURE: only tests/, __graft_entry__.smoke() and bench.py's CPU
-baseline use this module, as the checker or the timed CPU baseline. The product
-(particles4all_b200 / libp4a.so) never imports it.
+baseline use this module, as what the product's results are compared against or
+as the timed CPU baseline. The product (particles4all_b200 / libp4a.so) never
+imports it.
 
 PARITY UNPINNED: the reference (JS + WGSL in a browser) cannot run in this
 environment and ships no golden vectors; the restatement is pinned only by

@@ -1,6 +1,7 @@
 // p4a_oracle.cpp — CPU restatement of the Particles4All simulation step.
 //
-// TEST INFRASTRUCTURE (the checker and the timed CPU baseline), never the product.
+// TEST INFRASTRUCTURE (what the product's results are compared against, and the
+// timed CPU baseline), never the product.
 // PARITY UNPINNED: the reference cannot run here and ships no golden vectors; see
 // p4a_oracle.h for what pins this restatement instead.
 //

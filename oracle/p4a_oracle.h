@@ -2,8 +2,9 @@
  * p4a_oracle.h — CPU oracle for the Particles4All simulation step.
  *
  * TEST INFRASTRUCTURE, NOT PRODUCT CODE. Only the tests, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg load this library, and only as the checker /
- * the timed CPU baseline. The product path (libp4a.so) never calls it.
+ * and bench.py's CPU-baseline leg load this library, and only as what the
+ * product's results are compared against or as the timed CPU baseline. The
+ * product path (libp4a.so) never calls it.
  *
  * PARITY UNPINNED: the reference (a browser WebGPU demo, JS + WGSL) cannot be
  * executed in this environment (no JS runtime, no WebGPU/graphics stack) and
