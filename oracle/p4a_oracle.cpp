@@ -2168,8 +2168,8 @@ f3 o_cube_sample(const OEnv& E, f3 d) {
   const float v = std::fmin(std::fmax(0.5f * (tc / ma + 1.0f) * n - 0.5f, -1.0f), n);
   const float fu = std::floor(u), fv = std::floor(v);
   const float tx = u - fu, ty = v - fv;
-  const int x0 = std::max((int)fu, 0), x1 = std::min((int)fu + 1, E.size - 1);
-  const int y0 = std::max((int)fv, 0), y1 = std::min((int)fv + 1, E.size - 1);
+  const int x0 = std::min(std::max((int)fu, 0), E.size - 1), x1 = std::min(std::max((int)fu + 1, 0), E.size - 1);
+  const int y0 = std::min(std::max((int)fv, 0), E.size - 1), y1 = std::min(std::max((int)fv + 1, 0), E.size - 1);
   auto texel = [&](int y, int x) {
     const uint16_t* t = E.texels + ((((size_t)face * E.size + y) * E.size) + x) * 4;
     return f3{o_half_to_float(t[0]), o_half_to_float(t[1]), o_half_to_float(t[2])};
@@ -2858,8 +2858,10 @@ void o_surface(const orc_sim* s, const float* view, const float* vp, int W, int 
       if (!o_fan_tri(P, fan, W, H, T)) continue;
       const float lx = std::fmin(T.sx[0], std::fmin(T.sx[1], T.sx[2])), hx = std::fmax(T.sx[0], std::fmax(T.sx[1], T.sx[2]));
       const float ly = std::fmin(T.sy[0], std::fmin(T.sy[1], T.sy[2])), hy = std::fmax(T.sy[0], std::fmax(T.sy[1], T.sy[2]));
-      const int x0 = (int)std::fmax(std::ceil(lx - 0.5f), 0.0f), x1 = (int)std::fmin(std::floor(hx - 0.5f), (float)W - 1.0f);
-      const int y0 = (int)std::fmax(std::ceil(ly - 0.5f), 0.0f), y1 = (int)std::fmin(std::floor(hy - 0.5f), (float)H - 1.0f);
+      const int x0 = (int)std::fmin(std::fmax(std::ceil(lx - 0.5f), 0.0f), (float)W);
+      const int x1 = (int)std::fmax(std::fmin(std::floor(hx - 0.5f), (float)W - 1.0f), -1.0f);
+      const int y0 = (int)std::fmin(std::fmax(std::ceil(ly - 0.5f), 0.0f), (float)H);
+      const int y1 = (int)std::fmax(std::fmin(std::floor(hy - 0.5f), (float)H - 1.0f), -1.0f);
       for (int y = y0; y <= y1; y++)
         for (int x = x0; x <= x1; x++) {
           float b[3];

@@ -380,8 +380,11 @@ __global__ void k_surf_raster(const __grid_constant__ RayParams R, const __grid_
       if (!fan_tri(R, P, s, T)) continue;
       const float lo_x = fminf(T.sx[0], fminf(T.sx[1], T.sx[2])), hi_x = fmaxf(T.sx[0], fmaxf(T.sx[1], T.sx[2]));
       const float lo_y = fminf(T.sy[0], fminf(T.sy[1], T.sy[2])), hi_y = fmaxf(T.sy[0], fmaxf(T.sy[1], T.sy[2]));
-      const int x0 = (int)fmaxf(ceilf(lo_x - 0.5f), 0.0f), x1 = (int)fminf(floorf(hi_x - 0.5f), (float)R.width - 1.0f);
-      const int y0 = (int)fmaxf(ceilf(lo_y - 0.5f), 0.0f), y1 = (int)fminf(floorf(hi_y - 0.5f), (float)R.height - 1.0f);
+      // clamped before the conversion, so that infinite or NaN bounds stay in range
+      const int x0 = (int)fminf(fmaxf(ceilf(lo_x - 0.5f), 0.0f), (float)R.width);
+      const int x1 = (int)fmaxf(fminf(floorf(hi_x - 0.5f), (float)R.width - 1.0f), -1.0f);
+      const int y0 = (int)fminf(fmaxf(ceilf(lo_y - 0.5f), 0.0f), (float)R.height);
+      const int y1 = (int)fmaxf(fminf(floorf(hi_y - 0.5f), (float)R.height - 1.0f), -1.0f);
       const unsigned long long id = (unsigned long long)(t * 4u + (uint32_t)s);
       for (int py = y0; py <= y1; py++)
         for (int px = x0; px <= x1; px++) {

@@ -171,8 +171,8 @@ __device__ __forceinline__ F3 cube_sample(const EnvMap& E, F3 d) {
   const float v = fminf(fmaxf(0.5f * (tc / ma + 1.0f) * n - 0.5f, -1.0f), n);
   const float fu = floorf(u), fv = floorf(v);
   const float tx = u - fu, ty = v - fv;
-  const int x0 = max((int)fu, 0), x1 = min((int)fu + 1, E.size - 1);
-  const int y0 = max((int)fv, 0), y1 = min((int)fv + 1, E.size - 1);
+  const int x0 = min(max((int)fu, 0), E.size - 1), x1 = min(max((int)fu + 1, 0), E.size - 1);
+  const int y0 = min(max((int)fv, 0), E.size - 1), y1 = min(max((int)fv + 1, 0), E.size - 1);
   const ushort4* __restrict__ f = E.texels + (size_t)face * E.size * E.size;
   const ushort4 a = __ldg(&f[y0 * E.size + x0]), b = __ldg(&f[y0 * E.size + x1]);
   const ushort4 c = __ldg(&f[y1 * E.size + x0]), e = __ldg(&f[y1 * E.size + x1]);
