@@ -61,14 +61,30 @@ def test_cube_map_matches_oracle(scene):
     assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("floor,debug", [(0, 0), (1, 0), (0, 4)])
-def test_ssfr_with_environment(scene, floor, debug):
+def bodies():
+    """A sphere and a box in the renderers' packed layout: their shading reflects the
+    environment (envReflect)."""
+    b = np.zeros((2, 6, 4), np.float32)
+    b[0, 0] = [1.2, 0.9, 1.0, 1.0]
+    b[0, 1] = [0.6, 0.6, 0.6, 0.0]
+    b[0, 2:5, :3] = np.eye(3)
+    b[0, 5, :3] = [0.60, 0.88, 0.66]
+    b[1, 0] = [3.5, 0.7, 3.0, 0.0]
+    b[1, 1] = [0.5, 0.3, 0.4, 0.0]
+    b[1, 2:5, :3] = np.eye(3)
+    b[1, 5, :3] = [0.55, 0.72, 0.95]
+    return b
+
+
+@pytest.mark.parametrize("floor,debug,with_bodies", [(0, 0, False), (1, 0, True), (0, 4, False), (0, 0, True)])
+def test_ssfr_with_environment(scene, floor, debug, with_bodies):
     g, o = scene
     sp = default_ssfr()
     sp.update(matrices(80, 60))
     sp.update(env_intensity=1.4, env_yaw=0.9, floor_plane=floor, debug=debug)
-    g.ssfr(sp)
-    o.ssfr(sp)
+    b = bodies() if with_bodies else None
+    g.ssfr(sp, b)
+    o.ssfr(sp, b)
     a, b = g.ssfr_read("image"), o.ssfr_read("image")
     assert np.array_equal(a, b), np.argwhere(a != b)[:3].tolist()
 
@@ -80,12 +96,12 @@ def test_ray_with_environment(scene, surface):
     mp["resolution"] = 48
     g.mesh(mp)
     o.mesh(mp)
-    for floor, debug in ((0, 0), (1, 6)):
+    for floor, debug, packed in ((0, 0, None), (1, 6, None), (0, 0, bodies())):
         rp = default_ray()
         rp.update(matrices(64, 48))
         rp.update(env_intensity=0.8, env_yaw=-2.0, floor_plane=floor, debug=debug, use_surface=surface)
-        g.ray(rp)
-        a, b = g.ray_read(), o.ray(rp)
+        g.ray(rp, packed)
+        a, b = g.ray_read(), o.ray(rp, packed)
         assert np.array_equal(a, b), (floor, debug, np.argwhere(a != b)[:3].tolist())
 
 
