@@ -599,11 +599,29 @@ typedef struct p4a_grid {
   int32_t dim[3];
 } p4a_grid;
 size_t p4a_grid_sort_workspace_size(int32_t n, int32_t n_cells);
+/*   status              uint32 in DEVICE memory, or NULL. The scan's lookback
+ *                       waits on its predecessor tiles with a bounded spin; when
+ *                       one gives up, the outputs are invalid (every access still
+ *                       stays in bounds). With status != NULL the call returns once
+ *                       the work is queued and the error word is copied into
+ *                       *status on `stream` (0 = complete, nonzero = a wait gave
+ *                       up); with status == NULL the call waits for `stream` and
+ *                       returns P4A_ERR_TIMEOUT when a wait gave up.
+ * Returns P4A_ERR_ARG for a NULL grid, n < 0, a dim < 1 or h <= 0, and
+ * P4A_ERR_CAPACITY when dim[0]*dim[1]*dim[2] exceeds 2^31 - 1 or the workspace is
+ * too small; these checks run before any device work. */
 int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity,
                   const float* pos, const float* vel, const uint32_t* body, const float* rest,
                   float* pos_out, float* vel_out, float* pred_out, uint32_t* body_out,
                   float* rest_out, uint32_t* cell_start, uint32_t* slot_out, void* workspace,
-                  size_t workspace_bytes, void* stream);
+                  size_t workspace_bytes, uint32_t* status, void* stream);
+/* Test hook for the two grid-sort operators only (p4a_grid_sort and
+ * p4a_grid_sort_noalloc; the simulation's own steps are unaffected): the number
+ * of polls before the scan's lookback gives up (0 = the default, about 2^22
+ * polls, a quarter of a second), and, when skip_first_tile is 1, the scan's tile
+ * tickets start at 1, so tile 0 is never scanned and tile 1 waits on a flag that
+ * nothing sets until its limit runs out. Process-wide; restore with (0, 0). */
+int p4a_test_scan_wait(uint32_t spin_limit, int32_t skip_first_tile);
 
 /* ---- operator entry without allocation ---------------------------------- */
 /*
@@ -615,12 +633,18 @@ int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity,
  * output buffer; the scratch comes from one fixed device array inside the
  * library (about 8.4 MB, held by every GPU that loads the library until exit).
  *   - n <= P4A_NOALLOC_MAX_PARTICLES and dim[0]*dim[1]*dim[2] <=
- *     P4A_NOALLOC_MAX_CELLS, else P4A_ERR_CAPACITY with no device work.
+ *     P4A_NOALLOC_MAX_CELLS, else P4A_ERR_CAPACITY with no device work (each
+ *     dim is checked before it is multiplied in, so huge dims cannot wrap).
+ *   - `status` as for p4a_grid_sort: a device word that receives the scan's
+ *     error word on `stream`, or NULL to wait and get P4A_ERR_TIMEOUT.
  *   - Allocates nothing. The first call on a device looks up the array's
  *     address (once per device); make that first call before any stream capture.
- *   - The array is shared by all calls: the parts that must start at zero are
- *     cleared on `stream` at the start of each call, and calls whose work
- *     overlaps on the GPU race on it.
+ *     The address is kept until the process exits: a cudaDeviceReset after the
+ *     first call on that device is not supported.
+ *   - The array is shared by all calls: the parts that must start at zero (the
+ *     histogram and tile states the call's cell count uses, the ticket and the
+ *     error word) are cleared on `stream` at the start of each call, and calls
+ *     whose work overlaps on the GPU race on it.
  */
 #define P4A_NOALLOC_MAX_PARTICLES 524288
 #define P4A_NOALLOC_MAX_CELLS 524288
@@ -628,7 +652,7 @@ int p4a_grid_sort_noalloc(const p4a_grid* grid, int32_t n, float dt, float gravi
                           const float* pos, const float* vel, const uint32_t* body,
                           const float* rest, float* pos_out, float* vel_out, float* pred_out,
                           uint32_t* body_out, float* rest_out, uint32_t* cell_start,
-                          uint32_t* slot_out, void* stream);
+                          uint32_t* slot_out, uint32_t* status, void* stream);
 
 /* ---- host-side scene builder (src/scene.js:159-315) --------------------- */
 /* buildScene(params) into caller-provided host arrays; call once with NULL

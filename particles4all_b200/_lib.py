@@ -38,13 +38,14 @@ SIGNATURES = {
     "p4a_aniso": ([_vp, _vp], C.c_int),
     "p4a_default_aniso_params": ([_vp], C.c_int),
     "p4a_grid_sort_workspace_size": ([_i32, _i32], _sz),
-    "p4a_grid_sort": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp, _sz, _vp], C.c_int),
+    "p4a_grid_sort": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp, _sz, _vp, _vp], C.c_int),
+    "p4a_test_scan_wait": ([C.c_uint32, _i32], C.c_int),
     "p4a_build_scene": ([_vp] * 8, C.c_int),
     "p4a_profile_enable": ([_vp, _i32], C.c_int),
     "p4a_profile_reset": ([_vp], C.c_int),
     "p4a_profile_read": ([_vp, _vp, _i32, C.POINTER(_i32)], C.c_int),
     "p4a_kernel_launches": ([], C.c_uint64),
-    "p4a_grid_sort_noalloc": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp], C.c_int),
+    "p4a_grid_sort_noalloc": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp, _vp], C.c_int),
     "p4a_batch_create": ([C.c_int, _vp, C.POINTER(_vp)], C.c_int),
     "p4a_batch_footprint": ([_vp, C.POINTER(C.c_int64)], C.c_int),
     "p4a_batch_destroy": ([_vp], C.c_int),

@@ -1812,6 +1812,47 @@ uint64_t p4a_kernel_launches(void) { return g_launches.load(std::memory_order_re
 namespace p4a {
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+std::atomic<uint32_t> g_op_spin_limit{kScanSpinLimit};
+std::atomic<int32_t> g_op_skip_first_tile{0};
+
+int grid_sort_check(const p4a_grid* g, int32_t n, long long maxCells, long long* cells) {
+  if (!g || n < 0 || !(g->h > 0)) return P4A_ERR_ARG;
+  long long c = 1;
+  for (int k = 0; k < 3; k++) {
+    if (g->dim[k] < 1) return P4A_ERR_ARG;
+    // checked one factor at a time, so the product never overflows
+    if ((long long)g->dim[k] > maxCells / c) return P4A_ERR_CAPACITY;
+    c *= g->dim[k];
+  }
+  *cells = c;
+  return P4A_OK;
+}
+
+int grid_sort_launch(const p4a_grid& g, int32_t n, float dt, float gravity, const float* pos, const float* vel,
+                     const uint32_t* body, const float* rest, float* posOut, float* velOut, float* predOut,
+                     uint32_t* bodyOut, float* restOut, uint32_t* cellStart, uint32_t* slotOut, uint32_t* key,
+                     uint32_t* rank, uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
+                     uint32_t* ticket, uint32_t* err, uint32_t* status, cudaStream_t st) {
+  // test hook (p4a_test_scan_wait): start the tickets at 1, so tile 0 is never
+  // scanned and tile 1's lookback waits on a flag that nothing sets
+  if (g_op_skip_first_tile.load(std::memory_order_relaxed) &&
+      cudaMemsetAsync(ticket, 1, 1, st) != cudaSuccess)
+    return P4A_ERR_CUDA;
+  g_launches.fetch_add(4, std::memory_order_relaxed);
+  if (run_grid_sort(g, n, dt, gravity, pos, vel, body, rest, posOut, velOut, predOut, bodyOut, restOut, cellStart,
+                    slotOut, key, rank, unordered, cellCount, state, ticket, err, st,
+                    g_op_spin_limit.load(std::memory_order_relaxed)) != cudaSuccess)
+    return P4A_ERR_CUDA;
+  if (status) {  // the caller reads the error word when it reads the outputs
+    return cudaMemcpyAsync(status, err, 4, cudaMemcpyDeviceToDevice, st) == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+  }
+  uint32_t word = 0;
+  if (cudaMemcpyAsync(&word, err, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return P4A_ERR_CUDA;
+  return (word & ERR_SCAN_TIMEOUT) ? P4A_ERR_TIMEOUT : P4A_OK;
+}
+
 int resident_grid(const void* kernel, int block) {
   static std::mutex mu;
   static std::map<std::pair<int, const void*>, int> cache;
@@ -1843,15 +1884,22 @@ size_t p4a_grid_sort_workspace_size(int32_t n, int32_t nCells) {
          align256((size_t)scan_tiles(nCells) * 8) + align256(4) + align256(4);
 }
 
+int p4a_test_scan_wait(uint32_t spin_limit, int32_t skip_first_tile) {
+  if (skip_first_tile != 0 && skip_first_tile != 1) return P4A_ERR_ARG;
+  p4a::g_op_spin_limit.store(spin_limit ? spin_limit : p4a::kScanSpinLimit, std::memory_order_relaxed);
+  p4a::g_op_skip_first_tile.store(skip_first_tile, std::memory_order_relaxed);
+  return P4A_OK;
+}
+
 int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, const float* pos,
                   const float* vel, const uint32_t* body, const float* rest, float* pos_out,
                   float* vel_out, float* pred_out, uint32_t* body_out, float* rest_out,
                   uint32_t* cell_start, uint32_t* slot_out, void* workspace, size_t workspace_bytes,
-                  void* stream) {
-  if (!grid || n < 0 || grid->dim[0] < 1 || grid->dim[1] < 1 || grid->dim[2] < 1 || !(grid->h > 0))
-    return P4A_ERR_ARG;
-  const long long cellsLL = (long long)grid->dim[0] * grid->dim[1] * grid->dim[2];
-  if (cellsLL > 0x7fffffffLL) return P4A_ERR_CAPACITY;
+                  uint32_t* status, void* stream) {
+  using namespace p4a;
+  long long cellsLL = 0;
+  int rc = grid_sort_check(grid, n, 0x7fffffffLL, &cellsLL);
+  if (rc != P4A_OK) return rc;
   const int nCells = (int)cellsLL;
   if (n > 0 && (!pos || !vel || !pos_out || !vel_out || !pred_out)) return P4A_ERR_ARG;
   if ((body && !body_out) || (rest && !rest_out) || !cell_start) return P4A_ERR_ARG;
@@ -1868,11 +1916,9 @@ int p4a_grid_sort(const p4a_grid* grid, int32_t n, float dt, float gravity, cons
   uint32_t* errw = (uint32_t*)w;
   const size_t zeroBytes = (size_t)((char*)errw + 4 - (char*)cellCount);
   if (cudaMemsetAsync(cellCount, 0, zeroBytes, st) != cudaSuccess) return P4A_ERR_CUDA;
-  g_launches.fetch_add(4, std::memory_order_relaxed);
-  const cudaError_t e = run_grid_sort(*grid, n, dt, gravity, pos, vel, body, rest, pos_out, vel_out,
-                                      pred_out, body_out, rest_out, cell_start, slot_out, key, rank,
-                                      unordered, cellCount, state, ticket, errw, st);
-  return e == cudaSuccess ? P4A_OK : P4A_ERR_CUDA;
+  return grid_sort_launch(*grid, n, dt, gravity, pos, vel, body, rest, pos_out, vel_out, pred_out, body_out,
+                          rest_out, cell_start, slot_out, key, rank, unordered, cellCount, state, ticket, errw,
+                          status, st);
 }
 
 }  // extern "C"

@@ -131,7 +131,7 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
                                           uint32_t* __restrict__ cellStart, long long cellBase,
                                           long long limit, int tile, int firstTile, uint32_t seed,
                                           bool lastOfSegment, unsigned long long* __restrict__ state,
-                                          uint32_t epoch, uint32_t* __restrict__ err) {
+                                          uint32_t epoch, uint32_t* __restrict__ err, uint32_t spinLimit) {
   __shared__ uint32_t s_prefix;
   __shared__ uint32_t s_warp[kBlock / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -181,7 +181,7 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
           const uint32_t we = (uint32_t)(w64 >> 34);
           const unsigned long long wf = (w64 >> 32) & 3ull;
           if (we != epoch || wf == 0ull) {
-            if (++spins > (1u << 22)) {  // bounded wait: flag the error and stop looking
+            if (++spins > spinLimit) {  // bounded wait: flag the error and stop looking
               atomicOr(err, ERR_SCAN_TIMEOUT);
               break;
             }
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
                                                  uint32_t* __restrict__ cellStart, int nCells,
                                                  unsigned long long* __restrict__ state,
                                                  uint32_t* __restrict__ ticket, uint32_t epoch,
-                                                 int nTiles, uint32_t* __restrict__ err) {
+                                                 int nTiles, uint32_t* __restrict__ err, uint32_t spinLimit) {
   __shared__ uint32_t s_tile;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
     return;
   }
   scan_tile(cellCount, cellStart, (long long)tile * kScanTile, nCells, tile, 0, 0u,
-            tile == nTiles - 1, state, epoch, err);
+            tile == nTiles - 1, state, epoch, err, spinLimit);
   if (threadIdx.x == 0 && tile == nTiles - 1) *ticket = 0u;  // all tickets taken: reset
 }
 
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_b(const __grid_constant__ Batch
     const long long limit = (long long)P.cOff + P.nCells;
     const bool last = (long long)(lt + 1) * kScanTile >= (long long)P.nCells;
     scan_tile(d.cellCount, d.cellStart, (long long)P.cOff + (long long)lt * kScanTile, limit, (int)g,
-              (int)(g - lt), P.pOff, last, d.scanState, epoch, d.errorWord);
+              (int)(g - lt), P.pOff, last, d.scanState, epoch, d.errorWord, kScanSpinLimit);
   });
 }
 
@@ -244,9 +244,9 @@ void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_key_count<<<groups(work), kBlock, 0, st>>>(P, d);
 }
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells, unsigned long long* state,
-                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st) {
+                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st, uint32_t spinLimit) {
   const int tiles = scan_tiles(nCells);
-  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err);
+  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err, spinLimit);
 }
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_fill<<<groups(P.n), kBlock, 0, st>>>(P, d);
@@ -259,7 +259,7 @@ cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity,
                           float* velOut, float* predOut, uint32_t* bodyOut, float* restOut,
                           uint32_t* cellStart, uint32_t* slotOut, uint32_t* key, uint32_t* rank,
                           uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
-                          uint32_t* ticket, uint32_t* err, cudaStream_t st) {
+                          uint32_t* ticket, uint32_t* err, cudaStream_t st, uint32_t spinLimit) {
   SimParams P{};
   for (int k = 0; k < 3; k++) {
     P.boxMin[k] = g.box_min[k];
@@ -285,7 +285,7 @@ cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity,
   d.unordered = unordered;
   d.slotOut = slotOut;
   launch_key_count(P, d, st);
-  launch_scan(cellCount, cellStart, nCells, state, ticket, 1u, err, st);
+  launch_scan(cellCount, cellStart, nCells, state, ticket, 1u, err, st, spinLimit);
   launch_fill(P, d, st);
   launch_reorder(P, d, st);
   return cudaGetLastError();

@@ -20,6 +20,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../../include/p4a.h"
 
 namespace p4a {
@@ -241,6 +243,9 @@ struct BatchWork {
 constexpr int kBlock = 256;          // particles per block (the reference's workgroup)
 constexpr int kScanItems = 8;        // cells per scan thread
 constexpr int kScanTile = kBlock * kScanItems;
+// Polls of a predecessor tile's state before the scan's lookback gives up and sets
+// ERR_SCAN_TIMEOUT (each poll sleeps ~64 ns, so about a quarter of a second).
+constexpr uint32_t kScanSpinLimit = 1u << 22;
 
 inline int groups(long long n, int per = kBlock) {
   long long g = (n + per - 1) / per;
@@ -252,7 +257,7 @@ inline int scan_tiles(int nCells) { return groups(nCells, kScanTile); }
 void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells,
                  unsigned long long* state, uint32_t* ticket, uint32_t epoch, uint32_t* err,
-                 cudaStream_t st);
+                 cudaStream_t st, uint32_t spinLimit = kScanSpinLimit);
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_reorder(const SimParams& P, const DevScene& d, cudaStream_t st);
 // Kernels with tuned launch shapes (threads per block x minimum blocks per SM; the
@@ -310,7 +315,23 @@ cudaError_t run_grid_sort(const p4a_grid& g, int32_t n, float dt, float gravity,
                           float* velOut, float* predOut, uint32_t* bodyOut, float* restOut,
                           uint32_t* cellStart, uint32_t* slotOut, uint32_t* key, uint32_t* rank,
                           uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
-                          uint32_t* ticket, uint32_t* err, cudaStream_t st);
+                          uint32_t* ticket, uint32_t* err, cudaStream_t st,
+                          uint32_t spinLimit = kScanSpinLimit);
+
+// The operator entries' shared checks and tail (p4a_grid_sort, p4a_grid_sort_noalloc).
+// grid_sort_check: argument checks and the cell count, P4A_ERR_CAPACITY when it
+// exceeds maxCells (computed without overflow). grid_sort_launch: runs the sort on
+// zeroed scratch, then either queues a copy of the error word into `status`
+// (device memory) or, when status is NULL, waits for the stream and returns
+// P4A_ERR_TIMEOUT if the scan's bounded wait gave up.
+extern std::atomic<uint32_t> g_op_spin_limit;
+extern std::atomic<int32_t> g_op_skip_first_tile;
+int grid_sort_check(const p4a_grid* g, int32_t n, long long maxCells, long long* cells);
+int grid_sort_launch(const p4a_grid& g, int32_t n, float dt, float gravity, const float* pos, const float* vel,
+                     const uint32_t* body, const float* rest, float* posOut, float* velOut, float* predOut,
+                     uint32_t* bodyOut, float* restOut, uint32_t* cellStart, uint32_t* slotOut, uint32_t* key,
+                     uint32_t* rank, uint32_t* unordered, uint32_t* cellCount, unsigned long long* state,
+                     uint32_t* ticket, uint32_t* err, uint32_t* status, cudaStream_t st);
 
 // Adds to the process-wide count of kernels launched by the library.
 void count_launches(uint64_t n);

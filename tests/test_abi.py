@@ -109,10 +109,29 @@ def test_grid_sort_rejects_bad_arguments(built):
     assert L.p4a_grid_sort_workspace_size(100, 64) > 0
     assert L.p4a_grid_sort_workspace_size(-1, 64) == 0
     # missing workspace -> capacity error before any device work
-    rc = L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 9), C.c_void_p(16), None, None, 0, None)
+    rc = L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 9), C.c_void_p(16), None, None, 0, None, None)
     assert rc == _abi.P4A_ERR_CAPACITY
     g.dim[0] = 0
-    assert L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 11), None, 0, None) == _abi.P4A_ERR_ARG
+    assert L.p4a_grid_sort(C.byref(g), 0, 0.0, 0.0, *([None] * 11), None, 0, None, None) == _abi.P4A_ERR_ARG
+
+
+@pytest.mark.parametrize("dims", [(2**31 - 1, 2**31 - 1, 2**31 - 1), (2**20, 2**20, 2**20), (65536, 65536, 1),
+                                  (1, 2**16, 2**16), (2**31 - 1, 2, 1), (3, 2**30, 2**30)])
+def test_grid_sort_entries_reject_huge_dims_without_overflow(built, dims):
+    """A cell count beyond an entry's limit is rejected before any device work,
+    whatever the dims: the product is checked factor by factor, so it cannot wrap
+    to a small or negative count that would pass the check."""
+    L = _lib.lib()
+    g = _abi.Grid()
+    g.h = 1.0
+    for k in range(3):
+        g.dim[k] = dims[k]
+    assert dims[0] * dims[1] * dims[2] > 2**31 - 1  # beyond both entries' limits
+    dummy = [C.c_void_p(256)] * 11
+    rc = L.p4a_grid_sort_noalloc(C.byref(g), 16, 0.0, 0.0, *dummy, None, None)
+    assert rc == _abi.P4A_ERR_CAPACITY
+    rc = L.p4a_grid_sort(C.byref(g), 16, 0.0, 0.0, *dummy, C.c_void_p(256), 1 << 40, None, None)
+    assert rc == _abi.P4A_ERR_CAPACITY
 
 
 def test_tuning_table_host_side(built, tmp_path):

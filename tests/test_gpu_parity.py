@@ -100,7 +100,7 @@ def test_grid_sort_operator_matches_oracle():
         st = torch.cuda.current_stream().cuda_stream
         rc = L.p4a_grid_sort(C.byref(g), n, 1 / 240, 9.81, *[t.data_ptr() for t in t_in],
                              *[t.data_ptr() for t in t_out], cs.data_ptr(), slot.data_ptr(),
-                             ws.data_ptr(), wsz, st)
+                             ws.data_ptr(), wsz, None, st)
         assert rc == 0
         torch.cuda.synchronize()
         assert np.array_equal(cs.cpu().numpy().view(np.uint32), want["cell_start"])
