@@ -1,21 +1,27 @@
 #!/usr/bin/env python
 """bench.py — particle-substeps/s of the Particles4All simulation step on B200.
 
-One step = Sim.step(1/60) of the workload (2 substeps: grid sort, k PBF
-iterations, rigid shape matching, XSPH, surface tension, finalize, stats) plus
-the anisotropic-kernel pass the renderer runs per frame. Default workload: the
-medium scene with rigid bodies (medium_bodies_264k: 262,144 fluid particles +
-8 cubes of 216, tension, XSPH, anisotropic pass).
+Default workload (the headline): the seeded 96-scene mix (batched_mix_96: ~6.0 M
+particles, counts log-uniform in 4k-256k, boxes of 16-64 cells, 0-6 rigid cubes,
+surface tension on about half, 4 iterations, 2 substeps per 1/60 s frame) stepped
+as ONE batch (one launch per pass for all scenes, CUDA-graph frames), beside the
+plain per-scene loop (96 Sim handles stepped one after the other) on the same GPU.
+One step = one frame of every scene. The line also carries the large single scene
+with the hose (large_hose_2m) as `large_hose_2m`, the served Poisson workload, the
+render passes and the CPU baseline.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
   python bench.py --impl reference ...   # the reference's algorithm on the host cores
 
+--workload batched_mix_96 (default) | large_hose_2m | medium_bodies_264k | dam_break_32k.
+
 Multi-GPU: scenes are independent, so N GPUs run N replicas (weak scaling); no
-data-path collective. Device time is measured with CUDA events on the
-simulation's stream, max over ranks. Prints one JSON line on rank 0.
+data-path collective. Device time is measured with CUDA events on the stream the
+kernels run on, max over ranks. Prints one JSON line on rank 0.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -28,6 +34,7 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 METRIC = "particle-substeps/s"
+MIX = "batched_mix_96"
 L2_FLUSH_BYTES = 256 << 20
 # Algorithmic bytes per particle and launch (fixed formula of the workload
 # definition: neighbour re-reads are not counted).
@@ -47,21 +54,23 @@ ALGO_BYTES = {
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="medium_bodies_264k")
+    ap.add_argument("--workload", default=MIX)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-mix", action="store_true", help="skip the 96-scene batched vs plain comparison")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-scene loop of the mix")
+    ap.add_argument("--no-large", action="store_true", help="skip the large_hose_2m sub-line")
+    ap.add_argument("--large-steps", type=int, default=40)
     ap.add_argument("--no-render", action="store_true", help="skip the mesh / SSFR / ray-march timings")
-    ap.add_argument("--mix-frames", type=int, default=10)
     ap.add_argument("--only-render", action="store_true",
                     help="profiling aid: the workload scene, a few steps, then the render-pass timings alone")
     ap.add_argument("--only-mix", choices=["batched", "plain"], default=None,
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
                          "frames and exit; for profiling the two forms")
+    ap.add_argument("--mix-frames", type=int, default=10)
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="length of each served-workload run (batched, then plain); 0 skips it")
     ap.add_argument("--serve-budget-gb", type=float, default=160.0)
@@ -119,13 +128,6 @@ def committed_value(kernel, wl, key):
     return None
 
 
-def committed_issue(kernel, wl):
-    """Issue-slot utilisation (smsp__issue_active, fraction of peak) of the kernel's
-    committed ncu summary: the roof of an issue- and latency-bound pass."""
-    v = committed_value(kernel, wl, "issue_active_pct")
-    return None if v is None else v / 100.0
-
-
 # FP32 work of a neighbour pass that counts only the pairs within h: ~33 neighbours
 # per particle at h = 2 d, ~25 flops each (distance, kernel value and gradient, sums).
 NEIGHBOUR_FLOP_PER_PARTICLE = 33 * 25
@@ -141,18 +143,6 @@ def fp32_peak_tflops():
     except (OSError, ValueError):
         pass
     return 148 * 128 * 2 * mhz * 1e6 / 1e12
-
-
-def committed_traffic(kernel, wl):
-    """DRAM bytes per launch from the committed ncu summary of this kernel and workload."""
-    path = os.path.join(ROOT, "profiles", f"ncu_{kernel}_{wl}.txt")
-    try:
-        for line in open(path):
-            if line.startswith("dram_bytes_per_launch:"):
-                return int(float(line.split(":", 1)[1].split()[0]))
-    except OSError:
-        pass
-    return None
 
 
 class ClockSampler:
@@ -208,9 +198,74 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def _launches():
+    from particles4all_b200 import _lib
+    return _lib.lib().p4a_kernel_launches()
+
+
+def kernel_table(kern, particles_per_launch, peak):
+    """Per-kernel share, time per launch and HBM fraction (algorithmic bytes per
+    launch / average launch time). particles_per_launch(k) -> (particles, bytes per
+    particle) of one launch of kernel k."""
+    total_ms = sum(v[0] for v in kern.values()) or 1.0
+    out = {}
+    for k, (ms, nl) in sorted(kern.items(), key=lambda kv: -kv[1][0]):
+        row = {"ms_total": round(ms, 4), "launches": nl, "share": round(ms / total_ms, 4),
+               "us_per_launch": round(ms / max(1, nl) * 1000, 2)}
+        n, bpp = particles_per_launch(k)
+        if bpp and n:
+            gbs = bpp * n / (ms / max(1, nl) / 1000.0) / 1e9
+            row.update({"algorithmic_bytes_per_launch": int(bpp * n), "algorithmic_gbs": round(gbs, 1),
+                        "hbm_frac": round(gbs / peak, 4)})
+        out[k] = row
+    return out
+
+
+def roofline_of(kern, particles_per_launch, wl):
+    """Roofline of the dominant kernel of the timed region."""
+    peak, peak_kind = peaks()
+    name, (kms, kl) = max(kern.items(), key=lambda kv: kv[1][0])
+    n, bpp = particles_per_launch(name)
+    avg_s = kms / max(1, kl) / 1000.0
+    algo = bpp * n
+    achieved = algo / avg_s / 1e9
+    traffic = committed_value(name, wl, "dram_bytes_per_launch")
+    r = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": achieved / peak, "traffic": traffic,
+         "traffic_source": "committed ncu summary" if traffic is not None else None,
+         "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo, "avg_launch_us": avg_s * 1e6,
+         "timing": "CUDA events around every launch inside the timed steps (event-record nodes in the "
+                   "replayed graphs of a batched frame)",
+         "kernels": kernel_table(kern, particles_per_launch, peak)}
+    issue = committed_value(name, wl, "issue_active_pct")
+    l2 = committed_value(name, wl, "l2_hit_pct")
+    if issue is not None or l2 is not None:
+        r["ncu"] = {"issue_frac": None if issue is None else issue / 100.0, "l2_hit_pct": l2,
+                    "source": "committed ncu summary", "file": f"profiles/ncu_{name}_{wl}.txt"}
+    if name in NEIGHBOUR_KERNELS:
+        tf = NEIGHBOUR_FLOP_PER_PARTICLE * n / avg_s / 1e12
+        r["fp32"] = {"achieved_tflops": tf, "peak_tflops": fp32_peak_tflops(), "frac": tf / fp32_peak_tflops(),
+                     "flop_per_particle": NEIGHBOUR_FLOP_PER_PARTICLE,
+                     "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x max SM clock",
+                     "what": "FP32 work of the pairs within h only; neither this nor HBM bounds the pass"}
+        r["note"] = ("the neighbour passes are bound by instruction issue and the latency of the neighbour "
+                     "gathers, not HBM (their working set is mostly L2-resident)")
+    return r
+
+
+def bytes_per_particle_substep(iterations, bodies, tension):
+    """The workload definition's fixed algorithmic bytes per particle-substep:
+    sort 36 + 4 + 84, k x (lambda 24 + delta 36), finish 68, +64 with bodies,
+    +56 with tension."""
+    return 36 + 4 + 84 + iterations * (24 + 36) + 68 + (64 if bodies else 0) + (56 if tension else 0)
+
+
+# ---------------------------------------------------------------------------
+# the 96-scene mix
+
+
 def mix_arenas(mix):
     """Batch arena sizes that hold the whole mix."""
-    import math
     cap = sum((sc["pos"].shape[0] + 511) // 256 * 256 for _, sc in mix)
     cells = sum((int(math.prod(int(b) for b in p["box"])) // 2048 + 2) * 2048 for p, _ in mix)
     nbound = 0
@@ -221,6 +276,25 @@ def mix_arenas(mix):
     body_parts = sum(int((sc["phase"][:, 0] > 0).sum()) + 1 for _, sc in mix)
     return dict(max_particles=cap + 4096, max_cells=cells, max_scenes=len(mix) + 1, max_bodies=bodies + 8,
                 max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
+
+
+def mix_config(mix, world):
+    """The workload's `config`, the same dict in both arms."""
+    n = [sc["pos"].shape[0] for _, sc in mix]
+    return {"workload": MIX, "scenes": len(mix), "n_particles": int(sum(n)),
+            "particles_per_scene": [int(min(n)), int(max(n))],
+            "scenes_with_tension": sum(1 for p, _ in mix if p["surfaceTensionK"] > 0),
+            "scenes_with_bodies": sum(1 for _, sc in mix if sc["n_bodies"] > 0),
+            "rigid_bodies": int(sum(sc["n_bodies"] for _, sc in mix)),
+            "iterations": 4, "substeps_per_frame": 2, "seed": 12,
+            "step": "one 1/60 s frame of every scene",
+            "l2": "inputs larger than L2 (about 3.6 GB of state); L2 also flushed between timed steps",
+            "parallelism": f"replicas x{world}"}
+
+
+def mix_scene_flags(mix):
+    return [(sc["pos"].shape[0], sc["n_bodies"] > 0, p["surfaceTensionK"] > 0,
+             int((sc["phase"][:, 0] > 0).sum())) for p, sc in mix]
 
 
 def only_mix(form, frames):
@@ -256,83 +330,225 @@ def only_mix(form, frames):
     return 0
 
 
-def only_render(args):
-    """The workload scene stepped a few frames (anisotropic pass included), then the
-    render passes timed as in the full run."""
+def run_mix(args):
     import torch
-    from particles4all_b200 import Sim, default_aniso
-    params, scene, aniso = workload(args.workload)
-    stream = torch.cuda.Stream()
-    sim = Sim()
-    sim.set_stream(stream.cuda_stream)
-    sim.reset_scene(params, scene)
-    for _ in range(max(1, args.warmup)):
-        sim.step(1 / 60)
-    sim.aniso(aniso or default_aniso())
-    out = render_bench(sim, params, stream)
-    sim.close()
-    print(json.dumps({"only_render": out}), flush=True)
-    return 0
-
-
-def batched_mix_bench(frames, warmup):
-    """The 96-scene mix stepped (a) as one batch (one launch per pass for all
-    scenes, CUDA-graph frames) and (b) as the plain per-scene loop (96 Sim handles
-    on the same stream, one after the other). Device time per frame from CUDA
-    events; particle-substeps/s for both."""
-    import torch
-    from particles4all_b200 import Batch, Sim, configs
+    from particles4all_b200 import Batch, Sim, _lib, configs
+    from particles4all_b200.replicas import Replicas
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl")  # replicas only: no collective on the data path
     mix = configs.batched_mix()
-    total = sum(sc["pos"].shape[0] for _, sc in mix)
+    flags = mix_scene_flags(mix)
+    total = sum(f[0] for f in flags)
     stream = torch.cuda.Stream()
-    b = Batch(**mix_arenas(mix))
+    b = Batch(device=local, **mix_arenas(mix))
     b.set_stream(stream.cuda_stream)
     t0 = time.perf_counter()
     ids = [b.add_scene(p, sc) for p, sc in mix]
     admit_s = time.perf_counter() - t0
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    warm = max(3, args.warmup)
+
+    def sim_times():
+        return [b.info(s)["sim_time"] for s in ids]
+
+    def particle_substeps(t_before, t_after):
+        return sum(n * round((t1 - t0_) * 120.0) for (n, *_), t0_, t1 in zip(flags, t_before, t_after))
+
+    for _ in range(warm):
+        b.step(ids, 1 / 60)
+    b.synchronize()
+
+    # timed frames, with an event around every launch inside the replayed graphs
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    b.profile(True)
+    b.profile_reset()
+    clocks = ClockSampler(local)
+    clocks.start()
+    tb = sim_times()
+    launches0 = _launches()
+    rep.barrier()
+    torch.cuda.synchronize()
+    w0 = time.time()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush between timed frames (outside the events)
+            starts[k].record(stream)
+            b.step(ids, 1 / 60)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    rep.barrier()
+    w1 = time.time()
+    launches = _launches() - launches0
+    clocks.stop()
+    kern = b.profile_read()
+    b.profile(False)
+    done = particle_substeps(tb, sim_times())
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    dev_ms_max = rep.max(dev_ms)
+    value = world * done / (dev_ms_max / 1000.0)
+    subs_per_frame = done / max(1, total) / args.steps
+
+    n_plain = sum(f[0] for f in flags if not f[2])
+    n_tension = sum(f[0] for f in flags if f[2])
+    n_bodies_p = sum(f[0] for f in flags if f[1])
+
+    def per_launch(k):
+        if k in ("xsph_finalize",):
+            return n_plain, ALGO_BYTES[k]
+        if k in ("xsph_normals", "tension_finalize"):
+            return n_tension, ALGO_BYTES[k]
+        if k == "reorder":
+            return total, ALGO_BYTES[k] + 64 * n_bodies_p / max(1, total)
+        return total, ALGO_BYTES.get(k, 0)
+    roofline = roofline_of(kern, per_launch, MIX)
+
+    # whole frame against the workload definition's fixed bytes per particle-substep
+    frame_bytes = 0.0
+    for (n, bod, ten, nbp), (p, _) in zip(flags, mix):
+        cells = int(math.prod(math.ceil(x / (2 * p["spacing"])) for x in p["box"]))
+        frame_bytes += 2 * (n * bytes_per_particle_substep(4, bod, ten) + nbp * 88 * 4 + 8 * cells)
+    peak, peak_kind = peaks()
+    step_ach = frame_bytes * args.steps / (dev_ms / 1000.0) / 1e9
+    step_roofline = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_frame": frame_bytes,
+                     "what": "whole batched frame: the fixed algorithmic bytes of every scene over the "
+                             "device time of the timed frames"}
+
+    # end to end through the batch C ABI: host state in, frame, host state out
+    e2e = None
+    if not args.no_e2e:
+        e2e = mix_e2e(b, ids, flags, max(3, min(args.steps, 10)), rep, world)
+
+    plain = None
+    if world == 1 and not args.no_plain:
+        plain = mix_plain(mix, stream, flush, warm, args.steps)
+        plain["speedup"] = value / plain["value"]
+    b.close()
+
+    large = None
+    if world == 1 and not args.no_large:
+        large = single_scene("large_hose_2m", args.large_steps, warm, rep, world, local,
+                             e2e_on=not args.no_e2e, render=False)
+
+    served = None
+    if world == 1 and args.serve_seconds > 0:
+        try:
+            served = served_bench(args.serve_seconds, args.serve_budget_gb)
+        except Exception as e:  # the headline line is still printed
+            served = {"error": f"{type(e).__name__}: {e}"}
+
+    render = None
+    if world == 1 and not args.no_render:
+        render = medium_render(warm)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_mix(mix, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": warm, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": mix_config(mix, world),
+            "form": "batched: one launch per pass for all 96 scenes, persistent work-item kernels, "
+                    "CUDA-graph frames",
+            "substeps_per_step": subs_per_frame,
+            "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": launches, "admit_s": admit_s,
+            "plain": plain, "large_hose_2m": large, "served": served, "render": render,
+            "clocks": clocks.summary(w0, w1),
+        }
+        print(json.dumps(line), flush=True)
+    rep.close()
+    return 0
+
+
+def mix_e2e(b, ids, flags, frames, rep, world):
+    """Per frame through the public batch API: every scene's pos and vel written
+    from pinned host memory, the batched frame, pos and vel read back to pinned
+    host memory, all waited for. The state read back is the next frame's input."""
+    import torch
+    caps = [f[0] for f in flags]
+    total = sum(caps)
+    bufs = [torch.empty(total * 8, dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    offs = []
+    o = 0
+    for n in caps:
+        offs.append(o)
+        o += n * 8
+    src = bufs[0]
+    for s, n, off in zip(ids, caps, offs):
+        base = src.data_ptr() + off * 4
+        b.read_async(s, "pos", base, n * 16)
+        b.read_async(s, "vel", base + n * 16, n * 16)
+    b.synchronize()
+    rep.barrier()
+    t_before = [b.info(s)["sim_time"] for s in ids]
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for k in range(frames):
+        hin, hout = bufs[k & 1], bufs[(k + 1) & 1]
+        for s, n, off in zip(ids, caps, offs):
+            base = hin.data_ptr() + off * 4
+            b.write_async(s, "pos", base, n * 16)
+            b.write_async(s, "vel", base + n * 16, n * 16)
+            h2d += 32 * n
+        b.step(ids, 1 / 60)
+        for s, n, off in zip(ids, caps, offs):
+            base = hout.data_ptr() + off * 4
+            b.read_async(s, "pos", base, n * 16)
+            b.read_async(s, "vel", base + n * 16, n * 16)
+            d2h += 32 * n
+        b.synchronize()
+    t1 = time.perf_counter()
+    rep.barrier()
+    el = rep.max(t1 - t0)
+    done = sum(n * round((b.info(s)["sim_time"] - tb) * 120.0) for s, n, tb in zip(ids, caps, t_before))
+    return {"value": world * done / el, "unit": METRIC, "h2d_bytes_per_step": h2d // frames,
+            "d2h_bytes_per_step": d2h // frames, "steps": frames,
+            "what": "per frame through p4a_batch_write_async / p4a_batch_step / p4a_batch_read_async: every "
+                    "scene's pos+vel from pinned host memory, one batched frame, every scene's pos+vel back "
+                    "to pinned host memory, p4a_batch_synchronize; wall clock, max over ranks"}
+
+
+def mix_plain(mix, stream, flush, warm, steps):
+    """The same 96 scenes as 96 plain Sim handles stepped one after the other on one
+    stream: device time per frame from CUDA events."""
+    import torch
+    from particles4all_b200 import Sim
     sims = []
     for p, sc in mix:
         sim = Sim()
         sim.set_stream(stream.cuda_stream)
         sim.reset_scene(p, sc)
         sims.append(sim)
-
-    def timed(fn, k):
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k)]
-        subs = 0
-        for e0, e1 in ev:
-            e0.record(stream)
-            subs += fn()
-            e1.record(stream)
-        torch.cuda.synchronize()
-        return sum(e0.elapsed_time(e1) for e0, e1 in ev), subs
-
-    def batched():
-        b.step(ids, 1 / 60)
-        return 2
-
-    def plain():
+    for _ in range(warm):
         for sim in sims:
             sim.step(1 / 60)
-        return 2
-    timed(batched, warmup)
-    timed(plain, warmup)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    done = 0
     launches0 = _launches()
-    tb, sb = timed(batched, frames)
-    lb = _launches() - launches0
-    launches0 = _launches()
-    tp, sp = timed(plain, frames)
-    lp = _launches() - launches0
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            for sim in sims:
+                done += sim.info()["n"] * sim.step(1 / 60)
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    launches = _launches() - launches0
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     for sim in sims:
         sim.close()
-    b.close()
-    vb = total * sb / (tb / 1000.0)
-    vp = total * sp / (tp / 1000.0)
-    return {"scenes": len(mix), "particles": total, "frames": frames, "substeps_per_frame": 2,
-            "batched_value": vb, "plain_value": vp, "speedup": vb / vp, "unit": METRIC,
-            "batched_ms_per_frame": tb / frames, "plain_ms_per_frame": tp / frames,
-            "batched_launches_per_frame": lb / frames, "plain_launches_per_frame": lp / frames,
-            "admit_s_total": admit_s}
+    return {"value": done / (ms / 1000.0), "unit": METRIC, "ms_per_step": ms / steps, "steps": steps,
+            "launches_per_step": launches / steps,
+            "what": "the same 96 scenes as 96 Sim handles, p4a_step one after the other on one stream; "
+                    "CUDA events per frame, L2 flushed between frames"}
 
 
 def served_bench(seconds, budget_gb):
@@ -400,13 +616,225 @@ def render_bench(sim, params, stream, width=1920, height=1080, reps=5):
     return out
 
 
-def _launches():
-    from particles4all_b200 import _lib
-    return _lib.lib().p4a_kernel_launches()
+def medium_render(warm):
+    """The render passes on the medium scene after a few frames."""
+    import torch
+    from particles4all_b200 import Sim
+    params, scene, aniso = workload("medium_bodies_264k")
+    stream = torch.cuda.Stream()
+    sim = Sim()
+    sim.set_stream(stream.cuda_stream)
+    sim.reset_scene(params, scene)
+    for _ in range(warm):
+        sim.step(1 / 60)
+    sim.aniso(aniso)
+    out = render_bench(sim, params, stream)
+    out["workload"] = "medium_bodies_264k"
+    sim.close()
+    return out
 
 
-def cpu_baseline(params, scene, aniso, seconds):
-    """The oracle (a CPU restatement of the reference's passes) on this workload."""
+def only_render(args):
+    """The workload scene stepped a few frames (anisotropic pass included), then the
+    render passes timed as in the full run."""
+    import torch
+    from particles4all_b200 import Sim, default_aniso
+    name = "medium_bodies_264k" if args.workload == MIX else args.workload
+    params, scene, aniso = workload(name)
+    stream = torch.cuda.Stream()
+    sim = Sim()
+    sim.set_stream(stream.cuda_stream)
+    sim.reset_scene(params, scene)
+    for _ in range(max(1, args.warmup)):
+        sim.step(1 / 60)
+    sim.aniso(aniso or default_aniso())
+    out = render_bench(sim, params, stream)
+    sim.close()
+    print(json.dumps({"only_render": out}), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# one scene
+
+
+def single_scene(name, steps, warm, rep, world, local, e2e_on=True, render=False):
+    """One scene stepped `steps` frames (hose and anisotropic pass as the workload
+    has them), timed with CUDA events on the simulation's stream; per-kernel events
+    inside the timed frames; e2e through the plain C ABI with host buffers."""
+    import torch
+    from particles4all_b200 import Sim, _lib
+    params, scene, aniso = workload(name)
+    stream = torch.cuda.Stream()
+    sim = Sim(device=local)
+    sim.set_stream(stream.cuda_stream)
+    sim.reset_scene(params, scene)
+    n0 = sim.info()["n"]
+    hose = hose_for(params, scene)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    done = [0.0]
+    appended = [0]
+
+    def frame(between=None):
+        appended[0] += pour(sim, hose)
+        s = sim.step(1 / 60)
+        if between is not None:
+            between()
+        if aniso:
+            sim.aniso(aniso)
+        done[0] += sim.info()["n"] * s
+        return s
+
+    for _ in range(warm):
+        frame()
+    sim.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    sim.profile(True)
+    sim.profile_reset()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = _launches()
+    rep.barrier()
+    torch.cuda.synchronize()
+    w0 = time.time()
+    done[0] = 0.0
+    subs = 0
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            subs += frame()
+            ends[k].record(stream)
+    torch.cuda.synchronize()
+    rep.barrier()
+    w1 = time.time()
+    launches = _launches() - launches0
+    clocks.stop()
+    kern = sim.profile_read()
+    sim.profile(False)
+    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    done_timed = done[0]
+    dev_ms_max = rep.max(dev_ms)
+    value = world * done_timed / (dev_ms_max / 1000.0)
+    n_avg = done_timed / max(1, subs)
+    info = sim.info()
+
+    def per_launch(k):
+        if k == "aniso":
+            return n_avg, ALGO_BYTES[k]
+        return n_avg, ALGO_BYTES.get(k, 0) + (64 if k == "reorder" and info["n_bodies"] else 0)
+    roofline = roofline_of(kern, per_launch, name)
+
+    k_it = max(1, int(params["iterations"]))
+    bpp = bytes_per_particle_substep(k_it, info["n_bodies"] > 0, params.get("surfaceTensionK", 0) > 0)
+    step_bytes = done_timed * bpp + subs * (info["n_body_parts"] * 88 * k_it + 8 * info["n_cells"])
+    if aniso:
+        step_bytes += steps * n_avg * 64
+    peak, peak_kind = peaks()
+    step_ach = step_bytes / (dev_ms / 1000.0) / 1e9
+    step_roofline = {"bound": "hbm", "achieved": step_ach, "peak": peak, "unit": "GB/s", "frac": step_ach / peak,
+                     "peak_source": peak_kind, "bytes_per_particle_substep": bpp,
+                     "what": "whole step: fixed algorithmic bytes of the workload definition over the "
+                             "device time of the timed steps"}
+
+    e2e = None
+    if e2e_on:
+        L = _lib.lib()
+        check = _lib.check
+        h = sim._h
+        cap = max(1, info["cap"])
+        hp = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
+        hv = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
+        hs = torch.empty(8, dtype=torch.int32, pin_memory=True)
+        nb0 = info["n"] * 16
+        L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nb0)
+        L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nb0)
+        e_steps = max(3, min(steps, 20))
+        rep.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        done[0] = 0.0
+        appended[0] = 0
+        h2d = d2h = 0
+        nb2 = [0]
+
+        def read_state():
+            # the step's pos / vel leave on the copy stream while the anisotropic
+            # pass (which changes neither) runs
+            nb2[0] = sim.info()["n"] * 16
+            check(L.p4a_read_async(h, 0, -1, hp.data_ptr(), 0, nb2[0]), h, "read_async")
+            check(L.p4a_read_async(h, 1, -1, hv.data_ptr(), 0, nb2[0]), h, "read_async")
+        for _ in range(e_steps):
+            nb = sim.info()["n"] * 16
+            check(L.p4a_write(h, 0, -1, hp.data_ptr(), 0, nb), h, "write")
+            check(L.p4a_write(h, 1, -1, hv.data_ptr(), 0, nb), h, "write")
+            frame(read_state)
+            check(L.p4a_read(h, 17, -1, hs.data_ptr(), 0, 32), h, "read")
+            check(L.p4a_read_wait(h), h, "read_wait")
+            h2d += 2 * nb
+            d2h += 2 * nb2[0] + 32
+        t1 = time.perf_counter()
+        rep.barrier()
+        el = rep.max(t1 - t0)
+        h2d += appended[0] * 24  # the hose's layers (float3 pos + vel) go up through p4a_append_fluid
+        e2e = {"value": world * done[0] / el, "unit": METRIC, "h2d_bytes_per_step": h2d // e_steps,
+               "d2h_bytes_per_step": d2h // e_steps, "steps": e_steps,
+               "what": "per step: live pos+vel written from pinned host, Sim.step (+ hose, + aniso as the "
+                       "workload has them), pos+vel read back to pinned host on the copy stream (overlapping "
+                       "the anisotropic pass) and stats read back, all waited for"}
+
+    rend = render_bench(sim, params, stream) if render else None
+    st = sim.get_stats()
+    out = {"metric": METRIC, "value": value, "unit": METRIC, "steps": steps, "warmup": warm,
+           "ms_per_step": dev_ms_max / steps,
+           "config": {"workload": name, "n_particles": n0, "n_particles_end": info["n"],
+                      "hose": "2,048 particles per step at 3 m/s" if hose else None,
+                      "n_bodies": info["n_bodies"], "substeps_per_step": subs // max(1, steps),
+                      "iterations": params["iterations"], "surface_tension": params["surfaceTensionK"],
+                      "aniso_pass": bool(aniso),
+                      "l2": "flushed between timed steps (256 MiB write outside the timed events)",
+                      "parallelism": f"replicas x{world}"},
+           "roofline": roofline, "step_roofline": step_roofline, "e2e": e2e, "gpu_launches": launches,
+           "render": rend, "clocks": clocks.summary(w0, w1),
+           "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")}}
+    sim.close()
+    return out
+
+
+def run_single_line(args):
+    import torch
+    from particles4all_b200.replicas import Replicas
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    rep = Replicas("nccl")
+    warm = max(3, args.warmup)
+    out = single_scene(args.workload, args.steps, warm, rep, world, local, e2e_on=not args.no_e2e,
+                       render=(world == 1 and not args.no_render and args.workload.startswith("medium")))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        params, scene, aniso = workload(args.workload)
+        cpu = cpu_baseline_single(params, scene, aniso, args.cpu_seconds)
+    if rank == 0:
+        cfg = out.pop("config")
+        line = {"metric": METRIC, "value": out.pop("value"), "unit": METRIC, "n_gpus": world,
+                "steps": args.steps, "warmup": warm, "ms_per_step": out.pop("ms_per_step"),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "config": cfg, "cpu_baseline": cpu}
+        for k in ("steps", "warmup", "metric", "unit"):
+            out.pop(k, None)
+        line.update(out)
+        print(json.dumps(line), flush=True)
+    rep.close()
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the oracle on the host cores (CPU baseline and the reference arm)
+
+
+def cpu_baseline_single(params, scene, aniso, seconds):
+    """The oracle (a CPU restatement of the reference's passes) on one scene."""
     import oracle
     o = oracle.OracleSim()
     o.reset_scene(params, scene)
@@ -432,281 +860,103 @@ def cpu_baseline(params, scene, aniso, seconds):
                       f"{' + hose' if hose else ''}) of the same scene ({n} particles at the end) in {el:.1f} s"}
 
 
+def oracle_mix(mix):
+    import oracle
+    sims = []
+    for p, sc in mix:
+        o = oracle.OracleSim()
+        o.reset_scene(p, sc)
+        sims.append(o)
+    return sims
+
+
+def oracle_round(sims):
+    """One substep (1/120 s) of every scene of the mix; returns particle-substeps."""
+    ps = 0
+    for o in sims:
+        ps += o.info()["n"] * o.step(1 / 120)
+    return ps
+
+
+def cpu_baseline_mix(mix, seconds):
+    """The oracle on the same 96 scenes: rounds of one substep of every scene."""
+    import oracle
+    sims = oracle_mix(mix)
+    ps = 0
+    rounds = 0
+    t0 = time.perf_counter()
+    while True:
+        ps += oracle_round(sims)
+        rounds += 1
+        if time.perf_counter() - t0 >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return {"value": ps / el, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
+            "sample": f"{rounds} rounds of one substep of each of the 96 scenes ({ps} particle-substeps) "
+                      f"in {el:.1f} s, all host threads"}
+
+
 def run_reference(args):
-    rank, _, _ = dist_env()
+    rank, _, world = dist_env()
     if rank != 0:
         return 0
     import oracle
-    params, scene, aniso = workload(args.workload)
-    o = oracle.OracleSim()
-    o.reset_scene(params, scene)
-    hose = hose_for(params, scene)
-    n = o.info()["n"]
-    base = max(1, params["substeps"])
-    # a step is the full frame, or one substep of it when K frames would not fit
-    t0 = time.perf_counter()
-    o.step(1 / 60)
-    if aniso:
-        o.aniso(aniso)
-    frame_s = time.perf_counter() - t0
-    frame = frame_s * (args.steps + args.warmup) <= 150.0
-    dt = 1 / 60 if frame else (1 / 60) / base
-
-    def one():
-        if frame:
-            pour(o, hose)
-        s = o.step(dt)
-        if aniso and frame:
+    if args.workload == MIX:
+        from particles4all_b200 import configs
+        mix = configs.batched_mix()
+        sims = oracle_mix(mix)
+        for _ in range(max(0, args.warmup)):
+            oracle_round(sims)
+        ps = 0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ps += oracle_round(sims)
+        el = time.perf_counter() - t0
+        value = ps / el
+        sample = (f"each step one substep of every one of the 96 scenes (the mix's {ps // max(1, args.steps)} "
+                  f"particle-substeps), {args.steps} steps timed, all host threads")
+        config = mix_config(mix, world)
+    else:
+        params, scene, aniso = workload(args.workload)
+        o = oracle.OracleSim()
+        o.reset_scene(params, scene)
+        hose = hose_for(params, scene)
+        base = max(1, params["substeps"])
+        # a step is the full frame, or one substep of it when K frames would not fit
+        t0 = time.perf_counter()
+        o.step(1 / 60)
+        if aniso:
             o.aniso(aniso)
-        return s, o.info()["n"] * s
-    for _ in range(max(0, args.warmup - 1)):
-        one()
-    subs = 0
-    ps = 0.0
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        s, p = one()
-        subs += s
-        ps += p
-    el = time.perf_counter() - t0
-    value = ps / el
-    n = o.info()["n"]
-    sample = (f"{'full frames' if frame else 'single substeps'} of the {n}-particle scene, "
-              f"{subs} substeps timed, all host threads")
+        frame_s = time.perf_counter() - t0
+        frame = frame_s * (args.steps + args.warmup) <= 150.0
+        dt = 1 / 60 if frame else (1 / 60) / base
+
+        def one():
+            if frame:
+                pour(o, hose)
+            s = o.step(dt)
+            if aniso and frame:
+                o.aniso(aniso)
+            return o.info()["n"] * s
+        for _ in range(max(0, args.warmup - 1)):
+            one()
+        ps = 0.0
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ps += one()
+        el = time.perf_counter() - t0
+        value = ps / el
+        n = o.info()["n"]
+        sample = f"{'full frames' if frame else 'single substeps'} of the {n}-particle scene, all host threads"
+        config = {"workload": args.workload, "n_particles": n}
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": el * 1000 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": args.workload, "n_particles": n, "substeps_per_step": subs // max(1, args.steps)},
+            "impl": "reference", "config": config,
             "cpu_baseline": {"value": value, "unit": METRIC, "cores": oracle.threads(), "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-    return 0
-
-
-def run_ours(args):
-    import numpy as np
-    import torch
-    from particles4all_b200 import Sim, _lib
-
-    from particles4all_b200.replicas import Replicas
-    rank, local, world = dist_env()
-    torch.cuda.set_device(local)
-    rep = Replicas("nccl")  # replicas only: no collective on the data path
-    barrier, allmax = rep.barrier, rep.max
-
-    params, scene, aniso = workload(args.workload)
-    stream = torch.cuda.Stream()
-    sim = Sim(device=local)
-    sim.set_stream(stream.cuda_stream)
-    sim.reset_scene(params, scene)
-    n = sim.info()["n"]
-    hose = hose_for(params, scene)
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    done = [0.0]  # particle-substeps
-
-    def frame(between=None):
-        pour(sim, hose)
-        s = sim.step(1 / 60)
-        if between is not None:
-            between()
-        if aniso:
-            sim.aniso(aniso)
-        done[0] += sim.info()["n"] * s
-        return s
-
-    for _ in range(max(3, args.warmup)):
-        frame()
-    sim.synchronize()
-    # per-kernel breakdown: a pass with a CUDA event around every launch, before the
-    # timed pass (whose steps run without the extra event records)
-    prof_steps = max(3, min(args.steps, 30))
-    sim.profile(True)
-    sim.profile_reset()
-    done[0] = 0.0
-    prof_subs = 0
-    with torch.cuda.stream(stream):
-        for _ in range(prof_steps):
-            flush.zero_()
-            prof_subs += frame()
-    sim.synchronize()
-    kern = sim.profile_read()
-    sim.profile(False)
-    prof_n_avg = done[0] / max(1, prof_subs)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    clocks = ClockSampler(local)
-    clocks.start()
-    launches0 = _lib.lib().p4a_kernel_launches()
-    barrier()
-    torch.cuda.synchronize()
-    w0 = time.time()
-    done[0] = 0.0
-    subs = 0
-    with torch.cuda.stream(stream):
-        for k in range(args.steps):
-            flush.zero_()  # L2 flush between timed steps (not inside the events)
-            starts[k].record(stream)
-            subs += frame()
-            ends[k].record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    w1 = time.time()
-    launches = _lib.lib().p4a_kernel_launches() - launches0
-    clocks.stop()
-    dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    done_timed = done[0]
-    dev_ms_max = allmax(dev_ms)
-    value = world * done_timed / (dev_ms_max / 1000.0)
-
-    # roofline of the dominant kernel (live per-kernel events of the timed region)
-    top = max(kern.items(), key=lambda kv: kv[1][0])
-    name, (kms, kl) = top
-    total_ms = sum(x[0] for x in kern.values())
-
-    def kernel_bytes(k):
-        return ALGO_BYTES.get(k, 0) + (64 if k == "reorder" and sim.info()["n_bodies"] else 0)
-
-    def kernel_line(k, v):
-        """Per-kernel share and HBM fraction (algorithmic bytes / average launch time)."""
-        out = {"ms_total": round(v[0], 4), "launches": v[1], "share": round(v[0] / total_ms, 4),
-               "us_per_launch": round(v[0] / max(1, v[1]) * 1000, 2)}
-        if kernel_bytes(k):
-            gbs = kernel_bytes(k) * prof_n_avg / (v[0] / max(1, v[1]) / 1000.0) / 1e9
-            out.update({"algorithmic_gbs": round(gbs, 1), "hbm_frac": round(gbs / peaks()[0], 4)})
-        return out
-
-    per_p = kernel_bytes(name)
-    avg_s = kms / kl / 1000.0
-    n_avg = done_timed / max(1, subs)  # mean particles per substep (grows with a hose)
-    algo = per_p * prof_n_avg
-    peak, peak_kind = peaks()
-    achieved = algo / avg_s / 1e9
-    roofline = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": committed_traffic(name, args.workload),
-                "peak_source": peak_kind, "algorithmic_bytes_per_launch": algo,
-                "issue_frac_ncu": committed_issue(name, args.workload),
-                "l2_hit_pct_ncu": committed_value(name, args.workload, "l2_hit_pct"),
-                "note": "the neighbour passes are bound by instruction issue and load latency, not HBM: "
-                        "issue_frac_ncu is the kernel's issue-slot utilisation from its committed ncu summary",
-                "avg_launch_us": avg_s * 1e6,
-                "kernels": {k: kernel_line(k, v) for k, v in sorted(kern.items(), key=lambda kv: -kv[1][0])}}
-
-    if name in NEIGHBOUR_KERNELS:
-        tf = NEIGHBOUR_FLOP_PER_PARTICLE * prof_n_avg / avg_s / 1e12
-        roofline["fp32"] = {"achieved_tflops": tf, "peak_tflops": fp32_peak_tflops(),
-                            "frac": tf / fp32_peak_tflops(), "flop_per_particle": NEIGHBOUR_FLOP_PER_PARTICLE,
-                            "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x max SM clock",
-                            "what": "FP32 work of the pairs within h only; neither this nor HBM bounds the pass"}
-
-    # whole-step HBM roofline with the fixed per-particle-substep formula of the
-    # workload definition: sort (36 + 4 + 84), k x (lambda 24 + delta 36), finish 68,
-    # bodies +64 per particle and 88 x k per body particle, tension +56, scan 8 per
-    # cell, and 64 per particle per frame for the anisotropic pass
-    k_it = max(1, int(params["iterations"]))
-    info_now = sim.info()
-    bpp = 36 + 4 + 84 + k_it * (24 + 36) + 68 + (64 if info_now["n_bodies"] else 0) + \
-        (56 if params.get("surfaceTensionK", 0) > 0 else 0)
-    step_bytes = done_timed * bpp + subs * (info_now["n_body_parts"] * 88 * k_it + 8 * info_now["n_cells"])
-    if aniso:
-        step_bytes += args.steps * n_avg * 64
-    step_achieved = step_bytes / (dev_ms / 1000.0) / 1e9
-    step_roofline = {"bound": "hbm", "achieved": step_achieved, "peak": peak, "unit": "GB/s",
-                     "frac": step_achieved / peak, "peak_source": peak_kind,
-                     "bytes_per_particle_substep": bpp,
-                     "what": "whole step: fixed algorithmic bytes of the workload definition over the "
-                             "device time of the timed steps"}
-
-    # end to end through the public API: host state in, step, host state out
-    e2e = None
-    if not args.no_e2e:
-        L = _lib.lib()
-        check = _lib.check
-        h = sim._h
-        cap = max(1, sim.info()["cap"])
-        hp = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
-        hv = torch.empty(cap * 4, dtype=torch.float32, pin_memory=True)
-        hs = torch.empty(8, dtype=torch.int32, pin_memory=True)
-        nb0 = sim.info()["n"] * 16
-        L.p4a_read(h, 0, -1, hp.data_ptr(), 0, nb0)
-        L.p4a_read(h, 1, -1, hv.data_ptr(), 0, nb0)
-        e_steps = max(3, min(args.steps, 50))
-        barrier()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        done[0] = 0.0
-        h2d = d2h = 0
-        nb2 = [0]
-
-        def read_state():
-            # the step's pos / vel leave on the copy stream while the anisotropic
-            # pass (which changes neither) runs
-            nb2[0] = sim.info()["n"] * 16
-            check(L.p4a_read_async(h, 0, -1, hp.data_ptr(), 0, nb2[0]), h, "read_async")
-            check(L.p4a_read_async(h, 1, -1, hv.data_ptr(), 0, nb2[0]), h, "read_async")
-        for _ in range(e_steps):
-            nb = sim.info()["n"] * 16
-            check(L.p4a_write(h, 0, -1, hp.data_ptr(), 0, nb), h, "write")
-            check(L.p4a_write(h, 1, -1, hv.data_ptr(), 0, nb), h, "write")
-            frame(read_state)
-            check(L.p4a_read(h, 17, -1, hs.data_ptr(), 0, 32), h, "read")
-            check(L.p4a_read_wait(h), h, "read_wait")
-            h2d += 2 * nb
-            d2h += 2 * nb2[0] + 32
-        t1 = time.perf_counter()
-        barrier()
-        el = allmax(t1 - t0)
-        e2e = {"value": world * done[0] / el, "unit": METRIC, "h2d_bytes_per_step": h2d // e_steps,
-               "d2h_bytes_per_step": d2h // e_steps, "steps": e_steps,
-               "what": "per step: live pos+vel written from pinned host, Sim.step (+ hose, + aniso as the "
-                       "workload has them), pos+vel read back to pinned host on the copy stream (overlapping "
-                       "the anisotropic pass) and stats read back, all waited for"}
-
-    render = None
-    if world == 1 and aniso and not args.no_render:
-        render = render_bench(sim, params, stream)
-
-    mix = None
-    if world == 1 and not args.no_mix:
-        mix = batched_mix_bench(args.mix_frames, 3)
-
-    served = None
-    if world == 1 and args.serve_seconds > 0:
-        try:
-            served = served_bench(args.serve_seconds, args.serve_budget_gb)
-        except Exception as e:  # the headline line is still printed
-            served = {"error": f"{type(e).__name__}: {e}"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(params, scene, aniso, args.cpu_seconds)
-
-    if rank == 0:
-        st = sim.get_stats()
-        line = {
-            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-            "warmup": max(3, args.warmup), "ms_per_step": dev_ms_max / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": args.workload, "n_particles": n, "n_particles_end": sim.info()["n"],
-                       "hose": "2,048 particles per step at 3 m/s" if hose else None,
-                       "n_bodies": sim.info()["n_bodies"],
-                       "substeps_per_step": subs // args.steps, "iterations": params["iterations"],
-                       "surface_tension": params["surfaceTensionK"], "aniso_pass": bool(aniso),
-                       "l2": "flushed between timed steps (256 MiB write outside the timed events)",
-                       "parallelism": f"replicas x{world}"},
-            "roofline": roofline, "step_roofline": step_roofline, "cpu_baseline": cpu, "e2e": e2e,
-            "gpu_launches": launches,
-            "batched_mix": mix,
-            "render": render,
-            "served": served,
-            "clocks": clocks.summary(w0, w1),
-            "final_stats": {k: st[k] for k in ("avgRho", "maxRho", "maxSpeed")},
-        }
-        print(json.dumps(line), flush=True)
-    sim.close()
-    rep.close()
     return 0
 
 
@@ -718,7 +968,9 @@ def main():
         return only_mix(args.only_mix, args.mix_frames)
     if args.only_render:
         return only_render(args)
-    return run_ours(args)
+    if args.workload == MIX:
+        return run_mix(args)
+    return run_single_line(args)
 
 
 if __name__ == "__main__":

@@ -487,8 +487,25 @@ int p4a_batch_read(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which, vo
 int p4a_batch_write(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which, const void* host,
                     size_t offset, size_t bytes);
 int p4a_batch_stats(p4a_batch* b, int32_t scene_id, p4a_stats* out);
+/* Asynchronous per-scene copies on the batch's stream, ordered after the frames
+ * queued before them and before the ones queued after; the host memory (pinned
+ * for an asynchronous copy) stays in use until p4a_batch_synchronize. The
+ * cellStart buffer is not available here (p4a_batch_read converts its arena
+ * indices). */
+int p4a_batch_read_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which, void* host,
+                         size_t offset, size_t bytes);
+int p4a_batch_write_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which,
+                          const void* host, size_t offset, size_t bytes);
 /* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
 int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
+/* Per-kernel timing of batched frames, as p4a_profile_* for a Sim (the
+ * counterpart of the reference's GpuTimer phases, src/gputimer.js): with it on,
+ * every launch of a frame is bracketed by events (event-record nodes inside a
+ * replayed graph), and p4a_profile_read-style totals per kernel name ("lambda",
+ * "delta", ...) accumulate since the last reset. */
+int p4a_batch_profile_enable(p4a_batch* b, int32_t on);
+int p4a_batch_profile_reset(p4a_batch* b);
+int p4a_batch_profile_read(p4a_batch* b, p4a_phase_time* out, int32_t max_entries, int32_t* count);
 
 /* ---- serving loop (no counterpart in the reference) --------------------- */
 /*

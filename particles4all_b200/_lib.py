@@ -62,6 +62,11 @@ SIGNATURES = {
     "p4a_batch_write": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
     "p4a_batch_stats": ([_vp, _i32, _vp], C.c_int),
     "p4a_batch_use_graphs": ([_vp, _i32], C.c_int),
+    "p4a_batch_read_async": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_batch_write_async": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
+    "p4a_batch_profile_enable": ([_vp, _i32], C.c_int),
+    "p4a_batch_profile_reset": ([_vp], C.c_int),
+    "p4a_batch_profile_read": ([_vp, _vp, _i32, C.POINTER(_i32)], C.c_int),
     "p4a_server_default_config": ([_vp], C.c_int),
     "p4a_server_create": ([C.c_int, _vp, C.POINTER(_vp)], C.c_int),
     "p4a_server_destroy": ([_vp], C.c_int),

@@ -113,6 +113,30 @@ class Batch:
         self._check(self._L.p4a_batch_write(self._h, int(sid), bid, which, a.ctypes.data,
                                             offset_elems * 4 * comps, a.nbytes), "write")
 
+    def read_async(self, sid, name, host_ptr, nbytes, which=_abi.LIVE, offset=0):
+        """Queue a copy of the scene's buffer into host memory at host_ptr (pinned
+        for an asynchronous copy); complete after synchronize()."""
+        self._check(self._L.p4a_batch_read_async(self._h, int(sid), _abi.BUF[name], which, C.c_void_p(host_ptr),
+                                                 int(offset), int(nbytes)), "read_async")
+
+    def write_async(self, sid, name, host_ptr, nbytes, which=_abi.LIVE, offset=0):
+        """Queue a copy from host memory at host_ptr into the scene's buffer."""
+        self._check(self._L.p4a_batch_write_async(self._h, int(sid), _abi.BUF[name], which, C.c_void_p(host_ptr),
+                                                  int(offset), int(nbytes)), "write_async")
+
+    def profile(self, on=True):
+        self._check(self._L.p4a_batch_profile_enable(self._h, 1 if on else 0), "profile_enable")
+
+    def profile_reset(self):
+        self._check(self._L.p4a_batch_profile_reset(self._h), "profile_reset")
+
+    def profile_read(self):
+        """{kernel name: (device ms, launches)} of the frames since profile_reset()."""
+        arr = (_abi.PhaseTime * 32)()
+        cnt = C.c_int32()
+        self._check(self._L.p4a_batch_profile_read(self._h, arr, 32, C.byref(cnt)), "profile_read")
+        return {arr[i].name.decode(): (arr[i].ms, arr[i].launches) for i in range(min(cnt.value, 32))}
+
     def stats(self, sid):
         s = _abi.Stats()
         self._check(self._L.p4a_batch_stats(self._h, int(sid), C.byref(s)), "stats")

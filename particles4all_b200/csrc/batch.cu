@@ -156,17 +156,30 @@ WorkSeg push_items(Frame& F, uint32_t row, int64_t count, WorkSeg seg) {
 
 void add_launch(Frame& F, int kind, int sub, int it, WorkSeg seg) { F.launches.push_back({kind, sub, it, seg}); }
 
+constexpr const char* kLaunchNames[] = {"zero_stats", "key_count", "scan", "fill", "reorder", "body_seed",
+                                         "lambda", "delta", "body_match", "xsph_finalize", "xsph_normals",
+                                         "tension_finalize"};
+constexpr int kLaunchKinds = (int)(sizeof(kLaunchNames) / sizeof(kLaunchNames[0]));
+
 // Launches one frame on the batch's stream. Graph form: every launch of the shape
 // is issued with the resident grid and fixed-size clears (counts are read on the
 // device); direct form: empty launches are skipped and grids fit the counts.
-int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched) {
+// With `ev` (launches + 1 events), ev[L] is recorded before launch L and the last
+// one after the last launch (as event-record nodes when the stream is captured).
+int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched,
+              const std::vector<cudaEvent_t>* ev = nullptr) {
   cudaStream_t st = b->stream;
   DevScene& d = b->d;
   const int stride = b->cfg.max_scenes;
   uint64_t n = 0;
+  auto record = [&](size_t k) {
+    return graphForm ? cudaEventRecordWithFlags((*ev)[k], st, cudaEventRecordExternal)
+                     : cudaEventRecord((*ev)[k], st);
+  };
   BTRY(b, cudaMemsetAsync(b->dCursors, 0, F.launches.size() * sizeof(uint32_t), st));
   for (size_t L = 0; L < F.launches.size(); L++) {
     const LaunchRec& r = F.launches[L];
+    if (ev) BTRY(b, record(L));
     if (!graphForm && r.seg.count == 0) continue;
     BatchWork w;
     w.params = b->dParams + (size_t)r.sub * stride;
@@ -193,14 +206,57 @@ int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched) 
     }
     n++;
   }
+  if (ev) BTRY(b, record(F.launches.size()));
   BTRY(b, cudaGetLastError());
   if (launched) *launched = n;
   return P4A_OK;
 }
 
+// Adds the intervals of every profiled frame queued so far to the per-kernel totals.
+int resolve_profile(p4a_batch* b) {
+  for (auto& pf : b->profPending) {
+    BTRY(b, cudaEventSynchronize(pf.ev.back()));
+    for (size_t k = 0; k + 1 < pf.ev.size(); k++) {
+      if (pf.kinds[k] < 0) continue;
+      float ms = 0.0f;
+      BTRY(b, cudaEventElapsedTime(&ms, pf.ev[k], pf.ev[k + 1]));
+      b->profMs[pf.kinds[k]] += ms;
+      b->profLaunches[pf.kinds[k]]++;
+    }
+    b->profFree.push_back(std::move(pf.ev));
+  }
+  b->profPending.clear();
+  return P4A_OK;
+}
+
+// A set of `count` timing events from the pool (created on demand).
+int take_events(p4a_batch* b, size_t count, std::vector<cudaEvent_t>* out) {
+  for (size_t k = 0; k < b->profFree.size(); k++) {
+    if (b->profFree[k].size() == count) {
+      *out = std::move(b->profFree[k]);
+      b->profFree.erase(b->profFree.begin() + (long)k);
+      return P4A_OK;
+    }
+  }
+  out->assign(count, nullptr);
+  for (auto& e : *out) BTRY(b, cudaEventCreate(&e));
+  return P4A_OK;
+}
+
+void drop_profile_events(p4a_batch* b) {
+  for (auto& pf : b->profPending) b->profFree.push_back(std::move(pf.ev));
+  b->profPending.clear();
+  for (auto& set : b->profFree)
+    for (auto e : set) cudaEventDestroy(e);
+  b->profFree.clear();
+}
+
 void drop_graphs(p4a_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  for (auto& kv : b->profNodes)
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  b->profNodes.clear();
 }
 
 int ensure_device_lists(p4a_batch* b, int64_t nItems, int64_t nLaunches) {
@@ -264,18 +320,32 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
   if (iBytes) BTRY(b, cudaMemcpyAsync(b->dItems, h + pBytes, iBytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaMemcpyAsync(b->dSegs, segs, sBytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaEventRecord(b->stagingDone[k], b->stream));
+  const size_t nEv = F.launches.size() + 1;
+  p4a_batch::ProfPending pf;
+  if (b->prof) {
+    if (b->profPending.size() >= 64 && (rc = resolve_profile(b))) return rc;
+    if ((rc = take_events(b, nEv, &pf.ev))) return rc;
+    pf.kinds.assign(nEv, -1);
+  }
   if (!(allowGraph && b->useGraphs)) {
     uint64_t n = 0;
-    rc = run_frame(b, F, false, &n);
+    rc = run_frame(b, F, false, &n, b->prof ? &pf.ev : nullptr);
     count_launches(n);
+    if (b->prof) {
+      for (size_t L = 0; L < F.launches.size(); L++)
+        if (F.launches[L].seg.count) pf.kinds[L] = F.launches[L].kind;
+      b->profPending.push_back(std::move(pf));
+    }
     return rc;
   }
-  auto it = b->graphs.find(F.shape);
+  std::vector<int> key = F.shape;
+  if (b->prof) key.push_back(-1);  // the profiled graph of the shape has event nodes
+  auto it = b->graphs.find(key);
   if (it == b->graphs.end()) {
     if (b->graphs.size() >= 16) drop_graphs(b);
     cudaGraph_t g = nullptr;
     BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    const int brc = run_frame(b, F, true, nullptr);
+    const int brc = run_frame(b, F, true, nullptr, b->prof ? &pf.ev : nullptr);
     const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
     if (brc) {
       if (g) cudaGraphDestroy(g);
@@ -284,12 +354,50 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
     if (ec != cudaSuccess) return bfail(b, P4A_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
     cudaGraphExec_t ge = nullptr;
     const cudaError_t ei = cudaGraphInstantiate(&ge, g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) return bfail(b, P4A_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
-    it = b->graphs.emplace(F.shape, ge).first;
+    if (ei != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return bfail(b, P4A_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+    }
+    if (b->prof) {
+      // the event-record node of each event of the capture, by the event's index
+      p4a_batch::ProfNodes pn;
+      pn.graph = g;
+      pn.nodes.assign(nEv, nullptr);
+      size_t count = 0;
+      BTRY(b, cudaGraphGetNodes(g, nullptr, &count));
+      std::vector<cudaGraphNode_t> all(count);
+      BTRY(b, cudaGraphGetNodes(g, all.data(), &count));
+      for (auto node : all) {
+        cudaGraphNodeType t;
+        BTRY(b, cudaGraphNodeGetType(node, &t));
+        if (t != cudaGraphNodeTypeEventRecord) continue;
+        cudaEvent_t e = nullptr;
+        BTRY(b, cudaGraphEventRecordNodeGetEvent(node, &e));
+        for (size_t k = 0; k < nEv; k++)
+          if (pf.ev[k] == e) pn.nodes[k] = node;
+      }
+      for (auto node : pn.nodes)
+        if (!node) {
+          cudaGraphExecDestroy(ge);
+          cudaGraphDestroy(g);
+          return bfail(b, P4A_ERR_CUDA, "profiled graph: an event-record node is missing");
+        }
+      b->profNodes[key] = std::move(pn);
+    } else {
+      cudaGraphDestroy(g);
+    }
+    it = b->graphs.emplace(key, ge).first;
+  }
+  if (b->prof) {
+    // later replays may still be reading this set's events: point the nodes at it
+    const auto& pn = b->profNodes[key];
+    for (size_t k = 0; k < nEv; k++)
+      BTRY(b, cudaGraphExecEventRecordNodeSetEvent(it->second, pn.nodes[k], pf.ev[k]));
+    for (size_t L = 0; L < F.launches.size(); L++) pf.kinds[L] = F.launches[L].kind;
   }
   BTRY(b, cudaGraphLaunch(it->second, b->stream));
   count_launches(F.launches.size());
+  if (b->prof) b->profPending.push_back(std::move(pf));
   return P4A_OK;
 }
 
@@ -747,6 +855,7 @@ int p4a_batch_destroy(p4a_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
+  drop_profile_events(b);
   for (void* p : b->allocs) cudaFree(p);
   if (b->dItems) cudaFree(b->dItems);
   if (b->dSegs) cudaFree(b->dSegs);
@@ -783,6 +892,41 @@ int p4a_batch_use_graphs(p4a_batch* b, int32_t on) {
   if (!b) return P4A_ERR_ARG;
   b->useGraphs = on != 0;
   return P4A_OK;
+}
+
+int p4a_batch_profile_enable(p4a_batch* b, int32_t on) {
+  if (!b) return P4A_ERR_ARG;
+  b->prof = on != 0;
+  return P4A_OK;
+}
+
+int p4a_batch_profile_reset(p4a_batch* b) {
+  if (!b) return P4A_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int rc = resolve_profile(b);
+  for (int k = 0; k < kLaunchKinds; k++) {
+    b->profMs[k] = 0;
+    b->profLaunches[k] = 0;
+  }
+  return rc;
+}
+
+int p4a_batch_profile_read(p4a_batch* b, p4a_phase_time* out, int32_t maxEntries, int32_t* count) {
+  if (!b || (maxEntries > 0 && !out)) return P4A_ERR_ARG;
+  cudaSetDevice(b->device);
+  const int rc = resolve_profile(b);
+  int c = 0;
+  for (int k = 0; k < kLaunchKinds; k++) {
+    if (b->profLaunches[k] == 0) continue;
+    if (c < maxEntries) {
+      std::snprintf(out[c].name, sizeof(out[c].name), "%s", kLaunchNames[k]);
+      out[c].ms = b->profMs[k];
+      out[c].launches = b->profLaunches[k];
+    }
+    c++;
+  }
+  if (count) *count = c;
+  return rc;
 }
 
 int p4a_batch_add_scene(p4a_batch* b, const p4a_params* params, const p4a_scene_desc* sd, int32_t* id) {
@@ -955,6 +1099,43 @@ int p4a_batch_write(p4a_batch* b, int32_t id, int32_t bid, int32_t which, const 
   cudaSetDevice(b->device);
   BTRY(b, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, b->stream));
   BTRY(b, cudaStreamSynchronize(b->stream));
+  return P4A_OK;
+}
+
+// Asynchronous forms: the copy is queued on the batch's stream behind the frames
+// already queued (and before the next ones); host memory stays in use until
+// p4a_batch_synchronize. cellStart holds arena indices, so it is not offered here.
+int p4a_batch_read_async(p4a_batch* b, int32_t id, int32_t bid, int32_t which, void* host, size_t offset,
+                         size_t bytes) {
+  int rc = scene_ok(b, id);
+  if (rc) return rc;
+  if (!host && bytes) return P4A_ERR_ARG;
+  if (bid == P4A_BUF_CELL_START) return bfail(b, P4A_ERR_ARG, "cellStart is read with p4a_batch_read only");
+  const BScene& s = b->scenes[id];
+  void* p = nullptr;
+  size_t total = 0;
+  if ((rc = scene_buffer(b, s, bid, which, &p, &total))) return rc;
+  if (offset > total || bytes > total - offset) return bfail(b, P4A_ERR_ARG, "read beyond the scene's buffer");
+  if (!bytes) return P4A_OK;
+  cudaSetDevice(b->device);
+  BTRY(b, cudaMemcpyAsync(host, (const char*)p + offset, bytes, cudaMemcpyDeviceToHost, b->stream));
+  return P4A_OK;
+}
+
+int p4a_batch_write_async(p4a_batch* b, int32_t id, int32_t bid, int32_t which, const void* host, size_t offset,
+                          size_t bytes) {
+  int rc = scene_ok(b, id);
+  if (rc) return rc;
+  if (!host && bytes) return P4A_ERR_ARG;
+  if (bid == P4A_BUF_CELL_START) return bfail(b, P4A_ERR_ARG, "cellStart is written by the sort only");
+  const BScene& s = b->scenes[id];
+  void* p = nullptr;
+  size_t total = 0;
+  if ((rc = scene_buffer(b, s, bid, which, &p, &total))) return rc;
+  if (offset > total || bytes > total - offset) return bfail(b, P4A_ERR_ARG, "write beyond the scene's buffer");
+  if (!bytes) return P4A_OK;
+  cudaSetDevice(b->device);
+  BTRY(b, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, b->stream));
   return P4A_OK;
 }
 

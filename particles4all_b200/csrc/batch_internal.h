@@ -117,6 +117,23 @@ struct p4a_batch {
   bool useGraphs = true;
   cudaStream_t upStream = nullptr;  // admissions' uploads (serving loop)
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
+  // per-kernel timing of frames (p4a_batch_profile_*): an event before every launch
+  // of a frame and one after the last; in a graph these are event-record nodes,
+  // pointed at a fresh set of events before each replay
+  struct ProfNodes {
+    cudaGraph_t graph = nullptr;            // kept: the exec's nodes belong to it
+    std::vector<cudaGraphNode_t> nodes;     // event-record node of event index k
+  };
+  struct ProfPending {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kinds;  // launch kind of interval k (-1: nothing launched)
+  };
+  bool prof = false;
+  std::map<std::vector<int>, ProfNodes> profNodes;  // by graph key
+  std::vector<std::vector<cudaEvent_t>> profFree;
+  std::vector<ProfPending> profPending;
+  double profMs[16] = {};
+  long long profLaunches[16] = {};
 };
 
 
