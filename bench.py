@@ -100,8 +100,12 @@ def hose_for(params, scene):
 
 
 def pour(sim, hose):
+    """One hose layer: emitted on the device for the library's Sim (p4a_hose_emit),
+    computed on the host and appended for the oracle (the same bits)."""
     if hose is None:
         return 0
+    if hasattr(sim, "hoseEmit"):
+        return sim.hoseEmit(hose)
     pos, vel = hose.emit()
     return 0 if pos is None else sim.appendFluid(pos, vel)
 
@@ -266,16 +270,8 @@ def bytes_per_particle_substep(iterations, bodies, tension):
 
 def mix_arenas(mix):
     """Batch arena sizes that hold the whole mix."""
-    cap = sum((sc["pos"].shape[0] + 511) // 256 * 256 for _, sc in mix)
-    cells = sum((int(math.prod(int(b) for b in p["box"])) // 2048 + 2) * 2048 for p, _ in mix)
-    nbound = 0
-    for p, _ in mix:
-        nb = [max(2, math.ceil(b / p["spacing"]) + 1) for b in p["box"]]
-        nbound += nb[0] * nb[1] * nb[2] - (nb[0] - 2) * (nb[1] - 2) * (nb[2] - 2)
-    bodies = sum(sc["n_bodies"] + 1 for _, sc in mix)
-    body_parts = sum(int((sc["phase"][:, 0] > 0).sum()) + 1 for _, sc in mix)
-    return dict(max_particles=cap + 4096, max_cells=cells, max_scenes=len(mix) + 1, max_bodies=bodies + 8,
-                max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
+    from particles4all_b200.batch import arena_sizes
+    return arena_sizes(mix)
 
 
 def mix_config(mix, world):
@@ -777,12 +773,12 @@ def single_scene(name, steps, warm, rep, world, local, e2e_on=True, render=False
         t1 = time.perf_counter()
         rep.barrier()
         el = rep.max(t1 - t0)
-        h2d += appended[0] * 24  # the hose's layers (float3 pos + vel) go up through p4a_append_fluid
         e2e = {"value": world * done[0] / el, "unit": METRIC, "h2d_bytes_per_step": h2d // e_steps,
                "d2h_bytes_per_step": d2h // e_steps, "steps": e_steps,
                "what": "per step: live pos+vel written from pinned host, Sim.step (+ hose, + aniso as the "
-                       "workload has them), pos+vel read back to pinned host on the copy stream (overlapping "
-                       "the anisotropic pass) and stats read back, all waited for"}
+                       "workload has them; the hose layer is emitted on the device), pos+vel read back to "
+                       "pinned host on the copy stream (overlapping the anisotropic pass) and stats read back, "
+                       "all waited for"}
 
     rend = render_bench(sim, params, stream) if render else None
     st = sim.get_stats()

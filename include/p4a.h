@@ -213,6 +213,25 @@ int p4a_step(p4a_sim* sim, double frame_dt, int32_t* substeps_out);
  * arrays of `count` entries; appends min(count, cap - n), stored in *added. */
 int p4a_append_fluid(p4a_sim* sim, const float* pos3, const float* vel3, int32_t count,
                      int32_t* added);
+/* The layered hose of pourStep (src/main.js:106-160) at a fixed rate, emitted on
+ * the device: one layer of min(per_step, cap - n) particles appended at index n
+ * with the appendFluid semantics (src/sim.js:774-809: live pos/vel and the pred
+ * parity written, density rho0, zero lambda/corr/normal/body/rest), computed by a
+ * kernel from its emission index, so nothing crosses from the host and the call
+ * does not wait. Layer slot q: row iy = q / k, column iz = q % k with
+ * k = ceil(sqrt(per_step)); position nozzle + ((0, iy - c, iz - c) * spacing) + j,
+ * c = (k - 1) / 2, velocity (speed, 0, 0); j per axis uniform in
+ * [-jitter, jitter) from Philox4x32-10 keyed by (seed, emission, q). The host
+ * restatement is particles4all_b200.configs.Hose. */
+typedef struct p4a_hose {
+  float nozzle[3];
+  float spacing;
+  float jitter;
+  float speed;
+  int32_t per_step;
+  uint32_t seed;
+} p4a_hose;
+int p4a_hose_emit(p4a_sim* sim, const p4a_hose* hose, int64_t emission, int32_t* added);
 /* Sim.applyRayImpulse(origin, dir, impulse, radius, speedLimit) (src/sim.js:658-676). */
 int p4a_apply_ray_impulse(p4a_sim* sim, const double origin[3], const double dir[3],
                           const double impulse[3], double radius, double speed_limit);

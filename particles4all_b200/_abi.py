@@ -129,6 +129,11 @@ class Grid(C.Structure):
     _fields_ = [("box_min", C.c_float * 3), ("h", C.c_float), ("dim", C.c_int32 * 3)]
 
 
+class Hose(C.Structure):
+    _fields_ = [("nozzle", C.c_float * 3), ("spacing", C.c_float), ("jitter", C.c_float), ("speed", C.c_float),
+                ("per_step", C.c_int32), ("seed", C.c_uint32)]
+
+
 class SceneCounts(C.Structure):
     _fields_ = [
         ("n", C.c_int32), ("n_fluid", C.c_int32), ("n_body", C.c_int32),

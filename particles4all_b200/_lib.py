@@ -40,6 +40,7 @@ SIGNATURES = {
     "p4a_grid_sort_workspace_size": ([_i32, _i32], _sz),
     "p4a_grid_sort": ([_vp, _i32, _f32, _f32] + [_vp] * 11 + [_vp, _sz, _vp, _vp], C.c_int),
     "p4a_test_scan_wait": ([C.c_uint32, _i32], C.c_int),
+    "p4a_hose_emit": ([_vp, _vp, C.c_int64, C.POINTER(_i32)], C.c_int),
     "p4a_build_scene": ([_vp] * 8, C.c_int),
     "p4a_profile_enable": ([_vp, _i32], C.c_int),
     "p4a_profile_reset": ([_vp], C.c_int),

@@ -12,6 +12,7 @@ scene are bit-identical to stepping that scene alone.
     pos = b.read(sid, "pos")
 """
 import ctypes as C
+import math
 
 import numpy as np
 
@@ -19,6 +20,23 @@ from . import _abi
 from ._lib import P4AError, lib
 from ._scene_desc import scene_desc
 from .params import CParams
+
+
+def arena_sizes(scenes, spare_particles=4096):
+    """Batch arena sizes (keyword arguments of Batch) that hold every (params,
+    scene) of `scenes` at once: particle ranges rounded to 256 with room for
+    alignment, cell ranges padded to whole 2,048-cell scan tiles, the boundary
+    shell of each box at the scene's spacing, and each scene's bodies."""
+    cap = sum((sc["pos"].shape[0] + 511) // 256 * 256 for _, sc in scenes)
+    cells = sum((int(math.prod(int(b) for b in p["box"])) // 2048 + 2) * 2048 for p, _ in scenes)
+    nbound = 0
+    for p, _ in scenes:
+        nb = [max(2, math.ceil(b / p["spacing"]) + 1) for b in p["box"]]
+        nbound += nb[0] * nb[1] * nb[2] - (nb[0] - 2) * (nb[1] - 2) * (nb[2] - 2)
+    bodies = sum(sc["n_bodies"] + 1 for _, sc in scenes)
+    body_parts = sum(int((sc["phase"][:, 0] > 0).sum()) + 1 for _, sc in scenes)
+    return dict(max_particles=cap + spare_particles, max_cells=cells, max_scenes=len(scenes) + 1,
+                max_bodies=bodies + 8, max_boundary=nbound + 4096, max_body_parts=body_parts + 64)
 
 
 class Batch:

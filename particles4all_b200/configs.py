@@ -184,35 +184,87 @@ def large_hose_2m(seed=2, side=128, n_bodies=64, target_total=2_500_000):
     return params, scene
 
 
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Philox4x32-10 (Salmon, Moraes, Dror and Shaw, SC 2011) on numpy uint32
+    counter arrays with key (k0, k1): the generator of the device hose
+    (csrc/kernels_hose.cu), restated word for word."""
+    m0, m1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+    mask = np.uint64(0xFFFFFFFF)
+    c0, c1, c2, c3 = (np.asarray(c, np.uint32) for c in (c0, c1, c2, c3))
+    for _ in range(10):
+        p0 = m0 * c0.astype(np.uint64)
+        p1 = m1 * c2.astype(np.uint64)
+        hi0, lo0 = (p0 >> np.uint64(32)).astype(np.uint32), (p0 & mask).astype(np.uint32)
+        hi1, lo1 = (p1 >> np.uint64(32)).astype(np.uint32), (p1 & mask).astype(np.uint32)
+        c0, c1, c2, c3 = hi1 ^ c1 ^ np.uint32(k0), lo1, hi0 ^ c3 ^ np.uint32(k1), lo0
+        k0 = (k0 + 0x9E3779B9) & 0xFFFFFFFF
+        k1 = (k1 + 0xBB67AE85) & 0xFFFFFFFF
+    return c0, c1, c2, c3
+
+
 class Hose:
-    """A hose emitting `per_step` particles per step at `speed` from the near wall:
-    square k x k lattice layers (k = ceil(sqrt(per_step))) with seeded jitter, the
-    layered emitter of src/main.js:106-160 at a fixed rate."""
+    """A hose emitting `per_step` particles per step at `speed` along +x from the
+    near wall: square k x k lattice layers (k = ceil(sqrt(per_step))) with jitter,
+    the layered emitter of src/main.js:106-160 at a fixed rate, up to `limit`
+    particles in total. The jitter of emission e, slot q and axis a is uniform in
+    [-0.001 d, 0.001 d) from Philox4x32-10 keyed by (seed, e, q), so a layer is a
+    function of its emission index: Sim.hoseEmit computes it on the device, and
+    emit() computes the same float32 bits on the host (the oracle's input)."""
 
     def __init__(self, box, d, per_step=2048, speed=3.0, height=0.6, seed=22222, limit=None):
         self.box, self.d, self.per_step, self.speed = box, d, per_step, speed
         self.k = int(math.ceil(math.sqrt(per_step)))
-        self.nozzle = np.array([2.0 * d + d, height * box[1], 0.5 * box[2]])
-        self.rng = np.random.default_rng(seed)
+        self.nozzle = np.array([2.0 * d + d, height * box[1], 0.5 * box[2]]).astype(np.float32)
+        self.spacing = np.float32(d)
+        self.jitter = np.float32(0.001 * d)
+        self.seed = int(seed) & 0xFFFFFFFF
         self.left = limit
+        self.emission = 0
+
+    def c_struct(self):
+        from ._abi import Hose as CHose
+        h = CHose()
+        for a in range(3):
+            h.nozzle[a] = float(self.nozzle[a])
+        h.spacing, h.jitter, h.speed = float(self.spacing), float(self.jitter), float(self.speed)
+        h.per_step = self.per_step if self.left is None else max(0, min(self.per_step, self.left))
+        h.seed = self.seed
+        return h
+
+    def advance(self, n):
+        """Book one emission of n particles."""
+        self.emission += 1
+        if self.left is not None:
+            self.left -= n
+
+    def layer(self, emission, n):
+        """Positions and velocities (float32, n x 3) of slots [0, n) of an emission."""
+        q = np.arange(n, dtype=np.uint32)
+        e = np.uint64(emission)
+        w = philox4x32_10(np.full(n, e & np.uint64(0xFFFFFFFF), np.uint32),
+                          np.full(n, e >> np.uint64(32), np.uint32), q, np.zeros(n, np.uint32),
+                          self.seed, 0x5EED5EED)
+        f32 = np.float32
+        j = [((w[a] >> np.uint32(8)).astype(f32) * f32(2.0 ** -24) * f32(2.0) - f32(1.0)) * self.jitter
+             for a in range(3)]
+        iy, iz = (q // np.uint32(self.k)).astype(f32), (q % np.uint32(self.k)).astype(f32)
+        c = f32((self.k - 1) * 0.5)
+        pos = np.zeros((n, 3), f32)
+        pos[:, 0] = self.nozzle[0] + j[0]
+        pos[:, 1] = (self.nozzle[1] + (iy - c) * self.spacing) + j[1]
+        pos[:, 2] = (self.nozzle[2] + (iz - c) * self.spacing) + j[2]
+        vel = np.zeros((n, 3), f32)
+        vel[:, 0] = f32(self.speed)
+        return pos, vel
 
     def emit(self):
+        """The next layer on the host (None, None once the limit is reached)."""
         n = self.per_step if self.left is None else min(self.per_step, self.left)
         if n <= 0:
             return None, None
-        k, d = self.k, self.d
-        iy, iz = np.meshgrid(np.arange(k), np.arange(k), indexing="ij")
-        yz = np.stack([iy.ravel(), iz.ravel()], 1)[:n].astype(np.float64)
-        pos = np.zeros((n, 3))
-        pos[:, 0] = self.nozzle[0]
-        pos[:, 1] = self.nozzle[1] + (yz[:, 0] - (k - 1) / 2.0) * d
-        pos[:, 2] = self.nozzle[2] + (yz[:, 1] - (k - 1) / 2.0) * d
-        pos += self.rng.uniform(-0.001 * d, 0.001 * d, size=pos.shape)
-        vel = np.zeros((n, 3))
-        vel[:, 0] = self.speed
-        if self.left is not None:
-            self.left -= n
-        return pos.astype(np.float32), vel.astype(np.float32)
+        pos, vel = self.layer(self.emission, n)
+        self.advance(n)
+        return pos, vel
 
 
 def batched_mix(seed=12, count=96, n_lo=4000, n_hi=256000, cube=6):

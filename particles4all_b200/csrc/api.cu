@@ -39,13 +39,13 @@ const double kPi = 3.14159265358979323846;
 enum Phase {
   PH_DRAG, PH_KEY_COUNT, PH_SCAN, PH_FILL, PH_REORDER, PH_BODY_SEED, PH_LAMBDA, PH_DELTA,
   PH_BODY_MATCH, PH_XSPH_FINALIZE, PH_XSPH_NORMALS, PH_TENSION_FINALIZE, PH_ANISO, PH_IMPULSE,
-  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_SSFR, PH_RAY, PH_COUNT,
+  PH_RESIZE, PH_STATS_CLEAR, PH_MESH_FIELD, PH_MESH_BLUR, PH_MESH_MARCH, PH_SSFR, PH_RAY, PH_HOSE, PH_COUNT,
   PH_END = PH_COUNT
 };
 const char* const kPhaseNames[PH_COUNT] = {
     "body_drag", "key_count", "scan", "fill", "reorder", "body_seed", "lambda", "delta",
     "body_match", "xsph_finalize", "xsph_normals", "tension_finalize", "aniso", "impulse",
-    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march", "ssfr", "ray"};
+    "resize", "stats_clear", "mesh_field", "mesh_blur", "mesh_march", "ssfr", "ray", "hose"};
 
 std::atomic<uint64_t> g_launches{0};
 }  // namespace
@@ -378,7 +378,8 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.unordered, cap)) || (rc = dalloc(s, L, &s->d.statsOut, 8)) ||
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbList, cap * kListCap)) ||
       (rc = dalloc(s, L, &s->d.nbCount, cap)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
-      (rc = dalloc(s, L, &s->d.disp, kDispSlots)) || (rc = dalloc(s, L, &s->d.nbRef, cap)))
+      (rc = dalloc(s, L, &s->d.disp, kDispSlots)) || (rc = dalloc(s, L, &s->d.nbRef, cap)) ||
+      (rc = dalloc(s, L, &s->d.predLam, cap)))
     return rc;
   s->d.cap = (uint32_t)cap;
   if ((rc = alloc_cells(s))) return rc;
@@ -894,6 +895,39 @@ int p4a_append_fluid(p4a_sim* s, const float* pos3, const float* vel3, int32_t c
     CUDA_TRY(s, cudaMemsetAsync(d.rest[t] + o4, 0, bytes4, st));
   }
   CUDA_TRY(s, cudaStreamSynchronize(st));  // host staging vectors go out of scope
+  s->n += c;
+  return P4A_OK;
+}
+
+int p4a_hose_emit(p4a_sim* s, const p4a_hose* hose, int64_t emission, int32_t* added) {
+  if (!s || !hose || emission < 0 || hose->per_step < 0 || !(hose->spacing > 0) || !(hose->jitter >= 0))
+    return fail(s, P4A_ERR_ARG, "hose_emit: bad arguments");
+  if (!s->ready) return fail(s, P4A_ERR_STATE, "hose_emit before reset");
+  const int room = std::max(0, s->cap - s->n);
+  const int c = std::min(hose->per_step, room);
+  if (added) *added = std::max(0, c);
+  if (c <= 0) return P4A_OK;
+  cudaSetDevice(s->device);
+  after_reads(s, kAllBuffers);
+  s->sortedMoves = false;
+  HoseEmit H{};
+  uint32_t k = 1;
+  while ((int64_t)k * k < hose->per_step) k++;
+  for (int a = 0; a < 3; a++) H.nozzle[a] = hose->nozzle[a];
+  H.spacing = hose->spacing;
+  H.centre = (float)(k - 1) * 0.5f;
+  H.jitter = hose->jitter;
+  H.speed = hose->speed;
+  H.rho0 = (float)s->params.rest_density;
+  H.k = k;
+  H.count = (uint32_t)c;
+  H.first = (uint32_t)s->n;
+  H.seed = hose->seed;
+  H.emission = (uint64_t)emission;
+  mark(s, PH_HOSE);
+  launch_hose_emit(H, s->d, s->parity, s->predParity, s->stream);
+  mark(s, PH_END);
+  CUDA_TRY(s, cudaGetLastError());
   s->n += c;
   return P4A_OK;
 }

@@ -99,9 +99,9 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
     const uint32_t cap = d.cap;
     const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
     F3 acc = {0.f, 0.f, 0.f};
-    auto fluid = [&](uint32_t j) {
+    auto fluid = [&](uint32_t j, float4 q) {
       if (j == i) return;
-      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+      const F3 rij = sub3(pi, xyz(q));
       const float r2 = dot3(rij, rij);
       if (r2 >= P.h2) return;  // in the skin of a reused list only
       const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
@@ -133,9 +133,9 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
   d.nbCount[i] = count;
   F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
-  auto fluid = [&](uint32_t j) {
+  auto fluid = [&](uint32_t j, float4 q) {
     if (j == i) return;
-    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
     const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
@@ -171,8 +171,8 @@ __device__ __forceinline__ void tension_finalize_body(const SimParams& P, const 
     const RowWalk w(P, pi);
     const uint32_t count = __ldg(&d.nbCount[i]);  // xsph+normals' list for these positions
     F3 acc = {0.f, 0.f, 0.f};
-    auto fluid = [&](uint32_t j) {
-      const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    auto fluid = [&](uint32_t j, float4 q) {
+      const F3 rij = sub3(pi, xyz(q));
       const float r2 = dot3(rij, rij);
       if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
       const float rr = sqrtf(r2);

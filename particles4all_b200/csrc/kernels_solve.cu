@@ -56,9 +56,9 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;
-  auto fluid = [&](uint32_t j) {
+  auto fluid = [&](uint32_t j, float4 q) {
     if (j == i) return;
-    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+    const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of the list only
     rho = fmaf(P.mass, poly6(P, r2), rho);
@@ -71,8 +71,8 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
       sumGrad2 = sumGrad2 + dot3(g, g);
     }
   };
-  auto bound = [&](uint32_t k) {
-    const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+  auto bound = [&](uint32_t k, float4 q) {
+    const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float psi = __ldg(&d.bpsi[k]);
@@ -83,37 +83,40 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     gradSum = fma3(s, rij, gradSum);
   };
   if (count != kListOverflow) {
-    walk_list(d.nbList, cap, i, count, fluid, bound);
+    walk_list(d.nbList, cap, i, count, pred, d.bpos, fluid, bound);
   } else {
     walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
   }
   d.density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
+  float lam = 0.0f;
   if (C > 0.0f) {
     const float den = dot3(gradSum, gradSum) + sumGrad2 + P.cfmEps + 1.0e-12f;
-    d.lambda[i] = -C / den;
-  } else {
-    d.lambda[i] = 0.0f;
+    lam = -C / den;
   }
+  d.lambda[i] = lam;
+  // delta reads position and lambda of a neighbour with one 16-byte gather
+  d.predLam[i] = make_float4(pi.x, pi.y, pi.z, lam);
 }
 
 __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
-  const float4* __restrict__ pred = d.pred[L ^ (it & 1)];
   float4* __restrict__ predOut = d.pred[L ^ ((it + 1) & 1)];
   const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
   const uint32_t* __restrict__ bcs = d.bcellStart + P.cOff;
-  const float* __restrict__ lambda = d.lambda;
+  // lambda's (position, lambda) of this iteration: the positions of pred[L ^ (it & 1)]
+  const float4* __restrict__ pl = d.predLam;
   const uint32_t cap = d.cap;
-  const F3 pi = xyz(__ldg(&pred[i]));
-  const float li_ = __ldg(&lambda[i]);
+  const float4 self = __ldg(&pl[i]);
+  const F3 pi = xyz(self);
+  const float li_ = self.w;
   const uint32_t count = __ldg(&d.nbCount[i]);  // lambda's list for these positions
   F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
   float nc = 1.0f;
-  auto fluid = [&](uint32_t j) {
-    const F3 rij = sub3(pi, xyz(__ldg(&pred[j])));
+  auto fluid = [&](uint32_t j, float4 q) {
+    const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
     const float rr = sqrtf(r2);
@@ -123,12 +126,12 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     const float ratio = P.poly6 * t * t * t * P.sCorrWq;
     const float r2r = ratio * ratio;
     const float sc = -P.sCorrK * r2r * r2r;
-    const float coef = (li_ + __ldg(&lambda[j]) + sc) * s;
+    const float coef = (li_ + q.w + sc) * s;
     dsum = fma3(coef, rij, dsum);
     nc += 1.0f;
   };
-  auto bound = [&](uint32_t k) {
-    const F3 rij = sub3(pi, xyz(__ldg(&d.bpos[k])));
+  auto bound = [&](uint32_t k, float4 q) {
+    const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float rr = sqrtf(r2);
@@ -137,10 +140,10 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     dB = fma3(coef, rij, dB);
   };
   if (count != kListOverflow) {
-    walk_list(d.nbList, cap, i, count, fluid, bound);
+    walk_list(d.nbList, cap, i, count, pl, d.bpos, fluid, bound);
   } else {
     const RowWalk w(P, pi);
-    walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
+    walk_direct<true>(P, w, pi, pl, cs, bcs, d.bpos, fluid, bound);
   }
   const F3 dd = {fmaf(dB.x, P.invRho0, dsum.x * P.volume), fmaf(dB.y, P.invRho0, dsum.y * P.volume),
                  fmaf(dB.z, P.invRho0, dsum.z * P.volume)};

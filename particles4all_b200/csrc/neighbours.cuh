@@ -242,31 +242,48 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
   return V * 1.00001f <= P.skinHalf;
 }
 
-// Phase 2 over a list of `count` entries: fluid(j) for a fluid entry, bound(k) for
-// a boundary sample. The next entry is loaded while the current one is processed.
+// Phase 2 over a list of `count` entries: fluid(j, q) for a fluid entry with
+// q = fsrc[j], bound(k, q) for a boundary sample with q = bsrc[k] (bsrc may be
+// null when the pass skips boundary samples: q is then zero). The walk is software
+// pipelined two entries deep: while entry k is processed, the gather of entry k+1
+// and the list load of entry k+2 are already in flight, so the latency of the
+// dependent list-then-gather chain overlaps the arithmetic of the current pair.
 template <class FFluid, class FBound>
 __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
-                                          uint32_t count, FFluid&& fluid, FBound&& bound) {
+                                          uint32_t count, const float4* __restrict__ fsrc,
+                                          const float4* __restrict__ bsrc, FFluid&& fluid, FBound&& bound) {
   count &= kCountMask;
   if (count == 0u) return;
-  uint32_t e = __ldg(&list[i]);
+  auto fetch = [&](uint32_t e) {
+    if (!(e & kBoundTag)) return __ldg(&fsrc[e]);
+    return bsrc ? __ldg(&bsrc[e & ~kBoundTag]) : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  uint32_t e0 = __ldg(&list[i]);
+  float4 q0 = fetch(e0);
+  uint32_t e1 = count > 1u ? __ldg(&list[(size_t)cap + i]) : 0u;
   for (uint32_t k = 1; k <= count; k++) {
-    const uint32_t cur = e;
-    if (k < count) e = __ldg(&list[(size_t)k * cap + i]);
+    const uint32_t cur = e0;
+    const float4 qc = q0;
+    if (k < count) {
+      e0 = e1;
+      q0 = fetch(e1);
+      if (k + 1 < count) e1 = __ldg(&list[(size_t)(k + 1) * cap + i]);
+    }
     if (cur & kBoundTag) {
-      bound(cur & ~kBoundTag);
+      bound(cur & ~kBoundTag, qc);
     } else {
-      fluid(cur);
+      fluid(cur, qc);
     }
   }
 }
 
 // The reference's direct loop (particles whose list overflowed): every candidate
 // j of the nine rows with r^2 < h^2 (j == i included; the passes skip it), then,
-// when B, the row's boundary samples with 1e-12 <= r^2 < h^2.
+// when B, the row's boundary samples with 1e-12 <= r^2 < h^2. fsrc holds the
+// candidate positions in .xyz (and whatever the pass keeps in .w).
 template <bool B, class FFluid, class FBound>
 __device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w, F3 pi,
-                                            const float4* __restrict__ pred, const uint32_t* __restrict__ cs,
+                                            const float4* __restrict__ fsrc, const uint32_t* __restrict__ cs,
                                             const uint32_t* __restrict__ bcs, const float4* __restrict__ bpos,
                                             FFluid&& fluid, FBound&& bound) {
 #pragma unroll 1
@@ -276,31 +293,34 @@ __device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w
     const uint32_t b = __ldg(&cs[rb + w.x0]);
     const uint32_t e = min(__ldg(&cs[rb + w.x1 + 1]), P.pEnd);
     for (uint32_t j = b; j < e; j++) {
-      const F3 d = sub3(pi, xyz(__ldg(&pred[j])));
-      if (dot3(d, d) < P.h2) fluid(j);
+      const float4 q = __ldg(&fsrc[j]);
+      const F3 d = sub3(pi, xyz(q));
+      if (dot3(d, d) < P.h2) fluid(j, q);
     }
     if constexpr (B) {
       if (P.nBoundary > 0u) {
         const uint32_t bb = __ldg(&bcs[rb + w.x0]), be = __ldg(&bcs[rb + w.x1 + 1]);
         for (uint32_t k = bb; k < be; k++) {
-          const F3 d = sub3(pi, xyz(__ldg(&bpos[k])));
+          const float4 q = __ldg(&bpos[k]);
+          const F3 d = sub3(pi, xyz(q));
           const float r2 = dot3(d, d);
-          if (r2 < P.h2 && r2 >= 1.0e-12f) bound(k);
+          if (r2 < P.h2 && r2 >= 1.0e-12f) bound(k, q);
         }
       }
     }
   }
 }
 
-// Fluid-only passes: the list walk, or the direct loop for an overflowed list.
+// Fluid-only passes: the list walk (boundary samples in a reused list skipped), or
+// the direct loop for an overflowed list.
 template <class FFluid>
 __device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
                                                 const float4* __restrict__ pred,
                                                 const uint32_t* __restrict__ cs, const uint32_t* __restrict__ list,
                                                 uint32_t cap, uint32_t count, FFluid&& fluid) {
-  auto none = [](uint32_t) {};
+  auto none = [](uint32_t, float4) {};
   if (count != kListOverflow) {
-    walk_list(list, cap, i, count, fluid, none);
+    walk_list(list, cap, i, count, pred, nullptr, fluid, none);
   } else {
     walk_direct<false>(P, w, pi, pred, cs, nullptr, nullptr, fluid, none);
   }

@@ -222,6 +222,7 @@ struct DevScene {
                         // after each iteration
   uint32_t cellStride;  // cells per cellDisp slot
   float4* nbRef;        // [cap] positions at the start of the substep's iterations
+  float4* predLam;      // [cap] (position, lambda) written by lambda for the delta of the same iteration
   uint32_t cap;         // particle capacity (stride of nbList)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };
@@ -347,6 +348,14 @@ void launch_resize(uint32_t n, float4* pos, const float oldSize[3], const float 
                    const float clampMin[3], const float clampMax[3], cudaStream_t st);
 void launch_aniso(const AnisoParams& A, const float4* pos, const uint32_t* cellStart,
                   float4* smoothPos, float4* g, cudaStream_t st, int variant = -1);
+// One hose layer appended at index `first` (kernels_hose.cu).
+struct HoseEmit {
+  float nozzle[3];
+  float spacing, centre, jitter, speed, rho0;
+  uint32_t k, count, first, seed;
+  uint64_t emission;
+};
+void launch_hose_emit(const HoseEmit& H, const DevScene& d, int parity, int predParity, cudaStream_t st);
 
 
 // ---- surface mesh (kernels_mesh.cu) ----

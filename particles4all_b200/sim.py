@@ -86,6 +86,15 @@ class Sim:
               self._h, "appendFluid")
         return added.value
 
+    def hoseEmit(self, hose):
+        """One layer of the fixed-rate hose (configs.Hose) emitted on the device at
+        the hose's next emission index (p4a_hose_emit): no host copy, no wait."""
+        added = C.c_int32()
+        check(self._L.p4a_hose_emit(self._h, C.byref(hose.c_struct()), hose.emission, C.byref(added)),
+              self._h, "hoseEmit")
+        hose.advance(added.value)
+        return added.value
+
     def applyRayImpulse(self, origin, direction, impulse, radius, speedLimit):
         o, d, im = (np.asarray(x, np.float64).reshape(3) for x in (origin, direction, impulse))
         check(self._L.p4a_apply_ray_impulse(self._h, o.ctypes.data, d.ctypes.data, im.ctypes.data,

@@ -27,8 +27,7 @@ def run(params, scene, frames):
     box = np.array(params["box"])
     for _ in range(frames):
         n0 = s.info()["n"]
-        pos, vel = hose.emit()
-        added = s.appendFluid(pos, vel) if pos is not None else 0
+        added = s.hoseEmit(hose)
         s.step(1 / 60)
         info = s.info()
         n, c = info["n"], info["n_cells"]

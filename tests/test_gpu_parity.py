@@ -372,3 +372,31 @@ def test_thousand_steps_statistics(workload):
     assert g.get_stats()["raw"] == o.stats()["raw"]
     compare(g, o)
     g.close()
+
+
+def test_device_hose_layers_match_the_host_restatement():
+    """p4a_hose_emit writes each layer on the device from its emission index: the
+    appended positions, velocities and the appendFluid fields (pred = pos, density
+    rho0, zero lambda / body / rest) must equal the host restatement bit for bit,
+    over several emissions and up to the capacity limit."""
+    params, scene = configs.dam_break_32k(side=12)
+    scene = dict(scene, pour_budget=5000)
+    g, o = pair(params, scene)
+    hg, ho = (configs.Hose(params["box"], params["spacing"], per_step=2048, speed=3.0, limit=5000)
+              for _ in range(2))
+    for k in range(4):
+        n0 = g.info()["n"]
+        pos, vel = ho.emit()
+        added_o = 0 if pos is None else o.appendFluid(pos, vel)
+        added_g = g.hoseEmit(hg)
+        assert added_g == added_o == [2048, 2048, 904, 0][k]
+        n = g.info()["n"]
+        assert n == n0 + added_g
+        if added_g:
+            assert np.array_equal(g.read("pos")[n0:n, :3], pos)
+            assert np.all(g.read("pos")[n0:n, 3] == 1.0)
+            assert np.array_equal(g.read("vel")[n0:n, :3], vel)
+        compare(g, o, names=PARTICLE_BUFS + ("density", "lambda_"))
+        g.step(1 / 60)
+        o.step(1 / 60)
+        compare(g, o, h=1.0)
