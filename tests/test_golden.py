@@ -62,3 +62,158 @@ def test_gpu_against_golden(built, case):
         s.step((1 / 60) / p["substeps"])
     check(s.read, case, g, p)
     s.close()
+
+
+# ---- the ops fixtures (tests/golden/ops_small.npz) -------------------------------
+# Every scene here is the float64 transcription's own (tests/scene_f64.py), handed
+# to the simulation as an explicit scene, so neither scene builder under test feeds
+# the comparison.
+
+OPS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ops_small.npz")
+OPS_CASES = ["aniso", "stats", "impulse", "drag", "resize", "append"]
+
+
+class _View:
+    """The same calls on the oracle (buffer) and on the library (read)."""
+
+    def __init__(self, sim, gpu):
+        self.sim, self.gpu = sim, gpu
+
+    def get(self, name):
+        return self.sim.read(name) if self.gpu else self.sim.buffer(name)
+
+    def raw(self):
+        return self.sim.get_stats()["raw"] if self.gpu else self.sim.stats()["raw"]
+
+    def __getattr__(self, k):
+        return getattr(self.sim, k)
+
+
+def _scene(p, budget=0):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from scene_f64 import build_scene_f64
+    sc = build_scene_f64(p)
+    sc["pour_budget"] = budget
+    return sc
+
+
+def _close(v, want, what, h):
+    n = len(want[0])
+    assert np.max(np.abs(v.get("pos")[:n, :3] - want[0])) < 1e-5 * h, what
+    assert np.allclose(v.get("vel")[:n, :3], want[1], rtol=1e-3, atol=1e-4), what
+
+
+def run_ops_case(make, case):
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_golden as mg
+    g = np.load(OPS)
+    dt = (1 / 60) / 2
+    if case == "aniso":
+        p = mg.case_params("bodies")
+        v = make(p, _scene(p))
+        n = v.info()["n"]
+        h = 2 * p["spacing"]
+        assert np.array_equal(v.get("pos")[:n, :3], g["aniso_reset_pos"][:, :3])
+        assert np.array_equal(v.get("cellStart")[:len(g["aniso_cs"])], g["aniso_cs"])
+        for name in ("reset", "moved"):
+            v.write("pos", g[f"aniso_{name}_pos"])
+            v.aniso(mg.ANISO)
+            sm = v.get("smoothPos")[:n, :3]
+            G = v.get("aniso")[: 2 * n].reshape(n, 8)
+            want = g[f"aniso_{name}_G"]
+            assert np.max(np.abs(sm - g[f"aniso_{name}_smooth"])) < 1e-5 * h, name
+            scale = np.abs(want[:, :6]).max(1)
+            assert np.max(np.abs(G[:, :6] - want[:, :6]).max(1) / scale) < 1e-4, name
+            assert np.max(np.abs(G[:, 6] / want[:, 6] - 1)) < 1e-4, name
+            assert np.array_equal(G[:, 7], want[:, 7].astype(np.float32)), name  # neighbour counts
+        return
+    p = mg.case_params("fluid")
+    h = 2 * p["spacing"]
+    if case == "stats":
+        v = make(p, _scene(p))
+        v.step(1 / 60)
+        raw = np.array(v.raw()[:4], np.int64)
+        want = g["stats_raw"]
+        assert np.all(np.abs(raw - want) <= 2 + 2e-5 * want), (raw, want)
+    elif case == "impulse":
+        v = make(p, _scene(p))
+        n = v.info()["n"]
+        v.write("vel", g["impulse_vel_in"])
+        v.applyRayImpulse(*mg.IMPULSE)
+        assert np.allclose(v.get("vel")[:n, :3], g["impulse_vel"], rtol=1e-5, atol=1e-6)
+        v.step(dt)
+        _close(v, (g["impulse_step_pos"], g["impulse_step_vel"]), "impulse then substep", h)
+    elif case == "drag":
+        pb = mg.case_params("bodies")
+        v = make(pb, _scene(pb))
+        v.holdBody(*mg.HOLD)
+        v.step(1 / 60)
+        _close(v, (g["drag_pos"], g["drag_vel"]), "drag", h)
+        assert np.allclose(v.get("bodyCentre")[:1, :3], g["drag_centre"], atol=1e-5 * h)
+    elif case == "resize":
+        v = make(p, _scene(p))
+        v.step(dt)
+        v.resizeBox(mg.RESIZED)
+        v.step(dt)
+        _close(v, (g["resize_pos"], g["resize_vel"]), "resize", h)
+    elif case == "append":
+        v = make(p, _scene(p, mg.APPEND_BUDGET))
+        v.step(dt)
+        lp, lv = mg.appended_layer()
+        assert v.appendFluid(lp, lv) == 49
+        v.step(dt)
+        assert v.info()["n"] == len(g["append_pos"])
+        _close(v, (g["append_pos"], g["append_vel"]), "append", h)
+
+
+@pytest.mark.parametrize("case", OPS_CASES)
+def test_oracle_against_ops_golden(built, case):
+    def make(p, sc):
+        o = oracle.OracleSim()
+        o.reset_scene(p, sc)
+        return _View(o, False)
+    run_ops_case(make, case)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", OPS_CASES)
+def test_gpu_against_ops_golden(built, case):
+    if not _lib.device_available():
+        pytest.fail("libp4a cannot use GPU 0")
+
+    def make(p, sc):
+        s = Sim()
+        s.reset_scene(p, sc)
+        return _View(s, True)
+    run_ops_case(make, case)
+
+
+def test_scene_transcription_matches_both_scene_builders(built):
+    """The float64 buildScene transcription that feeds the fixtures equals the
+    oracle's scene builder and the library's (p4a_build_scene) bit for bit: float32
+    positions, rest offsets and phases, body centres and densities, and the
+    doubles mass and denomRest; and the boundary samples and psi."""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from scene_f64 import build_scene_f64
+    from test_scene import product_scene
+    from particles4all_b200.params import default_params
+    cases = [case_params(c) for c in CASES]
+    p = default_params("small")
+    p.update({"bodies": ["sphere:0.5", "torus:0.8", "box:1.4"], "bodySize": 0.04, "targetParticleCount": 600,
+              "box": [0.4, 0.3, 0.25]})
+    cases.append(p)
+    for p in cases:
+        a, b, c = build_scene_f64(p), oracle.build_scene(p), product_scene(p)
+        for other in (b, c):
+            assert a["n"] == other["n"] and a["n_bodies"] == other["n_bodies"]
+            for k in ("pos", "rest", "phase"):
+                assert np.array_equal(a[k], other[k]), k
+            assert a["mass"] == other["mass"] and a["denom_rest"] == other["denom_rest"]
+            nb = a["n_bodies"]
+            assert np.array_equal(a["body_centre"], other["body_centre"][:nb])
+            assert np.array_equal(a["body_density"], other["body_density"][:nb])
+        bp, bpsi = oracle.boundary(p, p["spacing"], 2 * p["spacing"])
+        assert np.array_equal(bp.astype(np.float64), a["boundary_pts"]) and np.array_equal(bpsi, a["boundary_psi"])

@@ -171,8 +171,51 @@ class Transcription:
             pred[idx] = self.centre[b] + self.rest[idx] @ R.T
         return pred
 
+    # ---- interactive calls (src/sim.js:658-809) ----
+    def append(self, pos3, vel3):
+        """appendFluid: the layer (float32 values) at the end, body 0, rest 0."""
+        k = len(pos3)
+        self.pos = np.vstack([self.pos, np.asarray(pos3, np.float32).astype(float)])
+        self.vel = np.vstack([self.vel, np.asarray(vel3, np.float32).astype(float)])
+        self.rest = np.vstack([self.rest, np.zeros((k, 3))])
+        self.body = np.concatenate([self.body, np.zeros(k, int)])
+
+    def hold(self, body1, target, rate, limit):
+        """holdBody: the drag applied before every substep's predict (src/wgsl.js:187-214)."""
+        self.held = (int(body1), np.array(target, float), float(rate), float(limit))
+
+    def resize(self, new_box, boundary):
+        """resizeBox: positions remapped and clamped (resize_f64), then the grid and the
+        boundary samples of the new box (boundary = its (pts, psi))."""
+        from ops_f64 import resize_f64
+        self.pos = resize_f64(self.pos, self.box, new_box, self.d)
+        self.box = np.array(new_box, float)
+        self.p = dict(self.p, box=list(new_box))
+        self.dim = np.maximum(1, np.floor(self.box / self.h)).astype(int)
+        self.C = int(np.prod(self.dim))
+        self.cmax = self.box - 0.5 * self.d
+        bpts, bpsi = boundary
+        bk = self.key(bpts.astype(np.float32).astype(float))
+        order = np.argsort(bk, kind="stable")
+        self.bpos, self.bpsi = bpts[order].astype(np.float32).astype(float), bpsi[order].astype(float)
+        self.bstart = np.searchsorted(bk[order], np.arange(self.C + 1))
+
+    def drag(self, dt):
+        held = getattr(self, "held", None)
+        if not held or held[0] < 1 or held[0] > self.nb:
+            return
+        b, goal, rate, limit = held
+        blend = 1 - math.exp(-max(dt, 0) / 0.02)
+        want = (goal - self.centre[b - 1]) * rate
+        sp = math.sqrt(want @ want)
+        if sp > limit:
+            want = want * (limit / sp)
+        idx = self.body == b
+        self.vel[idx] = self.vel[idx] + (want - self.vel[idx]) * blend
+
     def substep(self, dt):
         g = self.p["gravity"]
+        self.drag(dt)
         self.vel = self.vel + dt * np.array([0.0, -g, 0.0])
         pred = self.sort(self.pos + dt * self.vel)
         if self.nb:
