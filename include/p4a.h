@@ -609,6 +609,11 @@ int p4a_server_get_stats(p4a_server* s, p4a_server_stats* out);
  * >= the count, else variant 0. The table is process-wide.
  */
 enum { P4A_KERNEL_LAMBDA = 0, P4A_KERNEL_DELTA = 1, P4A_KERNEL_NORMALS = 2, P4A_KERNEL_ANISO = 3 };
+/* The batched launches (p4a_batch_step) of lambda, delta and xsph+normals have
+ * tables of their own, keyed by the frame's total particles; while one is empty
+ * the batched launch uses its plain kernel's table. Same shapes as the plain
+ * kernel (p4a_kernel_shapes). */
+enum { P4A_KERNEL_LAMBDA_BATCHED = 4, P4A_KERNEL_DELTA_BATCHED = 5, P4A_KERNEL_NORMALS_BATCHED = 6 };
 int p4a_kernel_shapes(int32_t kernel, int32_t* threads, int32_t* min_blocks, int32_t max,
                       int32_t* count);
 int p4a_tune_set(int32_t kernel, int64_t max_particles, int32_t variant);

@@ -10,6 +10,13 @@ from the library's per-kernel CUDA events. The fastest shape per (kernel,
 bucket) goes into the library's table (p4a_tune_set) and into tuning.json next
 to this file, which the library applies when it is loaded.
 
+The batched launches of lambda, delta and xsph+normals (p4a_batch_step) have tables
+of their own, keyed by the frame's total particles: their register budget differs
+from the plain launches' (each warp also carries its work-item state). For each
+batched bucket this admits a seeded mix of scenes (configs.batched_mix with that
+many scenes) into one Batch and times each shape on whole batched frames with the
+batch's per-kernel events.
+
     python -m particles4all_b200.autotune            # on the GPU: measure, write tuning.json
 """
 import argparse
@@ -23,8 +30,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_PATH = os.path.join(HERE, "tuning.json")
 
 KERNELS = {"lambda": 0, "delta": 1, "xsph_normals": 2, "aniso": 3}
+BATCHED = {"lambda_batched": 4, "delta_batched": 5, "xsph_normals_batched": 6}
+PROFILE_NAME = {"lambda_batched": "lambda", "delta_batched": "delta", "xsph_normals_batched": "xsph_normals"}
 # bucket upper bounds (particles) and the scene size measured for each
 BUCKETS = [(24_000, 12_000), (96_000, 48_000), (384_000, 192_000), (1_536_000, 768_000), (1 << 40, 2_000_000)]
+# batched buckets: upper bound of a frame's total particles and the scene count of
+# the seeded mix measured for it (96 scenes: about 6.0 M particles)
+BATCH_BUCKETS = [(3_000_000, 24), (1 << 40, 96)]
 
 
 def shapes(L, kernel):
@@ -41,7 +53,7 @@ def apply(table, L=None):
         from ._lib import lib
         L = lib()
     for name, buckets in table.get("kernels", {}).items():
-        k = KERNELS[name]
+        k = KERNELS[name] if name in KERNELS else BATCHED[name]
         L.p4a_tune_clear(k)
         for bound, v in buckets:
             L.p4a_tune_set(k, int(bound), int(v))
@@ -83,7 +95,56 @@ def measure(sim, aniso, frames=6, warmup=2):
     return {k: ms / max(1, n) for k, (ms, n) in prof.items()}
 
 
-def tune(buckets=BUCKETS, frames=6, path=DEFAULT_PATH, log=print):
+def _mix_batch(scenes):
+    from . import Batch, configs
+    from .batch import arena_sizes
+    mix = configs.batched_mix(count=scenes)
+    b = Batch(**arena_sizes(mix))
+    ids = [b.add_scene(p, sc) for p, sc in mix]
+    return b, ids, sum(sc["pos"].shape[0] for _, sc in mix)
+
+
+def measure_batch(b, ids, frames=4, warmup=2):
+    """Device ms per launch of every batched kernel over `frames` frames."""
+    for _ in range(warmup):
+        b.step(ids, 1 / 60)
+    b.synchronize()
+    b.profile(True)
+    b.profile_reset()
+    for _ in range(frames):
+        b.step(ids, 1 / 60)
+    b.synchronize()
+    prof = b.profile_read()
+    b.profile(False)
+    return {k: ms / max(1, n) for k, (ms, n) in prof.items()}
+
+
+def tune_batched(result, L, buckets=BATCH_BUCKETS, frames=4, log=print):
+    """Fills result["kernels"] / ["measured"] for the batched tables."""
+    for name in BATCHED:
+        result["kernels"][name] = []
+        result["shapes"][name] = shapes(L, BATCHED[name])
+    for bound, scenes in buckets:
+        b, ids, total = _mix_batch(scenes)
+        per = {}
+        for name, k in BATCHED.items():
+            times = []
+            for v in range(len(result["shapes"][name])):
+                L.p4a_tune_clear(k)
+                L.p4a_tune_set(k, 1 << 40, v)
+                times.append(measure_batch(b, ids, frames)[PROFILE_NAME[name]])
+            best = min(range(len(times)), key=times.__getitem__)
+            L.p4a_tune_clear(k)
+            L.p4a_tune_set(k, 1 << 40, best)
+            per[name] = {"ms_per_launch": [round(x, 5) for x in times], "best": best}
+            log(f"batch {total:>9} {name:21s} " + " ".join(f"{x * 1e3:7.1f}" for x in times) + f"  -> {best}")
+        b.close()
+        result["measured"][f"batch_{total}"] = per
+        for name in BATCHED:
+            result["kernels"][name].append([bound, per[name]["best"]])
+
+
+def tune(buckets=BUCKETS, frames=6, path=DEFAULT_PATH, log=print, batch_buckets=BATCH_BUCKETS):
     from ._lib import lib
     L = lib()
     L.p4a_tune_clear(-1)
@@ -111,6 +172,10 @@ def tune(buckets=BUCKETS, frames=6, path=DEFAULT_PATH, log=print):
         result["measured"][str(real_n)] = per
         for name in KERNELS:
             result["kernels"][name].append([bound, per[name]["best"]])
+    if batch_buckets:
+        L.p4a_tune_clear(-1)
+        apply(result, L)  # the plain tables as measured, then the batched ones on top
+        tune_batched(result, L, batch_buckets, log=log)
     result["seconds"] = round(time.time() - t0, 1)
     L.p4a_tune_clear(-1)
     apply(result, L)
@@ -125,9 +190,10 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=6)
     ap.add_argument("--out", default=DEFAULT_PATH)
     ap.add_argument("--max-n", type=int, default=None, help="skip buckets whose scene is larger")
+    ap.add_argument("--no-batched", action="store_true", help="tune the plain launches only")
     a = ap.parse_args(argv)
     b = [x for x in BUCKETS if a.max_n is None or x[1] <= a.max_n]
-    tune(b, a.frames, a.out)
+    tune(b, a.frames, a.out, batch_buckets=None if a.no_batched else BATCH_BUCKETS)
     return 0
 
 

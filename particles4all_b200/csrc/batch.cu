@@ -650,7 +650,7 @@ int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t 
   int64_t total = 0;
   for (int k = 0; k < count; k++) total += b->scenes[ids[k]].n;
   for (int k = 0; k < TK_COUNT; k++) {
-    F.variant[k] = tuned_variant(k, total);
+    F.variant[k] = tuned_variant_batched(k, total);
     F.shape.push_back(F.variant[k]);
   }
   F.shape.push_back(maxSub);

@@ -271,6 +271,11 @@ struct LaunchShape {
 };
 extern const LaunchShape kShapes[TK_COUNT][kVariants];
 int tuned_variant(int kernel, int64_t particles);
+// Tables 4..6 hold the batched launches of lambda, delta and xsph+normals (tuned on
+// batched frames: their register budget differs from the plain launches'); a
+// batched launch falls back to the plain table while its own is empty.
+constexpr int kTunedTables = 7;
+int tuned_variant_batched(int kernel, int64_t particles);
 
 void launch_lambda(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant = -1);
 void launch_delta(const SimParams& P, const DevScene& d, int it, cudaStream_t st, int variant = -1);

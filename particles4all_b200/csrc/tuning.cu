@@ -27,15 +27,28 @@ const LaunchShape kShapes[TK_COUNT][kVariants] = {
 
 namespace {
 std::mutex g_mu;
-std::vector<std::pair<int64_t, int>> g_table[TK_COUNT];  // (max particles, variant), ascending
+std::vector<std::pair<int64_t, int>> g_table[kTunedTables];  // (max particles, variant), ascending
+// the kernel whose launch shapes table k selects among
+int family(int k) { return k < TK_COUNT ? k : k - TK_COUNT; }
+int lookup(int table, int64_t particles) {
+  for (const auto& b : g_table[table])
+    if (particles <= b.first) return b.second;
+  return 0;
+}
 }  // namespace
 
 int tuned_variant(int kernel, int64_t particles) {
   if (kernel < 0 || kernel >= TK_COUNT) return 0;
   std::lock_guard<std::mutex> l(g_mu);
-  for (const auto& b : g_table[kernel])
-    if (particles <= b.first) return b.second;
-  return 0;
+  return lookup(kernel, particles);
+}
+
+int tuned_variant_batched(int kernel, int64_t particles) {
+  if (kernel < 0 || kernel >= TK_COUNT) return 0;
+  std::lock_guard<std::mutex> l(g_mu);
+  const int b = TK_COUNT + kernel;
+  if (b < kTunedTables && !g_table[b].empty()) return lookup(b, particles);
+  return lookup(kernel, particles);
 }
 
 }  // namespace p4a
@@ -45,18 +58,19 @@ using namespace p4a;
 extern "C" {
 
 int p4a_kernel_shapes(int32_t kernel, int32_t* threads, int32_t* min_blocks, int32_t max, int32_t* count) {
-  if (kernel < 0 || kernel >= TK_COUNT || !count || max < 0) return P4A_ERR_ARG;
+  if (kernel < 0 || kernel >= kTunedTables || !count || max < 0) return P4A_ERR_ARG;
   const int32_t c = std::min<int32_t>(max, kVariants);
+  const int f = family(kernel);
   for (int32_t v = 0; v < c; v++) {
-    if (threads) threads[v] = kShapes[kernel][v].threads;
-    if (min_blocks) min_blocks[v] = kShapes[kernel][v].minBlocks;
+    if (threads) threads[v] = kShapes[f][v].threads;
+    if (min_blocks) min_blocks[v] = kShapes[f][v].minBlocks;
   }
   *count = kVariants;
   return P4A_OK;
 }
 
 int p4a_tune_set(int32_t kernel, int64_t max_particles, int32_t variant) {
-  if (kernel < 0 || kernel >= TK_COUNT || variant < 0 || variant >= kVariants || max_particles < 0)
+  if (kernel < 0 || kernel >= kTunedTables || variant < 0 || variant >= kVariants || max_particles < 0)
     return P4A_ERR_ARG;
   std::lock_guard<std::mutex> l(g_mu);
   auto& t = g_table[kernel];
@@ -68,16 +82,16 @@ int p4a_tune_set(int32_t kernel, int64_t max_particles, int32_t variant) {
 }
 
 int p4a_tune_clear(int32_t kernel) {
-  if (kernel < -1 || kernel >= TK_COUNT) return P4A_ERR_ARG;
+  if (kernel < -1 || kernel >= kTunedTables) return P4A_ERR_ARG;
   std::lock_guard<std::mutex> l(g_mu);
-  for (int k = 0; k < TK_COUNT; k++)
+  for (int k = 0; k < kTunedTables; k++)
     if (kernel < 0 || kernel == k) g_table[k].clear();
   return P4A_OK;
 }
 
 int p4a_tune_get(int32_t kernel, int64_t particles, int32_t* variant) {
-  if (kernel < 0 || kernel >= TK_COUNT || !variant) return P4A_ERR_ARG;
-  *variant = tuned_variant(kernel, particles);
+  if (kernel < 0 || kernel >= kTunedTables || !variant) return P4A_ERR_ARG;
+  *variant = kernel < TK_COUNT ? tuned_variant(kernel, particles) : tuned_variant_batched(family(kernel), particles);
   return P4A_OK;
 }
 

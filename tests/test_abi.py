@@ -164,6 +164,31 @@ def test_tuning_table_host_side(built, tmp_path):
         autotune.load(L=L)
 
 
+
+def test_batched_tuning_tables_fall_back_to_the_plain_ones(built):
+    """The batched launches' tables (kernels 4-6) are their own; while one is empty,
+    a batched launch of that kernel uses the plain kernel's table."""
+    L = _lib.lib()
+    v = C.c_int32()
+    t = (C.c_int32 * 8)()
+    m = (C.c_int32 * 8)()
+    cnt = C.c_int32()
+    assert L.p4a_kernel_shapes(4, t, m, 8, C.byref(cnt)) == 0 and cnt.value == 6
+    assert L.p4a_kernel_shapes(7, t, m, 8, C.byref(cnt)) == _abi.P4A_ERR_ARG
+    try:
+        L.p4a_tune_clear(-1)
+        assert L.p4a_tune_set(0, 1 << 40, 2) == 0
+        assert L.p4a_tune_get(4, 5_000_000, C.byref(v)) == 0 and v.value == 2  # falls back to lambda's
+        assert L.p4a_tune_set(4, 1 << 40, 3) == 0
+        assert L.p4a_tune_get(4, 5_000_000, C.byref(v)) == 0 and v.value == 3
+        assert L.p4a_tune_get(0, 5_000_000, C.byref(v)) == 0 and v.value == 2  # plain table unchanged
+        L.p4a_tune_clear(4)
+        assert L.p4a_tune_get(4, 5_000_000, C.byref(v)) == 0 and v.value == 2
+    finally:
+        L.p4a_tune_clear(-1)
+        from particles4all_b200 import autotune
+        autotune.load()
+
 def test_batch_footprint_sizes_server_arenas(built):
     """p4a_batch_footprint counts the arenas p4a_batch_create would allocate (no
     device needed), and the serving loop's arena sizing stays within its budget."""
