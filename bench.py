@@ -71,6 +71,8 @@ def parse_args():
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
                          "frames and exit; for profiling the two forms")
     ap.add_argument("--mix-frames", type=int, default=10)
+    ap.add_argument("--mix-scenes", type=int, default=96,
+                    help="with --only-mix: the first N scenes of the seeded mix (a smaller case for profiling)")
     ap.add_argument("--serve-seconds", type=float, default=15.0,
                     help="length of each served-workload run (batched, then plain); 0 skips it")
     ap.add_argument("--serve-budget-gb", type=float, default=160.0)
@@ -293,11 +295,12 @@ def mix_scene_flags(mix):
              int((sc["phase"][:, 0] > 0).sum())) for p, sc in mix]
 
 
-def only_mix(form, frames):
-    """The mix stepped in one form only: admission (or reset) then `frames` frames."""
+def only_mix(form, frames, scenes=96):
+    """The mix (its first `scenes` scenes) stepped in one form only: admission (or
+    reset) then `frames` frames."""
     import torch
     from particles4all_b200 import Batch, Sim, configs
-    mix = configs.batched_mix()
+    mix = configs.batched_mix(count=scenes)
     stream = torch.cuda.Stream()
     t0 = time.perf_counter()
     if form == "batched":
@@ -961,7 +964,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.only_mix:
-        return only_mix(args.only_mix, args.mix_frames)
+        return only_mix(args.only_mix, args.mix_frames, args.mix_scenes)
     if args.only_render:
         return only_render(args)
     if args.workload == MIX:

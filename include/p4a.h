@@ -214,7 +214,7 @@ int p4a_step(p4a_sim* sim, double frame_dt, int32_t* substeps_out);
 int p4a_append_fluid(p4a_sim* sim, const float* pos3, const float* vel3, int32_t count,
                      int32_t* added);
 /* The layered hose of pourStep (src/main.js:106-160) at a fixed rate, emitted on
- * the device: one layer of min(per_step, cap - n) particles appended at index n
+ * the device: the first min(count, cap - n) slots of one layer appended at index n
  * with the appendFluid semantics (src/sim.js:774-809: live pos/vel and the pred
  * parity written, density rho0, zero lambda/corr/normal/body/rest), computed by a
  * kernel from its emission index, so nothing crosses from the host and the call
@@ -228,8 +228,10 @@ typedef struct p4a_hose {
   float spacing;
   float jitter;
   float speed;
-  int32_t per_step;
+  int32_t per_step;  /* slots of a full layer; sets the lattice side k          */
   uint32_t seed;
+  int32_t count;     /* slots of this emission, 0..per_step (the first ones of  */
+                     /* the layer); -1 = per_step. Capped by cap - n as well.   */
 } p4a_hose;
 int p4a_hose_emit(p4a_sim* sim, const p4a_hose* hose, int64_t emission, int32_t* added);
 /* Sim.applyRayImpulse(origin, dir, impulse, radius, speedLimit) (src/sim.js:658-676). */

@@ -131,7 +131,7 @@ class Grid(C.Structure):
 
 class Hose(C.Structure):
     _fields_ = [("nozzle", C.c_float * 3), ("spacing", C.c_float), ("jitter", C.c_float), ("speed", C.c_float),
-                ("per_step", C.c_int32), ("seed", C.c_uint32)]
+                ("per_step", C.c_int32), ("seed", C.c_uint32), ("count", C.c_int32)]
 
 
 class SceneCounts(C.Structure):

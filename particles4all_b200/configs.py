@@ -227,7 +227,8 @@ class Hose:
         for a in range(3):
             h.nozzle[a] = float(self.nozzle[a])
         h.spacing, h.jitter, h.speed = float(self.spacing), float(self.jitter), float(self.speed)
-        h.per_step = self.per_step if self.left is None else max(0, min(self.per_step, self.left))
+        h.per_step = self.per_step
+        h.count = self.per_step if self.left is None else max(0, min(self.per_step, self.left))
         h.seed = self.seed
         return h
 

@@ -904,7 +904,8 @@ int p4a_hose_emit(p4a_sim* s, const p4a_hose* hose, int64_t emission, int32_t* a
     return fail(s, P4A_ERR_ARG, "hose_emit: bad arguments");
   if (!s->ready) return fail(s, P4A_ERR_STATE, "hose_emit before reset");
   const int room = std::max(0, s->cap - s->n);
-  const int c = std::min(hose->per_step, room);
+  const int want = hose->count < 0 ? hose->per_step : std::min(hose->count, hose->per_step);
+  const int c = std::min(want, room);
   if (added) *added = std::max(0, c);
   if (c <= 0) return P4A_OK;
   cudaSetDevice(s->device);

@@ -96,9 +96,12 @@ __global__ void __launch_bounds__(kBlock) k_key_count(const __grid_constant__ Si
                                                       const __grid_constant__ DevScene d) {
   key_count_body(P, d, blockIdx.x * kBlock + threadIdx.x);
 }
+// The batched streaming passes take whole 256-particle tiles per claim (one atomic
+// per tile instead of one per 32-particle slice: their per-particle work is short,
+// so a cursor shared by every warp would serialise them).
 __global__ void __launch_bounds__(kBlock) k_key_count_b(const __grid_constant__ BatchWork w,
                                                         const __grid_constant__ DevScene d) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { key_count_body(P, d, li); });
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { key_count_body(P, d, t * kBlock + threadIdx.x); });
 }
 __global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimParams P,
                                                  const __grid_constant__ DevScene d) {
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(kBlock) k_fill(const __grid_constant__ SimPara
 }
 __global__ void __launch_bounds__(kBlock) k_fill_b(const __grid_constant__ BatchWork w,
                                                    const __grid_constant__ DevScene d) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { fill_body(P, d, li); });
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { fill_body(P, d, t * kBlock + threadIdx.x); });
 }
 __global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimParams P,
                                                     const __grid_constant__ DevScene d) {
@@ -114,11 +117,20 @@ __global__ void __launch_bounds__(kBlock) k_reorder(const __grid_constant__ SimP
 }
 __global__ void __launch_bounds__(kBlock) k_reorder_b(const __grid_constant__ BatchWork w,
                                                       const __grid_constant__ DevScene d) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { reorder_body(P, d, li); });
+  for_each_item(w, [&](const SimParams& P, uint32_t t, uint32_t) { reorder_body(P, d, t * kBlock + threadIdx.x); });
 }
 
 // Tile status word: epoch (30 bits) | flag (2 bits) | value (32 bits).
 constexpr unsigned long long kFlagAgg = 1ull, kFlagPrefix = 2ull;
+
+// A predecessor's status word, read at GPU scope every time (the word is published
+// with an atomic at L2; a load that may be served from the SM's L1 could keep
+// returning the stale word).
+__device__ __forceinline__ unsigned long long load_state(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ unsigned long long pack_state(uint32_t epoch, unsigned long long flag, uint32_t v) {
   return ((unsigned long long)epoch << 34) | (flag << 32) | (unsigned long long)v;
 }
@@ -167,33 +179,52 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
     }
     if (lane < kBlock / 32) s_warp[lane] = wi - wv;  // exclusive warp offsets
     const uint32_t aggregate = __shfl_sync(0xffffffffu, wi, kBlock / 32 - 1);
-    if (lane == 0) {
-      uint32_t exclusive = seed;
-      if (tile == firstTile) {
-        atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, seed + aggregate));
-      } else {
-        atomicExch(&state[tile], pack_state(epoch, kFlagAgg, aggregate));
-        exclusive = 0;
-        int j = tile - 1;
-        uint32_t spins = 0;
-        while (j >= firstTile) {
-          const unsigned long long w64 = *((volatile unsigned long long*)&state[j]);
-          const uint32_t we = (uint32_t)(w64 >> 34);
+    uint32_t exclusive = seed;
+    if (tile == firstTile) {
+      if (lane == 0) atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, seed + aggregate));
+    } else {
+      if (lane == 0) atomicExch(&state[tile], pack_state(epoch, kFlagAgg, aggregate));
+      // Warp-wide lookback: lane l reads the state of tile top - l, 32 predecessors
+      // per step. The nearest tile with an inclusive prefix ends the walk; every
+      // tile between it and this one must have published its aggregate first.
+      // Tiles before the segment's first count as a prefix of 0 (the first tile
+      // always publishes one, so the walk never passes it).
+      exclusive = 0;
+      int top = tile - 1;
+      uint32_t spins = 0;
+      while (true) {
+        const int t = top - lane;
+        bool ready = true, prefix = true;
+        uint32_t value = 0;
+        if (t >= firstTile) {
+          const unsigned long long w64 = load_state(&state[t]);
           const unsigned long long wf = (w64 >> 32) & 3ull;
-          if (we != epoch || wf == 0ull) {
-            if (++spins > spinLimit) {  // bounded wait: flag the error and stop looking
-              atomicOr(err, ERR_SCAN_TIMEOUT);
-              break;
-            }
-            __nanosleep(64);
-            continue;
-          }
-          exclusive += (uint32_t)w64;
-          if (wf == kFlagPrefix) break;
-          j--;
+          ready = (uint32_t)(w64 >> 34) == epoch && wf != 0ull;
+          prefix = ready && wf == kFlagPrefix;
+          value = (uint32_t)w64;
         }
-        atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, exclusive + aggregate));
+        const uint32_t prefixes = __ballot_sync(0xffffffffu, prefix);
+        const uint32_t waiting = __ballot_sync(0xffffffffu, !ready);
+        const int first = prefixes ? __ffs(prefixes) - 1 : 31;  // nearest prefix lane, or the window
+        const uint32_t span = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if (waiting & span) {
+          if (++spins > spinLimit) {  // bounded wait: flag the error and stop looking
+            if (lane == 0) atomicOr(err, ERR_SCAN_TIMEOUT);
+            break;
+          }
+          __nanosleep(64);
+          continue;
+        }
+        uint32_t part = lane <= first ? value : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        exclusive += part;
+        if (prefixes) break;
+        top -= 32;
       }
+      if (lane == 0) atomicExch(&state[tile], pack_state(epoch, kFlagPrefix, exclusive + aggregate));
+    }
+    if (lane == 0) {
       s_prefix = exclusive;
       if (lastOfSegment) cellStart[limit] = exclusive + aggregate;
     }

@@ -29,8 +29,11 @@
 
 namespace p4a {
 
-// Called by all 32 lanes of a warp (lanes past the scene's end only take part in the
+// Called by all 32 lanes of a warp. PF: whether the list walk runs the two-deep
+// prefetch pipeline (measured faster in the batched launches, slower in the plain
+// ones, whose register budget it squeezes; delta's walk always prefetches). (lanes past the scene's end only take part in the
 // warp's list builds).
+template <bool PF>
 __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& d, uint32_t li, int it) {
   const bool act = li < P.n;
   const uint32_t i = P.pOff + (act ? li : 0u);
@@ -83,7 +86,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     gradSum = fma3(s, rij, gradSum);
   };
   if (count != kListOverflow) {
-    walk_list(d.nbList, cap, i, count, pred, d.bpos, fluid, bound);
+    walk_list<PF>(d.nbList, cap, i, count, pred, d.bpos, fluid, bound);
   } else {
     walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
   }
@@ -170,12 +173,12 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda(const __grid_constant__ SimParams P,
                                                    const __grid_constant__ DevScene d, int it) {
-  lambda_body(P, d, blockIdx.x * TB + threadIdx.x, it);
+  lambda_body<false>(P, d, blockIdx.x * TB + threadIdx.x, it);
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_lambda_b(const __grid_constant__ BatchWork w,
                                                      const __grid_constant__ DevScene d, int it) {
-  for_each_slice(w, [&](const SimParams& P, uint32_t li) { lambda_body(P, d, li, it); });
+  for_each_slice(w, [&](const SimParams& P, uint32_t li) { lambda_body<true>(P, d, li, it); });
 }
 template <int TB, int MB>
 __global__ void __launch_bounds__(TB, MB) k_delta(const __grid_constant__ SimParams P,

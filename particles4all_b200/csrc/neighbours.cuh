@@ -244,35 +244,50 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
 
 // Phase 2 over a list of `count` entries: fluid(j, q) for a fluid entry with
 // q = fsrc[j], bound(k, q) for a boundary sample with q = bsrc[k] (bsrc may be
-// null when the pass skips boundary samples: q is then zero). The walk is software
+// null when the pass skips boundary samples). With PF the walk is software
 // pipelined two entries deep: while entry k is processed, the gather of entry k+1
 // and the list load of entry k+2 are already in flight, so the latency of the
 // dependent list-then-gather chain overlaps the arithmetic of the current pair.
-template <class FFluid, class FBound>
+// The gather address is chosen without a branch (a boundary entry of a pass
+// without boundary samples loads the particle's own fsrc[i], which is unused).
+template <bool PF = true, class FFluid, class FBound>
 __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
                                           uint32_t count, const float4* __restrict__ fsrc,
                                           const float4* __restrict__ bsrc, FFluid&& fluid, FBound&& bound) {
   count &= kCountMask;
   if (count == 0u) return;
   auto fetch = [&](uint32_t e) {
-    if (!(e & kBoundTag)) return __ldg(&fsrc[e]);
-    return bsrc ? __ldg(&bsrc[e & ~kBoundTag]) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const bool b = (e & kBoundTag) != 0u;
+    const float4* src = b && bsrc ? bsrc : fsrc;
+    const uint32_t idx = b ? (bsrc ? (e & ~kBoundTag) : i) : e;
+    return __ldg(src + idx);
+  };
+  auto visit = [&](uint32_t cur, float4 q) {
+    if (cur & kBoundTag) {
+      bound(cur & ~kBoundTag, q);
+    } else {
+      fluid(cur, q);
+    }
   };
   uint32_t e0 = __ldg(&list[i]);
-  float4 q0 = fetch(e0);
-  uint32_t e1 = count > 1u ? __ldg(&list[(size_t)cap + i]) : 0u;
-  for (uint32_t k = 1; k <= count; k++) {
-    const uint32_t cur = e0;
-    const float4 qc = q0;
-    if (k < count) {
-      e0 = e1;
-      q0 = fetch(e1);
-      if (k + 1 < count) e1 = __ldg(&list[(size_t)(k + 1) * cap + i]);
+  if constexpr (PF) {
+    float4 q0 = fetch(e0);
+    uint32_t e1 = count > 1u ? __ldg(&list[(size_t)cap + i]) : 0u;
+    for (uint32_t k = 1; k <= count; k++) {
+      const uint32_t cur = e0;
+      const float4 qc = q0;
+      if (k < count) {
+        e0 = e1;
+        q0 = fetch(e1);
+        if (k + 1 < count) e1 = __ldg(&list[(size_t)(k + 1) * cap + i]);
+      }
+      visit(cur, qc);
     }
-    if (cur & kBoundTag) {
-      bound(cur & ~kBoundTag, qc);
-    } else {
-      fluid(cur, qc);
+  } else {
+    for (uint32_t k = 1; k <= count; k++) {
+      const uint32_t cur = e0;
+      if (k < count) e0 = __ldg(&list[(size_t)k * cap + i]);
+      visit(cur, fetch(cur));
     }
   }
 }

@@ -40,4 +40,4 @@ def test_layer_lattice_jitter_and_limit():
     # a layer is a function of its emission index
     again = Hose([160.0, 96.0, 80.0], d, per_step=2048, speed=3.0).layer(1, 2048)[0]
     assert np.array_equal(again, p2)
-    assert h.c_struct().per_step == 0
+    assert h.c_struct().count == 0 and h.c_struct().per_step == 2048  # the lattice stays 46 x 46
