@@ -100,7 +100,6 @@ __device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const Dev
     const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
     F3 acc = {0.f, 0.f, 0.f};
     auto fluid = [&](uint32_t j, float4 q) {
-      if (j == i) return;
       const F3 rij = sub3(pi, xyz(q));
       const float r2 = dot3(rij, rij);
       if (r2 >= P.h2) return;  // in the skin of a reused list only
@@ -134,7 +133,6 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   d.nbCount[i] = count;
   F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
   auto fluid = [&](uint32_t j, float4 q) {
-    if (j == i) return;
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
@@ -174,7 +172,7 @@ __device__ __forceinline__ void tension_finalize_body(const SimParams& P, const 
     auto fluid = [&](uint32_t j, float4 q) {
       const F3 rij = sub3(pi, xyz(q));
       const float r2 = dot3(rij, rij);
-      if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
+      if (r2 >= P.h2 || r2 < 1.0e-12f) return;
       const float rr = sqrtf(r2);
       const float hrr = P.h - rr;
       const float k = hrr * hrr * hrr * rr * rr * rr;

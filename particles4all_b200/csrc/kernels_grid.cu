@@ -40,14 +40,7 @@ __device__ __forceinline__ void key_count_body(const SimParams& P, const DevScen
     const int leader = __ffs(peers) - 1;
     const uint32_t lt = peers & ((1u << lane) - 1u);
     uint32_t base = 0;
-    if (lane == leader) {
-      base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
-      // this substep's per-cell displacement slots start at zero for every occupied cell
-      if (d.cellDisp) {
-        const uint32_t slots = min(P.iters, (uint32_t)kDispSlots);
-        for (uint32_t t = 0; t < slots; t++) d.cellDisp[(size_t)t * d.cellStride + k] = 0.0f;
-      }
-    }
+    if (lane == leader) base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
     base = __shfl_sync(peers, base, leader);
     d.key[i] = k;
     d.rank[i] = base + (uint32_t)__popc(lt);
@@ -143,7 +136,8 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
                                           uint32_t* __restrict__ cellStart, long long cellBase,
                                           long long limit, int tile, int firstTile, uint32_t seed,
                                           bool lastOfSegment, unsigned long long* __restrict__ state,
-                                          uint32_t epoch, uint32_t* __restrict__ err, uint32_t spinLimit) {
+                                          uint32_t epoch, uint32_t* __restrict__ err, uint32_t spinLimit,
+                                          const DispClear& dc) {
   __shared__ uint32_t s_prefix;
   __shared__ uint32_t s_warp[kBlock / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -160,6 +154,15 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
   for (int j = 0; j < kScanItems; j++) {
     const long long idx = base + j;
     if (idx < limit) cellCount[idx] = 0u;
+  }
+  // this substep's per-cell displacement slots start at zero for every occupied cell
+  // (list reuse only: a slot left larger makes the bound looser, never wrong)
+  if (dc.disp) {
+    for (uint32_t t = 0; t < dc.slots; t++) {
+#pragma unroll
+      for (int j = 0; j < kScanItems; j++)
+        if (v[j] != 0u) dc.disp[(size_t)t * dc.stride + (size_t)(base + j)] = 0.0f;
+    }
   }
   uint32_t incl = sum;
 #pragma unroll
@@ -243,7 +246,8 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
                                                  uint32_t* __restrict__ cellStart, int nCells,
                                                  unsigned long long* __restrict__ state,
                                                  uint32_t* __restrict__ ticket, uint32_t epoch,
-                                                 int nTiles, uint32_t* __restrict__ err, uint32_t spinLimit) {
+                                                 int nTiles, uint32_t* __restrict__ err, uint32_t spinLimit,
+                                                 const DispClear dc) {
   __shared__ uint32_t s_tile;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
     return;
   }
   scan_tile(cellCount, cellStart, (long long)tile * kScanTile, nCells, tile, 0, 0u,
-            tile == nTiles - 1, state, epoch, err, spinLimit);
+            tile == nTiles - 1, state, epoch, err, spinLimit, dc);
   if (threadIdx.x == 0 && tile == nTiles - 1) *ticket = 0u;  // all tickets taken: reset
 }
 
@@ -262,11 +266,12 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
 // Tile states are indexed by g, the item's position in the launch's segment.
 __global__ void __launch_bounds__(kBlock) k_scan_b(const __grid_constant__ BatchWork w,
                                                    const __grid_constant__ DevScene d, uint32_t epoch) {
-  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
+  for_each_item<false>(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
     const long long limit = (long long)P.cOff + P.nCells;
     const bool last = (long long)(lt + 1) * kScanTile >= (long long)P.nCells;
+    const DispClear dc{d.cellDisp, d.cellStride, min(P.iters, (uint32_t)kDispSlots)};
     scan_tile(d.cellCount, d.cellStart, (long long)P.cOff + (long long)lt * kScanTile, limit, (int)g,
-              (int)(g - lt), P.pOff, last, d.scanState, epoch, d.errorWord, kScanSpinLimit);
+              (int)(g - lt), P.pOff, last, d.scanState, epoch, d.errorWord, kScanSpinLimit, dc);
   });
 }
 
@@ -275,9 +280,10 @@ void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_key_count<<<groups(work), kBlock, 0, st>>>(P, d);
 }
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells, unsigned long long* state,
-                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st, uint32_t spinLimit) {
+                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st, uint32_t spinLimit,
+                 const DispClear& dc) {
   const int tiles = scan_tiles(nCells);
-  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err, spinLimit);
+  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err, spinLimit, dc);
 }
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_fill<<<groups(P.n), kBlock, 0, st>>>(P, d);

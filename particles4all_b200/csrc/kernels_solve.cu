@@ -59,8 +59,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   float rho = P.mass * poly6(P, 0.0f);
   F3 gradSum = {0.f, 0.f, 0.f};
   float sumGrad2 = 0.0f;
-  auto fluid = [&](uint32_t j, float4 q) {
-    if (j == i) return;
+  auto fluid = [&](uint32_t, float4 q) {
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of the list only
@@ -88,7 +87,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
   if (count != kListOverflow) {
     walk_list<PF>(d.nbList, cap, i, count, pred, d.bpos, fluid, bound);
   } else {
-    walk_direct<true>(P, w, pi, pred, cs, bcs, d.bpos, fluid, bound);
+    walk_direct<true>(P, w, pi, i, pred, cs, bcs, d.bpos, fluid, bound);
   }
   d.density[i] = rho;
   const float C = rho * P.invRho0 - 1.0f;
@@ -118,10 +117,10 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   const uint32_t count = __ldg(&d.nbCount[i]);  // lambda's list for these positions
   F3 dsum = {0.f, 0.f, 0.f}, dB = {0.f, 0.f, 0.f};
   float nc = 1.0f;
-  auto fluid = [&](uint32_t j, float4 q) {
+  auto fluid = [&](uint32_t, float4 q) {
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
-    if (r2 >= P.h2 || r2 < 1.0e-12f || j == i) return;
+    if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = P.spikyGrad * hr * hr / rr;
@@ -146,7 +145,7 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     walk_list(d.nbList, cap, i, count, pl, d.bpos, fluid, bound);
   } else {
     const RowWalk w(P, pi);
-    walk_direct<true>(P, w, pi, pl, cs, bcs, d.bpos, fluid, bound);
+    walk_direct<true>(P, w, pi, i, pl, cs, bcs, d.bpos, fluid, bound);
   }
   const F3 dd = {fmaf(dB.x, P.invRho0, dsum.x * P.volume), fmaf(dB.y, P.invRho0, dsum.y * P.volume),
                  fmaf(dB.z, P.invRho0, dsum.z * P.volume)};

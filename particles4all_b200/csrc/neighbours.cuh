@@ -64,8 +64,12 @@ __device__ __forceinline__ uint32_t build_list(const SimParams& P, const RowWalk
                                                const float4* __restrict__ bpos, uint32_t* __restrict__ list,
                                                uint32_t cap, float r2lim) {
   uint32_t c = 0, flags = 0u;
+  uint32_t* __restrict__ out = list + i;  // entry c at list[c * cap + i]
   auto push = [&](uint32_t e) {
-    if (c < kListCap) list[(size_t)c * cap + i] = e;
+    if (c < kListCap) {
+      *out = e;
+      out += cap;
+    }
     c++;
   };
 #pragma unroll 1
@@ -269,35 +273,43 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uin
       fluid(cur, q);
     }
   };
-  uint32_t e0 = __ldg(&list[i]);
+  const uint32_t* __restrict__ at = list + i;  // entry k of the particle at list[k * cap + i]
+  uint32_t e0 = __ldg(at);
   if constexpr (PF) {
     float4 q0 = fetch(e0);
-    uint32_t e1 = count > 1u ? __ldg(&list[(size_t)cap + i]) : 0u;
+    at += cap;
+    uint32_t e1 = count > 1u ? __ldg(at) : 0u;
     for (uint32_t k = 1; k <= count; k++) {
       const uint32_t cur = e0;
       const float4 qc = q0;
       if (k < count) {
         e0 = e1;
         q0 = fetch(e1);
-        if (k + 1 < count) e1 = __ldg(&list[(size_t)(k + 1) * cap + i]);
+        if (k + 1 < count) {
+          at += cap;
+          e1 = __ldg(at);
+        }
       }
       visit(cur, qc);
     }
   } else {
     for (uint32_t k = 1; k <= count; k++) {
       const uint32_t cur = e0;
-      if (k < count) e0 = __ldg(&list[(size_t)k * cap + i]);
+      if (k < count) {
+        at += cap;
+        e0 = __ldg(at);
+      }
       visit(cur, fetch(cur));
     }
   }
 }
 
 // The reference's direct loop (particles whose list overflowed): every candidate
-// j of the nine rows with r^2 < h^2 (j == i included; the passes skip it), then,
-// when B, the row's boundary samples with 1e-12 <= r^2 < h^2. fsrc holds the
-// candidate positions in .xyz (and whatever the pass keeps in .w).
+// j != self of the nine rows with r^2 < h^2 (the particle itself contributes to
+// no pass), then, when B, the row's boundary samples with 1e-12 <= r^2 < h^2. fsrc
+// holds the candidate positions in .xyz (and whatever the pass keeps in .w).
 template <bool B, class FFluid, class FBound>
-__device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w, F3 pi,
+__device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w, F3 pi, uint32_t self,
                                             const float4* __restrict__ fsrc, const uint32_t* __restrict__ cs,
                                             const uint32_t* __restrict__ bcs, const float4* __restrict__ bpos,
                                             FFluid&& fluid, FBound&& bound) {
@@ -310,7 +322,7 @@ __device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w
     for (uint32_t j = b; j < e; j++) {
       const float4 q = __ldg(&fsrc[j]);
       const F3 d = sub3(pi, xyz(q));
-      if (dot3(d, d) < P.h2) fluid(j, q);
+      if (dot3(d, d) < P.h2 && j != self) fluid(j, q);
     }
     if constexpr (B) {
       if (P.nBoundary > 0u) {
@@ -337,7 +349,7 @@ __device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWal
   if (count != kListOverflow) {
     walk_list(list, cap, i, count, pred, nullptr, fluid, none);
   } else {
-    walk_direct<false>(P, w, pi, pred, cs, nullptr, nullptr, fluid, none);
+    walk_direct<false>(P, w, pi, i, pred, cs, nullptr, nullptr, fluid, none);
   }
 }
 

@@ -7,13 +7,17 @@ namespace p4a {
 // Batched form: the block pulls work items (scene slot, item) from its launch's
 // segment, one per cursor increment, and calls f(P, item, k) for each, with P the
 // item's SimParams in shared memory (reloaded only when the scene changes) and k
-// the item's position in the segment. The next item is claimed while the current
-// one runs, so the cursor's round trip is hidden. Items are claimed in increasing
-// k and a block claims its next item only while working on one, so the smallest
-// unfinished item is always being worked on: a block that waits on earlier items
-// (the scan's lookback) waits on blocks that finish.
+// the item's position in the segment. With AHEAD the next item is claimed while
+// the current one runs, so the cursor's round trip is hidden. Items are claimed in
+// increasing k and a block claims its next item only while working on one, so the
+// smallest unfinished item is always being worked on: a block that waits on
+// earlier items waits on blocks that finish. For items that wait on their
+// predecessors (the scan's lookback) AHEAD is off: the next item is claimed only
+// after the current one is done, so every claimed item is being worked on and no
+// item waits on one that is claimed but not started (such waits chained up and
+// made the batched scan ten times slower than its memory traffic).
 // f may contain block barriers: every thread of the block makes every call.
-template <class F>
+template <bool AHEAD = true, class F>
 __device__ __forceinline__ void for_each_item(const BatchWork& w, F&& f) {
   __shared__ __align__(16) SimParams sP;
   __shared__ uint32_t sNext[2], sSlot;
@@ -26,7 +30,7 @@ __device__ __forceinline__ void for_each_item(const BatchWork& w, F&& f) {
   for (int p = 0;; p ^= 1) {
     const uint32_t k = sNext[p];
     if (k >= seg.count) break;
-    if (threadIdx.x == 0) sNext[p ^ 1] = atomicAdd(w.cursor, 1u);
+    if (AHEAD && threadIdx.x == 0) sNext[p ^ 1] = atomicAdd(w.cursor, 1u);
     const uint2 it = w.items[seg.off + k];
     if (it.x != sSlot) {
       __syncthreads();  // every thread has compared against the old slot
@@ -37,6 +41,7 @@ __device__ __forceinline__ void for_each_item(const BatchWork& w, F&& f) {
       __syncthreads();
     }
     f(static_cast<const SimParams&>(sP), it.y, k);
+    if (!AHEAD && threadIdx.x == 0) sNext[p ^ 1] = atomicAdd(w.cursor, 1u);
     __syncthreads();  // the item is done with sP; sNext[p ^ 1] is visible
   }
 }
