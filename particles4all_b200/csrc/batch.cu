@@ -125,7 +125,7 @@ void pack(BScene& s, double dt, int slot) {
 
 // Kinds of the launches of a frame, in the order a substep issues them.
 enum LaunchKind : int {
-  LK_ZERO, LK_KEY, LK_SCAN, LK_FILL, LK_REORDER, LK_SEED, LK_LAMBDA, LK_DELTA, LK_MATCH,
+  LK_ZERO, LK_KEY, LK_SCAN_SUMS, LK_SCAN_OFFSETS, LK_SCAN, LK_FILL, LK_REORDER, LK_SEED, LK_LAMBDA, LK_DELTA, LK_MATCH,
   LK_FINISH, LK_NORMALS, LK_TENSION
 };
 
@@ -156,7 +156,8 @@ WorkSeg push_items(Frame& F, uint32_t row, int64_t count, WorkSeg seg) {
 
 void add_launch(Frame& F, int kind, int sub, int it, WorkSeg seg) { F.launches.push_back({kind, sub, it, seg}); }
 
-constexpr const char* kLaunchNames[] = {"zero_stats", "key_count", "scan", "fill", "reorder", "body_seed",
+constexpr const char* kLaunchNames[] = {"zero_stats", "key_count", "scan_sums", "scan_offsets", "scan", "fill",
+                                         "reorder", "body_seed",
                                          "lambda", "delta", "body_match", "xsph_finalize", "xsph_normals",
                                          "tension_finalize"};
 constexpr int kLaunchKinds = (int)(sizeof(kLaunchNames) / sizeof(kLaunchNames[0]));
@@ -190,10 +191,9 @@ int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched,
     switch (r.kind) {
       case LK_ZERO: launch_zero_stats_b(w, d.statsOut, st); break;
       case LK_KEY: launch_key_count_b(w, maxItems, d, st); break;
-      case LK_SCAN:
-        BTRY(b, cudaMemsetAsync(d.scanState, 0, (graphForm ? (size_t)b->scanTilesCap : r.seg.count) * 8, st));
-        launch_scan_b(w, maxItems, d, 1u, st);
-        break;
+      case LK_SCAN_SUMS: launch_scan_sums_b(w, maxItems, d, st); break;
+      case LK_SCAN_OFFSETS: launch_scan_offsets_b(w, maxItems, d, st); break;
+      case LK_SCAN: launch_scan_apply_b(w, maxItems, d, st); break;
       case LK_FILL: launch_fill_b(w, maxItems, d, st); break;
       case LK_REORDER: launch_reorder_b(w, maxItems, d, st); break;
       case LK_SEED: launch_body_seed_b(w, maxItems, d, st); break;
@@ -606,6 +606,8 @@ int prime_scenes(p4a_batch* b, const std::vector<int>& slots) {
   for (size_t k = 0; k < slots.size(); k++) scan = push_items(F, (uint32_t)k, scan_tiles(b->scenes[slots[k]].nCells), scan);
   for (size_t k = 0; k < slots.size(); k++) part = push_items(F, (uint32_t)k, groups(b->scenes[slots[k]].n), part);
   add_launch(F, LK_KEY, 0, 0, key);
+  add_launch(F, LK_SCAN_SUMS, 0, 0, scan);
+  add_launch(F, LK_SCAN_OFFSETS, 0, 0, scan);
   add_launch(F, LK_SCAN, 0, 0, scan);
   add_launch(F, LK_FILL, 0, 0, part);
   add_launch(F, LK_REORDER, 0, 0, part);
@@ -684,6 +686,8 @@ int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t 
     const WorkSeg part = seg([](const BScene& S) { return (int64_t)groups(S.n); });
     const WorkSeg seed = seg([](const BScene& S) { return (int64_t)(S.nBodyParts > 0 ? S.nBodies : 0); });
     add_launch(F, LK_KEY, s, 0, key);
+    add_launch(F, LK_SCAN_SUMS, s, 0, scan);
+    add_launch(F, LK_SCAN_OFFSETS, s, 0, scan);
     add_launch(F, LK_SCAN, s, 0, scan);
     add_launch(F, LK_FILL, s, 0, part);
     add_launch(F, LK_REORDER, s, 0, part);

@@ -296,7 +296,10 @@ void launch_tension_finalize(const SimParams& P, const DevScene& d, int substep,
 // resident on the device at once); pass a large value for a launch whose count is
 // only known on the device (a replayed graph).
 void launch_key_count_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
-void launch_scan_b(const BatchWork& w, int maxItems, const DevScene& d, uint32_t epoch, cudaStream_t st);
+// the batched scan in three launches over the same tile items (kernels_grid.cu)
+void launch_scan_sums_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_scan_offsets_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
+void launch_scan_apply_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
 void launch_fill_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
 void launch_reorder_b(const BatchWork& w, int maxItems, const DevScene& d, cudaStream_t st);
 void launch_lambda_b(const BatchWork& w, int maxItems, const DevScene& d, int it, cudaStream_t st, int variant);
