@@ -339,8 +339,7 @@ void grid_pass(p4a_sim* s, int par) {
   launch_key_count(s->P, d, st);
   mark(s, PH_SCAN);
   launch_scan(d.cellCount, d.cellStart, s->nCells, d.scanState, d.scanTicket, next_epoch(s),
-              d.errorWord, st, kScanSpinLimit,
-              DispClear{d.cellDisp, d.cellStride, (uint32_t)std::min(std::max(1, s->params.iterations), kDispSlots)});
+              d.errorWord, st);
   mark(s, PH_FILL);
   launch_fill(s->P, d, st);
   mark(s, PH_REORDER);

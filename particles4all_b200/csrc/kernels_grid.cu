@@ -40,7 +40,18 @@ __device__ __forceinline__ void key_count_body(const SimParams& P, const DevScen
     const int leader = __ffs(peers) - 1;
     const uint32_t lt = peers & ((1u << lane) - 1u);
     uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
+    if (lane == leader) {
+      base = atomicAdd(&d.cellCount[k], (uint32_t)__popc(peers));
+      // this substep's per-cell displacement slots start at zero for every occupied
+      // cell (list reuse only: a slot left larger makes the bound looser, never wrong).
+      // Done here by the warp leaders rather than in the scan: measured cheaper, the
+      // stores hide among the key pass's loads (a clear in the batched scan cost
+      // ~60 us per launch on the 96-scene mix and saved ~6 us here).
+      if (d.cellDisp) {
+        const uint32_t slots = min(P.iters, (uint32_t)kDispSlots);
+        for (uint32_t t = 0; t < slots; t++) d.cellDisp[(size_t)t * d.cellStride + k] = 0.0f;
+      }
+    }
     base = __shfl_sync(peers, base, leader);
     d.key[i] = k;
     d.rank[i] = base + (uint32_t)__popc(lt);
@@ -136,8 +147,7 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
                                           uint32_t* __restrict__ cellStart, long long cellBase,
                                           long long limit, int tile, int firstTile, uint32_t seed,
                                           bool lastOfSegment, unsigned long long* __restrict__ state,
-                                          uint32_t epoch, uint32_t* __restrict__ err, uint32_t spinLimit,
-                                          const DispClear& dc) {
+                                          uint32_t epoch, uint32_t* __restrict__ err, uint32_t spinLimit) {
   __shared__ uint32_t s_prefix;
   __shared__ uint32_t s_warp[kBlock / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -154,15 +164,6 @@ __device__ __forceinline__ void scan_tile(uint32_t* __restrict__ cellCount,
   for (int j = 0; j < kScanItems; j++) {
     const long long idx = base + j;
     if (idx < limit) cellCount[idx] = 0u;
-  }
-  // this substep's per-cell displacement slots start at zero for every occupied cell
-  // (list reuse only: a slot left larger makes the bound looser, never wrong)
-  if (dc.disp) {
-    for (uint32_t t = 0; t < dc.slots; t++) {
-#pragma unroll
-      for (int j = 0; j < kScanItems; j++)
-        if (v[j] != 0u) dc.disp[(size_t)t * dc.stride + (size_t)(base + j)] = 0.0f;
-    }
   }
   uint32_t incl = sum;
 #pragma unroll
@@ -246,8 +247,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
                                                  uint32_t* __restrict__ cellStart, int nCells,
                                                  unsigned long long* __restrict__ state,
                                                  uint32_t* __restrict__ ticket, uint32_t epoch,
-                                                 int nTiles, uint32_t* __restrict__ err, uint32_t spinLimit,
-                                                 const DispClear dc) {
+                                                 int nTiles, uint32_t* __restrict__ err, uint32_t spinLimit) {
   __shared__ uint32_t s_tile;
   if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
     return;
   }
   scan_tile(cellCount, cellStart, (long long)tile * kScanTile, nCells, tile, 0, 0u,
-            tile == nTiles - 1, state, epoch, err, spinLimit, dc);
+            tile == nTiles - 1, state, epoch, err, spinLimit);
   if (threadIdx.x == 0 && tile == nTiles - 1) *ticket = 0u;  // all tickets taken: reset
 }
 
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(kBlock) k_scan(uint32_t* __restrict__ cellCoun
 //   offsets  the block that gets a scene's first tile scans that scene's tile sums
 //            into tileOffset[g] = pOff + the sum of the scene's earlier tiles;
 //   apply    each tile's exclusive scan from tileOffset[g]: cellStart, the cleared
-//            histogram and displacement slots, and the scene's total from its last tile.
+//            histogram, and the scene's total from its last tile.
 // tileSum and tileOffset share the scan-state array (two u32 per tile). The
 // single-pass lookback of the plain scan serialised here: with thousands of tiles
 // of ~100 scenes in flight, its waits chained (178 us for 9.2 M cells).
@@ -359,15 +359,6 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply_b(const __grid_constant__
 #pragma unroll
     for (int j = 0; j < kScanItems; j++)
       if (base + j < limit) d.cellCount[base + j] = 0u;
-    // this substep's per-cell displacement slots start at zero for every occupied cell
-    if (d.cellDisp) {
-      const uint32_t slots = min(P.iters, (uint32_t)kDispSlots);
-      for (uint32_t t = 0; t < slots; t++) {
-#pragma unroll
-        for (int j = 0; j < kScanItems; j++)
-          if (v[j] != 0u) d.cellDisp[(size_t)t * d.cellStride + (size_t)(base + j)] = 0.0f;
-      }
-    }
     uint32_t total = 0;
     const uint32_t offset = st[2 * (size_t)g + 1];
     uint32_t run = offset + block_exclusive(sum, &total);
@@ -385,10 +376,9 @@ void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_key_count<<<groups(work), kBlock, 0, st>>>(P, d);
 }
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells, unsigned long long* state,
-                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st, uint32_t spinLimit,
-                 const DispClear& dc) {
+                 uint32_t* ticket, uint32_t epoch, uint32_t* err, cudaStream_t st, uint32_t spinLimit) {
   const int tiles = scan_tiles(nCells);
-  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err, spinLimit, dc);
+  k_scan<<<tiles, kBlock, 0, st>>>(cellCount, cellStart, nCells, state, ticket, epoch, tiles, err, spinLimit);
 }
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st) {
   k_fill<<<groups(P.n), kBlock, 0, st>>>(P, d);

@@ -256,15 +256,9 @@ inline int scan_tiles(int nCells) { return groups(nCells, kScanTile); }
 
 // ---- plain launchers (one scene; P.parity = live parity before the sort) ----
 void launch_key_count(const SimParams& P, const DevScene& d, cudaStream_t st);
-// The scan also clears the per-cell displacement slots of the occupied cells of the
-// step's sort (disp null: none, as for the operators and the mesh).
-struct DispClear {
-  float* disp;
-  uint32_t stride, slots;
-};
 void launch_scan(uint32_t* cellCount, uint32_t* cellStart, int nCells,
                  unsigned long long* state, uint32_t* ticket, uint32_t epoch, uint32_t* err,
-                 cudaStream_t st, uint32_t spinLimit = kScanSpinLimit, const DispClear& dc = DispClear{});
+                 cudaStream_t st, uint32_t spinLimit = kScanSpinLimit);
 void launch_fill(const SimParams& P, const DevScene& d, cudaStream_t st);
 void launch_reorder(const SimParams& P, const DevScene& d, cudaStream_t st);
 // Kernels with tuned launch shapes (threads per block x minimum blocks per SM; the
