@@ -59,7 +59,7 @@ struct SimParams {
 // iterations rebuild their masks.
 constexpr int kDispSlots = 16;
 // Skin of the reused masks, in units of h.
-constexpr double kSkin = 0.05;
+constexpr double kSkin = 0.03;
 
 // Anisotropic-kernel uniform (src/aniso_wgsl.js:4-21, packed by src/mesh.js:227-241).
 struct AnisoParams {
