@@ -61,6 +61,8 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--io-groups", type=int, default=0,
+                    help="frames per step of the mix's e2e run (0: chosen by p4a_batch_step_io)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-scene loop of the mix")
     ap.add_argument("--no-large", action="store_true", help="skip the large_hose_2m sub-line")
     ap.add_argument("--large-steps", type=int, default=40)
@@ -418,7 +420,7 @@ def run_mix(args):
     # end to end through the batch C ABI: host state in, frame, host state out
     e2e = None
     if not args.no_e2e:
-        e2e = mix_e2e(b, ids, flags, max(3, min(args.steps, 10)), rep, world)
+        e2e = mix_e2e(b, ids, flags, max(3, min(args.steps, 10)), rep, world, args.io_groups)
 
     plain = None
     if world == 1 and not args.no_plain:
@@ -465,10 +467,13 @@ def run_mix(args):
     return 0
 
 
-def mix_e2e(b, ids, flags, frames, rep, world):
+def mix_e2e(b, ids, flags, frames, rep, world, groups=0):
     """Per frame through the public batch API: every scene's pos and vel written
     from pinned host memory, the batched frame, pos and vel read back to pinned
-    host memory, all waited for. The state read back is the next frame's input."""
+    host memory, all waited for. The state read back is the next frame's input.
+    Timed twice: through p4a_batch_step_io (the scenes in `groups` frames, the
+    copies of each group overlapping the frames of the others; the reported
+    value) and as write_async, p4a_batch_step, read_async on the batch's stream."""
     import torch
     caps = [f[0] for f in flags]
     total = sum(caps)
@@ -484,33 +489,57 @@ def mix_e2e(b, ids, flags, frames, rep, world):
         b.read_async(s, "pos", base, n * 16)
         b.read_async(s, "vel", base + n * 16, n * 16)
     b.synchronize()
-    rep.barrier()
-    t_before = [b.info(s)["sim_time"] for s in ids]
-    t0 = time.perf_counter()
-    h2d = d2h = 0
-    for k in range(frames):
-        hin, hout = bufs[k & 1], bufs[(k + 1) & 1]
-        for s, n, off in zip(ids, caps, offs):
-            base = hin.data_ptr() + off * 4
-            b.write_async(s, "pos", base, n * 16)
-            b.write_async(s, "vel", base + n * 16, n * 16)
-            h2d += 32 * n
-        b.step(ids, 1 / 60)
-        for s, n, off in zip(ids, caps, offs):
-            base = hout.data_ptr() + off * 4
-            b.read_async(s, "pos", base, n * 16)
-            b.read_async(s, "vel", base + n * 16, n * 16)
-            d2h += 32 * n
+
+    cur = [0]  # the buffer holding the latest state read back
+
+    def frame(overlap):
+        hin, hout = bufs[cur[0]], bufs[cur[0] ^ 1]
+        cur[0] ^= 1
+        if overlap:
+            entries = []
+            for s, n, off in zip(ids, caps, offs):
+                bi, bo = hin.data_ptr() + off * 4, hout.data_ptr() + off * 4
+                entries.append((s, bi, bi + n * 16, bo, bo + n * 16))
+            b.step_io(entries, 1 / 60, groups)
+        else:
+            for s, n, off in zip(ids, caps, offs):
+                base = hin.data_ptr() + off * 4
+                b.write_async(s, "pos", base, n * 16)
+                b.write_async(s, "vel", base + n * 16, n * 16)
+            b.step(ids, 1 / 60)
+            for s, n, off in zip(ids, caps, offs):
+                base = hout.data_ptr() + off * 4
+                b.read_async(s, "pos", base, n * 16)
+                b.read_async(s, "vel", base + n * 16, n * 16)
         b.synchronize()
-    t1 = time.perf_counter()
-    rep.barrier()
-    el = rep.max(t1 - t0)
-    done = sum(n * round((b.info(s)["sim_time"] - tb) * 120.0) for s, n, tb in zip(ids, caps, t_before))
-    return {"value": world * done / el, "unit": METRIC, "h2d_bytes_per_step": h2d // frames,
-            "d2h_bytes_per_step": d2h // frames, "steps": frames,
-            "what": "per frame through p4a_batch_write_async / p4a_batch_step / p4a_batch_read_async: every "
-                    "scene's pos+vel from pinned host memory, one batched frame, every scene's pos+vel back "
-                    "to pinned host memory, p4a_batch_synchronize; wall clock, max over ranks"}
+
+    # the two forms alternate frame by frame, so that both see the same stage of
+    # the scenes' motion (later frames of the mix cost more); one untimed frame of
+    # each first captures its frame graphs
+    frame(False)
+    frame(True)
+    el = [0.0, 0.0]
+    done = [0, 0]
+    for k in range(2 * frames):
+        form = k & 1
+        tb = [b.info(s)["sim_time"] for s in ids]
+        rep.barrier()
+        t0 = time.perf_counter()
+        frame(bool(form))
+        t1 = time.perf_counter()
+        el[form] += rep.max(t1 - t0)
+        done[form] += sum(n * round((b.info(s)["sim_time"] - t) * 120.0) for s, n, t in zip(ids, caps, tb))
+    serial, value = world * done[0] / el[0], world * done[1] / el[1]
+    h2d = d2h = 32 * total
+    return {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "steps": frames, "io_groups": groups or "auto",
+            "serial_value": serial,
+            "what": "per frame through p4a_batch_step_io: every scene's pos+vel from pinned host memory, the "
+                    "scenes stepped as consecutive frames of about equal particle counts with each group's "
+                    "copies on two copy streams overlapping the other groups' frames, every scene's pos+vel "
+                    "back to pinned host memory, p4a_batch_synchronize; wall clock, max over ranks. "
+                    "serial_value: the same with write_async, one p4a_batch_step of all scenes and "
+                    "read_async on the batch's stream; the two forms alternate frame by frame"}
 
 
 def mix_plain(mix, stream, flush, warm, steps):

@@ -517,6 +517,31 @@ int p4a_batch_read_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t whi
                          size_t offset, size_t bytes);
 int p4a_batch_write_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t which,
                           const void* host, size_t offset, size_t bytes);
+/* One frame of the listed scenes with host I/O overlapped: every non-NULL pos_in /
+ * vel_in (n x float4, n = the scene's particle count) is written into the scene's
+ * live buffer, the scenes are stepped by frame_dt, and every non-NULL pos_out /
+ * vel_out receives the live buffer after the step. The results are those of
+ * write_async, p4a_batch_step and read_async in that order, bit for bit; here the
+ * scenes are stepped as `groups` consecutive frames of about equal particle counts
+ * (0: two from 3 M particles up, else one), with the host-to-device copies of later
+ * groups and the device-to-host copies of earlier ones on two copy streams of
+ * their own, so that they overlap the frames of the other groups. The copies of
+ * the first group's inputs and the last group's outputs stay exposed, and every
+ * extra group adds a frame's launch tails. The copies are ordered after all
+ * work queued on the batch's stream before the call and before all work queued
+ * after it; host memory (pinned, for overlap) stays in use until
+ * p4a_batch_synchronize. No counterpart in the reference, which steps one scene
+ * and hands its live buffers to the renderer on the device (livePos / liveVel,
+ * src/sim.js:811-812). */
+typedef struct p4a_batch_io {
+  int32_t scene_id;
+  const void* pos_in;
+  const void* vel_in;
+  void* pos_out;
+  void* vel_out;
+} p4a_batch_io;
+int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, double frame_dt,
+                      int32_t groups);
 /* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
 int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
 /* Per-kernel timing of batched frames, as p4a_profile_* for a Sim (the

@@ -157,6 +157,11 @@ class BatchUsage(C.Structure):
                 ("live_scenes", C.c_int32), ("device_bytes", C.c_int64)]
 
 
+class BatchIO(C.Structure):
+    _fields_ = [("scene_id", C.c_int32), ("pos_in", C.c_void_p), ("vel_in", C.c_void_p),
+                ("pos_out", C.c_void_p), ("vel_out", C.c_void_p)]
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("arenas", BatchConfig), ("builder_threads", C.c_int32), ("max_frames_in_flight", C.c_int32),
                 ("admit_timeout", C.c_double), ("max_pending_creates", C.c_int32), ("use_graphs", C.c_int32),

@@ -142,6 +142,19 @@ class Batch:
         self._check(self._L.p4a_batch_write_async(self._h, int(sid), _abi.BUF[name], which, C.c_void_p(host_ptr),
                                                   int(offset), int(nbytes)), "write_async")
 
+    def step_io(self, entries, frame_dt, groups=0):
+        """One frame of the scenes of `entries` with overlapped host I/O: each entry
+        is (sid, pos_in, vel_in, pos_out, vel_out), host addresses (pinned for
+        overlap) of n x float4 each, or None. Same bits as write_async, step and
+        read_async; the scenes run as `groups` frames (0: chosen from their size)
+        so that the copies of one group overlap the frames of the others. Host
+        memory stays in use until synchronize()."""
+        arr = (_abi.BatchIO * max(1, len(entries)))()
+        for k, (sid, pin, vin, pout, vout) in enumerate(entries):
+            arr[k] = _abi.BatchIO(int(sid), pin, vin, pout, vout)
+        self._check(self._L.p4a_batch_step_io(self._h, arr, len(entries), float(frame_dt), int(groups)),
+                    "step_io")
+
     def profile(self, on=True):
         self._check(self._L.p4a_batch_profile_enable(self._h, 1 if on else 0), "profile_enable")
 

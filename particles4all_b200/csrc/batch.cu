@@ -865,6 +865,9 @@ int p4a_batch_destroy(p4a_batch* b) {
   if (b->dSegs) cudaFree(b->dSegs);
   if (b->dCursors) cudaFree(b->dCursors);
   if (b->upStream) cudaStreamDestroy(b->upStream);
+  if (b->h2dStream) cudaStreamDestroy(b->h2dStream);
+  if (b->d2hStream) cudaStreamDestroy(b->d2hStream);
+  for (cudaEvent_t e : b->ioEvents) cudaEventDestroy(e);
   for (int k = 0; k < 2; k++) {
     if (b->staging[k]) cudaFreeHost(b->staging[k]);
     if (b->stagingDone[k]) cudaEventDestroy(b->stagingDone[k]);
@@ -1141,6 +1144,115 @@ int p4a_batch_write_async(p4a_batch* b, int32_t id, int32_t bid, int32_t which, 
   cudaSetDevice(b->device);
   BTRY(b, cudaMemcpyAsync((char*)p + offset, host, bytes, cudaMemcpyHostToDevice, b->stream));
   return P4A_OK;
+}
+
+int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, double frameDt, int32_t groups) {
+  if (!b || count < 0 || (count > 0 && !io) || groups < 0)
+    return bfail(b, P4A_ERR_ARG, "p4a_batch_step_io: bad list");
+  cudaSetDevice(b->device);
+  std::vector<char> seen(b->scenes.size(), 0);
+  int64_t total = 0;
+  for (int k = 0; k < count; k++) {
+    const int rc = scene_ok(b, io[k].scene_id);
+    if (rc) return rc;
+    if (seen[io[k].scene_id]++) return bfail(b, P4A_ERR_ARG, "p4a_batch_step_io: scene %d listed twice", io[k].scene_id);
+    total += b->scenes[io[k].scene_id].n;
+  }
+  if (count == 0) return P4A_OK;
+  // groups of about equal particle counts, in list order. By default two from 3 M
+  // particles up, else one: each split adds the launch tails of a whole frame (on
+  // the 6 M-particle mix a frame split in two took 6 % longer, in four 18 %), so a
+  // second group pays for itself only where half the copies it hides cost more.
+  int G = groups > 0 ? groups : (total >= 3000000 ? 2 : 1);
+  G = std::min(G, std::min(count, 64));
+  std::vector<int> first((size_t)G + 1, count);
+  first[0] = 0;
+  {
+    // group g starts after the first scene k at which the groups before it hold
+    // g / G of the particles, or where each later group is left one scene
+    int64_t acc = 0;
+    int g = 1;
+    for (int k = 0; k < count && g < G; k++) {
+      acc += b->scenes[io[k].scene_id].n;
+      const int left = count - (k + 1);
+      if (acc * G >= total * g || left == G - g) first[(size_t)g++] = k + 1;
+    }
+  }
+  if (!b->h2dStream) BTRY(b, cudaStreamCreateWithFlags(&b->h2dStream, cudaStreamNonBlocking));
+  if (!b->d2hStream) BTRY(b, cudaStreamCreateWithFlags(&b->d2hStream, cudaStreamNonBlocking));
+  while (b->ioEvents.size() < (size_t)(2 * G + 2)) {
+    cudaEvent_t e = nullptr;
+    BTRY(b, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ioEvents.push_back(e);
+  }
+  cudaEvent_t* ev = b->ioEvents.data();
+  auto live = [&](const BScene& S, int32_t bid, void** p) -> int {
+    size_t bytes = 0;
+    const int rc = scene_buffer(b, S, bid, P4A_LIVE, p, &bytes);
+    return rc ? rc : ((size_t)S.n * 16 > bytes ? bfail(b, P4A_ERR_ARG, "scene buffer too small") : P4A_OK);
+  };
+  // the copies start after everything queued on the batch's stream so far
+  BTRY(b, cudaEventRecord(ev[0], b->stream));
+  BTRY(b, cudaStreamWaitEvent(b->h2dStream, ev[0], 0));
+  BTRY(b, cudaStreamWaitEvent(b->d2hStream, ev[0], 0));
+  auto copies = [&](int g, bool in) -> int {
+    for (int k = first[(size_t)g]; k < first[(size_t)g + 1]; k++) {
+      const BScene& S = b->scenes[io[k].scene_id];
+      const size_t bytes = (size_t)S.n * 16;
+      const void* hp[2] = {in ? io[k].pos_in : io[k].pos_out, in ? io[k].vel_in : io[k].vel_out};
+      for (int q = 0; q < 2; q++) {
+        if (!hp[q] || !bytes) continue;
+        void* p = nullptr;
+        const int rc = live(S, q ? P4A_BUF_VEL : P4A_BUF_POS, &p);
+        if (rc) return rc;
+        if (in)
+          BTRY(b, cudaMemcpyAsync(p, hp[q], bytes, cudaMemcpyHostToDevice, b->h2dStream));
+        else
+          BTRY(b, cudaMemcpyAsync(const_cast<void*>(hp[q]), p, bytes, cudaMemcpyDeviceToHost, b->d2hStream));
+      }
+    }
+    return P4A_OK;
+  };
+  auto writes = [&](int g) -> int {
+    const int rc = copies(g, true);
+    if (rc) return rc;
+    BTRY(b, cudaEventRecord(ev[1 + 2 * g], b->h2dStream));
+    return P4A_OK;
+  };
+  std::vector<int32_t> ids;
+  auto frame = [&](int g) -> int {
+    // group g's frame waits for its own writes only
+    BTRY(b, cudaStreamWaitEvent(b->stream, ev[1 + 2 * g], 0));
+    ids.clear();
+    for (int k = first[(size_t)g]; k < first[(size_t)g + 1]; k++) ids.push_back(io[k].scene_id);
+    const std::vector<double> dts(ids.size(), frameDt);
+    const int rc = step_frame(b, ids.data(), dts.data(), (int32_t)ids.size());
+    if (rc) return rc;
+    BTRY(b, cudaEventRecord(ev[2 + 2 * g], b->stream));
+    return P4A_OK;
+  };
+  auto reads = [&](int g) -> int {
+    // group g's reads wait for its own frame only
+    BTRY(b, cudaStreamWaitEvent(b->d2hStream, ev[2 + 2 * g], 0));
+    return copies(g, false);
+  };
+  // Issued as W0 F0, then W(g) F(g) R(g-1), then the last reads: a copy queued
+  // behind one that waits for a frame never holds up an earlier frame, whether the
+  // copy engines serve the two copy streams apart or in issue order.
+  int rc = writes(0);
+  if (!rc) rc = frame(0);
+  for (int g = 1; g < G && !rc; g++) {
+    rc = writes(g);
+    if (!rc) rc = frame(g);
+    if (!rc) rc = reads(g - 1);
+  }
+  if (!rc) rc = reads(G - 1);
+  // later work on the batch's stream (and p4a_batch_synchronize) waits for every copy
+  BTRY(b, cudaEventRecord(ev[2 * G + 1], b->d2hStream));
+  BTRY(b, cudaStreamWaitEvent(b->stream, ev[2 * G + 1], 0));
+  BTRY(b, cudaEventRecord(ev[0], b->h2dStream));
+  BTRY(b, cudaStreamWaitEvent(b->stream, ev[0], 0));
+  return rc;
 }
 
 int p4a_batch_stats(p4a_batch* b, int32_t id, p4a_stats* o) {

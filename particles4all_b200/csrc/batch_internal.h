@@ -116,6 +116,11 @@ struct p4a_batch {
   // CUDA graphs of frame shapes (substeps and iterations per substep)
   bool useGraphs = true;
   cudaStream_t upStream = nullptr;  // admissions' uploads (serving loop)
+  // p4a_batch_step_io: a stream per copy direction and the events that order the
+  // copies against the frames ([0] the call's start, [1 + 2g] group g written,
+  // [2 + 2g] group g stepped, then the reads' end)
+  cudaStream_t h2dStream = nullptr, d2hStream = nullptr;
+  std::vector<cudaEvent_t> ioEvents;
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
   // per-kernel timing of frames (p4a_batch_profile_*): an event before every launch
   // of a frame and one after the last; in a graph these are event-record nodes,

@@ -79,42 +79,50 @@ __device__ __forceinline__ uint32_t finish_list(const SimParams& P, const DevSce
   return build_list<false>(P, w, i, pi, pred, cs, nullptr, nullptr, d.nbList, d.cap, P.h2);
 }
 
-// xsph (+ finalize) for scenes without surface tension. All threads reach the
-// stats tree, so there is no early return.
-__device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const DevScene& d, uint32_t tile,
-                                                   int substep) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
-  const bool act = li < P.n;
+// xsph (+ finalize) of scene-local particle li for scenes without surface
+// tension; returns its density and final velocity for the stats (zero past the
+// scene's end).
+__device__ __forceinline__ void xsph_finalize_particle(const SimParams& P, const DevScene& d, uint32_t li,
+                                                       float& rhoi, F3& vf) {
+  vf = {0.f, 0.f, 0.f};
+  rhoi = 0.0f;
+  if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
   const float4* __restrict__ pred = d.pred[L ^ ((int)P.iters & 1)];
   const float4* __restrict__ velIn = d.vel[L ^ 1];
   const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
-  F3 vf = {0.f, 0.f, 0.f};
-  float rhoi = 0.0f;
-  if (act) {
-    const float4 p4 = __ldg(&pred[i]);
-    const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
-    const RowWalk w(P, pi);
-    const uint32_t cap = d.cap;
-    const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
-    F3 acc = {0.f, 0.f, 0.f};
-    auto fluid = [&](uint32_t j, float4 q) {
-      const F3 rij = sub3(pi, xyz(q));
-      const float r2 = dot3(rij, rij);
-      if (r2 >= P.h2) return;  // in the skin of a reused list only
-      const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
-      acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
-    };
-    walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
-    const F3 corr = mul3(acc, P.xsphC);
-    vf = add3(vi, corr);
-    d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
-    d.pos[L][i] = p4;
-    if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
-    rhoi = __ldg(&d.density[i]);
-  }
-  if (substep == (int)P.subs - 1) block_stats(P, act, rhoi, vf, d.statsOut + 8 * P.slot);
+  const float4 p4 = __ldg(&pred[i]);
+  const F3 pi = xyz(p4), vi = xyz(__ldg(&velIn[i]));
+  const RowWalk w(P, pi);
+  const uint32_t cap = d.cap;
+  const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
+  F3 acc = {0.f, 0.f, 0.f};
+  auto fluid = [&](uint32_t j, float4 q) {
+    const F3 rij = sub3(pi, xyz(q));
+    const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2) return;  // in the skin of a reused list only
+    const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
+    acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+  };
+  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
+  const F3 corr = mul3(acc, P.xsphC);
+  vf = add3(vi, corr);
+  d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+  d.pos[L][i] = p4;
+  if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
+  rhoi = __ldg(&d.density[i]);
+}
+
+// Block form: 256-particle tile `tile`, with the stats tree after the last substep.
+// All threads reach the tree, so there is no early return.
+__device__ __forceinline__ void xsph_finalize_body(const SimParams& P, const DevScene& d, uint32_t tile,
+                                                   int substep) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  float rhoi;
+  F3 vf;
+  xsph_finalize_particle(P, d, li, rhoi, vf);
+  if (substep == (int)P.subs - 1) block_stats(P, li < P.n, rhoi, vf, d.statsOut + 8 * P.slot);
 }
 
 // xsph + normals (tension scenes): corr = xsphC * acc, normal = h * nacc.
@@ -150,51 +158,58 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   d.normal[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
 }
 
-// tension + finalize.
-__device__ __forceinline__ void tension_finalize_body(const SimParams& P, const DevScene& d,
-                                                      uint32_t tile, int substep) {
-  const uint32_t li = tile * kBlock + threadIdx.x;
-  const bool act = li < P.n;
+// tension + finalize of scene-local particle li; density and final velocity out
+// for the stats.
+__device__ __forceinline__ void tension_finalize_particle(const SimParams& P, const DevScene& d, uint32_t li,
+                                                          float& rhoi, F3& vf) {
+  vf = {0.f, 0.f, 0.f};
+  rhoi = 0.0f;
+  if (li >= P.n) return;
   const uint32_t i = P.pOff + li;
   const int L = (int)P.parity ^ 1;
   const float4* __restrict__ pred = d.pred[L ^ ((int)P.iters & 1)];
   const uint32_t* __restrict__ cs = d.cellStart + P.cOff;
   const uint32_t cap = d.cap;
-  F3 vf = {0.f, 0.f, 0.f};
-  float rhoi = 0.0f;
-  if (act) {
-    const float4 p4 = __ldg(&pred[i]);
-    const F3 pi = xyz(p4), ni = xyz(__ldg(&d.normal[i]));
-    rhoi = __ldg(&d.density[i]);
-    const RowWalk w(P, pi);
-    const uint32_t count = __ldg(&d.nbCount[i]);  // xsph+normals' list for these positions
-    F3 acc = {0.f, 0.f, 0.f};
-    auto fluid = [&](uint32_t j, float4 q) {
-      const F3 rij = sub3(pi, xyz(q));
-      const float r2 = dot3(rij, rij);
-      if (r2 >= P.h2 || r2 < 1.0e-12f) return;
-      const float rr = sqrtf(r2);
-      const float hrr = P.h - rr;
-      const float k = hrr * hrr * hrr * rr * rr * rr;
-      float cw = P.cohes * (2.0f * k - P.cohesTerm);
-      if (2.0f * rr > P.h) cw = P.cohes * k;
-      const float sCoh = -P.tension * P.mass * cw / rr;
-      const F3 fCoh = mul3(rij, sCoh);
-      const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
-      const float wgt = 2.0f * P.rho0 / (rhoi + __ldg(&d.density[j]));
-      acc = fma3(wgt, add3(fCoh, fCurv), acc);
-    };
-    walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
-    const float4 c0 = d.corr[i];
-    const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
-    d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);
-    const F3 vi = xyz(__ldg(&d.vel[L ^ 1][i]));
-    vf = add3(vi, cf);
-    d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
-    d.pos[L][i] = p4;
-    if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
-  }
-  if (substep == (int)P.subs - 1) block_stats(P, act, rhoi, vf, d.statsOut + 8 * P.slot);
+  const float4 p4 = __ldg(&pred[i]);
+  const F3 pi = xyz(p4), ni = xyz(__ldg(&d.normal[i]));
+  const float rho = __ldg(&d.density[i]);
+  const RowWalk w(P, pi);
+  const uint32_t count = __ldg(&d.nbCount[i]);  // xsph+normals' list for these positions
+  F3 acc = {0.f, 0.f, 0.f};
+  auto fluid = [&](uint32_t j, float4 q) {
+    const F3 rij = sub3(pi, xyz(q));
+    const float r2 = dot3(rij, rij);
+    if (r2 >= P.h2 || r2 < 1.0e-12f) return;
+    const float rr = sqrtf(r2);
+    const float hrr = P.h - rr;
+    const float k = hrr * hrr * hrr * rr * rr * rr;
+    float cw = P.cohes * (2.0f * k - P.cohesTerm);
+    if (2.0f * rr > P.h) cw = P.cohes * k;
+    const float sCoh = -P.tension * P.mass * cw / rr;
+    const F3 fCoh = mul3(rij, sCoh);
+    const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
+    const float wgt = 2.0f * P.rho0 / (rho + __ldg(&d.density[j]));
+    acc = fma3(wgt, add3(fCoh, fCurv), acc);
+  };
+  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
+  const float4 c0 = d.corr[i];
+  const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
+  d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);
+  const F3 vi = xyz(__ldg(&d.vel[L ^ 1][i]));
+  vf = add3(vi, cf);
+  d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
+  d.pos[L][i] = p4;
+  if ((P.iters & 1u) != 0u) d.pred[L][i] = p4;
+  rhoi = rho;
+}
+
+__device__ __forceinline__ void tension_finalize_body(const SimParams& P, const DevScene& d,
+                                                      uint32_t tile, int substep) {
+  const uint32_t li = tile * kBlock + threadIdx.x;
+  float rhoi;
+  F3 vf;
+  tension_finalize_particle(P, d, li, rhoi, vf);
+  if (substep == (int)P.subs - 1) block_stats(P, li < P.n, rhoi, vf, d.statsOut + 8 * P.slot);
 }
 
 __global__ void __launch_bounds__(kBlock, 5) k_xsph_finalize(const __grid_constant__ SimParams P,

@@ -246,18 +246,21 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
   return V * 1.00001f <= P.skinHalf;
 }
 
-// Phase 2 over a list of `count` entries: fluid(j, q) for a fluid entry with
-// q = fsrc[j], bound(k, q) for a boundary sample with q = bsrc[k] (bsrc may be
-// null when the pass skips boundary samples). With PF the walk is software
-// pipelined two entries deep: while entry k is processed, the gather of entry k+1
-// and the list load of entry k+2 are already in flight, so the latency of the
-// dependent list-then-gather chain overlaps the arithmetic of the current pair.
-// The gather address is chosen without a branch (a boundary entry of a pass
-// without boundary samples loads the particle's own fsrc[i], which is unused).
-template <bool PF = true, class FFluid, class FBound>
+// Phase 2 over a list of `count` entries: pair(idx, q, isBound) for every entry,
+// with q = fsrc[idx] for a fluid entry and q = bsrc[idx] for a boundary sample
+// (bsrc may be null when the pass skips boundary samples; their calls then carry
+// an unused q). One callback for both kinds, so that a pass can treat them on one
+// path with per-lane selects where that is cheaper than running both paths in
+// turn for a warp whose lanes hold entries of both kinds. With PF the walk is
+// software pipelined two entries deep: while entry k is processed, the gather of
+// entry k+1 and the list load of entry k+2 are already in flight, so the latency
+// of the dependent list-then-gather chain overlaps the arithmetic of the current
+// pair. The gather address is chosen without a branch (a boundary entry of a pass
+// without boundary samples loads the particle's own fsrc[i]).
+template <bool PF = true, class FPair>
 __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
                                           uint32_t count, const float4* __restrict__ fsrc,
-                                          const float4* __restrict__ bsrc, FFluid&& fluid, FBound&& bound) {
+                                          const float4* __restrict__ bsrc, FPair&& pair) {
   count &= kCountMask;
   if (count == 0u) return;
   auto fetch = [&](uint32_t e) {
@@ -266,13 +269,7 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uin
     const uint32_t idx = b ? (bsrc ? (e & ~kBoundTag) : i) : e;
     return __ldg(src + idx);
   };
-  auto visit = [&](uint32_t cur, float4 q) {
-    if (cur & kBoundTag) {
-      bound(cur & ~kBoundTag, q);
-    } else {
-      fluid(cur, q);
-    }
-  };
+  auto visit = [&](uint32_t cur, float4 q) { pair(cur & ~kBoundTag, q, (cur & kBoundTag) != 0u); };
   const uint32_t* __restrict__ at = list + i;  // entry k of the particle at list[k * cap + i]
   uint32_t e0 = __ldg(at);
   if constexpr (PF) {
@@ -347,7 +344,9 @@ __device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWal
                                                 uint32_t cap, uint32_t count, FFluid&& fluid) {
   auto none = [](uint32_t, float4) {};
   if (count != kListOverflow) {
-    walk_list(list, cap, i, count, pred, nullptr, fluid, none);
+    walk_list(list, cap, i, count, pred, nullptr, [&](uint32_t j, float4 q, bool isBound) {
+      if (!isBound) fluid(j, q);
+    });
   } else {
     walk_direct<false>(P, w, pi, i, pred, cs, nullptr, nullptr, fluid, none);
   }

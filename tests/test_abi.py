@@ -51,7 +51,8 @@ def test_struct_layouts_match_c_compiler(tmp_path):
                "p4a_server_config": _abi.ServerConfig, "p4a_completion": _abi.Completion,
                "p4a_server_stats": _abi.ServerStats, "p4a_mesh_params": _abi.MeshParams,
                "p4a_mesh_info": _abi.MeshInfo, "p4a_ssfr_params": _abi.SsfrParams,
-               "p4a_ssfr_info": _abi.SsfrInfo, "p4a_ray_params": _abi.RayParams}
+               "p4a_ssfr_info": _abi.SsfrInfo, "p4a_ray_params": _abi.RayParams,
+               "p4a_batch_io": _abi.BatchIO, "p4a_hose": _abi.Hose}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "p4a.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')

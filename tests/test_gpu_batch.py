@@ -116,3 +116,76 @@ def test_admission_rejects_when_full():
         b.add_scene(p, sc)
     assert e.value.status == 5
     assert b.usage()["live_scenes"] == 2
+
+
+@pytest.mark.parametrize("groups", [1, 2, 0, 7])
+def test_step_io_equals_write_step_read(groups):
+    """p4a_batch_step_io (host inputs, the scenes in `groups` frames with the copies
+    on their own streams) gives the bits of write_async + step + read_async."""
+    import torch
+    scenes = mixed_scenes()
+    b = Batch(max_particles=400_000, max_cells=800_000, max_scenes=16)
+    add = lambda p, sc: b.add_preset(p) if sc is None else b.add_scene(p, sc)
+    a_ids = [add(p, sc) for p, sc in scenes]
+    b_ids = [add(p, sc) for p, sc in scenes]
+    ns = [b.info(s)["n"] for s in a_ids]
+    rng = np.random.default_rng(5)
+    pin = lambda n: torch.zeros(n * 4, dtype=torch.float32, pin_memory=True)
+    inputs = []
+    for s, n in zip(a_ids, ns):
+        pos, vel = b.read(s, "pos")[:n].copy(), b.read(s, "vel")[:n].copy()
+        pos[:, :3] += rng.uniform(-2e-4, 2e-4, (n, 3)).astype(np.float32)
+        vel[:, :3] += rng.uniform(-0.3, 0.3, (n, 3)).astype(np.float32)
+        inputs.append((torch.from_numpy(pos.reshape(-1)).pin_memory(), torch.from_numpy(vel.reshape(-1)).pin_memory()))
+    outs_a = [(pin(n), pin(n)) for n in ns]
+    outs_b = [(pin(n), pin(n)) for n in ns]
+    for f, fd in enumerate([1 / 60, 1 / 45, 1 / 60]):
+        # frame 0 from the perturbed inputs, later frames from the previous outputs;
+        # velocities only in frame 1 (pos_in None), nothing read back in frame 2 for
+        # the odd scenes
+        src_a = inputs if f == 0 else outs_a
+        src_b = inputs if f == 0 else outs_b
+        if f > 0:
+            src_a = [(p.clone().pin_memory(), v.clone().pin_memory()) for p, v in src_a]
+            src_b = [(p.clone().pin_memory(), v.clone().pin_memory()) for p, v in src_b]
+        for k, (s, n) in enumerate(zip(a_ids, ns)):
+            if f != 1:
+                b.write_async(s, "pos", src_a[k][0].data_ptr(), n * 16)
+            b.write_async(s, "vel", src_a[k][1].data_ptr(), n * 16)
+        b.step(a_ids, fd)
+        for k, (s, n) in enumerate(zip(a_ids, ns)):
+            if f == 2 and k % 2:
+                continue
+            b.read_async(s, "pos", outs_a[k][0].data_ptr(), n * 16)
+            b.read_async(s, "vel", outs_a[k][1].data_ptr(), n * 16)
+        entries = []
+        for k, (s, n) in enumerate(zip(b_ids, ns)):
+            skip = f == 2 and k % 2
+            entries.append((s, None if f == 1 else src_b[k][0].data_ptr(), src_b[k][1].data_ptr(),
+                            None if skip else outs_b[k][0].data_ptr(), None if skip else outs_b[k][1].data_ptr()))
+        b.step_io(entries, fd, groups)
+        b.synchronize()
+        for k in range(len(ns)):
+            assert torch.equal(outs_a[k][0], outs_b[k][0]) and torch.equal(outs_a[k][1], outs_b[k][1]), (f, k)
+    for sa, sb in zip(a_ids, b_ids):
+        n = b.info(sa)["n"]
+        assert b.info(sa)["parity"] == b.info(sb)["parity"]
+        for name in NAMES:
+            assert np.array_equal(b.read(sa, name)[:n], b.read(sb, name)[:n]), name
+        assert b.stats(sa)["raw"] == b.stats(sb)["raw"]
+
+
+def test_step_io_rejects_bad_lists():
+    p, sc = configs.dam_break_32k(side=8)
+    b = Batch(max_particles=20_000, max_cells=100_000, max_scenes=4)
+    s = b.add_scene(p, sc)
+    with pytest.raises(P4AError):
+        b.step_io([(s, None, None, None, None), (s, None, None, None, None)], 1 / 60)
+    with pytest.raises(P4AError):
+        b.step_io([(s + 1, None, None, None, None)], 1 / 60)
+    with pytest.raises(P4AError):
+        b.step_io([(s, None, None, None, None)], 1 / 60, groups=-1)
+    b.step_io([], 1 / 60)
+    b.step_io([(s, None, None, None, None)], 1 / 60, groups=3)  # more groups than scenes
+    b.synchronize()
+    assert b.info(s)["sim_time"] > 0
