@@ -4,18 +4,19 @@ The library compiles lambda, delta, xsph+normals and the anisotropic pass in
 several launch shapes (threads per block x minimum resident blocks per SM, i.e.
 particles per block and the register budget); all shapes compute the same bits.
 For every size bucket this steps a seeded dam-break scene of that size (the
-served workload's scenes, with surface tension on so the normals pass runs) with
-each shape of one kernel in turn and reads that kernel's device time per launch
-from the library's per-kernel CUDA events. The fastest shape per (kernel,
-bucket) goes into the library's table (p4a_tune_set) and into tuning.json next
-to this file, which the library applies when it is loaded.
+served workload's scenes, with surface tension on so the normals pass runs),
+frame by frame with the shapes of one kernel taking turns, and reads that
+kernel's device time per launch from the library's per-kernel CUDA events. The
+fastest shape per (kernel, bucket) goes into the library's table (p4a_tune_set)
+and into tuning.json next to this file, which the library applies when it is
+loaded.
 
 The batched launches of lambda, delta and xsph+normals (p4a_batch_step) have tables
 of their own, keyed by the frame's total particles: their register budget differs
 from the plain launches' (each warp also carries its work-item state). For each
 batched bucket this admits a seeded mix of scenes (configs.batched_mix with that
-many scenes) into one Batch and times each shape on whole batched frames with the
-batch's per-kernel events.
+many scenes) into one Batch and times the shapes, taking turns, on whole batched
+frames with the batch's per-kernel events.
 
     python -m particles4all_b200.autotune            # on the GPU: measure, write tuning.json
 """
@@ -78,21 +79,37 @@ def _scene_sim(n):
     return s, default_aniso()
 
 
-def measure(sim, aniso, frames=6, warmup=2):
-    """Device ms per launch of every kernel over `frames` frames (step + aniso)."""
-    for _ in range(warmup):
-        sim.step(1 / 60)
-        sim.aniso(aniso)
-    sim.synchronize()
+def interleaved(step, profile, L, kernel, name, variants, rounds):
+    """Device ms per launch of kernel `name` for each shape in `variants`: every
+    round steps one frame with each shape in turn (the order rotated per round),
+    so that all shapes are timed over the same stretch of the scene's motion
+    (later frames of a settling scene cost more, and timing the shapes one after
+    another favoured the ones timed first)."""
+    ms = [0.0] * len(variants)
+    launches = [0] * len(variants)
+    for r in range(rounds):
+        order = list(range(len(variants)))
+        order = order[r % len(order):] + order[:r % len(order)]
+        for q in order:
+            L.p4a_tune_clear(kernel)
+            L.p4a_tune_set(kernel, 1 << 40, variants[q])
+            prof = profile(step)
+            if name in prof:
+                ms[q] += prof[name][0]
+                launches[q] += prof[name][1]
+    return [m / max(1, n) for m, n in zip(ms, launches)]
+
+
+def _sim_profile(sim, aniso):
+    """(run, step) for interleaved(): one frame of the Sim (step + aniso) and its
+    per-kernel profile."""
+    def run(step):
+        sim.profile_reset()
+        step()
+        sim.synchronize()
+        return sim.profile_read()
     sim.profile(True)
-    sim.profile_reset()
-    for _ in range(frames):
-        sim.step(1 / 60)
-        sim.aniso(aniso)
-    sim.synchronize()
-    prof = sim.profile_read()
-    sim.profile(False)
-    return {k: ms / max(1, n) for k, (ms, n) in prof.items()}
+    return run, lambda: (sim.step(1 / 60), sim.aniso(aniso))
 
 
 def _mix_batch(scenes):
@@ -104,19 +121,16 @@ def _mix_batch(scenes):
     return b, ids, sum(sc["pos"].shape[0] for _, sc in mix)
 
 
-def measure_batch(b, ids, frames=4, warmup=2):
-    """Device ms per launch of every batched kernel over `frames` frames."""
-    for _ in range(warmup):
-        b.step(ids, 1 / 60)
-    b.synchronize()
+def _batch_profile(b, ids):
+    """(run, step) for interleaved(): one batched frame of all scenes and its
+    per-kernel profile."""
+    def run(step):
+        b.profile_reset()
+        step()
+        b.synchronize()
+        return b.profile_read()
     b.profile(True)
-    b.profile_reset()
-    for _ in range(frames):
-        b.step(ids, 1 / 60)
-    b.synchronize()
-    prof = b.profile_read()
-    b.profile(False)
-    return {k: ms / max(1, n) for k, (ms, n) in prof.items()}
+    return run, lambda: b.step(ids, 1 / 60)
 
 
 def tune_batched(result, L, buckets=BATCH_BUCKETS, frames=4, log=print):
@@ -126,13 +140,13 @@ def tune_batched(result, L, buckets=BATCH_BUCKETS, frames=4, log=print):
         result["shapes"][name] = shapes(L, BATCHED[name])
     for bound, scenes in buckets:
         b, ids, total = _mix_batch(scenes)
+        for _ in range(2):
+            b.step(ids, 1 / 60)
+        run, step = _batch_profile(b, ids)
         per = {}
         for name, k in BATCHED.items():
-            times = []
-            for v in range(len(result["shapes"][name])):
-                L.p4a_tune_clear(k)
-                L.p4a_tune_set(k, 1 << 40, v)
-                times.append(measure_batch(b, ids, frames)[PROFILE_NAME[name]])
+            variants = list(range(len(result["shapes"][name])))
+            times = interleaved(step, run, L, k, PROFILE_NAME[name], variants, frames)
             best = min(range(len(times)), key=times.__getitem__)
             L.p4a_tune_clear(k)
             L.p4a_tune_set(k, 1 << 40, best)
@@ -155,14 +169,14 @@ def tune(buckets=BUCKETS, frames=6, path=DEFAULT_PATH, log=print, batch_buckets=
     for bound, n in buckets:
         sim, aniso = _scene_sim(n)
         real_n = sim.info()["n"]
+        for _ in range(2):
+            sim.step(1 / 60)
+            sim.aniso(aniso)
+        run, step = _sim_profile(sim, aniso)
         per = {}
         for name, k in KERNELS.items():
-            times = []
-            for v in range(len(result["shapes"][name])):
-                L.p4a_tune_clear(k)
-                L.p4a_tune_set(k, 1 << 40, v)
-                t = measure(sim, aniso, frames)[name]
-                times.append(t)
+            variants = list(range(len(result["shapes"][name])))
+            times = interleaved(step, run, L, k, name, variants, frames)
             best = min(range(len(times)), key=times.__getitem__)
             L.p4a_tune_clear(k)
             L.p4a_tune_set(k, 1 << 40, best)
