@@ -234,13 +234,23 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
   const I3 a = cell_of(P, xyz(__ldg(&d.nbRef[i])));
   const uint32_t ac = cell_index(P, a);
   float V = __ldg(&vNow[ac]) + (vB ? __ldg(&vB[ac]) : 0.0f);
-#pragma unroll 1
+  // The 27 cells with every load independent of the others (a loop over rows with
+  // a data-dependent skip issued them row by row, one memory latency per row): a
+  // row outside the grid reads the particle's own row and counts as 0, and x is
+  // clamped into the grid, which repeats x0 or x1 at an edge. The slots hold
+  // displacement lengths, so neither changes the maximum.
+  const int gx = P.gridDim[0], gy = P.gridDim[1], gz = P.gridDim[2];
+  const int ownRow = (w.c.z * gy + w.c.y) * gx;
+#pragma unroll
   for (int r = 0; r < kRows; r++) {
-    const int rb = w.row_base(P, r);
-    if (rb < 0) continue;
-    for (int x = w.x0; x <= w.x1; x++) {
+    const int z = w.c.z + r / 3 - 1, y = w.c.y + r % 3 - 1;
+    const bool in = z >= 0 && z < gz && y >= 0 && y < gy;
+    const int rb = in ? (z * gy + y) * gx : ownRow;
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++) {
+      const int x = min(max(w.c.x + dx, 0), gx - 1);
       const float v = __ldg(&vNow[rb + x]) + (vB ? __ldg(&vB[rb + x]) : 0.0f);
-      V = fmaxf(V, v);
+      V = fmaxf(V, in ? v : 0.0f);
     }
   }
   return V * 1.00001f <= P.skinHalf;
