@@ -290,6 +290,7 @@ void pack_params(p4a_sim* s, double dt) {
   F.slot = 0;
   F.skinH2 = (float)((h + kSkin * h) * (h + kSkin * h));
   F.skinHalf = (float)((kSkin * h - 1e-4 * h) * 0.5);
+  F.volSpiky = F.volume * F.spikyGrad;
 }
 
 uint32_t next_epoch(p4a_sim* s) {

@@ -121,6 +121,7 @@ void pack(BScene& s, double dt, int slot) {
   F.slot = (uint32_t)slot;
   F.skinH2 = (float)((h + kSkin * h) * (h + kSkin * h));
   F.skinHalf = (float)((kSkin * h - 1e-4 * h) * 0.5);
+  F.volSpiky = F.volume * F.spikyGrad;
 }
 
 // Kinds of the launches of a frame, in the order a substep issues them.

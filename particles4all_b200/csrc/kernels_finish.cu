@@ -102,7 +102,8 @@ __device__ __forceinline__ void xsph_finalize_particle(const SimParams& P, const
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
-    const float f = P.mass * poly6(P, r2) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
+    const float t = P.h2 - r2;
+    const float f = P.mass * (P.poly6 * t * t * t) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
     acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
   };
   walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
@@ -145,7 +146,8 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
     const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
-    const float f = P.mass * poly6(P, r2) / dj;
+    const float t = P.h2 - r2;  // r2 < h2 here: poly6 without its range test
+    const float f = P.mass * (P.poly6 * t * t * t) / dj;
     acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
     if (r2 < 1.0e-12f) return;
     const float rr = sqrtf(r2);

@@ -63,11 +63,12 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of the list only
-    rho = fmaf(P.mass, poly6(P, r2), rho);
+    const float t = P.h2 - r2;
+    rho = fmaf(P.mass, P.poly6 * t * t * t, rho);  // poly6 within h
     if (r2 > 1.0e-12f) {
       const float rr = sqrtf(r2);
       const float hr = P.h - rr;
-      const float s = P.volume * P.spikyGrad * hr * hr / rr;
+      const float s = P.volSpiky * hr * hr / rr;
       const F3 g = mul3(rij, s);
       gradSum = add3(gradSum, g);
       sumGrad2 = sumGrad2 + dot3(g, g);
@@ -78,7 +79,8 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2 || r2 < 1.0e-12f) return;
     const float psi = __ldg(&d.bpsi[k]);
-    rho = fmaf(psi, poly6(P, r2), rho);
+    const float t = P.h2 - r2;
+    rho = fmaf(psi, P.poly6 * t * t * t, rho);
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float s = psi * P.invRho0 * P.spikyGrad * hr * hr / rr;
@@ -103,12 +105,13 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
         const float r2 = dot3(rij, rij);
         if (r2 >= P.h2 || (isB && r2 < 1.0e-12f)) return;
         const float psi = isB ? __ldg(&d.bpsi[k]) : 0.0f;
-        rho = fmaf(isB ? psi : P.mass, poly6(P, r2), rho);
+        const float t = P.h2 - r2;
+        rho = fmaf(isB ? psi : P.mass, P.poly6 * t * t * t, rho);
         if (isB || r2 > 1.0e-12f) {
           const float rr = sqrtf(r2);
           const float hr = P.h - rr;
-          const float c0 = isB ? psi * P.invRho0 : P.volume;
-          const float s = c0 * P.spikyGrad * hr * hr / rr;
+          const float c0 = isB ? psi * P.invRho0 * P.spikyGrad : P.volSpiky;
+          const float s = c0 * hr * hr / rr;
           const F3 g = mul3(rij, s);
           const F3 gf = add3(gradSum, g), gb = fma3(s, rij, gradSum);
           gradSum = isB ? gb : gf;

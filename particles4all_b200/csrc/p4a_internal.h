@@ -53,6 +53,8 @@ struct SimParams {
   // neighbour masks reused across Jacobi iterations (kernels_solve.cu)
   float skinH2;     // (h + skin)^2: radius of the reused candidate masks
   float skinHalf;   // reuse while the displacement bound stays <= this
+  float volSpiky;   // volume * spikyGrad rounded to float: the first product of
+                    // lambda's fluid gradient term, formed once per substep
 };
 
 // Jacobi iterations whose displacement bounds are tracked per substep; later
