@@ -100,7 +100,7 @@ __device__ __forceinline__ void lambda_body(const SimParams& P, const DevScene& 
       // than the branches above in the plain launches (5-9 % per launch where
       // warps mix wall and interior particles), slower in the pipelined walk of
       // the batched ones, whose registers it squeezes.
-      walk_list<false>(d.nbList, cap, i, count, pred, d.bpos, [&](uint32_t k, float4 q, bool isB) {
+      walk_list<false, kFetchBound>(d.nbList, cap, i, count, pred, d.bpos, [&](uint32_t k, float4 q, bool isB) {
         const F3 rij = sub3(pi, xyz(q));
         const float r2 = dot3(rij, rij);
         if (r2 >= P.h2 || (isB && r2 < 1.0e-12f)) return;
@@ -176,7 +176,7 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
     dB = fma3(coef, rij, dB);
   };
   if (count != kListOverflow) {
-    walk_list(d.nbList, cap, i, count, pl, d.bpos, [&](uint32_t k, float4 q, bool isB) {
+    walk_list<true, kFetchBound>(d.nbList, cap, i, count, pl, d.bpos, [&](uint32_t k, float4 q, bool isB) {
       if (isB) {
         bound(k, q);
       } else {

@@ -258,16 +258,19 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
 
 // Phase 2 over a list of `count` entries: pair(idx, q, isBound) for every entry,
 // with q = fsrc[idx] for a fluid entry and q = bsrc[idx] for a boundary sample
-// (bsrc may be null when the pass skips boundary samples; their calls then carry
-// an unused q). One callback for both kinds, so that a pass can treat them on one
-// path with per-lane selects where that is cheaper than running both paths in
-// turn for a warp whose lanes hold entries of both kinds. With PF the walk is
+// (for a pass that skips boundary samples their calls carry an unused q). One callback for both kinds, so that a pass can treat them on one path with
+// per-lane selects where that is cheaper than running both paths in turn for a
+// warp whose lanes hold entries of both kinds. With PF the walk is
 // software pipelined two entries deep: while entry k is processed, the gather of
 // entry k+1 and the list load of entry k+2 are already in flight, so the latency
 // of the dependent list-then-gather chain overlaps the arithmetic of the current
-// pair. The gather address is chosen without a branch (a boundary entry of a pass
-// without boundary samples loads the particle's own fsrc[i]).
-template <bool PF = true, class FPair>
+// pair. The gather address is chosen without a branch, in one of three forms
+// (all give the same q; which is fastest depends on the kernel's register budget):
+// kFetchBound for a pass that reads boundary samples from bsrc, kFetchFluid for
+// one that skips them (a boundary entry loads the particle's own fsrc[i]), and
+// kFetchAny that decides by bsrc != null at run time.
+enum FetchForm { kFetchAny, kFetchBound, kFetchFluid };
+template <bool PF = true, FetchForm FORM = kFetchAny, class FPair>
 __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
                                           uint32_t count, const float4* __restrict__ fsrc,
                                           const float4* __restrict__ bsrc, FPair&& pair) {
@@ -275,9 +278,15 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uin
   if (count == 0u) return;
   auto fetch = [&](uint32_t e) {
     const bool b = (e & kBoundTag) != 0u;
-    const float4* src = b && bsrc ? bsrc : fsrc;
-    const uint32_t idx = b ? (bsrc ? (e & ~kBoundTag) : i) : e;
-    return __ldg(src + idx);
+    if constexpr (FORM == kFetchBound) {
+      return __ldg((b ? bsrc : fsrc) + (e & ~kBoundTag));  // a fluid entry has no tag bit
+    } else if constexpr (FORM == kFetchFluid) {
+      return __ldg(fsrc + (b ? i : e));
+    } else {
+      const float4* src = b && bsrc ? bsrc : fsrc;
+      const uint32_t idx = b ? (bsrc ? (e & ~kBoundTag) : i) : e;
+      return __ldg(src + idx);
+    }
   };
   auto visit = [&](uint32_t cur, float4 q) { pair(cur & ~kBoundTag, q, (cur & kBoundTag) != 0u); };
   const uint32_t* __restrict__ at = list + i;  // entry k of the particle at list[k * cap + i]
@@ -354,7 +363,7 @@ __device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWal
                                                 uint32_t cap, uint32_t count, FFluid&& fluid) {
   auto none = [](uint32_t, float4) {};
   if (count != kListOverflow) {
-    walk_list(list, cap, i, count, pred, nullptr, [&](uint32_t j, float4 q, bool isBound) {
+    walk_list<true, kFetchFluid>(list, cap, i, count, pred, nullptr, [&](uint32_t j, float4 q, bool isBound) {
       if (!isBound) fluid(j, q);
     });
   } else {
