@@ -380,7 +380,8 @@ int reset_common(p4a_sim* s) {
       (rc = dalloc(s, L, &s->d.errorWord, 4)) || (rc = dalloc(s, L, &s->d.nbList, cap * kListCap)) ||
       (rc = dalloc(s, L, &s->d.nbCount, cap)) || (rc = dalloc(s, L, &s->d.nbCell, cap)) ||
       (rc = dalloc(s, L, &s->d.disp, kDispSlots)) || (rc = dalloc(s, L, &s->d.nbRef, cap)) ||
-      (rc = dalloc(s, L, &s->d.predLam, cap)))
+      (rc = dalloc(s, L, &s->d.predLam, cap)) || (rc = dalloc(s, L, &s->d.velRho, cap)) ||
+      (rc = dalloc(s, L, &s->d.normRho, cap)))
     return rc;
   s->d.cap = (uint32_t)cap;
   if ((rc = alloc_cells(s))) return rc;

@@ -792,6 +792,7 @@ int alloc_arenas(p4a_batch* b) {
        (rc = balloc(b, &d.unordered, P)) || (rc = balloc(b, &d.nbList, P * kListCap)) || (rc = balloc(b, &d.nbCount, P)) ||
        (rc = balloc(b, &d.nbCell, P)) || (rc = balloc(b, &d.disp, (int64_t)cfg->max_scenes * kDispSlots)) ||
        (rc = balloc(b, &d.cellDisp, (int64_t)kDispSlots * Cc)) || (rc = balloc(b, &d.nbRef, P)) || (rc = balloc(b, &d.predLam, P)) ||
+       (rc = balloc(b, &d.velRho, P)) || (rc = balloc(b, &d.normRho, P)) ||
        (rc = balloc(b, &d.cellCount, Cc)) ||
        (rc = balloc(b, &d.cellStart, Cc)) || (rc = balloc(b, &d.bcellStart, Cc)) ||
        (rc = balloc(b, &d.scanState, b->scanTilesCap)) || (rc = balloc(b, &d.scanTicket, 4)) ||

@@ -98,15 +98,16 @@ __device__ __forceinline__ void xsph_finalize_particle(const SimParams& P, const
   const uint32_t cap = d.cap;
   const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
   F3 acc = {0.f, 0.f, 0.f};
-  auto fluid = [&](uint32_t j, float4 q) {
+  // g = (velFromPos, density) of neighbour j
+  auto fluid = [&](uint32_t, float4 q, float4 g) {
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
     const float t = P.h2 - r2;
-    const float f = P.mass * (P.poly6 * t * t * t) / fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
-    acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+    const float f = P.mass * (P.poly6 * t * t * t) / fmaxf(g.w, 0.5f * P.rho0);
+    acc = fma3(f, sub3(xyz(g), vi), acc);
   };
-  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
+  walk_neighbours2(P, w, i, pi, pred, d.velRho, cs, d.nbList, cap, count, fluid);
   const F3 corr = mul3(acc, P.xsphC);
   vf = add3(vi, corr);
   d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
@@ -141,23 +142,26 @@ __device__ __forceinline__ void xsph_normals_body(const SimParams& P, const DevS
   const uint32_t count = finish_list(P, d, w, i, pi, pred, cs);
   d.nbCount[i] = count;
   F3 acc = {0.f, 0.f, 0.f}, nacc = {0.f, 0.f, 0.f};
-  auto fluid = [&](uint32_t j, float4 q) {
+  // g = (velFromPos, density) of neighbour j
+  auto fluid = [&](uint32_t, float4 q, float4 g) {
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2) return;  // in the skin of a reused list only
-    const float dj = fmaxf(__ldg(&d.density[j]), 0.5f * P.rho0);
+    const float dj = fmaxf(g.w, 0.5f * P.rho0);
     const float t = P.h2 - r2;  // r2 < h2 here: poly6 without its range test
     const float f = P.mass * (P.poly6 * t * t * t) / dj;
-    acc = fma3(f, sub3(xyz(__ldg(&velIn[j])), vi), acc);
+    acc = fma3(f, sub3(xyz(g), vi), acc);
     if (r2 < 1.0e-12f) return;
     const float rr = sqrtf(r2);
     const float hr = P.h - rr;
     const float coef = (P.mass / dj) * (P.spikyGrad * hr * hr / rr);
     nacc = fma3(coef, rij, nacc);
   };
-  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
+  walk_neighbours2(P, w, i, pi, pred, d.velRho, cs, d.nbList, cap, count, fluid);
   d.corr[i] = make_float4(P.xsphC * acc.x, P.xsphC * acc.y, P.xsphC * acc.z, 0.0f);
-  d.normal[i] = make_float4(P.h * nacc.x, P.h * nacc.y, P.h * nacc.z, 0.0f);
+  const F3 nrm = {P.h * nacc.x, P.h * nacc.y, P.h * nacc.z};
+  d.normal[i] = make_float4(nrm.x, nrm.y, nrm.z, 0.0f);
+  d.normRho[i] = make_float4(nrm.x, nrm.y, nrm.z, __ldg(&d.density[i]));  // for tension's gathers
 }
 
 // tension + finalize of scene-local particle li; density and final velocity out
@@ -178,7 +182,8 @@ __device__ __forceinline__ void tension_finalize_particle(const SimParams& P, co
   const RowWalk w(P, pi);
   const uint32_t count = __ldg(&d.nbCount[i]);  // xsph+normals' list for these positions
   F3 acc = {0.f, 0.f, 0.f};
-  auto fluid = [&](uint32_t j, float4 q) {
+  // g = (normal, density) of neighbour j
+  auto fluid = [&](uint32_t, float4 q, float4 g) {
     const F3 rij = sub3(pi, xyz(q));
     const float r2 = dot3(rij, rij);
     if (r2 >= P.h2 || r2 < 1.0e-12f) return;
@@ -189,11 +194,11 @@ __device__ __forceinline__ void tension_finalize_particle(const SimParams& P, co
     if (2.0f * rr > P.h) cw = P.cohes * k;
     const float sCoh = -P.tension * P.mass * cw / rr;
     const F3 fCoh = mul3(rij, sCoh);
-    const F3 fCurv = mul3(sub3(ni, xyz(__ldg(&d.normal[j]))), -P.tension);
-    const float wgt = 2.0f * P.rho0 / (rho + __ldg(&d.density[j]));
+    const F3 fCurv = mul3(sub3(ni, xyz(g)), -P.tension);
+    const float wgt = 2.0f * P.rho0 / (rho + g.w);
     acc = fma3(wgt, add3(fCoh, fCurv), acc);
   };
-  walk_neighbours(P, w, i, pi, pred, cs, d.nbList, cap, count, fluid);
+  walk_neighbours2(P, w, i, pi, pred, d.normRho, cs, d.nbList, cap, count, fluid);
   const float4 c0 = d.corr[i];
   const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
   d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);

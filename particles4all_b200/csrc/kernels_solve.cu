@@ -202,8 +202,9 @@ __device__ __forceinline__ void delta_body(const SimParams& P, const DevScene& d
   }
   if (it == (int)P.iters - 1) {  // velFromPos into the non-live velocity copy
     const float4 p0 = __ldg(&d.pos[L][i]);
-    d.vel[L ^ 1][i] = make_float4((o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt,
-                                  (o.z - p0.z) * P.invDt, 0.0f);
+    const F3 v = {(o.x - p0.x) * P.invDt, (o.y - p0.y) * P.invDt, (o.z - p0.z) * P.invDt};
+    d.vel[L ^ 1][i] = make_float4(v.x, v.y, v.z, 0.0f);
+    d.velRho[i] = make_float4(v.x, v.y, v.z, __ldg(&d.density[i]));
   }
 }
 

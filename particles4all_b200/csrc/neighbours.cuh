@@ -264,12 +264,12 @@ __device__ __forceinline__ bool list_reusable(const SimParams& P, const DevScene
 // software pipelined two entries deep: while entry k is processed, the gather of
 // entry k+1 and the list load of entry k+2 are already in flight, so the latency
 // of the dependent list-then-gather chain overlaps the arithmetic of the current
-// pair. The gather address is chosen without a branch, in one of three forms
-// (all give the same q; which is fastest depends on the kernel's register budget):
-// kFetchBound for a pass that reads boundary samples from bsrc, kFetchFluid for
-// one that skips them (a boundary entry loads the particle's own fsrc[i]), and
-// kFetchAny that decides by bsrc != null at run time.
-enum FetchForm { kFetchAny, kFetchBound, kFetchFluid };
+// pair. The gather address is chosen without a branch, in one of two forms (both
+// give the same q; which is faster depends on the kernel's register budget):
+// kFetchBound for a pass that reads boundary samples from bsrc, and kFetchAny that
+// decides by bsrc != null at run time (a boundary entry of a pass without boundary
+// samples loads the particle's own fsrc[i]).
+enum FetchForm { kFetchAny, kFetchBound };
 template <bool PF = true, FetchForm FORM = kFetchAny, class FPair>
 __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uint32_t cap, uint32_t i,
                                           uint32_t count, const float4* __restrict__ fsrc,
@@ -280,8 +280,6 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uin
     const bool b = (e & kBoundTag) != 0u;
     if constexpr (FORM == kFetchBound) {
       return __ldg((b ? bsrc : fsrc) + (e & ~kBoundTag));  // a fluid entry has no tag bit
-    } else if constexpr (FORM == kFetchFluid) {
-      return __ldg(fsrc + (b ? i : e));
     } else {
       const float4* src = b && bsrc ? bsrc : fsrc;
       const uint32_t idx = b ? (bsrc ? (e & ~kBoundTag) : i) : e;
@@ -354,20 +352,45 @@ __device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w
   }
 }
 
-// Fluid-only passes: the list walk (boundary samples in a reused list skipped), or
-// the direct loop for an overflowed list.
+// Fluid-only passes (xsph, normals, tension): fluid(j, q, g) for every fluid
+// neighbour entry of the list, q = pred[j] and g = gsrc[j] (the pass's packed
+// per-neighbour values), both loaded in the walk's two-deep pipeline so that
+// neither gather's latency is waited for in the pair's arithmetic; boundary
+// entries of a reused list are skipped. An overflowed list walks the direct loop.
 template <class FFluid>
-__device__ __forceinline__ void walk_neighbours(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
-                                                const float4* __restrict__ pred,
-                                                const uint32_t* __restrict__ cs, const uint32_t* __restrict__ list,
-                                                uint32_t cap, uint32_t count, FFluid&& fluid) {
-  auto none = [](uint32_t, float4) {};
-  if (count != kListOverflow) {
-    walk_list<true, kFetchFluid>(list, cap, i, count, pred, nullptr, [&](uint32_t j, float4 q, bool isBound) {
-      if (!isBound) fluid(j, q);
-    });
-  } else {
-    walk_direct<false>(P, w, pi, i, pred, cs, nullptr, nullptr, fluid, none);
+__device__ __forceinline__ void walk_neighbours2(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
+                                                 const float4* __restrict__ pred,
+                                                 const float4* __restrict__ gsrc,
+                                                 const uint32_t* __restrict__ cs,
+                                                 const uint32_t* __restrict__ list, uint32_t cap, uint32_t count,
+                                                 FFluid&& fluid) {
+  if (count == kListOverflow) {
+    auto none = [](uint32_t, float4) {};
+    walk_direct<false>(P, w, pi, i, pred, cs, nullptr, nullptr,
+                       [&](uint32_t j, float4 q) { fluid(j, q, __ldg(&gsrc[j])); }, none);
+    return;
+  }
+  count &= kCountMask;
+  if (count == 0u) return;
+  auto slot = [&](uint32_t e) { return (e & kBoundTag) != 0u ? i : e; };  // a boundary entry loads i
+  const uint32_t* __restrict__ at = list + i;  // entry k of the particle at list[k * cap + i]
+  uint32_t e0 = __ldg(at);
+  float4 q0 = __ldg(pred + slot(e0)), g0 = __ldg(gsrc + slot(e0));
+  at += cap;
+  uint32_t e1 = count > 1u ? __ldg(at) : 0u;
+  for (uint32_t k = 1; k <= count; k++) {
+    const uint32_t cur = e0;
+    const float4 qc = q0, gc = g0;
+    if (k < count) {
+      e0 = e1;
+      q0 = __ldg(pred + slot(e1));
+      g0 = __ldg(gsrc + slot(e1));
+      if (k + 1 < count) {
+        at += cap;
+        e1 = __ldg(at);
+      }
+    }
+    if ((cur & kBoundTag) == 0u) fluid(cur, qc, gc);
   }
 }
 

@@ -225,6 +225,9 @@ struct DevScene {
   uint32_t cellStride;  // cells per cellDisp slot
   float4* nbRef;        // [cap] positions at the start of the substep's iterations
   float4* predLam;      // [cap] (position, lambda) written by lambda for the delta of the same iteration
+  float4* velRho;       // [cap] (velFromPos, density) of the substep's last iteration, the two
+                        // values xsph reads of each neighbour in one gather
+  float4* normRho;      // [cap] (normal, density) written by xsph+normals for tension
   uint32_t cap;         // particle capacity (stride of nbList)
   uint32_t* slotOut;    // optional: sorted position of each input particle
 };
