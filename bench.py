@@ -360,11 +360,9 @@ def run_mix(args):
         b.step(ids, 1 / 60)
     b.synchronize()
 
-    # timed frames, with an event around every launch inside the replayed graphs
+    # timed frames (two frame lanes: each frame runs as two concurrent halves)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    b.profile(True)
-    b.profile_reset()
     clocks = ClockSampler(local)
     clocks.start()
     tb = sim_times()
@@ -383,9 +381,19 @@ def run_mix(args):
     w1 = time.time()
     launches = _launches() - launches0
     clocks.stop()
+    done = particle_substeps(tb, sim_times())
+    # per-launch times: the next frames with an event around every launch (event-record
+    # nodes in the replayed graphs); profiled frames run whole, on one lane
+    prof_frames = max(4, args.steps // 2)
+    b.profile(True)
+    b.profile_reset()
+    with torch.cuda.stream(stream):
+        for k in range(prof_frames):
+            flush.zero_()
+            b.step(ids, 1 / 60)
+    torch.cuda.synchronize()
     kern = b.profile_read()
     b.profile(False)
-    done = particle_substeps(tb, sim_times())
     dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     dev_ms_max = rep.max(dev_ms)
     value = world * done / (dev_ms_max / 1000.0)
@@ -404,6 +412,10 @@ def run_mix(args):
             return total, ALGO_BYTES[k] + 64 * n_bodies_p / max(1, total)
         return total, ALGO_BYTES.get(k, 0)
     roofline = roofline_of(kern, per_launch, MIX)
+    if roofline:
+        roofline["timing"] = (f"CUDA events around every launch of {prof_frames} whole frames (event-record nodes "
+                              "in the replayed frame graphs) right after the timed frames, which run each frame "
+                              "as two concurrent halves")
 
     # whole frame against the workload definition's fixed bytes per particle-substep
     frame_bytes = 0.0

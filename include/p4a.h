@@ -525,9 +525,10 @@ int p4a_batch_write_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t wh
  * scenes are stepped as `groups` consecutive frames of about equal particle counts
  * (0: two from 3 M particles up, else one), with the host-to-device copies of later
  * groups and the device-to-host copies of earlier ones on two copy streams of
- * their own, so that they overlap the frames of the other groups. The copies of
- * the first group's inputs and the last group's outputs stay exposed, and every
- * extra group adds a frame's launch tails. The copies are ordered after all
+ * their own, so that they overlap the frames of the other groups; with two frame
+ * lanes (p4a_batch_set_lanes) odd groups run on the second lane, at the same time
+ * as the even ones. The copies of the first group's inputs and the last group's
+ * outputs stay exposed. The copies are ordered after all
  * work queued on the batch's stream before the call and before all work queued
  * after it; host memory (pinned, for overlap) stays in use until
  * p4a_batch_synchronize. No counterpart in the reference, which steps one scene
@@ -544,6 +545,14 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
                       int32_t groups);
 /* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
 int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
+/* Frame lanes of p4a_batch_step and the serving loop: with lanes = 2 (the default)
+ * a frame of at least min_particles particles (default 1,000,000) over two or more
+ * scenes runs as two halves of about equal particle counts at once, each on a
+ * stream of its own (the batch's stream waits for both), so that one half's launch
+ * tails overlap the other half's work; lanes = 1 runs every frame whole. Scenes are
+ * independent: every scene gets the same bits either way. Frames stay whole while
+ * profiling is on. No counterpart in the reference. */
+int p4a_batch_set_lanes(p4a_batch* b, int32_t lanes, int64_t min_particles);
 /* Per-kernel timing of batched frames, as p4a_profile_* for a Sim (the
  * counterpart of the reference's GpuTimer phases, src/gputimer.js): with it on,
  * every launch of a frame is bracketed by events (event-record nodes inside a

@@ -66,6 +66,7 @@ SIGNATURES = {
     "p4a_batch_read_async": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
     "p4a_batch_write_async": ([_vp, _i32, _i32, _i32, _vp, _sz, _sz], C.c_int),
     "p4a_batch_step_io": ([_vp, _vp, _i32, C.c_double, _i32], C.c_int),
+    "p4a_batch_set_lanes": ([_vp, _i32, C.c_int64], C.c_int),
     "p4a_batch_profile_enable": ([_vp, _i32], C.c_int),
     "p4a_batch_profile_reset": ([_vp], C.c_int),
     "p4a_batch_profile_read": ([_vp, _vp, _i32, C.POINTER(_i32)], C.c_int),

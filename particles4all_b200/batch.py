@@ -142,6 +142,11 @@ class Batch:
         self._check(self._L.p4a_batch_write_async(self._h, int(sid), _abi.BUF[name], which, C.c_void_p(host_ptr),
                                                   int(offset), int(nbytes)), "write_async")
 
+    def set_lanes(self, lanes=2, min_particles=1_000_000):
+        """Frames of at least min_particles particles run as two concurrent halves
+        (lanes=2, the default) or whole (lanes=1); the same bits either way."""
+        self._check(self._L.p4a_batch_set_lanes(self._h, int(lanes), int(min_particles)), "set_lanes")
+
     def step_io(self, entries, frame_dt, groups=0):
         """One frame of the scenes of `entries` with overlapped host I/O: each entry
         is (sid, pos_in, vel_in, pos_out, vel_out), host addresses (pinned for

@@ -170,7 +170,8 @@ constexpr int kLaunchKinds = (int)(sizeof(kLaunchNames) / sizeof(kLaunchNames[0]
 // one after the last launch (as event-record nodes when the stream is captured).
 int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched,
               const std::vector<cudaEvent_t>* ev = nullptr) {
-  cudaStream_t st = b->stream;
+  p4a_batch::Lane& Ln = *b->lane;
+  cudaStream_t st = Ln.stream;
   DevScene& d = b->d;
   const int stride = b->cfg.max_scenes;
   uint64_t n = 0;
@@ -178,16 +179,16 @@ int run_frame(p4a_batch* b, const Frame& F, bool graphForm, uint64_t* launched,
     return graphForm ? cudaEventRecordWithFlags((*ev)[k], st, cudaEventRecordExternal)
                      : cudaEventRecord((*ev)[k], st);
   };
-  BTRY(b, cudaMemsetAsync(b->dCursors, 0, F.launches.size() * sizeof(uint32_t), st));
+  BTRY(b, cudaMemsetAsync(Ln.dCursors, 0, F.launches.size() * sizeof(uint32_t), st));
   for (size_t L = 0; L < F.launches.size(); L++) {
     const LaunchRec& r = F.launches[L];
     if (ev) BTRY(b, record(L));
     if (!graphForm && r.seg.count == 0) continue;
     BatchWork w;
-    w.params = b->dParams + (size_t)r.sub * stride;
-    w.items = b->dItems;
-    w.seg = b->dSegs + L;
-    w.cursor = b->dCursors + L;
+    w.params = Ln.dParams + (size_t)r.sub * stride;
+    w.items = Ln.dItems;
+    w.seg = Ln.dSegs + L;
+    w.cursor = Ln.dCursors + L;
     const int maxItems = graphForm ? 0x7fffffff : (int)r.seg.count;
     switch (r.kind) {
       case LK_ZERO: launch_zero_stats_b(w, d.statsOut, st); break;
@@ -253,47 +254,52 @@ void drop_profile_events(p4a_batch* b) {
 }
 
 void drop_graphs(p4a_batch* b) {
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  b->graphs.clear();
+  for (auto& Ln : b->lanes) {
+    for (auto& kv : Ln.graphs) cudaGraphExecDestroy(kv.second);
+    Ln.graphs.clear();
+  }
   for (auto& kv : b->profNodes)
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   b->profNodes.clear();
 }
 
 int ensure_device_lists(p4a_batch* b, int64_t nItems, int64_t nLaunches) {
-  if (nItems <= b->itemsCap && nLaunches <= b->launchCap) return P4A_OK;
-  BTRY(b, cudaStreamSynchronize(b->stream));
+  p4a_batch::Lane& Ln = *b->lane;
+  if (nItems <= Ln.itemsCap && nLaunches <= Ln.launchCap) return P4A_OK;
+  for (auto& l : b->lanes)
+    if (l.stream) BTRY(b, cudaStreamSynchronize(l.stream));
   drop_graphs(b);  // graphs hold the old addresses
-  if (nItems > b->itemsCap) {
-    if (b->dItems) cudaFree(b->dItems);
-    b->dItems = nullptr;
+  if (nItems > Ln.itemsCap) {
+    if (Ln.dItems) cudaFree(Ln.dItems);
+    Ln.dItems = nullptr;
     const int64_t cap = std::max<int64_t>(nItems * 2, 4096);
-    BTRY(b, cudaMalloc((void**)&b->dItems, (size_t)cap * sizeof(uint2)));
-    b->itemsCap = cap;
+    BTRY(b, cudaMalloc((void**)&Ln.dItems, (size_t)cap * sizeof(uint2)));
+    Ln.itemsCap = cap;
   }
-  if (nLaunches > b->launchCap) {
-    if (b->dSegs) cudaFree(b->dSegs);
-    if (b->dCursors) cudaFree(b->dCursors);
-    b->dSegs = nullptr;
-    b->dCursors = nullptr;
+  if (nLaunches > Ln.launchCap) {
+    if (Ln.dSegs) cudaFree(Ln.dSegs);
+    if (Ln.dCursors) cudaFree(Ln.dCursors);
+    Ln.dSegs = nullptr;
+    Ln.dCursors = nullptr;
     const int64_t cap = std::max<int64_t>(nLaunches * 2, 256);
-    BTRY(b, cudaMalloc((void**)&b->dSegs, (size_t)cap * sizeof(WorkSeg)));
-    BTRY(b, cudaMalloc((void**)&b->dCursors, (size_t)cap * sizeof(uint32_t)));
-    b->launchCap = cap;
+    BTRY(b, cudaMalloc((void**)&Ln.dSegs, (size_t)cap * sizeof(WorkSeg)));
+    BTRY(b, cudaMalloc((void**)&Ln.dCursors, (size_t)cap * sizeof(uint32_t)));
+    Ln.launchCap = cap;
   }
   return P4A_OK;
 }
 
 int ensure_staging(p4a_batch* b, size_t bytes) {
-  if (bytes <= b->stagingCap) return P4A_OK;
+  p4a_batch::Lane& Ln = *b->lane;
+  if (bytes <= Ln.stagingCap) return P4A_OK;
   for (int k = 0; k < 2; k++) {
-    if (b->stagingDone[k]) cudaEventSynchronize(b->stagingDone[k]);
-    if (b->staging[k]) cudaFreeHost(b->staging[k]);
-    b->staging[k] = nullptr;
+    if (Ln.stagingDone[k]) cudaEventSynchronize(Ln.stagingDone[k]);
+    if (Ln.staging[k]) cudaFreeHost(Ln.staging[k]);
+    Ln.staging[k] = nullptr;
   }
   const size_t cap = std::max<size_t>(bytes * 2, 1 << 16);
-  for (int k = 0; k < 2; k++) BTRY(b, cudaHostAlloc((void**)&b->staging[k], cap, cudaHostAllocDefault));
-  b->stagingCap = cap;
+  for (int k = 0; k < 2; k++) BTRY(b, cudaHostAlloc((void**)&Ln.staging[k], cap, cudaHostAllocDefault));
+  Ln.stagingCap = cap;
   return P4A_OK;
 }
 
@@ -307,20 +313,21 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
   int rc;
   if ((rc = ensure_device_lists(b, (int64_t)F.items.size(), (int64_t)F.launches.size()))) return rc;
   if ((rc = ensure_staging(b, pBytes + iBytes + sBytes))) return rc;
-  const int k = b->stagingIdx;
-  b->stagingIdx ^= 1;
-  BTRY(b, cudaEventSynchronize(b->stagingDone[k]));  // the upload two frames ago has finished
-  unsigned char* h = b->staging[k];
+  p4a_batch::Lane& Ln = *b->lane;
+  const int k = Ln.stagingIdx;
+  Ln.stagingIdx ^= 1;
+  BTRY(b, cudaEventSynchronize(Ln.stagingDone[k]));  // the lane's upload two frames ago has finished
+  unsigned char* h = Ln.staging[k];
   std::memcpy(h, F.params.data(), pBytes);
   std::memcpy(h + pBytes, F.items.data(), iBytes);
   WorkSeg* segs = reinterpret_cast<WorkSeg*>(h + pBytes + iBytes);
   for (size_t L = 0; L < F.launches.size(); L++) segs[L] = F.launches[L].seg;
   for (int s = 0; s < F.nSubs; s++)
-    BTRY(b, cudaMemcpyAsync(b->dParams + (size_t)s * b->cfg.max_scenes, h + rowBytes * s, rowBytes,
-                            cudaMemcpyHostToDevice, b->stream));
-  if (iBytes) BTRY(b, cudaMemcpyAsync(b->dItems, h + pBytes, iBytes, cudaMemcpyHostToDevice, b->stream));
-  BTRY(b, cudaMemcpyAsync(b->dSegs, segs, sBytes, cudaMemcpyHostToDevice, b->stream));
-  BTRY(b, cudaEventRecord(b->stagingDone[k], b->stream));
+    BTRY(b, cudaMemcpyAsync(Ln.dParams + (size_t)s * b->cfg.max_scenes, h + rowBytes * s, rowBytes,
+                            cudaMemcpyHostToDevice, Ln.stream));
+  if (iBytes) BTRY(b, cudaMemcpyAsync(Ln.dItems, h + pBytes, iBytes, cudaMemcpyHostToDevice, Ln.stream));
+  BTRY(b, cudaMemcpyAsync(Ln.dSegs, segs, sBytes, cudaMemcpyHostToDevice, Ln.stream));
+  BTRY(b, cudaEventRecord(Ln.stagingDone[k], Ln.stream));
   const size_t nEv = F.launches.size() + 1;
   p4a_batch::ProfPending pf;
   if (b->prof) {
@@ -341,13 +348,17 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
   }
   std::vector<int> key = F.shape;
   if (b->prof) key.push_back(-1);  // the profiled graph of the shape has event nodes
-  auto it = b->graphs.find(key);
-  if (it == b->graphs.end()) {
-    if (b->graphs.size() >= 16) drop_graphs(b);
+  auto it = Ln.graphs.find(key);
+  if (it == Ln.graphs.end()) {
+    if (Ln.graphs.size() >= 16) {
+      for (auto& l : b->lanes)
+        if (l.stream) BTRY(b, cudaStreamSynchronize(l.stream));
+      drop_graphs(b);
+    }
     cudaGraph_t g = nullptr;
-    BTRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    BTRY(b, cudaStreamBeginCapture(Ln.stream, cudaStreamCaptureModeThreadLocal));
     const int brc = run_frame(b, F, true, nullptr, b->prof ? &pf.ev : nullptr);
-    const cudaError_t ec = cudaStreamEndCapture(b->stream, &g);
+    const cudaError_t ec = cudaStreamEndCapture(Ln.stream, &g);
     if (brc) {
       if (g) cudaGraphDestroy(g);
       return brc;
@@ -387,7 +398,7 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
     } else {
       cudaGraphDestroy(g);
     }
-    it = b->graphs.emplace(key, ge).first;
+    it = Ln.graphs.emplace(key, ge).first;
   }
   if (b->prof) {
     // later replays may still be reading this set's events: point the nodes at it
@@ -396,7 +407,7 @@ int execute(p4a_batch* b, const Frame& F, bool allowGraph) {
       BTRY(b, cudaGraphExecEventRecordNodeSetEvent(it->second, pn.nodes[k], pf.ev[k]));
     for (size_t L = 0; L < F.launches.size(); L++) pf.kinds[L] = F.launches[L].kind;
   }
-  BTRY(b, cudaGraphLaunch(it->second, b->stream));
+  BTRY(b, cudaGraphLaunch(it->second, Ln.stream));
   count_launches(F.launches.size());
   if (b->prof) b->profPending.push_back(std::move(pf));
   return P4A_OK;
@@ -735,6 +746,55 @@ int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t 
   return P4A_OK;
 }
 
+// One frame of the listed scenes: on lane 0, or, with two lanes and a frame of at
+// least laneMinParticles, as two halves of about equal particle counts that run at
+// once on the two lanes. Scenes are independent, so each scene gets the bits the
+// whole frame gives it; the batch's stream waits for both halves. Profiled frames
+// stay on one lane, so that their per-launch intervals do not overlap.
+int step_scenes(p4a_batch* b, const int32_t* ids, const double* dts, int32_t count) {
+  b->lane = &b->lanes[0];
+  int64_t total = 0;
+  for (int k = 0; k < count; k++) total += b->scenes[ids[k]].n;
+  if (b->laneCount < 2 || b->prof || count < 2 || total < b->laneMinParticles)
+    return step_frame(b, ids, dts, count);
+  // largest scenes first, each to the half with fewer particles so far; each half
+  // keeps the list order
+  std::vector<int> order((size_t)count);
+  for (int k = 0; k < count; k++) order[(size_t)k] = k;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return b->scenes[ids[x]].n > b->scenes[ids[y]].n; });
+  std::vector<char> half((size_t)count, 0);
+  int64_t n0 = 0, n1 = 0;
+  for (int k : order) {
+    const int64_t n = b->scenes[ids[k]].n;
+    if (n0 <= n1) {
+      n0 += n;
+    } else {
+      half[(size_t)k] = 1;
+      n1 += n;
+    }
+  }
+  std::vector<int32_t> id[2];
+  std::vector<double> dt[2];
+  for (int k = 0; k < count; k++) {
+    id[half[(size_t)k]].push_back(ids[k]);
+    dt[half[(size_t)k]].push_back(dts[k]);
+  }
+  if (id[1].empty()) return step_frame(b, ids, dts, count);
+  BTRY(b, cudaEventRecord(b->laneFork, b->stream));
+  BTRY(b, cudaStreamWaitEvent(b->lanes[1].stream, b->laneFork, 0));
+  int rc = step_frame(b, id[0].data(), dt[0].data(), (int32_t)id[0].size());
+  if (!rc) {
+    b->lane = &b->lanes[1];
+    rc = step_frame(b, id[1].data(), dt[1].data(), (int32_t)id[1].size());
+    b->lane = &b->lanes[0];
+  }
+  // whatever happened, later work on the batch's stream comes after lane 1's
+  BTRY(b, cudaEventRecord(b->laneJoin, b->lanes[1].stream));
+  BTRY(b, cudaStreamWaitEvent(b->stream, b->laneJoin, 0));
+  return rc;
+}
+
 }  // namespace p4a
 
 namespace {
@@ -803,7 +863,8 @@ int alloc_arenas(p4a_batch* b) {
        (rc = balloc(b, &d.bodyInfo, B1)) || (rc = balloc(b, &d.bodyStart, B1)) ||
        (rc = balloc(b, &d.bodyFill, B1)) || (rc = balloc(b, &d.bodyList, b->cfg.max_body_parts)) ||
        (rc = balloc(b, &d.statsOut, (int64_t)cfg->max_scenes * 8)) ||
-       (rc = balloc(b, &b->dParams, (int64_t)kMaxSubsteps * cfg->max_scenes))))
+       (rc = balloc(b, &b->lanes[0].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes)) ||
+       (rc = balloc(b, &b->lanes[1].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes))))
     ;
   return rc;
 }
@@ -837,7 +898,15 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
     return P4A_ERR_CUDA;
   }
   b->ownStream = true;
-  for (int k = 0; k < 2; k++) cudaEventCreateWithFlags(&b->stagingDone[k], cudaEventDisableTiming);
+  b->lanes[0].stream = b->stream;
+  if (cudaStreamCreateWithFlags(&b->lanes[1].stream, cudaStreamNonBlocking) != cudaSuccess) {
+    p4a_batch_destroy(b);
+    return P4A_ERR_CUDA;
+  }
+  for (auto& Ln : b->lanes)
+    for (int k = 0; k < 2; k++) cudaEventCreateWithFlags(&Ln.stagingDone[k], cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&b->laneFork, cudaEventDisableTiming);
+  cudaEventCreateWithFlags(&b->laneJoin, cudaEventDisableTiming);
   const int64_t P = cfg->max_particles, Cc = cfg->max_cells + (int64_t)cfg->max_scenes * (kScanTile + 2);
   int rc = alloc_arenas(b);
   if (rc) {
@@ -860,20 +929,26 @@ int p4a_batch_destroy(p4a_batch* b) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->lanes[1].stream) cudaStreamSynchronize(b->lanes[1].stream);
   drop_graphs(b);
   drop_profile_events(b);
   for (void* p : b->allocs) cudaFree(p);
-  if (b->dItems) cudaFree(b->dItems);
-  if (b->dSegs) cudaFree(b->dSegs);
-  if (b->dCursors) cudaFree(b->dCursors);
+  for (auto& Ln : b->lanes) {
+    if (Ln.dItems) cudaFree(Ln.dItems);
+    if (Ln.dSegs) cudaFree(Ln.dSegs);
+    if (Ln.dCursors) cudaFree(Ln.dCursors);
+    for (int k = 0; k < 2; k++) {
+      if (Ln.staging[k]) cudaFreeHost(Ln.staging[k]);
+      if (Ln.stagingDone[k]) cudaEventDestroy(Ln.stagingDone[k]);
+    }
+  }
+  if (b->lanes[1].stream) cudaStreamDestroy(b->lanes[1].stream);
+  if (b->laneFork) cudaEventDestroy(b->laneFork);
+  if (b->laneJoin) cudaEventDestroy(b->laneJoin);
   if (b->upStream) cudaStreamDestroy(b->upStream);
   if (b->h2dStream) cudaStreamDestroy(b->h2dStream);
   if (b->d2hStream) cudaStreamDestroy(b->d2hStream);
   for (cudaEvent_t e : b->ioEvents) cudaEventDestroy(e);
-  for (int k = 0; k < 2; k++) {
-    if (b->staging[k]) cudaFreeHost(b->staging[k]);
-    if (b->stagingDone[k]) cudaEventDestroy(b->stagingDone[k]);
-  }
   if (b->ownStream && b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return P4A_OK;
@@ -885,6 +960,7 @@ int p4a_batch_set_stream(p4a_batch* b, void* stream) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   BTRY(b, cudaStreamSynchronize(b->stream));
+  BTRY(b, cudaStreamSynchronize(b->lanes[1].stream));
   drop_graphs(b);
   if (stream) {
     if (b->ownStream) cudaStreamDestroy(b->stream);
@@ -894,6 +970,7 @@ int p4a_batch_set_stream(p4a_batch* b, void* stream) {
     BTRY(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     b->ownStream = true;
   }
+  b->lanes[0].stream = b->stream;
   return P4A_OK;
 }
 
@@ -996,7 +1073,14 @@ int p4a_batch_step(p4a_batch* b, const int32_t* ids, int32_t count, double frame
     if (seen[ids[k]]++) return bfail(b, P4A_ERR_ARG, "p4a_batch_step: scene %d listed twice", ids[k]);
   }
   const std::vector<double> dts((size_t)count, frameDt);
-  return step_frame(b, ids, dts.data(), count);
+  return step_scenes(b, ids, dts.data(), count);
+}
+
+int p4a_batch_set_lanes(p4a_batch* b, int32_t lanes, int64_t min_particles) {
+  if (!b || lanes < 1 || lanes > 2 || min_particles < 0) return bfail(b, P4A_ERR_ARG, "p4a_batch_set_lanes: bad value");
+  b->laneCount = lanes;
+  b->laneMinParticles = min_particles;
+  return P4A_OK;
 }
 
 int p4a_batch_synchronize(p4a_batch* b) {
@@ -1222,15 +1306,21 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
     return P4A_OK;
   };
   std::vector<int32_t> ids;
+  // with two lanes, odd groups run on lane 1, so that consecutive groups' frames run
+  // at once; profiled frames stay on lane 0
+  const bool twoLanes = b->laneCount == 2 && !b->prof;
   auto frame = [&](int g) -> int {
+    b->lane = &b->lanes[twoLanes ? (g & 1) : 0];
+    cudaStream_t fs = b->lane->stream;
     // group g's frame waits for its own writes only
-    BTRY(b, cudaStreamWaitEvent(b->stream, ev[1 + 2 * g], 0));
+    BTRY(b, cudaStreamWaitEvent(fs, ev[1 + 2 * g], 0));
     ids.clear();
     for (int k = first[(size_t)g]; k < first[(size_t)g + 1]; k++) ids.push_back(io[k].scene_id);
     const std::vector<double> dts(ids.size(), frameDt);
     const int rc = step_frame(b, ids.data(), dts.data(), (int32_t)ids.size());
+    b->lane = &b->lanes[0];
     if (rc) return rc;
-    BTRY(b, cudaEventRecord(ev[2 + 2 * g], b->stream));
+    BTRY(b, cudaEventRecord(ev[2 + 2 * g], fs));
     return P4A_OK;
   };
   auto reads = [&](int g) -> int {
@@ -1250,6 +1340,8 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
   }
   if (!rc) rc = reads(G - 1);
   // later work on the batch's stream (and p4a_batch_synchronize) waits for every copy
+  // and, through the reads' waits, for every group's frame
+  b->lane = &b->lanes[0];
   BTRY(b, cudaEventRecord(ev[2 * G + 1], b->d2hStream));
   BTRY(b, cudaStreamWaitEvent(b->stream, ev[2 * G + 1], 0));
   BTRY(b, cudaEventRecord(ev[0], b->h2dStream));

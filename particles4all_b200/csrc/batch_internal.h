@@ -102,18 +102,31 @@ struct p4a_batch {
   p4a::RangeAlloc partA, cellA, boundA, bodyA, listA;
   std::vector<p4a::BScene> scenes;
   int64_t scanTilesCap = 0;
-  // per-frame upload (double-buffered pinned staging): params rows, items, segments
-  p4a::SimParams* dParams = nullptr;  // [kMaxSubsteps][max_scenes], row k = the frame's k-th scene
-  uint2* dItems = nullptr;
-  int64_t itemsCap = 0;
-  p4a::WorkSeg* dSegs = nullptr;      // one per launch of the frame
-  uint32_t* dCursors = nullptr;  // pull cursors, one per launch
-  int64_t launchCap = 0;
-  unsigned char* staging[2] = {nullptr, nullptr};
-  size_t stagingCap = 0;
-  cudaEvent_t stagingDone[2] = {nullptr, nullptr};
-  int stagingIdx = 0;
-  // CUDA graphs of frame shapes (substeps and iterations per substep)
+  // Frame lanes. A lane holds what its frames upload (params rows, items, segments,
+  // through double-buffered pinned staging), their pull cursors, and the CUDA graphs
+  // of the frame shapes (substeps and iterations per substep), captured with the
+  // lane's table addresses. Lane 0 runs on the batch's stream, lane 1 on a stream of
+  // its own: p4a_batch_step splits a large frame into two halves that run at once,
+  // so that the launch tails of one half overlap the work of the other.
+  struct Lane {
+    cudaStream_t stream = nullptr;       // lane 0: the batch's stream
+    p4a::SimParams* dParams = nullptr;   // [kMaxSubsteps][max_scenes], row k = the frame's k-th scene
+    uint2* dItems = nullptr;
+    int64_t itemsCap = 0;
+    p4a::WorkSeg* dSegs = nullptr;       // one per launch of the frame
+    uint32_t* dCursors = nullptr;        // pull cursors, one per launch
+    int64_t launchCap = 0;
+    unsigned char* staging[2] = {nullptr, nullptr};
+    size_t stagingCap = 0;
+    cudaEvent_t stagingDone[2] = {nullptr, nullptr};
+    int stagingIdx = 0;
+    std::map<std::vector<int>, cudaGraphExec_t> graphs;
+  };
+  Lane lanes[2];
+  Lane* lane = &lanes[0];          // the lane the next frame runs on
+  int laneCount = 2;               // p4a_batch_set_lanes
+  int64_t laneMinParticles = 1000000;
+  cudaEvent_t laneFork = nullptr, laneJoin = nullptr;
   bool useGraphs = true;
   cudaStream_t upStream = nullptr;  // admissions' uploads (serving loop)
   // p4a_batch_step_io: a stream per copy direction and the events that order the
@@ -121,7 +134,6 @@ struct p4a_batch {
   // [2 + 2g] group g stepped, then the reads' end)
   cudaStream_t h2dStream = nullptr, d2hStream = nullptr;
   std::vector<cudaEvent_t> ioEvents;
-  std::map<std::vector<int>, cudaGraphExec_t> graphs;
   // per-kernel timing of frames (p4a_batch_profile_*): an event before every launch
   // of a frame and one after the last; in a graph these are event-record nodes,
   // pointed at a fresh set of events before each replay
@@ -180,6 +192,8 @@ int place_scene(p4a_batch* b, PreparedScene& ps, unsigned char* blob, cudaStream
 int prime_scenes(p4a_batch* b, const std::vector<int>& slots);
 // One frame: each listed scene advances by its own frame_dt (time bank and substeps).
 int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t count);
+// step_frame split across the batch's two frame lanes when the frame is large.
+int step_scenes(p4a_batch* b, const int32_t* ids, const double* dts, int32_t count);
 // Device pointer and byte size of a scene's view of buffer `id` (P4A_BUF_*), copy
 // `which` (P4A_LIVE, P4A_A, P4A_B).
 int scene_buffer(p4a_batch* b, const BScene& s, int32_t id, int32_t which, void** p, size_t* bytes);

@@ -316,33 +316,39 @@ __device__ __forceinline__ uint32_t block_exclusive(uint32_t x, uint32_t* total)
   return r;
 }
 
+// Tile sums and offsets of the batched scan live at the scene's own tiles (its cell
+// range starts on a tile boundary), so frames that run at once on different
+// streams, with different scenes, never share a slot.
+__device__ __forceinline__ size_t scene_tile0(const SimParams& P) { return (size_t)(P.cOff / kScanTile); }
+
 __global__ void __launch_bounds__(kBlock) k_scan_sums_b(const __grid_constant__ BatchWork w,
                                                         const __grid_constant__ DevScene d) {
   uint32_t* tileSum = reinterpret_cast<uint32_t*>(d.scanState);
-  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
+  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t) {
     const long long limit = (long long)P.cOff + P.nCells;
     const long long base = (long long)P.cOff + (long long)lt * kScanTile + (long long)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
     const uint32_t sum = tile_counts(d.cellCount, base, limit, v);
     uint32_t total = 0;
     block_exclusive(sum, &total);
-    if (threadIdx.x == 0) tileSum[2 * (size_t)g] = total;
+    if (threadIdx.x == 0) tileSum[2 * (scene_tile0(P) + lt)] = total;
   });
 }
 
 __global__ void __launch_bounds__(kBlock) k_scan_offsets_b(const __grid_constant__ BatchWork w,
                                                            const __grid_constant__ DevScene d) {
   uint32_t* st = reinterpret_cast<uint32_t*>(d.scanState);
-  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
+  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t) {
     if (lt != 0u) return;  // the block that gets a scene's first tile scans the scene
     const uint32_t tiles = (uint32_t)((P.nCells + kScanTile - 1) / kScanTile);
+    const size_t t0s = scene_tile0(P);
     uint32_t carry = P.pOff;
     for (uint32_t t0 = 0; t0 < tiles; t0 += kBlock) {
       const uint32_t t = t0 + threadIdx.x;
-      const uint32_t x = t < tiles ? st[2 * ((size_t)g + t)] : 0u;
+      const uint32_t x = t < tiles ? st[2 * (t0s + t)] : 0u;
       uint32_t total = 0;
       const uint32_t ex = block_exclusive(x, &total);
-      if (t < tiles) st[2 * ((size_t)g + t) + 1] = carry + ex;
+      if (t < tiles) st[2 * (t0s + t) + 1] = carry + ex;
       carry += total;
     }
   });
@@ -351,7 +357,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_offsets_b(const __grid_constant
 __global__ void __launch_bounds__(kBlock) k_scan_apply_b(const __grid_constant__ BatchWork w,
                                                          const __grid_constant__ DevScene d) {
   const uint32_t* st = reinterpret_cast<const uint32_t*>(d.scanState);
-  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t g) {
+  for_each_item(w, [&](const SimParams& P, uint32_t lt, uint32_t) {
     const long long limit = (long long)P.cOff + P.nCells;
     const long long base = (long long)P.cOff + (long long)lt * kScanTile + (long long)threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
@@ -360,7 +366,7 @@ __global__ void __launch_bounds__(kBlock) k_scan_apply_b(const __grid_constant__
     for (int j = 0; j < kScanItems; j++)
       if (base + j < limit) d.cellCount[base + j] = 0u;
     uint32_t total = 0;
-    const uint32_t offset = st[2 * (size_t)g + 1];
+    const uint32_t offset = st[2 * (scene_tile0(P) + lt) + 1];
     uint32_t run = offset + block_exclusive(sum, &total);
 #pragma unroll
     for (int j = 0; j < kScanItems; j++) {

@@ -619,7 +619,7 @@ bool launch(p4a_server* S) {
       ids.push_back(S->scenes[h].slot);
       dts.push_back(S->scenes[h].steps.front().dt);
     }
-    rc = step_frame(S->batch, ids.data(), dts.data(), (int32_t)ids.size());
+    rc = step_scenes(S->batch, ids.data(), dts.data(), (int32_t)ids.size());
     if (rc) set_err(S, "frame: %s", p4a_batch_last_error(S->batch));
     for (int32_t h : hs) F.substeps.push_back(S->batch->scenes[S->scenes[h].slot].lastSubsteps);
   }

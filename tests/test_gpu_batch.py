@@ -67,11 +67,13 @@ def assert_same(sim, batch, sid):
     assert sim.get_stats()["raw"] == batch.stats(sid)["raw"]
 
 
-@pytest.mark.parametrize("graphs", [True, False])
-def test_batch_equals_alone_bit_exact(graphs):
+@pytest.mark.parametrize("graphs,lanes", [(True, 1), (False, 1), (True, 2), (False, 2)])
+def test_batch_equals_alone_bit_exact(graphs, lanes):
+    """lanes = 2 with no size threshold: every frame runs as two concurrent halves."""
     scenes = mixed_scenes()
     frames = [1 / 60] * 6 + [1 / 45, 1 / 90, 1 / 60]
     b = Batch(max_particles=200_000, max_cells=400_000, max_scenes=16, graphs=graphs)
+    b.set_lanes(lanes, 0)
     ids = []
     for p, sc in scenes:
         ids.append(b.add_preset(p) if sc is None else b.add_scene(p, sc))
@@ -173,6 +175,32 @@ def test_step_io_equals_write_step_read(groups):
         for name in NAMES:
             assert np.array_equal(b.read(sa, name)[:n], b.read(sb, name)[:n]), name
         assert b.stats(sa)["raw"] == b.stats(sb)["raw"]
+
+
+def test_lanes_with_subsets_and_arena_reuse():
+    """Two-lane frames over changing scene subsets, across a removal and a new
+    admission, give each scene the bits it gets alone."""
+    scenes = mixed_scenes()
+    b = Batch(max_particles=200_000, max_cells=400_000, max_scenes=8)
+    b.set_lanes(2, 0)
+    ids = [b.add_preset(p) if sc is None else b.add_scene(p, sc) for p, sc in scenes[:4]]
+    b.step(ids, 1 / 60)
+    b.step(ids[1:], 1 / 60)
+    b.step(ids[:2], 1 / 45)
+    b.synchronize()
+    steps = {0: [1 / 60, 1 / 45], 1: [1 / 60, 1 / 60, 1 / 45], 2: [1 / 60, 1 / 60], 3: [1 / 60, 1 / 60]}
+    for k, sid in enumerate(ids):
+        p, sc = scenes[k]
+        assert_same(run_alone(p, sc, steps[k]), b, sid)
+    b.remove_scene(ids[2])
+    p4, s4 = scenes[4]
+    sid = b.add_preset(p4)
+    b.step([ids[0], sid, ids[3]], 1 / 60)
+    b.synchronize()
+    assert_same(run_alone(p4, s4, [1 / 60]), b, sid)
+    assert_same(run_alone(scenes[3][0], scenes[3][1], [1 / 60] * 3), b, ids[3])
+    with pytest.raises(P4AError):
+        b.set_lanes(3, 0)
 
 
 def test_step_io_rejects_bad_lists():
