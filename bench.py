@@ -73,6 +73,8 @@ def parse_args():
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
                          "frames and exit; for profiling the two forms")
     ap.add_argument("--mix-frames", type=int, default=10)
+    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2],
+                    help="frame lanes of the batched mix (2: a frame runs as two concurrent halves)")
     ap.add_argument("--mix-scenes", type=int, default=96,
                     help="with --only-mix: the first N scenes of the seeded mix (a smaller case for profiling)")
     ap.add_argument("--serve-seconds", type=float, default=15.0,
@@ -297,7 +299,7 @@ def mix_scene_flags(mix):
              int((sc["phase"][:, 0] > 0).sum())) for p, sc in mix]
 
 
-def only_mix(form, frames, scenes=96):
+def only_mix(form, frames, scenes=96, lanes=2):
     """The mix (its first `scenes` scenes) stepped in one form only: admission (or
     reset) then `frames` frames."""
     import torch
@@ -308,6 +310,7 @@ def only_mix(form, frames, scenes=96):
     if form == "batched":
         b = Batch(**mix_arenas(mix))
         b.set_stream(stream.cuda_stream)
+        b.set_lanes(lanes)
         ids = [b.add_scene(p, sc) for p, sc in mix]
         for _ in range(frames):
             b.step(ids, 1 / 60)
@@ -344,6 +347,7 @@ def run_mix(args):
     stream = torch.cuda.Stream()
     b = Batch(device=local, **mix_arenas(mix))
     b.set_stream(stream.cuda_stream)
+    b.set_lanes(args.lanes)
     t0 = time.perf_counter()
     ids = [b.add_scene(p, sc) for p, sc in mix]
     admit_s = time.perf_counter() - t0
@@ -1005,7 +1009,7 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.only_mix:
-        return only_mix(args.only_mix, args.mix_frames, args.mix_scenes)
+        return only_mix(args.only_mix, args.mix_frames, args.mix_scenes, args.lanes)
     if args.only_render:
         return only_render(args)
     if args.workload == MIX:
