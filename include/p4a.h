@@ -523,7 +523,8 @@ int p4a_batch_write_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t wh
  * vel_out receives the live buffer after the step. The results are those of
  * write_async, p4a_batch_step and read_async in that order, bit for bit; here the
  * scenes are stepped as `groups` consecutive frames of about equal particle counts
- * (0: two from 3 M particles up, else one), with the host-to-device copies of later
+ * (0: with two frame lanes one group per 750 k particles, at most 8; with one lane
+ * two from 3 M particles up, else one), with the host-to-device copies of later
  * groups and the device-to-host copies of earlier ones on two copy streams of
  * their own, so that they overlap the frames of the other groups; with two frame
  * lanes (p4a_batch_set_lanes) odd groups run on the second lane, at the same time

@@ -1245,11 +1245,17 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
     total += b->scenes[io[k].scene_id].n;
   }
   if (count == 0) return P4A_OK;
-  // groups of about equal particle counts, in list order. By default two from 3 M
-  // particles up, else one: each split adds the launch tails of a whole frame (on
-  // the 6 M-particle mix a frame split in two took 6 % longer, in four 18 %), so a
-  // second group pays for itself only where half the copies it hides cost more.
-  int G = groups > 0 ? groups : (total >= 3000000 ? 2 : 1);
+  // groups of about equal particle counts, in list order. By default, with two frame
+  // lanes, one group per 750 k particles (at most 8): consecutive groups run at once
+  // on the two lanes, so a group's launch tails overlap the other lane's work and
+  // only the first group's writes and the last groups' reads stay exposed (on the
+  // 6 M-particle mix: 391, 407, 417, 421 M particle-substeps/s end to end with 2, 4,
+  // 6, 8 groups). With one lane each split adds the launch tails of a whole frame (a
+  // frame split in two took 6 % longer, in four 18 %): two groups from 3 M up, else one.
+  const bool lanes2 = b->laneCount == 2 && !b->prof;
+  int G = groups > 0 ? groups
+                     : lanes2 ? (int)std::min<int64_t>(8, std::max<int64_t>(1, total / 750000))
+                              : (total >= 3000000 ? 2 : 1);
   G = std::min(G, std::min(count, 64));
   std::vector<int> first((size_t)G + 1, count);
   first[0] = 0;
@@ -1308,9 +1314,8 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
   std::vector<int32_t> ids;
   // with two lanes, odd groups run on lane 1, so that consecutive groups' frames run
   // at once; profiled frames stay on lane 0
-  const bool twoLanes = b->laneCount == 2 && !b->prof;
   auto frame = [&](int g) -> int {
-    b->lane = &b->lanes[twoLanes ? (g & 1) : 0];
+    b->lane = &b->lanes[lanes2 ? (g & 1) : 0];
     cudaStream_t fs = b->lane->stream;
     // group g's frame waits for its own writes only
     BTRY(b, cudaStreamWaitEvent(fs, ev[1 + 2 * g], 0));
