@@ -118,10 +118,12 @@ __device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* _
         xb = min(x1, max(x0, __float2int_rd((rel.x + half) * A.invSupport)));
       }
       const uint32_t jb = __ldg(&cs[rowBase + xa]), je = min(__ldg(&cs[rowBase + xb + 1]), A.count);
-      for (uint32_t j = jb; j < je; j++) {
-        const F3 d = sub3(xyz(__ldg(&pos[j])), xi);
+      // one candidate of the row in the reference's order; four loads are issued
+      // ahead of their tests, so the row's gathers overlap (the sums keep their order)
+      auto cand = [&](float4 q) {
+        const F3 d = sub3(xyz(q), xi);
         const float r2 = dot3(d, d);
-        if (r2 >= r2max) continue;
+        if (r2 >= r2max) return;
         const float t = sqrtf(r2) * invR;
         const float w = 1.0f - t * t * t;
         sd = fma3(w, d, sd);
@@ -130,7 +132,17 @@ __device__ __forceinline__ void aniso_body(const AnisoParams& A, const float4* _
         m2.c[2] = fma3(d.z * w, d, m2.c[2]);
         wsum = wsum + w;
         nn = nn + 1;
+      };
+      uint32_t j = jb;
+      for (; j + 4 <= je; j += 4) {
+        const float4 q0 = __ldg(&pos[j]), q1 = __ldg(&pos[j + 1]);
+        const float4 q2 = __ldg(&pos[j + 2]), q3 = __ldg(&pos[j + 3]);
+        cand(q0);
+        cand(q1);
+        cand(q2);
+        cand(q3);
       }
+      for (; j < je; j++) cand(__ldg(&pos[j]));
     }
   }
   if (wsum <= 0.0f) {
