@@ -73,7 +73,7 @@ def parse_args():
                     help="step the 96-scene mix only (one Batch, or 96 plain Sims) for --mix-frames "
                          "frames and exit; for profiling the two forms")
     ap.add_argument("--mix-frames", type=int, default=10)
-    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2],
+    ap.add_argument("--lanes", type=int, default=2, choices=[1, 2, 3, 4],
                     help="frame lanes of the batched mix (2: a frame runs as two concurrent halves)")
     ap.add_argument("--mix-scenes", type=int, default=96,
                     help="with --only-mix: the first N scenes of the seeded mix (a smaller case for profiling)")

@@ -523,12 +523,12 @@ int p4a_batch_write_async(p4a_batch* b, int32_t scene_id, int32_t id, int32_t wh
  * vel_out receives the live buffer after the step. The results are those of
  * write_async, p4a_batch_step and read_async in that order, bit for bit; here the
  * scenes are stepped as `groups` consecutive frames of about equal particle counts
- * (0: with two frame lanes one group per 750 k particles, at most 8; with one lane
- * two from 3 M particles up, else one), with the host-to-device copies of later
+ * (0: with two or more frame lanes one group per 750 k particles, at most 8; with
+ * one lane two from 3 M particles up, else one), with the host-to-device copies of later
  * groups and the device-to-host copies of earlier ones on two copy streams of
- * their own, so that they overlap the frames of the other groups; with two frame
- * lanes (p4a_batch_set_lanes) odd groups run on the second lane, at the same time
- * as the even ones. The copies of the first group's inputs and the last group's
+ * their own, so that they overlap the frames of the other groups; with frame lanes
+ * (p4a_batch_set_lanes) group g runs on lane g mod lanes, at the same time as the
+ * groups on the other lanes. The copies of the first group's inputs and the last group's
  * outputs stay exposed. The copies are ordered after all
  * work queued on the batch's stream before the call and before all work queued
  * after it; host memory (pinned, for overlap) stays in use until
@@ -546,11 +546,11 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
                       int32_t groups);
 /* Capture each distinct frame schedule as a CUDA graph and replay it (default on). */
 int p4a_batch_use_graphs(p4a_batch* b, int32_t on);
-/* Frame lanes of p4a_batch_step and the serving loop: with lanes = 2 (the default)
- * a frame of at least min_particles particles (default 1,000,000) over two or more
- * scenes runs as two halves of about equal particle counts at once, each on a
- * stream of its own (the batch's stream waits for both), so that one half's launch
- * tails overlap the other half's work; lanes = 1 runs every frame whole. Scenes are
+/* Frame lanes of p4a_batch_step and the serving loop: with lanes = L > 1 (1-4,
+ * default 2) a frame of at least min_particles particles (default 1,000,000) over
+ * two or more scenes runs as L parts of about equal particle counts at once, each on
+ * a stream of its own (the batch's stream waits for all), so that one part's launch
+ * tails overlap the others' work; lanes = 1 runs every frame whole. Scenes are
  * independent: every scene gets the same bits either way. Frames stay whole while
  * profiling is on. No counterpart in the reference. */
 int p4a_batch_set_lanes(p4a_batch* b, int32_t lanes, int64_t min_particles);

@@ -143,8 +143,8 @@ class Batch:
                                                   int(offset), int(nbytes)), "write_async")
 
     def set_lanes(self, lanes=2, min_particles=1_000_000):
-        """Frames of at least min_particles particles run as two concurrent halves
-        (lanes=2, the default) or whole (lanes=1); the same bits either way."""
+        """Frames of at least min_particles particles run as `lanes` concurrent parts
+        (1-4, default 2; 1 = whole); the same bits either way."""
         self._check(self._L.p4a_batch_set_lanes(self._h, int(lanes), int(min_particles)), "set_lanes")
 
     def step_io(self, entries, frame_dt, groups=0):

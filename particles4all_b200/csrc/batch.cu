@@ -746,52 +746,54 @@ int step_frame(p4a_batch* b, const int32_t* ids, const double* frameDt, int32_t 
   return P4A_OK;
 }
 
-// One frame of the listed scenes: on lane 0, or, with two lanes and a frame of at
-// least laneMinParticles, as two halves of about equal particle counts that run at
-// once on the two lanes. Scenes are independent, so each scene gets the bits the
-// whole frame gives it; the batch's stream waits for both halves. Profiled frames
-// stay on one lane, so that their per-launch intervals do not overlap.
+// One frame of the listed scenes: on lane 0, or, with L > 1 lanes and a frame of at
+// least laneMinParticles, as L parts of about equal particle counts that run at once,
+// one per lane. Scenes are independent, so each scene gets the bits the whole frame
+// gives it; the batch's stream waits for every part. Profiled frames stay whole, on
+// one lane, so that their per-launch intervals do not overlap.
 int step_scenes(p4a_batch* b, const int32_t* ids, const double* dts, int32_t count) {
   b->lane = &b->lanes[0];
   int64_t total = 0;
   for (int k = 0; k < count; k++) total += b->scenes[ids[k]].n;
-  if (b->laneCount < 2 || b->prof || count < 2 || total < b->laneMinParticles)
-    return step_frame(b, ids, dts, count);
-  // largest scenes first, each to the half with fewer particles so far; each half
-  // keeps the list order
+  const int L = std::min(b->laneCount, (int)count);
+  if (L < 2 || b->prof || total < b->laneMinParticles) return step_frame(b, ids, dts, count);
+  // largest scenes first, each to the part with the fewest particles so far; each
+  // part keeps the list order
   std::vector<int> order((size_t)count);
   for (int k = 0; k < count; k++) order[(size_t)k] = k;
   std::stable_sort(order.begin(), order.end(),
                    [&](int x, int y) { return b->scenes[ids[x]].n > b->scenes[ids[y]].n; });
-  std::vector<char> half((size_t)count, 0);
-  int64_t n0 = 0, n1 = 0;
+  std::vector<int> part((size_t)count, 0);
+  int64_t load[p4a_batch::kMaxLanes] = {};
   for (int k : order) {
-    const int64_t n = b->scenes[ids[k]].n;
-    if (n0 <= n1) {
-      n0 += n;
-    } else {
-      half[(size_t)k] = 1;
-      n1 += n;
+    int q = 0;
+    for (int t = 1; t < L; t++)
+      if (load[t] < load[q]) q = t;
+    part[(size_t)k] = q;
+    load[q] += b->scenes[ids[k]].n;
+  }
+  std::vector<int32_t> id[p4a_batch::kMaxLanes];
+  std::vector<double> dt[p4a_batch::kMaxLanes];
+  for (int k = 0; k < count; k++) {
+    id[part[(size_t)k]].push_back(ids[k]);
+    dt[part[(size_t)k]].push_back(dts[k]);
+  }
+  BTRY(b, cudaEventRecord(b->laneFork, b->stream));
+  int rc = P4A_OK;
+  for (int q = 0; q < L; q++) {
+    if (id[q].empty()) continue;
+    if (q > 0) BTRY(b, cudaStreamWaitEvent(b->lanes[q].stream, b->laneFork, 0));
+    if (!rc) {
+      b->lane = &b->lanes[q];
+      rc = step_frame(b, id[q].data(), dt[q].data(), (int32_t)id[q].size());
+      b->lane = &b->lanes[0];
+    }
+    // whatever happened, later work on the batch's stream comes after this lane's
+    if (q > 0) {
+      BTRY(b, cudaEventRecord(b->laneJoin[q], b->lanes[q].stream));
+      BTRY(b, cudaStreamWaitEvent(b->stream, b->laneJoin[q], 0));
     }
   }
-  std::vector<int32_t> id[2];
-  std::vector<double> dt[2];
-  for (int k = 0; k < count; k++) {
-    id[half[(size_t)k]].push_back(ids[k]);
-    dt[half[(size_t)k]].push_back(dts[k]);
-  }
-  if (id[1].empty()) return step_frame(b, ids, dts, count);
-  BTRY(b, cudaEventRecord(b->laneFork, b->stream));
-  BTRY(b, cudaStreamWaitEvent(b->lanes[1].stream, b->laneFork, 0));
-  int rc = step_frame(b, id[0].data(), dt[0].data(), (int32_t)id[0].size());
-  if (!rc) {
-    b->lane = &b->lanes[1];
-    rc = step_frame(b, id[1].data(), dt[1].data(), (int32_t)id[1].size());
-    b->lane = &b->lanes[0];
-  }
-  // whatever happened, later work on the batch's stream comes after lane 1's
-  BTRY(b, cudaEventRecord(b->laneJoin, b->lanes[1].stream));
-  BTRY(b, cudaStreamWaitEvent(b->stream, b->laneJoin, 0));
   return rc;
 }
 
@@ -864,7 +866,9 @@ int alloc_arenas(p4a_batch* b) {
        (rc = balloc(b, &d.bodyFill, B1)) || (rc = balloc(b, &d.bodyList, b->cfg.max_body_parts)) ||
        (rc = balloc(b, &d.statsOut, (int64_t)cfg->max_scenes * 8)) ||
        (rc = balloc(b, &b->lanes[0].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes)) ||
-       (rc = balloc(b, &b->lanes[1].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes))))
+       (rc = balloc(b, &b->lanes[1].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes)) ||
+       (rc = balloc(b, &b->lanes[2].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes)) ||
+       (rc = balloc(b, &b->lanes[3].dParams, (int64_t)kMaxSubsteps * cfg->max_scenes))))
     ;
   return rc;
 }
@@ -899,14 +903,15 @@ int p4a_batch_create(int device, const p4a_batch_config* cfg, p4a_batch** out) {
   }
   b->ownStream = true;
   b->lanes[0].stream = b->stream;
-  if (cudaStreamCreateWithFlags(&b->lanes[1].stream, cudaStreamNonBlocking) != cudaSuccess) {
-    p4a_batch_destroy(b);
-    return P4A_ERR_CUDA;
-  }
+  for (int q = 1; q < p4a_batch::kMaxLanes; q++)
+    if (cudaStreamCreateWithFlags(&b->lanes[q].stream, cudaStreamNonBlocking) != cudaSuccess) {
+      p4a_batch_destroy(b);
+      return P4A_ERR_CUDA;
+    }
   for (auto& Ln : b->lanes)
     for (int k = 0; k < 2; k++) cudaEventCreateWithFlags(&Ln.stagingDone[k], cudaEventDisableTiming);
   cudaEventCreateWithFlags(&b->laneFork, cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&b->laneJoin, cudaEventDisableTiming);
+  for (auto& e : b->laneJoin) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   const int64_t P = cfg->max_particles, Cc = cfg->max_cells + (int64_t)cfg->max_scenes * (kScanTile + 2);
   int rc = alloc_arenas(b);
   if (rc) {
@@ -929,7 +934,8 @@ int p4a_batch_destroy(p4a_batch* b) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
-  if (b->lanes[1].stream) cudaStreamSynchronize(b->lanes[1].stream);
+  for (int q = 1; q < p4a_batch::kMaxLanes; q++)
+    if (b->lanes[q].stream) cudaStreamSynchronize(b->lanes[q].stream);
   drop_graphs(b);
   drop_profile_events(b);
   for (void* p : b->allocs) cudaFree(p);
@@ -942,9 +948,11 @@ int p4a_batch_destroy(p4a_batch* b) {
       if (Ln.stagingDone[k]) cudaEventDestroy(Ln.stagingDone[k]);
     }
   }
-  if (b->lanes[1].stream) cudaStreamDestroy(b->lanes[1].stream);
+  for (int q = 1; q < p4a_batch::kMaxLanes; q++)
+    if (b->lanes[q].stream) cudaStreamDestroy(b->lanes[q].stream);
   if (b->laneFork) cudaEventDestroy(b->laneFork);
-  if (b->laneJoin) cudaEventDestroy(b->laneJoin);
+  for (auto e : b->laneJoin)
+    if (e) cudaEventDestroy(e);
   if (b->upStream) cudaStreamDestroy(b->upStream);
   if (b->h2dStream) cudaStreamDestroy(b->h2dStream);
   if (b->d2hStream) cudaStreamDestroy(b->d2hStream);
@@ -960,7 +968,7 @@ int p4a_batch_set_stream(p4a_batch* b, void* stream) {
   if (!b) return P4A_ERR_ARG;
   cudaSetDevice(b->device);
   BTRY(b, cudaStreamSynchronize(b->stream));
-  BTRY(b, cudaStreamSynchronize(b->lanes[1].stream));
+  for (int q = 1; q < p4a_batch::kMaxLanes; q++) BTRY(b, cudaStreamSynchronize(b->lanes[q].stream));
   drop_graphs(b);
   if (stream) {
     if (b->ownStream) cudaStreamDestroy(b->stream);
@@ -1077,7 +1085,8 @@ int p4a_batch_step(p4a_batch* b, const int32_t* ids, int32_t count, double frame
 }
 
 int p4a_batch_set_lanes(p4a_batch* b, int32_t lanes, int64_t min_particles) {
-  if (!b || lanes < 1 || lanes > 2 || min_particles < 0) return bfail(b, P4A_ERR_ARG, "p4a_batch_set_lanes: bad value");
+  if (!b || lanes < 1 || lanes > p4a_batch::kMaxLanes || min_particles < 0)
+    return bfail(b, P4A_ERR_ARG, "p4a_batch_set_lanes: bad value");
   b->laneCount = lanes;
   b->laneMinParticles = min_particles;
   return P4A_OK;
@@ -1252,7 +1261,8 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
   // 6 M-particle mix: 391, 407, 417, 421 M particle-substeps/s end to end with 2, 4,
   // 6, 8 groups). With one lane each split adds the launch tails of a whole frame (a
   // frame split in two took 6 % longer, in four 18 %): two groups from 3 M up, else one.
-  const bool lanes2 = b->laneCount == 2 && !b->prof;
+  const int nLanes = b->prof ? 1 : b->laneCount;
+  const bool lanes2 = nLanes >= 2;
   int G = groups > 0 ? groups
                      : lanes2 ? (int)std::min<int64_t>(8, std::max<int64_t>(1, total / 750000))
                               : (total >= 3000000 ? 2 : 1);
@@ -1315,7 +1325,7 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
   // with two lanes, odd groups run on lane 1, so that consecutive groups' frames run
   // at once; profiled frames stay on lane 0
   auto frame = [&](int g) -> int {
-    b->lane = &b->lanes[lanes2 ? (g & 1) : 0];
+    b->lane = &b->lanes[g % nLanes];
     cudaStream_t fs = b->lane->stream;
     // group g's frame waits for its own writes only
     BTRY(b, cudaStreamWaitEvent(fs, ev[1 + 2 * g], 0));

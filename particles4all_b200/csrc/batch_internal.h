@@ -105,9 +105,9 @@ struct p4a_batch {
   // Frame lanes. A lane holds what its frames upload (params rows, items, segments,
   // through double-buffered pinned staging), their pull cursors, and the CUDA graphs
   // of the frame shapes (substeps and iterations per substep), captured with the
-  // lane's table addresses. Lane 0 runs on the batch's stream, lane 1 on a stream of
-  // its own: p4a_batch_step splits a large frame into two halves that run at once,
-  // so that the launch tails of one half overlap the work of the other.
+  // lane's table addresses. Lane 0 runs on the batch's stream, every other lane on a
+  // stream of its own: p4a_batch_step splits a large frame into parts that run at
+  // once, one per lane, so that the launch tails of one part overlap the others' work.
   struct Lane {
     cudaStream_t stream = nullptr;       // lane 0: the batch's stream
     p4a::SimParams* dParams = nullptr;   // [kMaxSubsteps][max_scenes], row k = the frame's k-th scene
@@ -122,11 +122,13 @@ struct p4a_batch {
     int stagingIdx = 0;
     std::map<std::vector<int>, cudaGraphExec_t> graphs;
   };
-  Lane lanes[2];
+  static constexpr int kMaxLanes = 4;
+  Lane lanes[kMaxLanes];
   Lane* lane = &lanes[0];          // the lane the next frame runs on
   int laneCount = 2;               // p4a_batch_set_lanes
   int64_t laneMinParticles = 1000000;
-  cudaEvent_t laneFork = nullptr, laneJoin = nullptr;
+  cudaEvent_t laneFork = nullptr;
+  cudaEvent_t laneJoin[kMaxLanes] = {};
   bool useGraphs = true;
   cudaStream_t upStream = nullptr;  // admissions' uploads (serving loop)
   // p4a_batch_step_io: a stream per copy direction and the events that order the

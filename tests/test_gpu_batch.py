@@ -67,9 +67,9 @@ def assert_same(sim, batch, sid):
     assert sim.get_stats()["raw"] == batch.stats(sid)["raw"]
 
 
-@pytest.mark.parametrize("graphs,lanes", [(True, 1), (False, 1), (True, 2), (False, 2)])
+@pytest.mark.parametrize("graphs,lanes", [(True, 1), (False, 1), (True, 2), (False, 2), (True, 4)])
 def test_batch_equals_alone_bit_exact(graphs, lanes):
-    """lanes = 2 with no size threshold: every frame runs as two concurrent halves."""
+    """lanes > 1 with no size threshold: every frame runs as concurrent parts."""
     scenes = mixed_scenes()
     frames = [1 / 60] * 6 + [1 / 45, 1 / 90, 1 / 60]
     b = Batch(max_particles=200_000, max_cells=400_000, max_scenes=16, graphs=graphs)
@@ -200,7 +200,9 @@ def test_lanes_with_subsets_and_arena_reuse():
     assert_same(run_alone(p4, s4, [1 / 60]), b, sid)
     assert_same(run_alone(scenes[3][0], scenes[3][1], [1 / 60] * 3), b, ids[3])
     with pytest.raises(P4AError):
-        b.set_lanes(3, 0)
+        b.set_lanes(5, 0)
+    with pytest.raises(P4AError):
+        b.set_lanes(0, 0)
 
 
 def test_step_io_rejects_bad_lists():
