@@ -590,6 +590,9 @@ typedef struct p4a_server_config {
   int32_t plain;               /* 1 = plain per-scene stepping                      */
   int64_t upload_bytes;        /* pinned staging for scene uploads, default 1 GiB   */
   int64_t readback_bytes;      /* pinned staging for step readbacks, default 1 GiB  */
+  int32_t frame_lanes;         /* p4a_batch_set_lanes of the batched frames, 1-4,   */
+                               /* default 2 (0 = 1)                                  */
+  int64_t lane_min_particles;  /* frames split from this size on, default 1,000,000 */
 } p4a_server_config;
 enum { P4A_REQ_CREATE = 1, P4A_REQ_STEP = 2, P4A_REQ_DESTROY = 3 };
 typedef struct p4a_completion {

@@ -165,7 +165,8 @@ class BatchIO(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("arenas", BatchConfig), ("builder_threads", C.c_int32), ("max_frames_in_flight", C.c_int32),
                 ("admit_timeout", C.c_double), ("max_pending_creates", C.c_int32), ("use_graphs", C.c_int32),
-                ("plain", C.c_int32), ("upload_bytes", C.c_int64), ("readback_bytes", C.c_int64)]
+                ("plain", C.c_int32), ("upload_bytes", C.c_int64), ("readback_bytes", C.c_int64),
+                ("frame_lanes", C.c_int32), ("lane_min_particles", C.c_int64)]
 
 
 REQ_CREATE, REQ_STEP, REQ_DESTROY = 1, 2, 3

@@ -842,6 +842,8 @@ int p4a_server_default_config(p4a_server_config* c) {
   c->plain = 0;
   c->upload_bytes = 1LL << 30;
   c->readback_bytes = 1LL << 30;
+  c->frame_lanes = 2;
+  c->lane_min_particles = 1000000;
   return P4A_OK;
 }
 
@@ -861,6 +863,7 @@ int p4a_server_create(int device, const p4a_server_config* cfg, p4a_server** out
   if (!cfg->plain) {
     if ((rc = p4a_batch_create(device, &cfg->arenas, &S->batch))) return rc;
     p4a_batch_use_graphs(S->batch, cfg->use_graphs);
+    if ((rc = p4a_batch_set_lanes(S->batch, std::max(1, cfg->frame_lanes), cfg->lane_min_particles))) return rc;
     S->stream = S->batch->stream;
     if (cudaStreamCreateWithFlags(&S->up, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&S->upEvent, cudaEventDisableTiming) != cudaSuccess) {

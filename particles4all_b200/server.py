@@ -60,7 +60,8 @@ def arenas_for_budget(budget_bytes, max_scenes=4096):
 class Server:
     def __init__(self, device=0, budget_bytes=None, arenas=None, plain=False, builder_threads=4,
                  max_frames_in_flight=2, admit_timeout=0.0, max_pending_creates=0, graphs=True,
-                 upload_bytes=1 << 30, readback_bytes=1 << 30, max_scenes=1024):
+                 upload_bytes=1 << 30, readback_bytes=1 << 30, max_scenes=1024, lanes=2,
+                 lane_min_particles=1_000_000):
         self._L = lib()
         cfg = _abi.ServerConfig()
         self._L.p4a_server_default_config(C.byref(cfg))
@@ -76,6 +77,8 @@ class Server:
         cfg.plain = 1 if plain else 0
         cfg.upload_bytes = int(upload_bytes)
         cfg.readback_bytes = int(readback_bytes)
+        cfg.frame_lanes = int(lanes)
+        cfg.lane_min_particles = int(lane_min_particles)
         self.config = {k: getattr(cfg, k) for k, _ in _abi.ServerConfig._fields_ if k != "arenas"}
         self.config["arenas"] = {k: getattr(cfg.arenas, k) for k, _ in _abi.BatchConfig._fields_}
         h = C.c_void_p()

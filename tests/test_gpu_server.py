@@ -68,12 +68,14 @@ def step_with_readback(srv, sid, outs, rows=20_000):
     return srv.step(sid, 1 / 60, pos_out=pos, vel_out=vel)
 
 
-def serve_mix(plain):
+def serve_mix(plain, lanes=2):
     sc = scenes()
     steps = 4
+    # lane_min_particles 0: with lanes > 1 every batched frame runs as concurrent parts
     srv = Server(arenas=dict(max_particles=100_000, max_cells=400_000, max_boundary=400_000, max_scenes=8,
                              max_bodies=64, max_body_parts=20_000),
-                 plain=plain, builder_threads=2, upload_bytes=64 << 20, readback_bytes=64 << 20)
+                 plain=plain, builder_threads=2, upload_bytes=64 << 20, readback_bytes=64 << 20,
+                 lanes=lanes, lane_min_particles=0)
     outs = {}
     reqs = set()
     # two scenes first; the others arrive while those are stepping
@@ -101,9 +103,9 @@ def serve_mix(plain):
     return sc, sids, n, outs, st
 
 
-@pytest.mark.parametrize("plain", [False, True])
-def test_served_equals_alone_bit_exact(plain):
-    sc, sids, n, outs, st = serve_mix(plain)
+@pytest.mark.parametrize("plain,lanes", [(False, 1), (False, 2), (True, 1)])
+def test_served_equals_alone_bit_exact(plain, lanes):
+    sc, sids, n, outs, st = serve_mix(plain, lanes)
     for (p, s), sid in zip(sc, sids):
         ref = alone(p, s, len(outs[sid]))
         for k, ((pos, vel), (rp, rv)) in enumerate(zip(outs[sid], ref)):
