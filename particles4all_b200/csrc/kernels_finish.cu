@@ -107,7 +107,7 @@ __device__ __forceinline__ void xsph_finalize_particle(const SimParams& P, const
     const float f = P.mass * (P.poly6 * t * t * t) / fmaxf(g.w, 0.5f * P.rho0);
     acc = fma3(f, sub3(xyz(g), vi), acc);
   };
-  walk_neighbours2(P, w, i, pi, pred, d.velRho, cs, d.nbList, cap, count, fluid);
+  walk_neighbours2<true>(P, w, i, pi, pred, d.velRho, cs, d.nbList, cap, count, fluid);
   const F3 corr = mul3(acc, P.xsphC);
   vf = add3(vi, corr);
   d.vel[L][i] = make_float4(vf.x, vf.y, vf.z, 0.0f);
@@ -198,7 +198,7 @@ __device__ __forceinline__ void tension_finalize_particle(const SimParams& P, co
     const float wgt = 2.0f * P.rho0 / (rho + g.w);
     acc = fma3(wgt, add3(fCoh, fCurv), acc);
   };
-  walk_neighbours2(P, w, i, pi, pred, d.normRho, cs, d.nbList, cap, count, fluid);
+  walk_neighbours2<true>(P, w, i, pi, pred, d.normRho, cs, d.nbList, cap, count, fluid);
   const float4 c0 = d.corr[i];
   const F3 cf = {fmaf(P.dt, acc.x, c0.x), fmaf(P.dt, acc.y, c0.y), fmaf(P.dt, acc.z, c0.z)};
   d.corr[i] = make_float4(cf.x, cf.y, cf.z, 0.0f);

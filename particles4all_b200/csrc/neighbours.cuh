@@ -357,7 +357,10 @@ __device__ __forceinline__ void walk_direct(const SimParams& P, const RowWalk& w
 // per-neighbour values), both loaded in the walk's two-deep pipeline so that
 // neither gather's latency is waited for in the pair's arithmetic; boundary
 // entries of a reused list are skipped. An overflowed list walks the direct loop.
-template <class FFluid>
+// PEEL: the loop runs only while a next entry exists and the last two entries are
+// visited after it (no per-entry tests of what is left, the pair term inlined three
+// times), measured faster in the block-form finalize passes and slower elsewhere.
+template <bool PEEL = false, class FFluid>
 __device__ __forceinline__ void walk_neighbours2(const SimParams& P, const RowWalk& w, uint32_t i, F3 pi,
                                                  const float4* __restrict__ pred,
                                                  const float4* __restrict__ gsrc,
@@ -376,6 +379,36 @@ __device__ __forceinline__ void walk_neighbours2(const SimParams& P, const RowWa
   const uint32_t* __restrict__ at = list + i;  // entry k of the particle at list[k * cap + i]
   uint32_t e0 = __ldg(at);
   float4 q0 = __ldg(pred + slot(e0)), g0 = __ldg(gsrc + slot(e0));
+  if constexpr (PEEL) {
+    uint32_t e1 = 0u;
+    if (count > 1u) {
+      at += cap;
+      e1 = __ldg(at);
+    }
+    auto visit = [&](uint32_t cur, float4 qc, float4 gc) {
+      if ((cur & kBoundTag) == 0u) fluid(cur, qc, gc);
+    };
+    for (uint32_t k = 1; k + 1 < count; k++) {
+      const uint32_t cur = e0;
+      const float4 qc = q0, gc = g0;
+      e0 = e1;
+      q0 = __ldg(pred + slot(e1));
+      g0 = __ldg(gsrc + slot(e1));
+      at += cap;
+      e1 = __ldg(at);
+      visit(cur, qc, gc);
+    }
+    if (count > 1u) {
+      const uint32_t cur = e0;
+      const float4 qc = q0, gc = g0;
+      e0 = e1;
+      q0 = __ldg(pred + slot(e1));
+      g0 = __ldg(gsrc + slot(e1));
+      visit(cur, qc, gc);
+    }
+    visit(e0, q0, g0);
+    return;
+  }
   at += cap;
   uint32_t e1 = count > 1u ? __ldg(at) : 0u;
   for (uint32_t k = 1; k <= count; k++) {
