@@ -307,14 +307,15 @@ __device__ __forceinline__ void walk_list(const uint32_t* __restrict__ list, uin
       visit(cur, qc);
     }
   } else {
-    for (uint32_t k = 1; k <= count; k++) {
+    // one entry ahead; the loop runs while a next entry exists, the last entry is
+    // visited after it
+    for (uint32_t k = 1; k < count; k++) {
       const uint32_t cur = e0;
-      if (k < count) {
-        at += cap;
-        e0 = __ldg(at);
-      }
+      at += cap;
+      e0 = __ldg(at);
       visit(cur, fetch(cur));
     }
+    visit(e0, fetch(e0));
   }
 }
 
