@@ -1254,18 +1254,18 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
     total += b->scenes[io[k].scene_id].n;
   }
   if (count == 0) return P4A_OK;
-  // groups of about equal particle counts, in list order. By default, with two frame
-  // lanes, one group per 750 k particles (at most 8): consecutive groups run at once
-  // on the two lanes, so a group's launch tails overlap the other lane's work and
-  // only the first group's writes and the last groups' reads stay exposed (on the
-  // 6 M-particle mix: 391, 407, 417, 421 M particle-substeps/s end to end with 2, 4,
-  // 6, 8 groups). With one lane each split adds the launch tails of a whole frame (a
-  // frame split in two took 6 % longer, in four 18 %): two groups from 3 M up, else one.
+  // groups of about equal particle counts, in list order; group g runs on lane
+  // g mod lanes. By default, with two or more frame lanes, one group per 750 k
+  // particles (at most 8): consecutive groups run at once on different lanes, so a
+  // group's launch tails overlap the other lanes' work and only the first group's
+  // writes and the last groups' reads stay exposed (on the 6 M-particle mix with two
+  // lanes: 391, 407, 417, 421 M particle-substeps/s end to end with 2, 4, 6, 8
+  // groups). With one lane each split adds the launch tails of a whole frame (a frame
+  // split in two took 6 % longer, in four 18 %): two groups from 3 M up, else one.
   const int nLanes = b->prof ? 1 : b->laneCount;
-  const bool lanes2 = nLanes >= 2;
   int G = groups > 0 ? groups
-                     : lanes2 ? (int)std::min<int64_t>(8, std::max<int64_t>(1, total / 750000))
-                              : (total >= 3000000 ? 2 : 1);
+                     : nLanes > 1 ? (int)std::min<int64_t>(8, std::max<int64_t>(1, total / 750000))
+                                  : (total >= 3000000 ? 2 : 1);
   G = std::min(G, std::min(count, 64));
   std::vector<int> first((size_t)G + 1, count);
   first[0] = 0;
@@ -1322,8 +1322,8 @@ int p4a_batch_step_io(p4a_batch* b, const p4a_batch_io* io, int32_t count, doubl
     return P4A_OK;
   };
   std::vector<int32_t> ids;
-  // with two lanes, odd groups run on lane 1, so that consecutive groups' frames run
-  // at once; profiled frames stay on lane 0
+  // group g on lane g mod lanes, so that consecutive groups' frames run at once;
+  // profiled frames stay on lane 0
   auto frame = [&](int g) -> int {
     b->lane = &b->lanes[g % nLanes];
     cudaStream_t fs = b->lane->stream;
