@@ -97,7 +97,8 @@ def interleaved(step, profile, L, kernel, name, variants, rounds):
             if name in prof:
                 ms[q] += prof[name][0]
                 launches[q] += prof[name][1]
-    return [m / max(1, n) for m, n in zip(ms, launches)]
+    # a shape whose frames launched the kernel never is not a candidate
+    return [m / n if n else float("inf") for m, n in zip(ms, launches)]
 
 
 def _sim_profile(sim, aniso):
