@@ -190,6 +190,17 @@ def test_batched_tuning_tables_fall_back_to_the_plain_ones(built):
         from particles4all_b200 import autotune
         autotune.load()
 
+def test_server_default_config(built):
+    """p4a_server_default_config (host only): the documented defaults, frame lanes
+    included."""
+    L = _lib.lib()
+    cfg = _abi.ServerConfig()
+    assert L.p4a_server_default_config(C.byref(cfg)) == 0
+    assert (cfg.frame_lanes, cfg.lane_min_particles) == (2, 1_000_000)
+    assert (cfg.builder_threads, cfg.max_frames_in_flight, cfg.use_graphs, cfg.plain) == (4, 2, 1, 0)
+    assert cfg.upload_bytes == cfg.readback_bytes == 1 << 30
+
+
 def test_batch_footprint_sizes_server_arenas(built):
     """p4a_batch_footprint counts the arenas p4a_batch_create would allocate (no
     device needed), and the serving loop's arena sizing stays within its budget."""
@@ -200,9 +211,10 @@ def test_batch_footprint_sizes_server_arenas(built):
     assert L.p4a_batch_footprint(C.byref(cfg), C.byref(out)) == _abi.P4A_ERR_ARG
     small, big = server._arenas(1 << 16, 64), server._arenas(1 << 17, 64)
     fs, fb = server.arena_bytes(small), server.arena_bytes(big)
-    # per particle slot at least the ten float4 ping-pong arrays, the solver arrays
-    # and the two pairs of nine-row neighbour masks (u64 + u32 each)
-    assert (fb - fs) / (1 << 16) >= 160 + 44 + 2 * 9 * 12
+    # per particle slot at least the ten float4 ping-pong arrays, six float4 solver
+    # arrays (corr, normal, start positions, packed gathers), seven 4-byte ones and
+    # the neighbour list (96 entries of 4 B)
+    assert (fb - fs) / (1 << 16) >= 160 + 6 * 16 + 7 * 4 + 96 * 4
     for budget in (1 << 30, 8 << 30, 160_000_000_000):
         a = server.arenas_for_budget(budget, 4096)
         assert server.arena_bytes(a) <= budget
